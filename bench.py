@@ -1,0 +1,419 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 linear-octree neighbour search.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+Workload: a 10,000,000-point synthetic airborne-LiDAR tile (1.5 km x 1.5 km,
+seed 1, terrain + canopy cylinders), Hilbert keys, 64 points per leaf.  The
+cloud is uploaded, SFC-sorted and its octree built on the device (timed as the
+build, in Mpts/s), then every step answers one batch of queries at random
+cloud points: 500,000 radius searches (sphere kernel, neighborsPrune, r = 2.5 m,
+full CSR output) and 500,000 kNN searches (k = 50).  ``value`` is queries/s
+over the whole job (all ranks); the step's inputs are resident in HBM and L2
+is flushed before every step.  ``e2e`` is the same step through the host-buffer
+form of the C ABI (centres copied in from pinned memory, every result copied
+out).  With N GPUs every rank holds its own replica of the cloud and its own
+queries (weak scaling, no collective on the data path).
+
+``--impl reference`` times the reference's own CPU implementation (the
+reference headers compiled by ``make -C oracle ref``; the oracle's C
+restatement if that library is absent) on a bounded sample of the same query
+mix with every host thread, on rank 0 only.
+"""
+from __future__ import annotations
+
+import argparse
+import ctypes as C
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "queries/s & build Mpts/s at 10M pts, batched vs plain GPU; p99 serve latency"
+N_POINTS = 10_000_000
+TILE_M = 1500.0
+SEED = 1
+ENCODER = 5
+MAX_LEAF = 64
+RADIUS = 2.5
+KNN_K = 50
+Q_RADIUS = 500_000
+Q_KNN = 500_000
+L2_FLUSH_BYTES = 512 << 20
+BUILD_BYTES_PER_POINT = 112  # encode 32 + sort 20 + reorder 52 + leaf counting 8
+BUILD_BYTES_PER_NODE = 36    # offsets 4 + ranges 8 + centers 24
+
+
+def measured_peak():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def workload_config(world: int, extra=None):
+    cfg = {
+        "workload": f"{N_POINTS // 1_000_000}M-point synthetic LiDAR tile ({TILE_M / 1000:g} km, seed {SEED}), "
+                    f"Hilbert keys, leaf {MAX_LEAF}; per step {Q_RADIUS} radius queries (sphere, neighborsPrune, "
+                    f"r={RADIUS} m, CSR output) + {Q_KNN} kNN queries (k={KNN_K}) at random cloud points",
+        "n_points": N_POINTS,
+        "queries_per_step": Q_RADIUS + Q_KNN,
+        "parallelism": f"replicas x{world}" if world > 1 else "single",
+        "l2": "flushed (512 MB write) before every timed step; cloud coordinates 240 MB > L2",
+        "data": "synthetic stand-in for the reference's LiDAR clouds (not available offline)",
+    }
+    if extra:
+        cfg.update(extra)
+    return cfg
+
+
+# ------------------------------------------------------------------ clocks ---
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix=".csv")
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(self.gpu), "-f", self.path], stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        rows = []
+        try:
+            with open(self.path) as f:
+                for ln in f:
+                    p = [x.strip() for x in ln.split(",")]
+                    if len(p) >= 9:
+                        rows.append(p)
+        finally:
+            os.unlink(self.path)
+        if not rows:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["no samples"]}
+        sm = [float(r[1]) for r in rows if r[1].replace(".", "").isdigit()]
+        mx = [float(r[2]) for r in rows if r[2].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for r in rows for i in range(4) if r[5 + i].lower() == "active"})
+        load = [s for s in sm if s > 0.5 * (max(sm) if sm else 0)]
+        return {"sm_mhz": statistics.median(load) if load else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": reasons, "samples": len(rows)}
+
+
+# ---------------------------------------------------------- CPU baselines ---
+def cpu_arm(xyz, threads: int, target_s: float = 10.0):
+    """Time the reference CPU implementation on a bounded sample of the query mix.
+    Returns a dict describing the baseline and a function running one sample."""
+    from octrees_benchmark_b200.synth import query_indices
+    from oracle import oracle as orc
+
+    if orc.reference_available():
+        R = orc.Reference(ENCODER, xyz, MAX_LEAF, threads=threads)
+        kind = "reference"
+        sxyz = R.points()[0]
+        cores = R.max_threads() if threads <= 0 else threads
+
+        def run(qr, qk):
+            tr, _ = R.time_radius(1, 2, qr, RADIUS, threads)
+            tk, _ = R.time_knn(qk, KNN_K, threads)
+            return tr, tk
+    else:
+        P = orc.Port()
+        keys, perm, box, sxyz = P.encode_sort(ENCODER, xyz)
+        T = P.build(ENCODER, keys, MAX_LEAF, box)
+        kind = "port"
+        cores = os.cpu_count()
+
+        def run(qr, qk):
+            t0 = time.perf_counter()
+            T.radius(sxyz, 1, 2, qr, RADIUS)
+            t1 = time.perf_counter()
+            T.knn(sxyz, qk, KNN_K)
+            return t1 - t0, time.perf_counter() - t1
+    # calibrate the sample so that one run is about target_s / 2 of CPU work
+    cal = 4000
+    q = sxyz[query_indices(2 * cal, len(sxyz), seed=99)]
+    tr, tk = run(q[:cal], q[cal:])
+    per_q = (tr + tk) / (2 * cal)
+    m = int(max(cal, min(Q_RADIUS, target_s / 2 / max(per_q, 1e-9) / 2)))
+    sample = sxyz[query_indices(2 * m, len(sxyz), seed=98)]
+    return dict(kind=kind, cores=int(cores), sample_per_kind=m, run=run, sample=sample)
+
+
+def run_reference_arm(args, rank, world):
+    if rank != 0:
+        return 0
+    from octrees_benchmark_b200.synth import lidar_tile
+
+    xyz = lidar_tile(N_POINTS, TILE_M, SEED)
+    arm = cpu_arm(xyz, threads=0, target_s=args.cpu_seconds)
+    m = arm["sample_per_kind"]
+    q = arm["sample"]
+    for _ in range(args.warmup):
+        arm["run"](q[:m], q[m:])
+    times = []
+    for _ in range(args.steps):
+        tr, tk = arm["run"](q[:m], q[m:])
+        times.append(tr + tk)
+    total = sum(times)
+    value = 2 * m * args.steps / total
+    line = {
+        "metric": METRIC, "value": value, "unit": "queries/s", "impl": "reference", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+        "config": workload_config(1, {"sample": f"{m} radius + {m} kNN queries per step (bounded CPU sample)"}),
+        "cpu_baseline": {"value": value, "unit": "queries/s", "cores": arm["cores"], "kind": arm["kind"],
+                         "sample": f"{m} radius + {m} kNN queries of the same mix per step"},
+        "e2e": {"value": value, "unit": "queries/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+# --------------------------------------------------------------- B200 arm ---
+def run_b200(args, rank, world, local_rank):
+    import torch
+
+    from octrees_benchmark_b200 import capi
+    from octrees_benchmark_b200.synth import lidar_tile
+
+    L = capi.lib()
+    dev = local_rank
+    torch.cuda.set_device(dev)
+    stream = torch.cuda.Stream()
+    xyz_h = lidar_tile(N_POINTS, TILE_M, SEED)
+    xyz_d = torch.from_numpy(xyz_h).cuda()
+    p = capi.OctParams(MAX_LEAF, ENCODER, dev, 0)
+    h = C.c_void_p()
+    capi.check(L.oct_cloud_create(C.byref(p), C.byref(h)), None, "create")
+    capi.check(L.oct_cloud_set_stream(h, C.c_void_p(stream.cuda_stream)), h)
+    capi.check(L.oct_set_radius_group(h, args.radius_group), h)
+    info = capi.OctTreeInfo()
+    MD = capi.OCT_MEM_DEVICE
+
+    # ---- build: upload (device to device) + encode + sort + reorder + octree ----
+    def build_once():
+        capi.check(L.oct_set_points(h, xyz_d.data_ptr(), N_POINTS, MD), h, "set_points")
+        capi.check(L.oct_encode_sort(h, None, None, None, None, MD), h, "encode_sort")
+        capi.check(L.oct_build(h, C.byref(info)), h, "build")
+
+    for _ in range(max(1, args.warmup)):
+        build_once()
+    torch.cuda.synchronize()
+    bt = []
+    for _ in range(args.steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        build_once()
+        torch.cuda.synchronize()
+        bt.append(time.perf_counter() - t0)
+    build_s = statistics.median(bt)
+
+    # sorted cloud on the device, query centres = random cloud points
+    sorted_xyz = torch.empty((N_POINTS, 3), dtype=torch.float64, device="cuda")
+    capi.check(L.oct_encode_sort(h, None, None, None, sorted_xyz.data_ptr(), MD), h)
+    capi.check(L.oct_build(h, C.byref(info)), h)
+    torch.cuda.synchronize()
+    gen = torch.Generator(device="cuda")
+    n_batches = args.steps + args.warmup
+    batches = []
+    for b in range(n_batches):
+        gen.manual_seed(1000 * rank + b)
+        ir = torch.randint(0, N_POINTS, (Q_RADIUS,), device="cuda", generator=gen)
+        ik = torch.randint(0, N_POINTS, (Q_KNN,), device="cuda", generator=gen)
+        batches.append((sorted_xyz[ir].contiguous(), sorted_xyz[ik].contiguous()))
+    offs = torch.zeros(Q_RADIUS + 1, dtype=torch.int64, device="cuda")
+    tot = C.c_uint64()
+    st = L.oct_radius_search(h, 1, 2, batches[0][0].data_ptr(), Q_RADIUS, None, RADIUS, offs.data_ptr(), None, 0,
+                             C.byref(tot), MD)
+    assert st in (capi.OCT_OK, capi.OCT_ERR_CAPACITY)
+    cap = int(tot.value * 1.5) + 1024
+    idx_out = torch.empty(cap, dtype=torch.int32, device="cuda")
+    kidx = torch.empty((Q_KNN, KNN_K), dtype=torch.int32, device="cuda")
+    kd2 = torch.empty((Q_KNN, KNN_K), dtype=torch.float64, device="cuda")
+    kcnt = torch.empty(Q_KNN, dtype=torch.int32, device="cuda")
+    flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+
+    def step(b, timed):
+        qr, qk = batches[b]
+        with torch.cuda.stream(stream):
+            flush.zero_()
+            ev[0].record(stream)
+            capi.check(L.oct_radius_count(h, 1, 2, qr.data_ptr(), Q_RADIUS, None, RADIUS, offs.data_ptr(), MD), h)
+            ev[1].record(stream)
+            capi.check(L.oct_radius_search(h, 1, 2, qr.data_ptr(), Q_RADIUS, None, RADIUS, offs.data_ptr(),
+                                           idx_out.data_ptr(), cap, C.byref(tot), MD), h, "radius_search")
+            ev[2].record(stream)
+            capi.check(L.oct_knn(h, qk.data_ptr(), Q_KNN, KNN_K, kidx.data_ptr(), kd2.data_ptr(), kcnt.data_ptr(),
+                                 MD), h, "knn")
+            ev[3].record(stream)
+        stream.synchronize()
+        return ev[0].elapsed_time(ev[1]), ev[1].elapsed_time(ev[2]), ev[2].elapsed_time(ev[3]), int(tot.value)
+
+    for b in range(args.warmup):
+        step(b, False)
+    if world > 1:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    clocks = ClockSampler(int(os.environ.get("CUDA_VISIBLE_DEVICES", str(dev)).split(",")[0])
+                          if os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",")[0].isdigit() else dev)
+    clocks.start()
+    t_count = t_search = t_knn = 0.0
+    nbrs = 0
+    for s in range(args.steps):
+        a, b_, c, tt = step(args.warmup + s, True)
+        t_count += a
+        t_search += b_
+        t_knn += c
+        nbrs += tt
+    torch.cuda.synchronize()
+    if world > 1:
+        torch.distributed.barrier()
+    clk = clocks.stop()
+    step_ms = (t_search + t_knn) / args.steps  # the count-only call is a separate measurement
+    tmax = torch.tensor([step_ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        torch.distributed.all_reduce(tmax, op=torch.distributed.ReduceOp.MAX)
+    step_ms_max = float(tmax.item())
+    value = world * (Q_RADIUS + Q_KNN) / (step_ms_max / 1e3)
+
+    # ---- e2e through the host-buffer ABI (pinned buffers, copies in the timed region) ----
+    e2e_val = None
+    h2d = d2h = 0
+    if not args.no_e2e:
+        qrh = torch.empty((Q_RADIUS, 3), dtype=torch.float64).pin_memory().numpy()
+        qkh = torch.empty((Q_KNN, 3), dtype=torch.float64).pin_memory().numpy()
+        offs_h = torch.empty(Q_RADIUS + 1, dtype=torch.int64).pin_memory().numpy()
+        idx_h = torch.empty(cap, dtype=torch.int32).pin_memory().numpy()
+        kidx_h = torch.empty((Q_KNN, KNN_K), dtype=torch.int32).pin_memory().numpy()
+        kd2_h = torch.empty((Q_KNN, KNN_K), dtype=torch.float64).pin_memory().numpy()
+        kcnt_h = torch.empty(Q_KNN, dtype=torch.int32).pin_memory().numpy()
+        et = []
+        for s in range(args.warmup + args.steps):
+            qr, qk = batches[s]
+            qrh[:] = qr.cpu().numpy()
+            qkh[:] = qk.cpu().numpy()
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            capi.check(L.oct_radius_search(h, 1, 2, qrh.ctypes.data, Q_RADIUS, None, RADIUS, offs_h.ctypes.data,
+                                           idx_h.ctypes.data, cap, C.byref(tot), 0), h, "e2e radius")
+            capi.check(L.oct_knn(h, qkh.ctypes.data, Q_KNN, KNN_K, kidx_h.ctypes.data, kd2_h.ctypes.data,
+                                 kcnt_h.ctypes.data, 0), h, "e2e knn")
+            t1 = time.perf_counter()
+            if s >= args.warmup:
+                et.append(t1 - t0)
+                h2d = 24 * (Q_RADIUS + Q_KNN)
+                d2h = 8 * (Q_RADIUS + 1) + 4 * int(tot.value) + Q_KNN * KNN_K * 12 + 4 * Q_KNN
+        e2e_t = torch.tensor([sum(et) / len(et)], dtype=torch.float64, device="cuda")
+        if world > 1:
+            torch.distributed.all_reduce(e2e_t, op=torch.distributed.ReduceOp.MAX)
+        e2e_val = world * (Q_RADIUS + Q_KNN) / float(e2e_t.item())
+
+    # ---- roofline of the dominant kernel ----
+    peak, peak_kind = measured_peak()
+    avg_nbrs = nbrs / args.steps / Q_RADIUS
+    rad_bytes = 24 * Q_RADIUS + 28 * (nbrs / args.steps)
+    knn_bytes = (24 + 36 * KNN_K) * Q_KNN
+    rad_ms = t_search / args.steps
+    knn_ms = t_knn / args.steps
+    rad = {"kernel": "radius neighborsPrune sphere (count + scan + fill)", "ms": rad_ms,
+           "achieved": rad_bytes / (rad_ms / 1e3) / 1e9}
+    knn = {"kernel": "kNN k=50 (k_knn)", "ms": knn_ms, "achieved": knn_bytes / (knn_ms / 1e3) / 1e9}
+    dom = knn if knn_ms >= rad_ms else rad
+    roofline = {"bound": "hbm", "kernel": dom["kernel"], "achieved": dom["achieved"], "peak": peak, "unit": "GB/s",
+                "frac": dom["achieved"] / peak, "peak_source": peak_kind, "traffic": None,
+                "algorithmic_bytes": "radius 24 + 28 per neighbour; kNN 24 + 36 k per query"}
+    build_bytes = BUILD_BYTES_PER_POINT * N_POINTS + BUILD_BYTES_PER_NODE * info.n_total
+    build = {"ms": 1e3 * build_s, "mpts_s": N_POINTS / build_s / 1e6, "gbs": build_bytes / build_s / 1e9,
+             "frac": build_bytes / build_s / 1e9 / peak, "nodes": info.n_total, "leaves": info.n_leaf,
+             "depth": info.max_depth_seen, "includes": "upload (D2D) + bbox + encode + 8-bit onesweep sort + "
+                                                        "reorder + octree build, host syncs included"}
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu:
+        arm = cpu_arm(xyz_h, threads=0, target_s=args.cpu_seconds)
+        m = arm["sample_per_kind"]
+        tr, tk = arm["run"](arm["sample"][:m], arm["sample"][m:])
+        cpu = {"value": 2 * m / (tr + tk), "unit": "queries/s", "cores": arm["cores"], "kind": arm["kind"],
+               "sample": f"{m} radius (sphere, neighborsPrune, r={RADIUS}) + {m} kNN (k={KNN_K}) queries at random "
+                         f"points of the same 10M cloud, all host threads",
+               "radius_qps": m / tr, "knn_qps": m / tk}
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": "queries/s", "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": step_ms_max, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": workload_config(world, {"radius_group": args.radius_group, "path": "plain fp64"}),
+            "radius_qps": world * Q_RADIUS / (rad_ms / 1e3), "knn_qps": world * Q_KNN / (knn_ms / 1e3),
+            "radius_count_only_ms": t_count / args.steps, "avg_neighbours": avg_nbrs,
+            "build": build, "roofline": roofline, "cpu_baseline": cpu,
+            "e2e": {"value": e2e_val, "unit": "queries/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "gpu_launches": 6 * args.steps, "clocks": clk,
+        }
+        print(json.dumps(line), flush=True)
+    L.oct_cloud_destroy(h)
+    return 0
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=5)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    ap.add_argument("--radius-group", type=int, default=8)
+    ap.add_argument("--cpu-seconds", type=float, default=10.0)
+    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-e2e", action="store_true")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        return run_reference_arm(args, rank, world)
+    if world > 1:
+        import datetime
+
+        import torch
+
+        torch.cuda.set_device(local_rank)
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    try:
+        return run_b200(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch
+
+            torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    sys.exit(main())

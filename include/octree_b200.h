@@ -1,0 +1,170 @@
+/*
+ * octree_b200.h - C ABI of the B200 linear-octree neighbour search.
+ *
+ * A drop-in device implementation of the point-cloud neighbour-search path of
+ * derivada/octrees-benchmark: Morton/Hilbert 63-bit SFC keys, a stable key sort
+ * that reorders the points, the cornerstone linear octree, radius search with
+ * the sphere / cube / square / circle kernels through neighbors,
+ * neighborsPrune and neighborsStruct, and kNN.  Results are bitwise those of
+ * the reference: the same keys, sort order and octree arrays, the same
+ * neighbour index sets, and the same kNN squared distances (ties at the k-th
+ * distance resolved by the lowest point index).
+ *
+ * The reference has no FFI; its interface is the C++ template API that these
+ * entry points replace (file:line in the reference tree is given per function).
+ * A header-only C++ wrapper with the reference's method names sits on top of
+ * this ABI (octrees_benchmark_b200/csrc/linear_octree_gpu.hpp).
+ *
+ * Conventions
+ *  - Every function returns an oct_status; none exits or throws.
+ *  - Points and query centres are xyz triples of doubles (AoS, 3 per point).
+ *  - Point indices returned by searches index the SFC-sorted cloud, as in the
+ *    reference (the points are reordered in place by sortPoints).
+ *  - Buffers are host memory unless OCT_MEM_DEVICE is passed, in which case
+ *    every pointer argument of that call is device memory of the cloud's
+ *    device; host-memory calls synchronise the cloud's stream before they
+ *    return, device-memory calls that do not need a readback return without
+ *    waiting.
+ *  - One cloud is used by one host thread at a time; different clouds are
+ *    independent and may be used concurrently.
+ */
+#ifndef OCTREE_B200_H
+#define OCTREE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define OCT_ABI_VERSION 1
+
+typedef enum {
+    OCT_OK = 0,
+    OCT_ERR_INVALID_ARG = 1,   /* bad pointer, size, enum value */
+    OCT_ERR_CUDA = 2,          /* a CUDA call failed (see oct_last_error) */
+    OCT_ERR_OUT_OF_MEMORY = 3, /* a device allocation failed */
+    OCT_ERR_STATE = 4,         /* call out of order (e.g. search before build) */
+    OCT_ERR_CAPACITY = 5,      /* caller's output buffer too small; the needed size is returned */
+    OCT_ERR_DEVICE_LIMIT = 6,  /* a bounded device loop hit its limit (stack, spin) */
+    OCT_ERR_NO_DEVICE = 7      /* no usable CUDA device */
+} oct_status;
+
+/* Encoders: the reference's EncoderType values (inc/main_options.hpp:73-83). */
+typedef enum { OCT_ENC_MORTON_3D = 1, OCT_ENC_HILBERT_3D = 5 } oct_encoder;
+
+/* Search kernels: the reference's Kernel_t values (inc/main_options.hpp:97-103). */
+typedef enum { OCT_KERNEL_CIRCLE = 0, OCT_KERNEL_SPHERE = 1, OCT_KERNEL_SQUARE = 2, OCT_KERNEL_CUBE = 3 } oct_kernel;
+
+/* Radius-search variants of LinearOctree (inc/structures/linear_octree.hpp):
+ * neighbors 796-816, neighborsPrune 746-784, neighborsStruct 695-736. */
+typedef enum { OCT_NEIGHBORS = 1, OCT_NEIGHBORS_PRUNE = 2, OCT_NEIGHBORS_STRUCT = 3 } oct_algo;
+
+#define OCT_MEM_DEVICE 0x1u /* every buffer of the call is device memory */
+
+typedef struct {
+    uint32_t max_points_leaf; /* mainOptions.maxPointsLeaf (main_options.hpp:210); default 128 */
+    int32_t encoder;          /* oct_encoder */
+    int32_t device;           /* CUDA device ordinal */
+    uint32_t flags;           /* reserved, 0 */
+} oct_params;
+
+typedef struct {
+    uint64_t n_points;
+    uint32_t n_leaf;         /* LinearOctree::nLeaf */
+    uint32_t n_internal;     /* LinearOctree::nInternal = (nLeaf - 1) / 7 */
+    uint32_t n_total;        /* LinearOctree::nTotal */
+    uint32_t max_depth_seen; /* LinearOctree::maxDepthSeen */
+} oct_tree_info;
+
+typedef struct oct_cloud_s* oct_cloud;
+
+/* Library version (OCT_ABI_VERSION) and a static description of a status. */
+int oct_abi_version(void);
+const char* oct_status_string(int status);
+
+/* Create / destroy a device-resident cloud.  Replaces constructing the
+ * reference's encoder (getEncoder, inc/encoding/point_encoder_factory.hpp:12)
+ * and setting mainOptions.maxPointsLeaf; nothing global is read. */
+int oct_cloud_create(const oct_params* params, oct_cloud* out);
+int oct_cloud_destroy(oct_cloud cloud);
+
+/* Run the cloud's work on this CUDA stream (cudaStream_t) instead of its own. */
+int oct_cloud_set_stream(oct_cloud cloud, void* cuda_stream);
+
+/* Last error message of the cloud (NUL-terminated, truncated to len). */
+int oct_last_error(oct_cloud cloud, char* buf, size_t len);
+
+/* Wait for the cloud's queued device work and report an error latched by a
+ * device-memory call that returned before its kernels ran.  No reference
+ * counterpart (the reference is synchronous). */
+int oct_synchronize(oct_cloud cloud);
+
+/* Lanes per query of the radius traversal: 8, 16 or 32 (4, 2 or 1 queries per
+ * warp); other values select the default (8).  No reference counterpart: the
+ * autotuner sets it. */
+int oct_set_radius_group(oct_cloud cloud, int lanes);
+
+/* Upload n points (xyz AoS).  Replaces filling the reference's PointsAoS
+ * container (inc/geometry/point_containers.hpp:32-65). */
+int oct_set_points(oct_cloud cloud, const double* xyz, uint64_t n, uint32_t flags);
+
+/* Bounding box, SFC keys, stable key sort and point reorder.  Replaces
+ * PointEncoder::sortPoints(points, meta) (inc/encoding/point_encoder.hpp:484-503):
+ * box12 (center xyz, radii xyz, min xyz, max xyz of the returned Box),
+ * keys (n sorted keys), perm (n: input position of each sorted point, the
+ * reference's Point::id), sorted_xyz (n x 3, the reordered points).  Any
+ * output may be NULL. */
+int oct_encode_sort(oct_cloud cloud, double* box12, uint64_t* keys, uint32_t* perm, double* sorted_xyz,
+                    uint32_t flags);
+
+/* Build the linear octree over the sorted cloud.  Replaces the
+ * LinearOctree(points, codes, box, enc) constructor
+ * (inc/structures/linear_octree.hpp:614-623, buildOctree 567-605). */
+int oct_build(oct_cloud cloud, oct_tree_info* info);
+
+/* Export the built tree: offsets (n_total + 1, first child or 0 for a leaf),
+ * ranges (n_total x 2: first, last point), centers (n_total x 3), radii
+ * (22 x 3, precomputedRadii), half (3, halfLengths).  Any output may be NULL.
+ * The arrays are LinearOctree's members of the same names
+ * (linear_octree.hpp:112-121, 140). */
+int oct_tree_export(oct_cloud cloud, uint32_t* offsets, uint64_t* ranges, double* centers, double* radii,
+                    double* half, uint32_t flags);
+
+/* Radius search for nq centres (xyz AoS).  radii: per-query radii (nq
+ * doubles) or NULL to use `radius` for every query.
+ * Replaces neighbors / neighborsPrune (linear_octree.hpp:1050-1087): the
+ * result is CSR, offsets (nq + 1) and point indices (offsets[nq] of them, each
+ * query's ascending).  If idx_capacity is smaller than the total, offsets and
+ * *total are still written and OCT_ERR_CAPACITY is returned.  For
+ * OCT_NEIGHBORS_STRUCT the indices are those of the expanded ranges. */
+int oct_radius_search(oct_cloud cloud, int kernel, int algo, const double* centers, uint64_t nq,
+                      const double* radii, double radius, uint64_t* offsets, uint32_t* idx, uint64_t idx_capacity,
+                      uint64_t* total, uint32_t flags);
+
+/* Neighbour counts only (the size() of each result), per query. */
+int oct_radius_count(oct_cloud cloud, int kernel, int algo, const double* centers, uint64_t nq, const double* radii,
+                     double radius, uint64_t* counts, uint32_t flags);
+
+/* neighborsStruct ranges (linear_octree.hpp:1038-1042, NeighborSet
+ * neighbor_set.hpp:16-90): CSR over half-open ranges, range_offsets (nq + 1)
+ * and pairs (first, last) in ascending order, exactly the ranges the reference
+ * adds (one per fully-inside node, including empty ones, and each maximal run
+ * of inside points of a leaf); point_counts (nq, may be NULL) is
+ * NeighborSet::numberOfPoints.  Capacity handling as oct_radius_search. */
+int oct_struct_search(oct_cloud cloud, int kernel, const double* centers, uint64_t nq, const double* radii,
+                      double radius, uint64_t* range_offsets, uint32_t* pairs, uint64_t pair_capacity,
+                      uint64_t* total_ranges, uint64_t* point_counts, uint32_t flags);
+
+/* k nearest neighbours of nq centres.  Replaces LinearOctree::knn
+ * (linear_octree.hpp:899-942): idx and d2 are nq x k, ascending by squared
+ * distance (ties by index); counts[q] = min(n, k); unused slots hold
+ * UINT32_MAX / +inf.  counts may be NULL. */
+int oct_knn(oct_cloud cloud, const double* centers, uint64_t nq, uint32_t k, uint32_t* idx, double* d2,
+            uint32_t* counts, uint32_t flags);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* OCTREE_B200_H */

@@ -1,0 +1,107 @@
+"""ctypes binding of the C ABI in include/octree_b200.h (liboctree_b200.so).
+
+Loading fails loudly when the library has not been built: there is no CPU
+fallback anywhere in this package.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+import re
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "liboctree_b200.so")
+HEADER = os.path.join(os.path.dirname(PKG), "include", "octree_b200.h")
+
+OCT_OK = 0
+OCT_ERR_INVALID_ARG = 1
+OCT_ERR_CUDA = 2
+OCT_ERR_OUT_OF_MEMORY = 3
+OCT_ERR_STATE = 4
+OCT_ERR_CAPACITY = 5
+OCT_ERR_DEVICE_LIMIT = 6
+OCT_ERR_NO_DEVICE = 7
+OCT_MEM_DEVICE = 0x1
+
+ENCODERS = {"morton": 1, "mort": 1, "hilbert": 5, "hilb": 5, 1: 1, 5: 5}
+KERNELS = {"circle": 0, "sphere": 1, "square": 2, "cube": 3, 0: 0, 1: 1, 2: 2, 3: 3}
+ALGOS = {"neighbors": 1, "neighborsPrune": 2, "prune": 2, "neighborsStruct": 3, "struct": 3, 1: 1, 2: 2, 3: 3}
+
+
+class OctParams(C.Structure):
+    _fields_ = [("max_points_leaf", C.c_uint32), ("encoder", C.c_int32), ("device", C.c_int32),
+                ("flags", C.c_uint32)]
+
+
+class OctTreeInfo(C.Structure):
+    _fields_ = [("n_points", C.c_uint64), ("n_leaf", C.c_uint32), ("n_internal", C.c_uint32),
+                ("n_total", C.c_uint32), ("max_depth_seen", C.c_uint32)]
+
+
+class OctError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(msg)
+        self.status = status
+
+
+_lib = None
+
+_vp = C.c_void_p
+_u64 = C.c_uint64
+_u32 = C.c_uint32
+_int = C.c_int
+_dbl = C.c_double
+
+SIGNATURES = {
+    "oct_abi_version": ([], _int),
+    "oct_status_string": ([_int], C.c_char_p),
+    "oct_cloud_create": ([C.POINTER(OctParams), C.POINTER(_vp)], _int),
+    "oct_cloud_destroy": ([_vp], _int),
+    "oct_cloud_set_stream": ([_vp, _vp], _int),
+    "oct_last_error": ([_vp, C.c_char_p, C.c_size_t], _int),
+    "oct_synchronize": ([_vp], _int),
+    "oct_set_radius_group": ([_vp, _int], _int),
+    "oct_set_points": ([_vp, _vp, _u64, _u32], _int),
+    "oct_encode_sort": ([_vp, _vp, _vp, _vp, _vp, _u32], _int),
+    "oct_build": ([_vp, C.POINTER(OctTreeInfo)], _int),
+    "oct_tree_export": ([_vp, _vp, _vp, _vp, _vp, _vp, _u32], _int),
+    "oct_radius_search": ([_vp, _int, _int, _vp, _u64, _vp, _dbl, _vp, _vp, _u64, C.POINTER(_u64), _u32], _int),
+    "oct_radius_count": ([_vp, _int, _int, _vp, _u64, _vp, _dbl, _vp, _u32], _int),
+    "oct_struct_search": ([_vp, _int, _vp, _u64, _vp, _dbl, _vp, _vp, _u64, C.POINTER(_u64), _vp, _u32], _int),
+    "oct_knn": ([_vp, _vp, _u64, _u32, _vp, _vp, _vp, _u32], _int),
+}
+
+
+def header_functions(path: str = HEADER) -> list[str]:
+    """Names of the functions declared in include/octree_b200.h."""
+    txt = open(path).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    return sorted(set(re.findall(r"\b(oct_[a-z_0-9]+)\s*\(", txt)))
+
+
+def lib() -> C.CDLL:
+    """The loaded device library; raises if it is missing (no fallback)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"{LIB_PATH} is not built; run `python -m octrees_benchmark_b200.build`")
+        L = C.CDLL(LIB_PATH)
+        for name, (args, res) in SIGNATURES.items():
+            fn = getattr(L, name)
+            fn.argtypes = args
+            fn.restype = res
+        _lib = L
+    return _lib
+
+
+def check(status: int, cloud=None, what: str = "") -> None:
+    if status == OCT_OK:
+        return
+    L = lib()
+    msg = L.oct_status_string(status).decode()
+    if cloud:
+        buf = C.create_string_buffer(512)
+        L.oct_last_error(cloud, buf, 512)
+        if buf.value:
+            msg += ": " + buf.value.decode()
+    raise OctError(status, f"{what}: {msg}" if what else msg)

@@ -1,0 +1,541 @@
+// The extern "C" boundary (include/octree_b200.h): cloud handles, host/device
+// buffer handling, call ordering, and the error word the kernels latch.
+#include <algorithm>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <utility>
+
+#include "cloud.h"
+
+using namespace octb;
+
+struct oct_cloud_s {
+    Cloud c;
+};
+
+namespace {
+
+// Makes the cloud's device current for the duration of a call.
+struct DeviceGuard {
+    int prev = -1;
+    explicit DeviceGuard(int dev) {
+        if (cudaGetDevice(&prev) != cudaSuccess) prev = -1;
+        if (prev != dev) cudaSetDevice(dev);
+    }
+    ~DeviceGuard() {
+        int cur = -1;
+        if (prev >= 0 && cudaGetDevice(&cur) == cudaSuccess && cur != prev) cudaSetDevice(prev);
+    }
+};
+
+int set_error(Cloud& c, int status, const std::string& msg) {
+    c.last_error = msg;
+    return status;
+}
+
+int cuda_fail(Cloud& c, cudaError_t e, const char* what) {
+    char buf[512];
+    snprintf(buf, sizeof(buf), "%s: %s (%s)", what, cudaGetErrorName(e), cudaGetErrorString(e));
+    const int st = (e == cudaErrorMemoryAllocation) ? OCT_ERR_OUT_OF_MEMORY : OCT_ERR_CUDA;
+    cudaGetLastError();  // clear a sticky launch error
+    return set_error(c, st, buf);
+}
+
+#define CK(expr)                                          \
+    do {                                                  \
+        cudaError_t _e = (expr);                          \
+        if (_e != cudaSuccess) return cuda_fail(c, _e, #expr); \
+    } while (0)
+
+constexpr size_t kPinnedBytes = 4096;
+
+// Synchronise the stream and turn the latched device error word into a status.
+int sync_and_check(Cloud& c, uint32_t ignore_bits = 0) {
+    uint32_t* h = static_cast<uint32_t*>(c.pinned);
+    CK(cudaMemcpyAsync(h, c.d_err.ptr, 4, cudaMemcpyDeviceToHost, c.stream));
+    CK(cudaStreamSynchronize(c.stream));
+    const uint32_t bits = *h & ~ignore_bits;
+    if (*h) CK(cudaMemsetAsync(c.d_err.ptr, 0, 4, c.stream));
+    if (bits & kErrOutputCapacity) return set_error(c, OCT_ERR_CAPACITY, "output buffer smaller than the results");
+    if (bits & kErrBadInput) return set_error(c, OCT_ERR_INVALID_ARG, "device rejected an input");
+    if (bits) {
+        char buf[128];
+        snprintf(buf, sizeof(buf), "a bounded device loop hit its limit (error bits 0x%x)", bits);
+        return set_error(c, OCT_ERR_DEVICE_LIMIT, buf);
+    }
+    return OCT_OK;
+}
+
+// Copy a caller buffer to the device when it is host memory; return the device pointer.
+template <class T>
+int stage_in(Cloud& c, DevBuf& scratch, const T* src, size_t count, bool device, const T** out) {
+    if (device || src == nullptr) {
+        *out = src;
+        return OCT_OK;
+    }
+    CK(scratch.reserve(sizeof(T) * (count ? count : 1)));
+    if (count) CK(cudaMemcpyAsync(scratch.ptr, src, sizeof(T) * count, cudaMemcpyHostToDevice, c.stream));
+    *out = scratch.as<T>();
+    return OCT_OK;
+}
+
+template <class T>
+int copy_out(Cloud& c, T* dst, const T* dsrc, size_t count, bool device) {
+    if (!dst || count == 0) return OCT_OK;
+    CK(cudaMemcpyAsync(dst, dsrc, sizeof(T) * count, device ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost,
+                       c.stream));
+    return OCT_OK;
+}
+
+__global__ void k_soa_to_aos(const double* xs, const double* ys, const double* zs, uint64_t n, double* out) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        out[3 * i] = xs[i];
+        out[3 * i + 1] = ys[i];
+        out[3 * i + 2] = zs[i];
+    }
+}
+
+__global__ void k_widen_pairs(const uint2* in, uint64_t n, unsigned long long* out) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        const uint2 v = in[i];
+        out[2 * i] = v.x;
+        out[2 * i + 1] = v.y;
+    }
+}
+
+bool valid_kernel(int k) { return k >= OCT_KERNEL_CIRCLE && k <= OCT_KERNEL_CUBE; }
+bool valid_algo(int a) { return a >= OCT_NEIGHBORS && a <= OCT_NEIGHBORS_STRUCT; }
+
+// Lanes per query of the radius traversal (8, 16 or 32), set by oct_set_radius_group.
+int radius_group(const Cloud& c) { return c.radius_group; }
+
+int radius_common(Cloud& c, int kernel, int algo, const double* centers, uint64_t nq, const double* radii,
+                  double radius, bool device, const double** dq, const double** dr) {
+    if (!c.built) return set_error(c, OCT_ERR_STATE, "search before oct_build");
+    if (!valid_kernel(kernel) || !valid_algo(algo)) return set_error(c, OCT_ERR_INVALID_ARG, "bad kernel or algo");
+    if (nq && !centers) return set_error(c, OCT_ERR_INVALID_ARG, "centers is NULL");
+    int st;
+    if ((st = stage_in(c, c.q_centers, centers, 3 * nq, device, dq)) != OCT_OK) return st;
+    if ((st = stage_in(c, c.q_radii, radii, nq, device, dr)) != OCT_OK) return st;
+    (void)radius;
+    return OCT_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int oct_abi_version(void) { return OCT_ABI_VERSION; }
+
+const char* oct_status_string(int s) {
+    switch (s) {
+        case OCT_OK: return "ok";
+        case OCT_ERR_INVALID_ARG: return "invalid argument";
+        case OCT_ERR_CUDA: return "CUDA error";
+        case OCT_ERR_OUT_OF_MEMORY: return "out of device memory";
+        case OCT_ERR_STATE: return "call out of order";
+        case OCT_ERR_CAPACITY: return "output capacity too small";
+        case OCT_ERR_DEVICE_LIMIT: return "device loop limit reached";
+        case OCT_ERR_NO_DEVICE: return "no CUDA device";
+        default: return "unknown status";
+    }
+}
+
+int oct_cloud_create(const oct_params* p, oct_cloud* out) {
+    if (!p || !out) return OCT_ERR_INVALID_ARG;
+    *out = nullptr;
+    if (p->encoder != OCT_ENC_MORTON_3D && p->encoder != OCT_ENC_HILBERT_3D) return OCT_ERR_INVALID_ARG;
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return OCT_ERR_NO_DEVICE;
+    }
+    if (p->device < 0 || p->device >= ndev) return OCT_ERR_INVALID_ARG;
+    oct_cloud h = new (std::nothrow) oct_cloud_s();
+    if (!h) return OCT_ERR_OUT_OF_MEMORY;
+    Cloud& c = h->c;
+    c.params = *p;
+    c.device = p->device;
+    DeviceGuard g(c.device);
+    cudaError_t e = cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) {
+        c.own_stream = true;
+        e = c.d_err.reserve(256);
+    }
+    if (e == cudaSuccess) e = cudaMemsetAsync(c.d_err.ptr, 0, 256, c.stream);
+    if (e == cudaSuccess) e = cudaMallocHost(&c.pinned, kPinnedBytes);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c.stream);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        oct_cloud_destroy(h);
+        return e == cudaErrorMemoryAllocation ? OCT_ERR_OUT_OF_MEMORY : OCT_ERR_CUDA;
+    }
+    *out = h;
+    return OCT_OK;
+}
+
+int oct_cloud_destroy(oct_cloud h) {
+    if (!h) return OCT_ERR_INVALID_ARG;
+    Cloud& c = h->c;
+    {
+        DeviceGuard g(c.device);
+        if (c.stream) cudaStreamSynchronize(c.stream);
+        DevBuf* bufs[] = {&c.xyz_in, &c.xs, &c.ys, &c.zs, &c.keys, &c.keys_alt, &c.perm, &c.perm_alt,
+                          &c.sort_status, &c.d_ctl, &c.d_box, &c.d_err, &c.offsets, &c.ranges, &c.centers,
+                          &c.frontier, &c.masks, &c.parts, &c.d_build, &c.q_centers, &c.q_radii, &c.q_counts,
+                          &c.q_offsets, &c.q_out, &c.q_out2, &c.q_scan_tmp};
+        for (DevBuf* b : bufs) b->release();
+        if (c.pinned) cudaFreeHost(c.pinned);
+        if (c.own_stream && c.stream) cudaStreamDestroy(c.stream);
+    }
+    delete h;
+    return OCT_OK;
+}
+
+int oct_cloud_set_stream(oct_cloud h, void* stream) {
+    if (!h) return OCT_ERR_INVALID_ARG;
+    Cloud& c = h->c;
+    DeviceGuard g(c.device);
+    CK(cudaStreamSynchronize(c.stream));
+    if (c.own_stream) cudaStreamDestroy(c.stream);
+    c.own_stream = false;
+    c.stream = static_cast<cudaStream_t>(stream);
+    return OCT_OK;
+}
+
+int oct_last_error(oct_cloud h, char* buf, size_t len) {
+    if (!h || !buf || len == 0) return OCT_ERR_INVALID_ARG;
+    const std::string& m = h->c.last_error;
+    const size_t k = std::min(len - 1, m.size());
+    memcpy(buf, m.data(), k);
+    buf[k] = '\0';
+    return OCT_OK;
+}
+
+int oct_synchronize(oct_cloud h) {
+    if (!h) return OCT_ERR_INVALID_ARG;
+    Cloud& c = h->c;
+    DeviceGuard g(c.device);
+    return sync_and_check(c);
+}
+
+int oct_set_radius_group(oct_cloud h, int lanes) {
+    if (!h) return OCT_ERR_INVALID_ARG;
+    h->c.radius_group = (lanes == 16 || lanes == 32) ? lanes : 8;
+    return OCT_OK;
+}
+
+int oct_set_points(oct_cloud h, const double* xyz, uint64_t n, uint32_t flags) {
+    if (!h) return OCT_ERR_INVALID_ARG;
+    Cloud& c = h->c;
+    if (n && !xyz) return set_error(c, OCT_ERR_INVALID_ARG, "xyz is NULL");
+    if (n >= 0xffffffffull) return set_error(c, OCT_ERR_INVALID_ARG, "more than 2^32 - 2 points");
+    DeviceGuard g(c.device);
+    CK(c.xyz_in.reserve(24 * (n ? n : 1)));
+    if (n) {
+        CK(cudaMemcpyAsync(c.xyz_in.ptr, xyz, 24 * n,
+                           (flags & OCT_MEM_DEVICE) ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice, c.stream));
+    }
+    c.n = n;
+    c.sorted = false;
+    c.built = false;
+    c.node_capacity = 0;
+    if (!(flags & OCT_MEM_DEVICE)) CK(cudaStreamSynchronize(c.stream));
+    return OCT_OK;
+}
+
+int oct_encode_sort(oct_cloud h, double* box12, uint64_t* keys, uint32_t* perm, double* sorted_xyz,
+                    uint32_t flags) {
+    if (!h) return OCT_ERR_INVALID_ARG;
+    Cloud& c = h->c;
+    DeviceGuard g(c.device);
+    const bool dev = flags & OCT_MEM_DEVICE;
+    const double* xyz = c.xyz_in.as<double>();
+    CK(cudaMemsetAsync(c.d_err.ptr, 0, 4, c.stream));
+    CK(launch_bbox_encode(c, xyz));
+    uint32_t skip[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    if (c.n) {
+        CK(cudaMemcpyAsync(c.pinned, &c.d_ctl.as<SortCtl>()->skip[0], sizeof(skip), cudaMemcpyDeviceToHost,
+                           c.stream));
+        CK(cudaStreamSynchronize(c.stream));
+        memcpy(skip, c.pinned, sizeof(skip));
+    }
+    int sel = 0;
+    CK(launch_sort_passes(c, skip, &sel));
+    if (sel == 1) {
+        std::swap(c.keys, c.keys_alt);
+        std::swap(c.perm, c.perm_alt);
+    }
+    CK(launch_gather(c, xyz, c.perm.as<uint32_t>(), 0));
+    // box and level geometry back to the host
+    CK(cudaMemcpyAsync(c.pinned, c.d_box.ptr, sizeof(BoxD) + sizeof(LevelGeom), cudaMemcpyDeviceToHost, c.stream));
+    int st = sync_and_check(c);
+    if (st != OCT_OK) return st;
+    memcpy(&c.box, c.pinned, sizeof(BoxD));
+    memcpy(&c.geom, static_cast<unsigned char*>(c.pinned) + sizeof(BoxD), sizeof(LevelGeom));
+    c.sorted = true;
+    c.built = false;
+    c.node_capacity = 0;
+    if (box12) {
+        for (int a = 0; a < 3; ++a) {
+            box12[a] = c.box.center[a];
+            box12[3 + a] = c.box.radii[a];
+            box12[6 + a] = c.box.min[a];
+            box12[9 + a] = c.box.max[a];
+        }
+    }
+    const uint64_t n = c.n;
+    if ((st = copy_out(c, keys, c.keys.as<uint64_t>(), n, dev)) != OCT_OK) return st;
+    if ((st = copy_out(c, perm, c.perm.as<uint32_t>(), n, dev)) != OCT_OK) return st;
+    if (sorted_xyz && n) {
+        double* dst = sorted_xyz;
+        if (!dev) {
+            CK(c.q_out.reserve(24 * n));
+            dst = c.q_out.as<double>();
+        }
+        k_soa_to_aos<<<(unsigned)((n + 255) / 256), 256, 0, c.stream>>>(c.xs.as<double>(), c.ys.as<double>(),
+                                                                        c.zs.as<double>(), n, dst);
+        CK(cudaGetLastError());
+        if (!dev) CK(cudaMemcpyAsync(sorted_xyz, dst, 24 * n, cudaMemcpyDeviceToHost, c.stream));
+    }
+    if (!dev) CK(cudaStreamSynchronize(c.stream));
+    return OCT_OK;
+}
+
+int oct_build(oct_cloud h, oct_tree_info* info) {
+    if (!h) return OCT_ERR_INVALID_ARG;
+    Cloud& c = h->c;
+    if (!c.sorted) return set_error(c, OCT_ERR_STATE, "oct_build before oct_encode_sort");
+    DeviceGuard g(c.device);
+    for (int attempt = 0; attempt < 8; ++attempt) {
+        bool ok = true;
+        CK(launch_build(c, &ok));
+        CK(cudaMemcpyAsync(c.pinned, c.d_build.ptr, sizeof(BuildCtl), cudaMemcpyDeviceToHost, c.stream));
+        const int st = sync_and_check(c, kErrNodeCapacity);
+        BuildCtl bc;
+        memcpy(&bc, c.pinned, sizeof(BuildCtl));
+        if (st != OCT_OK) return st;
+        // sync_and_check cleared the word; a capacity miss shows as need_nodes > capacity
+        if (bc.need_nodes > c.node_capacity) {
+            uint64_t want = std::max<uint64_t>(2ull * bc.need_nodes, 2ull * c.node_capacity);
+            if (want > 0xfffffff0ull) want = 0xfffffff0ull;
+            if (want <= c.node_capacity) return set_error(c, OCT_ERR_OUT_OF_MEMORY, "octree exceeds 2^32 nodes");
+            c.node_capacity = (uint32_t)want;
+            continue;
+        }
+        c.n_total = bc.n_total;
+        c.n_internal = bc.n_internal;
+        c.n_leaf = bc.n_total - bc.n_internal;
+        c.max_depth_seen = bc.max_depth_seen;
+        CK(cudaMemsetAsync(c.offsets.as<uint32_t>() + c.n_total, 0, 4, c.stream));
+        c.built = true;
+        if (info) {
+            info->n_points = c.n;
+            info->n_leaf = c.n_leaf;
+            info->n_internal = c.n_internal;
+            info->n_total = c.n_total;
+            info->max_depth_seen = c.max_depth_seen;
+        }
+        return OCT_OK;
+    }
+    return set_error(c, OCT_ERR_OUT_OF_MEMORY, "octree node capacity retries exhausted");
+}
+
+int oct_tree_export(oct_cloud h, uint32_t* offsets, uint64_t* ranges, double* centers, double* radii, double* half,
+                    uint32_t flags) {
+    if (!h) return OCT_ERR_INVALID_ARG;
+    Cloud& c = h->c;
+    if (!c.built) return set_error(c, OCT_ERR_STATE, "export before oct_build");
+    DeviceGuard g(c.device);
+    const bool dev = flags & OCT_MEM_DEVICE;
+    const uint64_t nt = c.n_total;
+    int st;
+    if ((st = copy_out(c, offsets, c.offsets.as<uint32_t>(), nt + 1, dev)) != OCT_OK) return st;
+    if ((st = copy_out(c, centers, c.centers.as<double>(), 3 * nt, dev)) != OCT_OK) return st;
+    if (ranges) {
+        unsigned long long* dst = reinterpret_cast<unsigned long long*>(ranges);
+        if (!dev) {
+            CK(c.q_out2.reserve(16 * nt));
+            dst = c.q_out2.as<unsigned long long>();
+        }
+        k_widen_pairs<<<(unsigned)((nt + 255) / 256), 256, 0, c.stream>>>(c.ranges.as<uint2>(), nt, dst);
+        CK(cudaGetLastError());
+        if (!dev) CK(cudaMemcpyAsync(ranges, dst, 16 * nt, cudaMemcpyDeviceToHost, c.stream));
+    }
+    if (radii || half) {
+        if (dev) {
+            if (radii)
+                CK(cudaMemcpyAsync(radii, c.geom.radii, sizeof(c.geom.radii), cudaMemcpyHostToDevice, c.stream));
+            if (half) CK(cudaMemcpyAsync(half, c.geom.half, sizeof(c.geom.half), cudaMemcpyHostToDevice, c.stream));
+        } else {
+            if (radii) memcpy(radii, c.geom.radii, sizeof(c.geom.radii));
+            if (half) memcpy(half, c.geom.half, sizeof(c.geom.half));
+        }
+    }
+    CK(cudaStreamSynchronize(c.stream));
+    return OCT_OK;
+}
+
+int oct_radius_count(oct_cloud h, int kernel, int algo, const double* centers, uint64_t nq, const double* radii,
+                     double radius, uint64_t* counts, uint32_t flags) {
+    if (!h) return OCT_ERR_INVALID_ARG;
+    Cloud& c = h->c;
+    DeviceGuard g(c.device);
+    const bool dev = flags & OCT_MEM_DEVICE;
+    const double *dq, *dr;
+    int st = radius_common(c, kernel, algo, centers, nq, radii, radius, dev, &dq, &dr);
+    if (st != OCT_OK) return st;
+    unsigned long long* dc = reinterpret_cast<unsigned long long*>(counts);
+    if (!dev || !counts) {
+        CK(c.q_counts.reserve(8 * (nq ? nq : 1)));
+        dc = c.q_counts.as<unsigned long long>();
+    }
+    CK(c.q_out2.reserve(8 * (nq ? nq : 1)));
+    unsigned long long* dc_ranges = c.q_out2.as<unsigned long long>();
+    // for neighborsStruct the reported count is numberOfPoints
+    if (algo == OCT_NEIGHBORS_STRUCT)
+        CK(launch_radius(c, kernel, algo, radius_group(c), false, dq, nq, dr, radius, dc_ranges, dc, nullptr,
+                         nullptr, 0));
+    else
+        CK(launch_radius(c, kernel, algo, radius_group(c), false, dq, nq, dr, radius, dc, nullptr, nullptr, nullptr,
+                         0));
+    if (!dev && counts && nq) CK(cudaMemcpyAsync(counts, dc, 8 * nq, cudaMemcpyDeviceToHost, c.stream));
+    if (!dev) return sync_and_check(c);
+    return OCT_OK;
+}
+
+int oct_radius_search(oct_cloud h, int kernel, int algo, const double* centers, uint64_t nq, const double* radii,
+                      double radius, uint64_t* offsets, uint32_t* idx, uint64_t idx_capacity, uint64_t* total,
+                      uint32_t flags) {
+    if (!h) return OCT_ERR_INVALID_ARG;
+    Cloud& c = h->c;
+    DeviceGuard g(c.device);
+    const bool dev = flags & OCT_MEM_DEVICE;
+    const double *dq, *dr;
+    int st = radius_common(c, kernel, algo, centers, nq, radii, radius, dev, &dq, &dr);
+    if (st != OCT_OK) return st;
+    const int grp = radius_group(c);
+    CK(c.q_counts.reserve(8 * (nq ? nq : 1)));
+    unsigned long long* dc = c.q_counts.as<unsigned long long>();
+    unsigned long long* doffs = reinterpret_cast<unsigned long long*>(offsets);
+    if (!dev || !offsets) {
+        CK(c.q_offsets.reserve(8 * (nq + 1)));
+        doffs = c.q_offsets.as<unsigned long long>();
+    }
+    if (algo == OCT_NEIGHBORS_STRUCT) {
+        // expanded indices of the ranges: count points, fill as prune-style runs
+        CK(c.q_out2.reserve(8 * (nq ? nq : 1)));
+        CK(launch_radius(c, kernel, OCT_NEIGHBORS_STRUCT, grp, false, dq, nq, dr, radius, c.q_out2.as<unsigned long long>(),
+                         dc, nullptr, nullptr, 0));
+    } else {
+        CK(launch_radius(c, kernel, algo, grp, false, dq, nq, dr, radius, dc, nullptr, nullptr, nullptr, 0));
+    }
+    CK(launch_scan_u64(c, dc, doffs, nq));
+    CK(cudaMemcpyAsync(c.pinned, doffs + nq, 8, cudaMemcpyDeviceToHost, c.stream));
+    if ((st = sync_and_check(c)) != OCT_OK) return st;
+    uint64_t tot;
+    memcpy(&tot, c.pinned, 8);
+    if (total) *total = tot;
+    if (!dev && offsets) CK(cudaMemcpyAsync(offsets, doffs, 8 * (nq + 1), cudaMemcpyDeviceToHost, c.stream));
+    if (tot > idx_capacity || (tot && !idx)) {
+        CK(cudaStreamSynchronize(c.stream));
+        return set_error(c, OCT_ERR_CAPACITY, "idx capacity smaller than the number of results");
+    }
+    uint32_t* dout = idx;
+    if (!dev) {
+        CK(c.q_out.reserve(4 * (tot ? tot : 1)));
+        dout = c.q_out.as<uint32_t>();
+    }
+    // neighborsStruct's index set equals the points of its ranges; the prune
+    // traversal with the same kernel emits exactly that set (same decisions).
+    const int fill_algo = (algo == OCT_NEIGHBORS_STRUCT) ? OCT_NEIGHBORS_PRUNE : algo;
+    CK(launch_radius(c, kernel, fill_algo, grp, true, dq, nq, dr, radius, nullptr, nullptr, doffs, dout, tot));
+    if (!dev && tot) CK(cudaMemcpyAsync(idx, dout, 4 * tot, cudaMemcpyDeviceToHost, c.stream));
+    if (!dev) return sync_and_check(c);
+    return OCT_OK;
+}
+
+int oct_struct_search(oct_cloud h, int kernel, const double* centers, uint64_t nq, const double* radii,
+                      double radius, uint64_t* range_offsets, uint32_t* pairs, uint64_t pair_capacity,
+                      uint64_t* total_ranges, uint64_t* point_counts, uint32_t flags) {
+    if (!h) return OCT_ERR_INVALID_ARG;
+    Cloud& c = h->c;
+    DeviceGuard g(c.device);
+    const bool dev = flags & OCT_MEM_DEVICE;
+    const double *dq, *dr;
+    int st = radius_common(c, kernel, OCT_NEIGHBORS_STRUCT, centers, nq, radii, radius, dev, &dq, &dr);
+    if (st != OCT_OK) return st;
+    const int grp = radius_group(c);
+    CK(c.q_counts.reserve(8 * (nq ? nq : 1)));
+    CK(c.q_out2.reserve(8 * (nq ? nq : 1)));
+    unsigned long long* dranges = c.q_counts.as<unsigned long long>();
+    unsigned long long* dpoints = reinterpret_cast<unsigned long long*>(point_counts);
+    if (!dev || !point_counts) dpoints = c.q_out2.as<unsigned long long>();
+    unsigned long long* doffs = reinterpret_cast<unsigned long long*>(range_offsets);
+    if (!dev || !range_offsets) {
+        CK(c.q_offsets.reserve(8 * (nq + 1)));
+        doffs = c.q_offsets.as<unsigned long long>();
+    }
+    CK(launch_radius(c, kernel, OCT_NEIGHBORS_STRUCT, grp, false, dq, nq, dr, radius, dranges, dpoints, nullptr,
+                     nullptr, 0));
+    CK(launch_scan_u64(c, dranges, doffs, nq));
+    CK(cudaMemcpyAsync(c.pinned, doffs + nq, 8, cudaMemcpyDeviceToHost, c.stream));
+    if ((st = sync_and_check(c)) != OCT_OK) return st;
+    uint64_t tot;
+    memcpy(&tot, c.pinned, 8);
+    if (total_ranges) *total_ranges = tot;
+    if (!dev && range_offsets) CK(cudaMemcpyAsync(range_offsets, doffs, 8 * (nq + 1), cudaMemcpyDeviceToHost, c.stream));
+    if (!dev && point_counts && nq) CK(cudaMemcpyAsync(point_counts, dpoints, 8 * nq, cudaMemcpyDeviceToHost, c.stream));
+    if (tot > pair_capacity || (tot && !pairs)) {
+        CK(cudaStreamSynchronize(c.stream));
+        return set_error(c, OCT_ERR_CAPACITY, "pair capacity smaller than the number of ranges");
+    }
+    uint32_t* dout = pairs;
+    if (!dev) {
+        CK(c.q_out.reserve(8 * (tot ? tot : 1)));
+        dout = c.q_out.as<uint32_t>();
+    }
+    CK(launch_radius(c, kernel, OCT_NEIGHBORS_STRUCT, grp, true, dq, nq, dr, radius, nullptr, nullptr, doffs, dout,
+                     tot));
+    if (!dev && tot) CK(cudaMemcpyAsync(pairs, dout, 8 * tot, cudaMemcpyDeviceToHost, c.stream));
+    if (!dev) return sync_and_check(c);
+    return OCT_OK;
+}
+
+int oct_knn(oct_cloud h, const double* centers, uint64_t nq, uint32_t k, uint32_t* idx, double* d2,
+            uint32_t* counts, uint32_t flags) {
+    if (!h) return OCT_ERR_INVALID_ARG;
+    Cloud& c = h->c;
+    if (!c.built) return set_error(c, OCT_ERR_STATE, "knn before oct_build");
+    if (k == 0 || k > 1024) return set_error(c, OCT_ERR_INVALID_ARG, "k must be in [1, 1024]");
+    if (nq && (!centers || !idx || !d2)) return set_error(c, OCT_ERR_INVALID_ARG, "NULL buffer");
+    DeviceGuard g(c.device);
+    const bool dev = flags & OCT_MEM_DEVICE;
+    const double* dq;
+    int st = stage_in(c, c.q_centers, centers, 3 * nq, dev, &dq);
+    if (st != OCT_OK) return st;
+    uint32_t* di = idx;
+    double* dd = d2;
+    uint32_t* dc = counts;
+    if (!dev) {
+        CK(c.q_out.reserve(4 * nq * (uint64_t)k + 4));
+        CK(c.q_out2.reserve(8 * nq * (uint64_t)k + 8));
+        CK(c.q_counts.reserve(4 * (nq ? nq : 1)));
+        di = c.q_out.as<uint32_t>();
+        dd = c.q_out2.as<double>();
+        dc = counts ? c.q_counts.as<uint32_t>() : nullptr;
+    }
+    CK(launch_knn(c, dq, nq, k, di, dd, dc));
+    if (!dev && nq) {
+        CK(cudaMemcpyAsync(idx, di, 4 * nq * (uint64_t)k, cudaMemcpyDeviceToHost, c.stream));
+        CK(cudaMemcpyAsync(d2, dd, 8 * nq * (uint64_t)k, cudaMemcpyDeviceToHost, c.stream));
+        if (counts) CK(cudaMemcpyAsync(counts, dc, 4 * nq, cudaMemcpyDeviceToHost, c.stream));
+    }
+    if (!dev) return sync_and_check(c);
+    return OCT_OK;
+}
+
+}  // extern "C"

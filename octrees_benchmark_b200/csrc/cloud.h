@@ -1,0 +1,116 @@
+// Host-side state of one device-resident cloud (the object behind oct_cloud)
+// and the launchers each .cu file provides.  Internal to the library.
+#pragma once
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <string>
+
+#include "../../include/octree_b200.h"
+#include "oct_common.cuh"
+
+namespace octb {
+
+// A grow-only device allocation.
+struct DevBuf {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+    cudaError_t reserve(size_t want) {
+        if (want <= bytes) return cudaSuccess;
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        bytes = 0;
+        size_t b = want < 256 ? 256 : want;
+        cudaError_t e = cudaMalloc(&ptr, b);
+        if (e == cudaSuccess) bytes = b;
+        return e;
+    }
+    void release() {
+        if (ptr) cudaFree(ptr);
+        ptr = nullptr;
+        bytes = 0;
+    }
+    template <class T>
+    T* as() const { return static_cast<T*>(ptr); }
+};
+
+// Device-side record of the sort (one per cloud): the 8 digit histograms of
+// the keys, their exclusive scans, which passes are skipped (all keys share
+// the digit) and one tile counter per pass.
+struct SortCtl {
+    unsigned long long offs[8][256];
+    uint32_t hist[8][256];
+    uint32_t skip[8];
+    uint32_t tile_ctr[8];
+    uint32_t bbox_ctr;
+    uint32_t pad;
+};
+
+// Octree build bookkeeping written by the device.
+struct BuildCtl {
+    uint32_t level_start[kMaxDepth + 3];  // first node index of each level
+    uint32_t level_internal[kMaxDepth + 2];
+    uint32_t n_total;
+    uint32_t n_internal;
+    uint32_t max_depth_seen;
+    uint32_t need_nodes;                  // nodes the tree needs (valid when kErrNodeCapacity)
+    uint32_t barrier_count;
+    uint32_t barrier_gen;
+};
+
+struct Cloud {
+    oct_params params{};
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    bool own_stream = false;
+    uint64_t n = 0;
+    bool sorted = false;
+    bool built = false;
+    int radius_group = 8;
+    std::string last_error;
+
+    // points
+    DevBuf xyz_in;          // AoS input (n x 3 f64), as uploaded
+    DevBuf xs, ys, zs;      // SFC-sorted coordinates, SoA f64
+    DevBuf keys, keys_alt;  // u64 keys (sorted result lives in `keys`)
+    DevBuf perm, perm_alt;  // u32 input position of each sorted point
+    DevBuf sort_status;     // onesweep look-back words
+    uint32_t sort_epoch = 0;
+    DevBuf d_ctl;           // SortCtl
+    DevBuf d_box;           // BoxD
+    DevBuf d_err;           // uint32 error word
+    BoxD box{};             // host copy
+    LevelGeom geom{};       // host copy
+
+    // tree
+    DevBuf offsets;  // u32, n_total + 1
+    DevBuf ranges;   // uint2 (first, last) per node
+    DevBuf centers;  // 3 x f64 per node (AoS)
+    DevBuf frontier; // build scratch: internal nodes of the current/next level
+    DevBuf masks;    // build scratch: ballots of internal children
+    DevBuf parts;    // build scratch: per-block counts
+    DevBuf d_build;  // BuildCtl
+    uint32_t node_capacity = 0;
+    uint32_t n_total = 0, n_internal = 0, n_leaf = 0, max_depth_seen = 0;
+
+    // query scratch
+    DevBuf q_centers, q_radii, q_counts, q_offsets, q_out, q_out2, q_scan_tmp;
+
+    // pinned host staging for small readbacks
+    void* pinned = nullptr;
+};
+
+// ---- launchers (each returns a cudaError_t of the launch) ----
+cudaError_t launch_bbox_encode(Cloud& c, const double* d_xyz_aos);
+cudaError_t launch_sort_passes(Cloud& c, const uint32_t skip[8], int* final_sel);
+cudaError_t launch_gather(Cloud& c, const double* d_xyz_aos, const uint32_t* d_perm, int sel);
+cudaError_t launch_build(Cloud& c, bool* capacity_ok);
+cudaError_t launch_radius(Cloud& c, int kernel, int algo, int group, bool fill, const double* d_centers,
+                          uint64_t nq, const double* d_radii, double radius, unsigned long long* d_counts,
+                          unsigned long long* d_counts2, const unsigned long long* d_offsets, uint32_t* d_out,
+                          uint64_t out_capacity);
+cudaError_t launch_scan_u64(Cloud& c, const unsigned long long* d_in, unsigned long long* d_out, uint64_t n);
+cudaError_t launch_knn(Cloud& c, const double* d_centers, uint64_t nq, uint32_t k, uint32_t* d_idx, double* d_d2,
+                       uint32_t* d_counts);
+
+}  // namespace octb

@@ -1,0 +1,433 @@
+// Bounding box, SFC encoding and the stable key sort with point reorder.
+//
+// Reference path replaced: PointEncoder::sortPoints (inc/encoding/point_encoder.hpp:
+// 285-383, 484-503): mbb (inc/geometry/box.hpp:95-137) -> encodePoints -> an
+// 8 x 8-bit LSD radix sort that moves keys and points together.
+//
+// B200 design:
+//  * k_bbox: one pass over the AoS input, block min/max, the last block folds
+//    the partials and writes the Box and the per-level geometry.
+//  * k_encode: anchor coordinates + Morton/Hilbert key per point, and in the
+//    same pass the 8 digit histograms of every key (so no pass re-reads keys
+//    to count).
+//  * k_onesweep: one kernel per 8-bit digit, single-pass "onesweep" radix
+//    scatter: each 4096-key tile ranks its keys stably in shared memory (warp
+//    match + per-warp counters), publishes its digit counts, resolves its
+//    global digit offsets by decoupled look-back over the preceding tiles
+//    (bounded waits), and writes keys and 32-bit point ids out digit-grouped,
+//    which keeps the writes coalesced.  Digits equal for every key are
+//    skipped.  Values are generated on the fly in the first pass.
+//  * k_gather: reorders the coordinates into SoA float64 arrays.
+#include <cfloat>
+
+#include "cloud.h"
+#include "sfc.cuh"
+
+namespace octb {
+
+namespace {
+
+constexpr int kBboxThreads = 256;
+constexpr int kEncThreads = 256;
+constexpr int kSortThreads = 256;
+constexpr int kSortItems = 16;
+constexpr int kSortTile = kSortThreads * kSortItems;  // 4096 keys
+constexpr int kSortWarps = kSortThreads / 32;
+constexpr int kEncGridPerSM = 4;
+
+// look-back status word: flag (2 bits) | epoch (22 bits) | count (40 bits)
+constexpr unsigned long long kFlagLocal = 1ull << 62;
+constexpr unsigned long long kFlagPrefix = 2ull << 62;
+constexpr unsigned long long kCountMask = (1ull << 40) - 1;
+constexpr int kEpochShift = 40;
+constexpr unsigned long long kEpochMask = ((1ull << 22) - 1) << kEpochShift;
+
+struct BoxGeom {
+    BoxD box;
+    LevelGeom geom;
+};
+
+__device__ __forceinline__ unsigned long long ld_volatile_u64(const unsigned long long* p) {
+    unsigned long long v;
+    asm volatile("ld.relaxed.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_volatile_u64(unsigned long long* p, unsigned long long v) {
+    asm volatile("st.relaxed.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+__global__ void __launch_bounds__(kBboxThreads) k_bbox(const double* __restrict__ xyz, uint64_t n,
+                                                       double* __restrict__ partial, uint32_t* ctr,
+                                                       BoxGeom* out) {
+    double mn[3] = {DBL_MAX, DBL_MAX, DBL_MAX};
+    double mx[3] = {-DBL_MAX, -DBL_MAX, -DBL_MAX};
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            const double v = xyz[3 * i + a];
+            mn[a] = smin(mn[a], v);  // std::min(localMin, p)
+            mx[a] = smax(mx[a], v);  // std::max(localMax, p)
+        }
+    }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            mn[a] = smin(mn[a], __shfl_down_sync(0xffffffffu, mn[a], off));
+            mx[a] = smax(mx[a], __shfl_down_sync(0xffffffffu, mx[a], off));
+        }
+    }
+    __shared__ double s[kBboxThreads / 32][6];
+    __shared__ bool last;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0)
+        for (int a = 0; a < 3; ++a) { s[warp][a] = mn[a]; s[warp][3 + a] = mx[a]; }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < kBboxThreads / 32; ++w)
+            for (int a = 0; a < 3; ++a) {
+                s[0][a] = smin(s[0][a], s[w][a]);
+                s[0][3 + a] = smax(s[0][3 + a], s[w][3 + a]);
+            }
+        for (int a = 0; a < 6; ++a) partial[6 * blockIdx.x + a] = s[0][a];
+        __threadfence();
+        last = (atomicAdd(ctr, 1u) == gridDim.x - 1);
+    }
+    __syncthreads();
+    if (!last || threadIdx.x != 0) return;
+    __threadfence();
+    double gmn[3] = {DBL_MAX, DBL_MAX, DBL_MAX}, gmx[3] = {-DBL_MAX, -DBL_MAX, -DBL_MAX};
+    for (unsigned b = 0; b < gridDim.x; ++b)
+        for (int a = 0; a < 3; ++a) {
+            gmn[a] = smin(gmn[a], ((volatile double*)partial)[6 * b + a]);
+            gmx[a] = smax(gmx[a], ((volatile double*)partial)[6 * b + 3 + a]);
+        }
+    // Box(pair{min, max}) then Box(center, radii) (box.hpp:17-21, point_encoder.hpp:492-494)
+    BoxGeom bg;
+    for (int a = 0; a < 3; ++a) {
+        const double r = ddiv(dsub(gmx[a], gmn[a]), 2.0);
+        const double c = dadd(gmn[a], ddiv(dsub(gmx[a], gmn[a]), 2.0));
+        bg.box.center[a] = c;
+        bg.box.radii[a] = r;
+        bg.box.min[a] = dsub(c, r);
+        bg.box.max[a] = dadd(c, r);
+    }
+    // LinearOctree::setupBbox (linear_octree.hpp:439-455): half = 0.5f * eps * (max - min)
+    const double eps = 4.76837158203125e-07;  // (double)(1.0f / 2^21)
+    for (int a = 0; a < 3; ++a) bg.geom.half[a] = dmul(dmul(0.5, eps), dsub(bg.box.max[a], bg.box.min[a]));
+    for (uint32_t l = 0; l <= kMaxDepth; ++l)
+        for (int a = 0; a < 3; ++a) bg.geom.radii[l][a] = dmul((double)(1u << (kMaxDepth - l)), bg.geom.half[a]);
+    *out = bg;
+    *ctr = 0;
+}
+
+template <int ENC>
+__global__ void __launch_bounds__(kEncThreads) k_encode(const double* __restrict__ xyz, uint64_t n,
+                                                        const BoxGeom* __restrict__ bg, uint64_t* __restrict__ keys,
+                                                        SortCtl* ctl) {
+    __shared__ uint32_t hist[8 * 256];
+    for (int j = threadIdx.x; j < 8 * 256; j += blockDim.x) hist[j] = 0;
+    const double c0 = bg->box.center[0], c1 = bg->box.center[1], c2 = bg->box.center[2];
+    const double r0 = bg->box.radii[0], r1 = bg->box.radii[1], r2 = bg->box.radii[2];
+    __syncthreads();
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const double px = xyz[3 * i], py = xyz[3 * i + 1], pz = xyz[3 * i + 2];
+        const uint32_t ax = anchor_coord(px, c0, r0);
+        const uint32_t ay = anchor_coord(py, c1, r1);
+        const uint32_t az = anchor_coord(pz, c2, r2);
+        const uint64_t k = sfc_encode<ENC>(ax, ay, az);
+        keys[i] = k;
+#pragma unroll
+        for (int p = 0; p < 8; ++p) atomicAdd(&hist[p * 256 + (uint32_t)((k >> (8 * p)) & 255u)], 1u);
+    }
+    __syncthreads();
+    for (int j = threadIdx.x; j < 8 * 256; j += blockDim.x) {
+        const uint32_t v = hist[j];
+        if (v) atomicAdd(&ctl->hist[j >> 8][j & 255], v);
+    }
+}
+
+// Exclusive scans of the 8 histograms; pass p is skipped when one digit holds
+// every key.  One block of 256 threads.
+__global__ void __launch_bounds__(256) k_scan_hist(SortCtl* ctl, uint64_t n) {
+    __shared__ unsigned long long warp_sum[8];
+    const int d = threadIdx.x, lane = d & 31, warp = d >> 5;
+    for (int p = 0; p < 8; ++p) {
+        const unsigned long long v = ctl->hist[p][d];
+        unsigned long long x = v;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            const unsigned long long y = __shfl_up_sync(0xffffffffu, x, off);
+            if (lane >= off) x += y;
+        }
+        if (lane == 31) warp_sum[warp] = x;
+        const bool full = (v == n);
+        const int any_full = __syncthreads_or(full);
+        unsigned long long base = 0;
+        for (int w = 0; w < warp; ++w) base += warp_sum[w];
+        ctl->offs[p][d] = base + x - v;
+        if (d == 0) {
+            ctl->skip[p] = any_full ? 1u : 0u;
+            ctl->tile_ctr[p] = 0;
+        }
+        __syncthreads();
+    }
+}
+
+template <bool FIRST>
+__global__ void __launch_bounds__(kSortThreads) k_onesweep(const uint64_t* __restrict__ kin,
+                                                           const uint32_t* __restrict__ vin,
+                                                           uint64_t* __restrict__ kout, uint32_t* __restrict__ vout,
+                                                           uint64_t n, int pass, SortCtl* ctl,
+                                                           unsigned long long* status, uint32_t epoch,
+                                                           uint32_t* err) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    uint64_t* skeys = reinterpret_cast<uint64_t*>(smem);                       // kSortTile
+    uint32_t* svals = reinterpret_cast<uint32_t*>(skeys + kSortTile);          // kSortTile
+    uint32_t* wcnt = svals + kSortTile;                                        // kSortWarps x 256
+    uint32_t* tstart = wcnt + kSortWarps * 256;                                // 256
+    unsigned long long* gbase = reinterpret_cast<unsigned long long*>(tstart + 256);  // 256
+    __shared__ uint32_t s_tile;
+    __shared__ uint32_t s_wsum[kSortWarps];
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int shift = 8 * pass;
+    if (tid == 0) s_tile = atomicAdd(&ctl->tile_ctr[pass], 1u);
+    for (int j = tid; j < kSortWarps * 256; j += kSortThreads) wcnt[j] = 0;
+    __syncthreads();
+    const uint32_t tile = s_tile;
+    const uint64_t base = (uint64_t)tile * kSortTile;
+
+    uint64_t k[kSortItems];
+    uint32_t v[kSortItems];
+    uint32_t rank[kSortItems];
+#pragma unroll
+    for (int j = 0; j < kSortItems; ++j) {
+        const uint64_t idx = base + (uint64_t)warp * (32 * kSortItems) + (uint64_t)j * 32 + lane;
+        const bool valid = idx < n;
+        k[j] = valid ? kin[idx] : ~0ull;
+        if (FIRST) v[j] = (uint32_t)idx;
+        else v[j] = valid ? vin[idx] : 0u;
+    }
+    // stable rank inside the warp: item j of lane l precedes item j of lane l+1,
+    // and every item j precedes item j+1
+    uint32_t* cnt = wcnt + warp * 256;
+#pragma unroll
+    for (int j = 0; j < kSortItems; ++j) {
+        const uint64_t idx = base + (uint64_t)warp * (32 * kSortItems) + (uint64_t)j * 32 + lane;
+        const bool valid = idx < n;
+        const uint32_t d = valid ? (uint32_t)((k[j] >> shift) & 255u) : 256u;
+        const uint32_t peers = __match_any_sync(0xffffffffu, d);
+        uint32_t before = 0;
+        if (valid) before = cnt[d];
+        __syncwarp();
+        if (valid && lane == 31 - __clz(peers)) cnt[d] = before + __popc(peers);
+        __syncwarp();
+        rank[j] = before + __popc(peers & lanemask_lt());
+    }
+    __syncthreads();
+    // per digit: warp prefixes and the tile total
+    const int d = tid;  // kSortThreads == 256: one digit per thread
+    uint32_t total = 0;
+    for (int w = 0; w < kSortWarps; ++w) {
+        const uint32_t c = wcnt[w * 256 + d];
+        wcnt[w * 256 + d] = total;
+        total += c;
+    }
+    const unsigned long long ep = ((unsigned long long)epoch << kEpochShift) & kEpochMask;
+    unsigned long long* my = status + (uint64_t)tile * 256 + d;
+    st_volatile_u64(my, (tile == 0 ? kFlagPrefix : kFlagLocal) | ep | (unsigned long long)total);
+    // tile-local exclusive scan of totals over digits
+    {
+        uint32_t x = total;
+#pragma unroll
+        for (int off = 1; off < 32; off <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, x, off);
+            if (lane >= off) x += y;
+        }
+        if (lane == 31) s_wsum[warp] = x;
+        __syncthreads();
+        uint32_t pre = 0;
+        for (int w = 0; w < warp; ++w) pre += s_wsum[w];
+        tstart[d] = pre + x - total;
+    }
+    // decoupled look-back over the preceding tiles (bounded wait)
+    unsigned long long excl = 0;
+    if (tile > 0) {
+        int64_t t = (int64_t)tile - 1;
+        uint32_t spins = 0;
+        while (t >= 0) {
+            const unsigned long long s = ld_volatile_u64(status + (uint64_t)t * 256 + d);
+            const unsigned long long flag = s & (3ull << 62);
+            if ((s & kEpochMask) != ep || flag == 0) {
+                if (++spins > kSpinLimit) {
+                    set_err(err, kErrSpinLimit);
+                    break;
+                }
+                __nanosleep(32);
+                continue;
+            }
+            excl += s & kCountMask;
+            if (flag == kFlagPrefix) break;
+            --t;
+        }
+        st_volatile_u64(my, kFlagPrefix | ep | (excl + total));
+    }
+    gbase[d] = ctl->offs[pass][d] + excl;
+    __syncthreads();
+    // scatter into shared memory in digit order
+#pragma unroll
+    for (int j = 0; j < kSortItems; ++j) {
+        const uint64_t idx = base + (uint64_t)warp * (32 * kSortItems) + (uint64_t)j * 32 + lane;
+        if (idx < n) {
+            const uint32_t dd = (uint32_t)((k[j] >> shift) & 255u);
+            const uint32_t pos = tstart[dd] + wcnt[warp * 256 + dd] + rank[j];
+            skeys[pos] = k[j];
+            svals[pos] = v[j];
+        }
+    }
+    __syncthreads();
+    const uint32_t cnt_tile = (uint32_t)((n - base) < (uint64_t)kSortTile ? (n - base) : (uint64_t)kSortTile);
+    for (uint32_t s = tid; s < cnt_tile; s += kSortThreads) {
+        const uint64_t key = skeys[s];
+        const uint32_t dd = (uint32_t)((key >> shift) & 255u);
+        const unsigned long long o = gbase[dd] + (s - tstart[dd]);
+        kout[o] = key;
+        vout[o] = svals[s];
+    }
+}
+
+__global__ void k_iota(uint32_t* perm, uint64_t n) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) perm[i] = (uint32_t)i;
+}
+
+__global__ void k_gather(const double* __restrict__ xyz, const uint32_t* __restrict__ perm, uint64_t n,
+                         double* __restrict__ xs, double* __restrict__ ys, double* __restrict__ zs) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const uint64_t j = perm[i];
+        xs[i] = xyz[3 * j];
+        ys[i] = xyz[3 * j + 1];
+        zs[i] = xyz[3 * j + 2];
+    }
+}
+
+int sm_count(int device) {
+    static int cached[64] = {0};
+    if (device >= 0 && device < 64 && cached[device]) return cached[device];
+    int v = 148;
+    cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, device);
+    if (device >= 0 && device < 64) cached[device] = v;
+    return v;
+}
+
+size_t onesweep_smem() {
+    return (size_t)kSortTile * 8 + (size_t)kSortTile * 4 + (size_t)kSortWarps * 256 * 4 + 256 * 4 + 256 * 8;
+}
+
+}  // namespace
+
+cudaError_t launch_bbox_encode(Cloud& c, const double* d_xyz) {
+    cudaError_t e;
+    const uint64_t n = c.n;
+    const int sms = sm_count(c.device);
+    const int grid_bbox = sms * 4;
+    if ((e = c.d_box.reserve(sizeof(BoxGeom))) != cudaSuccess) return e;
+    if ((e = c.d_ctl.reserve(sizeof(SortCtl))) != cudaSuccess) return e;
+    if ((e = c.parts.reserve(sizeof(double) * 6 * grid_bbox + 64)) != cudaSuccess) return e;
+    if ((e = c.keys.reserve(8 * (n ? n : 1))) != cudaSuccess) return e;
+    SortCtl* ctl = c.d_ctl.as<SortCtl>();
+    if ((e = cudaMemsetAsync(ctl, 0, sizeof(SortCtl), c.stream)) != cudaSuccess) return e;
+    k_bbox<<<grid_bbox, kBboxThreads, 0, c.stream>>>(d_xyz, n, c.parts.as<double>(), &ctl->bbox_ctr,
+                                                     c.d_box.as<BoxGeom>());
+    if (n) {
+        const uint64_t want = (n + kEncThreads - 1) / kEncThreads;
+        const int grid = (int)(want < (uint64_t)sms * kEncGridPerSM ? want : (uint64_t)sms * kEncGridPerSM);
+        if (c.params.encoder == OCT_ENC_HILBERT_3D)
+            k_encode<5><<<grid, kEncThreads, 0, c.stream>>>(d_xyz, n, c.d_box.as<BoxGeom>(), c.keys.as<uint64_t>(),
+                                                            ctl);
+        else
+            k_encode<1><<<grid, kEncThreads, 0, c.stream>>>(d_xyz, n, c.d_box.as<BoxGeom>(), c.keys.as<uint64_t>(),
+                                                            ctl);
+        k_scan_hist<<<1, 256, 0, c.stream>>>(ctl, n);
+    }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sort_passes(Cloud& c, const uint32_t skip[8], int* final_sel) {
+    cudaError_t e;
+    const uint64_t n = c.n;
+    *final_sel = 0;
+    if ((e = c.perm.reserve(4 * (n ? n : 1))) != cudaSuccess) return e;
+    if (n == 0) return cudaSuccess;
+    if ((e = c.keys_alt.reserve(8 * n)) != cudaSuccess) return e;
+    if ((e = c.perm_alt.reserve(4 * n)) != cudaSuccess) return e;
+    const uint64_t tiles = (n + kSortTile - 1) / kSortTile;
+    const size_t status_bytes = tiles * 256 * sizeof(unsigned long long);
+    if (status_bytes > c.sort_status.bytes) {
+        if ((e = c.sort_status.reserve(status_bytes)) != cudaSuccess) return e;
+        if ((e = cudaMemsetAsync(c.sort_status.ptr, 0, c.sort_status.bytes, c.stream)) != cudaSuccess) return e;
+        c.sort_epoch = 0;
+    }
+    static bool attr_set[2] = {false, false};
+    const size_t smem = onesweep_smem();
+    if (!attr_set[0]) {
+        cudaFuncSetAttribute(k_onesweep<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaFuncSetAttribute(k_onesweep<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        attr_set[0] = attr_set[1] = true;
+    }
+    DevBuf* kb[2] = {&c.keys, &c.keys_alt};
+    DevBuf* vb[2] = {&c.perm, &c.perm_alt};
+    int sel = 0;
+    bool first = true;
+    SortCtl* ctl = c.d_ctl.as<SortCtl>();
+    for (int p = 0; p < 8; ++p) {
+        if (skip[p]) continue;
+        c.sort_epoch = (c.sort_epoch + 1) & ((1u << 22) - 1);
+        if (c.sort_epoch == 0) {  // epoch wrapped: clear stale words
+            if ((e = cudaMemsetAsync(c.sort_status.ptr, 0, c.sort_status.bytes, c.stream)) != cudaSuccess) return e;
+            c.sort_epoch = 1;
+        }
+        const uint64_t* kin = kb[sel]->as<uint64_t>();
+        uint64_t* kout = kb[sel ^ 1]->as<uint64_t>();
+        const uint32_t* vin = vb[sel]->as<uint32_t>();
+        uint32_t* vout = vb[sel ^ 1]->as<uint32_t>();
+        if (first)
+            k_onesweep<true><<<(unsigned)tiles, kSortThreads, smem, c.stream>>>(
+                kin, nullptr, kout, vout, n, p, ctl, c.sort_status.as<unsigned long long>(), c.sort_epoch,
+                c.d_err.as<uint32_t>());
+        else
+            k_onesweep<false><<<(unsigned)tiles, kSortThreads, smem, c.stream>>>(
+                kin, vin, kout, vout, n, p, ctl, c.sort_status.as<unsigned long long>(), c.sort_epoch,
+                c.d_err.as<uint32_t>());
+        first = false;
+        sel ^= 1;
+    }
+    if (first) {  // every digit constant: the order is the input order
+        k_iota<<<(unsigned)((n + 255) / 256), 256, 0, c.stream>>>(c.perm.as<uint32_t>(), n);
+        sel = 0;
+    }
+    *final_sel = sel;
+    return cudaGetLastError();
+}
+
+cudaError_t launch_gather(Cloud& c, const double* d_xyz, const uint32_t* d_perm, int /*sel*/) {
+    cudaError_t e;
+    const uint64_t n = c.n;
+    const size_t b = 8 * (n ? n : 1);
+    if ((e = c.xs.reserve(b)) != cudaSuccess) return e;
+    if ((e = c.ys.reserve(b)) != cudaSuccess) return e;
+    if ((e = c.zs.reserve(b)) != cudaSuccess) return e;
+    if (n == 0) return cudaSuccess;
+    const int sms = sm_count(c.device);
+    const uint64_t want = (n + 255) / 256;
+    const int grid = (int)(want < (uint64_t)sms * 8 ? want : (uint64_t)sms * 8);
+    k_gather<<<grid, 256, 0, c.stream>>>(d_xyz, d_perm, n, c.xs.as<double>(), c.ys.as<double>(),
+                                         c.zs.as<double>());
+    return cudaGetLastError();
+}
+
+}  // namespace octb

@@ -1,0 +1,143 @@
+// Space-filling-curve keys on the device: anchor coordinates, Morton and
+// Hilbert 63-bit encode/decode, and the key algebra of the linear octree.
+#pragma once
+#include "oct_common.cuh"
+
+namespace octb {
+
+// double -> 64-bit unsigned conversion with x86-64 semantics, which is what
+// the reference's (coords_t) cast compiles to: values below 2^63 (and NaN,
+// which compares unordered) take the signed truncation, whose out-of-range
+// result is 0x8000000000000000; values from 2^63 up take (v - 2^63) and an
+// xor of the top bit.  The CUDA cast saturates instead, so it is emulated.
+__device__ __forceinline__ uint64_t x86_cvt_u64(double v) {
+    const double two63 = 9223372036854775808.0;
+    if (v != v) return 1ull << 63;
+    if (v < two63) {
+        if (v <= -two63) return 1ull << 63;
+        return (uint64_t)__double2ll_rz(v);
+    }
+    double w = dsub(v, two63);
+    uint64_t s = (w < two63) ? (uint64_t)__double2ll_rz(w) : (1ull << 63);
+    return s ^ (1ull << 63);
+}
+
+// PointEncoder::getAnchorCoords, one axis (inc/encoding/point_encoder.hpp:37-49):
+// x = min((coords_t)(((p - c) + r) / (2 r) * 2^21), 2^21 - 1)
+__device__ __forceinline__ uint32_t anchor_coord(double p, double c, double r) {
+    double t = ddiv(dadd(dsub(p, c), r), dmul(2.0, r));
+    uint64_t u = x86_cvt_u64(dmul(t, 2097152.0));
+    return (uint32_t)(u < kMaxCoord ? u : kMaxCoord);
+}
+
+// Morton: coordinate bit i goes to key bit 3i (x), 3i+1 (y), 3i+2 (z), the
+// layout of libmorton's BMI2 masks (inc/encoding/libmorton/morton_BMI.h:40-58).
+// Spread 21 bits to every third position with shift-and-mask steps.
+__device__ __forceinline__ uint64_t spread3(uint64_t v) {
+    v &= 0x1fffffull;
+    v = (v | (v << 32)) & 0x1f00000000ffffull;
+    v = (v | (v << 16)) & 0x1f0000ff0000ffull;
+    v = (v | (v << 8)) & 0x100f00f00f00f00full;
+    v = (v | (v << 4)) & 0x10c30c30c30c30c3ull;
+    v = (v | (v << 2)) & 0x1249249249249249ull;
+    return v;
+}
+__device__ __forceinline__ uint32_t compact3(uint64_t v) {
+    v &= 0x1249249249249249ull;
+    v = (v ^ (v >> 2)) & 0x10c30c30c30c30c3ull;
+    v = (v ^ (v >> 4)) & 0x100f00f00f00f00full;
+    v = (v ^ (v >> 8)) & 0x1f0000ff0000ffull;
+    v = (v ^ (v >> 16)) & 0x1f00000000ffffull;
+    v = (v ^ (v >> 32)) & 0x1fffffull;
+    return (uint32_t)v;
+}
+__device__ __forceinline__ uint64_t morton_encode(uint32_t x, uint32_t y, uint32_t z) {
+    return spread3(x) | (spread3(y) << 1) | (spread3(z) << 2);
+}
+__device__ __forceinline__ void morton_decode(uint64_t k, uint32_t& x, uint32_t& y, uint32_t& z) {
+    // the reference's X mask also covers key bit 63 (as coordinate bit 21)
+    x = compact3(k) | (uint32_t)((k >> 63) << 21);
+    y = compact3(k >> 1);
+    z = compact3(k >> 2);
+}
+
+// Hilbert: HilbertEncoder3D::encode (inc/encoding/hilbert_encoder_3d.hpp:29-66),
+// 21 levels from the top; the octant goes through {0,1,3,2,7,6,4,5}, then the
+// coordinates are reflected and rotated (zi) or x/z swapped (!yi).
+__device__ __forceinline__ uint64_t hilbert_encode(uint32_t x, uint32_t y, uint32_t z) {
+    uint64_t key = 0;
+#pragma unroll
+    for (int level = (int)kMaxDepth - 1; level >= 0; --level) {
+        const uint32_t xi = (x >> level) & 1u, yi = (y >> level) & 1u, zi = (z >> level) & 1u;
+        const uint32_t oct = (xi << 2) | (yi << 1) | zi;
+        // {0,1,3,2,7,6,4,5} packed as 3-bit fields
+        const uint32_t digit = (0xB374C8u >> (3u * oct)) & 7u;
+        key = (key << 3) | digit;
+        const uint32_t nyi = yi ^ 1u, nzi = zi ^ 1u;
+        x ^= 0u - (xi & (nyi | zi));
+        y ^= 0u - ((xi & (yi | zi)) | (yi & nzi));
+        z ^= 0u - ((xi & nyi & nzi) | (yi & nzi));
+        if (zi) {
+            const uint32_t t = x; x = y; y = z; z = t;
+        } else if (!yi) {
+            const uint32_t t = x; x = z; z = t;
+        }
+    }
+    return key;
+}
+
+// HilbertEncoder3D::decode (hilbert_encoder_3d.hpp:256-289), from the lowest level.
+__device__ __forceinline__ void hilbert_decode(uint64_t code, uint32_t& ox, uint32_t& oy, uint32_t& oz) {
+    uint32_t x = 0, y = 0, z = 0;
+#pragma unroll
+    for (uint32_t level = 0; level < kMaxDepth; ++level) {
+        const uint32_t oct = (uint32_t)(code >> (3 * level)) & 7u;
+        const uint32_t xi = oct >> 2, yi = (oct >> 1) & 1u, zi = oct & 1u;
+        if (yi ^ zi) {
+            const uint32_t t = x; x = z; z = y; y = t;
+        } else if (oct == 0u || oct == 7u) {
+            const uint32_t t = x; x = z; z = t;
+        }
+        const uint32_t mask = (1u << level) - 1u;
+        const uint32_t nxi = xi ^ 1u, nyi = yi ^ 1u, nzi = zi ^ 1u;
+        x ^= mask & (0u - (xi & (yi | zi)));
+        y ^= mask & (0u - ((xi & (nyi | nzi)) | (nxi & yi & zi)));
+        z ^= mask & (0u - ((xi & nyi & nzi) | (yi & zi)));
+        x |= xi << level;
+        y |= (xi ^ yi) << level;
+        z |= (yi ^ zi) << level;
+    }
+    ox = x; oy = y; oz = z;
+}
+
+template <int ENC>
+__device__ __forceinline__ uint64_t sfc_encode(uint32_t x, uint32_t y, uint32_t z) {
+    if constexpr (ENC == 5) return hilbert_encode(x, y, z);
+    else return morton_encode(x, y, z);
+}
+template <int ENC>
+__device__ __forceinline__ void sfc_decode(uint64_t k, uint32_t& x, uint32_t& y, uint32_t& z) {
+    if constexpr (ENC == 5) hilbert_decode(k, x, y, z);
+    else morton_decode(k, x, y, z);
+}
+
+// Key range of one node at `level` (PointEncoder::nodeRange, point_encoder.hpp:591-597).
+__device__ __forceinline__ uint64_t node_range(uint32_t level) { return 1ull << (3u * (kMaxDepth - level)); }
+
+// Node centre (PointEncoder::getCenter, point_encoder.hpp:517-539):
+// decode the start key, mask the coordinates to the level, then
+// min + c * half * 2 + radii[level] per axis.
+template <int ENC>
+__device__ __forceinline__ void node_center(uint64_t start_key, uint32_t level, const BoxD& box, const LevelGeom& g,
+                                            double out[3]) {
+    uint32_t c[3];
+    sfc_decode<ENC>(start_key, c[0], c[1], c[2]);
+    const uint32_t mask = ((1u << kMaxDepth) - 1u) ^ ((1u << (kMaxDepth - level)) - 1u);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        double lo = dadd(box.min[a], dmul(dmul((double)(c[a] & mask), g.half[a]), 2.0));
+        out[a] = dadd(lo, g.radii[level][a]);
+    }
+}
+
+}  // namespace octb

@@ -1,0 +1,189 @@
+"""Python front end over the C ABI, with the reference's names.
+
+``LinearOctree(points, encoder, max_points_leaf)`` does what the reference's
+``PointEncoder::sortPoints`` (inc/encoding/point_encoder.hpp:484-503) followed by
+the ``LinearOctree<Container>`` constructor (inc/structures/linear_octree.hpp:
+614-623) do, on the GPU; the search methods are batched forms of
+``neighbors`` / ``neighborsPrune`` / ``neighborsStruct`` / ``knn``
+(linear_octree.hpp:695-942, 1038-1087): they take an (nq, 3) array of centres
+instead of one ``Point``.  As in the reference, the default kernel of the
+scalar-radius overloads is ``square``.
+
+Host (numpy) inputs go through the host-buffer form of the ABI; CUDA torch
+tensors go through the device-buffer form (``OCT_MEM_DEVICE``).
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from . import capi
+from .capi import ALGOS, ENCODERS, KERNELS, OCT_MEM_DEVICE, OctParams, OctTreeInfo, check, lib
+
+
+def _ptr(a) -> int:
+    if a is None:
+        return None
+    if isinstance(a, np.ndarray):
+        return a.ctypes.data
+    return a.data_ptr()  # torch tensor
+
+
+def _is_device(a) -> bool:
+    return not isinstance(a, np.ndarray) and getattr(a, "is_cuda", False)
+
+
+def _host_f64(a, shape_last=None):
+    a = np.ascontiguousarray(a, dtype=np.float64)
+    if shape_last is not None and a.ndim == 1:
+        a = a.reshape(-1, shape_last)
+    return a
+
+
+class LinearOctree:
+    """A device-resident cloud, SFC-sorted, with its linear octree built."""
+
+    def __init__(self, points, encoder="hilbert", max_points_leaf: int = 128, device: int = 0,
+                 radius_group: int = 8, stream=None):
+        L = lib()
+        self._L = L
+        self.encoder = ENCODERS[encoder]
+        self.max_points_leaf = int(max_points_leaf)
+        p = OctParams(self.max_points_leaf, self.encoder, device, 0)
+        h = C.c_void_p()
+        st = L.oct_cloud_create(C.byref(p), C.byref(h))
+        check(st, None, "oct_cloud_create")
+        self._h = h
+        if stream is not None:
+            check(L.oct_cloud_set_stream(h, C.c_void_p(stream)), h, "oct_cloud_set_stream")
+        check(L.oct_set_radius_group(h, radius_group), h)
+        dev = _is_device(points)
+        if not dev:
+            points = _host_f64(points, 3)
+        self.n = int(points.shape[0])
+        check(L.oct_set_points(h, _ptr(points), self.n, OCT_MEM_DEVICE if dev else 0), h, "oct_set_points")
+        box = np.zeros(12)
+        check(L.oct_encode_sort(h, box.ctypes.data, None, None, None, 0), h, "oct_encode_sort")
+        self.box = box
+        info = OctTreeInfo()
+        check(L.oct_build(h, C.byref(info)), h, "oct_build")
+        self.n_leaf = info.n_leaf
+        self.n_internal = info.n_internal
+        self.n_total = info.n_total
+        self.max_depth_seen = info.max_depth_seen
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.oct_cloud_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    def set_radius_group(self, lanes: int):
+        check(self._L.oct_set_radius_group(self._h, int(lanes)), self._h)
+
+    # ---- sortPoints outputs ------------------------------------------------
+    def sorted_points(self):
+        """(keys uint64[n], perm uint32[n], sorted xyz float64[n, 3]) - the
+        reordered cloud, the codes and the original ids of sortPoints."""
+        n = self.n
+        keys = np.zeros(n, np.uint64)
+        perm = np.zeros(n, np.uint32)
+        xyz = np.zeros((n, 3), np.float64)
+        check(self._L.oct_encode_sort(self._h, None, keys.ctypes.data, perm.ctypes.data, xyz.ctypes.data, 0),
+              self._h, "oct_encode_sort")
+        return keys, perm, xyz
+
+    def export(self):
+        """The tree arrays: offsets, ranges, centers, radii (precomputedRadii), half (halfLengths)."""
+        nt = self.n_total
+        off = np.zeros(nt + 1, np.uint32)
+        rng = np.zeros((nt, 2), np.uint64)
+        ctr = np.zeros((nt, 3), np.float64)
+        rad = np.zeros((22, 3), np.float64)
+        half = np.zeros(3, np.float64)
+        check(self._L.oct_tree_export(self._h, off.ctypes.data, rng.ctypes.data, ctr.ctypes.data, rad.ctypes.data,
+                                      half.ctypes.data, 0), self._h, "oct_tree_export")
+        return dict(offsets=off, ranges=rng, centers=ctr, radii=rad, half=half)
+
+    # ---- searches -------------------------------------------------------------
+    def _radii(self, centers, radius):
+        if np.ndim(radius) == 0:
+            return None, float(radius)
+        r = np.ascontiguousarray(radius, dtype=np.float64)
+        assert r.shape[0] == centers.shape[0]
+        return r, 0.0
+
+    def radius_search(self, centers, radius, kernel="square", algo="neighborsPrune"):
+        """CSR result: offsets uint64[nq + 1], indices uint32 (each query ascending)."""
+        L, h = self._L, self._h
+        centers = _host_f64(centers, 3)
+        nq = centers.shape[0]
+        radii, r0 = self._radii(centers, radius)
+        offs = np.zeros(nq + 1, np.uint64)
+        total = C.c_uint64(0)
+        # first call sizes the output (OCT_ERR_CAPACITY is expected when it is non-empty)
+        st = L.oct_radius_search(h, KERNELS[kernel], ALGOS[algo], centers.ctypes.data, nq, _ptr(radii), r0,
+                                 offs.ctypes.data, None, 0, C.byref(total), 0)
+        if st == capi.OCT_ERR_CAPACITY or (st == capi.OCT_OK and total.value == 0):
+            idx = np.zeros(max(1, total.value), np.uint32)
+            if total.value:
+                st = L.oct_radius_search(h, KERNELS[kernel], ALGOS[algo], centers.ctypes.data, nq, _ptr(radii), r0,
+                                         offs.ctypes.data, idx.ctypes.data, idx.shape[0], C.byref(total), 0)
+        check(st, h, "oct_radius_search")
+        return offs, idx[: total.value]
+
+    def neighbors(self, centers, radius, kernel="square"):
+        return self.radius_search(centers, radius, kernel, "neighbors")
+
+    def neighborsPrune(self, centers, radius, kernel="square"):
+        return self.radius_search(centers, radius, kernel, "neighborsPrune")
+
+    def neighborsStruct(self, centers, radius, kernel="square"):
+        """NeighborSet per query: (range offsets uint64[nq+1], pairs uint32[m, 2], numberOfPoints uint64[nq])."""
+        L, h = self._L, self._h
+        centers = _host_f64(centers, 3)
+        nq = centers.shape[0]
+        radii, r0 = self._radii(centers, radius)
+        offs = np.zeros(nq + 1, np.uint64)
+        pts = np.zeros(nq, np.uint64)
+        total = C.c_uint64(0)
+        st = L.oct_struct_search(h, KERNELS[kernel], centers.ctypes.data, nq, _ptr(radii), r0, offs.ctypes.data,
+                                 None, 0, C.byref(total), pts.ctypes.data, 0)
+        pairs = np.zeros((max(1, total.value), 2), np.uint32)
+        if st == capi.OCT_ERR_CAPACITY:
+            st = L.oct_struct_search(h, KERNELS[kernel], centers.ctypes.data, nq, _ptr(radii), r0, offs.ctypes.data,
+                                     pairs.ctypes.data, total.value, C.byref(total), pts.ctypes.data, 0)
+        check(st, h, "oct_struct_search")
+        return offs, pairs[: total.value], pts
+
+    def radius_count(self, centers, radius, kernel="square", algo="neighborsPrune"):
+        L, h = self._L, self._h
+        centers = _host_f64(centers, 3)
+        nq = centers.shape[0]
+        radii, r0 = self._radii(centers, radius)
+        cnt = np.zeros(nq, np.uint64)
+        check(L.oct_radius_count(h, KERNELS[kernel], ALGOS[algo], centers.ctypes.data, nq, _ptr(radii), r0,
+                                 cnt.ctypes.data, 0), h, "oct_radius_count")
+        return cnt
+
+    def knn(self, centers, k: int):
+        """(idx uint32[nq, k], d2 float64[nq, k], counts uint32[nq])."""
+        L, h = self._L, self._h
+        centers = _host_f64(centers, 3)
+        nq = centers.shape[0]
+        idx = np.zeros((nq, k), np.uint32)
+        d2 = np.zeros((nq, k), np.float64)
+        cnt = np.zeros(nq, np.uint32)
+        check(L.oct_knn(h, centers.ctypes.data, nq, k, idx.ctypes.data, d2.ctypes.data, cnt.ctypes.data, 0), h,
+              "oct_knn")
+        return idx, d2, cnt

@@ -1,0 +1,108 @@
+"""Deterministic synthetic airborne-LiDAR tiles.
+
+The reference benchmarks real clouds (Paris-Lille-3D, DALES, Semantic3D,
+Speulderbos; bench_neighbors.bash:7-21) that are not available here; these
+seeded tiles stand in for them with the same shape of data:
+
+* x, y uniform over a square tile of side ``tile_m`` metres;
+* 85 % of the points are terrain: z = sum of 4 sinusoids (wavelengths 50, 100,
+  200 and 400 m, random directions and phases, total amplitude 20 m) plus
+  Gaussian noise of sigma 0.05 m;
+* 15 % are canopy/building clusters: ``n_cyl`` vertical cylinders of radius
+  2-15 m; points are area-uniform in the cylinder's disk, with z uniform from
+  the terrain up to the cylinder's height (3-25 m above the terrain).
+
+Everything is drawn from ``numpy.random.default_rng(seed)``, so a (n, tile,
+seed) triple always gives the same float64 (n, 3) array.  Query centres are
+cloud points picked uniformly at random, as the reference's SearchSet does
+(inc/benchmarking/search_set.hpp:23-44); its mt19937(42) stream is replaced by
+numpy's PCG64 with the same seed.
+"""
+from __future__ import annotations
+
+import math
+
+import numpy as np
+
+WAVELENGTHS = (50.0, 100.0, 200.0, 400.0)
+AMPLITUDE = 20.0 / len(WAVELENGTHS)
+
+
+def _terrain(x, y, dirs, phases):
+    z = np.zeros_like(x)
+    for lam, th, ph in zip(WAVELENGTHS, dirs, phases):
+        z += AMPLITUDE * np.sin((2.0 * math.pi / lam) * (x * math.cos(th) + y * math.sin(th)) + ph)
+    return z
+
+
+def lidar_tile(n: int, tile_m: float, seed: int, n_cyl: int = 300, canopy_frac: float = 0.15,
+               noise: float = 0.05) -> np.ndarray:
+    """One synthetic tile of ``n`` points, float64 (n, 3), in random order."""
+    rng = np.random.default_rng(seed)
+    dirs = rng.uniform(0.0, math.pi, len(WAVELENGTHS))
+    phases = rng.uniform(0.0, 2.0 * math.pi, len(WAVELENGTHS))
+    n_can = int(round(n * canopy_frac)) if n_cyl > 0 else 0
+    n_ter = n - n_can
+    out = np.empty((n, 3), np.float64)
+    x = rng.uniform(0.0, tile_m, n_ter)
+    y = rng.uniform(0.0, tile_m, n_ter)
+    out[:n_ter, 0] = x
+    out[:n_ter, 1] = y
+    out[:n_ter, 2] = _terrain(x, y, dirs, phases) + rng.normal(0.0, noise, n_ter)
+    if n_can:
+        cr = np.minimum(rng.uniform(2.0, 15.0, n_cyl), 0.25 * tile_m)
+        cx = rng.uniform(cr, tile_m - cr)
+        cy = rng.uniform(cr, tile_m - cr)
+        ch = rng.uniform(3.0, 25.0, n_cyl)
+        w = cr * cr
+        which = rng.choice(n_cyl, size=n_can, p=w / w.sum())
+        rad = cr[which] * np.sqrt(rng.uniform(0.0, 1.0, n_can))
+        ang = rng.uniform(0.0, 2.0 * math.pi, n_can)
+        px = cx[which] + rad * np.cos(ang)
+        py = cy[which] + rad * np.sin(ang)
+        out[n_ter:, 0] = px
+        out[n_ter:, 1] = py
+        out[n_ter:, 2] = _terrain(px, py, dirs, phases) + rng.uniform(0.0, 1.0, n_can) * ch[which]
+    # random input order, as a LAS file would deliver it
+    return out[rng.permutation(n)]
+
+
+def query_indices(n_queries: int, cloud_size: int, seed: int = 42) -> np.ndarray:
+    """SearchSet-style random centre indices into the (sorted) cloud."""
+    rng = np.random.default_rng(seed)
+    return rng.integers(0, cloud_size, n_queries, dtype=np.int64)
+
+
+# The workloads the benchmark and the parity tests use, by name.
+CONFIGS = {
+    # 1M points, 500 m tile, seed 0, Morton, leaf 128; sphere r = 2.5 and 5.0, 10k centres
+    "c1_1M_morton": dict(n=1_000_000, tile_m=500.0, seed=0, encoder=1, max_leaf=128),
+    # 10M points, 1.5 km tile, seed 1, Hilbert, leaf 64; r = 1, 2.5, 5; k = 10, 50, 250
+    "c2_10M_hilbert": dict(n=10_000_000, tile_m=1500.0, seed=1, encoder=5, max_leaf=64),
+}
+
+
+def config_cloud(name: str, n: int | None = None) -> tuple[np.ndarray, dict]:
+    """Cloud of a named configuration; ``n`` scales it down at constant density."""
+    cfg = dict(CONFIGS[name])
+    if n is not None and n != cfg["n"]:
+        cfg["tile_m"] = cfg["tile_m"] * math.sqrt(n / cfg["n"])
+        cfg["n"] = n
+    xyz = lidar_tile(cfg["n"], cfg["tile_m"], cfg["seed"])
+    return xyz, cfg
+
+
+def batched_clouds(n_clouds: int = 256, seed: int = 2, n_min: int = 10_000, n_max: int = 2_000_000):
+    """Cloud descriptors of the multi-cloud (batched) workload: sizes log-uniform
+    in [n_min, n_max], density 4-40 points/m^2, Morton or Hilbert, leaf 32/64/128,
+    1k-200k query centres each (half radius r ~ U[0.5, 5], half kNN k in {10, 50})."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for c in range(n_clouds):
+        n = int(round(math.exp(rng.uniform(math.log(n_min), math.log(n_max)))))
+        dens = rng.uniform(4.0, 40.0)
+        tile = math.sqrt(n / dens)
+        out.append(dict(n=n, tile_m=tile, seed=int(rng.integers(0, 2**31 - 1)),
+                        encoder=int(rng.choice([1, 5])), max_leaf=int(rng.choice([32, 64, 128])),
+                        n_queries=int(rng.integers(1_000, 200_001))))
+    return out

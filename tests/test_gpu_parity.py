@@ -1,0 +1,143 @@
+"""Parity of the CUDA path against the reference's outputs (golden fixtures)
+and the CPU oracle, through the C ABI.  Bit-exact: keys, sort permutation, Box,
+octree arrays, every neighbour set (as sorted index sets), neighborsStruct
+ranges, kNN squared distances (ties at the k-th distance by lowest index)."""
+import glob
+import os
+
+import numpy as np
+import pytest
+
+from octrees_benchmark_b200 import LinearOctree
+from octrees_benchmark_b200.synth import lidar_tile, query_indices
+from tests.parity import assert_csr_equal, assert_knn_equal, assert_ranges_equal, same_f64
+
+pytestmark = pytest.mark.gpu
+
+GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
+CLOUDS = sorted(p for p in glob.glob(os.path.join(GOLDEN, "*.npz")) if not p.endswith("keys_anchor.npz"))
+KERNELS = {"sphere": 1, "circle": 0, "cube": 3, "square": 2}
+ALGO_NAMES = {1: "neighbors", 2: "neighborsPrune", 3: "neighborsStruct"}
+
+
+def load(path):
+    with np.load(path) as z:
+        return {k: z[k] for k in z.files}
+
+
+def check_cloud_against(oc, keys, ids, box, sxyz, info, arrays):
+    gk, gp, gx = oc.sorted_points()
+    assert same_f64(oc.box, box)
+    assert np.array_equal(gk, keys)
+    assert np.array_equal(gp.astype(np.uint64), np.asarray(ids, np.uint64))
+    assert same_f64(gx, sxyz)
+    assert [oc.n, oc.n_leaf, oc.n_internal, oc.n_total, oc.max_depth_seen] == [int(v) for v in info]
+    ex = oc.export()
+    assert np.array_equal(ex["offsets"], arrays["offsets"])
+    assert np.array_equal(ex["ranges"], np.asarray(arrays["ranges"], np.uint64))
+    for k in ("centers", "radii", "half"):
+        assert same_f64(ex[k], arrays[k]), k
+
+
+@pytest.mark.parametrize("path", CLOUDS, ids=[os.path.basename(p)[:-4] for p in CLOUDS])
+@pytest.mark.parametrize("group", [8, 32])
+def test_gpu_matches_reference_fixture(path, group):
+    g = load(path)
+    oc = LinearOctree(g["xyz"], encoder=int(g["encoder"]), max_points_leaf=int(g["max_leaf"]), radius_group=group)
+    arrays = {k[5:]: v for k, v in g.items() if k.startswith("tree_")}
+    check_cloud_against(oc, g["keys"], g["ids"], g["box"], g["sorted_xyz"], g["info"], arrays)
+    q = g["centers"]
+    sxyz = g["sorted_xyz"]
+    for ri, r in enumerate(g["radii"]):
+        for kn in KERNELS:
+            for algo in (1, 2, 3):
+                offs, idx = oc.radius_search(q, r, kn, ALGO_NAMES[algo])
+                assert_csr_equal(offs, idx, g[f"rad_{ri}_{kn}_{algo}_offs"], g[f"rad_{ri}_{kn}_{algo}_idx"],
+                                 f"{kn} {ALGO_NAMES[algo]} r={r}")
+                cnt = oc.radius_count(q, r, kn, ALGO_NAMES[algo])
+                assert np.array_equal(cnt, np.diff(g[f"rad_{ri}_{kn}_{algo}_offs"].astype(np.int64)))
+            ro, pairs, npts = oc.neighborsStruct(q, r, kn)
+            assert_ranges_equal(ro, pairs, g[f"struct_{ri}_{kn}_offs"], g[f"struct_{ri}_{kn}_pairs"], kn)
+            assert np.array_equal(npts, np.diff(g[f"rad_{ri}_{kn}_3_offs"].astype(np.int64)))
+    for k in g["ks"]:
+        k = int(k)
+        idx, d2, cnt = oc.knn(q, k)
+        assert_knn_equal(idx, d2, cnt, g[f"knn_{k}_idx"], g[f"knn_{k}_d2"], g[f"knn_{k}_cnt"], sxyz, q, f"k={k}")
+    oc.close()
+
+
+SYNTH = [
+    # (n, tile, seed, encoder, leaf)
+    (200_000, 220.0, 31, 5, 64),
+    (200_000, 220.0, 32, 1, 128),
+    (50_000, 60.0, 33, 5, 16),
+    (30_000, 50.0, 34, 1, 1),
+]
+
+
+@pytest.fixture(scope="module")
+def synth_cases(port):
+    out = []
+    for n, tile, seed, enc, leaf in SYNTH:
+        xyz = lidar_tile(n, tile, seed)
+        if leaf == 1:
+            xyz[::5] = xyz[11]  # exact duplicates force level-21 leaves
+        keys, perm, box, sxyz = port.encode_sort(enc, xyz)
+        t = port.build(enc, keys, leaf, box)
+        out.append((xyz, enc, leaf, keys, perm, box, sxyz, t))
+    return out
+
+
+@pytest.mark.parametrize("case", range(len(SYNTH)))
+def test_gpu_build_matches_oracle(synth_cases, case):
+    xyz, enc, leaf, keys, perm, box, sxyz, t = synth_cases[case]
+    oc = LinearOctree(xyz, encoder=enc, max_points_leaf=leaf)
+    info = [t.n, t.n_leaf, t.n_internal, t.n_total, t.max_depth]
+    check_cloud_against(oc, keys, perm, box, sxyz, info, t.arrays())
+    oc.close()
+
+
+@pytest.mark.parametrize("case", range(len(SYNTH)))
+@pytest.mark.parametrize("group", [8, 16, 32])
+def test_gpu_radius_matches_oracle(synth_cases, case, group):
+    xyz, enc, leaf, keys, perm, box, sxyz, t = synth_cases[case]
+    oc = LinearOctree(xyz, encoder=enc, max_points_leaf=leaf, radius_group=group)
+    q = sxyz[query_indices(400, len(sxyz), seed=case)]
+    radii = [0.5, 2.5, 5.0] if group == 8 else [2.5]
+    for r in radii:
+        for kn, kv in KERNELS.items():
+            for algo in (1, 2, 3):
+                offs, idx = oc.radius_search(q, r, kn, ALGO_NAMES[algo])
+                o2, i2 = t.radius(sxyz, kv, algo, q, r)
+                assert_csr_equal(offs, idx, o2, i2, f"{kn} {ALGO_NAMES[algo]} r={r}")
+                # every query's output is ascending (octants are visited in key order)
+                d = np.diff(idx.astype(np.int64))
+                mask = np.ones(len(d), bool)
+                starts = offs[1:-1].astype(np.int64)
+                mask[starts[(starts >= 1) & (starts <= len(d))] - 1] = False
+                assert np.all(d[mask] > 0)
+            ro, pairs, npts = oc.neighborsStruct(q, r, kn)
+            o2, p2 = t.struct_ranges(sxyz, kv, q, r)
+            assert_ranges_equal(ro, pairs, o2, p2, kn)
+    # per-query radii
+    rr = np.random.default_rng(case).uniform(0.5, 5.0, len(q))
+    offs, idx = oc.neighborsPrune(q, rr, "sphere")
+    o2, i2 = t.radius(sxyz, 1, 2, q, rr)
+    assert_csr_equal(offs, idx, o2, i2, "per-query radii")
+    oc.close()
+
+
+@pytest.mark.parametrize("case", range(len(SYNTH)))
+def test_gpu_knn_matches_oracle(synth_cases, case):
+    xyz, enc, leaf, keys, perm, box, sxyz, t = synth_cases[case]
+    oc = LinearOctree(xyz, encoder=enc, max_points_leaf=leaf)
+    q = sxyz[query_indices(300, len(sxyz), seed=100 + case)]
+    # also centres that are not cloud points
+    q = np.concatenate([q, q[:50] + np.random.default_rng(case).normal(0, 1.0, (50, 3))])
+    for k in (1, 10, 50, 250, 1000):
+        idx, d2, cnt = oc.knn(q, k)
+        i2, d22, c2 = t.knn(sxyz, q, k)
+        assert_knn_equal(idx, d2, cnt, i2, d22, c2, sxyz, q, f"k={k}")
+        # the oracle applies the same tie rule: identical arrays
+        assert np.array_equal(idx[:, :].astype(np.int64)[d2 < np.inf], i2.astype(np.int64)[d22 < np.inf])
+    oc.close()
