@@ -51,8 +51,11 @@ int cuda_fail(Cloud& c, cudaError_t e, const char* what) {
 constexpr size_t kPinnedBytes = 4096;
 
 // Synchronise the stream and turn the latched device error word into a status.
+// Pinned staging layout: [0, 2048) readbacks of structs, [2048, 2056) the error word.
+constexpr size_t kPinnedErrOffset = 2048;
+
 int sync_and_check(Cloud& c, uint32_t ignore_bits = 0) {
-    uint32_t* h = static_cast<uint32_t*>(c.pinned);
+    uint32_t* h = reinterpret_cast<uint32_t*>(static_cast<unsigned char*>(c.pinned) + kPinnedErrOffset);
     CK(cudaMemcpyAsync(h, c.d_err.ptr, 4, cudaMemcpyDeviceToHost, c.stream));
     CK(cudaStreamSynchronize(c.stream));
     const uint32_t bits = *h & ~ignore_bits;
@@ -121,6 +124,35 @@ int radius_common(Cloud& c, int kernel, int algo, const double* centers, uint64_
     if ((st = stage_in(c, c.q_centers, centers, 3 * nq, device, dq)) != OCT_OK) return st;
     if ((st = stage_in(c, c.q_radii, radii, nq, device, dr)) != OCT_OK) return st;
     (void)radius;
+    return OCT_OK;
+}
+
+// Outputs of a finished sort: the Box, keys, permutation, reordered points.
+int emit_sorted(Cloud& c, double* box12, uint64_t* keys, uint32_t* perm, double* sorted_xyz, bool dev) {
+    int st;
+    if (box12) {
+        for (int a = 0; a < 3; ++a) {
+            box12[a] = c.box.center[a];
+            box12[3 + a] = c.box.radii[a];
+            box12[6 + a] = c.box.min[a];
+            box12[9 + a] = c.box.max[a];
+        }
+    }
+    const uint64_t n = c.n;
+    if ((st = copy_out(c, keys, c.keys.as<uint64_t>(), n, dev)) != OCT_OK) return st;
+    if ((st = copy_out(c, perm, c.perm.as<uint32_t>(), n, dev)) != OCT_OK) return st;
+    if (sorted_xyz && n) {
+        double* dst = sorted_xyz;
+        if (!dev) {
+            CK(c.q_out.reserve(24 * n));
+            dst = c.q_out.as<double>();
+        }
+        k_soa_to_aos<<<(unsigned)((n + 255) / 256), 256, 0, c.stream>>>(c.xs.as<double>(), c.ys.as<double>(),
+                                                                        c.zs.as<double>(), n, dst);
+        CK(cudaGetLastError());
+        if (!dev) CK(cudaMemcpyAsync(sorted_xyz, dst, 24 * n, cudaMemcpyDeviceToHost, c.stream));
+    }
+    if (!dev) CK(cudaStreamSynchronize(c.stream));
     return OCT_OK;
 }
 
@@ -253,6 +285,7 @@ int oct_encode_sort(oct_cloud h, double* box12, uint64_t* keys, uint32_t* perm, 
     Cloud& c = h->c;
     DeviceGuard g(c.device);
     const bool dev = flags & OCT_MEM_DEVICE;
+    if (c.sorted) return emit_sorted(c, box12, keys, perm, sorted_xyz, dev);  // points unchanged since the last sort
     const double* xyz = c.xyz_in.as<double>();
     CK(cudaMemsetAsync(c.d_err.ptr, 0, 4, c.stream));
     CK(launch_bbox_encode(c, xyz));
@@ -279,30 +312,7 @@ int oct_encode_sort(oct_cloud h, double* box12, uint64_t* keys, uint32_t* perm, 
     c.sorted = true;
     c.built = false;
     c.node_capacity = 0;
-    if (box12) {
-        for (int a = 0; a < 3; ++a) {
-            box12[a] = c.box.center[a];
-            box12[3 + a] = c.box.radii[a];
-            box12[6 + a] = c.box.min[a];
-            box12[9 + a] = c.box.max[a];
-        }
-    }
-    const uint64_t n = c.n;
-    if ((st = copy_out(c, keys, c.keys.as<uint64_t>(), n, dev)) != OCT_OK) return st;
-    if ((st = copy_out(c, perm, c.perm.as<uint32_t>(), n, dev)) != OCT_OK) return st;
-    if (sorted_xyz && n) {
-        double* dst = sorted_xyz;
-        if (!dev) {
-            CK(c.q_out.reserve(24 * n));
-            dst = c.q_out.as<double>();
-        }
-        k_soa_to_aos<<<(unsigned)((n + 255) / 256), 256, 0, c.stream>>>(c.xs.as<double>(), c.ys.as<double>(),
-                                                                        c.zs.as<double>(), n, dst);
-        CK(cudaGetLastError());
-        if (!dev) CK(cudaMemcpyAsync(sorted_xyz, dst, 24 * n, cudaMemcpyDeviceToHost, c.stream));
-    }
-    if (!dev) CK(cudaStreamSynchronize(c.stream));
-    return OCT_OK;
+    return emit_sorted(c, box12, keys, perm, sorted_xyz, dev);
 }
 
 int oct_build(oct_cloud h, oct_tree_info* info) {

@@ -294,8 +294,10 @@ __global__ void __launch_bounds__(kSortThreads) k_onesweep(const uint64_t* __res
         const uint64_t key = skeys[s];
         const uint32_t dd = (uint32_t)((key >> shift) & 255u);
         const unsigned long long o = gbase[dd] + (s - tstart[dd]);
-        kout[o] = key;
-        vout[o] = svals[s];
+        if (o < n) {  // always true unless a look-back gave up (then err is set)
+            kout[o] = key;
+            vout[o] = svals[s];
+        }
     }
 }
 
@@ -308,7 +310,8 @@ __global__ void k_gather(const double* __restrict__ xyz, const uint32_t* __restr
                          double* __restrict__ xs, double* __restrict__ ys, double* __restrict__ zs) {
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
     for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-        const uint64_t j = perm[i];
+        uint64_t j = perm[i];
+        if (j >= n) j = 0;  // a permutation never does this; guards a failed sort
         xs[i] = xyz[3 * j];
         ys[i] = xyz[3 * j + 1];
         zs[i] = xyz[3 * j + 2];
