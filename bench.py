@@ -384,6 +384,7 @@ def run_b200(args, rank, world, local_rank):
 
 
 def main():
+    global N_POINTS, TILE_M, Q_RADIUS, Q_KNN
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
@@ -393,7 +394,13 @@ def main():
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--points", type=int, default=N_POINTS, help="cloud size (smaller cases for profiling)")
+    ap.add_argument("--queries", type=int, default=Q_RADIUS, help="radius and kNN queries per step, each")
     args = ap.parse_args()
+    if args.points != N_POINTS:
+        TILE_M = TILE_M * math.sqrt(args.points / N_POINTS)  # same point density
+        N_POINTS = args.points
+    Q_RADIUS = Q_KNN = args.queries
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
