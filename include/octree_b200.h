@@ -13,7 +13,7 @@
  * The reference has no FFI; its interface is the C++ template API that these
  * entry points replace (file:line in the reference tree is given per function).
  * A header-only C++ wrapper with the reference's method names sits on top of
- * this ABI (octrees_benchmark_b200/csrc/linear_octree_gpu.hpp).
+ * this ABI (include/linear_octree_gpu.hpp).
  *
  * Conventions
  *  - Every function returns an oct_status; none exits or throws.
@@ -163,6 +163,35 @@ int oct_struct_search(oct_cloud cloud, int kernel, const double* centers, uint64
  * UINT32_MAX / +inf.  counts may be NULL. */
 int oct_knn(oct_cloud cloud, const double* centers, uint64_t nq, uint32_t k, uint32_t* idx, double* d2,
             uint32_t* counts, uint32_t flags);
+
+/* Largest cloud oct_encode_sort_noalloc accepts. */
+#define OCT_NOALLOC_MAX_POINTS (1u << 18) /* 262,144 points */
+
+/* Allocation-free bounding box + SFC keys + stable sort, for callers that
+ * cannot allocate device memory when they call in: code running inside a
+ * memory pool or allocator it does not own, plugin hosts that forbid
+ * cudaMalloc / cudaFree on their streams, and latency-bound loops that cannot
+ * afford the device-wide synchronisation cudaMalloc / cudaFree cause.  No
+ * counterpart in the reference (whose PointEncoder::sortPoints allocates on
+ * the host heap); it computes what oct_encode_sort computes, bit for bit.
+ *
+ * All pointers are device memory of the current CUDA device: d_xyz (n x 3
+ * doubles, AoS), d_keys (n sorted keys), d_perm (n input positions of the
+ * sorted points) and d_box12 (12 doubles: center, radii, min, max).  The work
+ * is queued on `stream` (a cudaStream_t, NULL for the default stream) and the
+ * call returns without waiting.  It calls no cudaMalloc, cudaFree or other
+ * allocating routine: its scratch is one fixed device array of about 3.2 MB,
+ * which every GPU that loads this library holds until the process exits.
+ * Limits and rules:
+ *  - n above OCT_NOALLOC_MAX_POINTS is rejected with OCT_ERR_INVALID_ARG;
+ *  - the first call on a device looks up the scratch array's device address
+ *    (once per device, with that device current); make that first call before
+ *    any stream capture;
+ *  - every call on a device shares the one scratch array and clears what must
+ *    start at zero itself, so calls whose work overlaps on the GPU (other
+ *    streams, other host threads) race and must be serialised by the caller. */
+int oct_encode_sort_noalloc(int encoder, const double* d_xyz, uint64_t n, uint64_t* d_keys, uint32_t* d_perm,
+                            double* d_box12, void* stream);
 
 #ifdef __cplusplus
 }

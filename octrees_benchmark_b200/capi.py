@@ -22,6 +22,7 @@ OCT_ERR_CAPACITY = 5
 OCT_ERR_DEVICE_LIMIT = 6
 OCT_ERR_NO_DEVICE = 7
 OCT_MEM_DEVICE = 0x1
+OCT_NOALLOC_MAX_POINTS = 1 << 18
 
 ENCODERS = {"morton": 1, "mort": 1, "hilbert": 5, "hilb": 5, 1: 1, 5: 5}
 KERNELS = {"circle": 0, "sphere": 1, "square": 2, "cube": 3, 0: 0, 1: 1, 2: 2, 3: 3}
@@ -69,6 +70,7 @@ SIGNATURES = {
     "oct_radius_count": ([_vp, _int, _int, _vp, _u64, _vp, _dbl, _vp, _u32], _int),
     "oct_struct_search": ([_vp, _int, _vp, _u64, _vp, _dbl, _vp, _vp, _u64, C.POINTER(_u64), _vp, _u32], _int),
     "oct_knn": ([_vp, _vp, _u64, _u32, _vp, _vp, _vp, _u32], _int),
+    "oct_encode_sort_noalloc": ([_int, _vp, _u64, _vp, _vp, _vp, _vp], _int),
 }
 
 

@@ -19,6 +19,7 @@
 //    skipped.  Values are generated on the fly in the first pass.
 //  * k_gather: reorders the coordinates into SoA float64 arrays.
 #include <cfloat>
+#include <mutex>
 
 #include "cloud.h"
 #include "sfc.cuh"
@@ -433,4 +434,118 @@ cudaError_t launch_gather(Cloud& c, const double* d_xyz, const uint32_t* d_perm,
     return cudaGetLastError();
 }
 
+// ---------------------------------------------------------------------------
+// Allocation-free encode + sort (oct_encode_sort_noalloc).
+//
+// For callers that cannot allocate device memory at call time: code that runs
+// inside a memory pool or allocator it does not own, a plugin host that
+// forbids cudaMalloc/cudaFree on its streams, or a real-time loop that must
+// not block on the allocator (cudaMalloc/cudaFree synchronise the device).
+// The caller passes device buffers for the points and every output; the
+// scratch the sort needs (second key/id buffer, look-back words, histograms,
+// bounding-box partials) lives in the fixed array below, which every GPU that
+// loads this library holds until the process exits.
+// ---------------------------------------------------------------------------
+
+constexpr uint64_t kNoAllocTiles = (OCT_NOALLOC_MAX_POINTS + kSortTile - 1) / kSortTile;
+constexpr int kNoAllocBboxGrid = 148 * 4;
+
+struct NoAllocScratch {
+    uint64_t keys_alt[OCT_NOALLOC_MAX_POINTS];            // 2 MiB
+    uint32_t perm_alt[OCT_NOALLOC_MAX_POINTS];            // 1 MiB
+    unsigned long long status[kNoAllocTiles * 256];       // 128 KiB look-back words
+    SortCtl ctl;
+    BoxGeom bg;
+    double partial[6 * kNoAllocBboxGrid];
+};
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[sizeof(NoAllocScratch)];
+
+namespace {
+
+std::mutex g_noalloc_mu;
+NoAllocScratch* g_noalloc_ptr[64] = {nullptr};
+
+// Device address of the scratch array on the current device.  The array's
+// name is only a host-side stand-in in host code, so the address comes from
+// cudaGetSymbolAddress, once per device, with that device current.
+int noalloc_setup(int dev, NoAllocScratch** out) {
+    if (dev < 0 || dev >= 64) return OCT_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+        void* p = nullptr;
+        cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess || p == nullptr) {
+            cudaGetLastError();
+            return OCT_ERR_CUDA;
+        }
+        const int smem = (int)onesweep_smem();
+        if (cudaFuncSetAttribute(k_onesweep<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) != cudaSuccess ||
+            cudaFuncSetAttribute(k_onesweep<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem) !=
+                cudaSuccess) {
+            cudaGetLastError();
+            return OCT_ERR_CUDA;
+        }
+        g_noalloc_ptr[dev] = static_cast<NoAllocScratch*>(p);
+    }
+    *out = g_noalloc_ptr[dev];
+    return OCT_OK;
+}
+
+}  // namespace
+
 }  // namespace octb
+
+extern "C" int oct_encode_sort_noalloc(int encoder, const double* d_xyz, uint64_t n, uint64_t* d_keys,
+                                       uint32_t* d_perm, double* d_box12, void* stream) {
+    using namespace octb;
+    if (encoder != OCT_ENC_MORTON_3D && encoder != OCT_ENC_HILBERT_3D) return OCT_ERR_INVALID_ARG;
+    if (n > OCT_NOALLOC_MAX_POINTS) return OCT_ERR_INVALID_ARG;
+    if (n && (!d_xyz || !d_keys || !d_perm)) return OCT_ERR_INVALID_ARG;
+    if (!d_box12) return OCT_ERR_INVALID_ARG;
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess) {
+        cudaGetLastError();
+        return OCT_ERR_NO_DEVICE;
+    }
+    NoAllocScratch* sc = nullptr;
+    int st = noalloc_setup(dev, &sc);
+    if (st != OCT_OK) return st;
+    cudaStream_t s = static_cast<cudaStream_t>(stream);
+    SortCtl* ctl = &sc->ctl;
+    const uint64_t tiles = (n + kSortTile - 1) / kSortTile;
+    // every call shares the scratch: clear what must start at zero
+    if (cudaMemsetAsync(ctl, 0, sizeof(SortCtl), s) != cudaSuccess) return OCT_ERR_CUDA;
+    if (tiles && cudaMemsetAsync(sc->status, 0, tiles * 256 * sizeof(unsigned long long), s) != cudaSuccess)
+        return OCT_ERR_CUDA;
+    k_bbox<<<kNoAllocBboxGrid, kBboxThreads, 0, s>>>(d_xyz, n, sc->partial, &ctl->bbox_ctr, &sc->bg);
+    if (n) {
+        const uint64_t want = (n + kEncThreads - 1) / kEncThreads;
+        const int grid = (int)(want < (uint64_t)kNoAllocBboxGrid ? want : (uint64_t)kNoAllocBboxGrid);
+        if (encoder == OCT_ENC_HILBERT_3D) k_encode<5><<<grid, kEncThreads, 0, s>>>(d_xyz, n, &sc->bg, d_keys, ctl);
+        else k_encode<1><<<grid, kEncThreads, 0, s>>>(d_xyz, n, &sc->bg, d_keys, ctl);
+        k_scan_hist<<<1, 256, 0, s>>>(ctl, n);
+        // all 8 digit passes (no host readback of the skip flags), so the result
+        // ends in the caller's buffers: caller -> scratch -> caller ...
+        const size_t smem = onesweep_smem();
+        uint32_t* err = reinterpret_cast<uint32_t*>(&ctl->pad);
+        for (int p = 0; p < 8; ++p) {
+            const bool to_scratch = (p % 2) == 0;
+            const uint64_t* kin = to_scratch ? d_keys : sc->keys_alt;
+            uint64_t* kout = to_scratch ? sc->keys_alt : d_keys;
+            const uint32_t* vin = to_scratch ? d_perm : sc->perm_alt;
+            uint32_t* vout = to_scratch ? sc->perm_alt : d_perm;
+            if (p == 0)
+                k_onesweep<true><<<(unsigned)tiles, kSortThreads, smem, s>>>(kin, nullptr, kout, vout, n, p, ctl,
+                                                                             sc->status, (uint32_t)(p + 1), err);
+            else
+                k_onesweep<false><<<(unsigned)tiles, kSortThreads, smem, s>>>(kin, vin, kout, vout, n, p, ctl,
+                                                                              sc->status, (uint32_t)(p + 1), err);
+        }
+    }
+    // Box (center, radii, min, max): the 12 leading doubles of the scratch BoxGeom
+    if (cudaMemcpyAsync(d_box12, &sc->bg.box, 12 * sizeof(double), cudaMemcpyDeviceToDevice, s) != cudaSuccess)
+        return OCT_ERR_CUDA;
+    const cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? OCT_OK : OCT_ERR_CUDA;
+}
