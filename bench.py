@@ -49,6 +49,9 @@ KNN_K = 50
 Q_RADIUS = 500_000
 Q_KNN = 500_000
 L2_FLUSH_BYTES = 512 << 20
+# device launches of this library per timed step: radius search (count, 3 scan kernels, fill), kNN;
+# the packet paths add the query ordering (keys, histogram scan, 3 sort passes) to the radius and the kNN call
+LAUNCHES_PER_STEP = {"plain": 6, "packet": 6 + 10, "packet_fp32": 6 + 10, "knn_packet": 6 + 10}
 BUILD_BYTES_PER_POINT = 112  # encode 32 + sort 20 + reorder 52 + leaf counting 8
 BUILD_BYTES_PER_NODE = 36    # offsets 4 + ranges 8 + centers 24
 
@@ -262,7 +265,15 @@ def run_b200(args, rank, world, local_rank):
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
 
-    def step(b, timed):
+    SEARCH_PATHS = {"plain": (0, 0, args.radius_group, 0), "packet": (1, 0, 8, 0), "packet_fp32": (1, 1, 8, 0),
+                    "knn_packet": (1, 0, 8, 1)}
+
+    def configure(name):
+        packet, fp32, lanes, knn_packet = SEARCH_PATHS[name]
+        cfg = capi.OctSearchConfig(packet, fp32, lanes, knn_packet)
+        capi.check(L.oct_set_search_config(h, C.byref(cfg)), h, "search config")
+
+    def step(b):
         qr, qk = batches[b]
         with torch.cuda.stream(stream):
             flush.zero_()
@@ -278,32 +289,46 @@ def run_b200(args, rank, world, local_rank):
         stream.synchronize()
         return ev[0].elapsed_time(ev[1]), ev[1].elapsed_time(ev[2]), ev[2].elapsed_time(ev[3]), int(tot.value)
 
-    for b in range(args.warmup):
-        step(b, False)
-    if world > 1:
-        torch.distributed.barrier()
-    torch.cuda.synchronize()
     clocks = ClockSampler(int(os.environ.get("CUDA_VISIBLE_DEVICES", str(dev)).split(",")[0])
                           if os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",")[0].isdigit() else dev)
+    paths = {}
     clocks.start()
-    t_count = t_search = t_knn = 0.0
-    nbrs = 0
-    for s in range(args.steps):
-        a, b_, c, tt = step(args.warmup + s, True)
-        t_count += a
-        t_search += b_
-        t_knn += c
-        nbrs += tt
-    torch.cuda.synchronize()
-    if world > 1:
-        torch.distributed.barrier()
+    for name in SEARCH_PATHS:
+        configure(name)
+        for b in range(args.warmup):
+            step(b)
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+        L.oct_search_stats(h, None, None, 1)
+        t_count = t_search = t_knn = 0.0
+        nbrs = 0
+        for s in range(args.steps):
+            a_, b_, c_, tt = step(args.warmup + s)
+            t_count += a_
+            t_search += b_
+            t_knn += c_
+            nbrs += tt
+        torch.cuda.synchronize()
+        tests, retests = C.c_uint64(), C.c_uint64()
+        L.oct_search_stats(h, C.byref(tests), C.byref(retests), 1)
+        step_ms = (t_search + t_knn) / args.steps  # the count-only call is a separate measurement
+        tmax = torch.tensor([step_ms, t_search / args.steps, t_knn / args.steps], dtype=torch.float64, device="cuda")
+        if world > 1:
+            torch.distributed.barrier()
+            torch.distributed.all_reduce(tmax, op=torch.distributed.ReduceOp.MAX)
+        step_ms, rad_ms, knn_ms = (float(v) for v in tmax.tolist())
+        paths[name] = {"ms_per_step": step_ms, "qps": world * (Q_RADIUS + Q_KNN) / (step_ms / 1e3),
+                       "radius_qps": world * Q_RADIUS / (rad_ms / 1e3), "knn_qps": world * Q_KNN / (knn_ms / 1e3),
+                       "radius_ms": rad_ms, "knn_ms": knn_ms, "radius_count_only_ms": t_count / args.steps,
+                       "avg_neighbours": nbrs / args.steps / Q_RADIUS, "nbrs_per_step": nbrs / args.steps,
+                       "point_tests": tests.value, "fp64_retests": retests.value,
+                       "band_hit_fraction": (retests.value / tests.value) if tests.value else None}
     clk = clocks.stop()
-    step_ms = (t_search + t_knn) / args.steps  # the count-only call is a separate measurement
-    tmax = torch.tensor([step_ms], dtype=torch.float64, device="cuda")
-    if world > 1:
-        torch.distributed.all_reduce(tmax, op=torch.distributed.ReduceOp.MAX)
-    step_ms_max = float(tmax.item())
-    value = world * (Q_RADIUS + Q_KNN) / (step_ms_max / 1e3)
+    chosen = paths[args.search]
+    configure(args.search)
+    step_ms_max = chosen["ms_per_step"]
+    value = chosen["qps"]
 
     # ---- e2e through the host-buffer ABI (pinned buffers, copies in the timed region) ----
     e2e_val = None
@@ -337,20 +362,21 @@ def run_b200(args, rank, world, local_rank):
             torch.distributed.all_reduce(e2e_t, op=torch.distributed.ReduceOp.MAX)
         e2e_val = world * (Q_RADIUS + Q_KNN) / float(e2e_t.item())
 
-    # ---- roofline of the dominant kernel ----
+    # ---- roofline of the dominant kernel of the chosen path ----
     peak, peak_kind = measured_peak()
-    avg_nbrs = nbrs / args.steps / Q_RADIUS
-    rad_bytes = 24 * Q_RADIUS + 28 * (nbrs / args.steps)
+    rad_bytes = 24 * Q_RADIUS + 28 * chosen["nbrs_per_step"]
     knn_bytes = (24 + 36 * KNN_K) * Q_KNN
-    rad_ms = t_search / args.steps
-    knn_ms = t_knn / args.steps
-    rad = {"kernel": "radius neighborsPrune sphere (count + scan + fill)", "ms": rad_ms,
+    rad_ms, knn_ms = chosen["radius_ms"], chosen["knn_ms"]
+    rad = {"kernel": f"radius neighborsPrune sphere, {args.search} path (count + scan + fill)", "ms": rad_ms,
            "achieved": rad_bytes / (rad_ms / 1e3) / 1e9}
     knn = {"kernel": "kNN k=50 (k_knn)", "ms": knn_ms, "achieved": knn_bytes / (knn_ms / 1e3) / 1e9}
     dom = knn if knn_ms >= rad_ms else rad
     roofline = {"bound": "hbm", "kernel": dom["kernel"], "achieved": dom["achieved"], "peak": peak, "unit": "GB/s",
                 "frac": dom["achieved"] / peak, "peak_source": peak_kind, "traffic": None,
-                "algorithmic_bytes": "radius 24 + 28 per neighbour; kNN 24 + 36 k per query"}
+                "algorithmic_bytes": "radius 24 + 28 per neighbour; kNN 24 + 36 k per query",
+                "other": {"kernel": (rad if dom is knn else knn)["kernel"],
+                          "achieved": (rad if dom is knn else knn)["achieved"],
+                          "frac": (rad if dom is knn else knn)["achieved"] / peak}}
     build_bytes = BUILD_BYTES_PER_POINT * N_POINTS + BUILD_BYTES_PER_NODE * info.n_total
     build = {"ms": 1e3 * build_s, "mpts_s": N_POINTS / build_s / 1e6, "gbs": build_bytes / build_s / 1e9,
              "frac": build_bytes / build_s / 1e9 / peak, "nodes": info.n_total, "leaves": info.n_leaf,
@@ -371,12 +397,13 @@ def run_b200(args, rank, world, local_rank):
             "metric": METRIC, "value": value, "unit": "queries/s", "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": step_ms_max, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f64", "data": "synthetic",
-            "config": workload_config(world, {"radius_group": args.radius_group, "path": "plain fp64"}),
-            "radius_qps": world * Q_RADIUS / (rad_ms / 1e3), "knn_qps": world * Q_KNN / (knn_ms / 1e3),
-            "radius_count_only_ms": t_count / args.steps, "avg_neighbours": avg_nbrs,
+            "config": workload_config(world, {"search_path": args.search}),
+            "radius_qps": chosen["radius_qps"], "knn_qps": chosen["knn_qps"],
+            "avg_neighbours": chosen["avg_neighbours"], "paths": paths,
+            "batched_vs_plain": paths["packet"]["qps"] / paths["plain"]["qps"],
             "build": build, "roofline": roofline, "cpu_baseline": cpu,
             "e2e": {"value": e2e_val, "unit": "queries/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
-            "gpu_launches": 6 * args.steps, "clocks": clk,
+            "gpu_launches": LAUNCHES_PER_STEP[args.search] * args.steps, "clocks": clk,
         }
         print(json.dumps(line), flush=True)
     L.oct_cloud_destroy(h)
@@ -390,7 +417,9 @@ def main():
     ap.add_argument("--steps", type=int, default=5)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
-    ap.add_argument("--radius-group", type=int, default=8)
+    ap.add_argument("--radius-group", type=int, default=8, help="lanes per query of the plain path")
+    ap.add_argument("--search", default="packet", choices=["plain", "packet", "packet_fp32", "knn_packet"],
+                    help="search path whose numbers are the headline value")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")

@@ -106,6 +106,32 @@ int oct_synchronize(oct_cloud cloud);
  * autotuner sets it. */
 int oct_set_radius_group(oct_cloud cloud, int lanes);
 
+/* Search configuration of a cloud (no reference counterpart; set by the
+ * autotuner or the caller).  Results are identical in every configuration.
+ *  packet       1 (default): the query centres are ordered along the cloud's
+ *               curve and each warp walks the tree once for 32 neighbouring
+ *               queries; 0: one query per group of radius_lanes lanes.
+ *  fp32_filter  1: leaf points are tested in FP32 relative to their leaf's
+ *               centre and only points within a rigorous error band of the
+ *               boundary are re-tested in FP64 (packet path); 0 (default):
+ *               every test in FP64.
+ *  radius_lanes lanes per query when packet is 0: 8 (default), 16 or 32.
+ *  knn_packet   1: kNN also walks 32 queries per warp (each lane its own
+ *               k-heap; k <= 128); 0 (default): one warp per query, visited
+ *               in curve order when packet is 1. */
+typedef struct {
+    int32_t packet;
+    int32_t fp32_filter;
+    int32_t radius_lanes;
+    int32_t knn_packet;
+} oct_search_config;
+int oct_set_search_config(oct_cloud cloud, const oct_search_config* config);
+
+/* Counters of the packet radius searches since the last reset: point tests
+ * and FP64 re-tests of points inside the FP32 error band (the band-hit
+ * fraction is their ratio).  Waits for the cloud's stream. */
+int oct_search_stats(oct_cloud cloud, uint64_t* point_tests, uint64_t* fp64_retests, int reset);
+
 /* Upload n points (xyz AoS).  Replaces filling the reference's PointsAoS
  * container (inc/geometry/point_containers.hpp:32-65). */
 int oct_set_points(oct_cloud cloud, const double* xyz, uint64_t n, uint32_t flags);

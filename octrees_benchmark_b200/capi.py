@@ -34,6 +34,11 @@ class OctParams(C.Structure):
                 ("flags", C.c_uint32)]
 
 
+class OctSearchConfig(C.Structure):
+    _fields_ = [("packet", C.c_int32), ("fp32_filter", C.c_int32), ("radius_lanes", C.c_int32),
+                ("knn_packet", C.c_int32)]
+
+
 class OctTreeInfo(C.Structure):
     _fields_ = [("n_points", C.c_uint64), ("n_leaf", C.c_uint32), ("n_internal", C.c_uint32),
                 ("n_total", C.c_uint32), ("max_depth_seen", C.c_uint32)]
@@ -62,6 +67,8 @@ SIGNATURES = {
     "oct_last_error": ([_vp, C.c_char_p, C.c_size_t], _int),
     "oct_synchronize": ([_vp], _int),
     "oct_set_radius_group": ([_vp, _int], _int),
+    "oct_set_search_config": ([_vp, C.POINTER(OctSearchConfig)], _int),
+    "oct_search_stats": ([_vp, C.POINTER(_u64), C.POINTER(_u64), _int], _int),
     "oct_set_points": ([_vp, _vp, _u64, _u32], _int),
     "oct_encode_sort": ([_vp, _vp, _vp, _vp, _vp, _u32], _int),
     "oct_build": ([_vp, C.POINTER(OctTreeInfo)], _int),

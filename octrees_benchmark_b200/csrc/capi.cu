@@ -112,8 +112,24 @@ __global__ void k_widen_pairs(const uint2* in, uint64_t n, unsigned long long* o
 bool valid_kernel(int k) { return k >= OCT_KERNEL_CIRCLE && k <= OCT_KERNEL_CUBE; }
 bool valid_algo(int a) { return a >= OCT_NEIGHBORS && a <= OCT_NEIGHBORS_STRUCT; }
 
-// Lanes per query of the radius traversal (8, 16 or 32), set by oct_set_radius_group.
-int radius_group(const Cloud& c) { return c.radius_group; }
+// Count or fill pass of a radius search on the configured path.  With the
+// packet path the query order (sorted along the curve) is computed once per
+// call by the first pass and reused by the second.
+cudaError_t radius_pass(Cloud& c, int kernel, int algo, bool fill, const double* dq, uint64_t nq, const double* dr,
+                        double radius, unsigned long long* counts, unsigned long long* counts2,
+                        const unsigned long long* offs, uint32_t* out, uint64_t cap, const uint32_t** order) {
+    if (!c.packet) return launch_radius(c, kernel, algo, c.radius_group, fill, dq, nq, dr, radius, counts, counts2, offs,
+                                        out, cap);
+    cudaError_t e;
+    if (c.fp32_filter && !c.rel_built) {
+        if ((e = launch_leaf_rel(c)) != cudaSuccess) return e;
+        c.rel_built = true;
+    }
+    if ((e = c.stats.reserve(64)) != cudaSuccess) return e;
+    if (!*order && (e = launch_query_order(c, dq, nq, order)) != cudaSuccess) return e;
+    return launch_radius_packet(c, kernel, algo, fill, c.fp32_filter != 0, dq, nq, dr, radius, *order, counts, counts2,
+                                offs, out, cap);
+}
 
 int radius_common(Cloud& c, int kernel, int algo, const double* centers, uint64_t nq, const double* radii,
                   double radius, bool device, const double** dq, const double** dr) {
@@ -198,6 +214,8 @@ int oct_cloud_create(const oct_params* p, oct_cloud* out) {
         e = c.d_err.reserve(256);
     }
     if (e == cudaSuccess) e = cudaMemsetAsync(c.d_err.ptr, 0, 256, c.stream);
+    if (e == cudaSuccess) e = c.stats.reserve(64);
+    if (e == cudaSuccess) e = cudaMemsetAsync(c.stats.ptr, 0, 64, c.stream);
     if (e == cudaSuccess) e = cudaMallocHost(&c.pinned, kPinnedBytes);
     if (e == cudaSuccess) e = cudaStreamSynchronize(c.stream);
     if (e != cudaSuccess) {
@@ -218,7 +236,8 @@ int oct_cloud_destroy(oct_cloud h) {
         DevBuf* bufs[] = {&c.xyz_in, &c.xs, &c.ys, &c.zs, &c.keys, &c.keys_alt, &c.perm, &c.perm_alt,
                           &c.sort_status, &c.d_ctl, &c.d_box, &c.d_err, &c.offsets, &c.ranges, &c.centers,
                           &c.frontier, &c.masks, &c.parts, &c.d_build, &c.q_centers, &c.q_radii, &c.q_counts,
-                          &c.q_offsets, &c.q_out, &c.q_out2, &c.q_scan_tmp};
+                          &c.q_offsets, &c.q_out, &c.q_out2, &c.q_scan_tmp, &c.qs_keys, &c.qs_keys_alt, &c.qs_ord,
+                          &c.qs_ord_alt, &c.qs_status, &c.qs_ctl, &c.packet_ctr, &c.stats, &c.rel};
         for (DevBuf* b : bufs) b->release();
         if (c.pinned) cudaFreeHost(c.pinned);
         if (c.own_stream && c.stream) cudaStreamDestroy(c.stream);
@@ -260,6 +279,32 @@ int oct_set_radius_group(oct_cloud h, int lanes) {
     return OCT_OK;
 }
 
+int oct_set_search_config(oct_cloud h, const oct_search_config* cfg) {
+    if (!h || !cfg) return OCT_ERR_INVALID_ARG;
+    Cloud& c = h->c;
+    if (cfg->packet < 0 || cfg->packet > 1 || cfg->fp32_filter < 0 || cfg->fp32_filter > 1)
+        return set_error(c, OCT_ERR_INVALID_ARG, "packet and fp32_filter are 0 or 1");
+    c.packet = cfg->packet;
+    c.fp32_filter = cfg->fp32_filter;
+    c.radius_group = (cfg->radius_lanes == 16 || cfg->radius_lanes == 32) ? cfg->radius_lanes : 8;
+    c.knn_packet = cfg->knn_packet ? 1 : 0;
+    return OCT_OK;
+}
+
+int oct_search_stats(oct_cloud h, uint64_t* point_tests, uint64_t* fp64_retests, int reset) {
+    if (!h) return OCT_ERR_INVALID_ARG;
+    Cloud& c = h->c;
+    DeviceGuard g(c.device);
+    CK(c.stats.reserve(64));
+    unsigned long long v[2] = {0, 0};
+    CK(cudaStreamSynchronize(c.stream));
+    CK(cudaMemcpy(v, c.stats.ptr, sizeof(v), cudaMemcpyDeviceToHost));
+    if (point_tests) *point_tests = v[0];
+    if (fp64_retests) *fp64_retests = v[1];
+    if (reset) CK(cudaMemset(c.stats.ptr, 0, 64));
+    return OCT_OK;
+}
+
 int oct_set_points(oct_cloud h, const double* xyz, uint64_t n, uint32_t flags) {
     if (!h) return OCT_ERR_INVALID_ARG;
     Cloud& c = h->c;
@@ -274,6 +319,7 @@ int oct_set_points(oct_cloud h, const double* xyz, uint64_t n, uint32_t flags) {
     c.n = n;
     c.sorted = false;
     c.built = false;
+    c.rel_built = false;
     c.node_capacity = 0;
     if (!(flags & OCT_MEM_DEVICE)) CK(cudaStreamSynchronize(c.stream));
     return OCT_OK;
@@ -341,6 +387,11 @@ int oct_build(oct_cloud h, oct_tree_info* info) {
         c.n_leaf = bc.n_total - bc.n_internal;
         c.max_depth_seen = bc.max_depth_seen;
         CK(cudaMemsetAsync(c.offsets.as<uint32_t>() + c.n_total, 0, 4, c.stream));
+        c.rel_built = false;
+        if (c.fp32_filter && c.packet) {  // the FP32 search reads leaf-relative coordinates
+            CK(launch_leaf_rel(c));
+            c.rel_built = true;
+        }
         c.built = true;
         if (info) {
             info->n_points = c.n;
@@ -406,12 +457,11 @@ int oct_radius_count(oct_cloud h, int kernel, int algo, const double* centers, u
     CK(c.q_out2.reserve(8 * (nq ? nq : 1)));
     unsigned long long* dc_ranges = c.q_out2.as<unsigned long long>();
     // for neighborsStruct the reported count is numberOfPoints
+    const uint32_t* order = nullptr;
     if (algo == OCT_NEIGHBORS_STRUCT)
-        CK(launch_radius(c, kernel, algo, radius_group(c), false, dq, nq, dr, radius, dc_ranges, dc, nullptr,
-                         nullptr, 0));
+        CK(radius_pass(c, kernel, algo, false, dq, nq, dr, radius, dc_ranges, dc, nullptr, nullptr, 0, &order));
     else
-        CK(launch_radius(c, kernel, algo, radius_group(c), false, dq, nq, dr, radius, dc, nullptr, nullptr, nullptr,
-                         0));
+        CK(radius_pass(c, kernel, algo, false, dq, nq, dr, radius, dc, nullptr, nullptr, nullptr, 0, &order));
     if (!dev && counts && nq) CK(cudaMemcpyAsync(counts, dc, 8 * nq, cudaMemcpyDeviceToHost, c.stream));
     if (!dev) return sync_and_check(c);
     return OCT_OK;
@@ -427,7 +477,6 @@ int oct_radius_search(oct_cloud h, int kernel, int algo, const double* centers, 
     const double *dq, *dr;
     int st = radius_common(c, kernel, algo, centers, nq, radii, radius, dev, &dq, &dr);
     if (st != OCT_OK) return st;
-    const int grp = radius_group(c);
     CK(c.q_counts.reserve(8 * (nq ? nq : 1)));
     unsigned long long* dc = c.q_counts.as<unsigned long long>();
     unsigned long long* doffs = reinterpret_cast<unsigned long long*>(offsets);
@@ -435,13 +484,14 @@ int oct_radius_search(oct_cloud h, int kernel, int algo, const double* centers, 
         CK(c.q_offsets.reserve(8 * (nq + 1)));
         doffs = c.q_offsets.as<unsigned long long>();
     }
+    const uint32_t* order = nullptr;
     if (algo == OCT_NEIGHBORS_STRUCT) {
         // expanded indices of the ranges: count points, fill as prune-style runs
         CK(c.q_out2.reserve(8 * (nq ? nq : 1)));
-        CK(launch_radius(c, kernel, OCT_NEIGHBORS_STRUCT, grp, false, dq, nq, dr, radius, c.q_out2.as<unsigned long long>(),
-                         dc, nullptr, nullptr, 0));
+        CK(radius_pass(c, kernel, OCT_NEIGHBORS_STRUCT, false, dq, nq, dr, radius, c.q_out2.as<unsigned long long>(),
+                       dc, nullptr, nullptr, 0, &order));
     } else {
-        CK(launch_radius(c, kernel, algo, grp, false, dq, nq, dr, radius, dc, nullptr, nullptr, nullptr, 0));
+        CK(radius_pass(c, kernel, algo, false, dq, nq, dr, radius, dc, nullptr, nullptr, nullptr, 0, &order));
     }
     CK(launch_scan_u64(c, dc, doffs, nq));
     CK(cudaMemcpyAsync(c.pinned, doffs + nq, 8, cudaMemcpyDeviceToHost, c.stream));
@@ -462,7 +512,7 @@ int oct_radius_search(oct_cloud h, int kernel, int algo, const double* centers, 
     // neighborsStruct's index set equals the points of its ranges; the prune
     // traversal with the same kernel emits exactly that set (same decisions).
     const int fill_algo = (algo == OCT_NEIGHBORS_STRUCT) ? OCT_NEIGHBORS_PRUNE : algo;
-    CK(launch_radius(c, kernel, fill_algo, grp, true, dq, nq, dr, radius, nullptr, nullptr, doffs, dout, tot));
+    CK(radius_pass(c, kernel, fill_algo, true, dq, nq, dr, radius, nullptr, nullptr, doffs, dout, tot, &order));
     if (!dev && tot) CK(cudaMemcpyAsync(idx, dout, 4 * tot, cudaMemcpyDeviceToHost, c.stream));
     if (!dev) return sync_and_check(c);
     return OCT_OK;
@@ -478,7 +528,6 @@ int oct_struct_search(oct_cloud h, int kernel, const double* centers, uint64_t n
     const double *dq, *dr;
     int st = radius_common(c, kernel, OCT_NEIGHBORS_STRUCT, centers, nq, radii, radius, dev, &dq, &dr);
     if (st != OCT_OK) return st;
-    const int grp = radius_group(c);
     CK(c.q_counts.reserve(8 * (nq ? nq : 1)));
     CK(c.q_out2.reserve(8 * (nq ? nq : 1)));
     unsigned long long* dranges = c.q_counts.as<unsigned long long>();
@@ -489,8 +538,9 @@ int oct_struct_search(oct_cloud h, int kernel, const double* centers, uint64_t n
         CK(c.q_offsets.reserve(8 * (nq + 1)));
         doffs = c.q_offsets.as<unsigned long long>();
     }
-    CK(launch_radius(c, kernel, OCT_NEIGHBORS_STRUCT, grp, false, dq, nq, dr, radius, dranges, dpoints, nullptr,
-                     nullptr, 0));
+    const uint32_t* order = nullptr;
+    CK(radius_pass(c, kernel, OCT_NEIGHBORS_STRUCT, false, dq, nq, dr, radius, dranges, dpoints, nullptr, nullptr, 0,
+                   &order));
     CK(launch_scan_u64(c, dranges, doffs, nq));
     CK(cudaMemcpyAsync(c.pinned, doffs + nq, 8, cudaMemcpyDeviceToHost, c.stream));
     if ((st = sync_and_check(c)) != OCT_OK) return st;
@@ -508,8 +558,8 @@ int oct_struct_search(oct_cloud h, int kernel, const double* centers, uint64_t n
         CK(c.q_out.reserve(8 * (tot ? tot : 1)));
         dout = c.q_out.as<uint32_t>();
     }
-    CK(launch_radius(c, kernel, OCT_NEIGHBORS_STRUCT, grp, true, dq, nq, dr, radius, nullptr, nullptr, doffs, dout,
-                     tot));
+    CK(radius_pass(c, kernel, OCT_NEIGHBORS_STRUCT, true, dq, nq, dr, radius, nullptr, nullptr, doffs, dout, tot,
+                   &order));
     if (!dev && tot) CK(cudaMemcpyAsync(pairs, dout, 8 * tot, cudaMemcpyDeviceToHost, c.stream));
     if (!dev) return sync_and_check(c);
     return OCT_OK;

@@ -95,6 +95,18 @@ struct Cloud {
 
     // query scratch
     DevBuf q_centers, q_radii, q_counts, q_offsets, q_out, q_out2, q_scan_tmp;
+    // query ordering (packet searches): keys, order, look-back words, histograms
+    DevBuf qs_keys, qs_keys_alt, qs_ord, qs_ord_alt, qs_status, qs_ctl;
+    uint32_t qs_epoch = 0;
+    DevBuf packet_ctr;  // dynamic packet counters
+    DevBuf stats;       // device counters: points tested, FP64 band re-tests, ...
+    // FP32 leaf-relative coordinates (x, y, z, 0) per sorted point, built on demand
+    DevBuf rel;
+    bool rel_built = false;
+    // search configuration (oct_set_search_config)
+    int packet = 1;
+    int fp32_filter = 0;
+    int knn_packet = 0;
 
     // pinned host staging for small readbacks
     void* pinned = nullptr;
@@ -110,6 +122,12 @@ cudaError_t launch_radius(Cloud& c, int kernel, int algo, int group, bool fill, 
                           unsigned long long* d_counts2, const unsigned long long* d_offsets, uint32_t* d_out,
                           uint64_t out_capacity);
 cudaError_t launch_scan_u64(Cloud& c, const unsigned long long* d_in, unsigned long long* d_out, uint64_t n);
+cudaError_t launch_query_order(Cloud& c, const double* d_centers, uint64_t nq, const uint32_t** d_order);
+cudaError_t launch_leaf_rel(Cloud& c);
+cudaError_t launch_radius_packet(Cloud& c, int kernel, int algo, bool fill, bool fp32, const double* d_centers,
+                                 uint64_t nq, const double* d_radii, double radius, const uint32_t* d_order,
+                                 unsigned long long* d_counts, unsigned long long* d_counts2,
+                                 const unsigned long long* d_offsets, uint32_t* d_out, uint64_t out_capacity);
 cudaError_t launch_knn(Cloud& c, const double* d_centers, uint64_t nq, uint32_t k, uint32_t* d_idx, double* d_d2,
                        uint32_t* d_counts);
 

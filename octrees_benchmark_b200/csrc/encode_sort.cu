@@ -435,6 +435,94 @@ cudaError_t launch_gather(Cloud& c, const double* d_xyz, const uint32_t* d_perm,
 }
 
 // ---------------------------------------------------------------------------
+// Query ordering for the packet searches: the query centres are keyed with the
+// cloud's box and curve and stably sorted by the top 24 key bits (3 onesweep
+// passes), so that the 32 queries of a warp are spatial neighbours.
+// ---------------------------------------------------------------------------
+
+namespace {
+
+template <int ENC>
+__global__ void __launch_bounds__(kEncThreads) k_query_keys(const double* __restrict__ q, uint64_t nq,
+                                                            const BoxGeom* __restrict__ bg,
+                                                            uint64_t* __restrict__ keys, SortCtl* ctl) {
+    __shared__ uint32_t hist[3 * 256];
+    for (int j = threadIdx.x; j < 3 * 256; j += blockDim.x) hist[j] = 0;
+    const double c0 = bg->box.center[0], c1 = bg->box.center[1], c2 = bg->box.center[2];
+    const double r0 = bg->box.radii[0], r1 = bg->box.radii[1], r2 = bg->box.radii[2];
+    __syncthreads();
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < nq; i += stride) {
+        const uint64_t k = sfc_encode<ENC>(anchor_coord(q[3 * i], c0, r0), anchor_coord(q[3 * i + 1], c1, r1),
+                                           anchor_coord(q[3 * i + 2], c2, r2));
+        keys[i] = k;
+#pragma unroll
+        for (int p = 5; p < 8; ++p) atomicAdd(&hist[(p - 5) * 256 + (uint32_t)((k >> (8 * p)) & 255u)], 1u);
+    }
+    __syncthreads();
+    for (int j = threadIdx.x; j < 3 * 256; j += blockDim.x) {
+        const uint32_t v = hist[j];
+        if (v) atomicAdd(&ctl->hist[5 + (j >> 8)][j & 255], v);
+    }
+}
+
+}  // namespace
+
+cudaError_t launch_query_order(Cloud& c, const double* d_centers, uint64_t nq, const uint32_t** d_order) {
+    cudaError_t e;
+    *d_order = nullptr;
+    if (nq == 0) return cudaSuccess;
+    const uint64_t tiles = (nq + kSortTile - 1) / kSortTile;
+    if ((e = c.qs_keys.reserve(8 * nq)) != cudaSuccess) return e;
+    if ((e = c.qs_keys_alt.reserve(8 * nq)) != cudaSuccess) return e;
+    if ((e = c.qs_ord.reserve(4 * nq)) != cudaSuccess) return e;
+    if ((e = c.qs_ord_alt.reserve(4 * nq)) != cudaSuccess) return e;
+    if ((e = c.qs_ctl.reserve(sizeof(SortCtl))) != cudaSuccess) return e;
+    const size_t status_bytes = tiles * 256 * sizeof(unsigned long long);
+    if (status_bytes > c.qs_status.bytes) {
+        if ((e = c.qs_status.reserve(status_bytes)) != cudaSuccess) return e;
+        if ((e = cudaMemsetAsync(c.qs_status.ptr, 0, c.qs_status.bytes, c.stream)) != cudaSuccess) return e;
+        c.qs_epoch = 0;
+    }
+    const size_t smem = onesweep_smem();
+    cudaFuncSetAttribute(k_onesweep<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(k_onesweep<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    SortCtl* ctl = c.qs_ctl.as<SortCtl>();
+    if ((e = cudaMemsetAsync(ctl, 0, sizeof(SortCtl), c.stream)) != cudaSuccess) return e;
+    const int sms = sm_count(c.device);
+    const uint64_t want = (nq + kEncThreads - 1) / kEncThreads;
+    const int grid = (int)(want < (uint64_t)sms * kEncGridPerSM ? want : (uint64_t)sms * kEncGridPerSM);
+    const BoxGeom* bg = c.d_box.as<BoxGeom>();
+    if (c.params.encoder == OCT_ENC_HILBERT_3D)
+        k_query_keys<5><<<grid, kEncThreads, 0, c.stream>>>(d_centers, nq, bg, c.qs_keys.as<uint64_t>(), ctl);
+    else
+        k_query_keys<1><<<grid, kEncThreads, 0, c.stream>>>(d_centers, nq, bg, c.qs_keys.as<uint64_t>(), ctl);
+    k_scan_hist<<<1, 256, 0, c.stream>>>(ctl, nq);
+    DevBuf* kb[2] = {&c.qs_keys, &c.qs_keys_alt};
+    DevBuf* vb[2] = {&c.qs_ord, &c.qs_ord_alt};
+    int sel = 0;
+    for (int p = 5; p < 8; ++p) {
+        c.qs_epoch = (c.qs_epoch + 1) & ((1u << 22) - 1);
+        if (c.qs_epoch == 0) {
+            if ((e = cudaMemsetAsync(c.qs_status.ptr, 0, c.qs_status.bytes, c.stream)) != cudaSuccess) return e;
+            c.qs_epoch = 1;
+        }
+        if (p == 5)
+            k_onesweep<true><<<(unsigned)tiles, kSortThreads, smem, c.stream>>>(
+                kb[sel]->as<uint64_t>(), nullptr, kb[sel ^ 1]->as<uint64_t>(), vb[sel ^ 1]->as<uint32_t>(), nq, p,
+                ctl, c.qs_status.as<unsigned long long>(), c.qs_epoch, c.d_err.as<uint32_t>());
+        else
+            k_onesweep<false><<<(unsigned)tiles, kSortThreads, smem, c.stream>>>(
+                kb[sel]->as<uint64_t>(), vb[sel]->as<uint32_t>(), kb[sel ^ 1]->as<uint64_t>(),
+                vb[sel ^ 1]->as<uint32_t>(), nq, p, ctl, c.qs_status.as<unsigned long long>(), c.qs_epoch,
+                c.d_err.as<uint32_t>());
+        sel ^= 1;
+    }
+    *d_order = vb[sel]->as<uint32_t>();
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
 // Allocation-free encode + sort (oct_encode_sort_noalloc).
 //
 // For callers that cannot allocate device memory at call time: code that runs

@@ -42,6 +42,7 @@ struct KnnArgs {
     double* d2;
     uint32_t* counts;
     uint32_t* err;
+    const uint32_t* order;  // query visiting order (curve order), or nullptr
 };
 
 __device__ __forceinline__ bool pair_less(double da, uint32_t ia, double db, uint32_t ib) {
@@ -55,7 +56,8 @@ __device__ __forceinline__ void warp_bitonic_sort(double* d, uint32_t* ix) {
     for (int size = 2; size <= P; size <<= 1) {
         for (int stride = size >> 1; stride > 0; stride >>= 1) {
             for (int i = lane; i < P / 2; i += 32) {
-                const int lo = 2 * stride * (i / stride) + (i % stride);
+                // i-th compare pair of this step (stride is a power of two)
+                const int lo = ((i & ~(stride - 1)) << 1) | (i & (stride - 1));
                 const int hi = lo + stride;
                 const bool asc = (lo & size) == 0;
                 const double a = d[lo], b = d[hi];
@@ -92,7 +94,8 @@ __global__ void __launch_bounds__(kKnnThreads) k_knn(KnnArgs a) {
 
     const uint32_t K = a.k;
     const uint64_t nwarps = (uint64_t)gridDim.x * kKnnWarps;
-    for (uint64_t q = (uint64_t)blockIdx.x * kKnnWarps + warp; q < a.nq; q += nwarps) {
+    for (uint64_t qpos = (uint64_t)blockIdx.x * kKnnWarps + warp; qpos < a.nq; qpos += nwarps) {
+        const uint64_t q = a.order ? a.order[qpos] : qpos;
         const double p[3] = {a.q[3 * q], a.q[3 * q + 1], a.q[3 * q + 2]};
         for (int i = lane; i < P; i += 32) {
             sd[i] = INFINITY;
@@ -228,6 +231,442 @@ cudaError_t launch_l(const KnnArgs& a, int grid, cudaStream_t s) {
     return cudaGetLastError();
 }
 
+// ---------------------------------------------------------------------------
+// Register kNN for k <= 64: one warp per query, the k best (distance, index)
+// pairs held in registers as a sorted list (R = 1 or 2 entries per lane,
+// element j = r * 32 + lane).  A candidate that beats the k-th pair is placed
+// by one ballot per register (its rank) and a shuffle shift - no shared-memory
+// sort.  Children are judged with their ranges and first-child links loaded at
+// expansion time, so empty leaves are never pushed and a popped entry needs no
+// further dependent loads before its points are read.
+// ---------------------------------------------------------------------------
+
+template <int R>
+struct RegList {
+    double d[R];
+    uint32_t i[R];
+};
+
+template <int R>
+__device__ __forceinline__ void reglist_insert(RegList<R>& L, double cd, uint32_t ci, uint32_t K, uint32_t& nl) {
+    const int lane = threadIdx.x & 31;
+    int pos = 0;
+#pragma unroll
+    for (int r = 0; r < R; ++r) pos += __popc(__ballot_sync(0xffffffffu, pair_less(L.d[r], L.i[r], cd, ci)));
+    if (pos >= (int)K) return;
+    double upd[R];
+    uint32_t upi[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        upd[r] = __shfl_up_sync(0xffffffffu, L.d[r], 1);
+        upi[r] = __shfl_up_sync(0xffffffffu, L.i[r], 1);
+    }
+    double carry_d[R];
+    uint32_t carry_i[R];
+#pragma unroll
+    for (int r = 0; r < R; ++r) {
+        carry_d[r] = __shfl_sync(0xffffffffu, L.d[r], 31);
+        carry_i[r] = __shfl_sync(0xffffffffu, L.i[r], 31);
+    }
+#pragma unroll
+    for (int r = R - 1; r >= 0; --r) {
+        const int j = r * 32 + lane;
+        double prev_d = upd[r];
+        uint32_t prev_i = upi[r];
+        if (lane == 0) {
+            prev_d = (r > 0) ? carry_d[r > 0 ? r - 1 : 0] : (double)INFINITY;
+            prev_i = (r > 0) ? carry_i[r > 0 ? r - 1 : 0] : 0xffffffffu;
+        }
+        if (j == pos) {
+            L.d[r] = cd;
+            L.i[r] = ci;
+        } else if (j > pos) {
+            L.d[r] = prev_d;
+            L.i[r] = prev_i;
+        }
+        if (j >= (int)K) {
+            L.d[r] = INFINITY;
+            L.i[r] = 0xffffffffu;
+        }
+    }
+    if (nl < K) ++nl;
+}
+
+template <int R>
+__device__ __forceinline__ void reglist_kth(const RegList<R>& L, uint32_t K, double& td, uint32_t& ti) {
+    const int r = (int)(K - 1) >> 5, src = (int)(K - 1) & 31;
+    double d = L.d[0];
+    uint32_t i = L.i[0];
+#pragma unroll
+    for (int rr = 1; rr < R; ++rr)
+        if (rr == r) {
+            d = L.d[rr];
+            i = L.i[rr];
+        }
+    td = __shfl_sync(0xffffffffu, d, src);
+    ti = __shfl_sync(0xffffffffu, i, src);
+}
+
+template <int R>
+__global__ void __launch_bounds__(kKnnThreads) k_knn_reg(KnnArgs a) {
+    __shared__ uint32_t st_a[kKnnWarps][kKnnStack];   // leaf: first point; internal: first child
+    __shared__ uint32_t st_b[kKnnWarps][kKnnStack];   // leaf: end point; internal: 0xffffffff
+    __shared__ double st_lb[kKnnWarps][kKnnStack];
+    __shared__ uint8_t st_depth[kKnnWarps][kKnnStack];
+    __shared__ double s_radii[kMaxDepth + 1][3];
+    for (int i = threadIdx.x; i < (kMaxDepth + 1) * 3; i += kKnnThreads)
+        (&s_radii[0][0])[i] = (&a.geom->radii[0][0])[i];
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    uint32_t* sa = st_a[warp];
+    uint32_t* sb = st_b[warp];
+    double* sl = st_lb[warp];
+    uint8_t* sd = st_depth[warp];
+    const uint32_t K = a.k;
+    const uint64_t nwarps = (uint64_t)gridDim.x * kKnnWarps;
+    for (uint64_t qpos = (uint64_t)blockIdx.x * kKnnWarps + warp; qpos < a.nq; qpos += nwarps) {
+        const uint64_t q = a.order ? a.order[qpos] : qpos;
+        const double p[3] = {a.q[3 * q], a.q[3 * q + 1], a.q[3 * q + 2]};
+        RegList<R> L;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            L.d[r] = INFINITY;
+            L.i[r] = 0xffffffffu;
+        }
+        uint32_t nl = 0;
+        double thr = INFINITY;
+        uint32_t thr_i = 0xffffffffu;
+        bool failed = false;
+        // root (bound 0, linear_octree.hpp:904)
+        {
+            const uint32_t fc0 = a.offsets[0];
+            const uint2 rg0 = a.ranges[0];
+            if (lane == 0) {
+                sa[0] = fc0 ? fc0 : rg0.x;
+                sb[0] = fc0 ? 0xffffffffu : rg0.y;
+                sl[0] = 0.0;
+                sd[0] = 0;
+            }
+        }
+        __syncwarp();
+        int sp = 1;
+        while (sp > 0) {
+            --sp;
+            const uint32_t ea = sa[sp], eb = sb[sp];
+            const double lb = sl[sp];
+            const uint32_t depth = sd[sp];
+            __syncwarp();
+            if (lb > thr) continue;
+            if (eb != 0xffffffffu) {
+                // leaf [ea, eb): candidates beat the k-th pair
+                for (uint32_t b = ea; b < eb; b += 32) {
+                    const uint32_t i = b + lane;
+                    double d = INFINITY;
+                    bool cand = false;
+                    if (i < eb) {
+                        d = dist_pp(p[0], p[1], p[2], a.xs[i], a.ys[i], a.zs[i]);
+                        cand = pair_less(d, i, thr, thr_i);
+                    }
+                    uint32_t m = __ballot_sync(0xffffffffu, cand);
+                    while (m) {
+                        const int src = __ffs(m) - 1;
+                        m &= m - 1;
+                        const double cd = __shfl_sync(0xffffffffu, d, src);
+                        const uint32_t ci = b + (uint32_t)src;
+                        if (pair_less(cd, ci, thr, thr_i)) {
+                            reglist_insert<R>(L, cd, ci, K, nl);
+                            if (nl == K) reglist_kth<R>(L, K, thr, thr_i);
+                        }
+                    }
+                }
+                continue;
+            }
+            // internal: judge the 8 children (bound, first child / range), nearest on top
+            const uint32_t fc = ea;
+            const uint32_t cd = depth + 1;
+            double clb = INFINITY;
+            bool keep = false;
+            uint32_t ca = 0, cb = 0;
+            if (lane < 8) {
+                const uint32_t child = fc + lane;
+                clb = dist_po(p, a.centers + 3ull * child, s_radii[cd]);
+                const uint32_t cfc = a.offsets[child];
+                if (cfc) {
+                    ca = cfc;
+                    cb = 0xffffffffu;
+                    keep = !(clb > thr);
+                } else {
+                    const uint2 rg = a.ranges[child];
+                    ca = rg.x;
+                    cb = rg.y;
+                    keep = (rg.y > rg.x) && !(clb > thr);  // an empty leaf holds no candidate
+                }
+            }
+            const uint32_t km = __ballot_sync(0xffffffffu, keep) & 0xffu;
+            const int nk = __popc(km);
+            if (sp + nk > kKnnStack) {
+                failed = true;
+                break;
+            }
+            int pos = 0;
+#pragma unroll
+            for (int o = 0; o < 8; ++o) {
+                const double ol = __shfl_sync(0xffffffffu, clb, o);
+                const bool ok = (km >> o) & 1u;
+                if (ok && o != lane && ((ol > clb) || (ol == clb && o > lane))) ++pos;
+            }
+            if (keep) {
+                const int slot = sp + pos;
+                sa[slot] = ca;
+                sb[slot] = cb;
+                sl[slot] = clb;
+                sd[slot] = (uint8_t)cd;
+            }
+            __syncwarp();
+            sp += nk;
+        }
+        if (failed) set_err(a.err, kErrStackOverflow);
+        const uint64_t o = q * (uint64_t)K;
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            const uint32_t j = (uint32_t)(r * 32 + lane);
+            if (j < K) {
+                a.idx[o + j] = (j < nl) ? L.i[r] : 0xffffffffu;
+                a.d2[o + j] = (j < nl) ? L.d[r] : (double)INFINITY;
+            }
+        }
+        if (lane == 0 && a.counts) a.counts[q] = nl;
+        __syncwarp();
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Packet kNN: 32 curve-ordered queries per warp, one per lane.
+//
+// The warp walks the tree once for its 32 queries.  Every lane keeps its own
+// k best (squared distance, index) pairs in a max-heap in shared memory (root =
+// the current k-th pair), so a lane's threshold is the root once the heap is
+// full.  A node is visited by the lanes whose lower bound to it (the
+// reference's clamp-to-box distance) does not exceed their threshold; the
+// children of a node are pushed with the mask of lanes that accept them,
+// nearest to the packet's centroid on top.  A leaf's points are staged in
+// shared memory once per warp and every visiting lane offers them to its heap.
+// At the end each lane heap-sorts its pairs into ascending (distance, index)
+// order, which is the device's tie rule.
+// ---------------------------------------------------------------------------
+
+template <int KCAP>
+struct KnnPkShape {
+    static constexpr int kWarps = (KCAP <= 64) ? 4 : 2;
+};
+
+__device__ __forceinline__ bool pair_gt(double da, uint32_t ia, double db, uint32_t ib) {
+    return (da > db) || (da == db && ia > ib);
+}
+
+template <int KCAP>
+__global__ void __launch_bounds__(32 * KnnPkShape<KCAP>::kWarps) k_knn_packet(KnnArgs a, const uint32_t* order,
+                                                                              uint32_t* packet_ctr) {
+    constexpr int W = KnnPkShape<KCAP>::kWarps;
+    extern __shared__ __align__(16) unsigned char smem[];
+    // per warp: heap distances [KCAP][32], heap indices [KCAP][32]
+    double* hd_all = reinterpret_cast<double*>(smem);
+    uint32_t* hi_all = reinterpret_cast<uint32_t*>(hd_all + (size_t)W * KCAP * 32);
+    __shared__ uint32_t st_node[W][kKnnStack];
+    __shared__ uint32_t st_mask[W][kKnnStack];
+    __shared__ uint8_t st_depth[W][kKnnStack];
+    __shared__ double sx[W][32], sy[W][32], sz[W][32];
+    __shared__ double s_radii[kMaxDepth + 1][3];
+    for (int i = threadIdx.x; i < (kMaxDepth + 1) * 3; i += 32 * W) (&s_radii[0][0])[i] = (&a.geom->radii[0][0])[i];
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t lbit = 1u << lane;
+    double* hd = hd_all + (size_t)warp * KCAP * 32;
+    uint32_t* hx = hi_all + (size_t)warp * KCAP * 32;
+#define HD(j) hd[(j) * 32 + lane]
+#define HX(j) hx[(j) * 32 + lane]
+    const uint32_t K = a.k;
+
+    for (;;) {
+        uint32_t packet = 0;
+        if (lane == 0) packet = atomicAdd(packet_ctr, 1u);
+        packet = __shfl_sync(0xffffffffu, packet, 0);
+        const uint64_t i0 = (uint64_t)packet * 32;
+        if (i0 >= a.nq) break;
+        const uint64_t qpos = i0 + lane;
+        const bool valid = qpos < a.nq;
+        const uint32_t qi = valid ? order[qpos] : 0u;
+        const double p[3] = {a.q[3ull * qi], a.q[3ull * qi + 1], a.q[3ull * qi + 2]};
+        // packet centroid, used only to order children
+        const uint32_t vmask = __ballot_sync(0xffffffffu, valid);
+        const double inv = 1.0 / (double)__popc(vmask);
+        double cen[3];
+#pragma unroll
+        for (int ax = 0; ax < 3; ++ax) {
+            double v = valid ? p[ax] : 0.0;
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+            cen[ax] = v * inv;
+        }
+        uint32_t hs = 0;  // heap size of this lane
+        auto thr_d = [&]() { return (hs < K) ? (double)INFINITY : HD(0); };
+        auto offer = [&](double d, uint32_t idx) {
+            if (hs < K) {
+                uint32_t j = hs++;
+                while (j > 0) {
+                    const uint32_t pj = (j - 1) >> 1;
+                    if (!pair_gt(d, idx, HD(pj), HX(pj))) break;
+                    HD(j) = HD(pj);
+                    HX(j) = HX(pj);
+                    j = pj;
+                }
+                HD(j) = d;
+                HX(j) = idx;
+            } else if (pair_less(d, idx, HD(0), HX(0))) {
+                uint32_t j = 0;
+                for (;;) {
+                    const uint32_t l = 2 * j + 1;
+                    if (l >= K) break;
+                    uint32_t m = l;
+                    if (l + 1 < K && pair_gt(HD(l + 1), HX(l + 1), HD(l), HX(l))) m = l + 1;
+                    if (!pair_gt(HD(m), HX(m), d, idx)) break;
+                    HD(j) = HD(m);
+                    HX(j) = HX(m);
+                    j = m;
+                }
+                HD(j) = d;
+                HX(j) = idx;
+            }
+        };
+
+        int sp = 0;
+        if (lane == 0) {
+            st_node[warp][0] = 0;
+            st_mask[warp][0] = vmask;
+            st_depth[warp][0] = 0;
+        }
+        __syncwarp();
+        if (vmask) sp = 1;
+        bool failed = false;
+        while (sp > 0) {
+            --sp;
+            const uint32_t node = st_node[warp][sp];
+            const uint32_t mask = st_mask[warp][sp];
+            const uint32_t depth = st_depth[warp][sp];
+            __syncwarp();
+            // lanes still interested: lower bound within their threshold (root: bound 0)
+            bool act = (mask & lbit) != 0;
+            if (act && depth > 0) act = !(dist_po(p, a.centers + 3ull * node, s_radii[depth]) > thr_d());
+            const uint32_t am = __ballot_sync(0xffffffffu, act);
+            if (!am) continue;
+            const uint32_t fc = a.offsets[node];
+            if (fc == 0) {
+                const uint2 rg = a.ranges[node];
+                for (uint32_t b = rg.x; b < rg.y; b += 32) {
+                    const uint32_t idx = b + lane;
+                    if (idx < rg.y) {
+                        sx[warp][lane] = a.xs[idx];
+                        sy[warp][lane] = a.ys[idx];
+                        sz[warp][lane] = a.zs[idx];
+                    }
+                    __syncwarp();
+                    const uint32_t m = (rg.y - b < 32u) ? (rg.y - b) : 32u;
+                    if (act) {
+                        for (uint32_t t = 0; t < m; ++t) {
+                            const double d = dist_pp(p[0], p[1], p[2], sx[warp][t], sy[warp][t], sz[warp][t]);
+                            if (hs < K || !pair_gt(d, b + t, HD(0), HX(0))) offer(d, b + t);
+                        }
+                    }
+                    __syncwarp();
+                }
+                continue;
+            }
+            const uint32_t cd = depth + 1;
+            uint32_t cm[8];
+            const double th = act ? thr_d() : -1.0;
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                bool ok = false;
+                if (act) ok = !(dist_po(p, a.centers + 3ull * (fc + j), s_radii[cd]) > th);
+                cm[j] = __ballot_sync(0xffffffffu, ok);
+            }
+            // order key: the centroid's bound to each child, computed on lanes 0..7
+            double key = INFINITY;
+            if (lane < 8) key = dist_po(cen, a.centers + 3ull * (fc + lane), s_radii[cd]);
+            int np = 0;
+#pragma unroll
+            for (int j = 0; j < 8; ++j) np += (cm[j] != 0);
+            if (sp + np > kKnnStack) {
+                failed = true;
+                break;
+            }
+            // slot of child j among pushed children: farther (or equal and higher octant) ones go deeper
+            int pos = 0;
+            uint32_t myc = 0;
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                const double kj = __shfl_sync(0xffffffffu, key, j);
+                if (lane < 8 && cm[j] != 0 && j != lane && ((kj > key) || (kj == key && j > lane))) ++pos;
+                if (lane == j) myc = cm[j];
+            }
+            if (lane < 8 && myc != 0) {
+                st_node[warp][sp + pos] = fc + lane;
+                st_mask[warp][sp + pos] = myc;
+                st_depth[warp][sp + pos] = (uint8_t)cd;
+            }
+            __syncwarp();
+            sp += np;
+        }
+        if (failed) set_err(a.err, kErrStackOverflow);
+        if (valid) {
+            // heap-sort into ascending (distance, index)
+            for (uint32_t e = hs; e > 1; --e) {
+                const uint32_t last = e - 1;
+                const double d = HD(last);
+                const uint32_t ix = HX(last);
+                HD(last) = HD(0);
+                HX(last) = HX(0);
+                uint32_t j = 0;
+                for (;;) {
+                    const uint32_t l = 2 * j + 1;
+                    if (l >= last) break;
+                    uint32_t m = l;
+                    if (l + 1 < last && pair_gt(HD(l + 1), HX(l + 1), HD(l), HX(l))) m = l + 1;
+                    if (!pair_gt(HD(m), HX(m), d, ix)) break;
+                    HD(j) = HD(m);
+                    HX(j) = HX(m);
+                    j = m;
+                }
+                HD(j) = d;
+                HX(j) = ix;
+            }
+            const uint64_t o = (uint64_t)qi * K;
+            for (uint32_t j = 0; j < K; ++j) {
+                a.idx[o + j] = (j < hs) ? HX(j) : 0xffffffffu;
+                a.d2[o + j] = (j < hs) ? HD(j) : (double)INFINITY;
+            }
+            if (a.counts) a.counts[qi] = hs;
+        }
+        __syncwarp();
+    }
+#undef HD
+#undef HX
+}
+
+template <int KCAP>
+cudaError_t launch_knn_pk(const KnnArgs& a, const uint32_t* order, uint32_t* ctr, int sms, cudaStream_t s) {
+    constexpr int W = KnnPkShape<KCAP>::kWarps;
+    const size_t smem = (size_t)W * KCAP * 32 * 12;
+    cudaError_t e = cudaFuncSetAttribute(k_knn_packet<KCAP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    const uint64_t packets = (a.nq + 31) / 32;
+    const uint64_t want = (packets + W - 1) / W;
+    const uint64_t cap = (uint64_t)sms * 8;
+    const int grid = (int)(want < cap ? want : cap);
+    k_knn_packet<KCAP><<<grid, 32 * W, smem, s>>>(a, order, ctr);
+    return cudaGetLastError();
+}
+
 int sm_count_k(int device) {
     int v = 148;
     cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, device);
@@ -254,9 +693,34 @@ cudaError_t launch_knn(Cloud& c, const double* d_centers, uint64_t nq, uint32_t 
     a.d2 = d_d2;
     a.counts = d_counts;
     a.err = c.d_err.as<uint32_t>();
+    a.order = nullptr;
+    if (c.packet) {  // curve-ordered queries: neighbouring warps share octants in cache
+        cudaError_t e;
+        if ((e = launch_query_order(c, d_centers, nq, &a.order)) != cudaSuccess) return e;
+    }
+    if (c.packet && c.knn_packet && k <= 128) {
+        cudaError_t e;
+        const uint32_t* order = a.order;
+        if ((e = c.packet_ctr.reserve(256)) != cudaSuccess) return e;
+        if ((e = cudaMemsetAsync(c.packet_ctr.ptr, 0, 4, c.stream)) != cudaSuccess) return e;
+        uint32_t* ctr = c.packet_ctr.as<uint32_t>();
+        const int sms = sm_count_k(c.device);
+        if (k <= 16) return launch_knn_pk<16>(a, order, ctr, sms, c.stream);
+        if (k <= 32) return launch_knn_pk<32>(a, order, ctr, sms, c.stream);
+        if (k <= 64) return launch_knn_pk<64>(a, order, ctr, sms, c.stream);
+        return launch_knn_pk<128>(a, order, ctr, sms, c.stream);
+    }
     const uint64_t want = (nq + kKnnWarps - 1) / kKnnWarps;
     const uint64_t cap = (uint64_t)sm_count_k(c.device) * 16;
     const int grid = (int)(want < cap ? want : cap);
+    if (c.packet && k <= 32) {
+        k_knn_reg<1><<<grid, kKnnThreads, 0, c.stream>>>(a);
+        return cudaGetLastError();
+    }
+    if (c.packet && k <= 64) {
+        k_knn_reg<2><<<grid, kKnnThreads, 0, c.stream>>>(a);
+        return cudaGetLastError();
+    }
     if (k <= 32) return launch_l<32>(a, grid, c.stream);
     if (k <= 64) return launch_l<64>(a, grid, c.stream);
     if (k <= 128) return launch_l<128>(a, grid, c.stream);

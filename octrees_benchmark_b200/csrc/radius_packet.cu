@@ -1,0 +1,482 @@
+// Batched ("packet") radius search: neighbors / neighborsPrune / neighborsStruct
+// for 32 spatially ordered queries per warp.
+//
+// Reference path replaced: the same as radius_search.cu - singleTraversal
+// (inc/structures/linear_octree.hpp:653-686) with the criteria and leaf actions of
+// neighborsStruct (695-736), neighborsPrune (746-784) and neighbors (796-816).
+//
+// B200 design.  The query centres are first ordered along the cloud's curve
+// (launch_query_order), so the 32 queries of a warp are neighbours in space and
+// need almost the same octants.  The warp walks the tree once for all of them:
+// at every internal node each lane judges the 8 children for its own query (the
+// reference's predicates, bit for bit), and a child is pushed with two lane
+// masks - the lanes for which it is fully inside (they emit its whole range
+// when it is popped) and the lanes that must descend into it.  Pushing the
+// children lowest octant last keeps every lane's output in ascending order.  A
+// leaf's points are staged in shared memory once per warp (coalesced) and every
+// lane of the descend mask tests its query against all of them.  Packets are
+// handed out by an atomic counter so that long and short packets balance.
+//
+// FP32 variant (the precision form): each sorted point also has FP32
+// coordinates relative to its leaf's centre (x, y, z computed in FP64 and
+// rounded once; w = their L1 norm).  A lane tests its query, made relative to
+// the same centre, in FP32; a point whose FP32 result lies within a rigorous
+// error band of the decision boundary is re-tested in FP64 on the original
+// coordinates with the reference's expression, so every decision is still the
+// reference's.  Band (sphere / circle, inside iff d2 < r2 / d2 <= r2):
+//   |d2_fp32 - d2| <= 2^-23 (|q|_1 + |p|_1 + 1.74 r) r + 3 2^-24 d2 near the
+//   boundary, plus 2^-24 r2 for rounding r2 to FP32; the band used is 2 to 4
+//   times that:  2^-21 ((|q|_1 + |p|_1 + 2 r) r + r2).
+// Cube / square: per axis, the interval bounds bmin = c - r and bmax = c + r
+// (FP64) are made leaf-relative and rounded to FP32; an axis is certain when
+// its margin exceeds 2^-22 (|p_i| + |bound_i|).
+#include <cfloat>
+
+#include "cloud.h"
+#include "search_kernels.cuh"
+
+namespace octb {
+
+namespace {
+
+constexpr int kPkWarps = 4;
+constexpr int kPkThreads = 32 * kPkWarps;
+constexpr int kPkStack = 8 * (kMaxDepth + 1);
+
+struct PacketArgs {
+    const double* xs;
+    const double* ys;
+    const double* zs;
+    const float4* rel;
+    const uint32_t* offsets;
+    const uint2* ranges;
+    const double* centers;
+    const LevelGeom* geom;
+    const double* q;
+    const double* qr;
+    double radius;
+    const uint32_t* order;
+    uint64_t nq;
+    unsigned long long* counts;
+    unsigned long long* counts2;
+    const unsigned long long* offs;
+    uint32_t* out;
+    uint64_t out_cap;
+    uint32_t* packet_ctr;
+    unsigned long long* stats;  // [0] point tests, [1] FP64 re-tests
+    uint32_t* err;
+};
+
+// Per-lane FP32 context of one leaf.
+struct LeafCtx {
+    float qx, qy, qz;  // query centre relative to the leaf centre
+    float r2f;         // radius^2 rounded to FP32 (sphere, circle)
+    float b0, b1;      // band = b0 + b1 * |p|_1 (sphere, circle)
+    float lo[3], hi[3], tlo[3], thi[3];  // relative interval bounds and their tolerances (cube, square)
+};
+
+template <int KT>
+__device__ __forceinline__ void leaf_ctx(const SearchKernel& k, const double* lc, LeafCtx& c) {
+    c.qx = (float)dsub(k.c[0], lc[0]);
+    c.qy = (float)dsub(k.c[1], lc[1]);
+    c.qz = (float)dsub(k.c[2], lc[2]);
+    const float r = (float)k.r;
+    if constexpr (KT == kSphere || KT == kCircle) {
+        const float q1 = fabsf(c.qx) + fabsf(c.qy) + ((KT == kSphere) ? fabsf(c.qz) : 0.0f);
+        c.r2f = (float)k.r2;
+        const float s = 4.76837158203125e-07f;  // 2^-21
+        c.b0 = s * ((q1 + 2.0f * r) * r + c.r2f) + FLT_MIN;
+        c.b1 = s * r;
+    } else {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            c.lo[a] = (float)dsub(k.bmin[a], lc[a]);
+            c.hi[a] = (float)dsub(k.bmax[a], lc[a]);
+            c.tlo[a] = 2.384185791015625e-07f * fabsf(c.lo[a]);  // 2^-22 |bound|
+            c.thi[a] = 2.384185791015625e-07f * fabsf(c.hi[a]);
+        }
+    }
+}
+
+// FP32 test: 1 inside, 0 outside, -1 undecided (re-test in FP64).
+template <int KT>
+__device__ __forceinline__ int f32_test(const LeafCtx& c, float4 p) {
+    if constexpr (KT == kSphere || KT == kCircle) {
+        const float dx = p.x - c.qx, dy = p.y - c.qy;
+        float d2 = __fmaf_rn(dy, dy, __fmul_rn(dx, dx));
+        if constexpr (KT == kSphere) {
+            const float dz = p.z - c.qz;
+            d2 = __fmaf_rn(dz, dz, d2);
+        }
+        const float band = __fmaf_rn(c.b1, p.w, c.b0);
+        if (d2 < c.r2f - band) return 1;
+        if (d2 > c.r2f + band) return 0;
+        return -1;
+    } else {
+        constexpr int D = (KT == kCube) ? 3 : 2;
+        const float pv[3] = {p.x, p.y, p.z};
+        const float tp = 2.384185791015625e-07f * p.w;  // 2^-22 |p|_1 >= 2^-22 |p_i|
+        bool sure_in = true;
+#pragma unroll
+        for (int a = 0; a < D; ++a) {
+            const float ml = pv[a] - c.lo[a], mh = c.hi[a] - pv[a];
+            const float tl = tp + c.tlo[a], th = tp + c.thi[a];
+            if (ml < -tl || mh < -th) return 0;
+            sure_in = sure_in && (ml > tl) && (mh > th);
+        }
+        return sure_in ? 1 : -1;
+    }
+}
+
+template <int KT, int ALGO, bool FILL, bool F32>
+__global__ void __launch_bounds__(kPkThreads) k_radius_packet(PacketArgs a) {
+    __shared__ uint32_t st_node[kPkWarps][kPkStack];
+    __shared__ uint32_t st_fc[kPkWarps][kPkStack];     // first child, 0 for a leaf
+    __shared__ uint2 st_rg[kPkWarps][kPkStack];        // point range
+    __shared__ uint32_t st_over[kPkWarps][kPkStack];
+    __shared__ uint32_t st_in[kPkWarps][kPkStack];
+    __shared__ uint8_t st_depth[kPkWarps][kPkStack];
+    __shared__ double s_radii[kMaxDepth + 1][3];
+    __shared__ double sx[kPkWarps][32], sy[kPkWarps][32], sz[kPkWarps][32];
+    __shared__ float4 sp[kPkWarps][32];
+
+    for (int i = threadIdx.x; i < (kMaxDepth + 1) * 3; i += kPkThreads)
+        (&s_radii[0][0])[i] = (&a.geom->radii[0][0])[i];
+    __syncthreads();
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t lbit = 1u << lane;
+    uint32_t* sn = st_node[warp];
+    uint32_t* sf = st_fc[warp];
+    uint2* sr = st_rg[warp];
+    uint32_t* so = st_over[warp];
+    uint32_t* si = st_in[warp];
+    uint8_t* sd = st_depth[warp];
+    unsigned long long n_tests = 0, n_retests = 0;
+
+    for (;;) {
+        uint32_t packet = 0;
+        if (lane == 0) packet = atomicAdd(a.packet_ctr, 1u);
+        packet = __shfl_sync(0xffffffffu, packet, 0);
+        const uint64_t i0 = (uint64_t)packet * 32;
+        if (i0 >= a.nq) break;
+        const uint64_t i = i0 + lane;
+        const bool valid = i < a.nq;
+        const uint32_t qi = valid ? (a.order ? a.order[i] : (uint32_t)i) : 0u;
+        SearchKernel k;
+        k.init(a.q[3ull * qi], a.q[3ull * qi + 1], a.q[3ull * qi + 2], a.qr ? a.qr[qi] : a.radius);
+        unsigned long long cnt = 0, cnt2 = 0, base = 0;
+        if (FILL && valid) base = a.offs[qi];
+        bool overflow = false;
+        bool open = false;  // neighborsStruct: a run of inside points is open
+        uint32_t rs = 0;
+
+        auto emit_range = [&](uint32_t f, uint32_t l) {  // per lane
+            if constexpr (ALGO == kStruct) {
+                if (FILL) {
+                    const unsigned long long o = base + cnt;
+                    if (o < a.out_cap) {
+                        a.out[2 * o] = f;
+                        a.out[2 * o + 1] = l;
+                    } else {
+                        overflow = true;
+                    }
+                }
+                cnt += 1;
+                cnt2 += (unsigned long long)(l - f);
+            } else {
+                if (FILL) {
+                    for (uint32_t t = f; t < l; ++t) {
+                        const unsigned long long o = base + cnt + (t - f);
+                        if (o < a.out_cap) a.out[o] = t;
+                        else overflow = true;
+                    }
+                }
+                cnt += (unsigned long long)(l - f);
+            }
+        };
+        auto hit = [&](uint32_t idx, bool in) {  // per lane, points in order
+            if constexpr (ALGO == kStruct) {
+                if (in && !open) {
+                    open = true;
+                    rs = idx;
+                } else if (!in && open) {
+                    open = false;
+                    emit_range(rs, idx);
+                }
+            } else {
+                if (in) {
+                    if (FILL) {
+                        const unsigned long long o = base + cnt;
+                        if (o < a.out_cap) a.out[o] = idx;
+                        else overflow = true;
+                    }
+                    ++cnt;
+                }
+            }
+        };
+        auto scan_leaf = [&](uint32_t node, uint2 rg, uint32_t mask) {
+            const bool mine = (mask & lbit) != 0;
+            LeafCtx ctx;
+            if (F32 && mine) leaf_ctx<KT>(k, a.centers + 3ull * node, ctx);
+            for (uint32_t b = rg.x; b < rg.y; b += 32) {
+                const uint32_t idx = b + lane;
+                if (idx < rg.y) {
+                    if (F32) {
+                        sp[warp][lane] = a.rel[idx];
+                    } else {
+                        sx[warp][lane] = a.xs[idx];
+                        sy[warp][lane] = a.ys[idx];
+                        sz[warp][lane] = a.zs[idx];
+                    }
+                }
+                __syncwarp();
+                const uint32_t m = (rg.y - b < 32u) ? (rg.y - b) : 32u;
+                if (mine) {
+                    for (uint32_t t = 0; t < m; ++t) {
+                        bool in;
+                        if (F32) {
+                            const int r = f32_test<KT>(ctx, sp[warp][t]);
+                            if (r < 0) {
+                                in = is_inside<KT>(k, a.xs[b + t], a.ys[b + t], a.zs[b + t]);
+                                ++n_retests;
+                            } else {
+                                in = r > 0;
+                            }
+                        } else {
+                            in = is_inside<KT>(k, sx[warp][t], sy[warp][t], sz[warp][t]);
+                        }
+                        hit(b + t, in);
+                    }
+                    n_tests += m;
+                }
+                __syncwarp();
+            }
+            if (ALGO == kStruct && mine && open) {
+                open = false;
+                emit_range(rs, rg.y);
+            }
+        };
+
+        // root: continuationCriterion(0, 0)
+        bool over = false, in = false;
+        if (valid) {
+            if constexpr (ALGO == kNeighbors) {
+                over = box_overlap<KT>(k, a.centers, s_radii[0]);
+            } else {
+                const int j = box_intersect<KT>(k, a.centers, s_radii[0]);
+                in = (j == kInside);
+                over = (j == kOverlap);
+            }
+        }
+        int sp_top = 0;
+        {
+            const uint32_t mo = __ballot_sync(0xffffffffu, over);
+            const uint32_t mi = __ballot_sync(0xffffffffu, in);
+            if (mo | mi) {
+                const uint32_t fc0 = a.offsets[0];
+                const uint2 rg0 = a.ranges[0];
+                if (lane == 0) {
+                    sn[0] = 0;
+                    sf[0] = fc0;
+                    sr[0] = rg0;
+                    so[0] = mo;
+                    si[0] = mi;
+                    sd[0] = 0;
+                }
+                sp_top = 1;
+            }
+        }
+        __syncwarp();
+        while (sp_top > 0) {
+            --sp_top;
+            const uint32_t node = sn[sp_top];
+            const uint32_t fc = sf[sp_top];
+            const uint2 nrg = sr[sp_top];
+            const uint32_t mo = so[sp_top];
+            const uint32_t mi = si[sp_top];
+            const uint32_t depth = sd[sp_top];
+            __syncwarp();
+            if (mi & lbit) emit_range(nrg.x, nrg.y);
+            if (mo == 0) continue;
+            if (fc == 0) {
+                scan_leaf(node, nrg, mo);
+                continue;
+            }
+            const uint32_t cd = depth + 1;
+            const bool mine = (mo & lbit) != 0;
+            // lane j (< 8) keeps child j's first-child link, range and lane masks
+            uint32_t my_fc = 0, my_mo = 0, my_mi = 0;
+            uint2 my_rg = make_uint2(0u, 0u);
+            if (lane < 8) {
+                my_fc = a.offsets[fc + lane];
+                my_rg = a.ranges[fc + lane];
+            }
+#pragma unroll
+            for (int j = 0; j < 8; ++j) {
+                bool o = false, n = false;
+                if (mine) {
+                    const double* oc = a.centers + 3ull * (fc + j);
+                    if constexpr (ALGO == kNeighbors) {
+                        o = box_overlap<KT>(k, oc, s_radii[cd]);
+                    } else {
+                        const int jj = box_intersect<KT>(k, oc, s_radii[cd]);
+                        n = (jj == kInside);
+                        o = (jj == kOverlap);
+                    }
+                }
+                const uint32_t bo = __ballot_sync(0xffffffffu, o);
+                const uint32_t bi = __ballot_sync(0xffffffffu, n);
+                if (lane == j) {
+                    my_mo = bo;
+                    my_mi = bi;
+                }
+            }
+            if (lane < 8 && my_fc == 0 && my_rg.x == my_rg.y) {  // empty leaf: nothing to scan or add
+                my_mo = 0;
+                if (ALGO != kStruct) my_mi = 0;  // neighborsStruct still adds its empty range
+            }
+            const uint32_t pushm = __ballot_sync(0xffffffffu, lane < 8 && (my_mo | my_mi) != 0);
+            const int np = __popc(pushm);
+            if (sp_top + np > kPkStack) {
+                overflow = true;
+                break;
+            }
+            if ((pushm >> lane) & 1u) {
+                // lowest octant on top of the stack
+                const int slot = sp_top + __popc(pushm >> (lane + 1));
+                sn[slot] = fc + lane;
+                sf[slot] = my_fc;
+                sr[slot] = my_rg;
+                so[slot] = my_mo;
+                si[slot] = my_mi;
+                sd[slot] = (uint8_t)cd;
+            }
+            __syncwarp();
+            sp_top += np;
+        }
+        if (overflow) set_err(a.err, FILL ? kErrOutputCapacity : kErrStackOverflow);
+        if (!FILL && valid) {
+            a.counts[qi] = cnt;
+            if (ALGO == kStruct) a.counts2[qi] = cnt2;
+        }
+        __syncwarp();
+    }
+    if (a.stats) {
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) {
+            n_tests += __shfl_down_sync(0xffffffffu, n_tests, off);
+            n_retests += __shfl_down_sync(0xffffffffu, n_retests, off);
+        }
+        if (lane == 0) {
+            atomicAdd(&a.stats[0], n_tests);
+            atomicAdd(&a.stats[1], n_retests);
+        }
+    }
+}
+
+// FP32 leaf-relative coordinates: one warp per node; leaves write their points.
+__global__ void k_leaf_rel(const double* __restrict__ xs, const double* __restrict__ ys,
+                           const double* __restrict__ zs, const uint32_t* __restrict__ offsets,
+                           const uint2* __restrict__ ranges, const double* __restrict__ centers, uint32_t n_total,
+                           float4* __restrict__ rel) {
+    const uint64_t w = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const int lane = threadIdx.x & 31;
+    if (w >= n_total) return;
+    const uint32_t node = (uint32_t)w;
+    if (offsets[node] != 0) return;
+    const uint2 rg = ranges[node];
+    const double cx = centers[3ull * node], cy = centers[3ull * node + 1], cz = centers[3ull * node + 2];
+    for (uint32_t i = rg.x + lane; i < rg.y; i += 32) {
+        float4 v;
+        v.x = (float)dsub(xs[i], cx);
+        v.y = (float)dsub(ys[i], cy);
+        v.z = (float)dsub(zs[i], cz);
+        // L1 norm, rounded up so that it bounds the exact L1 norm of (x, y, z) so that it bounds the exact L1 norm of (x, y, z) in FP32
+        v.w = __fadd_ru(__fadd_ru(fabsf(v.x), fabsf(v.y)), fabsf(v.z));
+        rel[i] = v;
+    }
+}
+
+int sm_count_p(int device) {
+    int v = 148;
+    cudaDeviceGetAttribute(&v, cudaDevAttrMultiProcessorCount, device);
+    return v;
+}
+
+template <int KT, int ALGO>
+cudaError_t launch_pk(const PacketArgs& a, bool fill, bool fp32, int grid, cudaStream_t s) {
+    if (fill) {
+        if (fp32) k_radius_packet<KT, ALGO, true, true><<<grid, kPkThreads, 0, s>>>(a);
+        else k_radius_packet<KT, ALGO, true, false><<<grid, kPkThreads, 0, s>>>(a);
+    } else {
+        if (fp32) k_radius_packet<KT, ALGO, false, true><<<grid, kPkThreads, 0, s>>>(a);
+        else k_radius_packet<KT, ALGO, false, false><<<grid, kPkThreads, 0, s>>>(a);
+    }
+    return cudaGetLastError();
+}
+
+template <int KT>
+cudaError_t launch_pk_a(const PacketArgs& a, int algo, bool fill, bool fp32, int grid, cudaStream_t s) {
+    switch (algo) {
+        case kNeighbors: return launch_pk<KT, kNeighbors>(a, fill, fp32, grid, s);
+        case kStruct: return launch_pk<KT, kStruct>(a, fill, fp32, grid, s);
+        default: return launch_pk<KT, kPrune>(a, fill, fp32, grid, s);
+    }
+}
+
+}  // namespace
+
+cudaError_t launch_leaf_rel(Cloud& c) {
+    cudaError_t e;
+    if ((e = c.rel.reserve(16 * (c.n ? c.n : 1))) != cudaSuccess) return e;
+    if (c.n == 0 || c.n_total == 0) return cudaSuccess;
+    const uint64_t threads = 32ull * c.n_total;
+    k_leaf_rel<<<(unsigned)((threads + 255) / 256), 256, 0, c.stream>>>(
+        c.xs.as<double>(), c.ys.as<double>(), c.zs.as<double>(), c.offsets.as<uint32_t>(), c.ranges.as<uint2>(),
+        c.centers.as<double>(), c.n_total, c.rel.as<float4>());
+    return cudaGetLastError();
+}
+
+cudaError_t launch_radius_packet(Cloud& c, int kernel, int algo, bool fill, bool fp32, const double* d_centers,
+                                 uint64_t nq, const double* d_radii, double radius, const uint32_t* d_order,
+                                 unsigned long long* d_counts, unsigned long long* d_counts2,
+                                 const unsigned long long* d_offsets, uint32_t* d_out, uint64_t out_capacity) {
+    cudaError_t e;
+    if (nq == 0) return cudaSuccess;
+    if ((e = c.packet_ctr.reserve(256)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(c.packet_ctr.ptr, 0, 4, c.stream)) != cudaSuccess) return e;
+    PacketArgs a;
+    a.xs = c.xs.as<double>();
+    a.ys = c.ys.as<double>();
+    a.zs = c.zs.as<double>();
+    a.rel = c.rel.as<float4>();
+    a.offsets = c.offsets.as<uint32_t>();
+    a.ranges = c.ranges.as<uint2>();
+    a.centers = c.centers.as<double>();
+    a.geom = reinterpret_cast<const LevelGeom*>(c.d_box.as<unsigned char>() + sizeof(BoxD));
+    a.q = d_centers;
+    a.qr = d_radii;
+    a.radius = radius;
+    a.order = d_order;
+    a.nq = nq;
+    a.counts = d_counts;
+    a.counts2 = d_counts2;
+    a.offs = d_offsets;
+    a.out = d_out;
+    a.out_cap = out_capacity;
+    a.packet_ctr = c.packet_ctr.as<uint32_t>();
+    a.stats = c.stats.as<unsigned long long>();
+    a.err = c.d_err.as<uint32_t>();
+    const uint64_t packets = (nq + 31) / 32;
+    const uint64_t want = (packets + kPkWarps - 1) / kPkWarps;
+    const uint64_t cap = (uint64_t)sm_count_p(c.device) * 12;
+    const int grid = (int)(want < cap ? want : cap);
+    switch (kernel) {
+        case kCircle: return launch_pk_a<kCircle>(a, algo, fill, fp32, grid, c.stream);
+        case kSquare: return launch_pk_a<kSquare>(a, algo, fill, fp32, grid, c.stream);
+        case kCube: return launch_pk_a<kCube>(a, algo, fill, fp32, grid, c.stream);
+        default: return launch_pk_a<kSphere>(a, algo, fill, fp32, grid, c.stream);
+    }
+}
+
+}  // namespace octb

@@ -19,7 +19,7 @@ import ctypes as C
 import numpy as np
 
 from . import capi
-from .capi import ALGOS, ENCODERS, KERNELS, OCT_MEM_DEVICE, OctParams, OctTreeInfo, check, lib
+from .capi import ALGOS, ENCODERS, KERNELS, OCT_MEM_DEVICE, OctParams, OctSearchConfig, OctTreeInfo, check, lib
 
 
 def _ptr(a) -> int:
@@ -45,7 +45,8 @@ class LinearOctree:
     """A device-resident cloud, SFC-sorted, with its linear octree built."""
 
     def __init__(self, points, encoder="hilbert", max_points_leaf: int = 128, device: int = 0,
-                 radius_group: int = 8, stream=None):
+                 radius_group: int = 8, stream=None, packet: bool = True, fp32_filter: bool = False,
+                 knn_packet: bool = False):
         L = lib()
         self._L = L
         self.encoder = ENCODERS[encoder]
@@ -57,7 +58,8 @@ class LinearOctree:
         self._h = h
         if stream is not None:
             check(L.oct_cloud_set_stream(h, C.c_void_p(stream)), h, "oct_cloud_set_stream")
-        check(L.oct_set_radius_group(h, radius_group), h)
+        self.set_search_config(packet=packet, fp32_filter=fp32_filter, radius_lanes=radius_group,
+                               knn_packet=knn_packet)
         dev = _is_device(points)
         if not dev:
             points = _host_f64(points, 3)
@@ -90,6 +92,19 @@ class LinearOctree:
 
     def set_radius_group(self, lanes: int):
         check(self._L.oct_set_radius_group(self._h, int(lanes)), self._h)
+
+    def set_search_config(self, packet: bool = True, fp32_filter: bool = False, radius_lanes: int = 8,
+                          knn_packet: bool = False):
+        """Search path: packet (32 curve-ordered queries per warp) or one query per
+        ``radius_lanes`` lanes; FP32 leaf-relative filter with FP64 re-tests; kNN packets."""
+        cfg = OctSearchConfig(int(bool(packet)), int(bool(fp32_filter)), int(radius_lanes), int(bool(knn_packet)))
+        check(self._L.oct_set_search_config(self._h, C.byref(cfg)), self._h, "oct_set_search_config")
+
+    def search_stats(self, reset: bool = False):
+        """(point tests, FP64 re-tests) of the packet radius searches since the last reset."""
+        a, b = C.c_uint64(), C.c_uint64()
+        check(self._L.oct_search_stats(self._h, C.byref(a), C.byref(b), int(reset)), self._h)
+        return a.value, b.value
 
     # ---- sortPoints outputs ------------------------------------------------
     def sorted_points(self):

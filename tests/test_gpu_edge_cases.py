@@ -18,11 +18,21 @@ KERNELS = {"sphere": 1, "circle": 0, "cube": 3, "square": 2}
 ALGO_NAMES = {1: "neighbors", 2: "neighborsPrune", 3: "neighborsStruct"}
 
 
+SEARCH_PATHS = [dict(packet=False, fp32_filter=False), dict(packet=True, fp32_filter=False),
+                dict(packet=True, fp32_filter=True)]
+
+
 def full_check(port, pts, enc=1, leaf=128, centers=None, radii=(0.0, 0.25, 1.0, 2.5), ks=(1, 2, 5)):
+    for path in SEARCH_PATHS:
+        oc, sxyz = full_check_path(port, pts, enc, leaf, centers, radii, ks, path)
+    return oc, sxyz
+
+
+def full_check_path(port, pts, enc, leaf, centers, radii, ks, path):
     pts = np.asarray(pts, np.float64).reshape(-1, 3)
     keys, perm, box, sxyz = port.encode_sort(enc, pts)
     t = port.build(enc, keys, leaf, box)
-    oc = LinearOctree(pts, encoder=enc, max_points_leaf=leaf)
+    oc = LinearOctree(pts, encoder=enc, max_points_leaf=leaf, **path)
     gk, gp, gx = oc.sorted_points()
     assert same_f64(oc.box, box)
     assert np.array_equal(gk, keys) and np.array_equal(gp, perm) and same_f64(gx, sxyz)

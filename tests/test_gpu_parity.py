@@ -18,6 +18,16 @@ GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
 CLOUDS = sorted(p for p in glob.glob(os.path.join(GOLDEN, "*.npz")) if not p.endswith("keys_anchor.npz"))
 KERNELS = {"sphere": 1, "circle": 0, "cube": 3, "square": 2}
 ALGO_NAMES = {1: "neighbors", 2: "neighborsPrune", 3: "neighborsStruct"}
+# search paths: (packet, fp32_filter, lanes per query of the non-packet path)
+PATHS = {"lanes8": (False, False, 8, False), "lanes16": (False, False, 16, False),
+         "lanes32": (False, False, 32, False), "packet": (True, False, 8, False),
+         "packet_fp32": (True, True, 8, False), "knn_packet": (True, False, 8, True)}
+
+
+def octree(xyz, enc, leaf, path):
+    packet, fp32, lanes, knn_packet = PATHS[path]
+    return LinearOctree(xyz, encoder=enc, max_points_leaf=leaf, radius_group=lanes, packet=packet, fp32_filter=fp32,
+                        knn_packet=knn_packet)
 
 
 def load(path):
@@ -40,10 +50,10 @@ def check_cloud_against(oc, keys, ids, box, sxyz, info, arrays):
 
 
 @pytest.mark.parametrize("path", CLOUDS, ids=[os.path.basename(p)[:-4] for p in CLOUDS])
-@pytest.mark.parametrize("group", [8, 32])
-def test_gpu_matches_reference_fixture(path, group):
+@pytest.mark.parametrize("search", ["lanes8", "lanes32", "packet", "packet_fp32"])
+def test_gpu_matches_reference_fixture(path, search):
     g = load(path)
-    oc = LinearOctree(g["xyz"], encoder=int(g["encoder"]), max_points_leaf=int(g["max_leaf"]), radius_group=group)
+    oc = octree(g["xyz"], int(g["encoder"]), int(g["max_leaf"]), search)
     arrays = {k[5:]: v for k, v in g.items() if k.startswith("tree_")}
     check_cloud_against(oc, g["keys"], g["ids"], g["box"], g["sorted_xyz"], g["info"], arrays)
     q = g["centers"]
@@ -98,12 +108,15 @@ def test_gpu_build_matches_oracle(synth_cases, case):
 
 
 @pytest.mark.parametrize("case", range(len(SYNTH)))
-@pytest.mark.parametrize("group", [8, 16, 32])
-def test_gpu_radius_matches_oracle(synth_cases, case, group):
+@pytest.mark.parametrize("search", [p for p in PATHS if p != "knn_packet"])
+def test_gpu_radius_matches_oracle(synth_cases, case, search):
     xyz, enc, leaf, keys, perm, box, sxyz, t = synth_cases[case]
-    oc = LinearOctree(xyz, encoder=enc, max_points_leaf=leaf, radius_group=group)
+    oc = octree(xyz, enc, leaf, search)
     q = sxyz[query_indices(400, len(sxyz), seed=case)]
-    radii = [0.5, 2.5, 5.0] if group == 8 else [2.5]
+    # also centres that are not cloud points, some far outside the cloud
+    rng = np.random.default_rng(case)
+    q = np.concatenate([q, q[:60] + rng.normal(0, 2.0, (60, 3)), box[6:9] - 3.0 + rng.uniform(0, 1, (4, 3))])
+    radii = [0.5, 2.5, 5.0] if search in ("lanes8", "packet", "packet_fp32") else [2.5]
     for r in radii:
         for kn, kv in KERNELS.items():
             for algo in (1, 2, 3):
@@ -121,20 +134,25 @@ def test_gpu_radius_matches_oracle(synth_cases, case, group):
             assert_ranges_equal(ro, pairs, o2, p2, kn)
     # per-query radii
     rr = np.random.default_rng(case).uniform(0.5, 5.0, len(q))
-    offs, idx = oc.neighborsPrune(q, rr, "sphere")
-    o2, i2 = t.radius(sxyz, 1, 2, q, rr)
-    assert_csr_equal(offs, idx, o2, i2, "per-query radii")
+    for kn, kv in KERNELS.items():
+        offs, idx = oc.neighborsPrune(q, rr, kn)
+        o2, i2 = t.radius(sxyz, kv, 2, q, rr)
+        assert_csr_equal(offs, idx, o2, i2, f"per-query radii {kn}")
+    if search == "packet_fp32":
+        tests, retests = oc.search_stats()
+        assert tests > 0 and retests < tests  # the band catches few points
     oc.close()
 
 
 @pytest.mark.parametrize("case", range(len(SYNTH)))
-def test_gpu_knn_matches_oracle(synth_cases, case):
+@pytest.mark.parametrize("search", ["lanes8", "packet", "knn_packet"])
+def test_gpu_knn_matches_oracle(synth_cases, case, search):
     xyz, enc, leaf, keys, perm, box, sxyz, t = synth_cases[case]
-    oc = LinearOctree(xyz, encoder=enc, max_points_leaf=leaf)
+    oc = octree(xyz, enc, leaf, search)
     q = sxyz[query_indices(300, len(sxyz), seed=100 + case)]
     # also centres that are not cloud points
     q = np.concatenate([q, q[:50] + np.random.default_rng(case).normal(0, 1.0, (50, 3))])
-    for k in (1, 10, 50, 250, 1000):
+    for k in (1, 10, 16, 17, 50, 64, 65, 128, 250, 1000):
         idx, d2, cnt = oc.knn(q, k)
         i2, d22, c2 = t.knn(sxyz, q, k)
         assert_knn_equal(idx, d2, cnt, i2, d22, c2, sxyz, q, f"k={k}")
