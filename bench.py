@@ -270,7 +270,7 @@ def run_b200(args, rank, world, local_rank):
 
     def configure(name):
         packet, fp32, lanes, knn_packet = SEARCH_PATHS[name]
-        cfg = capi.OctSearchConfig(packet, fp32, lanes, knn_packet)
+        cfg = capi.OctSearchConfig(packet, fp32, lanes, knn_packet, args.knn_bucket)
         capi.check(L.oct_set_search_config(h, C.byref(cfg)), h, "search config")
 
     def step(b):
@@ -418,6 +418,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--radius-group", type=int, default=8, help="lanes per query of the plain path")
+    ap.add_argument("--knn-bucket", type=int, default=256, help="kNN: subtrees this small are scanned as one range")
     ap.add_argument("--search", default="packet", choices=["plain", "packet", "packet_fp32", "knn_packet"],
                     help="search path whose numbers are the headline value")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)

@@ -118,12 +118,18 @@ int oct_set_radius_group(oct_cloud cloud, int lanes);
  *  radius_lanes lanes per query when packet is 0: 8 (default), 16 or 32.
  *  knn_packet   1: kNN also walks 32 queries per warp (each lane its own
  *               k-heap; k <= 128); 0 (default): one warp per query, visited
- *               in curve order when packet is 1. */
+ *               in curve order when packet is 1.
+ *  knn_bucket   kNN with k <= 64 on the packet path scans any subtree of at
+ *               most this many points as one contiguous range instead of
+ *               descending into it (default 256; 0 descends to the leaves).
+ *               Extra points cannot change the k best pairs. */
 typedef struct {
     int32_t packet;
     int32_t fp32_filter;
     int32_t radius_lanes;
     int32_t knn_packet;
+    int32_t knn_bucket;
+    int32_t reserved[3];
 } oct_search_config;
 int oct_set_search_config(oct_cloud cloud, const oct_search_config* config);
 

@@ -36,7 +36,7 @@ class OctParams(C.Structure):
 
 class OctSearchConfig(C.Structure):
     _fields_ = [("packet", C.c_int32), ("fp32_filter", C.c_int32), ("radius_lanes", C.c_int32),
-                ("knn_packet", C.c_int32)]
+                ("knn_packet", C.c_int32), ("knn_bucket", C.c_int32), ("reserved", C.c_int32 * 3)]
 
 
 class OctTreeInfo(C.Structure):

@@ -288,6 +288,7 @@ int oct_set_search_config(oct_cloud h, const oct_search_config* cfg) {
     c.fp32_filter = cfg->fp32_filter;
     c.radius_group = (cfg->radius_lanes == 16 || cfg->radius_lanes == 32) ? cfg->radius_lanes : 8;
     c.knn_packet = cfg->knn_packet ? 1 : 0;
+    c.knn_bucket = cfg->knn_bucket > 0 ? (uint32_t)cfg->knn_bucket : 0u;
     return OCT_OK;
 }
 

@@ -107,6 +107,7 @@ struct Cloud {
     int packet = 1;
     int fp32_filter = 0;
     int knn_packet = 0;
+    uint32_t knn_bucket = 256;
 
     // pinned host staging for small readbacks
     void* pinned = nullptr;

@@ -43,6 +43,7 @@ struct KnnArgs {
     uint32_t* counts;
     uint32_t* err;
     const uint32_t* order;  // query visiting order (curve order), or nullptr
+    uint32_t bucket;        // subtrees with at most this many points are scanned as one range
 };
 
 __device__ __forceinline__ bool pair_less(double da, uint32_t ia, double db, uint32_t ib) {
@@ -234,9 +235,9 @@ cudaError_t launch_l(const KnnArgs& a, int grid, cudaStream_t s) {
 // ---------------------------------------------------------------------------
 // Register kNN for k <= 64: one warp per query, the k best (distance, index)
 // pairs held in registers as a sorted list (R = 1 or 2 entries per lane,
-// element j = r * 32 + lane).  A candidate that beats the k-th pair is placed
-// by one ballot per register (its rank) and a shuffle shift - no shared-memory
-// sort.  Children are judged with their ranges and first-child links loaded at
+// element j = r * 32 + lane).  Leaf points that beat the k-th pair collect in a
+// 32-entry shared buffer; a full buffer is merged into the list by a register
+// bitonic sort + merge (xor shuffles, no shared-memory sort).  Children are judged with their ranges and first-child links loaded at
 // expansion time, so empty leaves are never pushed and a popped entry needs no
 // further dependent loads before its points are read.
 // ---------------------------------------------------------------------------
@@ -246,51 +247,6 @@ struct RegList {
     double d[R];
     uint32_t i[R];
 };
-
-template <int R>
-__device__ __forceinline__ void reglist_insert(RegList<R>& L, double cd, uint32_t ci, uint32_t K, uint32_t& nl) {
-    const int lane = threadIdx.x & 31;
-    int pos = 0;
-#pragma unroll
-    for (int r = 0; r < R; ++r) pos += __popc(__ballot_sync(0xffffffffu, pair_less(L.d[r], L.i[r], cd, ci)));
-    if (pos >= (int)K) return;
-    double upd[R];
-    uint32_t upi[R];
-#pragma unroll
-    for (int r = 0; r < R; ++r) {
-        upd[r] = __shfl_up_sync(0xffffffffu, L.d[r], 1);
-        upi[r] = __shfl_up_sync(0xffffffffu, L.i[r], 1);
-    }
-    double carry_d[R];
-    uint32_t carry_i[R];
-#pragma unroll
-    for (int r = 0; r < R; ++r) {
-        carry_d[r] = __shfl_sync(0xffffffffu, L.d[r], 31);
-        carry_i[r] = __shfl_sync(0xffffffffu, L.i[r], 31);
-    }
-#pragma unroll
-    for (int r = R - 1; r >= 0; --r) {
-        const int j = r * 32 + lane;
-        double prev_d = upd[r];
-        uint32_t prev_i = upi[r];
-        if (lane == 0) {
-            prev_d = (r > 0) ? carry_d[r > 0 ? r - 1 : 0] : (double)INFINITY;
-            prev_i = (r > 0) ? carry_i[r > 0 ? r - 1 : 0] : 0xffffffffu;
-        }
-        if (j == pos) {
-            L.d[r] = cd;
-            L.i[r] = ci;
-        } else if (j > pos) {
-            L.d[r] = prev_d;
-            L.i[r] = prev_i;
-        }
-        if (j >= (int)K) {
-            L.d[r] = INFINITY;
-            L.i[r] = 0xffffffffu;
-        }
-    }
-    if (nl < K) ++nl;
-}
 
 template <int R>
 __device__ __forceinline__ void reglist_kth(const RegList<R>& L, uint32_t K, double& td, uint32_t& ti) {
@@ -307,6 +263,75 @@ __device__ __forceinline__ void reglist_kth(const RegList<R>& L, uint32_t K, dou
     ti = __shfl_sync(0xffffffffu, i, src);
 }
 
+// Compare-exchange with the lane `lane ^ j`: keep the smaller pair when
+// `keep_min`, else the larger.
+__device__ __forceinline__ void cx_xor(double& d, uint32_t& i, int j, bool keep_min) {
+    const double pd = __shfl_xor_sync(0xffffffffu, d, j);
+    const uint32_t pi = __shfl_xor_sync(0xffffffffu, i, j);
+    const bool partner_less = pair_less(pd, pi, d, i);
+    if (partner_less == keep_min) {
+        d = pd;
+        i = pi;
+    }
+}
+
+// Ascending bitonic sort of one pair per lane (32 pairs).
+__device__ __forceinline__ void warp_sort32(double& d, uint32_t& i) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int k = 2; k <= 32; k <<= 1)
+#pragma unroll
+        for (int j = k >> 1; j > 0; j >>= 1) cx_xor(d, i, j, ((lane & j) == 0) == ((lane & k) == 0));
+}
+
+// Sort a bitonic sequence of 32 pairs (one per lane) ascending.
+__device__ __forceinline__ void warp_bitonic_merge32(double& d, uint32_t& i) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int j = 16; j > 0; j >>= 1) cx_xor(d, i, j, (lane & j) == 0);
+}
+
+// Merge 32 unsorted candidate pairs (one per lane, +inf for none) into the
+// sorted register list, keeping the smallest 32 * R pairs.  For R = 2: the 32
+// smallest of (upper half, candidates) are min(upper[l], sorted_cand[31 - l]),
+// and the 64 smallest of everything are the lower half merged with those.
+template <int R>
+__device__ __forceinline__ void reglist_merge32(RegList<R>& L, double cd, uint32_t ci) {
+    const int lane = threadIdx.x & 31;
+    warp_sort32(cd, ci);
+    const double rd = __shfl_sync(0xffffffffu, cd, 31 - lane);
+    const uint32_t ri = __shfl_sync(0xffffffffu, ci, 31 - lane);
+    double md = L.d[R - 1];
+    uint32_t mi = L.i[R - 1];
+    if (pair_less(rd, ri, md, mi)) {
+        md = rd;
+        mi = ri;
+    }
+    warp_bitonic_merge32(md, mi);
+    if constexpr (R == 1) {
+        L.d[0] = md;
+        L.i[0] = mi;
+    } else {
+        // lower half L0 (ascending) against reversed M: min goes low, max goes high
+        const double xd = __shfl_sync(0xffffffffu, md, 31 - lane);
+        const uint32_t xi = __shfl_sync(0xffffffffu, mi, 31 - lane);
+        double lo_d = L.d[0], hi_d = xd;
+        uint32_t lo_i = L.i[0], hi_i = xi;
+        if (pair_less(xd, xi, lo_d, lo_i)) {
+            hi_d = lo_d;
+            hi_i = lo_i;
+            lo_d = xd;
+            lo_i = xi;
+        }
+        warp_bitonic_merge32(lo_d, lo_i);
+        warp_bitonic_merge32(hi_d, hi_i);
+        L.d[0] = lo_d;
+        L.i[0] = lo_i;
+        L.d[1] = hi_d;
+        L.i[1] = hi_i;
+    }
+}
+
 template <int R>
 __global__ void __launch_bounds__(kKnnThreads) k_knn_reg(KnnArgs a) {
     __shared__ uint32_t st_a[kKnnWarps][kKnnStack];   // leaf: first point; internal: first child
@@ -314,6 +339,8 @@ __global__ void __launch_bounds__(kKnnThreads) k_knn_reg(KnnArgs a) {
     __shared__ double st_lb[kKnnWarps][kKnnStack];
     __shared__ uint8_t st_depth[kKnnWarps][kKnnStack];
     __shared__ double s_radii[kMaxDepth + 1][3];
+    __shared__ double s_bd[kKnnWarps][32];
+    __shared__ uint32_t s_bi[kKnnWarps][32];
     for (int i = threadIdx.x; i < (kMaxDepth + 1) * 3; i += kKnnThreads)
         (&s_radii[0][0])[i] = (&a.geom->radii[0][0])[i];
     __syncthreads();
@@ -337,13 +364,26 @@ __global__ void __launch_bounds__(kKnnThreads) k_knn_reg(KnnArgs a) {
         double thr = INFINITY;
         uint32_t thr_i = 0xffffffffu;
         bool failed = false;
+        uint32_t nb = 0;  // candidates waiting in the shared buffer
+        double* bd = s_bd[warp];
+        uint32_t* bi = s_bi[warp];
+        auto merge_buf = [&]() {
+            const double cdv = (lane < (int)nb) ? bd[lane] : (double)INFINITY;
+            const uint32_t civ = (lane < (int)nb) ? bi[lane] : 0xffffffffu;
+            __syncwarp();
+            reglist_merge32<R>(L, cdv, civ);
+            nl = (nl + nb < K) ? nl + nb : K;
+            nb = 0;
+            if (nl == K) reglist_kth<R>(L, K, thr, thr_i);
+        };
         // root (bound 0, linear_octree.hpp:904)
         {
             const uint32_t fc0 = a.offsets[0];
             const uint2 rg0 = a.ranges[0];
+            const bool scan0 = fc0 == 0 || rg0.y - rg0.x <= a.bucket;
             if (lane == 0) {
-                sa[0] = fc0 ? fc0 : rg0.x;
-                sb[0] = fc0 ? 0xffffffffu : rg0.y;
+                sa[0] = scan0 ? rg0.x : fc0;
+                sb[0] = scan0 ? rg0.y : 0xffffffffu;
                 sl[0] = 0.0;
                 sd[0] = 0;
             }
@@ -368,16 +408,18 @@ __global__ void __launch_bounds__(kKnnThreads) k_knn_reg(KnnArgs a) {
                         cand = pair_less(d, i, thr, thr_i);
                     }
                     uint32_t m = __ballot_sync(0xffffffffu, cand);
-                    while (m) {
-                        const int src = __ffs(m) - 1;
-                        m &= m - 1;
-                        const double cd = __shfl_sync(0xffffffffu, d, src);
-                        const uint32_t ci = b + (uint32_t)src;
-                        if (pair_less(cd, ci, thr, thr_i)) {
-                            reglist_insert<R>(L, cd, ci, K, nl);
-                            if (nl == K) reglist_kth<R>(L, K, thr, thr_i);
-                        }
+                    if (nb + __popc(m) > 32) {
+                        merge_buf();
+                        cand = cand && pair_less(d, i, thr, thr_i);
+                        m = __ballot_sync(0xffffffffu, cand);
                     }
+                    if (cand) {
+                        const uint32_t slot = nb + __popc(m & lanemask_lt());
+                        bd[slot] = d;
+                        bi[slot] = i;
+                    }
+                    nb += __popc(m);
+                    __syncwarp();
                 }
                 continue;
             }
@@ -391,12 +433,14 @@ __global__ void __launch_bounds__(kKnnThreads) k_knn_reg(KnnArgs a) {
                 const uint32_t child = fc + lane;
                 clb = dist_po(p, a.centers + 3ull * child, s_radii[cd]);
                 const uint32_t cfc = a.offsets[child];
-                if (cfc) {
+                const uint2 rg = a.ranges[child];
+                if (cfc && rg.y - rg.x > a.bucket) {
                     ca = cfc;
                     cb = 0xffffffffu;
                     keep = !(clb > thr);
                 } else {
-                    const uint2 rg = a.ranges[child];
+                    // a leaf, or a small subtree scanned as one range: extra points can only be
+                    // rejected by the k-th pair, so the k best pairs are unchanged
                     ca = rg.x;
                     cb = rg.y;
                     keep = (rg.y > rg.x) && !(clb > thr);  // an empty leaf holds no candidate
@@ -426,6 +470,7 @@ __global__ void __launch_bounds__(kKnnThreads) k_knn_reg(KnnArgs a) {
             sp += nk;
         }
         if (failed) set_err(a.err, kErrStackOverflow);
+        if (nb) merge_buf();
         const uint64_t o = q * (uint64_t)K;
 #pragma unroll
         for (int r = 0; r < R; ++r) {
@@ -693,6 +738,7 @@ cudaError_t launch_knn(Cloud& c, const double* d_centers, uint64_t nq, uint32_t 
     a.d2 = d_d2;
     a.counts = d_counts;
     a.err = c.d_err.as<uint32_t>();
+    a.bucket = c.knn_bucket;
     a.order = nullptr;
     if (c.packet) {  // curve-ordered queries: neighbouring warps share octants in cache
         cudaError_t e;

@@ -46,7 +46,7 @@ class LinearOctree:
 
     def __init__(self, points, encoder="hilbert", max_points_leaf: int = 128, device: int = 0,
                  radius_group: int = 8, stream=None, packet: bool = True, fp32_filter: bool = False,
-                 knn_packet: bool = False):
+                 knn_packet: bool = False, knn_bucket: int = 256):
         L = lib()
         self._L = L
         self.encoder = ENCODERS[encoder]
@@ -59,7 +59,7 @@ class LinearOctree:
         if stream is not None:
             check(L.oct_cloud_set_stream(h, C.c_void_p(stream)), h, "oct_cloud_set_stream")
         self.set_search_config(packet=packet, fp32_filter=fp32_filter, radius_lanes=radius_group,
-                               knn_packet=knn_packet)
+                               knn_packet=knn_packet, knn_bucket=knn_bucket)
         dev = _is_device(points)
         if not dev:
             points = _host_f64(points, 3)
@@ -94,10 +94,11 @@ class LinearOctree:
         check(self._L.oct_set_radius_group(self._h, int(lanes)), self._h)
 
     def set_search_config(self, packet: bool = True, fp32_filter: bool = False, radius_lanes: int = 8,
-                          knn_packet: bool = False):
+                          knn_packet: bool = False, knn_bucket: int = 256):
         """Search path: packet (32 curve-ordered queries per warp) or one query per
         ``radius_lanes`` lanes; FP32 leaf-relative filter with FP64 re-tests; kNN packets."""
-        cfg = OctSearchConfig(int(bool(packet)), int(bool(fp32_filter)), int(radius_lanes), int(bool(knn_packet)))
+        cfg = OctSearchConfig(int(bool(packet)), int(bool(fp32_filter)), int(radius_lanes), int(bool(knn_packet)),
+                              int(knn_bucket))
         check(self._L.oct_set_search_config(self._h, C.byref(cfg)), self._h, "oct_set_search_config")
 
     def search_stats(self, reset: bool = False):

@@ -19,15 +19,16 @@ CLOUDS = sorted(p for p in glob.glob(os.path.join(GOLDEN, "*.npz")) if not p.end
 KERNELS = {"sphere": 1, "circle": 0, "cube": 3, "square": 2}
 ALGO_NAMES = {1: "neighbors", 2: "neighborsPrune", 3: "neighborsStruct"}
 # search paths: (packet, fp32_filter, lanes per query of the non-packet path)
-PATHS = {"lanes8": (False, False, 8, False), "lanes16": (False, False, 16, False),
-         "lanes32": (False, False, 32, False), "packet": (True, False, 8, False),
-         "packet_fp32": (True, True, 8, False), "knn_packet": (True, False, 8, True)}
+PATHS = {"lanes8": (False, False, 8, False, 256), "lanes16": (False, False, 16, False, 256),
+         "lanes32": (False, False, 32, False, 256), "packet": (True, False, 8, False, 256),
+         "packet_fp32": (True, True, 8, False, 256), "knn_packet": (True, False, 8, True, 256),
+         "knn_leaves": (True, False, 8, False, 0), "knn_bucket2k": (True, False, 8, False, 2048)}
 
 
 def octree(xyz, enc, leaf, path):
-    packet, fp32, lanes, knn_packet = PATHS[path]
+    packet, fp32, lanes, knn_packet, bucket = PATHS[path]
     return LinearOctree(xyz, encoder=enc, max_points_leaf=leaf, radius_group=lanes, packet=packet, fp32_filter=fp32,
-                        knn_packet=knn_packet)
+                        knn_packet=knn_packet, knn_bucket=bucket)
 
 
 def load(path):
@@ -108,7 +109,7 @@ def test_gpu_build_matches_oracle(synth_cases, case):
 
 
 @pytest.mark.parametrize("case", range(len(SYNTH)))
-@pytest.mark.parametrize("search", [p for p in PATHS if p != "knn_packet"])
+@pytest.mark.parametrize("search", [p for p in PATHS if not p.startswith("knn")])
 def test_gpu_radius_matches_oracle(synth_cases, case, search):
     xyz, enc, leaf, keys, perm, box, sxyz, t = synth_cases[case]
     oc = octree(xyz, enc, leaf, search)
@@ -145,7 +146,7 @@ def test_gpu_radius_matches_oracle(synth_cases, case, search):
 
 
 @pytest.mark.parametrize("case", range(len(SYNTH)))
-@pytest.mark.parametrize("search", ["lanes8", "packet", "knn_packet"])
+@pytest.mark.parametrize("search", ["lanes8", "packet", "knn_packet", "knn_leaves", "knn_bucket2k"])
 def test_gpu_knn_matches_oracle(synth_cases, case, search):
     xyz, enc, leaf, keys, perm, box, sxyz, t = synth_cases[case]
     oc = octree(xyz, enc, leaf, search)
