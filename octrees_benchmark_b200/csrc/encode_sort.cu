@@ -63,12 +63,32 @@ __global__ void __launch_bounds__(kBboxThreads) k_bbox(const double* __restrict_
     double mn[3] = {DBL_MAX, DBL_MAX, DBL_MAX};
     double mx[3] = {-DBL_MAX, -DBL_MAX, -DBL_MAX};
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+    // two points per thread and step: three aligned 16-byte loads (x0 y0 | z0 x1 | y1 z1);
+    // a buffer that is not 16-byte aligned takes the scalar loop
+    const bool vec = (reinterpret_cast<uintptr_t>(xyz) & 15u) == 0;
+    const uint64_t npairs = vec ? n / 2 : 0;
+    const double2* xyz2 = reinterpret_cast<const double2*>(xyz);
+    for (uint64_t i = vec ? n : (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
-            const double v = xyz[3 * i + a];
-            mn[a] = smin(mn[a], v);  // std::min(localMin, p)
-            mx[a] = smax(mx[a], v);  // std::max(localMax, p)
+            mn[a] = smin(mn[a], xyz[3 * i + a]);
+            mx[a] = smax(mx[a], xyz[3 * i + a]);
+        }
+    }
+    for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < npairs; t += stride) {
+        const double2 a = xyz2[3 * t], b = xyz2[3 * t + 1], c = xyz2[3 * t + 2];
+        const double v[6] = {a.x, a.y, b.x, b.y, c.x, c.y};
+#pragma unroll
+        for (int e = 0; e < 6; ++e) {
+            mn[e % 3] = smin(mn[e % 3], v[e]);  // std::min(localMin, p)
+            mx[e % 3] = smax(mx[e % 3], v[e]);  // std::max(localMax, p)
+        }
+    }
+    if (vec && (n & 1) && blockIdx.x == 0 && threadIdx.x == 0) {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            mn[a] = smin(mn[a], xyz[3 * (n - 1) + a]);
+            mx[a] = smax(mx[a], xyz[3 * (n - 1) + a]);
         }
     }
 #pragma unroll
@@ -128,21 +148,40 @@ __global__ void __launch_bounds__(kEncThreads) k_encode(const double* __restrict
                                                         const BoxGeom* __restrict__ bg, uint64_t* __restrict__ keys,
                                                         SortCtl* ctl) {
     __shared__ uint32_t hist[8 * 256];
+    __shared__ uint8_t htbl[kHilbertStates * 8];
     for (int j = threadIdx.x; j < 8 * 256; j += blockDim.x) hist[j] = 0;
+    for (int j = threadIdx.x; j < kHilbertStates * 8; j += blockDim.x) htbl[j] = kHilbertTable[j];
     const double c0 = bg->box.center[0], c1 = bg->box.center[1], c2 = bg->box.center[2];
     const double r0 = bg->box.radii[0], r1 = bg->box.radii[1], r2 = bg->box.radii[2];
+    const double i0 = __drcp_rn(dmul(2.0, r0)), i1 = __drcp_rn(dmul(2.0, r1)), i2 = __drcp_rn(dmul(2.0, r2));
     __syncthreads();
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-        const double px = xyz[3 * i], py = xyz[3 * i + 1], pz = xyz[3 * i + 2];
-        const uint32_t ax = anchor_coord(px, c0, r0);
-        const uint32_t ay = anchor_coord(py, c1, r1);
-        const uint32_t az = anchor_coord(pz, c2, r2);
-        const uint64_t k = sfc_encode<ENC>(ax, ay, az);
-        keys[i] = k;
+    auto key_of = [&](double px, double py, double pz) {
+        const uint32_t ax = anchor_coord_fast(px, c0, r0, i0);
+        const uint32_t ay = anchor_coord_fast(py, c1, r1, i1);
+        const uint32_t az = anchor_coord_fast(pz, c2, r2, i2);
+        const uint64_t k = (ENC == 5) ? hilbert_encode_tbl(ax, ay, az, htbl) : morton_encode(ax, ay, az);
 #pragma unroll
         for (int p = 0; p < 8; ++p) atomicAdd(&hist[p * 256 + (uint32_t)((k >> (8 * p)) & 255u)], 1u);
+        return k;
+    };
+    // two points per thread and step: three aligned 16-byte loads, one 16-byte store;
+    // buffers that are not 16-byte aligned take the scalar loop
+    const bool vec = ((reinterpret_cast<uintptr_t>(xyz) | reinterpret_cast<uintptr_t>(keys)) & 15u) == 0;
+    const uint64_t npairs = vec ? n / 2 : 0;
+    for (uint64_t i = vec ? n : (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+        keys[i] = key_of(xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]);
+    const double2* xyz2 = reinterpret_cast<const double2*>(xyz);
+    ulonglong2* keys2 = reinterpret_cast<ulonglong2*>(keys);
+    for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < npairs; t += stride) {
+        const double2 a = xyz2[3 * t], b = xyz2[3 * t + 1], c = xyz2[3 * t + 2];
+        ulonglong2 kk;
+        kk.x = key_of(a.x, a.y, b.x);
+        kk.y = key_of(b.y, c.x, c.y);
+        keys2[t] = kk;
     }
+    if (vec && (n & 1) && blockIdx.x == 0 && threadIdx.x == 0)
+        keys[n - 1] = key_of(xyz[3 * (n - 1)], xyz[3 * (n - 1) + 1], xyz[3 * (n - 1) + 2]);
     __syncthreads();
     for (int j = threadIdx.x; j < 8 * 256; j += blockDim.x) {
         const uint32_t v = hist[j];
@@ -348,7 +387,7 @@ cudaError_t launch_bbox_encode(Cloud& c, const double* d_xyz) {
     k_bbox<<<grid_bbox, kBboxThreads, 0, c.stream>>>(d_xyz, n, c.parts.as<double>(), &ctl->bbox_ctr,
                                                      c.d_box.as<BoxGeom>());
     if (n) {
-        const uint64_t want = (n + kEncThreads - 1) / kEncThreads;
+        const uint64_t want = (n / 2 + kEncThreads) / kEncThreads;
         const int grid = (int)(want < (uint64_t)sms * kEncGridPerSM ? want : (uint64_t)sms * kEncGridPerSM);
         if (c.params.encoder == OCT_ENC_HILBERT_3D)
             k_encode<5><<<grid, kEncThreads, 0, c.stream>>>(d_xyz, n, c.d_box.as<BoxGeom>(), c.keys.as<uint64_t>(),

@@ -110,6 +110,71 @@ __device__ __forceinline__ void hilbert_decode(uint64_t code, uint32_t& ox, uint
     ox = x; oy = y; oz = z;
 }
 
+// The same Hilbert keys from a 24-state automaton (states: the axis
+// permutation and inversions the per-level transform has accumulated), as
+// generated by csrc/gen_hilbert_table.py: entry = next_state << 3 | digit,
+// indexed [state * 8 + octant of the ORIGINAL coordinates].  Kernels copy it
+// to shared memory and pass it here.
+constexpr int kHilbertStates = 24;
+__device__ const uint8_t kHilbertTable[kHilbertStates * 8] = {
+    160,  97,  11,  98, 183, 118,  12, 117,
+    122,   3, 121, 184, 109,   4, 110, 175,
+    126, 167, 125,  28, 105, 176, 106,  27,
+     20, 101, 191, 102,  19, 114, 168, 113,
+     96,  43, 161, 162, 119,  44, 182, 181,
+    186, 185,  35, 120, 173, 174,  36, 111,
+    190, 189, 103,  60, 169, 170, 112,  59,
+     52, 127, 165, 166,  51, 104, 178, 177,
+    128,  33, 151,  54,  75,  34,  76,  53,
+     58,  67,  45,  68,  57, 152,  46, 143,
+     62, 135,  41, 144,  61,  92,  42,  91,
+     84,  37,  83,  50, 159,  38, 136,  49,
+     32, 107,  55, 108, 129, 130, 150, 149,
+    154, 153, 141, 142,  99,  56, 100,  47,
+    158, 157, 137, 138,  39, 124,  48, 123,
+    116,  63, 115,  40, 133, 134, 146, 145,
+     64,  87,   1,  22, 139, 140,   2,  21,
+     26,  13, 131, 132,  25,  14,  88,  79,
+     30,   9,  71,  80,  29,  10, 156, 155,
+    148, 147,   5,  18,  95,  72,   6,  17,
+      0,  23, 171, 172,  65,  86,  66,  85,
+     90,  77,  89,  78, 163, 164,  24,  15,
+     94,  73,  93,  74,   7,  16, 188, 187,
+    180, 179,  31,   8,  69,  82,  70,  81
+};
+
+__device__ __forceinline__ uint64_t hilbert_encode_tbl(uint32_t x, uint32_t y, uint32_t z, const uint8_t* tbl) {
+    uint64_t key = 0;
+    uint32_t st = 0;
+#pragma unroll
+    for (int level = (int)kMaxDepth - 1; level >= 0; --level) {
+        const uint32_t o = (((x >> level) & 1u) << 2) | (((y >> level) & 1u) << 1) | ((z >> level) & 1u);
+        const uint32_t e = tbl[st * 8 + o];
+        key = (key << 3) | (e & 7u);
+        st = e >> 3;
+    }
+    return key;
+}
+
+// Anchor coordinate through a reciprocal: t' = x * RN(1 / 2r) differs from the
+// reference's t = RN(x / 2r) by at most 1.5 * 2^-52 |t|, so for |t| <= 1 the
+// scaled values differ by at most 2^-30.  When t' * 2^21 lies in [0, 2^21) and
+// more than 2^-20 away from an integer, both truncate to the same coordinate;
+// otherwise (boundaries, points outside the box, flat axes) the exact division
+// decides.
+__device__ __forceinline__ uint32_t anchor_coord_fast(double p, double c, double r, double inv2r) {
+    const double x = dadd(dsub(p, c), r);
+    const double v = dmul(dmul(x, inv2r), 2097152.0);
+    if (v >= 0.0 && v < 2097152.0) {
+        const double fl = floor(v);
+        const double fr = dsub(v, fl);
+        if (fr > 9.5367431640625e-07 && fr < 0.99999904632568359375) return (uint32_t)fl;
+    }
+    const double t = ddiv(x, dmul(2.0, r));
+    const uint64_t u = x86_cvt_u64(dmul(t, 2097152.0));
+    return (uint32_t)(u < kMaxCoord ? u : kMaxCoord);
+}
+
 template <int ENC>
 __device__ __forceinline__ uint64_t sfc_encode(uint32_t x, uint32_t y, uint32_t z) {
     if constexpr (ENC == 5) return hilbert_encode(x, y, z);

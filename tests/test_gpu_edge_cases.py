@@ -107,6 +107,19 @@ def test_degenerate_line_plane_and_offsets(port):
 
 
 @pytest.mark.parametrize("enc", [1, 5])
+def test_points_on_cell_boundaries(port, enc):
+    # box [0, 1024]^3: anchor coordinates x * 2048 land exactly on integers (the
+    # encoder's exact-division path) and a few ulps either side of them
+    rng = np.random.default_rng(11 + enc)
+    base = rng.integers(0, 1025, (3000, 3)).astype(np.float64)
+    base[0] = 0.0
+    base[1] = 1024.0
+    nudged = base[2:1500] + rng.choice([-1, 1], (1498, 3)) * np.spacing(base[2:1500]) * rng.integers(1, 4, (1498, 3))
+    pts = np.concatenate([base, np.clip(nudged, 0.0, 1024.0)])
+    full_check(port, pts, enc=enc, leaf=8, radii=(0.0, 1.0, 7.5), ks=(1, 9))
+
+
+@pytest.mark.parametrize("enc", [1, 5])
 def test_leaf_size_one_and_clusters(port, enc):
     rng = np.random.default_rng(enc)
     pts = np.concatenate([rng.normal(0, 1e-9, (200, 3)), rng.uniform(-5, 5, (300, 3)), np.zeros((50, 3))])

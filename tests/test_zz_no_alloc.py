@@ -74,6 +74,26 @@ def test_noalloc_matches_regular_entry_point_on_two_calls_in_a_row():
         assert same_f64(box.cpu().numpy(), rb)
 
 
+def test_noalloc_accepts_a_buffer_that_is_only_8_byte_aligned():
+    torch = pytest.importorskip("torch")
+    L = capi.lib()
+    xyz = lidar_tile(30_001, 60.0, seed=43)
+    flat = torch.zeros(3 * len(xyz) + 1, dtype=torch.float64, device="cuda")
+    flat[1:] = torch.from_numpy(xyz.reshape(-1)).cuda()
+    d_xyz = flat[1:]  # 8-byte offset from a 256-byte aligned allocation
+    n = len(xyz)
+    keys = torch.empty(n + 1, dtype=torch.int64, device="cuda")[1:]
+    perm = torch.empty(n, dtype=torch.int32, device="cuda")
+    box = torch.empty(12, dtype=torch.float64, device="cuda")
+    st = L.oct_encode_sort_noalloc(5, d_xyz.data_ptr(), n, keys.data_ptr(), perm.data_ptr(), box.data_ptr(), None)
+    assert st == capi.OCT_OK
+    torch.cuda.synchronize()
+    rk, rp, rb = regular_encode_sort(xyz, 5)
+    assert np.array_equal(keys.cpu().numpy().view(np.uint64), rk)
+    assert np.array_equal(perm.cpu().numpy().view(np.uint32), rp)
+    assert same_f64(box.cpu().numpy(), rb)
+
+
 def test_noalloc_rejects_clouds_above_the_limit():
     torch = pytest.importorskip("torch")
     L = capi.lib()
