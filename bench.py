@@ -337,6 +337,7 @@ def run_b200(args, rank, world, local_rank):
 
     # ---- e2e through the host-buffer ABI (pinned buffers, copies in the timed region) ----
     e2e_val = None
+    e2e_detail = None
     h2d = d2h = 0
     if not args.no_e2e:
         qrh = torch.empty((Q_RADIUS, 3), dtype=torch.float64).pin_memory().numpy()
@@ -346,7 +347,7 @@ def run_b200(args, rank, world, local_rank):
         kidx_h = torch.empty((Q_KNN, KNN_K), dtype=torch.int32).pin_memory().numpy()
         kd2_h = torch.empty((Q_KNN, KNN_K), dtype=torch.float64).pin_memory().numpy()
         kcnt_h = torch.empty(Q_KNN, dtype=torch.int32).pin_memory().numpy()
-        et = []
+        et, er, ek = [], [], []
         for s in range(args.warmup + args.steps):
             qr, qk = batches[s]
             qrh[:] = qr.cpu().numpy()
@@ -355,17 +356,31 @@ def run_b200(args, rank, world, local_rank):
             t0 = time.perf_counter()
             capi.check(L.oct_radius_search(h, 1, 2, qrh.ctypes.data, Q_RADIUS, None, RADIUS, offs_h.ctypes.data,
                                            idx_h.ctypes.data, cap, C.byref(tot), 0), h, "e2e radius")
+            tm = time.perf_counter()
             capi.check(L.oct_knn(h, qkh.ctypes.data, Q_KNN, KNN_K, kidx_h.ctypes.data, kd2_h.ctypes.data,
                                  kcnt_h.ctypes.data, 0), h, "e2e knn")
             t1 = time.perf_counter()
             if s >= args.warmup:
                 et.append(t1 - t0)
+                er.append(tm - t0)
+                ek.append(t1 - tm)
                 h2d = 24 * (Q_RADIUS + Q_KNN)
                 d2h = 8 * (Q_RADIUS + 1) + 4 * int(tot.value) + Q_KNN * KNN_K * 12 + 4 * Q_KNN
-        e2e_t = torch.tensor([sum(et) / len(et)], dtype=torch.float64, device="cuda")
+        e2e_t = torch.tensor([statistics.median(et)], dtype=torch.float64, device="cuda")
         if world > 1:
             torch.distributed.all_reduce(e2e_t, op=torch.distributed.ReduceOp.MAX)
         e2e_val = world * (Q_RADIUS + Q_KNN) / float(e2e_t.item())
+        # the box's device-to-host bandwidth into pinned memory, for reading e2e
+        probe = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+        probe_h = torch.empty(256 << 20, dtype=torch.uint8).pin_memory()
+        probe_h.copy_(probe)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        probe_h.copy_(probe)
+        torch.cuda.synchronize()
+        d2h_gbs = (256 << 20) / (time.perf_counter() - t0) / 1e9
+        e2e_detail = {"radius_ms": 1e3 * statistics.median(er), "knn_ms": 1e3 * statistics.median(ek),
+                      "step_ms_all": [round(1e3 * v, 2) for v in et], "pinned_d2h_gbs": d2h_gbs}
 
     # ---- roofline of the dominant kernel of the chosen path ----
     peak, peak_kind = measured_peak()
@@ -408,7 +423,8 @@ def run_b200(args, rank, world, local_rank):
             "avg_neighbours": chosen["avg_neighbours"], "paths": paths,
             "batched_vs_plain": paths["packet"]["qps"] / paths["plain"]["qps"],
             "build": build, "roofline": roofline, "cpu_baseline": cpu,
-            "e2e": {"value": e2e_val, "unit": "queries/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h},
+            "e2e": {"value": e2e_val, "unit": "queries/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
+                    "detail": e2e_detail},
             "gpu_launches": LAUNCHES_PER_STEP[args.search] * args.steps, "clocks": clk,
         }
         print(json.dumps(line), flush=True)

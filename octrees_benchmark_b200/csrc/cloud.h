@@ -58,6 +58,33 @@ struct BuildCtl {
     uint32_t barrier_gen;
 };
 
+// Device pointers of one built cloud, as the search kernels read them.
+struct CloudView {
+    const double* xs;
+    const double* ys;
+    const double* zs;
+    const float4* rel;          // FP32 leaf-relative points (packet FP32 path), may be null
+    const uint32_t* offsets;
+    const uint2* ranges;
+    const double* centers;
+    const LevelGeom* geom;      // per-level radii
+};
+
+// One request of a search launch (device copy).  A launch covers a table of
+// requests; every query of the launch has a global position q in
+// [q_begin, q_end) of its request, and outputs are indexed by q.
+struct SearchReq {
+    CloudView cv;
+    const double* centers;      // the request's nq x 3 centres
+    const double* radii;        // per-query radii (radius requests) or null
+    double radius;              // radius when radii is null
+    uint64_t q_begin, q_end;    // global query positions of this request
+    uint64_t packet_begin;      // first packet (32 queries) of the request in the launch
+    uint64_t out_begin;         // kNN: first output slot (previous requests' nq * k)
+    uint32_t k;                 // kNN k
+    uint32_t cloud_id;          // distinct per cloud within the table (radii reload key)
+};
+
 struct Cloud {
     oct_params params{};
     int device = 0;
@@ -129,6 +156,18 @@ cudaError_t launch_radius_packet(Cloud& c, int kernel, int algo, bool fill, bool
                                  uint64_t nq, const double* d_radii, double radius, const uint32_t* d_order,
                                  unsigned long long* d_counts, unsigned long long* d_counts2,
                                  const unsigned long long* d_offsets, uint32_t* d_out, uint64_t out_capacity);
+// Packet radius search over a request table (device), nreq entries, `packets` packets in total.
+cudaError_t launch_radius_table(int device, cudaStream_t s, int kernel, int algo, bool fill, bool fp32,
+                                const SearchReq* d_reqs, uint32_t nreq, uint64_t packets, const uint32_t* d_order,
+                                unsigned long long* d_counts, unsigned long long* d_counts2,
+                                const unsigned long long* d_offsets, uint32_t* d_out, uint64_t out_capacity,
+                                uint32_t* d_packet_ctr, unsigned long long* d_stats, uint32_t* d_err,
+                                const SearchReq* single = nullptr);
+// Register kNN (k <= 64) over a request table: one warp per query, nq queries in total.
+cudaError_t launch_knn_table(int device, cudaStream_t s, const SearchReq* d_reqs, uint32_t nreq, uint64_t nq,
+                             uint32_t kmax, const uint32_t* d_order, uint32_t bucket, uint32_t* d_idx, double* d_d2,
+                             uint32_t* d_counts, uint32_t* d_err, const SearchReq* single = nullptr);
+CloudView cloud_view(const Cloud& c);
 cudaError_t launch_knn(Cloud& c, const double* d_centers, uint64_t nq, uint32_t k, uint32_t* d_idx, double* d_d2,
                        uint32_t* d_counts);
 

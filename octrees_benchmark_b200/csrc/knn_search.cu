@@ -332,28 +332,60 @@ __device__ __forceinline__ void reglist_merge32(RegList<R>& L, double cd, uint32
     }
 }
 
-template <int R>
-__global__ void __launch_bounds__(kKnnThreads) k_knn_reg(KnnArgs a) {
+struct KnnTableArgs {
+    SearchReq single;        // the request of a single-cloud search (reqs == null)
+    const SearchReq* reqs;   // request table of a multi-request launch (q_begin ascending)
+    uint32_t nreq;
+    uint64_t nq;             // queries of the whole launch
+    const uint32_t* order;   // visiting order (global query positions), or null
+    uint32_t bucket;
+    uint32_t* idx;
+    double* d2;
+    uint32_t* counts;
+    uint32_t* err;
+};
+
+#define KRQ(f) (MULTI ? a.reqs[ri].f : a.single.f)
+template <int R, bool MULTI>
+__global__ void __launch_bounds__(kKnnThreads) k_knn_reg(KnnTableArgs a) {
     __shared__ uint32_t st_a[kKnnWarps][kKnnStack];   // leaf: first point; internal: first child
     __shared__ uint32_t st_b[kKnnWarps][kKnnStack];   // leaf: end point; internal: 0xffffffff
     __shared__ double st_lb[kKnnWarps][kKnnStack];
     __shared__ uint8_t st_depth[kKnnWarps][kKnnStack];
-    __shared__ double s_radii[kMaxDepth + 1][3];
+    __shared__ double s_rad[kKnnWarps][kMaxDepth + 1][3];
     __shared__ double s_bd[kKnnWarps][32];
     __shared__ uint32_t s_bi[kKnnWarps][32];
-    for (int i = threadIdx.x; i < (kMaxDepth + 1) * 3; i += kKnnThreads)
-        (&s_radii[0][0])[i] = (&a.geom->radii[0][0])[i];
-    __syncthreads();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    double (*s_radii)[3] = s_rad[warp];
+    uint32_t cur_cloud = 0xffffffffu;
     uint32_t* sa = st_a[warp];
     uint32_t* sb = st_b[warp];
     double* sl = st_lb[warp];
     uint8_t* sd = st_depth[warp];
-    const uint32_t K = a.k;
     const uint64_t nwarps = (uint64_t)gridDim.x * kKnnWarps;
     for (uint64_t qpos = (uint64_t)blockIdx.x * kKnnWarps + warp; qpos < a.nq; qpos += nwarps) {
-        const uint64_t q = a.order ? a.order[qpos] : qpos;
-        const double p[3] = {a.q[3 * q], a.q[3 * q + 1], a.q[3 * q + 2]};
+        uint32_t ri = 0;
+        if (MULTI) {  // the request whose positions contain qpos (q_begin ascending)
+            uint32_t lo = 0, hi = a.nreq;
+            while (hi - lo > 1) {
+                const uint32_t mid = (lo + hi) >> 1;
+                if (a.reqs[mid].q_begin <= qpos) lo = mid;
+                else hi = mid;
+            }
+            ri = lo;
+        }
+        if (KRQ(cloud_id) != cur_cloud) {
+            __syncwarp();
+            const double* gr = &KRQ(cv.geom)->radii[0][0];
+            for (int t = lane; t < (kMaxDepth + 1) * 3; t += 32) (&s_radii[0][0])[t] = gr[t];
+            cur_cloud = KRQ(cloud_id);
+            __syncwarp();
+        }
+        const uint32_t K = KRQ(k);
+        const uint64_t q = a.order ? a.order[qpos] : qpos;  // global query position
+        const uint64_t ql = q - KRQ(q_begin);
+        const double* qc = KRQ(centers);
+        const double p[3] = {qc[3 * ql], qc[3 * ql + 1], qc[3 * ql + 2]};
         RegList<R> L;
 #pragma unroll
         for (int r = 0; r < R; ++r) {
@@ -378,8 +410,8 @@ __global__ void __launch_bounds__(kKnnThreads) k_knn_reg(KnnArgs a) {
         };
         // root (bound 0, linear_octree.hpp:904)
         {
-            const uint32_t fc0 = a.offsets[0];
-            const uint2 rg0 = a.ranges[0];
+            const uint32_t fc0 = KRQ(cv.offsets)[0];
+            const uint2 rg0 = KRQ(cv.ranges)[0];
             const bool scan0 = fc0 == 0 || rg0.y - rg0.x <= a.bucket;
             if (lane == 0) {
                 sa[0] = scan0 ? rg0.x : fc0;
@@ -404,7 +436,7 @@ __global__ void __launch_bounds__(kKnnThreads) k_knn_reg(KnnArgs a) {
                     double d = INFINITY;
                     bool cand = false;
                     if (i < eb) {
-                        d = dist_pp(p[0], p[1], p[2], a.xs[i], a.ys[i], a.zs[i]);
+                        d = dist_pp(p[0], p[1], p[2], KRQ(cv.xs)[i], KRQ(cv.ys)[i], KRQ(cv.zs)[i]);
                         cand = pair_less(d, i, thr, thr_i);
                     }
                     uint32_t m = __ballot_sync(0xffffffffu, cand);
@@ -431,9 +463,9 @@ __global__ void __launch_bounds__(kKnnThreads) k_knn_reg(KnnArgs a) {
             uint32_t ca = 0, cb = 0;
             if (lane < 8) {
                 const uint32_t child = fc + lane;
-                clb = dist_po(p, a.centers + 3ull * child, s_radii[cd]);
-                const uint32_t cfc = a.offsets[child];
-                const uint2 rg = a.ranges[child];
+                clb = dist_po(p, KRQ(cv.centers) + 3ull * child, s_radii[cd]);
+                const uint32_t cfc = KRQ(cv.offsets)[child];
+                const uint2 rg = KRQ(cv.ranges)[child];
                 if (cfc && rg.y - rg.x > a.bucket) {
                     ca = cfc;
                     cb = 0xffffffffu;
@@ -471,7 +503,7 @@ __global__ void __launch_bounds__(kKnnThreads) k_knn_reg(KnnArgs a) {
         }
         if (failed) set_err(a.err, kErrStackOverflow);
         if (nb) merge_buf();
-        const uint64_t o = q * (uint64_t)K;
+        const uint64_t o = KRQ(out_begin) + ql * (uint64_t)K;
 #pragma unroll
         for (int r = 0; r < R; ++r) {
             const uint32_t j = (uint32_t)(r * 32 + lane);
@@ -720,6 +752,34 @@ int sm_count_k(int device) {
 
 }  // namespace
 
+cudaError_t launch_knn_table(int device, cudaStream_t s, const SearchReq* d_reqs, uint32_t nreq, uint64_t nq,
+                             uint32_t kmax, const uint32_t* d_order, uint32_t bucket, uint32_t* d_idx, double* d_d2,
+                             uint32_t* d_counts, uint32_t* d_err, const SearchReq* single) {
+    if (nq == 0 || nreq == 0) return cudaSuccess;
+    KnnTableArgs a;
+    a.single = single ? *single : SearchReq{};
+    a.reqs = single ? nullptr : d_reqs;
+    a.nreq = nreq;
+    a.nq = nq;
+    a.order = d_order;
+    a.bucket = bucket;
+    a.idx = d_idx;
+    a.d2 = d_d2;
+    a.counts = d_counts;
+    a.err = d_err;
+    const uint64_t want = (nq + kKnnWarps - 1) / kKnnWarps;
+    const uint64_t cap = (uint64_t)sm_count_k(device) * 16;
+    const int grid = (int)(want < cap ? want : cap);
+    if (a.reqs) {
+        if (kmax <= 32) k_knn_reg<1, true><<<grid, kKnnThreads, 0, s>>>(a);
+        else k_knn_reg<2, true><<<grid, kKnnThreads, 0, s>>>(a);
+    } else {
+        if (kmax <= 32) k_knn_reg<1, false><<<grid, kKnnThreads, 0, s>>>(a);
+        else k_knn_reg<2, false><<<grid, kKnnThreads, 0, s>>>(a);
+    }
+    return cudaGetLastError();
+}
+
 cudaError_t launch_knn(Cloud& c, const double* d_centers, uint64_t nq, uint32_t k, uint32_t* d_idx, double* d_d2,
                        uint32_t* d_counts) {
     if (nq == 0 || k == 0) return cudaSuccess;
@@ -759,13 +819,15 @@ cudaError_t launch_knn(Cloud& c, const double* d_centers, uint64_t nq, uint32_t 
     const uint64_t want = (nq + kKnnWarps - 1) / kKnnWarps;
     const uint64_t cap = (uint64_t)sm_count_k(c.device) * 16;
     const int grid = (int)(want < cap ? want : cap);
-    if (c.packet && k <= 32) {
-        k_knn_reg<1><<<grid, kKnnThreads, 0, c.stream>>>(a);
-        return cudaGetLastError();
-    }
     if (c.packet && k <= 64) {
-        k_knn_reg<2><<<grid, kKnnThreads, 0, c.stream>>>(a);
-        return cudaGetLastError();
+        SearchReq r{};
+        r.cv = cloud_view(c);
+        r.centers = d_centers;
+        r.q_begin = 0;
+        r.q_end = nq;
+        r.k = k;
+        return launch_knn_table(c.device, c.stream, nullptr, 1, nq, k, a.order, c.knn_bucket, d_idx, d_d2, d_counts,
+                                c.d_err.as<uint32_t>(), &r);
     }
     if (k <= 32) return launch_l<32>(a, grid, c.stream);
     if (k <= 64) return launch_l<64>(a, grid, c.stream);

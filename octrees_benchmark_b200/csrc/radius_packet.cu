@@ -44,19 +44,11 @@ constexpr int kPkThreads = 32 * kPkWarps;
 constexpr int kPkStack = 8 * (kMaxDepth + 1);
 
 struct PacketArgs {
-    const double* xs;
-    const double* ys;
-    const double* zs;
-    const float4* rel;
-    const uint32_t* offsets;
-    const uint2* ranges;
-    const double* centers;
-    const LevelGeom* geom;
-    const double* q;
-    const double* qr;
-    double radius;
-    const uint32_t* order;
-    uint64_t nq;
+    SearchReq single;           // the request of a single-cloud search (reqs == null)
+    const SearchReq* reqs;      // request table of a multi-request launch
+    uint32_t nreq;
+    uint64_t packets;           // packets of the whole launch
+    const uint32_t* order;      // query visiting order (global positions), or null
     unsigned long long* counts;
     unsigned long long* counts2;
     const unsigned long long* offs;
@@ -128,7 +120,10 @@ __device__ __forceinline__ int f32_test(const LeafCtx& c, float4 p) {
     }
 }
 
-template <int KT, int ALGO, bool FILL, bool F32>
+// MULTI: the launch covers a request table; otherwise the single request is read
+// from the kernel parameters (constant-bank operands, no registers held).
+#define RQ(f) (MULTI ? a.reqs[cur_req].f : a.single.f)
+template <int KT, int ALGO, bool FILL, bool F32, bool MULTI>
 __global__ void __launch_bounds__(kPkThreads) k_radius_packet(PacketArgs a) {
     __shared__ uint32_t st_node[kPkWarps][kPkStack];
     __shared__ uint32_t st_fc[kPkWarps][kPkStack];     // first child, 0 for a leaf
@@ -136,14 +131,14 @@ __global__ void __launch_bounds__(kPkThreads) k_radius_packet(PacketArgs a) {
     __shared__ uint32_t st_over[kPkWarps][kPkStack];
     __shared__ uint32_t st_in[kPkWarps][kPkStack];
     __shared__ uint8_t st_depth[kPkWarps][kPkStack];
-    __shared__ double s_radii[kMaxDepth + 1][3];
+    __shared__ double s_rad[kPkWarps][kMaxDepth + 1][3];
     __shared__ double sx[kPkWarps][32], sy[kPkWarps][32], sz[kPkWarps][32];
     __shared__ float4 sp[kPkWarps][32];
 
-    for (int i = threadIdx.x; i < (kMaxDepth + 1) * 3; i += kPkThreads)
-        (&s_radii[0][0])[i] = (&a.geom->radii[0][0])[i];
-    __syncthreads();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    double (*s_radii)[3] = s_rad[warp];
+    uint32_t cur_cloud = 0xffffffffu;
+    uint32_t cur_req = 0;
     const uint32_t lbit = 1u << lane;
     uint32_t* sn = st_node[warp];
     uint32_t* sf = st_fc[warp];
@@ -157,13 +152,34 @@ __global__ void __launch_bounds__(kPkThreads) k_radius_packet(PacketArgs a) {
         uint32_t packet = 0;
         if (lane == 0) packet = atomicAdd(a.packet_ctr, 1u);
         packet = __shfl_sync(0xffffffffu, packet, 0);
-        const uint64_t i0 = (uint64_t)packet * 32;
-        if (i0 >= a.nq) break;
-        const uint64_t i = i0 + lane;
-        const bool valid = i < a.nq;
-        const uint32_t qi = valid ? (a.order ? a.order[i] : (uint32_t)i) : 0u;
+        if (packet >= a.packets) break;
+        // the request of this packet: packet_begin is ascending over the table
+        if (MULTI) {
+            uint32_t lo = 0, hi = a.nreq;
+            while (hi - lo > 1) {
+                const uint32_t mid = (lo + hi) >> 1;
+                if (a.reqs[mid].packet_begin <= packet) lo = mid;
+                else hi = mid;
+            }
+            cur_req = lo;
+        }
+        if (RQ(cloud_id) != cur_cloud) {  // this warp's level radii follow the packet's cloud
+            __syncwarp();
+            const double* gr = &RQ(cv.geom)->radii[0][0];
+            for (int t = lane; t < (kMaxDepth + 1) * 3; t += 32) (&s_radii[0][0])[t] = gr[t];
+            cur_cloud = RQ(cloud_id);
+            __syncwarp();
+        }
+        const uint64_t q_begin = RQ(q_begin);
+        const uint64_t i = q_begin + 32ull * (packet - RQ(packet_begin)) + lane;
+        const bool valid = i < RQ(q_end);
+        const uint64_t qg = valid ? (a.order ? (uint64_t)a.order[i] : i) : q_begin;  // global query position
+        const uint64_t ql = qg - q_begin;                                              // within the request
+        const uint32_t qi = (uint32_t)qg;
+        const double* qc = RQ(centers);
+        const double* qrad = RQ(radii);
         SearchKernel k;
-        k.init(a.q[3ull * qi], a.q[3ull * qi + 1], a.q[3ull * qi + 2], a.qr ? a.qr[qi] : a.radius);
+        k.init(qc[3 * ql], qc[3 * ql + 1], qc[3 * ql + 2], qrad ? qrad[ql] : RQ(radius));
         unsigned long long cnt = 0, cnt2 = 0, base = 0;
         if (FILL && valid) base = a.offs[qi];
         bool overflow = false;
@@ -217,16 +233,16 @@ __global__ void __launch_bounds__(kPkThreads) k_radius_packet(PacketArgs a) {
         auto scan_leaf = [&](uint32_t node, uint2 rg, uint32_t mask) {
             const bool mine = (mask & lbit) != 0;
             LeafCtx ctx;
-            if (F32 && mine) leaf_ctx<KT>(k, a.centers + 3ull * node, ctx);
+            if (F32 && mine) leaf_ctx<KT>(k, RQ(cv.centers) + 3ull * node, ctx);
             for (uint32_t b = rg.x; b < rg.y; b += 32) {
                 const uint32_t idx = b + lane;
                 if (idx < rg.y) {
                     if (F32) {
-                        sp[warp][lane] = a.rel[idx];
+                        sp[warp][lane] = RQ(cv.rel)[idx];
                     } else {
-                        sx[warp][lane] = a.xs[idx];
-                        sy[warp][lane] = a.ys[idx];
-                        sz[warp][lane] = a.zs[idx];
+                        sx[warp][lane] = RQ(cv.xs)[idx];
+                        sy[warp][lane] = RQ(cv.ys)[idx];
+                        sz[warp][lane] = RQ(cv.zs)[idx];
                     }
                 }
                 __syncwarp();
@@ -237,7 +253,7 @@ __global__ void __launch_bounds__(kPkThreads) k_radius_packet(PacketArgs a) {
                         if (F32) {
                             const int r = f32_test<KT>(ctx, sp[warp][t]);
                             if (r < 0) {
-                                in = is_inside<KT>(k, a.xs[b + t], a.ys[b + t], a.zs[b + t]);
+                                in = is_inside<KT>(k, RQ(cv.xs)[b + t], RQ(cv.ys)[b + t], RQ(cv.zs)[b + t]);
                                 ++n_retests;
                             } else {
                                 in = r > 0;
@@ -261,9 +277,9 @@ __global__ void __launch_bounds__(kPkThreads) k_radius_packet(PacketArgs a) {
         bool over = false, in = false;
         if (valid) {
             if constexpr (ALGO == kNeighbors) {
-                over = box_overlap<KT>(k, a.centers, s_radii[0]);
+                over = box_overlap<KT>(k, RQ(cv.centers), s_radii[0]);
             } else {
-                const int j = box_intersect<KT>(k, a.centers, s_radii[0]);
+                const int j = box_intersect<KT>(k, RQ(cv.centers), s_radii[0]);
                 in = (j == kInside);
                 over = (j == kOverlap);
             }
@@ -273,8 +289,8 @@ __global__ void __launch_bounds__(kPkThreads) k_radius_packet(PacketArgs a) {
             const uint32_t mo = __ballot_sync(0xffffffffu, over);
             const uint32_t mi = __ballot_sync(0xffffffffu, in);
             if (mo | mi) {
-                const uint32_t fc0 = a.offsets[0];
-                const uint2 rg0 = a.ranges[0];
+                const uint32_t fc0 = RQ(cv.offsets)[0];
+                const uint2 rg0 = RQ(cv.ranges)[0];
                 if (lane == 0) {
                     sn[0] = 0;
                     sf[0] = fc0;
@@ -308,14 +324,14 @@ __global__ void __launch_bounds__(kPkThreads) k_radius_packet(PacketArgs a) {
             uint32_t my_fc = 0, my_mo = 0, my_mi = 0;
             uint2 my_rg = make_uint2(0u, 0u);
             if (lane < 8) {
-                my_fc = a.offsets[fc + lane];
-                my_rg = a.ranges[fc + lane];
+                my_fc = RQ(cv.offsets)[fc + lane];
+                my_rg = RQ(cv.ranges)[fc + lane];
             }
 #pragma unroll
             for (int j = 0; j < 8; ++j) {
                 bool o = false, n = false;
                 if (mine) {
-                    const double* oc = a.centers + 3ull * (fc + j);
+                    const double* oc = RQ(cv.centers) + 3ull * (fc + j);
                     if constexpr (ALGO == kNeighbors) {
                         o = box_overlap<KT>(k, oc, s_radii[cd]);
                     } else {
@@ -403,16 +419,22 @@ int sm_count_p(int device) {
     return v;
 }
 
-template <int KT, int ALGO>
-cudaError_t launch_pk(const PacketArgs& a, bool fill, bool fp32, int grid, cudaStream_t s) {
+template <int KT, int ALGO, bool MULTI>
+cudaError_t launch_pk_m(const PacketArgs& a, bool fill, bool fp32, int grid, cudaStream_t s) {
     if (fill) {
-        if (fp32) k_radius_packet<KT, ALGO, true, true><<<grid, kPkThreads, 0, s>>>(a);
-        else k_radius_packet<KT, ALGO, true, false><<<grid, kPkThreads, 0, s>>>(a);
+        if (fp32) k_radius_packet<KT, ALGO, true, true, MULTI><<<grid, kPkThreads, 0, s>>>(a);
+        else k_radius_packet<KT, ALGO, true, false, MULTI><<<grid, kPkThreads, 0, s>>>(a);
     } else {
-        if (fp32) k_radius_packet<KT, ALGO, false, true><<<grid, kPkThreads, 0, s>>>(a);
-        else k_radius_packet<KT, ALGO, false, false><<<grid, kPkThreads, 0, s>>>(a);
+        if (fp32) k_radius_packet<KT, ALGO, false, true, MULTI><<<grid, kPkThreads, 0, s>>>(a);
+        else k_radius_packet<KT, ALGO, false, false, MULTI><<<grid, kPkThreads, 0, s>>>(a);
     }
     return cudaGetLastError();
+}
+
+template <int KT, int ALGO>
+cudaError_t launch_pk(const PacketArgs& a, bool fill, bool fp32, int grid, cudaStream_t s) {
+    if (a.reqs) return launch_pk_m<KT, ALGO, true>(a, fill, fp32, grid, s);
+    return launch_pk_m<KT, ALGO, false>(a, fill, fp32, grid, s);
 }
 
 template <int KT>
@@ -437,6 +459,53 @@ cudaError_t launch_leaf_rel(Cloud& c) {
     return cudaGetLastError();
 }
 
+CloudView cloud_view(const Cloud& c) {
+    CloudView v;
+    v.xs = c.xs.as<double>();
+    v.ys = c.ys.as<double>();
+    v.zs = c.zs.as<double>();
+    v.rel = c.rel.as<float4>();
+    v.offsets = c.offsets.as<uint32_t>();
+    v.ranges = c.ranges.as<uint2>();
+    v.centers = c.centers.as<double>();
+    v.geom = reinterpret_cast<const LevelGeom*>(c.d_box.as<unsigned char>() + sizeof(BoxD));
+    return v;
+}
+
+cudaError_t launch_radius_table(int device, cudaStream_t s, int kernel, int algo, bool fill, bool fp32,
+                                const SearchReq* d_reqs, uint32_t nreq, uint64_t packets, const uint32_t* d_order,
+                                unsigned long long* d_counts, unsigned long long* d_counts2,
+                                const unsigned long long* d_offsets, uint32_t* d_out, uint64_t out_capacity,
+                                uint32_t* d_packet_ctr, unsigned long long* d_stats, uint32_t* d_err,
+                                const SearchReq* single) {
+    cudaError_t e;
+    if (packets == 0 || nreq == 0) return cudaSuccess;
+    if ((e = cudaMemsetAsync(d_packet_ctr, 0, 4, s)) != cudaSuccess) return e;
+    PacketArgs a;
+    a.single = single ? *single : SearchReq{};
+    a.reqs = single ? nullptr : d_reqs;
+    a.nreq = nreq;
+    a.packets = packets;
+    a.order = d_order;
+    a.counts = d_counts;
+    a.counts2 = d_counts2;
+    a.offs = d_offsets;
+    a.out = d_out;
+    a.out_cap = out_capacity;
+    a.packet_ctr = d_packet_ctr;
+    a.stats = d_stats;
+    a.err = d_err;
+    const uint64_t want = (packets + kPkWarps - 1) / kPkWarps;
+    const uint64_t cap = (uint64_t)sm_count_p(device) * 12;
+    const int grid = (int)(want < cap ? want : cap);
+    switch (kernel) {
+        case kCircle: return launch_pk_a<kCircle>(a, algo, fill, fp32, grid, s);
+        case kSquare: return launch_pk_a<kSquare>(a, algo, fill, fp32, grid, s);
+        case kCube: return launch_pk_a<kCube>(a, algo, fill, fp32, grid, s);
+        default: return launch_pk_a<kSphere>(a, algo, fill, fp32, grid, s);
+    }
+}
+
 cudaError_t launch_radius_packet(Cloud& c, int kernel, int algo, bool fill, bool fp32, const double* d_centers,
                                  uint64_t nq, const double* d_radii, double radius, const uint32_t* d_order,
                                  unsigned long long* d_counts, unsigned long long* d_counts2,
@@ -444,39 +513,20 @@ cudaError_t launch_radius_packet(Cloud& c, int kernel, int algo, bool fill, bool
     cudaError_t e;
     if (nq == 0) return cudaSuccess;
     if ((e = c.packet_ctr.reserve(256)) != cudaSuccess) return e;
-    if ((e = cudaMemsetAsync(c.packet_ctr.ptr, 0, 4, c.stream)) != cudaSuccess) return e;
-    PacketArgs a;
-    a.xs = c.xs.as<double>();
-    a.ys = c.ys.as<double>();
-    a.zs = c.zs.as<double>();
-    a.rel = c.rel.as<float4>();
-    a.offsets = c.offsets.as<uint32_t>();
-    a.ranges = c.ranges.as<uint2>();
-    a.centers = c.centers.as<double>();
-    a.geom = reinterpret_cast<const LevelGeom*>(c.d_box.as<unsigned char>() + sizeof(BoxD));
-    a.q = d_centers;
-    a.qr = d_radii;
-    a.radius = radius;
-    a.order = d_order;
-    a.nq = nq;
-    a.counts = d_counts;
-    a.counts2 = d_counts2;
-    a.offs = d_offsets;
-    a.out = d_out;
-    a.out_cap = out_capacity;
-    a.packet_ctr = c.packet_ctr.as<uint32_t>();
-    a.stats = c.stats.as<unsigned long long>();
-    a.err = c.d_err.as<uint32_t>();
-    const uint64_t packets = (nq + 31) / 32;
-    const uint64_t want = (packets + kPkWarps - 1) / kPkWarps;
-    const uint64_t cap = (uint64_t)sm_count_p(c.device) * 12;
-    const int grid = (int)(want < cap ? want : cap);
-    switch (kernel) {
-        case kCircle: return launch_pk_a<kCircle>(a, algo, fill, fp32, grid, c.stream);
-        case kSquare: return launch_pk_a<kSquare>(a, algo, fill, fp32, grid, c.stream);
-        case kCube: return launch_pk_a<kCube>(a, algo, fill, fp32, grid, c.stream);
-        default: return launch_pk_a<kSphere>(a, algo, fill, fp32, grid, c.stream);
-    }
+    SearchReq r{};
+    r.cv = cloud_view(c);
+    r.centers = d_centers;
+    r.radii = d_radii;
+    r.radius = radius;
+    r.q_begin = 0;
+    r.q_end = nq;
+    r.packet_begin = 0;
+    r.out_begin = 0;
+    r.k = 0;
+    r.cloud_id = 0;
+    return launch_radius_table(c.device, c.stream, kernel, algo, fill, fp32, nullptr, 1, (nq + 31) / 32, d_order,
+                               d_counts, d_counts2, d_offsets, d_out, out_capacity, c.packet_ctr.as<uint32_t>(),
+                               c.stats.as<unsigned long long>(), c.d_err.as<uint32_t>(), &r);
 }
 
 }  // namespace octb
