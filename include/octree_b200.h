@@ -196,6 +196,95 @@ int oct_struct_search(oct_cloud cloud, int kernel, const double* centers, uint64
 int oct_knn(oct_cloud cloud, const double* centers, uint64_t nq, uint32_t k, uint32_t* idx, double* d2,
             uint32_t* counts, uint32_t flags);
 
+/* ---- Batched engine: many clouds and request sets in one launch ----------
+ *
+ * No reference counterpart: the reference answers one query at a time per
+ * OpenMP thread (neighbor_benchmarks.hpp:502-568).  An engine runs a batch of
+ * requests (each a set of radius or kNN centres against one built cloud) as
+ * one device pass: the centres of every request are ordered along their
+ * cloud's curve by one sort, then one persistent launch per kernel variant
+ * answers all radius requests (count, scan, fill) while the kNN requests run
+ * on a second stream.  Sizes are read on the device, so the launch sequence
+ * of a batch shape (which variants occur) is captured once as a CUDA graph
+ * and replayed for every later batch of that shape.  Results are bitwise
+ * those of the single-cloud calls. */
+typedef struct oct_engine_s* oct_engine;
+
+#define OCT_ENGINE_NO_GRAPH 0x1u /* launch the sequence directly instead of through a graph */
+
+typedef struct {
+    int32_t device;        /* CUDA device ordinal; clouds of a batch must live there */
+    uint32_t flags;        /* OCT_ENGINE_* */
+    uint64_t reserve_queries; /* initial capacity hint: centres per batch (0: grow on demand) */
+    uint64_t reserve_results; /* initial capacity hint: radius results per batch */
+} oct_engine_params;
+
+typedef enum { OCT_REQ_RADIUS = 0, OCT_REQ_KNN = 1 } oct_request_type;
+
+/* One request of a batch.  centers (and radii) are device memory of the
+ * engine's device and must stay valid until the batch has completed. */
+typedef struct {
+    oct_cloud cloud;       /* a built cloud */
+    int32_t type;          /* oct_request_type */
+    int32_t kernel;        /* radius: oct_kernel */
+    int32_t algo;          /* radius: OCT_NEIGHBORS or OCT_NEIGHBORS_PRUNE */
+    uint32_t k;            /* kNN: 1..64 */
+    const double* centers; /* nq x 3 */
+    uint64_t nq;
+    const double* radii;   /* radius: nq per-centre radii, or NULL to use `radius` */
+    double radius;
+} oct_request;
+
+/* Where a request's results are in the engine's output arrays
+ * (oct_engine_outputs).  Radius: offsets[q_begin .. q_begin + nq] index the
+ * indices array (each centre's neighbours ascending).  kNN: rows of k slots
+ * from out_begin in knn_idx / knn_d2 (nq x k), counts at knn_counts[q_begin +
+ * i]. */
+typedef struct {
+    uint64_t q_begin;
+    uint64_t out_begin;
+    uint64_t nq;
+    uint64_t n_results;    /* radius: neighbours of the request (after completion) */
+} oct_request_place;
+
+int oct_engine_create(const oct_engine_params* params, oct_engine* out);
+int oct_engine_destroy(oct_engine engine);
+/* Run on this CUDA stream (cudaStream_t); kNN work forks onto a private stream and joins back. */
+int oct_engine_set_stream(oct_engine engine, void* cuda_stream);
+int oct_engine_last_error(oct_engine engine, char* buf, size_t len);
+/* Search configuration of the engine (oct_search_config: fp32_filter, knn_bucket;
+ * reserved[0] = radius blocks per SM, reserved[1] = kNN blocks per SM, 0 = default). */
+int oct_engine_set_config(oct_engine engine, const oct_search_config* config);
+int oct_engine_get_config(oct_engine engine, oct_search_config* config);
+
+/* Enqueue a batch (returns without waiting); places (n entries, may be NULL
+ * until oct_engine_wait) receive each request's output position.  One batch
+ * is in flight per engine: a second submit waits for the first. */
+int oct_engine_submit(oct_engine engine, const oct_request* requests, uint32_t n, oct_request_place* places);
+/* Wait for the submitted batch; grows the result array and re-runs the batch
+ * when its results did not fit.  radius_total (may be NULL) = all radius
+ * results of the batch; places as in submit, with n_results filled in. */
+int oct_engine_wait(oct_engine engine, oct_request_place* places, uint64_t* radius_total);
+/* submit + wait. */
+int oct_engine_run(oct_engine engine, const oct_request* requests, uint32_t n, oct_request_place* places,
+                   uint64_t* radius_total);
+/* Device pointers of the output arrays of the last completed batch (valid until the next submit). */
+int oct_engine_outputs(oct_engine engine, uint64_t** offsets, uint32_t** indices, uint32_t** knn_idx,
+                       double** knn_d2, uint32_t** knn_counts);
+/* Copy one request's results out (host memory unless flags has OCT_MEM_DEVICE).
+ * Radius: offsets (nq + 1, rebased to 0) and idx (up to idx_capacity).  kNN:
+ * idx, d2 (nq x k) and counts (nq); any may be NULL. */
+int oct_engine_copy_radius(oct_engine engine, const oct_request_place* place, uint64_t* offsets, uint32_t* idx,
+                           uint64_t idx_capacity, uint32_t flags);
+int oct_engine_copy_knn(oct_engine engine, const oct_request_place* place, uint32_t k, uint32_t* idx, double* d2,
+                        uint32_t* counts, uint32_t flags);
+/* Time the candidate configurations (FP32 filter, blocks per SM, kNN bucket)
+ * on a sample batch and keep the fastest; *chosen (may be NULL) receives it.
+ * Results do not depend on the configuration. */
+int oct_engine_autotune(oct_engine engine, const oct_request* requests, uint32_t n, oct_search_config* chosen);
+/* Device time (ms) of the last completed batch, from events around its launch sequence. */
+int oct_engine_last_ms(oct_engine engine, float* ms);
+
 /* Largest cloud oct_encode_sort_noalloc accepts. */
 #define OCT_NOALLOC_MAX_POINTS (1u << 18) /* 262,144 points */
 

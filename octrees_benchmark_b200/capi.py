@@ -44,6 +44,27 @@ class OctTreeInfo(C.Structure):
                 ("n_total", C.c_uint32), ("max_depth_seen", C.c_uint32)]
 
 
+OCT_ENGINE_NO_GRAPH = 0x1
+OCT_REQ_RADIUS = 0
+OCT_REQ_KNN = 1
+
+
+class OctEngineParams(C.Structure):
+    _fields_ = [("device", C.c_int32), ("flags", C.c_uint32), ("reserve_queries", C.c_uint64),
+                ("reserve_results", C.c_uint64)]
+
+
+class OctRequest(C.Structure):
+    _fields_ = [("cloud", C.c_void_p), ("type", C.c_int32), ("kernel", C.c_int32), ("algo", C.c_int32),
+                ("k", C.c_uint32), ("centers", C.c_void_p), ("nq", C.c_uint64), ("radii", C.c_void_p),
+                ("radius", C.c_double)]
+
+
+class OctRequestPlace(C.Structure):
+    _fields_ = [("q_begin", C.c_uint64), ("out_begin", C.c_uint64), ("nq", C.c_uint64),
+                ("n_results", C.c_uint64)]
+
+
 class OctError(RuntimeError):
     def __init__(self, status: int, msg: str):
         super().__init__(msg)
@@ -78,6 +99,21 @@ SIGNATURES = {
     "oct_struct_search": ([_vp, _int, _vp, _u64, _vp, _dbl, _vp, _vp, _u64, C.POINTER(_u64), _vp, _u32], _int),
     "oct_knn": ([_vp, _vp, _u64, _u32, _vp, _vp, _vp, _u32], _int),
     "oct_encode_sort_noalloc": ([_int, _vp, _u64, _vp, _vp, _vp, _vp], _int),
+    "oct_engine_create": ([C.POINTER(OctEngineParams), C.POINTER(_vp)], _int),
+    "oct_engine_destroy": ([_vp], _int),
+    "oct_engine_set_stream": ([_vp, _vp], _int),
+    "oct_engine_last_error": ([_vp, C.c_char_p, C.c_size_t], _int),
+    "oct_engine_set_config": ([_vp, C.POINTER(OctSearchConfig)], _int),
+    "oct_engine_get_config": ([_vp, C.POINTER(OctSearchConfig)], _int),
+    "oct_engine_submit": ([_vp, C.POINTER(OctRequest), _u32, C.POINTER(OctRequestPlace)], _int),
+    "oct_engine_wait": ([_vp, C.POINTER(OctRequestPlace), C.POINTER(_u64)], _int),
+    "oct_engine_run": ([_vp, C.POINTER(OctRequest), _u32, C.POINTER(OctRequestPlace), C.POINTER(_u64)], _int),
+    "oct_engine_outputs": ([_vp, C.POINTER(_vp), C.POINTER(_vp), C.POINTER(_vp), C.POINTER(_vp), C.POINTER(_vp)],
+                           _int),
+    "oct_engine_copy_radius": ([_vp, C.POINTER(OctRequestPlace), _vp, _vp, _u64, _u32], _int),
+    "oct_engine_copy_knn": ([_vp, C.POINTER(OctRequestPlace), _u32, _vp, _vp, _vp, _u32], _int),
+    "oct_engine_autotune": ([_vp, C.POINTER(OctRequest), _u32, C.POINTER(OctSearchConfig)], _int),
+    "oct_engine_last_ms": ([_vp, C.POINTER(C.c_float)], _int),
 }
 
 

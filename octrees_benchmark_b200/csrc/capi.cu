@@ -10,10 +10,6 @@
 
 using namespace octb;
 
-struct oct_cloud_s {
-    Cloud c;
-};
-
 namespace {
 
 // Makes the cloud's device current for the duration of a call.

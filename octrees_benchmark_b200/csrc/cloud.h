@@ -68,6 +68,9 @@ struct CloudView {
     const uint2* ranges;
     const double* centers;
     const LevelGeom* geom;      // per-level radii
+    const BoxD* box;            // the cloud's Box (anchor frame of its keys)
+    int32_t encoder;            // OCT_ENC_MORTON_3D or OCT_ENC_HILBERT_3D
+    uint32_t pad;
 };
 
 // One request of a search launch (device copy).  A launch covers a table of
@@ -83,6 +86,18 @@ struct SearchReq {
     uint64_t out_begin;         // kNN: first output slot (previous requests' nq * k)
     uint32_t k;                 // kNN k
     uint32_t cloud_id;          // distinct per cloud within the table (radii reload key)
+};
+
+// Launch sizes of one kernel group of a batch, in device memory.  The host
+// writes them before the batch runs, so one launch configuration (and one
+// captured graph) serves batches of any size.
+struct DynGroup {
+    const SearchReq* reqs;      // the group's requests (device), positions ascending
+    uint32_t nreq;
+    uint32_t kmax;              // kNN: largest k of the group
+    uint64_t packets;           // radius: 32-query packets of the group
+    uint64_t q_begin;           // first query position of the group
+    uint64_t nq;                // queries of the group
 };
 
 struct Cloud {
@@ -156,19 +171,33 @@ cudaError_t launch_radius_packet(Cloud& c, int kernel, int algo, bool fill, bool
                                  uint64_t nq, const double* d_radii, double radius, const uint32_t* d_order,
                                  unsigned long long* d_counts, unsigned long long* d_counts2,
                                  const unsigned long long* d_offsets, uint32_t* d_out, uint64_t out_capacity);
-// Packet radius search over a request table (device), nreq entries, `packets` packets in total.
+// Packet radius search.  Either one request (`single`, host copy, `packets`
+// packets) or the group of a batch (`d_grp`, sizes read on the device).
 cudaError_t launch_radius_table(int device, cudaStream_t s, int kernel, int algo, bool fill, bool fp32,
-                                const SearchReq* d_reqs, uint32_t nreq, uint64_t packets, const uint32_t* d_order,
-                                unsigned long long* d_counts, unsigned long long* d_counts2,
+                                const DynGroup* d_grp, const SearchReq* single, uint64_t packets,
+                                const uint32_t* d_order, unsigned long long* d_counts, unsigned long long* d_counts2,
                                 const unsigned long long* d_offsets, uint32_t* d_out, uint64_t out_capacity,
                                 uint32_t* d_packet_ctr, unsigned long long* d_stats, uint32_t* d_err,
-                                const SearchReq* single = nullptr);
-// Register kNN (k <= 64) over a request table: one warp per query, nq queries in total.
-cudaError_t launch_knn_table(int device, cudaStream_t s, const SearchReq* d_reqs, uint32_t nreq, uint64_t nq,
+                                int blocks_per_sm = 0);
+// Register kNN (k <= 64), one warp per query.  Either one request (`single`,
+// nq queries) or the group of a batch (`d_grp`, kmax = the group's largest k).
+cudaError_t launch_knn_table(int device, cudaStream_t s, const DynGroup* d_grp, const SearchReq* single, uint64_t nq,
                              uint32_t kmax, const uint32_t* d_order, uint32_t bucket, uint32_t* d_idx, double* d_d2,
-                             uint32_t* d_counts, uint32_t* d_err, const SearchReq* single = nullptr);
+                             uint32_t* d_counts, uint32_t* d_err, int blocks_per_sm = 0);
 CloudView cloud_view(const Cloud& c);
+// Batched engine: the sort of query keys with device-side sizes (encode_sort.cu).
+cudaError_t prepare_sort_dyn();
+size_t sort_tile_keys();
+cudaError_t launch_sort_dyn(int device, cudaStream_t s, uint64_t* k0, uint64_t* k1, uint32_t* v0, uint32_t* v1,
+                            const uint64_t* d_n, uint64_t max_n, int passes, SortCtl* ctl,
+                            unsigned long long* status, const uint32_t* d_epoch, uint32_t* err,
+                            uint32_t** result_vals);
 cudaError_t launch_knn(Cloud& c, const double* d_centers, uint64_t nq, uint32_t k, uint32_t* d_idx, double* d_d2,
                        uint32_t* d_counts);
 
 }  // namespace octb
+
+// The object behind the ABI's oct_cloud handle.
+struct oct_cloud_s {
+    octb::Cloud c;
+};

@@ -191,8 +191,9 @@ __global__ void __launch_bounds__(kEncThreads) k_encode(const double* __restrict
 
 // Exclusive scans of the 8 histograms; pass p is skipped when one digit holds
 // every key.  One block of 256 threads.
-__global__ void __launch_bounds__(256) k_scan_hist(SortCtl* ctl, uint64_t n) {
+__global__ void __launch_bounds__(256) k_scan_hist(SortCtl* ctl, uint64_t n, const uint64_t* d_n = nullptr) {
     __shared__ unsigned long long warp_sum[8];
+    if (d_n) n = *d_n;
     const int d = threadIdx.x, lane = d & 31, warp = d >> 5;
     for (int p = 0; p < 8; ++p) {
         const unsigned long long v = ctl->hist[p][d];
@@ -222,7 +223,8 @@ __global__ void __launch_bounds__(kSortThreads) k_onesweep(const uint64_t* __res
                                                            uint64_t* __restrict__ kout, uint32_t* __restrict__ vout,
                                                            uint64_t n, int pass, SortCtl* ctl,
                                                            unsigned long long* status, uint32_t epoch,
-                                                           uint32_t* err) {
+                                                           uint32_t* err, const uint64_t* d_n = nullptr,
+                                                           const uint32_t* d_epoch = nullptr) {
     extern __shared__ __align__(16) unsigned char smem[];
     uint64_t* skeys = reinterpret_cast<uint64_t*>(smem);                       // kSortTile
     uint32_t* svals = reinterpret_cast<uint32_t*>(skeys + kSortTile);          // kSortTile
@@ -234,10 +236,19 @@ __global__ void __launch_bounds__(kSortThreads) k_onesweep(const uint64_t* __res
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int shift = 8 * pass;
+    // sizes set on the device (batched launches): key count, and the epoch base
+    // of this batch's passes
+    if (d_n) n = *d_n;
+    if (d_epoch) epoch = (*d_epoch + (uint32_t)pass) & ((1u << 22) - 1);
+    const uint64_t ntiles = (n + kSortTile - 1) / kSortTile;
+    // persistent: a block takes tiles in order until none is left; a tile only
+    // waits on lower tiles, which running blocks hold
+    for (;;) {
     if (tid == 0) s_tile = atomicAdd(&ctl->tile_ctr[pass], 1u);
     for (int j = tid; j < kSortWarps * 256; j += kSortThreads) wcnt[j] = 0;
     __syncthreads();
     const uint32_t tile = s_tile;
+    if ((uint64_t)tile >= ntiles) break;
     const uint64_t base = (uint64_t)tile * kSortTile;
 
     uint64_t k[kSortItems];
@@ -338,6 +349,8 @@ __global__ void __launch_bounds__(kSortThreads) k_onesweep(const uint64_t* __res
             kout[o] = key;
             vout[o] = svals[s];
         }
+    }
+    __syncthreads();  // shared memory and s_tile are reused by the next tile
     }
 }
 
@@ -477,6 +490,44 @@ cudaError_t launch_gather(Cloud& c, const double* d_xyz, const uint32_t* d_perm,
 // Query ordering for the packet searches: the query centres are keyed with the
 // cloud's box and curve and stably sorted by the top 24 key bits (3 onesweep
 // passes), so that the 32 queries of a warp are spatial neighbours.
+// ---------------------------------------------------------------------------
+// Device-sized sort of a batch's query keys (the batched engine): the key
+// count and the epoch base are read on the device, and every pass runs a fixed
+// persistent grid, so the launch sequence can be captured once as a graph.
+
+cudaError_t prepare_sort_dyn() {
+    const int smem = (int)onesweep_smem();
+    cudaError_t e = cudaFuncSetAttribute(k_onesweep<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+    if (e != cudaSuccess) return e;
+    return cudaFuncSetAttribute(k_onesweep<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, smem);
+}
+
+size_t sort_tile_keys() { return kSortTile; }
+
+cudaError_t launch_sort_dyn(int device, cudaStream_t s, uint64_t* k0, uint64_t* k1, uint32_t* v0, uint32_t* v1,
+                            const uint64_t* d_n, uint64_t max_n, int passes, SortCtl* ctl,
+                            unsigned long long* status, const uint32_t* d_epoch, uint32_t* err,
+                            uint32_t** result_vals) {
+    const size_t smem = onesweep_smem();
+    const uint64_t max_tiles = (max_n + kSortTile - 1) / kSortTile;
+    const uint64_t resident = (uint64_t)sm_count(device) * 3;  // 3 x 60 KB tiles per SM
+    const unsigned grid = (unsigned)(max_tiles < resident ? (max_tiles ? max_tiles : 1) : resident);
+    k_scan_hist<<<1, 256, 0, s>>>(ctl, 0, d_n);
+    uint64_t* kb[2] = {k0, k1};
+    uint32_t* vb[2] = {v0, v1};
+    for (int p = 0; p < passes; ++p) {
+        const int i = p & 1, o = i ^ 1;
+        if (p == 0)
+            k_onesweep<true><<<grid, kSortThreads, smem, s>>>(kb[i], nullptr, kb[o], vb[o], 0, p, ctl, status, 0,
+                                                              err, d_n, d_epoch);
+        else
+            k_onesweep<false><<<grid, kSortThreads, smem, s>>>(kb[i], vb[i], kb[o], vb[o], 0, p, ctl, status, 0,
+                                                               err, d_n, d_epoch);
+    }
+    *result_vals = vb[passes & 1];
+    return cudaGetLastError();
+}
+
 // ---------------------------------------------------------------------------
 
 namespace {

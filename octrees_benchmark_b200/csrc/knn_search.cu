@@ -333,10 +333,9 @@ __device__ __forceinline__ void reglist_merge32(RegList<R>& L, double cd, uint32
 }
 
 struct KnnTableArgs {
-    SearchReq single;        // the request of a single-cloud search (reqs == null)
-    const SearchReq* reqs;   // request table of a multi-request launch (q_begin ascending)
-    uint32_t nreq;
-    uint64_t nq;             // queries of the whole launch
+    SearchReq single;        // the request of a single-cloud search (grp == null)
+    const DynGroup* grp;     // sizes and request table of a batch group (device)
+    uint64_t nq;             // queries of a single-request launch
     const uint32_t* order;   // visiting order (global query positions), or null
     uint32_t bucket;
     uint32_t* idx;
@@ -345,7 +344,7 @@ struct KnnTableArgs {
     uint32_t* err;
 };
 
-#define KRQ(f) (MULTI ? a.reqs[ri].f : a.single.f)
+#define KRQ(f) (MULTI ? reqs[ri].f : a.single.f)
 template <int R, bool MULTI>
 __global__ void __launch_bounds__(kKnnThreads) k_knn_reg(KnnTableArgs a) {
     __shared__ uint32_t st_a[kKnnWarps][kKnnStack];   // leaf: first point; internal: first child
@@ -362,14 +361,24 @@ __global__ void __launch_bounds__(kKnnThreads) k_knn_reg(KnnTableArgs a) {
     uint32_t* sb = st_b[warp];
     double* sl = st_lb[warp];
     uint8_t* sd = st_depth[warp];
+    const SearchReq* reqs = nullptr;
+    uint32_t nreq = 1;
+    uint64_t q0 = 0, nq = a.nq;
+    if (MULTI) {
+        reqs = a.grp->reqs;
+        nreq = a.grp->nreq;
+        q0 = a.grp->q_begin;
+        nq = a.grp->nq;
+    }
     const uint64_t nwarps = (uint64_t)gridDim.x * kKnnWarps;
-    for (uint64_t qpos = (uint64_t)blockIdx.x * kKnnWarps + warp; qpos < a.nq; qpos += nwarps) {
+    for (uint64_t w = (uint64_t)blockIdx.x * kKnnWarps + warp; w < nq; w += nwarps) {
+        const uint64_t qpos = q0 + w;
         uint32_t ri = 0;
         if (MULTI) {  // the request whose positions contain qpos (q_begin ascending)
-            uint32_t lo = 0, hi = a.nreq;
+            uint32_t lo = 0, hi = nreq;
             while (hi - lo > 1) {
                 const uint32_t mid = (lo + hi) >> 1;
-                if (a.reqs[mid].q_begin <= qpos) lo = mid;
+                if (reqs[mid].q_begin <= qpos) lo = mid;
                 else hi = mid;
             }
             ri = lo;
@@ -752,14 +761,13 @@ int sm_count_k(int device) {
 
 }  // namespace
 
-cudaError_t launch_knn_table(int device, cudaStream_t s, const SearchReq* d_reqs, uint32_t nreq, uint64_t nq,
+cudaError_t launch_knn_table(int device, cudaStream_t s, const DynGroup* d_grp, const SearchReq* single, uint64_t nq,
                              uint32_t kmax, const uint32_t* d_order, uint32_t bucket, uint32_t* d_idx, double* d_d2,
-                             uint32_t* d_counts, uint32_t* d_err, const SearchReq* single) {
-    if (nq == 0 || nreq == 0) return cudaSuccess;
+                             uint32_t* d_counts, uint32_t* d_err, int blocks_per_sm) {
+    if (!d_grp && nq == 0) return cudaSuccess;
     KnnTableArgs a;
     a.single = single ? *single : SearchReq{};
-    a.reqs = single ? nullptr : d_reqs;
-    a.nreq = nreq;
+    a.grp = d_grp;
     a.nq = nq;
     a.order = d_order;
     a.bucket = bucket;
@@ -767,10 +775,10 @@ cudaError_t launch_knn_table(int device, cudaStream_t s, const SearchReq* d_reqs
     a.d2 = d_d2;
     a.counts = d_counts;
     a.err = d_err;
-    const uint64_t want = (nq + kKnnWarps - 1) / kKnnWarps;
-    const uint64_t cap = (uint64_t)sm_count_k(device) * 16;
+    const uint64_t cap = (uint64_t)sm_count_k(device) * (blocks_per_sm > 0 ? blocks_per_sm : 16);
+    const uint64_t want = d_grp ? cap : (nq + kKnnWarps - 1) / kKnnWarps;
     const int grid = (int)(want < cap ? want : cap);
-    if (a.reqs) {
+    if (d_grp) {
         if (kmax <= 32) k_knn_reg<1, true><<<grid, kKnnThreads, 0, s>>>(a);
         else k_knn_reg<2, true><<<grid, kKnnThreads, 0, s>>>(a);
     } else {
@@ -826,8 +834,8 @@ cudaError_t launch_knn(Cloud& c, const double* d_centers, uint64_t nq, uint32_t 
         r.q_begin = 0;
         r.q_end = nq;
         r.k = k;
-        return launch_knn_table(c.device, c.stream, nullptr, 1, nq, k, a.order, c.knn_bucket, d_idx, d_d2, d_counts,
-                                c.d_err.as<uint32_t>(), &r);
+        return launch_knn_table(c.device, c.stream, nullptr, &r, nq, k, a.order, c.knn_bucket, d_idx, d_d2, d_counts,
+                                c.d_err.as<uint32_t>());
     }
     if (k <= 32) return launch_l<32>(a, grid, c.stream);
     if (k <= 64) return launch_l<64>(a, grid, c.stream);

@@ -44,10 +44,9 @@ constexpr int kPkThreads = 32 * kPkWarps;
 constexpr int kPkStack = 8 * (kMaxDepth + 1);
 
 struct PacketArgs {
-    SearchReq single;           // the request of a single-cloud search (reqs == null)
-    const SearchReq* reqs;      // request table of a multi-request launch
-    uint32_t nreq;
-    uint64_t packets;           // packets of the whole launch
+    SearchReq single;           // the request of a single-cloud search (grp == null)
+    const DynGroup* grp;        // sizes and request table of a batch group (device)
+    uint64_t packets;           // packets of a single-request launch
     const uint32_t* order;      // query visiting order (global positions), or null
     unsigned long long* counts;
     unsigned long long* counts2;
@@ -122,7 +121,7 @@ __device__ __forceinline__ int f32_test(const LeafCtx& c, float4 p) {
 
 // MULTI: the launch covers a request table; otherwise the single request is read
 // from the kernel parameters (constant-bank operands, no registers held).
-#define RQ(f) (MULTI ? a.reqs[cur_req].f : a.single.f)
+#define RQ(f) (MULTI ? reqs[cur_req].f : a.single.f)
 template <int KT, int ALGO, bool FILL, bool F32, bool MULTI>
 __global__ void __launch_bounds__(kPkThreads) k_radius_packet(PacketArgs a) {
     __shared__ uint32_t st_node[kPkWarps][kPkStack];
@@ -139,6 +138,14 @@ __global__ void __launch_bounds__(kPkThreads) k_radius_packet(PacketArgs a) {
     double (*s_radii)[3] = s_rad[warp];
     uint32_t cur_cloud = 0xffffffffu;
     uint32_t cur_req = 0;
+    const SearchReq* reqs = nullptr;
+    uint32_t nreq = 1;
+    uint64_t packets = a.packets;
+    if (MULTI) {
+        reqs = a.grp->reqs;
+        nreq = a.grp->nreq;
+        packets = a.grp->packets;
+    }
     const uint32_t lbit = 1u << lane;
     uint32_t* sn = st_node[warp];
     uint32_t* sf = st_fc[warp];
@@ -152,13 +159,13 @@ __global__ void __launch_bounds__(kPkThreads) k_radius_packet(PacketArgs a) {
         uint32_t packet = 0;
         if (lane == 0) packet = atomicAdd(a.packet_ctr, 1u);
         packet = __shfl_sync(0xffffffffu, packet, 0);
-        if (packet >= a.packets) break;
+        if (packet >= packets) break;
         // the request of this packet: packet_begin is ascending over the table
         if (MULTI) {
-            uint32_t lo = 0, hi = a.nreq;
+            uint32_t lo = 0, hi = nreq;
             while (hi - lo > 1) {
                 const uint32_t mid = (lo + hi) >> 1;
-                if (a.reqs[mid].packet_begin <= packet) lo = mid;
+                if (reqs[mid].packet_begin <= packet) lo = mid;
                 else hi = mid;
             }
             cur_req = lo;
@@ -433,7 +440,7 @@ cudaError_t launch_pk_m(const PacketArgs& a, bool fill, bool fp32, int grid, cud
 
 template <int KT, int ALGO>
 cudaError_t launch_pk(const PacketArgs& a, bool fill, bool fp32, int grid, cudaStream_t s) {
-    if (a.reqs) return launch_pk_m<KT, ALGO, true>(a, fill, fp32, grid, s);
+    if (a.grp) return launch_pk_m<KT, ALGO, true>(a, fill, fp32, grid, s);
     return launch_pk_m<KT, ALGO, false>(a, fill, fp32, grid, s);
 }
 
@@ -469,22 +476,24 @@ CloudView cloud_view(const Cloud& c) {
     v.ranges = c.ranges.as<uint2>();
     v.centers = c.centers.as<double>();
     v.geom = reinterpret_cast<const LevelGeom*>(c.d_box.as<unsigned char>() + sizeof(BoxD));
+    v.box = c.d_box.as<BoxD>();
+    v.encoder = c.params.encoder;
+    v.pad = 0;
     return v;
 }
 
 cudaError_t launch_radius_table(int device, cudaStream_t s, int kernel, int algo, bool fill, bool fp32,
-                                const SearchReq* d_reqs, uint32_t nreq, uint64_t packets, const uint32_t* d_order,
-                                unsigned long long* d_counts, unsigned long long* d_counts2,
+                                const DynGroup* d_grp, const SearchReq* single, uint64_t packets,
+                                const uint32_t* d_order, unsigned long long* d_counts, unsigned long long* d_counts2,
                                 const unsigned long long* d_offsets, uint32_t* d_out, uint64_t out_capacity,
                                 uint32_t* d_packet_ctr, unsigned long long* d_stats, uint32_t* d_err,
-                                const SearchReq* single) {
+                                int blocks_per_sm) {
     cudaError_t e;
-    if (packets == 0 || nreq == 0) return cudaSuccess;
+    if (!d_grp && packets == 0) return cudaSuccess;
     if ((e = cudaMemsetAsync(d_packet_ctr, 0, 4, s)) != cudaSuccess) return e;
     PacketArgs a;
     a.single = single ? *single : SearchReq{};
-    a.reqs = single ? nullptr : d_reqs;
-    a.nreq = nreq;
+    a.grp = d_grp;
     a.packets = packets;
     a.order = d_order;
     a.counts = d_counts;
@@ -495,8 +504,9 @@ cudaError_t launch_radius_table(int device, cudaStream_t s, int kernel, int algo
     a.packet_ctr = d_packet_ctr;
     a.stats = d_stats;
     a.err = d_err;
-    const uint64_t want = (packets + kPkWarps - 1) / kPkWarps;
-    const uint64_t cap = (uint64_t)sm_count_p(device) * 12;
+    // persistent grid: warps take packets from the counter until none is left
+    const uint64_t cap = (uint64_t)sm_count_p(device) * (blocks_per_sm > 0 ? blocks_per_sm : 12);
+    const uint64_t want = d_grp ? cap : (packets + kPkWarps - 1) / kPkWarps;
     const int grid = (int)(want < cap ? want : cap);
     switch (kernel) {
         case kCircle: return launch_pk_a<kCircle>(a, algo, fill, fp32, grid, s);
@@ -524,9 +534,9 @@ cudaError_t launch_radius_packet(Cloud& c, int kernel, int algo, bool fill, bool
     r.out_begin = 0;
     r.k = 0;
     r.cloud_id = 0;
-    return launch_radius_table(c.device, c.stream, kernel, algo, fill, fp32, nullptr, 1, (nq + 31) / 32, d_order,
+    return launch_radius_table(c.device, c.stream, kernel, algo, fill, fp32, nullptr, &r, (nq + 31) / 32, d_order,
                                d_counts, d_counts2, d_offsets, d_out, out_capacity, c.packet_ctr.as<uint32_t>(),
-                               c.stats.as<unsigned long long>(), c.d_err.as<uint32_t>(), &r);
+                               c.stats.as<unsigned long long>(), c.d_err.as<uint32_t>());
 }
 
 }  // namespace octb
