@@ -51,7 +51,10 @@ Q_KNN = 500_000
 L2_FLUSH_BYTES = 512 << 20
 # device launches of this library per timed step: radius search (count, 3 scan kernels, fill), kNN;
 # the packet paths add the query ordering (keys, histogram scan, 3 sort passes) to the radius and the kNN call
-LAUNCHES_PER_STEP = {"plain": 6, "packet": 6 + 10, "packet_fp32": 6 + 10, "knn_packet": 6 + 10}
+LAUNCHES_PER_STEP = {"plain": 6, "packet": 6 + 10, "packet_fp32": 6 + 10, "knn_packet": 6 + 10,
+                     # engine: epoch, keys, histogram scan, 4 sort passes, radius count, 3 scan kernels,
+                     # radius fill, request totals, kNN
+                     "engine": 14}
 BUILD_BYTES_PER_POINT = 112  # encode 32 + sort 20 + reorder 52 + leaf counting 8
 BUILD_BYTES_PER_NODE = 36    # offsets 4 + ranges 8 + centers 24
 
@@ -200,6 +203,70 @@ def run_reference_arm(args, rank, world):
     return 0
 
 
+# ------------------------------------------------------ multi-cloud batch ---
+def run_batched(args, dev):
+    """256 clouds with their own query sets: one engine batch against sequential per-cloud calls."""
+    import torch
+
+    from octrees_benchmark_b200.engine import BatchEngine
+    from octrees_benchmark_b200.workloads import BatchedWorkload, sequential
+
+    wl = BatchedWorkload(device=dev)
+    eng = BatchEngine(device=dev)
+    tune = eng.autotune(wl.sample(4096))
+    for _ in range(args.warmup):
+        places = eng.run(wl.requests)
+    dev_ms, wall_ms = [], []
+    for _ in range(args.batched_steps):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        places = eng.run(wl.requests)
+        wall_ms.append(1e3 * (time.perf_counter() - t0))
+        dev_ms.append(eng.last_ms)
+    radius_totals = [pl.n_results for pl, r in zip(places, wl.requests) if r.kind == "radius"]
+    n_results = sum(radius_totals)
+    out_cap = max(radius_totals) + 1024
+    eng_kidx, eng_kd2, _ = eng.knn_result(places[-1], wl.requests[-1].k)
+    del eng
+    torch.cuda.empty_cache()
+    seq = {}
+    stream = torch.cuda.Stream()
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    for name, packet in (("sequential_plain", False), ("sequential_packet", True)):
+        sequential(wl, stream, out_cap, packet)  # warm-up (first call of each cloud sizes its scratch)
+        times = []
+        for _ in range(args.batched_steps):
+            stream.synchronize()
+            ev0.record(stream)
+            totals, kidx, kd2 = sequential(wl, stream, out_cap, packet)
+            ev1.record(stream)
+            stream.synchronize()
+            times.append(ev0.elapsed_time(ev1))
+        # the same results as the batch: every radius request's count, the last kNN request's pairs
+        assert totals == radius_totals, f"{name}: radius result counts differ from the batch"
+        nk, k = int(wl.requests[-1].centers.shape[0]), wl.requests[-1].k
+        assert np.array_equal(kidx[: nk * k].cpu().numpy().view(np.uint32).reshape(nk, k), eng_kidx)
+        assert np.array_equal(kd2[: nk * k].cpu().numpy().reshape(nk, k), eng_kd2)
+        seq[name] = {"ms": statistics.median(times), "qps": wl.n_queries / (statistics.median(times) / 1e3)}
+    b_ms = statistics.median(dev_ms)
+    return {
+        "workload": wl.describe(),
+        "queries": wl.n_queries, "radius_results": n_results,
+        "batched_ms": b_ms, "batched_wall_ms": statistics.median(wall_ms), "batched_qps": wl.n_queries / (b_ms / 1e3),
+        "sequential_plain_ms": seq["sequential_plain"]["ms"], "sequential_plain_qps": seq["sequential_plain"]["qps"],
+        "sequential_packet_ms": seq["sequential_packet"]["ms"],
+        "sequential_packet_qps": seq["sequential_packet"]["qps"],
+        "speedup_vs_sequential_plain": seq["sequential_plain"]["ms"] / b_ms,
+        "speedup_vs_sequential_packet": seq["sequential_packet"]["ms"] / b_ms,
+        "autotuned": tune, "steps": args.batched_steps, "warmup": args.warmup,
+        "timing": "batch: CUDA events around the engine's whole device sequence (descriptor copy to summary copy); "
+                  "sequential: CUDA events around all 512 calls on one stream, host syncs of the calls included",
+        "generate_s": wl.gen_s, "build_all_clouds_s": wl.build_s,
+        "parity": "every radius request's result count and the last kNN request's pairs equal between batch and "
+                  "sequential calls (full bitwise parity is in the GPU tests)",
+    }
+
+
 # --------------------------------------------------------------- B200 arm ---
 def run_b200(args, rank, world, local_rank):
     import torch
@@ -271,7 +338,26 @@ def run_b200(args, rank, world, local_rank):
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
 
     SEARCH_PATHS = {"plain": (0, 0, args.radius_group, 0), "packet": (1, 0, 8, 0), "packet_fp32": (1, 1, 8, 0),
-                    "knn_packet": (1, 0, 8, 1)}
+                    "knn_packet": (1, 0, 8, 1), "engine": (1, 0, 8, 0)}
+
+    # the batched engine: both request sets of a step in one graph launch (kNN beside the radius search)
+    from types import SimpleNamespace
+
+    from octrees_benchmark_b200.engine import BatchEngine, Request
+
+    proxy = SimpleNamespace(handle=h)
+    eng = BatchEngine(device=dev, reserve_results=cap)
+    eng_reqs = [[Request(proxy, "radius", qr, radius=RADIUS, kernel="sphere", algo="neighborsPrune"),
+                 Request(proxy, "knn", qk, k=KNN_K)] for qr, qk in batches]
+    eng_cfg = eng.autotune(eng_reqs[0])
+
+    def engine_step(b):
+        with torch.cuda.stream(stream):
+            flush.zero_()
+        stream.synchronize()
+        places = eng.run(eng_reqs[b])
+        ms = eng.last_ms
+        return None, ms, 0.0, int(places[0].n_results)
 
     def configure(name):
         packet, fp32, lanes, knn_packet = SEARCH_PATHS[name]
@@ -300,8 +386,9 @@ def run_b200(args, rank, world, local_rank):
     clocks.start()
     for name in SEARCH_PATHS:
         configure(name)
+        run_step = engine_step if name == "engine" else step
         for b in range(args.warmup):
-            step(b)
+            run_step(b)
         if world > 1:
             torch.distributed.barrier()
         torch.cuda.synchronize()
@@ -309,8 +396,8 @@ def run_b200(args, rank, world, local_rank):
         t_count = t_search = t_knn = 0.0
         nbrs = 0
         for s in range(args.steps):
-            a_, b_, c_, tt = step(args.warmup + s)
-            t_count += a_
+            a_, b_, c_, tt = run_step(args.warmup + s)
+            t_count += a_ or 0.0
             t_search += b_
             t_knn += c_
             nbrs += tt
@@ -323,9 +410,13 @@ def run_b200(args, rank, world, local_rank):
             torch.distributed.barrier()
             torch.distributed.all_reduce(tmax, op=torch.distributed.ReduceOp.MAX)
         step_ms, rad_ms, knn_ms = (float(v) for v in tmax.tolist())
+        if name == "engine":  # radius and kNN overlap: one device time for the whole batch
+            rad_ms = knn_ms = float("nan")
         paths[name] = {"ms_per_step": step_ms, "qps": world * (Q_RADIUS + Q_KNN) / (step_ms / 1e3),
-                       "radius_qps": world * Q_RADIUS / (rad_ms / 1e3), "knn_qps": world * Q_KNN / (knn_ms / 1e3),
-                       "radius_ms": rad_ms, "knn_ms": knn_ms, "radius_count_only_ms": t_count / args.steps,
+                       "radius_qps": world * Q_RADIUS / (rad_ms / 1e3) if rad_ms == rad_ms else None,
+                       "knn_qps": world * Q_KNN / (knn_ms / 1e3) if knn_ms == knn_ms else None,
+                       "radius_ms": rad_ms if rad_ms == rad_ms else None, "knn_ms": knn_ms if knn_ms == knn_ms else None,
+                       "radius_count_only_ms": t_count / args.steps if name != "engine" else None,
                        "avg_neighbours": nbrs / args.steps / Q_RADIUS, "nbrs_per_step": nbrs / args.steps,
                        "point_tests": tests.value, "fp64_retests": retests.value,
                        "band_hit_fraction": (retests.value / tests.value) if tests.value else None}
@@ -339,7 +430,48 @@ def run_b200(args, rank, world, local_rank):
     e2e_val = None
     e2e_detail = None
     h2d = d2h = 0
-    if not args.no_e2e:
+    if not args.no_e2e and args.search == "engine":
+        # through the engine's public API: centres copied in from pinned host memory, every result copied out
+        qrh = torch.empty((Q_RADIUS, 3), dtype=torch.float64).pin_memory()
+        qkh = torch.empty((Q_KNN, 3), dtype=torch.float64).pin_memory()
+        qrd = torch.empty((Q_RADIUS, 3), dtype=torch.float64, device="cuda")
+        qkd = torch.empty((Q_KNN, 3), dtype=torch.float64, device="cuda")
+        offs_h = torch.empty(Q_RADIUS + 1, dtype=torch.int64).pin_memory().numpy()
+        idx_h = torch.empty(cap, dtype=torch.int32).pin_memory().numpy()
+        kidx_h = torch.empty((Q_KNN, KNN_K), dtype=torch.int32).pin_memory().numpy()
+        kd2_h = torch.empty((Q_KNN, KNN_K), dtype=torch.float64).pin_memory().numpy()
+        kcnt_h = torch.empty(Q_KNN, dtype=torch.int32).pin_memory().numpy()
+        L_ = capi.lib()
+        reqs_e2e = [Request(proxy, "radius", qrd, radius=RADIUS, kernel="sphere", algo="neighborsPrune"),
+                    Request(proxy, "knn", qkd, k=KNN_K)]
+        et = []
+        for s_ in range(args.warmup + args.steps):
+            qr, qk = batches[s_]
+            qrh.copy_(qr)
+            qkh.copy_(qk)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            with torch.cuda.stream(stream):
+                qrd.copy_(qrh, non_blocking=True)
+                qkd.copy_(qkh, non_blocking=True)
+            stream.synchronize()
+            pl = eng.run(reqs_e2e)
+            capi.check(L_.oct_engine_copy_radius(eng._h, C.byref(pl[0]), offs_h.ctypes.data, idx_h.ctypes.data, cap,
+                                                 0), None, "e2e copy radius")
+            capi.check(L_.oct_engine_copy_knn(eng._h, C.byref(pl[1]), KNN_K, kidx_h.ctypes.data, kd2_h.ctypes.data,
+                                              kcnt_h.ctypes.data, 0), None, "e2e copy kNN")
+            t1 = time.perf_counter()
+            if s_ >= args.warmup:
+                et.append(t1 - t0)
+                h2d = 24 * (Q_RADIUS + Q_KNN)
+                d2h = 8 * (Q_RADIUS + 1) + 4 * int(pl[0].n_results) + Q_KNN * KNN_K * 12 + 4 * Q_KNN
+        e2e_t = torch.tensor([statistics.median(et)], dtype=torch.float64, device="cuda")
+        if world > 1:
+            torch.distributed.all_reduce(e2e_t, op=torch.distributed.ReduceOp.MAX)
+        e2e_val = world * (Q_RADIUS + Q_KNN) / float(e2e_t.item())
+        e2e_detail = {"api": "oct_engine_run + oct_engine_copy_radius / oct_engine_copy_knn",
+                      "step_ms_all": [round(1e3 * v, 2) for v in et]}
+    elif not args.no_e2e:
         qrh = torch.empty((Q_RADIUS, 3), dtype=torch.float64).pin_memory().numpy()
         qkh = torch.empty((Q_KNN, 3), dtype=torch.float64).pin_memory().numpy()
         offs_h = torch.empty(Q_RADIUS + 1, dtype=torch.int64).pin_memory().numpy()
@@ -386,8 +518,10 @@ def run_b200(args, rank, world, local_rank):
     peak, peak_kind = measured_peak()
     rad_bytes = 24 * Q_RADIUS + 28 * chosen["nbrs_per_step"]
     knn_bytes = (24 + 36 * KNN_K) * Q_KNN
-    rad_ms, knn_ms = chosen["radius_ms"], chosen["knn_ms"]
-    rad = {"kernel": f"radius neighborsPrune sphere, {args.search} path (count + scan + fill)", "ms": rad_ms,
+    # per-kernel times: the engine runs the packet path's kernels side by side, so they are timed there alone
+    kpath = args.search if chosen["radius_ms"] is not None else "packet"
+    rad_ms, knn_ms = paths[kpath]["radius_ms"], paths[kpath]["knn_ms"]
+    rad = {"kernel": f"radius neighborsPrune sphere, {kpath} path (count + scan + fill)", "ms": rad_ms,
            "achieved": rad_bytes / (rad_ms / 1e3) / 1e9}
     knn = {"kernel": "kNN k=50 (k_knn)", "ms": knn_ms, "achieved": knn_bytes / (knn_ms / 1e3) / 1e9}
     dom = knn if knn_ms >= rad_ms else rad
@@ -403,6 +537,10 @@ def run_b200(args, rank, world, local_rank):
              "depth": info.max_depth_seen, "upload_ms": 1e3 * upload_s,
              "includes": "bbox + encode + 8-bit onesweep sort + reorder + octree build from points resident in "
                          "HBM, host syncs included (wall clock)"}
+
+    batched = None
+    if world == 1 and not args.no_batched:
+        batched = run_batched(args, dev)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -421,8 +559,8 @@ def run_b200(args, rank, world, local_rank):
             "config": workload_config(world, {"search_path": args.search}),
             "radius_qps": chosen["radius_qps"], "knn_qps": chosen["knn_qps"],
             "avg_neighbours": chosen["avg_neighbours"], "paths": paths,
-            "batched_vs_plain": paths["packet"]["qps"] / paths["plain"]["qps"],
-            "build": build, "roofline": roofline, "cpu_baseline": cpu,
+            "batched_vs_plain": paths["engine"]["qps"] / paths["plain"]["qps"], "engine_config": eng_cfg,
+            "build": build, "batched": batched, "roofline": roofline, "cpu_baseline": cpu,
             "e2e": {"value": e2e_val, "unit": "queries/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "detail": e2e_detail},
             "gpu_launches": LAUNCHES_PER_STEP[args.search] * args.steps, "clocks": clk,
@@ -441,11 +579,13 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--radius-group", type=int, default=8, help="lanes per query of the plain path")
     ap.add_argument("--knn-bucket", type=int, default=256, help="kNN: subtrees this small are scanned as one range")
-    ap.add_argument("--search", default="packet", choices=["plain", "packet", "packet_fp32", "knn_packet"],
+    ap.add_argument("--search", default="engine", choices=["plain", "packet", "packet_fp32", "knn_packet", "engine"],
                     help="search path whose numbers are the headline value")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-e2e", action="store_true")
+    ap.add_argument("--no-batched", action="store_true", help="skip the 256-cloud batch")
+    ap.add_argument("--batched-steps", type=int, default=3, help="timed repetitions of the 256-cloud batch")
     ap.add_argument("--points", type=int, default=N_POINTS, help="cloud size (smaller cases for profiling)")
     ap.add_argument("--queries", type=int, default=Q_RADIUS, help="radius and kNN queries per step, each")
     args = ap.parse_args()

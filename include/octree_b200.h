@@ -253,7 +253,8 @@ int oct_engine_destroy(oct_engine engine);
 int oct_engine_set_stream(oct_engine engine, void* cuda_stream);
 int oct_engine_last_error(oct_engine engine, char* buf, size_t len);
 /* Search configuration of the engine (oct_search_config: fp32_filter, knn_bucket;
- * reserved[0] = radius blocks per SM, reserved[1] = kNN blocks per SM, 0 = default). */
+ * reserved[0] = radius blocks per SM, reserved[1] = kNN blocks per SM, 0 = default;
+ * reserved[2] = 1 to run kNN after the radius search instead of beside it). */
 int oct_engine_set_config(oct_engine engine, const oct_search_config* config);
 int oct_engine_get_config(oct_engine engine, oct_search_config* config);
 

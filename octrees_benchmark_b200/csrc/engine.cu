@@ -243,6 +243,7 @@ struct oct_engine_s {
     int fp32 = 0;
     uint32_t bucket = 128;
     int radius_bps = 0, knn_bps = 0;
+    int serial = 0;  // 1: kNN after the radius search on one stream; 0: kNN forked beside it
     // device arrays
     DevBuf desc;  // EngineDyn, then the SearchReq table
     DevBuf keys[2], ord[2];
@@ -354,17 +355,21 @@ cudaError_t enqueue_work(oct_engine e) {
     const bool any_knn = ((e->sig >> kRadiusVariants) & 3ull) != 0;
     uint32_t* ctr = e->ctrs.as<uint32_t>();
     unsigned long long* stats = e->stats.as<unsigned long long>();
-    if (any_knn) {
+    const bool fork = any_knn && !e->serial;
+    auto knn_groups = [&](cudaStream_t ks) -> cudaError_t {
+        cudaError_t r2 = cudaSuccess;
+        for (int v = 0; v < kKnnVariants && r2 == cudaSuccess; ++v) {
+            if (!((e->sig >> (kRadiusVariants + v)) & 1ull)) continue;
+            r2 = launch_knn_table(e->device, ks, &dyn->groups[kRadiusVariants + v], nullptr, 0, v == 0 ? 32u : 64u,
+                                  order, e->bucket, e->knn_idx.as<uint32_t>(), e->knn_d2.as<double>(),
+                                  e->knn_counts.as<uint32_t>(), err, e->knn_bps);
+        }
+        return r2;
+    };
+    if (fork) {
         if ((r = cudaEventRecord(e->ev_fork, s)) != cudaSuccess) return r;
         if ((r = cudaStreamWaitEvent(e->side, e->ev_fork, 0)) != cudaSuccess) return r;
-        for (int v = 0; v < kKnnVariants; ++v) {
-            if (!((e->sig >> (kRadiusVariants + v)) & 1ull)) continue;
-            if ((r = launch_knn_table(e->device, e->side, &dyn->groups[kRadiusVariants + v], nullptr, 0,
-                                      v == 0 ? 32u : 64u, order, e->bucket, e->knn_idx.as<uint32_t>(),
-                                      e->knn_d2.as<double>(), e->knn_counts.as<uint32_t>(), err, e->knn_bps)) !=
-                cudaSuccess)
-                return r;
-        }
+        if ((r = knn_groups(e->side)) != cudaSuccess) return r;
         if ((r = cudaEventRecord(e->ev_join, e->side)) != cudaSuccess) return r;
     }
     if (any_radius) {
@@ -393,7 +398,8 @@ cudaError_t enqueue_work(oct_engine e) {
         const uint32_t cap_req = (uint32_t)(e->totals.bytes / sizeof(ReqTotal));
         k_req_totals<<<(cap_req + tb - 1) / tb, tb, 0, s>>>(dyn, table, offs, e->totals.as<ReqTotal>());
     }
-    if (any_knn && (r = cudaStreamWaitEvent(s, e->ev_join, 0)) != cudaSuccess) return r;
+    if (any_knn && !fork && (r = knn_groups(s)) != cudaSuccess) return r;
+    if (fork && (r = cudaStreamWaitEvent(s, e->ev_join, 0)) != cudaSuccess) return r;
     if ((r = cudaMemcpyAsync(e->h_summary, sum, sizeof(Summary), cudaMemcpyDeviceToHost, s)) != cudaSuccess)
         return r;
     return cudaGetLastError();
@@ -401,7 +407,7 @@ cudaError_t enqueue_work(oct_engine e) {
 
 // Launch the current batch: the captured graph of its shape (captured now if
 // new) or the direct sequence.
-int launch_batch(oct_engine e) {
+int launch_batch(oct_engine e, bool record_start) {
     DeviceGuardE g(e->device);
     if (e->host_epoch + kEpochStep > kEpochLimit) {  // the look-back epochs wrap: clear the status words
         EK(cudaMemsetAsync(e->sort_status.ptr, 0, e->sort_status.bytes, e->stream));
@@ -409,7 +415,7 @@ int launch_batch(oct_engine e) {
         e->host_epoch = 0;
     }
     e->host_epoch += kEpochStep;
-    EK(cudaEventRecord(e->ev_t0, e->stream));
+    if (record_start) EK(cudaEventRecord(e->ev_t0, e->stream));
     const bool use_graph = !(e->flags & OCT_ENGINE_NO_GRAPH) && e->stream != nullptr;
     if (!use_graph) {
         EK(enqueue_work(e));
@@ -473,7 +479,7 @@ int finish(oct_engine e) {
         // the results did not fit: grow the result array and run the batch again
         int st = grow(e, e->out, 4 * (size_t)(sm.radius_total + sm.radius_total / 8 + 1024));
         if (st != OCT_OK) return st;
-        if ((st = launch_batch(e)) != OCT_OK) return st;
+        if ((st = launch_batch(e, true)) != OCT_OK) return st;
     }
     return fail(e, OCT_ERR_CAPACITY, "radius results kept outgrowing the result array");
 }
@@ -638,6 +644,7 @@ int submit(oct_engine e, const oct_request* rq, uint32_t n) {
     e->knn_slots = knn_slots;
     e->nreq = m;
     e->desc_bytes = desc_bytes;
+    EK(cudaEventRecord(e->ev_t0, e->stream));  // the batch's device time starts with its descriptor copy
     EK(cudaMemcpyAsync(e->desc.ptr, e->h_stage, tbl + (size_t)m * sizeof(SearchReq), cudaMemcpyHostToDevice,
                        e->stream));
     if (m == 0) {  // nothing to search
@@ -647,7 +654,7 @@ int submit(oct_engine e, const oct_request* rq, uint32_t n) {
         e->have_results = true;
         return OCT_OK;
     }
-    if ((st = launch_batch(e)) != OCT_OK) return st;
+    if ((st = launch_batch(e, false)) != OCT_OK) return st;
     e->in_flight = true;
     return OCT_OK;
 }
@@ -758,7 +765,7 @@ int oct_engine_last_error(oct_engine e, char* buf, size_t len) {
 int oct_engine_set_config(oct_engine e, const oct_search_config* cfg) {
     if (!e || !cfg) return OCT_ERR_INVALID_ARG;
     if (cfg->knn_bucket < 0 || cfg->reserved[0] < 0 || cfg->reserved[0] > 16 || cfg->reserved[1] < 0 ||
-        cfg->reserved[1] > 16)
+        cfg->reserved[1] > 16 || cfg->reserved[2] < 0 || cfg->reserved[2] > 1)
         return fail(e, OCT_ERR_INVALID_ARG, "bad engine configuration");
     if (e->in_flight) {
         const int st = finish(e);
@@ -767,12 +774,13 @@ int oct_engine_set_config(oct_engine e, const oct_search_config* cfg) {
     const int fp32 = cfg->fp32_filter ? 1 : 0;
     const uint32_t bucket = (uint32_t)cfg->knn_bucket;
     if (fp32 != e->fp32 || bucket != e->bucket || cfg->reserved[0] != e->radius_bps ||
-        cfg->reserved[1] != e->knn_bps)
+        cfg->reserved[1] != e->knn_bps || cfg->reserved[2] != e->serial)
         drop_graphs(e);
     e->fp32 = fp32;
     e->bucket = bucket;
     e->radius_bps = cfg->reserved[0];
     e->knn_bps = cfg->reserved[1];
+    e->serial = cfg->reserved[2];
     return OCT_OK;
 }
 
@@ -785,6 +793,7 @@ int oct_engine_get_config(oct_engine e, oct_search_config* cfg) {
     cfg->knn_bucket = (int32_t)e->bucket;
     cfg->reserved[0] = e->radius_bps;
     cfg->reserved[1] = e->knn_bps;
+    cfg->reserved[2] = e->serial;
     return OCT_OK;
 }
 
@@ -944,6 +953,23 @@ int oct_engine_autotune(oct_engine e, const oct_request* rq, uint32_t n, oct_sea
             }
         cfg.knn_bucket = pick.knn_bucket;
         cfg.reserved[1] = pick.reserved[1];
+    }
+    if (!radius.empty() && !knn.empty()) {  // kNN beside the radius search, or after it
+        std::vector<oct_request> all(rq, rq + n);
+        float best = 1e30f;
+        int pick = 0;
+        for (int ser = 0; ser < 2; ++ser) {
+            oct_search_config c2 = cfg;
+            c2.reserved[2] = ser;
+            if ((st = oct_engine_set_config(e, &c2)) != OCT_OK) return st;
+            float t;
+            if ((st = time_cfg(all, &t)) != OCT_OK) return st;
+            if (t < best) {
+                best = t;
+                pick = ser;
+            }
+        }
+        cfg.reserved[2] = pick;
     }
     if ((st = oct_engine_set_config(e, &cfg)) != OCT_OK) return st;
     if (chosen) *chosen = cfg;

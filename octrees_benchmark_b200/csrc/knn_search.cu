@@ -345,6 +345,8 @@ struct KnnTableArgs {
 };
 
 #define KRQ(f) (MULTI ? reqs[ri].f : a.single.f)
+// cloud pointers of the warp's current request: shared memory in a table launch
+#define KRQV(f) (MULTI ? s_view[warp].f : a.single.cv.f)
 template <int R, bool MULTI>
 __global__ void __launch_bounds__(kKnnThreads) k_knn_reg(KnnTableArgs a) {
     __shared__ uint32_t st_a[kKnnWarps][kKnnStack];   // leaf: first point; internal: first child
@@ -354,6 +356,7 @@ __global__ void __launch_bounds__(kKnnThreads) k_knn_reg(KnnTableArgs a) {
     __shared__ double s_rad[kKnnWarps][kMaxDepth + 1][3];
     __shared__ double s_bd[kKnnWarps][32];
     __shared__ uint32_t s_bi[kKnnWarps][32];
+    __shared__ CloudView s_view[MULTI ? kKnnWarps : 1];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     double (*s_radii)[3] = s_rad[warp];
     uint32_t cur_cloud = 0xffffffffu;
@@ -387,6 +390,7 @@ __global__ void __launch_bounds__(kKnnThreads) k_knn_reg(KnnTableArgs a) {
             __syncwarp();
             const double* gr = &KRQ(cv.geom)->radii[0][0];
             for (int t = lane; t < (kMaxDepth + 1) * 3; t += 32) (&s_radii[0][0])[t] = gr[t];
+            if (MULTI && lane == 0) s_view[warp] = reqs[ri].cv;
             cur_cloud = KRQ(cloud_id);
             __syncwarp();
         }
@@ -419,8 +423,8 @@ __global__ void __launch_bounds__(kKnnThreads) k_knn_reg(KnnTableArgs a) {
         };
         // root (bound 0, linear_octree.hpp:904)
         {
-            const uint32_t fc0 = KRQ(cv.offsets)[0];
-            const uint2 rg0 = KRQ(cv.ranges)[0];
+            const uint32_t fc0 = KRQV(offsets)[0];
+            const uint2 rg0 = KRQV(ranges)[0];
             const bool scan0 = fc0 == 0 || rg0.y - rg0.x <= a.bucket;
             if (lane == 0) {
                 sa[0] = scan0 ? rg0.x : fc0;
@@ -445,7 +449,7 @@ __global__ void __launch_bounds__(kKnnThreads) k_knn_reg(KnnTableArgs a) {
                     double d = INFINITY;
                     bool cand = false;
                     if (i < eb) {
-                        d = dist_pp(p[0], p[1], p[2], KRQ(cv.xs)[i], KRQ(cv.ys)[i], KRQ(cv.zs)[i]);
+                        d = dist_pp(p[0], p[1], p[2], KRQV(xs)[i], KRQV(ys)[i], KRQV(zs)[i]);
                         cand = pair_less(d, i, thr, thr_i);
                     }
                     uint32_t m = __ballot_sync(0xffffffffu, cand);
@@ -472,9 +476,9 @@ __global__ void __launch_bounds__(kKnnThreads) k_knn_reg(KnnTableArgs a) {
             uint32_t ca = 0, cb = 0;
             if (lane < 8) {
                 const uint32_t child = fc + lane;
-                clb = dist_po(p, KRQ(cv.centers) + 3ull * child, s_radii[cd]);
-                const uint32_t cfc = KRQ(cv.offsets)[child];
-                const uint2 rg = KRQ(cv.ranges)[child];
+                clb = dist_po(p, KRQV(centers) + 3ull * child, s_radii[cd]);
+                const uint32_t cfc = KRQV(offsets)[child];
+                const uint2 rg = KRQV(ranges)[child];
                 if (cfc && rg.y - rg.x > a.bucket) {
                     ca = cfc;
                     cb = 0xffffffffu;

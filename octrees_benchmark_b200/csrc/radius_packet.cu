@@ -120,10 +120,52 @@ __device__ __forceinline__ int f32_test(const LeafCtx& c, float4 p) {
 }
 
 // MULTI: the launch covers a request table; otherwise the single request is read
-// from the kernel parameters (constant-bank operands, no registers held).
+// from the kernel parameters (constant-bank operands, no registers held).  In
+// a table launch the cloud pointers of the warp's current request live in
+// shared memory (RQV), so the hot loops do not re-load them from the table.
 #define RQ(f) (MULTI ? reqs[cur_req].f : a.single.f)
+#define RQV(f) (MULTI ? s_view[warp].f : a.single.cv.f)
+
+// Query parameters of lane j for the transposed leaf test: sphere / circle
+// (c0, c1, c2, r2), cube / square (bmin0..2, bmax0..2).
+template <int KT>
+__device__ __forceinline__ void put_query(double (*q)[32], int lane, const SearchKernel& k) {
+    if constexpr (KT == kSphere || KT == kCircle) {
+        q[0][lane] = k.c[0];
+        q[1][lane] = k.c[1];
+        q[2][lane] = k.c[2];
+        q[3][lane] = k.r2;
+    } else {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            q[a][lane] = k.bmin[a];
+            q[3 + a][lane] = k.bmax[a];
+        }
+    }
+}
+
+// is_inside of lane j's query for point p: the same expressions, operand for operand.
+template <int KT>
+__device__ __forceinline__ bool inside_of(const double (*q)[32], int j, double px, double py, double pz) {
+    if constexpr (KT == kSphere) {
+        return dsq3(dsub(px, q[0][j]), dsub(py, q[1][j]), dsub(pz, q[2][j])) < q[3][j];
+    } else if constexpr (KT == kCircle) {
+        return dsq2(dsub(px, q[0][j]), dsub(py, q[1][j])) <= q[3][j];
+    } else if constexpr (KT == kCube) {
+        return px >= q[0][j] && px <= q[3][j] && py >= q[1][j] && py <= q[4][j] && pz >= q[2][j] && pz <= q[5][j];
+    } else {
+        return px >= q[0][j] && px <= q[3][j] && py >= q[1][j] && py <= q[4][j];
+    }
+}
+
 template <int KT, int ALGO, bool FILL, bool F32, bool MULTI>
 __global__ void __launch_bounds__(kPkThreads) k_radius_packet(PacketArgs a) {
+    // Transposed leaf test (FP64, neighbors / neighborsPrune): the lanes hold
+    // consecutive points and test them against one query of the mask at a time,
+    // so every lane does useful work and the ballot is that query's hit mask.
+    constexpr bool kT = (ALGO != kStruct) && !F32;
+    constexpr int kStage = kT ? 1 : kPkWarps;  // point staging, per-lane loop forms only
+    __shared__ CloudView s_view[MULTI ? kPkWarps : 1];
     __shared__ uint32_t st_node[kPkWarps][kPkStack];
     __shared__ uint32_t st_fc[kPkWarps][kPkStack];     // first child, 0 for a leaf
     __shared__ uint2 st_rg[kPkWarps][kPkStack];        // point range
@@ -131,8 +173,9 @@ __global__ void __launch_bounds__(kPkThreads) k_radius_packet(PacketArgs a) {
     __shared__ uint32_t st_in[kPkWarps][kPkStack];
     __shared__ uint8_t st_depth[kPkWarps][kPkStack];
     __shared__ double s_rad[kPkWarps][kMaxDepth + 1][3];
-    __shared__ double sx[kPkWarps][32], sy[kPkWarps][32], sz[kPkWarps][32];
-    __shared__ float4 sp[kPkWarps][32];
+    __shared__ double s_qp[kT ? kPkWarps : 1][6][32];
+    __shared__ double sx[kStage][32], sy[kStage][32], sz[kStage][32];
+    __shared__ float4 sp[F32 ? kPkWarps : 1][32];
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     double (*s_radii)[3] = s_rad[warp];
@@ -170,10 +213,11 @@ __global__ void __launch_bounds__(kPkThreads) k_radius_packet(PacketArgs a) {
             }
             cur_req = lo;
         }
-        if (RQ(cloud_id) != cur_cloud) {  // this warp's level radii follow the packet's cloud
+        if (RQ(cloud_id) != cur_cloud) {  // this warp's level radii and cloud follow the packet's cloud
             __syncwarp();
             const double* gr = &RQ(cv.geom)->radii[0][0];
             for (int t = lane; t < (kMaxDepth + 1) * 3; t += 32) (&s_radii[0][0])[t] = gr[t];
+            if (MULTI && lane == 0) s_view[warp] = reqs[cur_req].cv;
             cur_cloud = RQ(cloud_id);
             __syncwarp();
         }
@@ -187,6 +231,7 @@ __global__ void __launch_bounds__(kPkThreads) k_radius_packet(PacketArgs a) {
         const double* qrad = RQ(radii);
         SearchKernel k;
         k.init(qc[3 * ql], qc[3 * ql + 1], qc[3 * ql + 2], qrad ? qrad[ql] : RQ(radius));
+        if constexpr (kT) put_query<KT>(s_qp[warp], lane, k);  // read by the other lanes after a __syncwarp
         unsigned long long cnt = 0, cnt2 = 0, base = 0;
         if (FILL && valid) base = a.offs[qi];
         bool overflow = false;
@@ -238,29 +283,61 @@ __global__ void __launch_bounds__(kPkThreads) k_radius_packet(PacketArgs a) {
             }
         };
         auto scan_leaf = [&](uint32_t node, uint2 rg, uint32_t mask) {
+            if constexpr (kT) {
+                (void)node;
+                for (uint32_t b = rg.x; b < rg.y; b += 32) {
+                    const uint32_t idx = b + lane;
+                    const bool in_range = idx < rg.y;
+                    double px = 0.0, py = 0.0, pz = 0.0;
+                    if (in_range) {
+                        px = RQV(xs)[idx];
+                        py = RQV(ys)[idx];
+                        pz = RQV(zs)[idx];
+                    }
+                    uint32_t rem = mask;
+                    while (rem) {
+                        const int j = __ffs(rem) - 1;
+                        rem &= rem - 1;
+                        const bool in = in_range && inside_of<KT>(s_qp[warp], j, px, py, pz);
+                        const uint32_t hb = __ballot_sync(0xffffffffu, in);
+                        if (FILL && hb) {  // query j's hits, ascending, in one coalesced store
+                            const unsigned long long o0 = __shfl_sync(0xffffffffu, base + cnt, j);
+                            if (in) {
+                                const unsigned long long o = o0 + __popc(hb & lanemask_lt());
+                                if (o < a.out_cap) a.out[o] = idx;
+                                else overflow = true;
+                            }
+                        }
+                        if (lane == j) cnt += __popc(hb);
+                    }
+                    if (lane == 0) n_tests += (unsigned long long)__popc(mask) * ((rg.y - b < 32u) ? (rg.y - b) : 32u);
+                }
+            } else {
             const bool mine = (mask & lbit) != 0;
             LeafCtx ctx;
-            if (F32 && mine) leaf_ctx<KT>(k, RQ(cv.centers) + 3ull * node, ctx);
+            if (F32 && mine) leaf_ctx<KT>(k, RQV(centers) + 3ull * node, ctx);
             for (uint32_t b = rg.x; b < rg.y; b += 32) {
                 const uint32_t idx = b + lane;
                 if (idx < rg.y) {
-                    if (F32) {
-                        sp[warp][lane] = RQ(cv.rel)[idx];
+                    if constexpr (F32) {
+                        sp[warp][lane] = RQV(rel)[idx];
                     } else {
-                        sx[warp][lane] = RQ(cv.xs)[idx];
-                        sy[warp][lane] = RQ(cv.ys)[idx];
-                        sz[warp][lane] = RQ(cv.zs)[idx];
+                        sx[warp][lane] = RQV(xs)[idx];
+                        sy[warp][lane] = RQV(ys)[idx];
+                        sz[warp][lane] = RQV(zs)[idx];
                     }
                 }
                 __syncwarp();
                 const uint32_t m = (rg.y - b < 32u) ? (rg.y - b) : 32u;
+                // bit t: staged point t is inside this lane's query
+                uint32_t hits = 0;
                 if (mine) {
                     for (uint32_t t = 0; t < m; ++t) {
                         bool in;
-                        if (F32) {
+                        if constexpr (F32) {
                             const int r = f32_test<KT>(ctx, sp[warp][t]);
                             if (r < 0) {
-                                in = is_inside<KT>(k, RQ(cv.xs)[b + t], RQ(cv.ys)[b + t], RQ(cv.zs)[b + t]);
+                                in = is_inside<KT>(k, RQV(xs)[b + t], RQV(ys)[b + t], RQV(zs)[b + t]);
                                 ++n_retests;
                             } else {
                                 in = r > 0;
@@ -268,9 +345,27 @@ __global__ void __launch_bounds__(kPkThreads) k_radius_packet(PacketArgs a) {
                         } else {
                             in = is_inside<KT>(k, sx[warp][t], sy[warp][t], sz[warp][t]);
                         }
-                        hit(b + t, in);
+                        if constexpr (ALGO == kStruct) hit(b + t, in);
+                        else hits |= (uint32_t)in << t;
                     }
                     n_tests += m;
+                }
+                if constexpr (ALGO != kStruct) {
+                    if (FILL) {  // every lane's hits in one coalesced store, lane after lane
+                        uint32_t rem = __ballot_sync(0xffffffffu, hits != 0);
+                        while (rem) {
+                            const int j = __ffs(rem) - 1;
+                            rem &= rem - 1;
+                            const uint32_t hj = __shfl_sync(0xffffffffu, hits, j);
+                            const unsigned long long o0 = __shfl_sync(0xffffffffu, base + cnt, j);
+                            if ((hj >> lane) & 1u) {
+                                const unsigned long long o = o0 + __popc(hj & lanemask_lt());
+                                if (o < a.out_cap) a.out[o] = b + lane;
+                                else overflow = true;
+                            }
+                        }
+                    }
+                    cnt += __popc(hits);
                 }
                 __syncwarp();
             }
@@ -278,15 +373,16 @@ __global__ void __launch_bounds__(kPkThreads) k_radius_packet(PacketArgs a) {
                 open = false;
                 emit_range(rs, rg.y);
             }
+            }
         };
 
         // root: continuationCriterion(0, 0)
         bool over = false, in = false;
         if (valid) {
             if constexpr (ALGO == kNeighbors) {
-                over = box_overlap<KT>(k, RQ(cv.centers), s_radii[0]);
+                over = box_overlap<KT>(k, RQV(centers), s_radii[0]);
             } else {
-                const int j = box_intersect<KT>(k, RQ(cv.centers), s_radii[0]);
+                const int j = box_intersect<KT>(k, RQV(centers), s_radii[0]);
                 in = (j == kInside);
                 over = (j == kOverlap);
             }
@@ -296,8 +392,8 @@ __global__ void __launch_bounds__(kPkThreads) k_radius_packet(PacketArgs a) {
             const uint32_t mo = __ballot_sync(0xffffffffu, over);
             const uint32_t mi = __ballot_sync(0xffffffffu, in);
             if (mo | mi) {
-                const uint32_t fc0 = RQ(cv.offsets)[0];
-                const uint2 rg0 = RQ(cv.ranges)[0];
+                const uint32_t fc0 = RQV(offsets)[0];
+                const uint2 rg0 = RQV(ranges)[0];
                 if (lane == 0) {
                     sn[0] = 0;
                     sf[0] = fc0;
@@ -319,7 +415,27 @@ __global__ void __launch_bounds__(kPkThreads) k_radius_packet(PacketArgs a) {
             const uint32_t mi = si[sp_top];
             const uint32_t depth = sd[sp_top];
             __syncwarp();
-            if (mi & lbit) emit_range(nrg.x, nrg.y);
+            if constexpr (ALGO == kStruct) {
+                if (mi & lbit) emit_range(nrg.x, nrg.y);
+            } else if (mi) {
+                // a fully-inside node: every lane of mi adds the node's whole range; the
+                // warp writes it for one lane at a time, 32 consecutive indices per store
+                const uint32_t len = nrg.y - nrg.x;
+                if (FILL) {
+                    uint32_t rem = mi;
+                    while (rem) {
+                        const int j = __ffs(rem) - 1;
+                        rem &= rem - 1;
+                        const unsigned long long o0 = __shfl_sync(0xffffffffu, base + cnt, j);
+                        for (uint32_t t = lane; t < len; t += 32) {
+                            const unsigned long long o = o0 + t;
+                            if (o < a.out_cap) a.out[o] = nrg.x + t;
+                            else overflow = true;
+                        }
+                    }
+                }
+                if (mi & lbit) cnt += len;
+            }
             if (mo == 0) continue;
             if (fc == 0) {
                 scan_leaf(node, nrg, mo);
@@ -331,14 +447,14 @@ __global__ void __launch_bounds__(kPkThreads) k_radius_packet(PacketArgs a) {
             uint32_t my_fc = 0, my_mo = 0, my_mi = 0;
             uint2 my_rg = make_uint2(0u, 0u);
             if (lane < 8) {
-                my_fc = RQ(cv.offsets)[fc + lane];
-                my_rg = RQ(cv.ranges)[fc + lane];
+                my_fc = RQV(offsets)[fc + lane];
+                my_rg = RQV(ranges)[fc + lane];
             }
 #pragma unroll
             for (int j = 0; j < 8; ++j) {
                 bool o = false, n = false;
                 if (mine) {
-                    const double* oc = RQ(cv.centers) + 3ull * (fc + j);
+                    const double* oc = RQV(centers) + 3ull * (fc + j);
                     if constexpr (ALGO == kNeighbors) {
                         o = box_overlap<KT>(k, oc, s_radii[cd]);
                     } else {

@@ -91,17 +91,18 @@ class BatchEngine:
 
     # ---- configuration ------------------------------------------------------
     def set_config(self, fp32_filter: bool = False, knn_bucket: int = 128, radius_blocks_per_sm: int = 0,
-                   knn_blocks_per_sm: int = 0):
+                   knn_blocks_per_sm: int = 0, serial: bool = False):
         cfg = OctSearchConfig(1, int(bool(fp32_filter)), 32, 0, int(knn_bucket))
         cfg.reserved[0] = int(radius_blocks_per_sm)
         cfg.reserved[1] = int(knn_blocks_per_sm)
+        cfg.reserved[2] = int(bool(serial))
         _engine_check(self._L.oct_engine_set_config(self._h, C.byref(cfg)), self._h, "oct_engine_set_config")
 
     def config(self) -> dict:
         cfg = OctSearchConfig()
         _engine_check(self._L.oct_engine_get_config(self._h, C.byref(cfg)), self._h, "oct_engine_get_config")
         return dict(fp32_filter=cfg.fp32_filter, knn_bucket=cfg.knn_bucket, radius_blocks_per_sm=cfg.reserved[0],
-                    knn_blocks_per_sm=cfg.reserved[1])
+                    knn_blocks_per_sm=cfg.reserved[1], serial=cfg.reserved[2])
 
     def autotune(self, requests: Sequence[Request]) -> dict:
         arr = (OctRequest * max(1, len(requests)))(*[r.to_c() for r in requests])
