@@ -228,7 +228,7 @@ typedef struct {
     int32_t type;          /* oct_request_type */
     int32_t kernel;        /* radius: oct_kernel */
     int32_t algo;          /* radius: OCT_NEIGHBORS or OCT_NEIGHBORS_PRUNE */
-    uint32_t k;            /* kNN: 1..64 */
+    uint32_t k;            /* kNN: 1..1024 */
     const double* centers; /* nq x 3 */
     uint64_t nq;
     const double* radii;   /* radius: nq per-centre radii, or NULL to use `radius` */
@@ -285,6 +285,80 @@ int oct_engine_copy_knn(oct_engine engine, const oct_request_place* place, uint3
 int oct_engine_autotune(oct_engine engine, const oct_request* requests, uint32_t n, oct_search_config* chosen);
 /* Device time (ms) of the last completed batch, from events around its launch sequence. */
 int oct_engine_last_ms(oct_engine engine, float* ms);
+/* *ready = 1 when the submitted batch has finished on the device (oct_engine_wait will not block). */
+int oct_engine_ready(oct_engine engine, int* ready);
+/* Device bytes the engine's arrays hold. */
+int oct_engine_memory(oct_engine engine, uint64_t* bytes);
+/* Device bytes a cloud holds (points, keys, tree, search scratch). */
+int oct_cloud_memory(oct_cloud cloud, uint64_t* bytes);
+
+/* ---- Serving: continuous batching over device-resident clouds ------------
+ *
+ * No reference counterpart.  A server owns `slots` engines, each on its own
+ * stream.  Clients submit requests from any thread; a scheduler thread forms a
+ * batch from the queue (arrival order) whenever a slot is free, admitting
+ * requests while the registered clouds, the batches in flight and the new
+ * batch fit the HBM budget (a request that does not fit waits: an admission
+ * stall), and launches it.  Batches on different slots overlap on the device.
+ * A completed request's results stay in its slot until the client releases
+ * the ticket; a slot is reused once all its tickets are released.  With
+ * OCT_SERVER_PLAIN the server instead runs one request per launch through the
+ * single-cloud path, first come first served (the baseline). */
+typedef struct oct_server_s* oct_server;
+
+#define OCT_SERVER_PLAIN 0x1u /* one request per launch, single-cloud plain path */
+#define OCT_CLOUD_OWNED 0x1u  /* oct_server_add_cloud: the server destroys the cloud when it evicts or removes it */
+
+typedef struct {
+    int32_t device;
+    uint32_t flags;              /* OCT_SERVER_* */
+    uint32_t slots;              /* batches in flight at once; 0: 3 */
+    uint32_t max_batch_requests; /* 0: 1024 */
+    uint64_t max_batch_queries;  /* 0: 4M */
+    uint64_t hbm_budget;         /* bytes for the clouds and the admitted batches; 0: 120 GB */
+} oct_server_params;
+
+typedef struct {
+    uint64_t ticket;
+    int32_t status;    /* oct_status of the request */
+    int32_t type;      /* oct_request_type */
+    uint64_t nq;
+    uint64_t n_results; /* radius: neighbours of the request */
+    double queue_ms;   /* submit to launch */
+    double latency_ms; /* submit to results complete on the device */
+} oct_completion;
+
+typedef struct {
+    uint64_t submitted, completed, batches, admission_stalls, evictions, queries;
+    uint64_t cloud_bytes, inflight_bytes, peak_bytes;
+    uint32_t queued, in_flight;
+} oct_server_stats;
+
+int oct_server_create(const oct_server_params* params, oct_server* out);
+int oct_server_destroy(oct_server server);
+int oct_server_last_error(oct_server server, char* buf, size_t len);
+/* Search configuration of every slot (as oct_engine_set_config). */
+int oct_server_set_config(oct_server server, const oct_search_config* config);
+/* Register a built cloud (its bytes count against the budget).  When it does
+ * not fit, idle clouds added with OCT_CLOUD_OWNED are evicted, least recently
+ * used first; OCT_ERR_OUT_OF_MEMORY if that is not enough. */
+int oct_server_add_cloud(oct_server server, oct_cloud cloud, uint32_t flags);
+/* Unregister a cloud once no queued or running request uses it. */
+int oct_server_remove_cloud(oct_server server, oct_cloud cloud);
+/* Queue a request on a registered cloud (centres as oct_engine_submit: device
+ * memory, valid until the request completes).  For admission, a radius
+ * request with per-centre radii should set `radius` to their maximum. */
+int oct_server_submit(oct_server server, const oct_request* request, uint64_t* ticket);
+/* Completed requests, up to max; waits up to wait_ms for the first one. */
+int oct_server_poll(oct_server server, oct_completion* out, uint32_t max, uint32_t* n, int32_t wait_ms);
+/* A completed request's results, as oct_engine_copy_radius / oct_engine_copy_knn. */
+int oct_server_copy_radius(oct_server server, uint64_t ticket, uint64_t* offsets, uint32_t* idx,
+                           uint64_t idx_capacity, uint32_t flags);
+int oct_server_copy_knn(oct_server server, uint64_t ticket, uint32_t* idx, double* d2, uint32_t* counts,
+                        uint32_t flags);
+/* The client is done with a completed request's results. */
+int oct_server_release(oct_server server, uint64_t ticket);
+int oct_server_get_stats(oct_server server, oct_server_stats* stats);
 
 /* Largest cloud oct_encode_sort_noalloc accepts. */
 #define OCT_NOALLOC_MAX_POINTS (1u << 18) /* 262,144 points */

@@ -302,6 +302,20 @@ int oct_search_stats(oct_cloud h, uint64_t* point_tests, uint64_t* fp64_retests,
     return OCT_OK;
 }
 
+int oct_cloud_memory(oct_cloud h, uint64_t* bytes) {
+    if (!h || !bytes) return OCT_ERR_INVALID_ARG;
+    Cloud& c = h->c;
+    const DevBuf* bufs[] = {&c.xyz_in, &c.xs, &c.ys, &c.zs, &c.keys, &c.keys_alt, &c.perm, &c.perm_alt,
+                            &c.sort_status, &c.d_ctl, &c.d_box, &c.d_err, &c.offsets, &c.ranges, &c.centers,
+                            &c.frontier, &c.masks, &c.parts, &c.d_build, &c.q_centers, &c.q_radii, &c.q_counts,
+                            &c.q_offsets, &c.q_out, &c.q_out2, &c.q_scan_tmp, &c.qs_keys, &c.qs_keys_alt, &c.qs_ord,
+                            &c.qs_ord_alt, &c.qs_status, &c.qs_ctl, &c.packet_ctr, &c.stats, &c.rel};
+    uint64_t s = 0;
+    for (const DevBuf* b : bufs) s += b->bytes;
+    *bytes = s;
+    return OCT_OK;
+}
+
 int oct_set_points(oct_cloud h, const double* xyz, uint64_t n, uint32_t flags) {
     if (!h) return OCT_ERR_INVALID_ARG;
     Cloud& c = h->c;

@@ -179,14 +179,17 @@ cudaError_t launch_radius_table(int device, cudaStream_t s, int kernel, int algo
                                 const unsigned long long* d_offsets, uint32_t* d_out, uint64_t out_capacity,
                                 uint32_t* d_packet_ctr, unsigned long long* d_stats, uint32_t* d_err,
                                 int blocks_per_sm = 0);
-// Register kNN (k <= 64), one warp per query.  Either one request (`single`,
-// nq queries) or the group of a batch (`d_grp`, kmax = the group's largest k).
+// kNN, one warp per query.  Either one request (`single`, nq queries, k <= 64,
+// register lists) or the group of a batch (`d_grp`, kmax = the group's largest
+// k: register lists up to 64, shared-memory lists up to 1024).
 cudaError_t launch_knn_table(int device, cudaStream_t s, const DynGroup* d_grp, const SearchReq* single, uint64_t nq,
                              uint32_t kmax, const uint32_t* d_order, uint32_t bucket, uint32_t* d_idx, double* d_d2,
                              uint32_t* d_counts, uint32_t* d_err, int blocks_per_sm = 0);
 CloudView cloud_view(const Cloud& c);
-// Batched engine: the sort of query keys with device-side sizes (encode_sort.cu).
+// Batched engine: the sort of query keys with device-side sizes (encode_sort.cu),
+// and the shared-memory limits of the table kNN list kernels (knn_search.cu).
 cudaError_t prepare_sort_dyn();
+cudaError_t prepare_knn_dyn();
 size_t sort_tile_keys();
 cudaError_t launch_sort_dyn(int device, cudaStream_t s, uint64_t* k0, uint64_t* k1, uint32_t* v0, uint32_t* v1,
                             const uint64_t* d_n, uint64_t max_n, int passes, SortCtl* ctl,

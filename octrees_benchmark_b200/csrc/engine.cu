@@ -37,7 +37,7 @@ using namespace octb;
 namespace {
 
 constexpr int kRadiusVariants = 16;  // kernel (4) x algo (neighbors, prune) x FP32 filter (2)
-constexpr int kKnnVariants = 2;      // k <= 32 (one register pair per lane), k <= 64 (two)
+constexpr int kKnnVariants = 6;      // k <= 32, 64 (register lists), 128, 256, 512, 1024 (shared-memory lists)
 constexpr int kGroups = kRadiusVariants + kKnnVariants;
 constexpr int kScanBlocks = 296;
 constexpr int kScanThreads = 256;
@@ -352,7 +352,7 @@ cudaError_t enqueue_work(oct_engine e) {
         return r;
     const uint64_t radius_bits = (1ull << kRadiusVariants) - 1;
     const bool any_radius = (e->sig & radius_bits) != 0;
-    const bool any_knn = ((e->sig >> kRadiusVariants) & 3ull) != 0;
+    const bool any_knn = ((e->sig >> kRadiusVariants) & ((1ull << kKnnVariants) - 1)) != 0;
     uint32_t* ctr = e->ctrs.as<uint32_t>();
     unsigned long long* stats = e->stats.as<unsigned long long>();
     const bool fork = any_knn && !e->serial;
@@ -360,7 +360,7 @@ cudaError_t enqueue_work(oct_engine e) {
         cudaError_t r2 = cudaSuccess;
         for (int v = 0; v < kKnnVariants && r2 == cudaSuccess; ++v) {
             if (!((e->sig >> (kRadiusVariants + v)) & 1ull)) continue;
-            r2 = launch_knn_table(e->device, ks, &dyn->groups[kRadiusVariants + v], nullptr, 0, v == 0 ? 32u : 64u,
+            r2 = launch_knn_table(e->device, ks, &dyn->groups[kRadiusVariants + v], nullptr, 0, 32u << v,
                                   order, e->bucket, e->knn_idx.as<uint32_t>(), e->knn_d2.as<double>(),
                                   e->knn_counts.as<uint32_t>(), err, e->knn_bps);
         }
@@ -496,7 +496,7 @@ int validate(oct_engine e, const oct_request& r) {
         if (r.algo != OCT_NEIGHBORS && r.algo != OCT_NEIGHBORS_PRUNE)
             return fail(e, OCT_ERR_INVALID_ARG, "batched radius requests take neighbors or neighborsPrune");
     } else if (r.type == OCT_REQ_KNN) {
-        if (r.k < 1 || r.k > 64) return fail(e, OCT_ERR_INVALID_ARG, "batched kNN takes 1 <= k <= 64");
+        if (r.k < 1 || r.k > 1024) return fail(e, OCT_ERR_INVALID_ARG, "batched kNN takes 1 <= k <= 1024");
     } else {
         return fail(e, OCT_ERR_INVALID_ARG, "bad request type");
     }
@@ -515,8 +515,9 @@ int submit(oct_engine e, const oct_request* rq, uint32_t n) {
     std::vector<uint32_t> rows;
     rows.reserve(n);
     for (uint32_t i = 0; i < n; ++i) {
-        var[i] = rq[i].type == OCT_REQ_RADIUS ? radius_variant(rq[i].kernel, rq[i].algo, e->fp32)
-                                              : kRadiusVariants + (rq[i].k <= 32 ? 0 : 1);
+        int kv = 0;
+        while (rq[i].type == OCT_REQ_KNN && (32u << kv) < rq[i].k) ++kv;
+        var[i] = rq[i].type == OCT_REQ_RADIUS ? radius_variant(rq[i].kernel, rq[i].algo, e->fp32) : kRadiusVariants + kv;
         if (rq[i].nq) rows.push_back(i);
     }
     std::stable_sort(rows.begin(), rows.end(), [&](uint32_t a, uint32_t b) { return var[a] < var[b]; });
@@ -693,6 +694,7 @@ int oct_engine_create(const oct_engine_params* p, oct_engine* out) {
     if (r == cudaSuccess) r = cudaEventCreate(&e->ev_t0);
     if (r == cudaSuccess) r = cudaEventCreate(&e->ev_t1);
     if (r == cudaSuccess) r = prepare_sort_dyn();
+    if (r == cudaSuccess) r = prepare_knn_dyn();
     if (r == cudaSuccess) r = e->sort_ctl.reserve(sizeof(SortCtl));
     if (r == cudaSuccess) r = e->epoch.reserve(256);
     if (r == cudaSuccess) r = e->ctrs.reserve(4 * 2 * kRadiusVariants);
@@ -891,6 +893,34 @@ int oct_engine_copy_knn(oct_engine e, const oct_request_place* pl, uint32_t k, u
 int oct_engine_last_ms(oct_engine e, float* ms) {
     if (!e || !ms) return OCT_ERR_INVALID_ARG;
     *ms = e->last_ms;
+    return OCT_OK;
+}
+
+int oct_engine_ready(oct_engine e, int* ready) {
+    if (!e || !ready) return OCT_ERR_INVALID_ARG;
+    if (!e->in_flight) {
+        *ready = 1;
+        return OCT_OK;
+    }
+    DeviceGuardE g(e->device);
+    const cudaError_t r = cudaStreamQuery(e->stream);
+    if (r == cudaErrorNotReady) {
+        *ready = 0;
+        return OCT_OK;
+    }
+    EK(r);
+    *ready = 1;
+    return OCT_OK;
+}
+
+int oct_engine_memory(oct_engine e, uint64_t* bytes) {
+    if (!e || !bytes) return OCT_ERR_INVALID_ARG;
+    const DevBuf* bufs[] = {&e->desc, &e->keys[0], &e->keys[1], &e->ord[0], &e->ord[1], &e->sort_ctl,
+                            &e->sort_status, &e->epoch, &e->counts, &e->offs, &e->part, &e->out, &e->knn_idx,
+                            &e->knn_d2, &e->knn_counts, &e->ctrs, &e->stats, &e->summary, &e->totals};
+    uint64_t s = 0;
+    for (const DevBuf* b : bufs) s += b->bytes;
+    *bytes = s;
     return OCT_OK;
 }
 

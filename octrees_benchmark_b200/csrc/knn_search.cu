@@ -14,6 +14,7 @@
 // a bitonic sort.  All distances are the reference's FP64 expressions, so the
 // returned squared distances are bitwise the reference's, and ordering by
 // (distance, index) resolves ties at the k-th distance by the lowest index.
+#include <algorithm>
 #include <cfloat>
 
 #include "cloud.h"
@@ -44,6 +45,7 @@ struct KnnArgs {
     uint32_t* err;
     const uint32_t* order;  // query visiting order (curve order), or nullptr
     uint32_t bucket;        // subtrees with at most this many points are scanned as one range
+    const DynGroup* grp;    // table launch (k_knn<LCAP, true>): sizes and requests on the device
 };
 
 __device__ __forceinline__ bool pair_less(double da, uint32_t ia, double db, uint32_t ib) {
@@ -75,7 +77,10 @@ __device__ __forceinline__ void warp_bitonic_sort(double* d, uint32_t* ix) {
 }
 
 // LCAP: list capacity (power of two >= k); the candidate buffer has LCAP slots too.
-template <int LCAP>
+// MULTI: a table launch (the batched engine): each query's request gives its
+// cloud (kept per warp in shared memory), k and output slots.
+#define KV(f) (MULTI ? s_view[warp].f : a.f)
+template <int LCAP, bool MULTI>
 __global__ void __launch_bounds__(kKnnThreads) k_knn(KnnArgs a) {
     constexpr int P = 2 * LCAP;
     extern __shared__ __align__(16) unsigned char smem[];
@@ -89,15 +94,52 @@ __global__ void __launch_bounds__(kKnnThreads) k_knn(KnnArgs a) {
     uint32_t* st_node = base_u + (size_t)kKnnWarps * P + (size_t)warp * kKnnStack;
     uint8_t* st_depth =
         reinterpret_cast<uint8_t*>(base_u + (size_t)kKnnWarps * (P + kKnnStack)) + (size_t)warp * kKnnStack;
-    __shared__ double s_radii[kMaxDepth + 1][3];
-    for (int i = threadIdx.x; i < (kMaxDepth + 1) * 3; i += kKnnThreads) (&s_radii[0][0])[i] = (&a.geom->radii[0][0])[i];
-    __syncthreads();
-
-    const uint32_t K = a.k;
+    __shared__ double s_rad[MULTI ? kKnnWarps : 1][kMaxDepth + 1][3];
+    __shared__ CloudView s_view[MULTI ? kKnnWarps : 1];
+    double (*s_radii)[3] = s_rad[MULTI ? warp : 0];
+    if (!MULTI) {
+        for (int i = threadIdx.x; i < (kMaxDepth + 1) * 3; i += kKnnThreads)
+            (&s_radii[0][0])[i] = (&a.geom->radii[0][0])[i];
+        __syncthreads();
+    }
+    const SearchReq* reqs = nullptr;
+    uint32_t nreq = 1, cur_cloud = 0xffffffffu;
+    uint64_t q0 = 0, nq = a.nq;
+    if (MULTI) {
+        reqs = a.grp->reqs;
+        nreq = a.grp->nreq;
+        q0 = a.grp->q_begin;
+        nq = a.grp->nq;
+    }
     const uint64_t nwarps = (uint64_t)gridDim.x * kKnnWarps;
-    for (uint64_t qpos = (uint64_t)blockIdx.x * kKnnWarps + warp; qpos < a.nq; qpos += nwarps) {
+    for (uint64_t w = (uint64_t)blockIdx.x * kKnnWarps + warp; w < nq; w += nwarps) {
+        const uint64_t qpos = q0 + w;
         const uint64_t q = a.order ? a.order[qpos] : qpos;
-        const double p[3] = {a.q[3 * q], a.q[3 * q + 1], a.q[3 * q + 2]};
+        uint32_t K = a.k;
+        uint64_t o = q * (uint64_t)K;  // first output slot of this query
+        const double* qc = a.q + 3 * q;
+        if (MULTI) {  // the request whose positions contain qpos (q_begin ascending)
+            uint32_t lo = 0, hi = nreq;
+            while (hi - lo > 1) {
+                const uint32_t mid = (lo + hi) >> 1;
+                if (reqs[mid].q_begin <= qpos) lo = mid;
+                else hi = mid;
+            }
+            const SearchReq& rq = reqs[lo];
+            if (rq.cloud_id != cur_cloud) {
+                __syncwarp();
+                const double* gr = &rq.cv.geom->radii[0][0];
+                for (int t = lane; t < (kMaxDepth + 1) * 3; t += 32) (&s_radii[0][0])[t] = gr[t];
+                if (lane == 0) s_view[warp] = rq.cv;
+                cur_cloud = rq.cloud_id;
+                __syncwarp();
+            }
+            K = rq.k;
+            const uint64_t ql = q - rq.q_begin;
+            o = rq.out_begin + ql * (uint64_t)K;
+            qc = rq.centers + 3 * ql;
+        }
+        const double p[3] = {qc[0], qc[1], qc[2]};
         for (int i = lane; i < P; i += 32) {
             sd[i] = INFINITY;
             si[i] = 0xffffffffu;
@@ -140,16 +182,16 @@ __global__ void __launch_bounds__(kKnnThreads) k_knn(KnnArgs a) {
             const uint32_t depth = st_depth[sp];
             __syncwarp();
             if (lb > thr) continue;
-            const uint32_t fc = a.offsets[node];
+            const uint32_t fc = KV(offsets)[node];
             if (fc == 0) {
                 // leaf: distances of its points, candidates into the buffer
-                const uint2 rg = a.ranges[node];
+                const uint2 rg = KV(ranges)[node];
                 for (uint32_t b = rg.x; b < rg.y; b += 32) {
                     const uint32_t i = b + lane;
                     double d = INFINITY;
                     bool cand = false;
                     if (i < rg.y) {
-                        d = dist_pp(p[0], p[1], p[2], a.xs[i], a.ys[i], a.zs[i]);
+                        d = dist_pp(p[0], p[1], p[2], KV(xs)[i], KV(ys)[i], KV(zs)[i]);
                         cand = pair_less(d, i, thr, thr_i);
                     }
                     uint32_t m = __ballot_sync(0xffffffffu, cand);
@@ -172,7 +214,7 @@ __global__ void __launch_bounds__(kKnnThreads) k_knn(KnnArgs a) {
                 double clb = INFINITY;
                 bool keep = false;
                 if (lane < 8) {
-                    clb = dist_po(p, a.centers + 3ull * (fc + lane), s_radii[cd]);
+                    clb = dist_po(p, KV(centers) + 3ull * (fc + lane), s_radii[cd]);
                     keep = !(clb > thr);
                 }
                 const uint32_t km = __ballot_sync(0xffffffffu, keep) & 0xffu;
@@ -201,7 +243,6 @@ __global__ void __launch_bounds__(kKnnThreads) k_knn(KnnArgs a) {
         }
         if (failed) set_err(a.err, kErrStackOverflow);
         if (nb > 0) merge();
-        const uint64_t o = q * (uint64_t)K;
         for (uint32_t j = lane; j < K; j += 32) {
             if (j < nl) {
                 a.idx[o + j] = si[j];
@@ -226,9 +267,24 @@ size_t knn_smem() {
 template <int LCAP>
 cudaError_t launch_l(const KnnArgs& a, int grid, cudaStream_t s) {
     const size_t smem = knn_smem<LCAP>();
-    cudaError_t e = cudaFuncSetAttribute(k_knn<LCAP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaError_t e = cudaFuncSetAttribute(k_knn<LCAP, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    k_knn<LCAP><<<grid, kKnnThreads, smem, s>>>(a);
+    k_knn<LCAP, false><<<grid, kKnnThreads, smem, s>>>(a);
+    return cudaGetLastError();
+}
+
+// Table launch of the list kernel (the engine's kNN groups with 64 < k <= LCAP).
+template <int LCAP>
+cudaError_t launch_l_table(const DynGroup* d_grp, const uint32_t* order, uint32_t* idx, double* d2, uint32_t* counts,
+                           uint32_t* err, int grid, cudaStream_t s) {
+    KnnArgs a{};
+    a.grp = d_grp;
+    a.order = order;
+    a.idx = idx;
+    a.d2 = d2;
+    a.counts = counts;
+    a.err = err;
+    k_knn<LCAP, true><<<grid, kKnnThreads, knn_smem<LCAP>(), s>>>(a);
     return cudaGetLastError();
 }
 
@@ -348,7 +404,7 @@ struct KnnTableArgs {
 // cloud pointers of the warp's current request: shared memory in a table launch
 #define KRQV(f) (MULTI ? s_view[warp].f : a.single.cv.f)
 template <int R, bool MULTI>
-__global__ void __launch_bounds__(kKnnThreads) k_knn_reg(KnnTableArgs a) {
+__global__ void __launch_bounds__(kKnnThreads, 8) k_knn_reg(KnnTableArgs a) {
     __shared__ uint32_t st_a[kKnnWarps][kKnnStack];   // leaf: first point; internal: first child
     __shared__ uint32_t st_b[kKnnWarps][kKnnStack];   // leaf: end point; internal: 0xffffffff
     __shared__ double st_lb[kKnnWarps][kKnnStack];
@@ -779,10 +835,21 @@ cudaError_t launch_knn_table(int device, cudaStream_t s, const DynGroup* d_grp, 
     a.d2 = d_d2;
     a.counts = d_counts;
     a.err = d_err;
-    const uint64_t cap = (uint64_t)sm_count_k(device) * (blocks_per_sm > 0 ? blocks_per_sm : 16);
+    const int sms = sm_count_k(device);
+    const uint64_t cap = (uint64_t)sms * (blocks_per_sm > 0 ? blocks_per_sm : 16);
     const uint64_t want = d_grp ? cap : (nq + kKnnWarps - 1) / kKnnWarps;
     const int grid = (int)(want < cap ? want : cap);
     if (d_grp) {
+        if (kmax > 64) {  // the shared-memory list kernel, blocks per SM as its list fits
+            auto lgrid = [&](size_t smem) { return sms * (int)std::max<size_t>(1, (200u << 10) / smem); };
+            if (kmax <= 128) return launch_l_table<128>(d_grp, d_order, d_idx, d_d2, d_counts, d_err,
+                                                        lgrid(knn_smem<128>()), s);
+            if (kmax <= 256) return launch_l_table<256>(d_grp, d_order, d_idx, d_d2, d_counts, d_err,
+                                                        lgrid(knn_smem<256>()), s);
+            if (kmax <= 512) return launch_l_table<512>(d_grp, d_order, d_idx, d_d2, d_counts, d_err,
+                                                        lgrid(knn_smem<512>()), s);
+            return launch_l_table<1024>(d_grp, d_order, d_idx, d_d2, d_counts, d_err, lgrid(knn_smem<1024>()), s);
+        }
         if (kmax <= 32) k_knn_reg<1, true><<<grid, kKnnThreads, 0, s>>>(a);
         else k_knn_reg<2, true><<<grid, kKnnThreads, 0, s>>>(a);
     } else {
@@ -792,10 +859,25 @@ cudaError_t launch_knn_table(int device, cudaStream_t s, const DynGroup* d_grp, 
     return cudaGetLastError();
 }
 
+cudaError_t prepare_knn_dyn() {
+    cudaError_t e;
+    if ((e = cudaFuncSetAttribute(k_knn<128, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)knn_smem<128>())) != cudaSuccess)
+        return e;
+    if ((e = cudaFuncSetAttribute(k_knn<256, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)knn_smem<256>())) != cudaSuccess)
+        return e;
+    if ((e = cudaFuncSetAttribute(k_knn<512, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)knn_smem<512>())) != cudaSuccess)
+        return e;
+    return cudaFuncSetAttribute(k_knn<1024, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)knn_smem<1024>());
+}
+
 cudaError_t launch_knn(Cloud& c, const double* d_centers, uint64_t nq, uint32_t k, uint32_t* d_idx, double* d_d2,
                        uint32_t* d_counts) {
     if (nq == 0 || k == 0) return cudaSuccess;
-    KnnArgs a;
+    KnnArgs a{};
     a.xs = c.xs.as<double>();
     a.ys = c.ys.as<double>();
     a.zs = c.zs.as<double>();

@@ -2,8 +2,8 @@
 
 A batch mixes clouds (Morton and Hilbert keys, several leaf sizes), radius
 requests of every kernel with neighbors and neighborsPrune (one radius or one
-per centre), kNN requests with k on both sides of the 32 boundary, and empty
-requests.  Every request's result must be bitwise the single-cloud call's
+per centre), kNN requests with k on both sides of the 32 and 64 boundaries (the
+register lists and the shared-memory lists), and empty requests.  Every request's result must be bitwise the single-cloud call's
 result (neighbour lists in the same ascending order, kNN indices and squared
 distances identical), and two of them are also checked against the oracle.
 The same batch through the captured graph, its replay, the direct launch
@@ -48,7 +48,7 @@ def centres(torch, sxyz, nq, seed):
 
 
 def mixed_batch(torch, clouds, seed=0):
-    """Requests over every cloud: radius with each kernel/algo, kNN k in {1, 10, 33, 64}, empties."""
+    """Requests over every cloud: radius with each kernel/algo, kNN k in {1, 10, 33, 64, 65, 250}, empties."""
     rng = np.random.default_rng(seed)
     reqs, host = [], []
     for ci, (oc, sxyz) in enumerate(clouds):
@@ -64,7 +64,7 @@ def mixed_batch(torch, clouds, seed=0):
                 r = float(rng.uniform(0.5, 3.0))
                 reqs.append(Request(oc, "radius", dc, radius=r, kernel=kern, algo=algo))
                 host.append(("radius", ci, c, r, kern, algo))
-        for k in (1, 10, 33, 64):
+        for k in (1, 10, 33, 64, 65, 250):
             nq = int(rng.integers(1, 300))
             c, dc = centres(torch, sxyz, nq, 1000 + 10 * ci + k)
             reqs.append(Request(oc, "knn", dc, k=k))
@@ -192,7 +192,7 @@ def test_engine_rejects_bad_requests(torch, clouds):
     oc, sxyz = clouds[0]
     _, dc = centres(torch, sxyz, 10, 3)
     eng = BatchEngine()
-    for bad in (Request(oc, "knn", dc, k=0), Request(oc, "knn", dc, k=65),
+    for bad in (Request(oc, "knn", dc, k=0), Request(oc, "knn", dc, k=1025),
                 Request(oc, "radius", dc, radius=1.0, algo="neighborsStruct")):
         with pytest.raises(capi.OctError) as ei:
             eng.run([bad])
