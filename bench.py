@@ -24,6 +24,7 @@ from __future__ import annotations
 
 import argparse
 import ctypes as C
+import gc
 import json
 import math
 import os
@@ -264,6 +265,35 @@ def run_batched(args, dev):
         "generate_s": wl.gen_s, "build_all_clouds_s": wl.build_s,
         "parity": "every radius request's result count and the last kNN request's pairs equal between batch and "
                   "sequential calls (full bitwise parity is in the GPU tests)",
+    }
+
+
+# ------------------------------------------------------------------ serving ---
+def run_serving(args, dev):
+    """The serving stream replayed in real time: the batching server, then the plain one-request-per-launch one."""
+    from octrees_benchmark_b200.serve import Server, ServingWorkload, replay
+
+    wl = ServingWorkload(device=dev, seconds=args.serve_seconds)
+    clocks = ClockSampler(dev)
+    clocks.start()
+    srv = Server(device=dev)
+    batched = replay(wl, srv, drain_s=args.serve_drain)
+    srv.close()
+    clk = clocks.stop()
+    srv = Server(device=dev, plain=True)
+    plain = replay(wl, srv, drain_s=args.serve_drain)
+    srv.close()
+    return {
+        "workload": wl.describe(),
+        "batched": batched, "plain": plain,
+        "p50_ms": batched["p50_ms"], "p99_ms": batched["p99_ms"], "qps": batched["qps"],
+        "p99_vs_plain": (plain["p99_ms"] / batched["p99_ms"]) if batched["p99_ms"] and plain["p99_ms"] else None,
+        "qps_vs_plain": (batched["qps"] / plain["qps"]) if plain["qps"] else None,
+        "clocks_batched": clk,
+        "timing": "latency = submit to results complete on the device (scheduler clock); qps = centres answered / "
+                  "wall time from the first arrival to the last completion; a server still busy "
+                  f"{args.serve_drain:g} s after the stream ends is stopped and its unanswered requests reported",
+        "generate_s": wl.gen_s,
     }
 
 
@@ -541,6 +571,13 @@ def run_b200(args, rank, world, local_rank):
     batched = None
     if world == 1 and not args.no_batched:
         batched = run_batched(args, dev)
+        gc.collect()
+        torch.cuda.empty_cache()
+    serving = None
+    if world == 1 and not args.no_serve:
+        serving = run_serving(args, dev)
+        gc.collect()
+        torch.cuda.empty_cache()
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -560,7 +597,7 @@ def run_b200(args, rank, world, local_rank):
             "radius_qps": chosen["radius_qps"], "knn_qps": chosen["knn_qps"],
             "avg_neighbours": chosen["avg_neighbours"], "paths": paths,
             "batched_vs_plain": paths["engine"]["qps"] / paths["plain"]["qps"], "engine_config": eng_cfg,
-            "build": build, "batched": batched, "roofline": roofline, "cpu_baseline": cpu,
+            "build": build, "batched": batched, "serving": serving, "roofline": roofline, "cpu_baseline": cpu,
             "e2e": {"value": e2e_val, "unit": "queries/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "detail": e2e_detail},
             "gpu_launches": LAUNCHES_PER_STEP[args.search] * args.steps, "clocks": clk,
@@ -586,6 +623,10 @@ def main():
     ap.add_argument("--no-e2e", action="store_true")
     ap.add_argument("--no-batched", action="store_true", help="skip the 256-cloud batch")
     ap.add_argument("--batched-steps", type=int, default=3, help="timed repetitions of the 256-cloud batch")
+    ap.add_argument("--no-serve", action="store_true", help="skip the serving stream")
+    ap.add_argument("--serve-seconds", type=float, default=60.0, help="length of the serving request stream")
+    ap.add_argument("--serve-drain", type=float, default=30.0,
+                    help="seconds each server may take after the stream ends before it is stopped")
     ap.add_argument("--points", type=int, default=N_POINTS, help="cloud size (smaller cases for profiling)")
     ap.add_argument("--queries", type=int, default=Q_RADIUS, help="radius and kNN queries per step, each")
     args = ap.parse_args()

@@ -65,6 +65,27 @@ class OctRequestPlace(C.Structure):
                 ("n_results", C.c_uint64)]
 
 
+OCT_SERVER_PLAIN = 0x1
+OCT_CLOUD_OWNED = 0x1
+
+
+class OctServerParams(C.Structure):
+    _fields_ = [("device", C.c_int32), ("flags", C.c_uint32), ("slots", C.c_uint32),
+                ("max_batch_requests", C.c_uint32), ("max_batch_queries", C.c_uint64), ("hbm_budget", C.c_uint64)]
+
+
+class OctCompletion(C.Structure):
+    _fields_ = [("ticket", C.c_uint64), ("status", C.c_int32), ("type", C.c_int32), ("nq", C.c_uint64),
+                ("n_results", C.c_uint64), ("queue_ms", C.c_double), ("latency_ms", C.c_double)]
+
+
+class OctServerStats(C.Structure):
+    _fields_ = [("submitted", C.c_uint64), ("completed", C.c_uint64), ("batches", C.c_uint64),
+                ("admission_stalls", C.c_uint64), ("evictions", C.c_uint64), ("queries", C.c_uint64),
+                ("cloud_bytes", C.c_uint64), ("inflight_bytes", C.c_uint64), ("peak_bytes", C.c_uint64),
+                ("queued", C.c_uint32), ("in_flight", C.c_uint32)]
+
+
 class OctError(RuntimeError):
     def __init__(self, status: int, msg: str):
         super().__init__(msg)
@@ -114,6 +135,21 @@ SIGNATURES = {
     "oct_engine_copy_knn": ([_vp, C.POINTER(OctRequestPlace), _u32, _vp, _vp, _vp, _u32], _int),
     "oct_engine_autotune": ([_vp, C.POINTER(OctRequest), _u32, C.POINTER(OctSearchConfig)], _int),
     "oct_engine_last_ms": ([_vp, C.POINTER(C.c_float)], _int),
+    "oct_engine_ready": ([_vp, C.POINTER(_int)], _int),
+    "oct_engine_memory": ([_vp, C.POINTER(_u64)], _int),
+    "oct_cloud_memory": ([_vp, C.POINTER(_u64)], _int),
+    "oct_server_create": ([C.POINTER(OctServerParams), C.POINTER(_vp)], _int),
+    "oct_server_destroy": ([_vp], _int),
+    "oct_server_last_error": ([_vp, C.c_char_p, C.c_size_t], _int),
+    "oct_server_set_config": ([_vp, C.POINTER(OctSearchConfig)], _int),
+    "oct_server_add_cloud": ([_vp, _vp, _u32], _int),
+    "oct_server_remove_cloud": ([_vp, _vp], _int),
+    "oct_server_submit": ([_vp, C.POINTER(OctRequest), C.POINTER(_u64)], _int),
+    "oct_server_poll": ([_vp, C.POINTER(OctCompletion), _u32, C.POINTER(_u32), C.c_int32], _int),
+    "oct_server_copy_radius": ([_vp, _u64, _vp, _vp, _u64, _u32], _int),
+    "oct_server_copy_knn": ([_vp, _u64, _vp, _vp, _vp, _u32], _int),
+    "oct_server_release": ([_vp, _u64], _int),
+    "oct_server_get_stats": ([_vp, C.POINTER(OctServerStats)], _int),
 }
 
 

@@ -23,6 +23,7 @@ import numpy as np
 from . import capi
 from .capi import (ALGOS, KERNELS, OCT_MEM_DEVICE, OCT_REQ_KNN, OCT_REQ_RADIUS, OctEngineParams, OctRequest,
                    OctRequestPlace, OctSearchConfig, lib)
+from .linear_octree import _sync_current_stream
 
 
 @dataclass
@@ -105,6 +106,7 @@ class BatchEngine:
                     knn_blocks_per_sm=cfg.reserved[1], serial=cfg.reserved[2])
 
     def autotune(self, requests: Sequence[Request]) -> dict:
+        _sync_current_stream()
         arr = (OctRequest * max(1, len(requests)))(*[r.to_c() for r in requests])
         cfg = OctSearchConfig()
         _engine_check(self._L.oct_engine_autotune(self._h, arr, len(requests), C.byref(cfg)), self._h,
@@ -113,6 +115,8 @@ class BatchEngine:
 
     # ---- batches --------------------------------------------------------------
     def submit(self, requests: Sequence[Request]):
+        if requests:
+            _sync_current_stream()  # the engine reads the centre tensors on its own stream
         arr = (OctRequest * max(1, len(requests)))(*[r.to_c() for r in requests])
         self._keep = list(requests)
         _engine_check(self._L.oct_engine_submit(self._h, arr, len(requests), None), self._h, "oct_engine_submit")

@@ -34,6 +34,14 @@ def _is_device(a) -> bool:
     return not isinstance(a, np.ndarray) and getattr(a, "is_cuda", False)
 
 
+def _sync_current_stream():
+    """Wait for the caller's current torch stream: the library reads device
+    tensors on its own (non-blocking) streams."""
+    import torch
+
+    torch.cuda.current_stream().synchronize()
+
+
 def _host_f64(a, shape_last=None):
     a = np.ascontiguousarray(a, dtype=np.float64)
     if shape_last is not None and a.ndim == 1:
@@ -63,6 +71,8 @@ class LinearOctree:
         dev = _is_device(points)
         if not dev:
             points = _host_f64(points, 3)
+        else:
+            _sync_current_stream()  # the cloud reads the tensor on its own stream
         self.n = int(points.shape[0])
         check(L.oct_set_points(h, _ptr(points), self.n, OCT_MEM_DEVICE if dev else 0), h, "oct_set_points")
         box = np.zeros(12)
