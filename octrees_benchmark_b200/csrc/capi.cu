@@ -123,8 +123,67 @@ cudaError_t radius_pass(Cloud& c, int kernel, int algo, bool fill, const double*
     }
     if ((e = c.stats.reserve(64)) != cudaSuccess) return e;
     if (!*order && (e = launch_query_order(c, dq, nq, order)) != cudaSuccess) return e;
-    return launch_radius_packet(c, kernel, algo, fill, c.fp32_filter != 0, dq, nq, dr, radius, *order, counts, counts2,
-                                offs, out, cap);
+    return launch_radius_packet(c, kernel, algo, fill ? 1 : 0, c.fp32_filter != 0, dq, nq, dr, radius, *order, counts,
+                                counts2, offs, out, cap);
+}
+
+// Radius search in one traversal (packet path, FP64): every query's results go
+// to its chain of result chunks, the counts are scanned, and the chains are
+// compacted into the CSR output.  A pool that turned out too small leaves the
+// counts exact: it is sized from the total and the traversal runs once more.
+int radius_one_pass(Cloud& c, int kernel, int algo, const double* dq, uint64_t nq, const double* dr, double radius,
+                    unsigned long long* doffs, uint64_t* offsets, uint32_t* idx, uint64_t idx_capacity,
+                    uint64_t* total, bool dev) {
+    const int pass_algo = (algo == OCT_NEIGHBORS_STRUCT) ? OCT_NEIGHBORS_PRUNE : algo;  // same index set
+    unsigned long long* dc = c.q_counts.as<unsigned long long>();
+    CK(c.stats.reserve(64));
+    CK(c.ck_first.reserve(4 * nq));
+    CK(c.ck_ctr.reserve(256));
+    const uint32_t* order = nullptr;
+    CK(launch_query_order(c, dq, nq, &order));
+    uint64_t tot = 0;
+    for (int attempt = 0; attempt < 2; ++attempt) {
+        // pool: every query's partial last chunk plus the results (a guess of 128 per query at first)
+        const uint64_t want = attempt == 0 ? std::max<uint64_t>(c.ck_cap, 3 * nq + 1024)
+                                           : tot / kResultChunk + nq + 1024;
+        if (want > 0xfffffff0ull) return set_error(c, OCT_ERR_INVALID_ARG, "too many results for one call");
+        if (want > c.ck_cap) {
+            CK(c.ck_pool.reserve(4ull * kResultChunk * want));
+            CK(c.ck_next.reserve(4ull * want));
+            c.ck_cap = (uint32_t)want;
+        }
+        ChunkArgs ck{c.ck_pool.as<uint32_t>(), c.ck_next.as<uint32_t>(), c.ck_first.as<uint32_t>(),
+                     c.ck_ctr.as<uint32_t>(), c.ck_cap};
+        CK(cudaMemsetAsync(ck.ctr, 0, 4, c.stream));
+        CK(launch_radius_packet(c, kernel, pass_algo, 2, false, dq, nq, dr, radius, order, dc, nullptr, nullptr,
+                                nullptr, 0, &ck));
+        CK(launch_scan_u64(c, dc, doffs, nq));
+        CK(cudaMemcpyAsync(c.pinned, doffs + nq, 8, cudaMemcpyDeviceToHost, c.stream));
+        const int st = sync_and_check(c, kErrChunkCapacity);
+        memcpy(&tot, c.pinned, 8);
+        uint32_t* hw = reinterpret_cast<uint32_t*>(static_cast<unsigned char*>(c.pinned) + kPinnedErrOffset);
+        const bool pool_short = (*hw & kErrChunkCapacity) != 0;
+        if (st != OCT_OK) return st;
+        if (!pool_short) break;
+        if (attempt == 1) return set_error(c, OCT_ERR_DEVICE_LIMIT, "result chunk pool still too small");
+    }
+    if (total) *total = tot;
+    if (!dev && offsets) CK(cudaMemcpyAsync(offsets, doffs, 8 * (nq + 1), cudaMemcpyDeviceToHost, c.stream));
+    if (tot > idx_capacity || (tot && !idx)) {
+        CK(cudaStreamSynchronize(c.stream));
+        return set_error(c, OCT_ERR_CAPACITY, "idx capacity smaller than the number of results");
+    }
+    uint32_t* dout = idx;
+    if (!dev) {
+        CK(c.q_out.reserve(4 * (tot ? tot : 1)));
+        dout = c.q_out.as<uint32_t>();
+    }
+    ChunkArgs ck{c.ck_pool.as<uint32_t>(), c.ck_next.as<uint32_t>(), c.ck_first.as<uint32_t>(),
+                 c.ck_ctr.as<uint32_t>(), c.ck_cap};
+    CK(launch_chunk_compact(c.device, c.stream, dc, doffs, ck, dout, tot, nq, nullptr, c.d_err.as<uint32_t>()));
+    if (!dev && tot) CK(cudaMemcpyAsync(idx, dout, 4 * tot, cudaMemcpyDeviceToHost, c.stream));
+    if (!dev) return sync_and_check(c);
+    return OCT_OK;
 }
 
 int radius_common(Cloud& c, int kernel, int algo, const double* centers, uint64_t nq, const double* radii,
@@ -285,6 +344,7 @@ int oct_set_search_config(oct_cloud h, const oct_search_config* cfg) {
     c.radius_group = (cfg->radius_lanes == 16 || cfg->radius_lanes == 32) ? cfg->radius_lanes : 8;
     c.knn_packet = cfg->knn_packet ? 1 : 0;
     c.knn_bucket = cfg->knn_bucket > 0 ? (uint32_t)cfg->knn_bucket : 0u;
+    c.two_pass = cfg->reserved[0] ? 1 : 0;
     return OCT_OK;
 }
 
@@ -496,6 +556,9 @@ int oct_radius_search(oct_cloud h, int kernel, int algo, const double* centers, 
         doffs = c.q_offsets.as<unsigned long long>();
     }
     const uint32_t* order = nullptr;
+    if (c.packet && !c.fp32_filter && !c.two_pass && nq) return radius_one_pass(c, kernel, algo, dq, nq, dr, radius,
+                                                                               doffs, offsets, idx, idx_capacity,
+                                                                               total, dev);
     if (algo == OCT_NEIGHBORS_STRUCT) {
         // expanded indices of the ranges: count points, fill as prune-style runs
         CK(c.q_out2.reserve(8 * (nq ? nq : 1)));

@@ -150,6 +150,10 @@ struct Cloud {
     int fp32_filter = 0;
     int knn_packet = 0;
     uint32_t knn_bucket = 256;
+    int two_pass = 0;   // 1: packet radius searches count, then fill (no result chunks)
+    // one-pass radius search: result chunk pool, links, first chunk per query, counter
+    DevBuf ck_pool, ck_next, ck_first, ck_ctr;
+    uint32_t ck_cap = 0;
 
     // pinned host staging for small readbacks
     void* pinned = nullptr;
@@ -167,18 +171,38 @@ cudaError_t launch_radius(Cloud& c, int kernel, int algo, int group, bool fill, 
 cudaError_t launch_scan_u64(Cloud& c, const unsigned long long* d_in, unsigned long long* d_out, uint64_t n);
 cudaError_t launch_query_order(Cloud& c, const double* d_centers, uint64_t nq, const uint32_t** d_order);
 cudaError_t launch_leaf_rel(Cloud& c);
-cudaError_t launch_radius_packet(Cloud& c, int kernel, int algo, bool fill, bool fp32, const double* d_centers,
+struct ChunkArgs;
+// mode as launch_radius_table (0 count, 1 fill, 2 one pass into `chunks`)
+cudaError_t launch_radius_packet(Cloud& c, int kernel, int algo, int mode, bool fp32, const double* d_centers,
                                  uint64_t nq, const double* d_radii, double radius, const uint32_t* d_order,
                                  unsigned long long* d_counts, unsigned long long* d_counts2,
-                                 const unsigned long long* d_offsets, uint32_t* d_out, uint64_t out_capacity);
+                                 const unsigned long long* d_offsets, uint32_t* d_out, uint64_t out_capacity,
+                                 const ChunkArgs* chunks = nullptr);
+// Result chunks of the one-pass radius search: `cap` chunks of 64 entries, the
+// next-chunk links, each query's first chunk, and the hand-out counter.
+struct ChunkArgs {
+    uint32_t* pool;
+    uint32_t* next;
+    uint32_t* first;
+    uint32_t* ctr;
+    uint32_t cap;
+};
+constexpr uint32_t kResultChunk = 64;
+
 // Packet radius search.  Either one request (`single`, host copy, `packets`
 // packets) or the group of a batch (`d_grp`, sizes read on the device).
-cudaError_t launch_radius_table(int device, cudaStream_t s, int kernel, int algo, bool fill, bool fp32,
+// mode: 0 count, 1 fill at d_offsets, 2 one pass into `chunks` (counts and
+// first chunks written; neighbors / neighborsPrune, FP64 only).
+cudaError_t launch_radius_table(int device, cudaStream_t s, int kernel, int algo, int mode, bool fp32,
                                 const DynGroup* d_grp, const SearchReq* single, uint64_t packets,
                                 const uint32_t* d_order, unsigned long long* d_counts, unsigned long long* d_counts2,
                                 const unsigned long long* d_offsets, uint32_t* d_out, uint64_t out_capacity,
                                 uint32_t* d_packet_ctr, unsigned long long* d_stats, uint32_t* d_err,
-                                int blocks_per_sm = 0);
+                                int blocks_per_sm = 0, const ChunkArgs* chunks = nullptr);
+// Chains of result chunks into CSR (after the counts are scanned into d_offsets).
+cudaError_t launch_chunk_compact(int device, cudaStream_t s, const unsigned long long* d_counts,
+                                 const unsigned long long* d_offsets, const ChunkArgs& chunks, uint32_t* d_out,
+                                 uint64_t out_capacity, uint64_t n, const uint64_t* d_n, uint32_t* d_err);
 // kNN, one warp per query.  Either one request (`single`, nq queries, k <= 64,
 // register lists) or the group of a batch (`d_grp`, kmax = the group's largest
 // k: register lists up to 64, shared-memory lists up to 1024).

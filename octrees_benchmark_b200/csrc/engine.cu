@@ -251,6 +251,7 @@ struct oct_engine_s {
     DevBuf counts, offs, part, out;
     DevBuf knn_idx, knn_d2, knn_counts;
     DevBuf ctrs, stats, summary, totals;
+    DevBuf ck_pool, ck_next, ck_first, ck_ctr;  // one-pass radius: result chunks (ck_next has one word per chunk)
     // pinned host staging
     unsigned char* h_stage = nullptr;
     size_t h_stage_bytes = 0;
@@ -328,6 +329,15 @@ int grow_pinned(oct_engine e, size_t bytes) {
 
 size_t table_offset() { return (sizeof(EngineDyn) + 255) & ~(size_t)255; }
 
+ChunkArgs chunk_args(oct_engine e) {
+    const uint64_t cap = std::min<uint64_t>(e->ck_next.bytes / 4, e->ck_pool.bytes / (4ull * kResultChunk));
+    return ChunkArgs{e->ck_pool.as<uint32_t>(), e->ck_next.as<uint32_t>(), e->ck_first.as<uint32_t>(),
+                     e->ck_ctr.as<uint32_t>(), (uint32_t)std::min<uint64_t>(cap, 0xfffffff0ull)};
+}
+
+// Result chunks for `chunks` chunks (grows both arrays; a new address drops the graphs).
+int grow_chunks(oct_engine e, uint64_t chunks);
+
 // The launch sequence of the batch in the descriptor (captured or direct).
 cudaError_t enqueue_work(oct_engine e) {
     cudaError_t r;
@@ -375,23 +385,43 @@ cudaError_t enqueue_work(oct_engine e) {
     if (any_radius) {
         unsigned long long* counts = e->counts.as<unsigned long long>();
         unsigned long long* offs = e->offs.as<unsigned long long>();
-        for (int pass = 0; pass < 2; ++pass) {
-            const bool fill = pass == 1;
-            if (fill) {
-                unsigned long long* part = e->part.as<unsigned long long>();
-                k_escan_reduce<<<kScanBlocks, kScanThreads, 0, s>>>(counts, &dyn->n_radius, part);
-                k_escan_top<<<1, kScanThreads, 0, s>>>(part, kScanBlocks, sum);
-                k_escan_apply<<<kScanBlocks, kScanThreads, 0, s>>>(counts, &dyn->n_radius, part, offs);
-            }
+        unsigned long long* part = e->part.as<unsigned long long>();
+        auto scan = [&]() {
+            k_escan_reduce<<<kScanBlocks, kScanThreads, 0, s>>>(counts, &dyn->n_radius, part);
+            k_escan_top<<<1, kScanThreads, 0, s>>>(part, kScanBlocks, sum);
+            k_escan_apply<<<kScanBlocks, kScanThreads, 0, s>>>(counts, &dyn->n_radius, part, offs);
+        };
+        if (!e->fp32) {
+            // one traversal: results into chunk chains, scan, chains compacted into the result array
+            const ChunkArgs ck = chunk_args(e);
+            if ((r = cudaMemsetAsync(ck.ctr, 0, 4, s)) != cudaSuccess) return r;
             for (int v = 0; v < kRadiusVariants; ++v) {
                 if (!((e->sig >> v) & 1ull)) continue;
                 const int kernel = v >> 2, algo = (v & 2) ? OCT_NEIGHBORS_PRUNE : OCT_NEIGHBORS;
-                if ((r = launch_radius_table(e->device, s, kernel, algo, fill, (v & 1) != 0, &dyn->groups[v],
-                                             nullptr, 0, order, fill ? nullptr : counts, nullptr,
-                                             fill ? offs : nullptr, fill ? e->out.as<uint32_t>() : nullptr,
-                                             fill ? e->out.bytes / 4 : 0, ctr + 2 * v + pass, stats, err,
-                                             e->radius_bps)) != cudaSuccess)
+                if ((r = launch_radius_table(e->device, s, kernel, algo, 2, false, &dyn->groups[v], nullptr, 0, order,
+                                             counts, nullptr, nullptr, nullptr, 0, ctr + 2 * v, stats, err,
+                                             e->radius_bps, &ck)) != cudaSuccess)
                     return r;
+            }
+            scan();
+            if ((r = launch_chunk_compact(e->device, s, counts, offs, ck, e->out.as<uint32_t>(), e->out.bytes / 4, 0,
+                                          &dyn->n_radius, err)) != cudaSuccess)
+                return r;
+        } else {
+            // FP32 filter: count, scan, fill
+            for (int pass = 0; pass < 2; ++pass) {
+                const bool fill = pass == 1;
+                if (fill) scan();
+                for (int v = 0; v < kRadiusVariants; ++v) {
+                    if (!((e->sig >> v) & 1ull)) continue;
+                    const int kernel = v >> 2, algo = (v & 2) ? OCT_NEIGHBORS_PRUNE : OCT_NEIGHBORS;
+                    if ((r = launch_radius_table(e->device, s, kernel, algo, fill ? 1 : 0, (v & 1) != 0,
+                                                 &dyn->groups[v], nullptr, 0, order, fill ? nullptr : counts, nullptr,
+                                                 fill ? offs : nullptr, fill ? e->out.as<uint32_t>() : nullptr,
+                                                 fill ? e->out.bytes / 4 : 0, ctr + 2 * v + pass, stats, err,
+                                                 e->radius_bps)) != cudaSuccess)
+                        return r;
+                }
             }
         }
         const int tb = 128;
@@ -448,6 +478,13 @@ int launch_batch(oct_engine e, bool record_start) {
     return OCT_OK;
 }
 
+int grow_chunks(oct_engine e, uint64_t chunks) {
+    if (chunks > 0xfffffff0ull) return fail(e, OCT_ERR_INVALID_ARG, "too many radius results for one batch");
+    int st;
+    if ((st = grow(e, e->ck_next, 4 * chunks)) != OCT_OK) return st;
+    return grow(e, e->ck_pool, 4ull * kResultChunk * chunks);
+}
+
 int finish(oct_engine e) {
     DeviceGuardE g(e->device);
     e->in_flight = false;
@@ -455,14 +492,15 @@ int finish(oct_engine e) {
         EK(cudaStreamSynchronize(e->stream));
         const Summary sm = *e->h_summary;
         const uint64_t cap = e->out.bytes / 4;
-        const uint32_t bits = sm.err & ~(uint32_t)kErrOutputCapacity;
+        const uint32_t grow_bits = (uint32_t)kErrOutputCapacity | (uint32_t)kErrChunkCapacity;
+        const uint32_t bits = sm.err & ~grow_bits;
         if (bits & kErrBadInput) return fail(e, OCT_ERR_INVALID_ARG, "device rejected an input");
         if (bits) {
             char buf[128];
             snprintf(buf, sizeof(buf), "a bounded device loop hit its limit (error bits 0x%x)", bits);
             return fail(e, OCT_ERR_DEVICE_LIMIT, buf);
         }
-        if (sm.radius_total <= cap && !(sm.err & kErrOutputCapacity)) {
+        if (sm.radius_total <= cap && !(sm.err & grow_bits)) {
             e->radius_total = sm.radius_total;
             float ms = 0.f;
             if (cudaEventElapsedTime(&ms, e->ev_t0, e->ev_t1) == cudaSuccess) e->last_ms = ms;
@@ -476,9 +514,12 @@ int finish(oct_engine e) {
             e->have_results = true;
             return OCT_OK;
         }
-        // the results did not fit: grow the result array and run the batch again
+        // the results did not fit: grow the result array (and the chunk pool: every
+        // query's last chunk may be partial) from the exact total and run the batch again
         int st = grow(e, e->out, 4 * (size_t)(sm.radius_total + sm.radius_total / 8 + 1024));
         if (st != OCT_OK) return st;
+        if (!e->fp32 && (st = grow_chunks(e, sm.radius_total / kResultChunk + e->n_radius + 1024)) != OCT_OK)
+            return st;
         if ((st = launch_batch(e, true)) != OCT_OK) return st;
     }
     return fail(e, OCT_ERR_CAPACITY, "radius results kept outgrowing the result array");
@@ -567,6 +608,13 @@ int submit(oct_engine e, const oct_request* rq, uint32_t n) {
     if ((st = grow(e, e->knn_d2, 8 * std::max<uint64_t>(knn_slots, 1))) != OCT_OK) return st;
     if ((st = grow(e, e->knn_counts, 4 * std::max<uint64_t>(n_total, 1))) != OCT_OK) return st;
     if ((st = grow(e, e->totals, sizeof(ReqTotal) * std::max<uint32_t>(m, 1))) != OCT_OK) return st;
+    if (!e->fp32 && n_radius) {  // one-pass radius: a first chunk per query, a pool of at least 3 chunks per query
+        if ((st = grow(e, e->ck_first, 4 * n_radius)) != OCT_OK) return st;
+        if ((st = grow(e, e->ck_ctr, 256)) != OCT_OK) return st;
+        const uint64_t have = chunk_args(e).cap;
+        const uint64_t want = std::max<uint64_t>(3 * n_radius + 1024, e->out.bytes / (4ull * kResultChunk) + n_radius);
+        if (have < want && (st = grow_chunks(e, want)) != OCT_OK) return st;
+    }
     if (e->out.bytes == 0 && (st = grow(e, e->out, 4 * std::max<uint64_t>(64 * n_radius, 1u << 20))) != OCT_OK)
         return st;
     if (m > e->h_totals_cap) {
@@ -725,7 +773,8 @@ int oct_engine_destroy(oct_engine e) {
         drop_graphs(e);
         DevBuf* bufs[] = {&e->desc, &e->keys[0], &e->keys[1], &e->ord[0], &e->ord[1], &e->sort_ctl, &e->sort_status,
                           &e->epoch, &e->counts, &e->offs, &e->part, &e->out, &e->knn_idx, &e->knn_d2,
-                          &e->knn_counts, &e->ctrs, &e->stats, &e->summary, &e->totals};
+                          &e->knn_counts, &e->ctrs, &e->stats, &e->summary, &e->totals,
+                          &e->ck_pool, &e->ck_next, &e->ck_first, &e->ck_ctr};
         for (DevBuf* b : bufs) b->release();
         if (e->h_stage) cudaFreeHost(e->h_stage);
         if (e->h_summary) cudaFreeHost(e->h_summary);
@@ -917,7 +966,8 @@ int oct_engine_memory(oct_engine e, uint64_t* bytes) {
     if (!e || !bytes) return OCT_ERR_INVALID_ARG;
     const DevBuf* bufs[] = {&e->desc, &e->keys[0], &e->keys[1], &e->ord[0], &e->ord[1], &e->sort_ctl,
                             &e->sort_status, &e->epoch, &e->counts, &e->offs, &e->part, &e->out, &e->knn_idx,
-                            &e->knn_d2, &e->knn_counts, &e->ctrs, &e->stats, &e->summary, &e->totals};
+                            &e->knn_d2, &e->knn_counts, &e->ctrs, &e->stats, &e->summary, &e->totals,
+                            &e->ck_pool, &e->ck_next, &e->ck_first, &e->ck_ctr};
     uint64_t s = 0;
     for (const DevBuf* b : bufs) s += b->bytes;
     *bytes = s;

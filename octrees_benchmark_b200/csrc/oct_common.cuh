@@ -16,6 +16,7 @@ enum ErrBits : uint32_t {
     kErrNodeCapacity = 1u << 2,   // octree node arrays too small (host re-runs larger)
     kErrOutputCapacity = 1u << 3, // result buffer smaller than the counted results
     kErrBadInput = 1u << 4,       // invalid query (e.g. k larger than supported)
+    kErrChunkCapacity = 1u << 5,  // one-pass radius: result chunk pool too small (counts still exact)
 };
 
 // Bounded spin: every wait in this library gives up after this many polls.

@@ -12,10 +12,18 @@
 // reference's predicates, bit for bit), and a child is pushed with two lane
 // masks - the lanes for which it is fully inside (they emit its whole range
 // when it is popped) and the lanes that must descend into it.  Pushing the
-// children lowest octant last keeps every lane's output in ascending order.  A
-// leaf's points are staged in shared memory once per warp (coalesced) and every
-// lane of the descend mask tests its query against all of them.  Packets are
+// children lowest octant last keeps every lane's output in ascending order.
+// Leaves, FP64 neighbors / neighborsPrune (the transposed test): the lanes load
+// 32 consecutive points and test them against one query of the descend mask at
+// a time, so all lanes work and the ballot is that query's hit mask, stored in
+// one coalesced write.  neighborsStruct and the FP32 form stage a leaf's points
+// in shared memory and every lane of the mask tests its own query against all
+// of them.  Fully-inside ranges are written by the whole warp.  Packets are
 // handed out by an atomic counter so that long and short packets balance.
+//
+// Output: count pass + scan + fill at the scanned offsets, or one pass in which
+// every query appends its results to its own chain of 64-entry chunks (see
+// k_radius_packet's CHUNK form) that k_chunk_compact moves into the CSR array.
 //
 // FP32 variant (the precision form): each sorted point also has FP32
 // coordinates relative to its leaf's centre (x, y, z computed in FP64 and
@@ -42,6 +50,8 @@ namespace {
 constexpr int kPkWarps = 4;
 constexpr int kPkThreads = 32 * kPkWarps;
 constexpr int kPkStack = 8 * (kMaxDepth + 1);
+constexpr uint32_t kChunk = kResultChunk;  // entries per result chunk (one-pass mode)
+constexpr uint32_t kNoChunk = 0xffffffffu;
 
 struct PacketArgs {
     SearchReq single;           // the request of a single-cloud search (grp == null)
@@ -56,6 +66,12 @@ struct PacketArgs {
     uint32_t* packet_ctr;
     unsigned long long* stats;  // [0] point tests, [1] FP64 re-tests
     uint32_t* err;
+    // one-pass mode: each query's results go to its own chain of kChunk-entry chunks
+    uint32_t* chunk_pool;       // chunk_cap x kChunk entries
+    uint32_t* chunk_next;       // next chunk of a chain (chunk_cap)
+    uint32_t* chunk_first;      // first chunk of each query (per query position)
+    uint32_t* chunk_ctr;        // chunks handed out
+    uint32_t chunk_cap;
 };
 
 // Per-lane FP32 context of one leaf.
@@ -158,12 +174,18 @@ __device__ __forceinline__ bool inside_of(const double (*q)[32], int j, double p
     }
 }
 
-template <int KT, int ALGO, bool FILL, bool F32, bool MULTI>
+// CHUNK (with FILL, transposed form only): one pass instead of count + fill.
+// Each query appends its results to its own chain of kChunk-entry chunks taken
+// from a pool (contiguous chunks for one long range, so positions stay
+// linear); per query the count and the first chunk are written, and
+// k_chunk_compact moves every chain into the CSR array after the scan.
+template <int KT, int ALGO, bool FILL, bool F32, bool MULTI, bool CHUNK = false>
 __global__ void __launch_bounds__(kPkThreads) k_radius_packet(PacketArgs a) {
     // Transposed leaf test (FP64, neighbors / neighborsPrune): the lanes hold
     // consecutive points and test them against one query of the mask at a time,
     // so every lane does useful work and the ballot is that query's hit mask.
     constexpr bool kT = (ALGO != kStruct) && !F32;
+    static_assert(!CHUNK || (FILL && kT), "one-pass mode needs the transposed FP64 form");
     constexpr int kStage = kT ? 1 : kPkWarps;  // point staging, per-lane loop forms only
     __shared__ CloudView s_view[MULTI ? kPkWarps : 1];
     __shared__ uint32_t st_node[kPkWarps][kPkStack];
@@ -233,10 +255,54 @@ __global__ void __launch_bounds__(kPkThreads) k_radius_packet(PacketArgs a) {
         k.init(qc[3 * ql], qc[3 * ql + 1], qc[3 * ql + 2], qrad ? qrad[ql] : RQ(radius));
         if constexpr (kT) put_query<KT>(s_qp[warp], lane, k);  // read by the other lanes after a __syncwarp
         unsigned long long cnt = 0, cnt2 = 0, base = 0;
-        if (FILL && valid) base = a.offs[qi];
+        if (FILL && !CHUNK && valid) base = a.offs[qi];
         bool overflow = false;
         bool open = false;  // neighborsStruct: a run of inside points is open
         uint32_t rs = 0;
+        // one-pass mode: this lane's chain (current chunk, entries used in it, first chunk)
+        uint32_t ck_cur = kNoChunk, ck_fill = kChunk, ck_first = kNoChunk;
+        bool ck_over = false;
+
+        // Reserve n > 0 entries at the end of lane j's chain (warp-uniform call):
+        // returns where they go - the first `room` continue chunk `cur`, the rest
+        // are linear from chunk `nc` on (new chunks taken as one contiguous run).
+        struct ChunkPos {
+            uint32_t cur, fill, room, nc;
+        };
+        auto chunk_reserve = [&](int j, uint32_t n) -> ChunkPos {
+            ChunkPos p;
+            p.cur = __shfl_sync(0xffffffffu, ck_cur, j);
+            p.fill = __shfl_sync(0xffffffffu, ck_fill, j);
+            p.room = kChunk - p.fill;
+            p.nc = kNoChunk;
+            if (n > p.room) {
+                const uint32_t m = (n - p.room + kChunk - 1) / kChunk;
+                uint32_t nc = 0;
+                if (lane == 0) nc = atomicAdd(a.chunk_ctr, m);
+                nc = __shfl_sync(0xffffffffu, nc, 0);
+                p.nc = nc;
+                const bool fits = (uint64_t)nc + m <= a.chunk_cap;
+                if (!fits) ck_over = true;  // the pool is too small: counts stay exact, the host re-runs
+                if (fits) {
+                    if (lane == 0 && p.cur != kNoChunk) a.chunk_next[p.cur] = nc;
+                    for (uint32_t t = lane; t + 1 < m; t += 32) a.chunk_next[nc + t] = nc + t + 1;
+                }
+                if (lane == j) {
+                    if (ck_cur == kNoChunk) ck_first = nc;
+                    ck_cur = nc + m - 1;
+                    ck_fill = n - p.room - (m - 1) * kChunk;
+                }
+            } else if (lane == j) {
+                ck_fill += n;
+            }
+            if (lane == j) cnt += n;
+            return p;
+        };
+        auto chunk_store = [&](const ChunkPos& p, uint32_t r, uint32_t v) {
+            const uint64_t pos = (r < p.room) ? (uint64_t)p.cur * kChunk + p.fill + r
+                                              : (uint64_t)p.nc * kChunk + (r - p.room);
+            if (pos < (uint64_t)a.chunk_cap * kChunk) a.chunk_pool[pos] = v;
+        };
 
         auto emit_range = [&](uint32_t f, uint32_t l) {  // per lane
             if constexpr (ALGO == kStruct) {
@@ -300,6 +366,13 @@ __global__ void __launch_bounds__(kPkThreads) k_radius_packet(PacketArgs a) {
                         rem &= rem - 1;
                         const bool in = in_range && inside_of<KT>(s_qp[warp], j, px, py, pz);
                         const uint32_t hb = __ballot_sync(0xffffffffu, in);
+                        if constexpr (CHUNK) {
+                            if (hb) {
+                                const ChunkPos p = chunk_reserve(j, __popc(hb));
+                                if (in) chunk_store(p, __popc(hb & lanemask_lt()), idx);
+                            }
+                            continue;
+                        }
                         if (FILL && hb) {  // query j's hits, ascending, in one coalesced store
                             const unsigned long long o0 = __shfl_sync(0xffffffffu, base + cnt, j);
                             if (in) {
@@ -421,20 +494,32 @@ __global__ void __launch_bounds__(kPkThreads) k_radius_packet(PacketArgs a) {
                 // a fully-inside node: every lane of mi adds the node's whole range; the
                 // warp writes it for one lane at a time, 32 consecutive indices per store
                 const uint32_t len = nrg.y - nrg.x;
-                if (FILL) {
-                    uint32_t rem = mi;
-                    while (rem) {
-                        const int j = __ffs(rem) - 1;
-                        rem &= rem - 1;
-                        const unsigned long long o0 = __shfl_sync(0xffffffffu, base + cnt, j);
-                        for (uint32_t t = lane; t < len; t += 32) {
-                            const unsigned long long o = o0 + t;
-                            if (o < a.out_cap) a.out[o] = nrg.x + t;
-                            else overflow = true;
+                if constexpr (CHUNK) {
+                    if (len) {
+                        uint32_t rem = mi;
+                        while (rem) {
+                            const int j = __ffs(rem) - 1;
+                            rem &= rem - 1;
+                            const ChunkPos p = chunk_reserve(j, len);
+                            for (uint32_t t = lane; t < len; t += 32) chunk_store(p, t, nrg.x + t);
                         }
                     }
+                } else {
+                    if (FILL) {
+                        uint32_t rem = mi;
+                        while (rem) {
+                            const int j = __ffs(rem) - 1;
+                            rem &= rem - 1;
+                            const unsigned long long o0 = __shfl_sync(0xffffffffu, base + cnt, j);
+                            for (uint32_t t = lane; t < len; t += 32) {
+                                const unsigned long long o = o0 + t;
+                                if (o < a.out_cap) a.out[o] = nrg.x + t;
+                                else overflow = true;
+                            }
+                        }
+                    }
+                    if (mi & lbit) cnt += len;
                 }
-                if (mi & lbit) cnt += len;
             }
             if (mo == 0) continue;
             if (fc == 0) {
@@ -493,9 +578,11 @@ __global__ void __launch_bounds__(kPkThreads) k_radius_packet(PacketArgs a) {
             __syncwarp();
             sp_top += np;
         }
-        if (overflow) set_err(a.err, FILL ? kErrOutputCapacity : kErrStackOverflow);
-        if (!FILL && valid) {
+        if (overflow) set_err(a.err, (FILL && !CHUNK) ? kErrOutputCapacity : kErrStackOverflow);
+        if (CHUNK && ck_over) set_err(a.err, kErrChunkCapacity);
+        if ((!FILL || CHUNK) && valid) {
             a.counts[qi] = cnt;
+            if (CHUNK) a.chunk_first[qi] = ck_first;
             if (ALGO == kStruct) a.counts2[qi] = cnt2;
         }
         __syncwarp();
@@ -530,7 +617,7 @@ __global__ void k_leaf_rel(const double* __restrict__ xs, const double* __restri
         v.x = (float)dsub(xs[i], cx);
         v.y = (float)dsub(ys[i], cy);
         v.z = (float)dsub(zs[i], cz);
-        // L1 norm, rounded up so that it bounds the exact L1 norm of (x, y, z) so that it bounds the exact L1 norm of (x, y, z) in FP32
+        // L1 norm, rounded up so that it bounds the exact L1 norm of the FP32 (x, y, z)
         v.w = __fadd_ru(__fadd_ru(fabsf(v.x), fabsf(v.y)), fabsf(v.z));
         rel[i] = v;
     }
@@ -542,9 +629,12 @@ int sm_count_p(int device) {
     return v;
 }
 
+// mode: 0 count, 1 fill at known offsets, 2 one pass into result chunks
 template <int KT, int ALGO, bool MULTI>
-cudaError_t launch_pk_m(const PacketArgs& a, bool fill, bool fp32, int grid, cudaStream_t s) {
-    if (fill) {
+cudaError_t launch_pk_m(const PacketArgs& a, int mode, bool fp32, int grid, cudaStream_t s) {
+    if (mode == 2) {
+        if constexpr (ALGO != kStruct) k_radius_packet<KT, ALGO, true, false, MULTI, true><<<grid, kPkThreads, 0, s>>>(a);
+    } else if (mode == 1) {
         if (fp32) k_radius_packet<KT, ALGO, true, true, MULTI><<<grid, kPkThreads, 0, s>>>(a);
         else k_radius_packet<KT, ALGO, true, false, MULTI><<<grid, kPkThreads, 0, s>>>(a);
     } else {
@@ -555,17 +645,53 @@ cudaError_t launch_pk_m(const PacketArgs& a, bool fill, bool fp32, int grid, cud
 }
 
 template <int KT, int ALGO>
-cudaError_t launch_pk(const PacketArgs& a, bool fill, bool fp32, int grid, cudaStream_t s) {
-    if (a.grp) return launch_pk_m<KT, ALGO, true>(a, fill, fp32, grid, s);
-    return launch_pk_m<KT, ALGO, false>(a, fill, fp32, grid, s);
+cudaError_t launch_pk(const PacketArgs& a, int mode, bool fp32, int grid, cudaStream_t s) {
+    if (a.grp) return launch_pk_m<KT, ALGO, true>(a, mode, fp32, grid, s);
+    return launch_pk_m<KT, ALGO, false>(a, mode, fp32, grid, s);
 }
 
 template <int KT>
-cudaError_t launch_pk_a(const PacketArgs& a, int algo, bool fill, bool fp32, int grid, cudaStream_t s) {
+cudaError_t launch_pk_a(const PacketArgs& a, int algo, int mode, bool fp32, int grid, cudaStream_t s) {
     switch (algo) {
-        case kNeighbors: return launch_pk<KT, kNeighbors>(a, fill, fp32, grid, s);
-        case kStruct: return launch_pk<KT, kStruct>(a, fill, fp32, grid, s);
-        default: return launch_pk<KT, kPrune>(a, fill, fp32, grid, s);
+        case kNeighbors: return launch_pk<KT, kNeighbors>(a, mode, fp32, grid, s);
+        case kStruct: return launch_pk<KT, kStruct>(a, mode, fp32, grid, s);
+        default: return launch_pk<KT, kPrune>(a, mode, fp32, grid, s);
+    }
+}
+
+// Each radius query's chain of result chunks into its CSR slot: one warp per
+// query, chunks copied 32 entries per store.
+__global__ void __launch_bounds__(256) k_chunk_compact(const unsigned long long* __restrict__ counts,
+                                                       const unsigned long long* __restrict__ offs,
+                                                       const uint32_t* __restrict__ first,
+                                                       const uint32_t* __restrict__ next,
+                                                       const uint32_t* __restrict__ pool, uint64_t chunk_cap,
+                                                       uint32_t* __restrict__ out, uint64_t out_cap, uint64_t n,
+                                                       const uint64_t* d_n, uint32_t* err) {
+    if (d_n) n = *d_n;
+    const int lane = threadIdx.x & 31;
+    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t q = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; q < n; q += nwarps) {
+        const unsigned long long cnt = counts[q];
+        if (cnt == 0) continue;
+        const unsigned long long o = offs[q];
+        uint32_t c = first[q];
+        bool bad = false;
+        for (unsigned long long done = 0; done < cnt;) {
+            if (c >= chunk_cap) {  // a chain cut short by a pool overflow (reported by the search kernel)
+                bad = true;
+                break;
+            }
+            const unsigned long long m = (cnt - done < kChunk) ? (cnt - done) : kChunk;
+            for (uint32_t t = lane; t < m; t += 32) {
+                const unsigned long long w = o + done + t;
+                if (w < out_cap) out[w] = pool[(uint64_t)c * kChunk + t];
+                else bad = true;
+            }
+            done += m;
+            if (done < cnt) c = next[c];
+        }
+        if (bad && lane == 0) set_err(err, kErrOutputCapacity);
     }
 }
 
@@ -598,12 +724,12 @@ CloudView cloud_view(const Cloud& c) {
     return v;
 }
 
-cudaError_t launch_radius_table(int device, cudaStream_t s, int kernel, int algo, bool fill, bool fp32,
+cudaError_t launch_radius_table(int device, cudaStream_t s, int kernel, int algo, int mode, bool fp32,
                                 const DynGroup* d_grp, const SearchReq* single, uint64_t packets,
                                 const uint32_t* d_order, unsigned long long* d_counts, unsigned long long* d_counts2,
                                 const unsigned long long* d_offsets, uint32_t* d_out, uint64_t out_capacity,
                                 uint32_t* d_packet_ctr, unsigned long long* d_stats, uint32_t* d_err,
-                                int blocks_per_sm) {
+                                int blocks_per_sm, const ChunkArgs* chunks) {
     cudaError_t e;
     if (!d_grp && packets == 0) return cudaSuccess;
     if ((e = cudaMemsetAsync(d_packet_ctr, 0, 4, s)) != cudaSuccess) return e;
@@ -620,22 +746,41 @@ cudaError_t launch_radius_table(int device, cudaStream_t s, int kernel, int algo
     a.packet_ctr = d_packet_ctr;
     a.stats = d_stats;
     a.err = d_err;
+    a.chunk_pool = chunks ? chunks->pool : nullptr;
+    a.chunk_next = chunks ? chunks->next : nullptr;
+    a.chunk_first = chunks ? chunks->first : nullptr;
+    a.chunk_ctr = chunks ? chunks->ctr : nullptr;
+    a.chunk_cap = chunks ? chunks->cap : 0;
+    if (mode == 2 && (!chunks || fp32 || algo == kStruct)) return cudaErrorInvalidValue;
     // persistent grid: warps take packets from the counter until none is left
     const uint64_t cap = (uint64_t)sm_count_p(device) * (blocks_per_sm > 0 ? blocks_per_sm : 12);
     const uint64_t want = d_grp ? cap : (packets + kPkWarps - 1) / kPkWarps;
     const int grid = (int)(want < cap ? want : cap);
     switch (kernel) {
-        case kCircle: return launch_pk_a<kCircle>(a, algo, fill, fp32, grid, s);
-        case kSquare: return launch_pk_a<kSquare>(a, algo, fill, fp32, grid, s);
-        case kCube: return launch_pk_a<kCube>(a, algo, fill, fp32, grid, s);
-        default: return launch_pk_a<kSphere>(a, algo, fill, fp32, grid, s);
+        case kCircle: return launch_pk_a<kCircle>(a, algo, mode, fp32, grid, s);
+        case kSquare: return launch_pk_a<kSquare>(a, algo, mode, fp32, grid, s);
+        case kCube: return launch_pk_a<kCube>(a, algo, mode, fp32, grid, s);
+        default: return launch_pk_a<kSphere>(a, algo, mode, fp32, grid, s);
     }
 }
 
-cudaError_t launch_radius_packet(Cloud& c, int kernel, int algo, bool fill, bool fp32, const double* d_centers,
+cudaError_t launch_chunk_compact(int device, cudaStream_t s, const unsigned long long* d_counts,
+                                 const unsigned long long* d_offsets, const ChunkArgs& chunks, uint32_t* d_out,
+                                 uint64_t out_capacity, uint64_t n, const uint64_t* d_n, uint32_t* d_err) {
+    if (!d_n && n == 0) return cudaSuccess;
+    const uint64_t cap = (uint64_t)sm_count_p(device) * 8;
+    const uint64_t want = d_n ? cap : (n + 7) / 8;
+    const int grid = (int)(want < cap ? (want ? want : 1) : cap);
+    k_chunk_compact<<<grid, 256, 0, s>>>(d_counts, d_offsets, chunks.first, chunks.next, chunks.pool, chunks.cap,
+                                         d_out, out_capacity, n, d_n, d_err);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_radius_packet(Cloud& c, int kernel, int algo, int mode, bool fp32, const double* d_centers,
                                  uint64_t nq, const double* d_radii, double radius, const uint32_t* d_order,
                                  unsigned long long* d_counts, unsigned long long* d_counts2,
-                                 const unsigned long long* d_offsets, uint32_t* d_out, uint64_t out_capacity) {
+                                 const unsigned long long* d_offsets, uint32_t* d_out, uint64_t out_capacity,
+                                 const ChunkArgs* chunks) {
     cudaError_t e;
     if (nq == 0) return cudaSuccess;
     if ((e = c.packet_ctr.reserve(256)) != cudaSuccess) return e;
@@ -650,9 +795,9 @@ cudaError_t launch_radius_packet(Cloud& c, int kernel, int algo, bool fill, bool
     r.out_begin = 0;
     r.k = 0;
     r.cloud_id = 0;
-    return launch_radius_table(c.device, c.stream, kernel, algo, fill, fp32, nullptr, &r, (nq + 31) / 32, d_order,
+    return launch_radius_table(c.device, c.stream, kernel, algo, mode, fp32, nullptr, &r, (nq + 31) / 32, d_order,
                                d_counts, d_counts2, d_offsets, d_out, out_capacity, c.packet_ctr.as<uint32_t>(),
-                               c.stats.as<unsigned long long>(), c.d_err.as<uint32_t>());
+                               c.stats.as<unsigned long long>(), c.d_err.as<uint32_t>(), 0, chunks);
 }
 
 }  // namespace octb
