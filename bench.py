@@ -268,6 +268,132 @@ def run_batched(args, dev):
     }
 
 
+# ----------------------------------------------------------- large skewed cloud ---
+def run_large(args, dev):
+    """500M points on a 10 km tile (rural 5 pts/m^2 + urban building clusters ~2000 pts/m^2), built from HBM;
+    10M radius centres (r = 2.5 m, counts) and 10M kNN centres (k = 1000, in batches) on the FP32-filter
+    configuration; a 1% sample of each compared with the plain FP64 path."""
+    import torch
+
+    from octrees_benchmark_b200 import capi
+    from octrees_benchmark_b200.synth import large_tile_device
+
+    L = capi.lib()
+    MD = capi.OCT_MEM_DEVICE
+    n = args.large_points
+    t0 = time.perf_counter()
+    xyz = large_tile_device(n)
+    torch.cuda.synchronize()
+    gen_s = time.perf_counter() - t0
+    p = capi.OctParams(64, ENCODER, dev, 0)
+    h = C.c_void_p()
+    capi.check(L.oct_cloud_create(C.byref(p), C.byref(h)), None, "create")
+    info = capi.OctTreeInfo()
+    bt = []
+    for rep in range(3):
+        capi.check(L.oct_set_points(h, xyz.data_ptr(), n, MD), h)
+        capi.check(L.oct_synchronize(h), h)
+        t1 = time.perf_counter()
+        capi.check(L.oct_encode_sort(h, None, None, None, None, MD), h)
+        capi.check(L.oct_build(h, C.byref(info)), h)
+        torch.cuda.synchronize()
+        if rep:
+            bt.append(time.perf_counter() - t1)
+    build_s = min(bt)
+    peak, _ = measured_peak()
+    build_bytes = BUILD_BYTES_PER_POINT * n + BUILD_BYTES_PER_NODE * info.n_total
+    g = torch.Generator(device="cuda").manual_seed(30)
+    nq = args.large_queries
+    qr = xyz[torch.randint(0, n, (nq,), device="cuda", generator=g)].contiguous()
+    qk = xyz[torch.randint(0, n, (nq,), device="cuda", generator=g)].contiguous()
+    del xyz
+    torch.cuda.empty_cache()
+    stream = torch.cuda.Stream()
+    capi.check(L.oct_cloud_set_stream(h, C.c_void_p(stream.cuda_stream)), h)
+    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+
+    def config(packet, fp32):
+        cfg = capi.OctSearchConfig(packet, fp32, 8, 0, 256)
+        capi.check(L.oct_set_search_config(h, C.byref(cfg)), h)
+
+    # radius r = 2.5 m: neighbour counts of every centre, FP32 filter + FP64 band
+    config(1, 1)
+    counts = torch.empty(nq, dtype=torch.int64, device="cuda")
+    L.oct_search_stats(h, None, None, 1)
+    capi.check(L.oct_radius_count(h, 1, 2, qr.data_ptr(), min(nq, 100_000), None, RADIUS, counts.data_ptr(), MD), h)
+    ev0.record(stream)
+    capi.check(L.oct_radius_count(h, 1, 2, qr.data_ptr(), nq, None, RADIUS, counts.data_ptr(), MD), h)
+    ev1.record(stream)
+    capi.check(L.oct_synchronize(h), h)
+    rad_ms = ev0.elapsed_time(ev1)
+    tests, retests = C.c_uint64(), C.c_uint64()
+    L.oct_search_stats(h, C.byref(tests), C.byref(retests), 1)
+    total_nbrs = int(counts.sum().item())
+    # kNN k = 1000 in batches (the outputs of all 10M centres would be 120 GB)
+    K = args.large_k
+    kb = min(nq, 1_000_000)
+    kidx = torch.empty((kb, K), dtype=torch.int32, device="cuda")
+    kd2 = torch.empty((kb, K), dtype=torch.float64, device="cuda")
+    knn_ms = 0.0
+    for s in range(0, nq, kb):
+        m = min(kb, nq - s)
+        ev0.record(stream)
+        capi.check(L.oct_knn(h, qk[s:].data_ptr(), m, K, kidx.data_ptr(), kd2.data_ptr(), None, MD), h, "large kNN")
+        ev1.record(stream)
+        capi.check(L.oct_synchronize(h), h)
+        knn_ms += ev0.elapsed_time(ev1)
+    # parity on a 1 % sample: FP32-filter configuration against the plain FP64 path
+    ns = max(1, nq // 100)
+
+    def radius_csr(packet, fp32):
+        config(packet, fp32)
+        offs = torch.zeros(ns + 1, dtype=torch.int64, device="cuda")
+        tot = C.c_uint64()
+        st = L.oct_radius_search(h, 1, 2, qr.data_ptr(), ns, None, RADIUS, offs.data_ptr(), None, 0, C.byref(tot), MD)
+        assert st in (capi.OCT_OK, capi.OCT_ERR_CAPACITY)
+        out = torch.empty(max(1, tot.value), dtype=torch.int32, device="cuda")
+        capi.check(L.oct_radius_search(h, 1, 2, qr.data_ptr(), ns, None, RADIUS, offs.data_ptr(), out.data_ptr(),
+                                       tot.value, C.byref(tot), MD), h)
+        capi.check(L.oct_synchronize(h), h)
+        return offs, out[: tot.value]
+
+    def knn_sample(packet):
+        config(packet, 0)
+        i = torch.empty((ns, K), dtype=torch.int32, device="cuda")
+        d = torch.empty((ns, K), dtype=torch.float64, device="cuda")
+        capi.check(L.oct_knn(h, qk.data_ptr(), ns, K, i.data_ptr(), d.data_ptr(), None, MD), h)
+        capi.check(L.oct_synchronize(h), h)
+        return i, d
+
+    o1, i1 = radius_csr(1, 1)
+    o2, i2 = radius_csr(0, 0)
+    radius_same = bool(torch.equal(o1, o2) and torch.equal(i1, i2))
+    sample_nbrs = int(o1[-1].item())
+    del i1, i2
+    a1, d1 = knn_sample(1)
+    a2, d2 = knn_sample(0)
+    knn_same_d2 = bool(torch.equal(d1, d2))
+    knn_same_idx = bool(torch.equal(a1, a2))
+    L.oct_cloud_destroy(h)
+    return {
+        "workload": f"{n:,} points on a {10:g} km tile (seed 3, generated on the device): rural ground 5 pts/m^2 "
+                    f"(60 %), 50 urban building clusters of radius 10-40 m (~2000 pts/m^2, 40 %); Hilbert, leaf 64; "
+                    f"{nq:,} radius centres (sphere, neighborsPrune, r={RADIUS} m, FP32 filter + FP64 band, neighbour "
+                    f"counts) and {nq:,} kNN centres (k={K}, batches of {kb:,}) at random cloud points",
+        "build_ms": 1e3 * build_s, "build_mpts_s": n / build_s / 1e6,
+        "build_frac_of_hbm": build_bytes / build_s / 1e9 / peak, "nodes": info.n_total, "depth": info.max_depth_seen,
+        "radius_ms": rad_ms, "radius_qps": nq / (rad_ms / 1e3), "radius_neighbours": total_nbrs,
+        "radius_neighbours_per_s": total_nbrs / (rad_ms / 1e3),
+        "band_hit_fraction": retests.value / tests.value if tests.value else None,
+        "knn_ms": knn_ms, "knn_qps": nq / (knn_ms / 1e3),
+        "parity_sample": {"centres": ns, "radius_neighbours": sample_nbrs, "radius_csr_equal_plain": radius_same,
+                          "knn_d2_equal_plain": knn_same_d2, "knn_idx_equal_plain": knn_same_idx},
+        "generate_s": gen_s,
+        "timing": "build: wall clock of encode + sort + reorder + octree from points in HBM (best of 2 after a "
+                  "warm-up); radius and kNN: CUDA events around the calls on the cloud's stream",
+    }
+
+
 # ------------------------------------------------------------------ serving ---
 def run_serving(args, dev):
     """The serving stream replayed in real time: the batching server, then the plain one-request-per-launch one."""
@@ -578,6 +704,13 @@ def run_b200(args, rank, world, local_rank):
         serving = run_serving(args, dev)
         gc.collect()
         torch.cuda.empty_cache()
+    large = None
+    if world == 1 and args.large:
+        L.oct_cloud_destroy(h)  # room for the large cloud
+        h = None
+        gc.collect()
+        torch.cuda.empty_cache()
+        large = run_large(args, dev)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -597,7 +730,7 @@ def run_b200(args, rank, world, local_rank):
             "radius_qps": chosen["radius_qps"], "knn_qps": chosen["knn_qps"],
             "avg_neighbours": chosen["avg_neighbours"], "paths": paths,
             "batched_vs_plain": paths["engine"]["qps"] / paths["plain"]["qps"], "engine_config": eng_cfg,
-            "build": build, "batched": batched, "serving": serving, "roofline": roofline, "cpu_baseline": cpu,
+            "build": build, "batched": batched, "serving": serving, "large": large, "roofline": roofline, "cpu_baseline": cpu,
             "e2e": {"value": e2e_val, "unit": "queries/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "detail": e2e_detail},
             "gpu_launches": LAUNCHES_PER_STEP[args.search] * args.steps, "clocks": clk,
@@ -627,6 +760,10 @@ def main():
     ap.add_argument("--serve-seconds", type=float, default=60.0, help="length of the serving request stream")
     ap.add_argument("--serve-drain", type=float, default=30.0,
                     help="seconds each server may take after the stream ends before it is stopped")
+    ap.add_argument("--large", action="store_true", help="also run the 500M-point skewed cloud (not in the default run)")
+    ap.add_argument("--large-points", type=int, default=500_000_000)
+    ap.add_argument("--large-queries", type=int, default=10_000_000)
+    ap.add_argument("--large-k", type=int, default=1000)
     ap.add_argument("--points", type=int, default=N_POINTS, help="cloud size (smaller cases for profiling)")
     ap.add_argument("--queries", type=int, default=Q_RADIUS, help="radius and kNN queries per step, each")
     args = ap.parse_args()

@@ -67,6 +67,63 @@ def lidar_tile(n: int, tile_m: float, seed: int, n_cyl: int = 300, canopy_frac: 
     return out[rng.permutation(n)]
 
 
+def large_tile_device(n: int = 500_000_000, tile_m: float = 10_000.0, seed: int = 3, urban_frac: float = 0.4,
+                      n_clusters: int = 50, rural_density: float = 5.0, chunk: int = 50_000_000):
+    """A large skewed tile generated on the current CUDA device (torch, float64 (n, 3)).
+
+    Rural ground: ``(1 - urban_frac) n`` points at ``rural_density`` points/m^2
+    over a full-width band of the tile (its depth follows from the density),
+    z = the terrain of ``lidar_tile`` + N(0, 0.05 m).  Urban: ``urban_frac n``
+    points in ``n_clusters`` building clusters of radius 10-40 m anywhere on
+    the tile, each cluster's share proportional to its footprint (with the
+    defaults about 1,800-2,000 points/m^2), z uniform from the terrain up to the
+    building's height (5-30 m).  Drawn from a seeded CUDA generator in chunks;
+    rural points come first, then urban (the pipeline sorts them anyway)."""
+    import torch
+
+    g = torch.Generator(device="cuda").manual_seed(seed)
+    dev = torch.device("cuda", torch.cuda.current_device())
+    rng = np.random.default_rng(seed)
+    dirs = rng.uniform(0.0, math.pi, len(WAVELENGTHS))
+    phases = rng.uniform(0.0, 2.0 * math.pi, len(WAVELENGTHS))
+
+    def terrain(x, y):
+        z = torch.zeros_like(x)
+        for lam, th, ph in zip(WAVELENGTHS, dirs, phases):
+            z += AMPLITUDE * torch.sin((2.0 * math.pi / lam) * (x * math.cos(th) + y * math.sin(th)) + ph)
+        return z
+
+    out = torch.empty((n, 3), dtype=torch.float64, device=dev)
+    n_urb = int(round(n * urban_frac))
+    n_rur = n - n_urb
+    depth = min(tile_m, n_rur / (rural_density * tile_m)) if n_rur else 0.0
+    for s in range(0, n_rur, chunk):
+        m = min(chunk, n_rur - s)
+        x = torch.rand(m, dtype=torch.float64, device=dev, generator=g) * tile_m
+        y = torch.rand(m, dtype=torch.float64, device=dev, generator=g) * depth
+        out[s:s + m, 0] = x
+        out[s:s + m, 1] = y
+        out[s:s + m, 2] = terrain(x, y) + 0.05 * torch.randn(m, dtype=torch.float64, device=dev, generator=g)
+    if n_urb:
+        cr = torch.tensor(rng.uniform(10.0, 40.0, n_clusters), dtype=torch.float64, device=dev)
+        cx = torch.tensor(rng.uniform(40.0, tile_m - 40.0, n_clusters), dtype=torch.float64, device=dev)
+        cy = torch.tensor(rng.uniform(40.0, tile_m - 40.0, n_clusters), dtype=torch.float64, device=dev)
+        ch = torch.tensor(rng.uniform(5.0, 30.0, n_clusters), dtype=torch.float64, device=dev)
+        w = cr * cr
+        for s in range(0, n_urb, chunk):
+            m = min(chunk, n_urb - s)
+            which = torch.multinomial(w, m, replacement=True, generator=g)
+            rad = cr[which] * torch.sqrt(torch.rand(m, dtype=torch.float64, device=dev, generator=g))
+            ang = torch.rand(m, dtype=torch.float64, device=dev, generator=g) * (2.0 * math.pi)
+            px = cx[which] + rad * torch.cos(ang)
+            py = cy[which] + rad * torch.sin(ang)
+            o = n_rur + s
+            out[o:o + m, 0] = px
+            out[o:o + m, 1] = py
+            out[o:o + m, 2] = terrain(px, py) + torch.rand(m, dtype=torch.float64, device=dev, generator=g) * ch[which]
+    return out
+
+
 def query_indices(n_queries: int, cloud_size: int, seed: int = 42) -> np.ndarray:
     """SearchSet-style random centre indices into the (sorted) cloud."""
     rng = np.random.default_rng(seed)
