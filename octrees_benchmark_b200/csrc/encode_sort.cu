@@ -75,13 +75,30 @@ __global__ void __launch_bounds__(kBboxThreads) k_bbox(const double* __restrict_
             mx[a] = smax(mx[a], xyz[3 * i + a]);
         }
     }
-    for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < npairs; t += stride) {
-        const double2 a = xyz2[3 * t], b = xyz2[3 * t + 1], c = xyz2[3 * t + 2];
-        const double v[6] = {a.x, a.y, b.x, b.y, c.x, c.y};
+    // four pairs per thread and step (12 independent 16-byte loads in flight)
+    for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < npairs; t += 4 * stride) {
+        double2 v[4][3];
 #pragma unroll
-        for (int e = 0; e < 6; ++e) {
-            mn[e % 3] = smin(mn[e % 3], v[e]);  // std::min(localMin, p)
-            mx[e % 3] = smax(mx[e % 3], v[e]);  // std::max(localMax, p)
+        for (int u = 0; u < 4; ++u) {
+            const uint64_t tu = t + (uint64_t)u * stride;
+            if (tu < npairs) {
+                v[u][0] = xyz2[3 * tu];
+                v[u][1] = xyz2[3 * tu + 1];
+                v[u][2] = xyz2[3 * tu + 2];
+            } else {  // repeat a pair already read: min / max unchanged
+                v[u][0] = v[0][0];
+                v[u][1] = v[0][1];
+                v[u][2] = v[0][2];
+            }
+        }
+#pragma unroll
+        for (int u = 0; u < 4; ++u) {
+            const double e6[6] = {v[u][0].x, v[u][0].y, v[u][1].x, v[u][1].y, v[u][2].x, v[u][2].y};
+#pragma unroll
+            for (int e = 0; e < 6; ++e) {
+                mn[e % 3] = smin(mn[e % 3], e6[e]);  // std::min(localMin, p)
+                mx[e % 3] = smax(mx[e % 3], e6[e]);  // std::max(localMax, p)
+            }
         }
     }
     if (vec && (n & 1) && blockIdx.x == 0 && threadIdx.x == 0) {
@@ -218,7 +235,7 @@ __global__ void __launch_bounds__(256) k_scan_hist(SortCtl* ctl, uint64_t n, con
 }
 
 template <bool FIRST>
-__global__ void __launch_bounds__(kSortThreads) k_onesweep(const uint64_t* __restrict__ kin,
+__global__ void __launch_bounds__(kSortThreads, 3) k_onesweep(const uint64_t* __restrict__ kin,
                                                            const uint32_t* __restrict__ vin,
                                                            uint64_t* __restrict__ kout, uint32_t* __restrict__ vout,
                                                            uint64_t n, int pass, SortCtl* ctl,

@@ -10,8 +10,8 @@
 // lower bound), and prunes every octant whose lower bound exceeds the current
 // k-th distance.  The k best (squared distance, index) pairs live in a sorted
 // list in shared memory; leaf points that beat the k-th pair are appended to a
-// candidate buffer with a ballot, and a full buffer is merged into the list by
-// a bitonic sort.  All distances are the reference's FP64 expressions, so the
+// candidate buffer with a ballot, and a full buffer is sorted (descending) and
+// bitonic-merged into the list.  All distances are the reference's FP64 expressions, so the
 // returned squared distances are bitwise the reference's, and ordering by
 // (distance, index) resolves ties at the k-th distance by the lowest index.
 #include <algorithm>
@@ -52,17 +52,16 @@ __device__ __forceinline__ bool pair_less(double da, uint32_t ia, double db, uin
     return (da < db) || (da == db && ia < ib);
 }
 
-// Bitonic sort of P (power of two) (dist, idx) pairs in shared memory, one warp.
-template <int P>
-__device__ __forceinline__ void warp_bitonic_sort(double* d, uint32_t* ix) {
+// Bitonic sort of N (power of two) pairs in shared memory into descending order, one warp.
+template <int N>
+__device__ __forceinline__ void warp_bitonic_sort_desc(double* d, uint32_t* ix) {
     const int lane = threadIdx.x & 31;
-    for (int size = 2; size <= P; size <<= 1) {
+    for (int size = 2; size <= N; size <<= 1) {
         for (int stride = size >> 1; stride > 0; stride >>= 1) {
-            for (int i = lane; i < P / 2; i += 32) {
-                // i-th compare pair of this step (stride is a power of two)
+            for (int i = lane; i < N / 2; i += 32) {
                 const int lo = ((i & ~(stride - 1)) << 1) | (i & (stride - 1));
                 const int hi = lo + stride;
-                const bool asc = (lo & size) == 0;
+                const bool asc = (lo & size) != 0;  // mirrored network: the last stage runs descending
                 const double a = d[lo], b = d[hi];
                 const uint32_t ia = ix[lo], ib = ix[hi];
                 const bool swap = asc ? pair_less(b, ib, a, ia) : pair_less(a, ia, b, ib);
@@ -73,6 +72,25 @@ __device__ __forceinline__ void warp_bitonic_sort(double* d, uint32_t* ix) {
             }
             __syncwarp();
         }
+    }
+}
+
+// A bitonic sequence of N (power of two) pairs into ascending order, one warp.
+template <int N>
+__device__ __forceinline__ void warp_bitonic_merge(double* d, uint32_t* ix) {
+    const int lane = threadIdx.x & 31;
+    for (int stride = N >> 1; stride > 0; stride >>= 1) {
+        for (int i = lane; i < N / 2; i += 32) {
+            const int lo = ((i & ~(stride - 1)) << 1) | (i & (stride - 1));
+            const int hi = lo + stride;
+            const double a = d[lo], b = d[hi];
+            const uint32_t ia = ix[lo], ib = ix[hi];
+            if (pair_less(b, ib, a, ia)) {
+                d[lo] = b; d[hi] = a;
+                ix[lo] = ib; ix[hi] = ia;
+            }
+        }
+        __syncwarp();
     }
 }
 
@@ -152,7 +170,10 @@ __global__ void __launch_bounds__(kKnnThreads) k_knn(KnnArgs a) {
         bool failed = false;
 
         auto merge = [&]() {
-            warp_bitonic_sort<P>(sd, si);
+            // the list half is sorted already: sort the buffer half descending, then one
+            // bitonic merge of (ascending list, descending buffer) sorts all P pairs
+            warp_bitonic_sort_desc<LCAP>(sd + LCAP, si + LCAP);
+            warp_bitonic_merge<P>(sd, si);
             uint32_t tot = nl + nb;
             nl = tot < K ? tot : K;
             nb = 0;
