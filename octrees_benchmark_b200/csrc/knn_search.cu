@@ -97,8 +97,12 @@ __device__ __forceinline__ void warp_bitonic_merge(double* d, uint32_t* ix) {
 // LCAP: list capacity (power of two >= k); the candidate buffer has LCAP slots too.
 // MULTI: a table launch (the batched engine): each query's request gives its
 // cloud (kept per warp in shared memory), k and output slots.
+// CARRY: children's records are read when their parent is expanded and carried
+// on the stack (no dependent loads at a pop, empty leaves never pushed, subtrees
+// of at most `bucket` points scanned as one range); without it (the plain path)
+// a popped node's record is read then, one leaf at a time.
 #define KV(f) (MULTI ? s_view[warp].f : a.f)
-template <int LCAP, bool MULTI>
+template <int LCAP, bool MULTI, bool CARRY = true>
 __global__ void __launch_bounds__(kKnnThreads) k_knn(KnnArgs a) {
     constexpr int P = 2 * LCAP;
     extern __shared__ __align__(16) unsigned char smem[];
@@ -109,9 +113,11 @@ __global__ void __launch_bounds__(kKnnThreads) k_knn(KnnArgs a) {
     double* st_lb = base_d + (size_t)kKnnWarps * P + (size_t)warp * kKnnStack;
     uint32_t* base_u = reinterpret_cast<uint32_t*>(base_d + (size_t)kKnnWarps * (P + kKnnStack));
     uint32_t* si = base_u + (size_t)warp * P;
-    uint32_t* st_node = base_u + (size_t)kKnnWarps * P + (size_t)warp * kKnnStack;
+    // stack entry: a range [st_a, st_b) to scan, or (st_b == 0xffffffff) an internal node whose first child is st_a
+    uint32_t* st_a = base_u + (size_t)kKnnWarps * P + (size_t)warp * kKnnStack;
+    uint32_t* st_b = base_u + (size_t)kKnnWarps * (P + kKnnStack) + (size_t)warp * kKnnStack;
     uint8_t* st_depth =
-        reinterpret_cast<uint8_t*>(base_u + (size_t)kKnnWarps * (P + kKnnStack)) + (size_t)warp * kKnnStack;
+        reinterpret_cast<uint8_t*>(base_u + (size_t)kKnnWarps * (P + 2 * kKnnStack)) + (size_t)warp * kKnnStack;
     __shared__ double s_rad[MULTI ? kKnnWarps : 1][kMaxDepth + 1][3];
     __shared__ CloudView s_view[MULTI ? kKnnWarps : 1];
     double (*s_radii)[3] = s_rad[MULTI ? warp : 0];
@@ -188,9 +194,23 @@ __global__ void __launch_bounds__(kKnnThreads) k_knn(KnnArgs a) {
             }
         };
 
-        // stack of (node, depth, lower bound); the root's bound is 0 (linear_octree.hpp:904)
-        if (lane == 0) {
-            st_node[0] = 0;
+        // stack of (range or first child, depth, lower bound); the root's bound is 0
+        // (linear_octree.hpp:904).  Child records are read when their parent is
+        // expanded, so a popped entry needs no further dependent loads; empty leaves
+        // are never pushed and subtrees of at most `bucket` points are scanned as one
+        // range (extra points cannot change the k best pairs).
+        if constexpr (CARRY) {
+            const uint32_t fc0 = KV(offsets)[0];
+            const uint2 rg0 = KV(ranges)[0];
+            const bool scan0 = fc0 == 0 || rg0.y - rg0.x <= a.bucket;
+            if (lane == 0) {
+                st_a[0] = scan0 ? rg0.x : fc0;
+                st_b[0] = scan0 ? rg0.y : 0xffffffffu;
+                st_depth[0] = 0;
+                st_lb[0] = 0.0;
+            }
+        } else if (lane == 0) {
+            st_a[0] = 0;  // the root node
             st_depth[0] = 0;
             st_lb[0] = 0.0;
         }
@@ -198,20 +218,30 @@ __global__ void __launch_bounds__(kKnnThreads) k_knn(KnnArgs a) {
         int sp = 1;
         while (sp > 0 && !failed) {
             --sp;
-            const uint32_t node = st_node[sp];
+            uint32_t ea = st_a[sp], eb = st_b[sp];
             const double lb = st_lb[sp];
             const uint32_t depth = st_depth[sp];
             __syncwarp();
             if (lb > thr) continue;
-            const uint32_t fc = KV(offsets)[node];
-            if (fc == 0) {
-                // leaf: distances of its points, candidates into the buffer
-                const uint2 rg = KV(ranges)[node];
-                for (uint32_t b = rg.x; b < rg.y; b += 32) {
+            if constexpr (!CARRY) {  // plain: the popped node's record
+                const uint32_t node = ea;
+                const uint32_t fcn = KV(offsets)[node];
+                if (fcn == 0) {
+                    const uint2 rg = KV(ranges)[node];
+                    ea = rg.x;
+                    eb = rg.y;
+                } else {
+                    ea = fcn;
+                    eb = 0xffffffffu;
+                }
+            }
+            if (eb != 0xffffffffu) {
+                // points [ea, eb): distances, candidates into the buffer
+                for (uint32_t b = ea; b < eb; b += 32) {
                     const uint32_t i = b + lane;
                     double d = INFINITY;
                     bool cand = false;
-                    if (i < rg.y) {
+                    if (i < eb) {
                         d = dist_pp(p[0], p[1], p[2], KV(xs)[i], KV(ys)[i], KV(zs)[i]);
                         cand = pair_less(d, i, thr, thr_i);
                     }
@@ -230,13 +260,31 @@ __global__ void __launch_bounds__(kKnnThreads) k_knn(KnnArgs a) {
                     __syncwarp();
                 }
             } else {
-                // internal: lower bounds of the 8 children, nearest pushed last
+                // internal: lower bounds and records of the 8 children, nearest pushed last
+                const uint32_t fc = ea;
                 const uint32_t cd = depth + 1;
                 double clb = INFINITY;
                 bool keep = false;
+                uint32_t ca = 0, cb = 0;
                 if (lane < 8) {
-                    clb = dist_po(p, KV(centers) + 3ull * (fc + lane), s_radii[cd]);
-                    keep = !(clb > thr);
+                    const uint32_t child = fc + lane;
+                    clb = dist_po(p, KV(centers) + 3ull * child, s_radii[cd]);
+                    if constexpr (CARRY) {
+                        const uint32_t cfc = KV(offsets)[child];
+                        const uint2 rg = KV(ranges)[child];
+                        if (cfc && rg.y - rg.x > a.bucket) {
+                            ca = cfc;
+                            cb = 0xffffffffu;
+                            keep = !(clb > thr);
+                        } else {
+                            ca = rg.x;
+                            cb = rg.y;
+                            keep = (rg.y > rg.x) && !(clb > thr);
+                        }
+                    } else {
+                        ca = child;  // its record is read when it is popped
+                        keep = !(clb > thr);
+                    }
                 }
                 const uint32_t km = __ballot_sync(0xffffffffu, keep) & 0xffu;
                 const int nk = __popc(km);
@@ -254,7 +302,8 @@ __global__ void __launch_bounds__(kKnnThreads) k_knn(KnnArgs a) {
                 }
                 if (keep) {
                     const int slot = sp + pos;
-                    st_node[slot] = fc + lane;
+                    st_a[slot] = ca;
+                    st_b[slot] = cb;
                     st_lb[slot] = clb;
                     st_depth[slot] = (uint8_t)cd;
                 }
@@ -282,24 +331,34 @@ template <int LCAP>
 size_t knn_smem() {
     const size_t P = 2 * LCAP;
     const size_t per = P + kKnnStack;
-    return (size_t)kKnnWarps * (per * 8 + per * 4 + kKnnStack) + 16;
+    return (size_t)kKnnWarps * (per * 8 + (per + kKnnStack) * 4 + kKnnStack) + 16;
 }
 
 template <int LCAP>
-cudaError_t launch_l(const KnnArgs& a, int grid, cudaStream_t s) {
+cudaError_t launch_l(const KnnArgs& a, int grid, cudaStream_t s, bool carry) {
     const size_t smem = knn_smem<LCAP>();
-    cudaError_t e = cudaFuncSetAttribute(k_knn<LCAP, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    k_knn<LCAP, false><<<grid, kKnnThreads, smem, s>>>(a);
+    cudaError_t e;
+    if (carry) {
+        if ((e = cudaFuncSetAttribute(k_knn<LCAP, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)smem)) != cudaSuccess)
+            return e;
+        k_knn<LCAP, false, true><<<grid, kKnnThreads, smem, s>>>(a);
+    } else {
+        if ((e = cudaFuncSetAttribute(k_knn<LCAP, false, false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                      (int)smem)) != cudaSuccess)
+            return e;
+        k_knn<LCAP, false, false><<<grid, kKnnThreads, smem, s>>>(a);
+    }
     return cudaGetLastError();
 }
 
 // Table launch of the list kernel (the engine's kNN groups with 64 < k <= LCAP).
 template <int LCAP>
-cudaError_t launch_l_table(const DynGroup* d_grp, const uint32_t* order, uint32_t* idx, double* d2, uint32_t* counts,
-                           uint32_t* err, int grid, cudaStream_t s) {
+cudaError_t launch_l_table(const DynGroup* d_grp, const uint32_t* order, uint32_t bucket, uint32_t* idx, double* d2,
+                           uint32_t* counts, uint32_t* err, int grid, cudaStream_t s) {
     KnnArgs a{};
     a.grp = d_grp;
+    a.bucket = bucket;
     a.order = order;
     a.idx = idx;
     a.d2 = d2;
@@ -862,14 +921,15 @@ cudaError_t launch_knn_table(int device, cudaStream_t s, const DynGroup* d_grp, 
     const int grid = (int)(want < cap ? want : cap);
     if (d_grp) {
         if (kmax > 64) {  // the shared-memory list kernel, blocks per SM as its list fits
-            auto lgrid = [&](size_t smem) { return sms * (int)std::max<size_t>(1, (200u << 10) / smem); };
-            if (kmax <= 128) return launch_l_table<128>(d_grp, d_order, d_idx, d_d2, d_counts, d_err,
+            auto lgrid = [&](size_t smem) { return sms * (int)std::max<size_t>(1, (224u << 10) / (smem + 3072)); };
+            if (kmax <= 128) return launch_l_table<128>(d_grp, d_order, bucket, d_idx, d_d2, d_counts, d_err,
                                                         lgrid(knn_smem<128>()), s);
-            if (kmax <= 256) return launch_l_table<256>(d_grp, d_order, d_idx, d_d2, d_counts, d_err,
+            if (kmax <= 256) return launch_l_table<256>(d_grp, d_order, bucket, d_idx, d_d2, d_counts, d_err,
                                                         lgrid(knn_smem<256>()), s);
-            if (kmax <= 512) return launch_l_table<512>(d_grp, d_order, d_idx, d_d2, d_counts, d_err,
+            if (kmax <= 512) return launch_l_table<512>(d_grp, d_order, bucket, d_idx, d_d2, d_counts, d_err,
                                                         lgrid(knn_smem<512>()), s);
-            return launch_l_table<1024>(d_grp, d_order, d_idx, d_d2, d_counts, d_err, lgrid(knn_smem<1024>()), s);
+            return launch_l_table<1024>(d_grp, d_order, bucket, d_idx, d_d2, d_counts, d_err, lgrid(knn_smem<1024>()),
+                                        s);
         }
         if (kmax <= 32) k_knn_reg<1, true><<<grid, kKnnThreads, 0, s>>>(a);
         else k_knn_reg<2, true><<<grid, kKnnThreads, 0, s>>>(a);
@@ -913,7 +973,7 @@ cudaError_t launch_knn(Cloud& c, const double* d_centers, uint64_t nq, uint32_t 
     a.d2 = d_d2;
     a.counts = d_counts;
     a.err = c.d_err.as<uint32_t>();
-    a.bucket = c.knn_bucket;
+    a.bucket = c.packet ? c.knn_bucket : 0;  // the plain path descends to the leaves
     a.order = nullptr;
     if (c.packet) {  // curve-ordered queries: neighbouring warps share octants in cache
         cudaError_t e;
@@ -944,12 +1004,12 @@ cudaError_t launch_knn(Cloud& c, const double* d_centers, uint64_t nq, uint32_t 
         return launch_knn_table(c.device, c.stream, nullptr, &r, nq, k, a.order, c.knn_bucket, d_idx, d_d2, d_counts,
                                 c.d_err.as<uint32_t>());
     }
-    if (k <= 32) return launch_l<32>(a, grid, c.stream);
-    if (k <= 64) return launch_l<64>(a, grid, c.stream);
-    if (k <= 128) return launch_l<128>(a, grid, c.stream);
-    if (k <= 256) return launch_l<256>(a, grid, c.stream);
-    if (k <= 512) return launch_l<512>(a, grid, c.stream);
-    return launch_l<1024>(a, grid, c.stream);
+    if (k <= 32) return launch_l<32>(a, grid, c.stream, c.packet != 0);
+    if (k <= 64) return launch_l<64>(a, grid, c.stream, c.packet != 0);
+    if (k <= 128) return launch_l<128>(a, grid, c.stream, c.packet != 0);
+    if (k <= 256) return launch_l<256>(a, grid, c.stream, c.packet != 0);
+    if (k <= 512) return launch_l<512>(a, grid, c.stream, c.packet != 0);
+    return launch_l<1024>(a, grid, c.stream, c.packet != 0);
 }
 
 }  // namespace octb
