@@ -122,7 +122,12 @@ int oct_set_radius_group(oct_cloud cloud, int lanes);
  *  knn_bucket   kNN with k <= 64 on the packet path scans any subtree of at
  *               most this many points as one contiguous range instead of
  *               descending into it (default 256; 0 descends to the leaves).
- *               Extra points cannot change the k best pairs. */
+ *               Extra points cannot change the k best pairs.
+ *  reserved[0]  1: packet radius searches count, then fill at the scanned
+ *               offsets; 0 (default): one pass into per-query result chunks.
+ *  reserved[1]  kNN (k <= 64, packet path) provisional threshold, in percent of
+ *               the radius holding k points at the density of the query's first
+ *               cell: 0 = the default (120), < 0 = off.  Results are the same. */
 typedef struct {
     int32_t packet;
     int32_t fp32_filter;

@@ -345,6 +345,8 @@ int oct_set_search_config(oct_cloud h, const oct_search_config* cfg) {
     c.knn_packet = cfg->knn_packet ? 1 : 0;
     c.knn_bucket = cfg->knn_bucket > 0 ? (uint32_t)cfg->knn_bucket : 0u;
     c.two_pass = cfg->reserved[0] ? 1 : 0;
+    // provisional kNN threshold factor in percent: 0 the default, < 0 off
+    c.knn_est = cfg->reserved[1] > 0 ? cfg->reserved[1] / 100.0 : (cfg->reserved[1] == 0 ? kKnnEstimate : 0.0);
     return OCT_OK;
 }
 

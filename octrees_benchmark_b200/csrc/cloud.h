@@ -100,6 +100,10 @@ struct DynGroup {
     uint64_t nq;                // queries of the group
 };
 
+// Register kNN: provisional k-th distance = this factor x the radius that holds k
+// points at the density of the query's first cell (exact either way).
+constexpr double kKnnEstimate = 1.2;
+
 struct Cloud {
     oct_params params{};
     int device = 0;
@@ -151,6 +155,7 @@ struct Cloud {
     int knn_packet = 0;
     uint32_t knn_bucket = 256;
     int two_pass = 0;   // 1: packet radius searches count, then fill (no result chunks)
+    double knn_est = kKnnEstimate;  // register kNN: provisional-threshold factor (0: off)
     // one-pass radius search: result chunk pool, links, first chunk per query, counter
     DevBuf ck_pool, ck_next, ck_first, ck_ctr;
     uint32_t ck_cap = 0;
@@ -190,7 +195,9 @@ struct ChunkArgs {
 constexpr uint32_t kResultChunk = 64;
 
 // Packet radius search.  Either one request (`single`, host copy, `packets`
-// packets) or the group of a batch (`d_grp`, sizes read on the device).
+// packets) or the group of a batch (`d_grp`, sizes read on the device); with
+// both, every request of the group is on the cloud `single->cv` (kernel
+// parameters instead of per-request views).
 // mode: 0 count, 1 fill at d_offsets, 2 one pass into `chunks` (counts and
 // first chunks written; neighbors / neighborsPrune, FP64 only).
 cudaError_t launch_radius_table(int device, cudaStream_t s, int kernel, int algo, int mode, bool fp32,
@@ -208,7 +215,7 @@ cudaError_t launch_chunk_compact(int device, cudaStream_t s, const unsigned long
 // k: register lists up to 64, shared-memory lists up to 1024).
 cudaError_t launch_knn_table(int device, cudaStream_t s, const DynGroup* d_grp, const SearchReq* single, uint64_t nq,
                              uint32_t kmax, const uint32_t* d_order, uint32_t bucket, uint32_t* d_idx, double* d_d2,
-                             uint32_t* d_counts, uint32_t* d_err, int blocks_per_sm = 0);
+                             uint32_t* d_counts, uint32_t* d_err, int blocks_per_sm = 0, double est = 0.0);
 CloudView cloud_view(const Cloud& c);
 // Batched engine: the sort of query keys with device-side sizes (encode_sort.cu),
 // and the shared-memory limits of the table kNN list kernels (knn_search.cu).

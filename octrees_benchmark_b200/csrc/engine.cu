@@ -259,7 +259,15 @@ struct oct_engine_s {
     ReqTotal* h_totals = nullptr;
     size_t h_totals_cap = 0;
     uint32_t host_epoch = 0;
-    std::vector<std::pair<uint64_t, cudaGraphExec_t>> graphs;
+    struct Graph {
+        uint64_t sig;
+        bool one_cloud;
+        CloudView view;  // the cloud a one-cloud graph's kernels take as parameters
+        cudaGraphExec_t exec;
+    };
+    std::vector<Graph> graphs;
+    bool one_cloud = false;  // every request of the current batch is on one cloud
+    CloudView one_view{};
     // the batch in flight (or the last one)
     bool in_flight = false;
     bool have_results = false;
@@ -296,7 +304,7 @@ int cuda_fail_e(oct_engine e, cudaError_t err, const char* what) {
     } while (0)
 
 void drop_graphs(oct_engine e) {
-    for (auto& g : e->graphs) cudaGraphExecDestroy(g.second);
+    for (auto& g : e->graphs) cudaGraphExecDestroy(g.exec);
     e->graphs.clear();
 }
 
@@ -347,6 +355,10 @@ cudaError_t enqueue_work(oct_engine e) {
     Summary* sum = e->summary.as<Summary>();
     uint32_t* err = &sum->err;
     SortCtl* ctl = e->sort_ctl.as<SortCtl>();
+    // a batch on one cloud: its pointers go to the kernels as parameters
+    SearchReq one_req{};
+    one_req.cv = e->one_view;
+    const SearchReq* one = e->one_cloud ? &one_req : nullptr;
     if ((r = cudaMemsetAsync(sum, 0, sizeof(Summary), s)) != cudaSuccess) return r;
     if ((r = cudaMemsetAsync(ctl, 0, sizeof(SortCtl), s)) != cudaSuccess) return r;
     k_epoch_advance<<<1, 1, 0, s>>>(e->epoch.as<uint32_t>());
@@ -370,9 +382,9 @@ cudaError_t enqueue_work(oct_engine e) {
         cudaError_t r2 = cudaSuccess;
         for (int v = 0; v < kKnnVariants && r2 == cudaSuccess; ++v) {
             if (!((e->sig >> (kRadiusVariants + v)) & 1ull)) continue;
-            r2 = launch_knn_table(e->device, ks, &dyn->groups[kRadiusVariants + v], nullptr, 0, 32u << v,
+            r2 = launch_knn_table(e->device, ks, &dyn->groups[kRadiusVariants + v], one, 0, 32u << v,
                                   order, e->bucket, e->knn_idx.as<uint32_t>(), e->knn_d2.as<double>(),
-                                  e->knn_counts.as<uint32_t>(), err, e->knn_bps);
+                                  e->knn_counts.as<uint32_t>(), err, e->knn_bps, kKnnEstimate);
         }
         return r2;
     };
@@ -398,7 +410,7 @@ cudaError_t enqueue_work(oct_engine e) {
             for (int v = 0; v < kRadiusVariants; ++v) {
                 if (!((e->sig >> v) & 1ull)) continue;
                 const int kernel = v >> 2, algo = (v & 2) ? OCT_NEIGHBORS_PRUNE : OCT_NEIGHBORS;
-                if ((r = launch_radius_table(e->device, s, kernel, algo, 2, false, &dyn->groups[v], nullptr, 0, order,
+                if ((r = launch_radius_table(e->device, s, kernel, algo, 2, false, &dyn->groups[v], one, 0, order,
                                              counts, nullptr, nullptr, nullptr, 0, ctr + 2 * v, stats, err,
                                              e->radius_bps, &ck)) != cudaSuccess)
                     return r;
@@ -416,7 +428,7 @@ cudaError_t enqueue_work(oct_engine e) {
                     if (!((e->sig >> v) & 1ull)) continue;
                     const int kernel = v >> 2, algo = (v & 2) ? OCT_NEIGHBORS_PRUNE : OCT_NEIGHBORS;
                     if ((r = launch_radius_table(e->device, s, kernel, algo, fill ? 1 : 0, (v & 1) != 0,
-                                                 &dyn->groups[v], nullptr, 0, order, fill ? nullptr : counts, nullptr,
+                                                 &dyn->groups[v], one, 0, order, fill ? nullptr : counts, nullptr,
                                                  fill ? offs : nullptr, fill ? e->out.as<uint32_t>() : nullptr,
                                                  fill ? e->out.bytes / 4 : 0, ctr + 2 * v + pass, stats, err,
                                                  e->radius_bps)) != cudaSuccess)
@@ -453,8 +465,14 @@ int launch_batch(oct_engine e, bool record_start) {
         const uint64_t key = e->sig;
         cudaGraphExec_t exec = nullptr;
         for (auto& p : e->graphs)
-            if (p.first == key) exec = p.second;
+            if (p.sig == key && p.one_cloud == e->one_cloud &&
+                (!e->one_cloud || std::memcmp(&p.view, &e->one_view, sizeof(CloudView)) == 0))
+                exec = p.exec;
         if (!exec) {
+            if (e->graphs.size() >= 16) {  // keep the cache small: the oldest graph goes
+                cudaGraphExecDestroy(e->graphs.front().exec);
+                e->graphs.erase(e->graphs.begin());
+            }
             cudaGraph_t graph = nullptr;
             EK(cudaStreamBeginCapture(e->stream, cudaStreamCaptureModeThreadLocal));
             const cudaError_t r = enqueue_work(e);
@@ -467,7 +485,7 @@ int launch_batch(oct_engine e, bool record_start) {
             const cudaError_t r3 = cudaGraphInstantiate(&exec, graph, 0);
             cudaGraphDestroy(graph);
             EK(r3);
-            e->graphs.emplace_back(key, exec);
+            e->graphs.push_back({key, e->one_cloud, e->one_view, exec});
         }
         EK(cudaGraphLaunch(exec, e->stream));
     }
@@ -684,6 +702,9 @@ int submit(oct_engine e, const oct_request* rq, uint32_t n) {
     dyn->n_total = n_total;
     dyn->n_radius = n_radius;
     dyn->nreq = m;
+    // one cloud: the kernels take its pointers as parameters (the graph is kept per cloud view)
+    e->one_cloud = cloud_ids.size() == 1;
+    if (e->one_cloud) e->one_view = cloud_view(*cloud_ids.begin()->first);
     int req_bits = 0;
     while (m > 1 && (1u << req_bits) < m) ++req_bits;
     e->passes = 3 + (req_bits + 7) / 8;

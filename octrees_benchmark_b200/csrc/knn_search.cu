@@ -478,12 +478,15 @@ struct KnnTableArgs {
     double* d2;
     uint32_t* counts;
     uint32_t* err;
+    double est;              // > 0: provisional k-th distance from the first range's density (factor), 0: off
 };
 
+// MULTI 0: one request in the kernel parameters; 1: a request table, the
+// current request's cloud pointers in shared memory; 2: a request table whose
+// requests are all on the cloud single.cv (kernel parameters)
 #define KRQ(f) (MULTI ? reqs[ri].f : a.single.f)
-// cloud pointers of the warp's current request: shared memory in a table launch
-#define KRQV(f) (MULTI ? s_view[warp].f : a.single.cv.f)
-template <int R, bool MULTI>
+#define KRQV(f) (MULTI == 1 ? s_view[warp].f : a.single.cv.f)
+template <int R, int MULTI>
 __global__ void __launch_bounds__(kKnnThreads, 8) k_knn_reg(KnnTableArgs a) {
     __shared__ uint32_t st_a[kKnnWarps][kKnnStack];   // leaf: first point; internal: first child
     __shared__ uint32_t st_b[kKnnWarps][kKnnStack];   // leaf: end point; internal: 0xffffffff
@@ -492,7 +495,7 @@ __global__ void __launch_bounds__(kKnnThreads, 8) k_knn_reg(KnnTableArgs a) {
     __shared__ double s_rad[kKnnWarps][kMaxDepth + 1][3];
     __shared__ double s_bd[kKnnWarps][32];
     __shared__ uint32_t s_bi[kKnnWarps][32];
-    __shared__ CloudView s_view[MULTI ? kKnnWarps : 1];
+    __shared__ CloudView s_view[MULTI == 1 ? kKnnWarps : 1];
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     double (*s_radii)[3] = s_rad[warp];
     uint32_t cur_cloud = 0xffffffffu;
@@ -526,7 +529,7 @@ __global__ void __launch_bounds__(kKnnThreads, 8) k_knn_reg(KnnTableArgs a) {
             __syncwarp();
             const double* gr = &KRQ(cv.geom)->radii[0][0];
             for (int t = lane; t < (kMaxDepth + 1) * 3; t += 32) (&s_radii[0][0])[t] = gr[t];
-            if (MULTI && lane == 0) s_view[warp] = reqs[ri].cv;
+            if (MULTI == 1 && lane == 0) s_view[warp] = reqs[ri].cv;
             cur_cloud = KRQ(cloud_id);
             __syncwarp();
         }
@@ -548,6 +551,15 @@ __global__ void __launch_bounds__(kKnnThreads, 8) k_knn_reg(KnnTableArgs a) {
         uint32_t nb = 0;  // candidates waiting in the shared buffer
         double* bd = s_bd[warp];
         uint32_t* bi = s_bi[warp];
+        // Provisional threshold: at the first point range the search reaches (the
+        // query's own cell, nearest first), the squared radius holding about
+        // `est` x k points at that cell's points per unit of xy area.  Nodes and
+        // points beyond it are skipped; every point within it is still visited
+        // (lower bounds never exceed distances), so if at least k points lie
+        // within it the k best are exact, and otherwise the query runs again
+        // without it.
+        bool est_pending = a.est > 0.0, est_used = false;
+        for (int attempt = 0; attempt < 2; ++attempt) {
         auto merge_buf = [&]() {
             const double cdv = (lane < (int)nb) ? bd[lane] : (double)INFINITY;
             const uint32_t civ = (lane < (int)nb) ? bi[lane] : 0xffffffffu;
@@ -579,6 +591,15 @@ __global__ void __launch_bounds__(kKnnThreads, 8) k_knn_reg(KnnTableArgs a) {
             __syncwarp();
             if (lb > thr) continue;
             if (eb != 0xffffffffu) {
+                if (est_pending) {
+                    est_pending = false;
+                    const double area = 4.0 * s_radii[depth][0] * s_radii[depth][1];
+                    if (area > 0.0) {
+                        thr = a.est * (double)K * area / (3.14159265358979323846 * (double)(eb - ea));
+                        thr_i = 0xffffffffu;  // with the pair order this accepts d <= thr
+                        est_used = true;
+                    }
+                }
                 // leaf [ea, eb): candidates beat the k-th pair
                 for (uint32_t b = ea; b < eb; b += 32) {
                     const uint32_t i = b + lane;
@@ -650,8 +671,21 @@ __global__ void __launch_bounds__(kKnnThreads, 8) k_knn_reg(KnnTableArgs a) {
             __syncwarp();
             sp += nk;
         }
-        if (failed) set_err(a.err, kErrStackOverflow);
         if (nb) merge_buf();
+        if (!(est_used && nl < K) || failed) break;
+        // fewer than k points within the provisional threshold: again, without it
+#pragma unroll
+        for (int r = 0; r < R; ++r) {
+            L.d[r] = INFINITY;
+            L.i[r] = 0xffffffffu;
+        }
+        nl = 0;
+        thr = INFINITY;
+        thr_i = 0xffffffffu;
+        est_used = false;
+        __syncwarp();
+        }
+        if (failed) set_err(a.err, kErrStackOverflow);
         const uint64_t o = KRQ(out_begin) + ql * (uint64_t)K;
 #pragma unroll
         for (int r = 0; r < R; ++r) {
@@ -903,7 +937,7 @@ int sm_count_k(int device) {
 
 cudaError_t launch_knn_table(int device, cudaStream_t s, const DynGroup* d_grp, const SearchReq* single, uint64_t nq,
                              uint32_t kmax, const uint32_t* d_order, uint32_t bucket, uint32_t* d_idx, double* d_d2,
-                             uint32_t* d_counts, uint32_t* d_err, int blocks_per_sm) {
+                             uint32_t* d_counts, uint32_t* d_err, int blocks_per_sm, double est) {
     if (!d_grp && nq == 0) return cudaSuccess;
     KnnTableArgs a;
     a.single = single ? *single : SearchReq{};
@@ -915,6 +949,7 @@ cudaError_t launch_knn_table(int device, cudaStream_t s, const DynGroup* d_grp, 
     a.d2 = d_d2;
     a.counts = d_counts;
     a.err = d_err;
+    a.est = est;
     const int sms = sm_count_k(device);
     const uint64_t cap = (uint64_t)sms * (blocks_per_sm > 0 ? blocks_per_sm : 16);
     const uint64_t want = d_grp ? cap : (nq + kKnnWarps - 1) / kKnnWarps;
@@ -931,11 +966,16 @@ cudaError_t launch_knn_table(int device, cudaStream_t s, const DynGroup* d_grp, 
             return launch_l_table<1024>(d_grp, d_order, bucket, d_idx, d_d2, d_counts, d_err, lgrid(knn_smem<1024>()),
                                         s);
         }
-        if (kmax <= 32) k_knn_reg<1, true><<<grid, kKnnThreads, 0, s>>>(a);
-        else k_knn_reg<2, true><<<grid, kKnnThreads, 0, s>>>(a);
+        if (single) {  // every request of the group on the cloud single->cv
+            if (kmax <= 32) k_knn_reg<1, 2><<<grid, kKnnThreads, 0, s>>>(a);
+            else k_knn_reg<2, 2><<<grid, kKnnThreads, 0, s>>>(a);
+        } else {
+            if (kmax <= 32) k_knn_reg<1, 1><<<grid, kKnnThreads, 0, s>>>(a);
+            else k_knn_reg<2, 1><<<grid, kKnnThreads, 0, s>>>(a);
+        }
     } else {
-        if (kmax <= 32) k_knn_reg<1, false><<<grid, kKnnThreads, 0, s>>>(a);
-        else k_knn_reg<2, false><<<grid, kKnnThreads, 0, s>>>(a);
+        if (kmax <= 32) k_knn_reg<1, 0><<<grid, kKnnThreads, 0, s>>>(a);
+        else k_knn_reg<2, 0><<<grid, kKnnThreads, 0, s>>>(a);
     }
     return cudaGetLastError();
 }
@@ -1002,7 +1042,7 @@ cudaError_t launch_knn(Cloud& c, const double* d_centers, uint64_t nq, uint32_t 
         r.q_end = nq;
         r.k = k;
         return launch_knn_table(c.device, c.stream, nullptr, &r, nq, k, a.order, c.knn_bucket, d_idx, d_d2, d_counts,
-                                c.d_err.as<uint32_t>());
+                                c.d_err.as<uint32_t>(), 0, c.knn_est);
     }
     if (k <= 32) return launch_l<32>(a, grid, c.stream, c.packet != 0);
     if (k <= 64) return launch_l<64>(a, grid, c.stream, c.packet != 0);

@@ -54,9 +54,11 @@ constexpr uint32_t kChunk = kResultChunk;  // entries per result chunk (one-pass
 constexpr uint32_t kNoChunk = 0xffffffffu;
 
 struct PacketArgs {
-    SearchReq single;           // the request of a single-cloud search (grp == null)
+    SearchReq single;           // the request of a single-cloud search (grp == null); with
+                                // one_cloud, single.cv is the cloud of every request of grp
     const DynGroup* grp;        // sizes and request table of a batch group (device)
     uint64_t packets;           // packets of a single-request launch
+    bool one_cloud;             // host dispatch: grp's requests all search single.cv
     const uint32_t* order;      // query visiting order (global positions), or null
     unsigned long long* counts;
     unsigned long long* counts2;
@@ -135,12 +137,14 @@ __device__ __forceinline__ int f32_test(const LeafCtx& c, float4 p) {
     }
 }
 
-// MULTI: the launch covers a request table; otherwise the single request is read
-// from the kernel parameters (constant-bank operands, no registers held).  In
-// a table launch the cloud pointers of the warp's current request live in
-// shared memory (RQV), so the hot loops do not re-load them from the table.
+// MULTI 0: one request, read from the kernel parameters (constant-bank
+// operands, no registers held).  1: a request table; the cloud pointers of the
+// warp's current request live in shared memory (RQV), so the hot loops do not
+// re-load them from the table.  2: a request table whose requests are all on
+// one cloud, whose pointers are kernel parameters again (no shared-memory
+// reads in the hot loops).
 #define RQ(f) (MULTI ? reqs[cur_req].f : a.single.f)
-#define RQV(f) (MULTI ? s_view[warp].f : a.single.cv.f)
+#define RQV(f) (MULTI == 1 ? s_view[warp].f : a.single.cv.f)
 
 // Query parameters of lane j for the transposed leaf test: sphere / circle
 // (c0, c1, c2, r2), cube / square (bmin0..2, bmax0..2).
@@ -179,7 +183,7 @@ __device__ __forceinline__ bool inside_of(const double (*q)[32], int j, double p
 // from a pool (contiguous chunks for one long range, so positions stay
 // linear); per query the count and the first chunk are written, and
 // k_chunk_compact moves every chain into the CSR array after the scan.
-template <int KT, int ALGO, bool FILL, bool F32, bool MULTI, bool CHUNK = false>
+template <int KT, int ALGO, bool FILL, bool F32, int MULTI, bool CHUNK = false>
 __global__ void __launch_bounds__(kPkThreads) k_radius_packet(PacketArgs a) {
     // Transposed leaf test (FP64, neighbors / neighborsPrune): the lanes hold
     // consecutive points and test them against one query of the mask at a time,
@@ -187,7 +191,7 @@ __global__ void __launch_bounds__(kPkThreads) k_radius_packet(PacketArgs a) {
     constexpr bool kT = (ALGO != kStruct) && !F32;
     static_assert(!CHUNK || (FILL && kT), "one-pass mode needs the transposed FP64 form");
     constexpr int kStage = kT ? 1 : kPkWarps;  // point staging, per-lane loop forms only
-    __shared__ CloudView s_view[MULTI ? kPkWarps : 1];
+    __shared__ CloudView s_view[MULTI == 1 ? kPkWarps : 1];
     __shared__ uint32_t st_node[kPkWarps][kPkStack];
     __shared__ uint32_t st_fc[kPkWarps][kPkStack];     // first child, 0 for a leaf
     __shared__ uint2 st_rg[kPkWarps][kPkStack];        // point range
@@ -239,7 +243,7 @@ __global__ void __launch_bounds__(kPkThreads) k_radius_packet(PacketArgs a) {
             __syncwarp();
             const double* gr = &RQ(cv.geom)->radii[0][0];
             for (int t = lane; t < (kMaxDepth + 1) * 3; t += 32) (&s_radii[0][0])[t] = gr[t];
-            if (MULTI && lane == 0) s_view[warp] = reqs[cur_req].cv;
+            if (MULTI == 1 && lane == 0) s_view[warp] = reqs[cur_req].cv;
             cur_cloud = RQ(cloud_id);
             __syncwarp();
         }
@@ -630,8 +634,11 @@ int sm_count_p(int device) {
 }
 
 // mode: 0 count, 1 fill at known offsets, 2 one pass into result chunks
-template <int KT, int ALGO, bool MULTI>
+template <int KT, int ALGO, int MULTI>
 cudaError_t launch_pk_m(const PacketArgs& a, int mode, bool fp32, int grid, cudaStream_t s) {
+    if constexpr (MULTI == 2 && ALGO == kStruct) {  // batches do not search neighborsStruct
+        return cudaErrorInvalidValue;
+    }
     if (mode == 2) {
         if constexpr (ALGO != kStruct) k_radius_packet<KT, ALGO, true, false, MULTI, true><<<grid, kPkThreads, 0, s>>>(a);
     } else if (mode == 1) {
@@ -646,8 +653,11 @@ cudaError_t launch_pk_m(const PacketArgs& a, int mode, bool fp32, int grid, cuda
 
 template <int KT, int ALGO>
 cudaError_t launch_pk(const PacketArgs& a, int mode, bool fp32, int grid, cudaStream_t s) {
-    if (a.grp) return launch_pk_m<KT, ALGO, true>(a, mode, fp32, grid, s);
-    return launch_pk_m<KT, ALGO, false>(a, mode, fp32, grid, s);
+    if (a.grp) {
+        if (a.one_cloud) return launch_pk_m<KT, ALGO, 2>(a, mode, fp32, grid, s);
+        return launch_pk_m<KT, ALGO, 1>(a, mode, fp32, grid, s);
+    }
+    return launch_pk_m<KT, ALGO, 0>(a, mode, fp32, grid, s);
 }
 
 template <int KT>
@@ -736,6 +746,7 @@ cudaError_t launch_radius_table(int device, cudaStream_t s, int kernel, int algo
     PacketArgs a;
     a.single = single ? *single : SearchReq{};
     a.grp = d_grp;
+    a.one_cloud = d_grp != nullptr && single != nullptr;  // a batch on one cloud: its view in `single`
     a.packets = packets;
     a.order = d_order;
     a.counts = d_counts;

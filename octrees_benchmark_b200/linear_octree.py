@@ -104,13 +104,15 @@ class LinearOctree:
         check(self._L.oct_set_radius_group(self._h, int(lanes)), self._h)
 
     def set_search_config(self, packet: bool = True, fp32_filter: bool = False, radius_lanes: int = 8,
-                          knn_packet: bool = False, knn_bucket: int = 256, two_pass: bool = False):
+                          knn_packet: bool = False, knn_bucket: int = 256, two_pass: bool = False,
+                          knn_estimate: int = 0):
         """Search path: packet (32 curve-ordered queries per warp) or one query per
         ``radius_lanes`` lanes; FP32 leaf-relative filter with FP64 re-tests; kNN packets;
         ``two_pass`` counts then fills instead of the one-pass packet radius search."""
         cfg = OctSearchConfig(int(bool(packet)), int(bool(fp32_filter)), int(radius_lanes), int(bool(knn_packet)),
                               int(knn_bucket))
         cfg.reserved[0] = int(bool(two_pass))
+        cfg.reserved[1] = int(knn_estimate)  # kNN provisional threshold, percent; 0 default, < 0 off
         check(self._L.oct_set_search_config(self._h, C.byref(cfg)), self._h, "oct_set_search_config")
 
     def search_stats(self, reset: bool = False):
