@@ -52,7 +52,7 @@ Q_KNN = 500_000
 L2_FLUSH_BYTES = 512 << 20
 # device launches of this library per timed step: radius search (count, 3 scan kernels, fill), kNN;
 # the packet paths add the query ordering (keys, histogram scan, 3 sort passes) to the radius and the kNN call
-LAUNCHES_PER_STEP = {"plain": 6, "packet": 6 + 10, "packet_fp32": 6 + 10, "knn_packet": 6 + 10,
+LAUNCHES_PER_STEP = {"plain": 6, "packet": 6 + 10, "packet_fp32": 6 + 10, "knn_per_query": 6 + 10,
                      # engine: epoch, keys, histogram scan, 4 sort passes, radius count, 3 scan kernels,
                      # radius fill, request totals, kNN
                      "engine": 14}
@@ -493,8 +493,9 @@ def run_b200(args, rank, world, local_rank):
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
 
-    SEARCH_PATHS = {"plain": (0, 0, args.radius_group, 0), "packet": (1, 0, 8, 0), "packet_fp32": (1, 1, 8, 0),
-                    "knn_packet": (1, 0, 8, 1), "engine": (1, 0, 8, 0)}
+    # (packet, fp32_filter, lanes, kNN in groups of 8 queries per warp)
+    SEARCH_PATHS = {"plain": (0, 0, args.radius_group, 0), "packet": (1, 0, 8, 1), "packet_fp32": (1, 1, 8, 1),
+                    "knn_per_query": (1, 0, 8, 0), "engine": (1, 0, 8, 1)}
 
     # the batched engine: both request sets of a step in one graph launch (kNN beside the radius search)
     from types import SimpleNamespace
@@ -749,7 +750,7 @@ def main():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--radius-group", type=int, default=8, help="lanes per query of the plain path")
     ap.add_argument("--knn-bucket", type=int, default=256, help="kNN: subtrees this small are scanned as one range")
-    ap.add_argument("--search", default="engine", choices=["plain", "packet", "packet_fp32", "knn_packet", "engine"],
+    ap.add_argument("--search", default="engine", choices=["plain", "packet", "packet_fp32", "knn_per_query", "engine"],
                     help="search path whose numbers are the headline value")
     ap.add_argument("--cpu-seconds", type=float, default=10.0)
     ap.add_argument("--no-cpu", action="store_true")

@@ -116,9 +116,11 @@ int oct_set_radius_group(oct_cloud cloud, int lanes);
  *               boundary are re-tested in FP64 (packet path); 0 (default):
  *               every test in FP64.
  *  radius_lanes lanes per query when packet is 0: 8 (default), 16 or 32.
- *  knn_packet   1: kNN also walks 32 queries per warp (each lane its own
- *               k-heap; k <= 128); 0 (default): one warp per query, visited
- *               in curve order when packet is 1.
+ *  knn_packet   1 (default): kNN with k <= 64 on the packet path walks the
+ *               tree once per group of 8 curve-ordered queries per warp
+ *               (queries whose provisional threshold turns out too small
+ *               finish on the per-query kernel); 0: one warp per query,
+ *               visited in curve order when packet is 1.
  *  knn_bucket   kNN with k <= 64 on the packet path scans any subtree of at
  *               most this many points as one contiguous range instead of
  *               descending into it (default 256; 0 descends to the leaves).
@@ -127,7 +129,11 @@ int oct_set_radius_group(oct_cloud cloud, int lanes);
  *               offsets; 0 (default): one pass into per-query result chunks.
  *  reserved[1]  kNN (k <= 64, packet path) provisional threshold, in percent of
  *               the radius holding k points at the density of the query's first
- *               cell: 0 = the default (120), < 0 = off.  Results are the same. */
+ *               cell: 0 = the default (120), < 0 = off.  Results are the same.
+ *  reserved[2]  knn_packet: consecutive query groups a warp takes at a time
+ *               (1-64; 0 = the default); every group after the first of a
+ *               run starts from the previous group's k-th distances.  Results
+ *               are the same. */
 typedef struct {
     int32_t packet;
     int32_t fp32_filter;
@@ -258,6 +264,8 @@ int oct_engine_destroy(oct_engine engine);
 int oct_engine_set_stream(oct_engine engine, void* cuda_stream);
 int oct_engine_last_error(oct_engine engine, char* buf, size_t len);
 /* Search configuration of the engine (oct_search_config: fp32_filter, knn_bucket;
+ * knn_packet = 1 (the engine's default): kNN with k <= 64 in groups of 8
+ * curve-ordered queries per warp, 0: one warp per query;
  * reserved[0] = radius blocks per SM, reserved[1] = kNN blocks per SM, 0 = default;
  * reserved[2] = 1 to run kNN after the radius search instead of beside it). */
 int oct_engine_set_config(oct_engine engine, const oct_search_config* config);

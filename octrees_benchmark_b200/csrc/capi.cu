@@ -292,7 +292,8 @@ int oct_cloud_destroy(oct_cloud h) {
                           &c.sort_status, &c.d_ctl, &c.d_box, &c.d_err, &c.offsets, &c.ranges, &c.centers,
                           &c.frontier, &c.masks, &c.parts, &c.d_build, &c.q_centers, &c.q_radii, &c.q_counts,
                           &c.q_offsets, &c.q_out, &c.q_out2, &c.q_scan_tmp, &c.qs_keys, &c.qs_keys_alt, &c.qs_ord,
-                          &c.qs_ord_alt, &c.qs_status, &c.qs_ctl, &c.packet_ctr, &c.stats, &c.rel};
+                          &c.qs_ord_alt, &c.qs_status, &c.qs_ctl, &c.packet_ctr, &c.stats, &c.rel,
+                          &c.ck_pool, &c.ck_next, &c.ck_first, &c.ck_ctr, &c.knn_fb};
         for (DevBuf* b : bufs) b->release();
         if (c.pinned) cudaFreeHost(c.pinned);
         if (c.own_stream && c.stream) cudaStreamDestroy(c.stream);
@@ -347,6 +348,9 @@ int oct_set_search_config(oct_cloud h, const oct_search_config* cfg) {
     c.two_pass = cfg->reserved[0] ? 1 : 0;
     // provisional kNN threshold factor in percent: 0 the default, < 0 off
     c.knn_est = cfg->reserved[1] > 0 ? cfg->reserved[1] / 100.0 : (cfg->reserved[1] == 0 ? kKnnEstimate : 0.0);
+    if (cfg->reserved[2] < 0 || cfg->reserved[2] > 64)
+        return set_error(c, OCT_ERR_INVALID_ARG, "kNN group run length is 0 (default) to 64");
+    c.knn_chunk = cfg->reserved[2] > 0 ? (uint32_t)cfg->reserved[2] : kKnnGroupChunk;
     return OCT_OK;
 }
 
@@ -371,7 +375,8 @@ int oct_cloud_memory(oct_cloud h, uint64_t* bytes) {
                             &c.sort_status, &c.d_ctl, &c.d_box, &c.d_err, &c.offsets, &c.ranges, &c.centers,
                             &c.frontier, &c.masks, &c.parts, &c.d_build, &c.q_centers, &c.q_radii, &c.q_counts,
                             &c.q_offsets, &c.q_out, &c.q_out2, &c.q_scan_tmp, &c.qs_keys, &c.qs_keys_alt, &c.qs_ord,
-                            &c.qs_ord_alt, &c.qs_status, &c.qs_ctl, &c.packet_ctr, &c.stats, &c.rel};
+                            &c.qs_ord_alt, &c.qs_status, &c.qs_ctl, &c.packet_ctr, &c.stats, &c.rel,
+                            &c.ck_pool, &c.ck_next, &c.ck_first, &c.ck_ctr, &c.knn_fb};
     uint64_t s = 0;
     for (const DevBuf* b : bufs) s += b->bytes;
     *bytes = s;

@@ -103,6 +103,10 @@ struct DynGroup {
 // Register kNN: provisional k-th distance = this factor x the radius that holds k
 // points at the density of the query's first cell (exact either way).
 constexpr double kKnnEstimate = 1.2;
+// Group kNN: consecutive query groups a warp takes at a time (the later ones start
+// from the previous group's k-th distances).
+constexpr uint32_t kKnnGroupChunk = 4;
+constexpr uint32_t kKnnGroupQueries = 8;  // queries per warp of the group kNN
 
 struct Cloud {
     oct_params params{};
@@ -145,6 +149,7 @@ struct Cloud {
     DevBuf qs_keys, qs_keys_alt, qs_ord, qs_ord_alt, qs_status, qs_ctl;
     uint32_t qs_epoch = 0;
     DevBuf packet_ctr;  // dynamic packet counters
+    DevBuf knn_fb;      // group kNN: fallback count (u64) at 0, fallback query list (u32) from byte 16
     DevBuf stats;       // device counters: points tested, FP64 band re-tests, ...
     // FP32 leaf-relative coordinates (x, y, z, 0) per sorted point, built on demand
     DevBuf rel;
@@ -152,10 +157,11 @@ struct Cloud {
     // search configuration (oct_set_search_config)
     int packet = 1;
     int fp32_filter = 0;
-    int knn_packet = 0;
+    int knn_packet = 1;  // kNN (k <= 64, packet path): groups of queries per warp
     uint32_t knn_bucket = 256;
     int two_pass = 0;   // 1: packet radius searches count, then fill (no result chunks)
     double knn_est = kKnnEstimate;  // register kNN: provisional-threshold factor (0: off)
+    uint32_t knn_chunk = kKnnGroupChunk;  // group kNN: consecutive groups per warp fetch
     // one-pass radius search: result chunk pool, links, first chunk per query, counter
     DevBuf ck_pool, ck_next, ck_first, ck_ctr;
     uint32_t ck_cap = 0;
@@ -216,6 +222,16 @@ cudaError_t launch_chunk_compact(int device, cudaStream_t s, const unsigned long
 cudaError_t launch_knn_table(int device, cudaStream_t s, const DynGroup* d_grp, const SearchReq* single, uint64_t nq,
                              uint32_t kmax, const uint32_t* d_order, uint32_t bucket, uint32_t* d_idx, double* d_d2,
                              uint32_t* d_counts, uint32_t* d_err, int blocks_per_sm = 0, double est = 0.0);
+// Group kNN of a batch group (kmax <= 64: 8 curve-ordered queries per warp),
+// then the per-query kernel over the queries it hands back.  d_fb: the
+// fallback group (requests, kmax and q_begin of d_grp, nq = 0 before the
+// launch); d_fb_list: one entry per query position of the batch; d_packet_ctr:
+// two counters.
+cudaError_t launch_knn_group_table(int device, cudaStream_t s, const DynGroup* d_grp, DynGroup* d_fb,
+                                   const SearchReq* single, uint32_t kmax, const uint32_t* d_order, uint32_t bucket,
+                                   uint32_t* d_idx, double* d_d2, uint32_t* d_counts, uint32_t* d_err,
+                                   uint32_t* d_packet_ctr, uint32_t* d_fb_list, double est, uint32_t chunk,
+                                   int fb_blocks_per_sm);
 CloudView cloud_view(const Cloud& c);
 // Batched engine: the sort of query keys with device-side sizes (encode_sort.cu),
 // and the shared-memory limits of the table kNN list kernels (knn_search.cu).

@@ -48,6 +48,7 @@ constexpr uint32_t kEpochLimit = (1u << 22) - 1;
 
 struct EngineDyn {
     DynGroup groups[kGroups];
+    DynGroup fb[2];     // group kNN (k <= 32, 64): the queries handed back to the per-query kernel
     uint64_t n_total;   // query positions of the batch (the sort size)
     uint64_t n_radius;  // radius positions [0, n_radius); kNN positions follow
     uint32_t nreq;      // requests in the table (non-empty ones)
@@ -244,6 +245,7 @@ struct oct_engine_s {
     uint32_t bucket = 128;
     int radius_bps = 0, knn_bps = 0;
     int serial = 0;  // 1: kNN after the radius search on one stream; 0: kNN forked beside it
+    int knn_group = 1;  // kNN with k <= 64: groups of 8 queries per warp (0: one warp per query)
     // device arrays
     DevBuf desc;  // EngineDyn, then the SearchReq table
     DevBuf keys[2], ord[2];
@@ -252,6 +254,7 @@ struct oct_engine_s {
     DevBuf knn_idx, knn_d2, knn_counts;
     DevBuf ctrs, stats, summary, totals;
     DevBuf ck_pool, ck_next, ck_first, ck_ctr;  // one-pass radius: result chunks (ck_next has one word per chunk)
+    DevBuf knn_fb;  // group kNN fallback list, one entry per query position
     // pinned host staging
     unsigned char* h_stage = nullptr;
     size_t h_stage_bytes = 0;
@@ -382,9 +385,16 @@ cudaError_t enqueue_work(oct_engine e) {
         cudaError_t r2 = cudaSuccess;
         for (int v = 0; v < kKnnVariants && r2 == cudaSuccess; ++v) {
             if (!((e->sig >> (kRadiusVariants + v)) & 1ull)) continue;
-            r2 = launch_knn_table(e->device, ks, &dyn->groups[kRadiusVariants + v], one, 0, 32u << v,
-                                  order, e->bucket, e->knn_idx.as<uint32_t>(), e->knn_d2.as<double>(),
-                                  e->knn_counts.as<uint32_t>(), err, e->knn_bps, kKnnEstimate);
+            if (v < 2 && e->knn_group)
+                r2 = launch_knn_group_table(e->device, ks, &dyn->groups[kRadiusVariants + v], &dyn->fb[v], one,
+                                            32u << v, order, e->bucket, e->knn_idx.as<uint32_t>(),
+                                            e->knn_d2.as<double>(), e->knn_counts.as<uint32_t>(), err,
+                                            ctr + 2 * kRadiusVariants + 2 * v, e->knn_fb.as<uint32_t>(),
+                                            kKnnEstimate, kKnnGroupChunk, e->knn_bps);
+            else
+                r2 = launch_knn_table(e->device, ks, &dyn->groups[kRadiusVariants + v], one, 0, 32u << v,
+                                      order, e->bucket, e->knn_idx.as<uint32_t>(), e->knn_d2.as<double>(),
+                                      e->knn_counts.as<uint32_t>(), err, e->knn_bps, kKnnEstimate);
         }
         return r2;
     };
@@ -625,6 +635,7 @@ int submit(oct_engine e, const oct_request* rq, uint32_t n) {
     if ((st = grow(e, e->knn_idx, 4 * std::max<uint64_t>(knn_slots, 1))) != OCT_OK) return st;
     if ((st = grow(e, e->knn_d2, 8 * std::max<uint64_t>(knn_slots, 1))) != OCT_OK) return st;
     if ((st = grow(e, e->knn_counts, 4 * std::max<uint64_t>(n_total, 1))) != OCT_OK) return st;
+    if (knn_slots && e->knn_group && (st = grow(e, e->knn_fb, 4 * n_total)) != OCT_OK) return st;
     if ((st = grow(e, e->totals, sizeof(ReqTotal) * std::max<uint32_t>(m, 1))) != OCT_OK) return st;
     if (!e->fp32 && n_radius) {  // one-pass radius: a first chunk per query, a pool of at least 3 chunks per query
         if ((st = grow(e, e->ck_first, 4 * n_radius)) != OCT_OK) return st;
@@ -665,6 +676,9 @@ int submit(oct_engine e, const oct_request* rq, uint32_t n) {
         gr.reqs = d_table + t;
         gr.q_begin = pos;
         gr.kmax = 0;
+        // packets: 32 queries (radius), kGrpQ queries (group kNN); the per-query kNN kernel ignores them
+        const bool group_knn = e->knn_group && v >= kRadiusVariants && v < kRadiusVariants + 2;
+        const uint64_t per = group_knn ? kKnnGroupQueries : 32;
         uint32_t t0 = t;
         for (; t < m && var[rows[t]] == v; ++t) {
             const uint32_t i = rows[t];
@@ -692,11 +706,18 @@ int submit(oct_engine e, const oct_request* rq, uint32_t n) {
             table[t] = s;
             e->places[i].q_begin = pos;
             e->place_row[i] = (int32_t)t;
-            gr.packets += (r.nq + 31) / 32;
+            gr.packets += (r.nq + per - 1) / per;
             pos += r.nq;
         }
         gr.nreq = t - t0;
         gr.nq = pos - gr.q_begin;
+        if (group_knn) {  // the fallback group: the same requests, its count starts at 0
+            DynGroup& fb = dyn->fb[v - kRadiusVariants];
+            fb.reqs = gr.reqs;
+            fb.nreq = gr.nreq;
+            fb.kmax = gr.kmax;
+            fb.q_begin = gr.q_begin;
+        }
         sig |= 1ull << v;
     }
     dyn->n_total = n_total;
@@ -766,7 +787,7 @@ int oct_engine_create(const oct_engine_params* p, oct_engine* out) {
     if (r == cudaSuccess) r = prepare_knn_dyn();
     if (r == cudaSuccess) r = e->sort_ctl.reserve(sizeof(SortCtl));
     if (r == cudaSuccess) r = e->epoch.reserve(256);
-    if (r == cudaSuccess) r = e->ctrs.reserve(4 * 2 * kRadiusVariants);
+    if (r == cudaSuccess) r = e->ctrs.reserve(4 * 2 * (kRadiusVariants + 2));  // + group kNN (2 per variant)
     if (r == cudaSuccess) r = e->stats.reserve(64);
     if (r == cudaSuccess) r = e->summary.reserve(256);
     if (r == cudaSuccess) r = e->part.reserve(8 * (kScanBlocks + 1));
@@ -795,7 +816,7 @@ int oct_engine_destroy(oct_engine e) {
         DevBuf* bufs[] = {&e->desc, &e->keys[0], &e->keys[1], &e->ord[0], &e->ord[1], &e->sort_ctl, &e->sort_status,
                           &e->epoch, &e->counts, &e->offs, &e->part, &e->out, &e->knn_idx, &e->knn_d2,
                           &e->knn_counts, &e->ctrs, &e->stats, &e->summary, &e->totals,
-                          &e->ck_pool, &e->ck_next, &e->ck_first, &e->ck_ctr};
+                          &e->ck_pool, &e->ck_next, &e->ck_first, &e->ck_ctr, &e->knn_fb};
         for (DevBuf* b : bufs) b->release();
         if (e->h_stage) cudaFreeHost(e->h_stage);
         if (e->h_summary) cudaFreeHost(e->h_summary);
@@ -845,14 +866,16 @@ int oct_engine_set_config(oct_engine e, const oct_search_config* cfg) {
     }
     const int fp32 = cfg->fp32_filter ? 1 : 0;
     const uint32_t bucket = (uint32_t)cfg->knn_bucket;
+    const int knn_group = cfg->knn_packet ? 1 : 0;
     if (fp32 != e->fp32 || bucket != e->bucket || cfg->reserved[0] != e->radius_bps ||
-        cfg->reserved[1] != e->knn_bps || cfg->reserved[2] != e->serial)
+        cfg->reserved[1] != e->knn_bps || cfg->reserved[2] != e->serial || knn_group != e->knn_group)
         drop_graphs(e);
     e->fp32 = fp32;
     e->bucket = bucket;
     e->radius_bps = cfg->reserved[0];
     e->knn_bps = cfg->reserved[1];
     e->serial = cfg->reserved[2];
+    e->knn_group = knn_group;
     return OCT_OK;
 }
 
@@ -862,6 +885,7 @@ int oct_engine_get_config(oct_engine e, oct_search_config* cfg) {
     cfg->packet = 1;
     cfg->fp32_filter = e->fp32;
     cfg->radius_lanes = 32;
+    cfg->knn_packet = e->knn_group;
     cfg->knn_bucket = (int32_t)e->bucket;
     cfg->reserved[0] = e->radius_bps;
     cfg->reserved[1] = e->knn_bps;
@@ -988,7 +1012,7 @@ int oct_engine_memory(oct_engine e, uint64_t* bytes) {
     const DevBuf* bufs[] = {&e->desc, &e->keys[0], &e->keys[1], &e->ord[0], &e->ord[1], &e->sort_ctl,
                             &e->sort_status, &e->epoch, &e->counts, &e->offs, &e->part, &e->out, &e->knn_idx,
                             &e->knn_d2, &e->knn_counts, &e->ctrs, &e->stats, &e->summary, &e->totals,
-                            &e->ck_pool, &e->ck_next, &e->ck_first, &e->ck_ctr};
+                            &e->ck_pool, &e->ck_next, &e->ck_first, &e->ck_ctr, &e->knn_fb};
     uint64_t s = 0;
     for (const DevBuf* b : bufs) s += b->bytes;
     *bytes = s;
@@ -1035,23 +1059,28 @@ int oct_engine_autotune(oct_engine e, const oct_request* rq, uint32_t n, oct_sea
         cfg.reserved[0] = pick.reserved[0];
     }
     if (!knn.empty()) {
-        const int buckets[4] = {0, 64, 128, 256};
-        const int bps[2] = {8, 16};
+        // groups of queries per warp (blocks per SM follow from its shared memory), then one warp per query
+        struct KnnCfg {
+            int group, bucket, bps;
+        };
+        const KnnCfg cands[10] = {{1, 128, 0}, {1, 256, 0}, {0, 0, 8},   {0, 0, 16},  {0, 64, 8},
+                                  {0, 64, 16}, {0, 128, 8}, {0, 128, 16}, {0, 256, 8}, {0, 256, 16}};
         float best = 1e30f;
         oct_search_config pick = cfg;
-        for (int bk : buckets)
-            for (int b : bps) {
-                oct_search_config c2 = cfg;
-                c2.knn_bucket = bk;
-                c2.reserved[1] = b;
-                if ((st = oct_engine_set_config(e, &c2)) != OCT_OK) return st;
-                float t;
-                if ((st = time_cfg(knn, &t)) != OCT_OK) return st;
-                if (t < best) {
-                    best = t;
-                    pick = c2;
-                }
+        for (const KnnCfg& kc : cands) {
+            oct_search_config c2 = cfg;
+            c2.knn_packet = kc.group;
+            c2.knn_bucket = kc.bucket;
+            c2.reserved[1] = kc.bps;
+            if ((st = oct_engine_set_config(e, &c2)) != OCT_OK) return st;
+            float t;
+            if ((st = time_cfg(knn, &t)) != OCT_OK) return st;
+            if (t < best) {
+                best = t;
+                pick = c2;
             }
+        }
+        cfg.knn_packet = pick.knn_packet;
         cfg.knn_bucket = pick.knn_bucket;
         cfg.reserved[1] = pick.reserved[1];
     }

@@ -479,6 +479,7 @@ struct KnnTableArgs {
     uint32_t* counts;
     uint32_t* err;
     double est;              // > 0: provisional k-th distance from the first range's density (factor), 0: off
+    const unsigned long long* nq_dev;  // single-request launch: the query count in device memory (else nq)
 };
 
 // MULTI 0: one request in the kernel parameters; 1: a request table, the
@@ -511,16 +512,19 @@ __global__ void __launch_bounds__(kKnnThreads, 8) k_knn_reg(KnnTableArgs a) {
         nreq = a.grp->nreq;
         q0 = a.grp->q_begin;
         nq = a.grp->nq;
+    } else if (a.nq_dev) {
+        nq = *a.nq_dev;
     }
     const uint64_t nwarps = (uint64_t)gridDim.x * kKnnWarps;
     for (uint64_t w = (uint64_t)blockIdx.x * kKnnWarps + warp; w < nq; w += nwarps) {
         const uint64_t qpos = q0 + w;
+        const uint64_t q = a.order ? a.order[qpos] : qpos;  // global query position
         uint32_t ri = 0;
-        if (MULTI) {  // the request whose positions contain qpos (q_begin ascending)
+        if (MULTI) {  // the request whose positions contain q (q_begin ascending)
             uint32_t lo = 0, hi = nreq;
             while (hi - lo > 1) {
                 const uint32_t mid = (lo + hi) >> 1;
-                if (reqs[mid].q_begin <= qpos) lo = mid;
+                if (reqs[mid].q_begin <= q) lo = mid;
                 else hi = mid;
             }
             ri = lo;
@@ -534,7 +538,6 @@ __global__ void __launch_bounds__(kKnnThreads, 8) k_knn_reg(KnnTableArgs a) {
             __syncwarp();
         }
         const uint32_t K = KRQ(k);
-        const uint64_t q = a.order ? a.order[qpos] : qpos;  // global query position
         const uint64_t ql = q - KRQ(q_begin);
         const double* qc = KRQ(centers);
         const double p[3] = {qc[3 * ql], qc[3 * ql + 1], qc[3 * ql + 2]};
@@ -701,229 +704,437 @@ __global__ void __launch_bounds__(kKnnThreads, 8) k_knn_reg(KnnTableArgs a) {
 }
 
 // ---------------------------------------------------------------------------
-// Packet kNN: 32 curve-ordered queries per warp, one per lane.
+// Group kNN (k <= 64): kGrpQ curve-ordered queries per warp share one walk.
 //
-// The warp walks the tree once for its 32 queries.  Every lane keeps its own
-// k best (squared distance, index) pairs in a max-heap in shared memory (root =
-// the current k-th pair), so a lane's threshold is the root once the heap is
-// full.  A node is visited by the lanes whose lower bound to it (the
-// reference's clamp-to-box distance) does not exceed their threshold; the
-// children of a node are pushed with the mask of lanes that accept them,
-// nearest to the packet's centroid on top.  A leaf's points are staged in
-// shared memory once per warp and every visiting lane offers them to its heap.
-// At the end each lane heap-sorts its pairs into ascending (distance, index)
-// order, which is the device's tie rule.
+// Consecutive queries along the curve are a few metres apart, so the octants
+// their searches need overlap almost entirely: 8 of them visit ~2.6 internal
+// nodes per query where one query alone visits ~14 (10M-point tile, k = 50).
+// The warp walks the tree once for its group, nearest first by the smallest
+// lower bound of the group; a child is pushed with the mask of queries that
+// accept it and, per query, its lower bound rounded down to FP32 (a popped
+// entry is skipped for a query whose threshold has since dropped below it; the
+// rounding only keeps entries).  At an internal node four lanes per query
+// judge two children each.  A range (leaf, or subtree of at most `bucket`
+// points) is tested transposed: the lanes hold 32 consecutive points and test
+// them against one accepting query at a time, and the query's candidates
+// (pairs that beat its k-th pair) go to its own 32-entry buffer in shared
+// memory; a full buffer is merged into the query's sorted list (in shared
+// memory, R x 32 pairs) by the warp with the same register bitonic merge as
+// k_knn_reg.  Provisional thresholds: a warp takes `chunk` consecutive groups
+// at a time, and every group after the first of a run starts each query at
+// kGrpSeed x the largest k-th distance of the group before it (the k-th
+// distance varies slowly along the curve: this holds ~1.4 k points where the
+// density estimate of k_knn_reg holds several times more, so half the
+// candidates and merges go; longer runs widen the stretch of the curve that
+// the warps work on at once, which costs L2 hits).  The first group of a run,
+// and groups handed out one at a time at the end, take k_knn_reg's density
+// estimate from the first range each query reaches.  A query that ends with fewer than k pairs
+// inside its provisional threshold, and every query of a group whose stack
+// overflowed, is appended to a fallback list that k_knn_reg completes exactly.
 // ---------------------------------------------------------------------------
 
-template <int KCAP>
-struct KnnPkShape {
-    static constexpr int kWarps = (KCAP <= 64) ? 4 : 2;
+constexpr int kGrpQ = (int)kKnnGroupQueries;  // queries per warp (8: the bit masks are 8 bits)
+constexpr int kGrpWarps = 2;
+constexpr int kGrpThreads = 32 * kGrpWarps;
+constexpr int kGrpStack = 88;
+constexpr double kGrpSeed = 1.3;  // provisional threshold / previous group's largest k-th distance
+
+struct KnnGroupArgs {
+    SearchReq single;                 // one request (grp == null)
+    const DynGroup* grp;              // a batch group: sizes and requests on the device
+    uint64_t packets;                 // single: groups of kGrpQ queries
+    const uint32_t* order;            // visiting order (global query positions)
+    uint32_t bucket;
+    uint32_t* idx;
+    double* d2;
+    uint32_t* counts;
+    uint32_t* err;
+    double est;                       // provisional-threshold factor (0: off, also no seeding)
+    uint32_t* packet_ctr;             // [0] runs of `chunk` groups, [1] single groups at the end
+    uint32_t chunk;                   // consecutive groups per fetch (>= 1)
+    uint32_t* fb_list;                // queries left to k_knn_reg (global positions; a batch group's
+                                      // entries start at its q_begin)
+    unsigned long long* fb_count;
 };
 
-__device__ __forceinline__ bool pair_gt(double da, uint32_t ia, double db, uint32_t ib) {
-    return (da > db) || (da == db && ia > ib);
-}
+template <int R, int MULTI>
+__global__ void __launch_bounds__(kGrpThreads, 8) k_knn_group(KnnGroupArgs a) {
+    constexpr int G = kGrpQ;
+    constexpr int LC = 32 * R;
+    __shared__ double s_ld[kGrpWarps][G][LC];
+    __shared__ uint32_t s_li[kGrpWarps][G][LC];
+    __shared__ double s_bd[kGrpWarps][G][32];
+    __shared__ uint32_t s_bi[kGrpWarps][G][32];
+    __shared__ double s_q[kGrpWarps][G][3];
+    __shared__ double s_thr[kGrpWarps][G];
+    __shared__ uint32_t s_thri[kGrpWarps][G];
+    __shared__ uint32_t s_nl[kGrpWarps][G];
+    __shared__ uint32_t s_nb[kGrpWarps][G];
+    __shared__ uint32_t s_qg[kGrpWarps][G];
+    __shared__ uint32_t st_a[kGrpWarps][kGrpStack];
+    __shared__ uint32_t st_b[kGrpWarps][kGrpStack];
+    __shared__ float st_lb[kGrpWarps][kGrpStack][G];
+    __shared__ uint8_t st_d[kGrpWarps][kGrpStack];
+    __shared__ uint8_t st_m[kGrpWarps][kGrpStack];
+    __shared__ double s_rad[kGrpWarps][kMaxDepth + 1][3];
+    __shared__ CloudView s_view[MULTI == 1 ? kGrpWarps : 1];
 
-template <int KCAP>
-__global__ void __launch_bounds__(32 * KnnPkShape<KCAP>::kWarps) k_knn_packet(KnnArgs a, const uint32_t* order,
-                                                                              uint32_t* packet_ctr) {
-    constexpr int W = KnnPkShape<KCAP>::kWarps;
-    extern __shared__ __align__(16) unsigned char smem[];
-    // per warp: heap distances [KCAP][32], heap indices [KCAP][32]
-    double* hd_all = reinterpret_cast<double*>(smem);
-    uint32_t* hi_all = reinterpret_cast<uint32_t*>(hd_all + (size_t)W * KCAP * 32);
-    __shared__ uint32_t st_node[W][kKnnStack];
-    __shared__ uint32_t st_mask[W][kKnnStack];
-    __shared__ uint8_t st_depth[W][kKnnStack];
-    __shared__ double sx[W][32], sy[W][32], sz[W][32];
-    __shared__ double s_radii[kMaxDepth + 1][3];
-    for (int i = threadIdx.x; i < (kMaxDepth + 1) * 3; i += 32 * W) (&s_radii[0][0])[i] = (&a.geom->radii[0][0])[i];
-    __syncthreads();
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const uint32_t lbit = 1u << lane;
-    double* hd = hd_all + (size_t)warp * KCAP * 32;
-    uint32_t* hx = hi_all + (size_t)warp * KCAP * 32;
-#define HD(j) hd[(j) * 32 + lane]
-#define HX(j) hx[(j) * 32 + lane]
-    const uint32_t K = a.k;
+    double (*s_radii)[3] = s_rad[warp];
+    double (*ld)[LC] = s_ld[warp];
+    uint32_t (*li)[LC] = s_li[warp];
+    double (*bd)[32] = s_bd[warp];
+    uint32_t (*bi)[32] = s_bi[warp];
+    double (*qs)[3] = s_q[warp];
+    double* thr = s_thr[warp];
+    uint32_t* thri = s_thri[warp];
+    uint32_t* nls = s_nl[warp];
+    uint32_t* nbs = s_nb[warp];
+    uint32_t* sa = st_a[warp];
+    uint32_t* sb = st_b[warp];
+    float (*slb)[G] = st_lb[warp];
+    uint8_t* sdp = st_d[warp];
+    uint8_t* smk = st_m[warp];
+    uint32_t cur_cloud = 0xffffffffu;
+    const SearchReq* reqs = nullptr;
+    uint32_t nreq = 1;
+    uint64_t packets = a.packets;
+    uint64_t fb_base = 0;  // the fallback entries of a batch group start at its first position
+    if (MULTI) {
+        reqs = a.grp->reqs;
+        nreq = a.grp->nreq;
+        packets = a.grp->packets;
+        fb_base = a.grp->q_begin;
+    }
+    // lane roles at an internal node: query qj, children 2 cs and 2 cs + 1
+    const int qj = lane >> 2, cs = lane & 3;
+    // groups [0, p_chunked) go out in chunks, the rest one at a time
+    const uint64_t nw = (uint64_t)gridDim.x * kGrpWarps;
+    const uint64_t chunk = a.chunk;
+    const uint64_t p_chunked = (chunk > 1 && packets > 2 * nw) ? (packets - 2 * nw) / chunk * chunk : 0;
+    uint64_t next = 0, chunk_end = 0;
+    // seed: the previous group's largest k-th distance (< 0: none), its group and request
+    double seed_thr = -1.0;
+    uint64_t seed_packet = 0;
+    uint32_t seed_ri = 0;
 
     for (;;) {
-        uint32_t packet = 0;
-        if (lane == 0) packet = atomicAdd(packet_ctr, 1u);
-        packet = __shfl_sync(0xffffffffu, packet, 0);
-        const uint64_t i0 = (uint64_t)packet * 32;
-        if (i0 >= a.nq) break;
-        const uint64_t qpos = i0 + lane;
-        const bool valid = qpos < a.nq;
-        const uint32_t qi = valid ? order[qpos] : 0u;
-        const double p[3] = {a.q[3ull * qi], a.q[3ull * qi + 1], a.q[3ull * qi + 2]};
-        // packet centroid, used only to order children
-        const uint32_t vmask = __ballot_sync(0xffffffffu, valid);
-        const double inv = 1.0 / (double)__popc(vmask);
-        double cen[3];
-#pragma unroll
-        for (int ax = 0; ax < 3; ++ax) {
-            double v = valid ? p[ax] : 0.0;
-#pragma unroll
-            for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
-            cen[ax] = v * inv;
-        }
-        uint32_t hs = 0;  // heap size of this lane
-        auto thr_d = [&]() { return (hs < K) ? (double)INFINITY : HD(0); };
-        auto offer = [&](double d, uint32_t idx) {
-            if (hs < K) {
-                uint32_t j = hs++;
-                while (j > 0) {
-                    const uint32_t pj = (j - 1) >> 1;
-                    if (!pair_gt(d, idx, HD(pj), HX(pj))) break;
-                    HD(j) = HD(pj);
-                    HX(j) = HX(pj);
-                    j = pj;
-                }
-                HD(j) = d;
-                HX(j) = idx;
-            } else if (pair_less(d, idx, HD(0), HX(0))) {
-                uint32_t j = 0;
-                for (;;) {
-                    const uint32_t l = 2 * j + 1;
-                    if (l >= K) break;
-                    uint32_t m = l;
-                    if (l + 1 < K && pair_gt(HD(l + 1), HX(l + 1), HD(l), HX(l))) m = l + 1;
-                    if (!pair_gt(HD(m), HX(m), d, idx)) break;
-                    HD(j) = HD(m);
-                    HX(j) = HX(m);
-                    j = m;
-                }
-                HD(j) = d;
-                HX(j) = idx;
+        uint64_t packet;
+        if (next < chunk_end) {
+            packet = next++;
+        } else {
+            uint32_t v = 0;
+            if (lane == 0) v = atomicAdd(&a.packet_ctr[0], 1u);
+            v = __shfl_sync(0xffffffffu, v, 0);
+            const uint64_t c0 = (uint64_t)v * chunk;
+            if (c0 < p_chunked) {
+                packet = c0;
+                next = c0 + 1;
+                chunk_end = c0 + chunk;
+            } else {
+                uint32_t s = 0;
+                if (lane == 0) s = atomicAdd(&a.packet_ctr[1], 1u);
+                s = __shfl_sync(0xffffffffu, s, 0);
+                packet = p_chunked + s;
+                next = chunk_end = 0;
             }
+        }
+        if (packet >= packets) break;
+        uint32_t ri = 0;
+        if (MULTI) {  // the request of this group (packet_begin ascending over the table)
+            uint32_t lo = 0, hi = nreq;
+            while (hi - lo > 1) {
+                const uint32_t mid = (lo + hi) >> 1;
+                if (reqs[mid].packet_begin <= packet) lo = mid;
+                else hi = mid;
+            }
+            ri = lo;
+        }
+        if (KRQ(cloud_id) != cur_cloud) {
+            __syncwarp();
+            const double* gr = &KRQ(cv.geom)->radii[0][0];
+            for (int t = lane; t < (kMaxDepth + 1) * 3; t += 32) (&s_radii[0][0])[t] = gr[t];
+            if (MULTI == 1 && lane == 0) s_view[warp] = reqs[ri].cv;
+            cur_cloud = KRQ(cloud_id);
+            __syncwarp();
+        }
+        const uint32_t K = KRQ(k);
+        const uint64_t q_begin = KRQ(q_begin);
+        const uint64_t pos0 = q_begin + (uint64_t)G * (packet - KRQ(packet_begin));
+        const uint64_t q_end = KRQ(q_end);
+        const bool seeded = a.est > 0.0 && seed_thr >= 0.0 && packet == seed_packet + 1 && ri == seed_ri;
+        // lanes j < G: load query j, reset its state
+        bool valid = false;
+        if (lane < G) {
+            const uint64_t pos = pos0 + lane;
+            valid = pos < q_end;
+            const uint64_t q = valid ? (uint64_t)a.order[pos] : q_begin;
+            const uint64_t ql = q - q_begin;
+            const double* qc = KRQ(centers);
+            qs[lane][0] = qc[3 * ql];
+            qs[lane][1] = qc[3 * ql + 1];
+            qs[lane][2] = qc[3 * ql + 2];
+            thr[lane] = seeded ? kGrpSeed * seed_thr : (double)INFINITY;
+            thri[lane] = 0xffffffffu;  // with the pair order a provisional threshold accepts d <= thr
+            nls[lane] = 0;
+            nbs[lane] = 0;
+            s_qg[warp][lane] = (uint32_t)q;
+        }
+        for (int t = lane; t < G * LC; t += 32) {
+            (&ld[0][0])[t] = INFINITY;
+            (&li[0][0])[t] = 0xffffffffu;
+        }
+        const uint32_t vm = __ballot_sync(0xffffffffu, valid) & ((1u << G) - 1u);
+        uint32_t est_pend = (a.est > 0.0 && !seeded) ? vm : 0u, est_used = seeded ? vm : 0u;
+        bool failed = false;
+
+        // Merge query j's buffer (nb > 0 pairs) into its list (warp-uniform call).
+        auto merge = [&](int j, uint32_t nb) {
+            const double cdv = (lane < (int)nb) ? bd[j][lane] : (double)INFINITY;
+            const uint32_t civ = (lane < (int)nb) ? bi[j][lane] : 0xffffffffu;
+            RegList<R> L;
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                L.d[r] = ld[j][r * 32 + lane];
+                L.i[r] = li[j][r * 32 + lane];
+            }
+            reglist_merge32<R>(L, cdv, civ);
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                ld[j][r * 32 + lane] = L.d[r];
+                li[j][r * 32 + lane] = L.i[r];
+            }
+            uint32_t nl = nls[j] + nb;
+            if (nl > K) nl = K;
+            double td = 0.0;
+            uint32_t ti = 0;
+            if (nl == K) reglist_kth<R>(L, K, td, ti);
+            __syncwarp();
+            if (lane == 0) {
+                nls[j] = nl;
+                nbs[j] = 0;
+                if (nl == K) {
+                    thr[j] = td;
+                    thri[j] = ti;
+                }
+            }
+            __syncwarp();
         };
 
-        int sp = 0;
-        if (lane == 0) {
-            st_node[warp][0] = 0;
-            st_mask[warp][0] = vmask;
-            st_depth[warp][0] = 0;
+        // root (bound 0)
+        {
+            const uint32_t fc0 = KRQV(offsets)[0];
+            const uint2 rg0 = KRQV(ranges)[0];
+            const bool scan0 = fc0 == 0 || rg0.y - rg0.x <= a.bucket;
+            if (lane == 0) {
+                sa[0] = scan0 ? rg0.x : fc0;
+                sb[0] = scan0 ? rg0.y : 0xffffffffu;
+                sdp[0] = 0;
+                smk[0] = (uint8_t)vm;
+            }
+            if (lane < G) slb[0][lane] = 0.0f;
         }
         __syncwarp();
-        if (vmask) sp = 1;
-        bool failed = false;
+        int sp = vm ? 1 : 0;
         while (sp > 0) {
             --sp;
-            const uint32_t node = st_node[warp][sp];
-            const uint32_t mask = st_mask[warp][sp];
-            const uint32_t depth = st_depth[warp][sp];
+            const uint32_t ea = sa[sp], eb = sb[sp];
+            const uint32_t depth = sdp[sp];
+            bool act = false;
+            if (lane < G) act = ((smk[sp] >> lane) & 1u) && !((double)slb[sp][lane] > thr[lane]);
+            const uint32_t m = __ballot_sync(0xffffffffu, act) & ((1u << G) - 1u);
             __syncwarp();
-            // lanes still interested: lower bound within their threshold (root: bound 0)
-            bool act = (mask & lbit) != 0;
-            if (act && depth > 0) act = !(dist_po(p, a.centers + 3ull * node, s_radii[depth]) > thr_d());
-            const uint32_t am = __ballot_sync(0xffffffffu, act);
-            if (!am) continue;
-            const uint32_t fc = a.offsets[node];
-            if (fc == 0) {
-                const uint2 rg = a.ranges[node];
-                for (uint32_t b = rg.x; b < rg.y; b += 32) {
-                    const uint32_t idx = b + lane;
-                    if (idx < rg.y) {
-                        sx[warp][lane] = a.xs[idx];
-                        sy[warp][lane] = a.ys[idx];
-                        sz[warp][lane] = a.zs[idx];
-                    }
-                    __syncwarp();
-                    const uint32_t m = (rg.y - b < 32u) ? (rg.y - b) : 32u;
-                    if (act) {
-                        for (uint32_t t = 0; t < m; ++t) {
-                            const double d = dist_pp(p[0], p[1], p[2], sx[warp][t], sy[warp][t], sz[warp][t]);
-                            if (hs < K || !pair_gt(d, b + t, HD(0), HX(0))) offer(d, b + t);
+            if (!m) continue;
+            if (eb != 0xffffffffu) {
+                // a range [ea, eb)
+                const uint32_t pend = est_pend & m;
+                if (pend) {
+                    const double area = 4.0 * s_radii[depth][0] * s_radii[depth][1];
+                    if (area > 0.0) {
+                        if (lane < G && ((pend >> lane) & 1u)) {
+                            thr[lane] = a.est * (double)K * area / (3.14159265358979323846 * (double)(eb - ea));
+                            thri[lane] = 0xffffffffu;  // with the pair order this accepts d <= thr
                         }
+                        est_used |= pend;
                     }
+                    est_pend &= ~pend;
                     __syncwarp();
+                }
+                for (uint32_t b = ea; b < eb; b += 32) {
+                    const uint32_t i = b + lane;
+                    const bool in = i < eb;
+                    double px = 0.0, py = 0.0, pz = 0.0;
+                    if (in) {
+                        px = KRQV(xs)[i];
+                        py = KRQV(ys)[i];
+                        pz = KRQV(zs)[i];
+                    }
+                    uint32_t rem = m;
+                    while (rem) {
+                        const int j = __ffs(rem) - 1;
+                        rem &= rem - 1;
+                        const double d = dist_pp(qs[j][0], qs[j][1], qs[j][2], px, py, pz);
+                        bool cand = in && pair_less(d, i, thr[j], thri[j]);
+                        uint32_t hb = __ballot_sync(0xffffffffu, cand);
+                        if (!hb) continue;
+                        uint32_t nb = nbs[j];
+                        if (nb + __popc(hb) > 32u) {
+                            merge(j, nb);
+                            nb = 0;
+                            cand = cand && pair_less(d, i, thr[j], thri[j]);
+                            hb = __ballot_sync(0xffffffffu, cand);
+                        }
+                        if (cand) {
+                            const uint32_t slot = nb + __popc(hb & lanemask_lt());
+                            bd[j][slot] = d;
+                            bi[j][slot] = i;
+                        }
+                        __syncwarp();
+                        if (lane == 0) nbs[j] = nb + __popc(hb);
+                        __syncwarp();
+                    }
                 }
                 continue;
             }
+            // internal node: lane (qj, cs) judges children 2 cs and 2 cs + 1 for query qj
+            const uint32_t fc = ea;
             const uint32_t cd = depth + 1;
-            uint32_t cm[8];
-            const double th = act ? thr_d() : -1.0;
-#pragma unroll
-            for (int j = 0; j < 8; ++j) {
-                bool ok = false;
-                if (act) ok = !(dist_po(p, a.centers + 3ull * (fc + j), s_radii[cd]) > th);
-                cm[j] = __ballot_sync(0xffffffffu, ok);
+            const bool qa = (m >> qj) & 1u;
+            double lb0 = INFINITY, lb1 = INFINITY;
+            bool k0 = false, k1 = false;
+            if (qa) {
+                const double* c0 = KRQV(centers) + 3ull * (fc + 2 * cs);
+                const double t = thr[qj];
+                lb0 = dist_po(qs[qj], c0, s_radii[cd]);
+                lb1 = dist_po(qs[qj], c0 + 3, s_radii[cd]);
+                k0 = !(lb0 > t);
+                k1 = !(lb1 > t);
             }
-            // order key: the centroid's bound to each child, computed on lanes 0..7
-            double key = INFINITY;
-            if (lane < 8) key = dist_po(cen, a.centers + 3ull * (fc + lane), s_radii[cd]);
-            int np = 0;
+            const uint32_t B0 = __ballot_sync(0xffffffffu, k0);
+            const uint32_t B1 = __ballot_sync(0xffffffffu, k1);
+            // smallest accepting bound per child, over the lanes judging the same children
+            double v0 = k0 ? lb0 : (double)INFINITY, v1 = k1 ? lb1 : (double)INFINITY;
 #pragma unroll
-            for (int j = 0; j < 8; ++j) np += (cm[j] != 0);
-            if (sp + np > kKnnStack) {
+            for (int off = 4; off < 32; off <<= 1) {
+                v0 = fmin(v0, __shfl_xor_sync(0xffffffffu, v0, off));
+                v1 = fmin(v1, __shfl_xor_sync(0xffffffffu, v1, off));
+            }
+            // lane c < 8: child c's query mask, bound and record
+            const int cc = lane & 7;
+            const double x0 = __shfl_sync(0xffffffffu, v0, cc >> 1);
+            const double x1 = __shfl_sync(0xffffffffu, v1, cc >> 1);
+            double key = (cc & 1) ? x1 : x0;
+            uint32_t cm = 0;
+            uint32_t ca = 0, cb = 0;
+            if (lane < 8) {
+                const uint32_t Bw = (cc & 1) ? B1 : B0;
+#pragma unroll
+                for (int j = 0; j < G; ++j) cm |= ((Bw >> (4 * j + (cc >> 1))) & 1u) << j;
+                const uint32_t child = fc + lane;
+                const uint32_t cfc = KRQV(offsets)[child];
+                const uint2 rg = KRQV(ranges)[child];
+                if (cfc && rg.y - rg.x > a.bucket) {
+                    ca = cfc;
+                    cb = 0xffffffffu;
+                } else {
+                    ca = rg.x;
+                    cb = rg.y;
+                    if (rg.y == rg.x) cm = 0;  // an empty leaf holds no candidate
+                }
+            } else {
+                key = INFINITY;
+            }
+            const uint32_t pushm = __ballot_sync(0xffffffffu, lane < 8 && cm != 0);
+            const int np = __popc(pushm);
+            if (sp + np > kGrpStack) {
                 failed = true;
                 break;
             }
-            // slot of child j among pushed children: farther (or equal and higher octant) ones go deeper
+            // nearest on top: slot below every farther (or equal and higher octant) child
             int pos = 0;
-            uint32_t myc = 0;
 #pragma unroll
-            for (int j = 0; j < 8; ++j) {
-                const double kj = __shfl_sync(0xffffffffu, key, j);
-                if (lane < 8 && cm[j] != 0 && j != lane && ((kj > key) || (kj == key && j > lane))) ++pos;
-                if (lane == j) myc = cm[j];
+            for (int o = 0; o < 8; ++o) {
+                const double ol = __shfl_sync(0xffffffffu, key, o);
+                if (((pushm >> o) & 1u) && o != lane && ((ol > key) || (ol == key && o > lane))) ++pos;
             }
-            if (lane < 8 && myc != 0) {
-                st_node[warp][sp + pos] = fc + lane;
-                st_mask[warp][sp + pos] = myc;
-                st_depth[warp][sp + pos] = (uint8_t)cd;
+            const int slot = sp + pos;
+            if (lane < 8 && cm != 0) {
+                sa[slot] = ca;
+                sb[slot] = cb;
+                sdp[slot] = (uint8_t)cd;
+                smk[slot] = (uint8_t)cm;
             }
+            // per-query bounds of the pushed children, rounded down
+            const int s0 = __shfl_sync(0xffffffffu, slot, 2 * cs);
+            const int s1 = __shfl_sync(0xffffffffu, slot, 2 * cs + 1);
+            if (k0 && ((pushm >> (2 * cs)) & 1u)) slb[s0][qj] = __double2float_rd(lb0);
+            if (k1 && ((pushm >> (2 * cs + 1)) & 1u)) slb[s1][qj] = __double2float_rd(lb1);
             __syncwarp();
             sp += np;
         }
-        if (failed) set_err(a.err, kErrStackOverflow);
-        if (valid) {
-            // heap-sort into ascending (distance, index)
-            for (uint32_t e = hs; e > 1; --e) {
-                const uint32_t last = e - 1;
-                const double d = HD(last);
-                const uint32_t ix = HX(last);
-                HD(last) = HD(0);
-                HX(last) = HX(0);
-                uint32_t j = 0;
-                for (;;) {
-                    const uint32_t l = 2 * j + 1;
-                    if (l >= last) break;
-                    uint32_t m = l;
-                    if (l + 1 < last && pair_gt(HD(l + 1), HX(l + 1), HD(l), HX(l))) m = l + 1;
-                    if (!pair_gt(HD(m), HX(m), d, ix)) break;
-                    HD(j) = HD(m);
-                    HX(j) = HX(m);
-                    j = m;
+        __syncwarp();
+        // flush the buffers, then write each query's pairs or hand it to the fallback
+        uint32_t rem = vm;
+        while (rem) {
+            const int j = __ffs(rem) - 1;
+            rem &= rem - 1;
+            const uint32_t nb = nbs[j];
+            if (nb) merge(j, nb);
+            const uint32_t nl = nls[j];
+            const uint64_t q = s_qg[warp][j];
+            if (failed || (((est_used >> j) & 1u) && nl < K)) {
+                if (lane == 0) {
+                    const unsigned long long f = atomicAdd(a.fb_count, 1ull);
+                    a.fb_list[fb_base + f] = (uint32_t)q;
                 }
-                HD(j) = d;
-                HX(j) = ix;
+                continue;
             }
-            const uint64_t o = (uint64_t)qi * K;
-            for (uint32_t j = 0; j < K; ++j) {
-                a.idx[o + j] = (j < hs) ? HX(j) : 0xffffffffu;
-                a.d2[o + j] = (j < hs) ? HD(j) : (double)INFINITY;
+            const uint64_t o = KRQ(out_begin) + (q - q_begin) * (uint64_t)K;
+#pragma unroll
+            for (int r = 0; r < R; ++r) {
+                const uint32_t jj = (uint32_t)(r * 32 + lane);
+                if (jj < K) {
+                    a.idx[o + jj] = (jj < nl) ? li[j][jj] : 0xffffffffu;
+                    a.d2[o + jj] = (jj < nl) ? ld[j][jj] : (double)INFINITY;
+                }
             }
-            if (a.counts) a.counts[qi] = hs;
+            if (lane == 0 && a.counts) a.counts[q] = nl;
         }
+        // seed of the next group: the largest k-th distance of the queries that found k pairs
+        double mx = -1.0;
+        if (lane < G && ((vm >> lane) & 1u) && !failed && nls[lane] == K) mx = thr[lane];
+#pragma unroll
+        for (int off = 4; off > 0; off >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, off));
+        mx = __shfl_sync(0xffffffffu, mx, 0);
+        seed_thr = mx;
+        seed_packet = packet;
+        seed_ri = ri;
         __syncwarp();
     }
-#undef HD
-#undef HX
 }
 
-template <int KCAP>
-cudaError_t launch_knn_pk(const KnnArgs& a, const uint32_t* order, uint32_t* ctr, int sms, cudaStream_t s) {
-    constexpr int W = KnnPkShape<KCAP>::kWarps;
-    const size_t smem = (size_t)W * KCAP * 32 * 12;
-    cudaError_t e = cudaFuncSetAttribute(k_knn_packet<KCAP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    if (e != cudaSuccess) return e;
-    const uint64_t packets = (a.nq + 31) / 32;
-    const uint64_t want = (packets + W - 1) / W;
-    const uint64_t cap = (uint64_t)sms * 8;
-    const int grid = (int)(want < cap ? want : cap);
-    k_knn_packet<KCAP><<<grid, 32 * W, smem, s>>>(a, order, ctr);
+// Blocks per SM of a group-kNN instantiation (its shared memory sets it).
+template <int R, int MULTI>
+int group_blocks_per_sm() {
+    static int per = 0;
+    if (per == 0) {
+        int v = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, k_knn_group<R, MULTI>, kGrpThreads, 0) != cudaSuccess)
+            v = 1;
+        per = v > 0 ? v : 1;
+    }
+    return per;
+}
+
+template <int R, int MULTI>
+cudaError_t launch_group(const KnnGroupArgs& g, int sms, cudaStream_t s) {
+    uint64_t grid = (uint64_t)sms * group_blocks_per_sm<R, MULTI>();
+    if (!g.grp) {
+        const uint64_t want = (g.packets + kGrpWarps - 1) / kGrpWarps;
+        if (want < grid) grid = want;
+    }
+    if (grid == 0) return cudaSuccess;
+    k_knn_group<R, MULTI><<<(int)grid, kGrpThreads, 0, s>>>(g);
     return cudaGetLastError();
 }
 
@@ -939,7 +1150,7 @@ cudaError_t launch_knn_table(int device, cudaStream_t s, const DynGroup* d_grp, 
                              uint32_t kmax, const uint32_t* d_order, uint32_t bucket, uint32_t* d_idx, double* d_d2,
                              uint32_t* d_counts, uint32_t* d_err, int blocks_per_sm, double est) {
     if (!d_grp && nq == 0) return cudaSuccess;
-    KnnTableArgs a;
+    KnnTableArgs a{};
     a.single = single ? *single : SearchReq{};
     a.grp = d_grp;
     a.nq = nq;
@@ -978,6 +1189,37 @@ cudaError_t launch_knn_table(int device, cudaStream_t s, const DynGroup* d_grp, 
         else k_knn_reg<2, 0><<<grid, kKnnThreads, 0, s>>>(a);
     }
     return cudaGetLastError();
+}
+
+cudaError_t launch_knn_group_table(int device, cudaStream_t s, const DynGroup* d_grp, DynGroup* d_fb,
+                                   const SearchReq* single, uint32_t kmax, const uint32_t* d_order, uint32_t bucket,
+                                   uint32_t* d_idx, double* d_d2, uint32_t* d_counts, uint32_t* d_err,
+                                   uint32_t* d_packet_ctr, uint32_t* d_fb_list, double est, uint32_t chunk,
+                                   int fb_blocks_per_sm) {
+    if (kmax > 64) return cudaErrorInvalidValue;
+    cudaError_t e;
+    if ((e = cudaMemsetAsync(d_packet_ctr, 0, 8, s)) != cudaSuccess) return e;
+    KnnGroupArgs g{};
+    g.single = single ? *single : SearchReq{};
+    g.grp = d_grp;
+    g.order = d_order;
+    g.bucket = bucket;
+    g.idx = d_idx;
+    g.d2 = d_d2;
+    g.counts = d_counts;
+    g.err = d_err;
+    g.est = est;
+    g.packet_ctr = d_packet_ctr;
+    g.chunk = chunk > 0 ? chunk : 1;
+    g.fb_list = d_fb_list;
+    g.fb_count = reinterpret_cast<unsigned long long*>(&d_fb->nq);
+    const int sms = sm_count_k(device);
+    if (single) e = (kmax <= 32) ? launch_group<1, 2>(g, sms, s) : launch_group<2, 2>(g, sms, s);
+    else e = (kmax <= 32) ? launch_group<1, 1>(g, sms, s) : launch_group<2, 1>(g, sms, s);
+    if (e != cudaSuccess) return e;
+    // the queries handed back, exactly and without the provisional threshold
+    return launch_knn_table(device, s, d_fb, single, 0, kmax, d_fb_list, bucket, d_idx, d_d2, d_counts, d_err,
+                            fb_blocks_per_sm, 0.0);
 }
 
 cudaError_t prepare_knn_dyn() {
@@ -1019,18 +1261,6 @@ cudaError_t launch_knn(Cloud& c, const double* d_centers, uint64_t nq, uint32_t 
         cudaError_t e;
         if ((e = launch_query_order(c, d_centers, nq, &a.order)) != cudaSuccess) return e;
     }
-    if (c.packet && c.knn_packet && k <= 128) {
-        cudaError_t e;
-        const uint32_t* order = a.order;
-        if ((e = c.packet_ctr.reserve(256)) != cudaSuccess) return e;
-        if ((e = cudaMemsetAsync(c.packet_ctr.ptr, 0, 4, c.stream)) != cudaSuccess) return e;
-        uint32_t* ctr = c.packet_ctr.as<uint32_t>();
-        const int sms = sm_count_k(c.device);
-        if (k <= 16) return launch_knn_pk<16>(a, order, ctr, sms, c.stream);
-        if (k <= 32) return launch_knn_pk<32>(a, order, ctr, sms, c.stream);
-        if (k <= 64) return launch_knn_pk<64>(a, order, ctr, sms, c.stream);
-        return launch_knn_pk<128>(a, order, ctr, sms, c.stream);
-    }
     const uint64_t want = (nq + kKnnWarps - 1) / kKnnWarps;
     const uint64_t cap = (uint64_t)sm_count_k(c.device) * 16;
     const int grid = (int)(want < cap ? want : cap);
@@ -1041,8 +1271,48 @@ cudaError_t launch_knn(Cloud& c, const double* d_centers, uint64_t nq, uint32_t 
         r.q_begin = 0;
         r.q_end = nq;
         r.k = k;
-        return launch_knn_table(c.device, c.stream, nullptr, &r, nq, k, a.order, c.knn_bucket, d_idx, d_d2, d_counts,
-                                c.d_err.as<uint32_t>(), 0, c.knn_est);
+        if (!c.knn_packet)
+            return launch_knn_table(c.device, c.stream, nullptr, &r, nq, k, a.order, c.knn_bucket, d_idx, d_d2,
+                                    d_counts, c.d_err.as<uint32_t>(), 0, c.knn_est);
+        // groups of curve-ordered queries, then the exact per-query kernel for the queries they hand back
+        cudaError_t e;
+        if ((e = c.packet_ctr.reserve(256)) != cudaSuccess) return e;
+        if ((e = c.knn_fb.reserve(16 + 4 * nq)) != cudaSuccess) return e;
+        if ((e = cudaMemsetAsync(c.packet_ctr.ptr, 0, 8, c.stream)) != cudaSuccess) return e;
+        if ((e = cudaMemsetAsync(c.knn_fb.ptr, 0, 8, c.stream)) != cudaSuccess) return e;
+        KnnGroupArgs g{};
+        g.single = r;
+        g.grp = nullptr;
+        g.packets = (nq + kGrpQ - 1) / kGrpQ;
+        g.order = a.order;
+        g.bucket = c.knn_bucket;
+        g.idx = d_idx;
+        g.d2 = d_d2;
+        g.counts = d_counts;
+        g.err = c.d_err.as<uint32_t>();
+        g.est = c.knn_est;
+        g.packet_ctr = c.packet_ctr.as<uint32_t>();
+        g.chunk = c.knn_chunk;
+        g.fb_count = c.knn_fb.as<unsigned long long>();
+        g.fb_list = reinterpret_cast<uint32_t*>(c.knn_fb.as<unsigned char>() + 16);
+        const int sms = sm_count_k(c.device);
+        e = (k <= 32) ? launch_group<1, 0>(g, sms, c.stream) : launch_group<2, 0>(g, sms, c.stream);
+        if (e != cudaSuccess) return e;
+        KnnTableArgs f{};
+        f.single = r;
+        f.nq = nq;
+        f.nq_dev = g.fb_count;
+        f.order = g.fb_list;
+        f.bucket = c.knn_bucket;
+        f.idx = d_idx;
+        f.d2 = d_d2;
+        f.counts = d_counts;
+        f.err = g.err;
+        f.est = 0.0;  // exact without the provisional threshold
+        const int fgrid = sms * 16;
+        if (k <= 32) k_knn_reg<1, 0><<<fgrid, kKnnThreads, 0, c.stream>>>(f);
+        else k_knn_reg<2, 0><<<fgrid, kKnnThreads, 0, c.stream>>>(f);
+        return cudaGetLastError();
     }
     if (k <= 32) return launch_l<32>(a, grid, c.stream, c.packet != 0);
     if (k <= 64) return launch_l<64>(a, grid, c.stream, c.packet != 0);

@@ -92,8 +92,8 @@ class BatchEngine:
 
     # ---- configuration ------------------------------------------------------
     def set_config(self, fp32_filter: bool = False, knn_bucket: int = 128, radius_blocks_per_sm: int = 0,
-                   knn_blocks_per_sm: int = 0, serial: bool = False):
-        cfg = OctSearchConfig(1, int(bool(fp32_filter)), 32, 0, int(knn_bucket))
+                   knn_blocks_per_sm: int = 0, serial: bool = False, knn_group: bool = True):
+        cfg = OctSearchConfig(1, int(bool(fp32_filter)), 32, int(bool(knn_group)), int(knn_bucket))
         cfg.reserved[0] = int(radius_blocks_per_sm)
         cfg.reserved[1] = int(knn_blocks_per_sm)
         cfg.reserved[2] = int(bool(serial))
@@ -103,7 +103,7 @@ class BatchEngine:
         cfg = OctSearchConfig()
         _engine_check(self._L.oct_engine_get_config(self._h, C.byref(cfg)), self._h, "oct_engine_get_config")
         return dict(fp32_filter=cfg.fp32_filter, knn_bucket=cfg.knn_bucket, radius_blocks_per_sm=cfg.reserved[0],
-                    knn_blocks_per_sm=cfg.reserved[1], serial=cfg.reserved[2])
+                    knn_blocks_per_sm=cfg.reserved[1], serial=cfg.reserved[2], knn_group=cfg.knn_packet)
 
     def autotune(self, requests: Sequence[Request]) -> dict:
         _sync_current_stream()

@@ -54,7 +54,7 @@ class LinearOctree:
 
     def __init__(self, points, encoder="hilbert", max_points_leaf: int = 128, device: int = 0,
                  radius_group: int = 8, stream=None, packet: bool = True, fp32_filter: bool = False,
-                 knn_packet: bool = False, knn_bucket: int = 256):
+                 knn_packet: bool = True, knn_bucket: int = 256):
         L = lib()
         self._L = L
         self.encoder = ENCODERS[encoder]
@@ -104,15 +104,17 @@ class LinearOctree:
         check(self._L.oct_set_radius_group(self._h, int(lanes)), self._h)
 
     def set_search_config(self, packet: bool = True, fp32_filter: bool = False, radius_lanes: int = 8,
-                          knn_packet: bool = False, knn_bucket: int = 256, two_pass: bool = False,
-                          knn_estimate: int = 0):
+                          knn_packet: bool = True, knn_bucket: int = 256, two_pass: bool = False,
+                          knn_estimate: int = 0, knn_group_run: int = 0):
         """Search path: packet (32 curve-ordered queries per warp) or one query per
-        ``radius_lanes`` lanes; FP32 leaf-relative filter with FP64 re-tests; kNN packets;
-        ``two_pass`` counts then fills instead of the one-pass packet radius search."""
+        ``radius_lanes`` lanes; FP32 leaf-relative filter with FP64 re-tests; kNN in groups
+        of 8 queries per warp (``knn_packet``; else one warp per query); ``two_pass`` counts
+        then fills instead of the one-pass packet radius search."""
         cfg = OctSearchConfig(int(bool(packet)), int(bool(fp32_filter)), int(radius_lanes), int(bool(knn_packet)),
                               int(knn_bucket))
         cfg.reserved[0] = int(bool(two_pass))
         cfg.reserved[1] = int(knn_estimate)  # kNN provisional threshold, percent; 0 default, < 0 off
+        cfg.reserved[2] = int(knn_group_run)  # consecutive kNN groups per warp fetch; 0 default
         check(self._L.oct_set_search_config(self._h, C.byref(cfg)), self._h, "oct_set_search_config")
 
     def search_stats(self, reset: bool = False):

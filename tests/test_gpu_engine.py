@@ -132,6 +132,34 @@ def test_engine_matches_oracle(torch, clouds, port):
     assert_knn_equal(idx, d2, cnt, oi, od, ocnt, sxyz, c, "engine kNN vs oracle")
 
 
+@pytest.mark.parametrize("one_cloud", [False, True])
+def test_group_knn_matches_per_query(torch, clouds, one_cloud):
+    """kNN in groups of 8 queries per warp (runs of seeded groups, requests that end mid-group,
+    the fallback group for centres whose provisional threshold undershoots) against one warp
+    per query, on a multi-cloud batch and on a one-cloud batch."""
+    rng = np.random.default_rng(5)
+    use = [2] if one_cloud else range(len(clouds))
+    reqs, host = [], []
+    for ci in use:
+        oc, sxyz = clouds[ci]
+        for k in (1, 10, 32, 33, 50, 64):
+            nq = int(rng.integers(1, 3000))
+            c, _ = centres(torch, sxyz, nq, 2000 + 10 * ci + k)
+            c = c.copy()
+            c[::17, 2] += 40.0  # above the terrain: fewer than k points near the first cells
+            reqs.append(Request(oc, "knn", torch.from_numpy(c).cuda(), k=k))
+            host.append(("knn", ci, c, k))
+    eng_g, eng_q = BatchEngine(), BatchEngine()
+    eng_g.set_config(knn_group=True, knn_bucket=256)
+    eng_q.set_config(knn_group=False, knn_bucket=256)
+    got_g = engine_results(eng_g, eng_g.run(reqs), host)
+    got_q = engine_results(eng_q, eng_q.run(reqs), host)
+    for i, (a, b) in enumerate(zip(got_g, got_q)):
+        assert_same(a, b, f"group vs per-query, request {i}")
+    for i in range(0, len(host), 5):
+        assert_same(got_g[i], single_cloud(clouds, host[i]), f"group vs single-cloud call, request {i}")
+
+
 def test_graph_replay_direct_and_fp32_agree(torch, clouds):
     reqs, host = mixed_batch(torch, clouds, seed=1)
     eng = BatchEngine()
