@@ -50,12 +50,14 @@ KNN_K = 50
 Q_RADIUS = 500_000
 Q_KNN = 500_000
 L2_FLUSH_BYTES = 512 << 20
-# device launches of this library per timed step: radius search (count, 3 scan kernels, fill), kNN;
-# the packet paths add the query ordering (keys, histogram scan, 3 sort passes) to the radius and the kNN call
-LAUNCHES_PER_STEP = {"plain": 6, "packet": 6 + 10, "packet_fp32": 6 + 10, "knn_per_query": 6 + 10,
-                     # engine: epoch, keys, histogram scan, 4 sort passes, radius count, 3 scan kernels,
-                     # radius fill, request totals, kNN
-                     "engine": 14}
+# device launches of this library per timed step (counted from an ncu launch list of this bench):
+# plain: radius count, 3 scan kernels, fill; kNN.  The packet paths order the queries of each call first
+# (keys, histogram scan, 3 sort passes) and search the radius set in one pass (+ 3 scan kernels and the
+# chunk compaction), or count and fill with the FP32 filter; kNN in groups adds the fallback launch.
+LAUNCHES_PER_STEP = {"plain": 6, "packet": 10 + 7, "packet_fp32": 10 + 7, "knn_per_query": 10 + 6,
+                     # engine: epoch, keys, histogram scan, 4 sort passes, one-pass radius, 3 scan kernels,
+                     # chunk compaction, request totals, group kNN, fallback kNN
+                     "engine": 15}
 BUILD_BYTES_PER_POINT = 112  # encode 32 + sort 20 + reorder 52 + leaf counting 8
 BUILD_BYTES_PER_NODE = 36    # offsets 4 + ranges 8 + centers 24
 
@@ -493,7 +495,7 @@ def run_b200(args, rank, world, local_rank):
     flush = torch.empty(L2_FLUSH_BYTES // 4, dtype=torch.float32, device="cuda")
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
 
-    # (packet, fp32_filter, lanes, kNN in groups of 8 queries per warp)
+    # (packet, fp32_filter, lanes, kNN in groups of 4 queries per warp)
     SEARCH_PATHS = {"plain": (0, 0, args.radius_group, 0), "packet": (1, 0, 8, 1), "packet_fp32": (1, 1, 8, 1),
                     "knn_per_query": (1, 0, 8, 0), "engine": (1, 0, 8, 1)}
 

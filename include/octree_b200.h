@@ -117,7 +117,7 @@ int oct_set_radius_group(oct_cloud cloud, int lanes);
  *               every test in FP64.
  *  radius_lanes lanes per query when packet is 0: 8 (default), 16 or 32.
  *  knn_packet   1 (default): kNN with k <= 64 on the packet path walks the
- *               tree once per group of 8 curve-ordered queries per warp
+ *               tree once per group of 4 curve-ordered queries per warp
  *               (queries whose provisional threshold turns out too small
  *               finish on the per-query kernel); 0: one warp per query,
  *               visited in curve order when packet is 1.
@@ -264,7 +264,7 @@ int oct_engine_destroy(oct_engine engine);
 int oct_engine_set_stream(oct_engine engine, void* cuda_stream);
 int oct_engine_last_error(oct_engine engine, char* buf, size_t len);
 /* Search configuration of the engine (oct_search_config: fp32_filter, knn_bucket;
- * knn_packet = 1 (the engine's default): kNN with k <= 64 in groups of 8
+ * knn_packet = 1 (the engine's default): kNN with k <= 64 in groups of 4
  * curve-ordered queries per warp, 0: one warp per query;
  * reserved[0] = radius blocks per SM, reserved[1] = kNN blocks per SM, 0 = default;
  * reserved[2] = 1 to run kNN after the radius search instead of beside it). */

@@ -245,7 +245,7 @@ struct oct_engine_s {
     uint32_t bucket = 128;
     int radius_bps = 0, knn_bps = 0;
     int serial = 0;  // 1: kNN after the radius search on one stream; 0: kNN forked beside it
-    int knn_group = 1;  // kNN with k <= 64: groups of 8 queries per warp (0: one warp per query)
+    int knn_group = 1;  // kNN with k <= 64: groups of kKnnGroupQueries queries per warp (0: one per warp)
     // device arrays
     DevBuf desc;  // EngineDyn, then the SearchReq table
     DevBuf keys[2], ord[2];
@@ -676,7 +676,7 @@ int submit(oct_engine e, const oct_request* rq, uint32_t n) {
         gr.reqs = d_table + t;
         gr.q_begin = pos;
         gr.kmax = 0;
-        // packets: 32 queries (radius), kGrpQ queries (group kNN); the per-query kNN kernel ignores them
+        // packets: 32 queries (radius), kKnnGroupQueries (group kNN); the per-query kNN kernel ignores them
         const bool group_knn = e->knn_group && v >= kRadiusVariants && v < kRadiusVariants + 2;
         const uint64_t per = group_knn ? kKnnGroupQueries : 32;
         uint32_t t0 = t;

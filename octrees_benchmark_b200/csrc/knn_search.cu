@@ -704,17 +704,19 @@ __global__ void __launch_bounds__(kKnnThreads, 8) k_knn_reg(KnnTableArgs a) {
 }
 
 // ---------------------------------------------------------------------------
-// Group kNN (k <= 64): kGrpQ curve-ordered queries per warp share one walk.
+// Group kNN (k <= 64): kGrpQ (4) curve-ordered queries per warp share one walk.
 //
 // Consecutive queries along the curve are a few metres apart, so the octants
-// their searches need overlap almost entirely: 8 of them visit ~2.6 internal
-// nodes per query where one query alone visits ~14 (10M-point tile, k = 50).
+// their searches need overlap almost entirely: 4 of them visit ~4.7 internal
+// nodes per query (8: ~2.9) where one query alone visits ~14 (10M-point tile,
+// k = 50).  Groups of 4 rather than 8 halve the shared memory per warp, so 28
+// warps fit on an SM instead of 16, which this latency-bound walk needs more.
 // The warp walks the tree once for its group, nearest first by the smallest
 // lower bound of the group; a child is pushed with the mask of queries that
 // accept it and, per query, its lower bound rounded down to FP32 (a popped
 // entry is skipped for a query whose threshold has since dropped below it; the
-// rounding only keeps entries).  At an internal node four lanes per query
-// judge two children each.  A range (leaf, or subtree of at most `bucket`
+// rounding only keeps entries).  At an internal node 32 / kGrpQ lanes per
+// query judge the 8 children.  A range (leaf, or subtree of at most `bucket`
 // points) is tested transposed: the lanes hold 32 consecutive points and test
 // them against one accepting query at a time, and the query's candidates
 // (pairs that beat its k-th pair) go to its own 32-entry buffer in shared
@@ -733,8 +735,10 @@ __global__ void __launch_bounds__(kKnnThreads, 8) k_knn_reg(KnnTableArgs a) {
 // overflowed, is appended to a fallback list that k_knn_reg completes exactly.
 // ---------------------------------------------------------------------------
 
-constexpr int kGrpQ = (int)kKnnGroupQueries;  // queries per warp (8: the bit masks are 8 bits)
-constexpr int kGrpWarps = 2;
+constexpr int kGrpQ = (int)kKnnGroupQueries;  // queries per warp: 4 or 8 (query masks are 8 bits)
+// blocks as shared memory allows: ~13.8 KB per warp of 8 queries, ~7.5 KB per warp of 4
+constexpr int kGrpWarps = kGrpQ == 8 ? 2 : 4;
+constexpr int kGrpMinBlocks = kGrpQ == 8 ? 8 : 7;
 constexpr int kGrpThreads = 32 * kGrpWarps;
 constexpr int kGrpStack = 88;
 constexpr double kGrpSeed = 1.3;  // provisional threshold / previous group's largest k-th distance
@@ -758,7 +762,7 @@ struct KnnGroupArgs {
 };
 
 template <int R, int MULTI>
-__global__ void __launch_bounds__(kGrpThreads, 8) k_knn_group(KnnGroupArgs a) {
+__global__ void __launch_bounds__(kGrpThreads, kGrpMinBlocks) k_knn_group(KnnGroupArgs a) {
     constexpr int G = kGrpQ;
     constexpr int LC = 32 * R;
     __shared__ double s_ld[kGrpWarps][G][LC];
@@ -806,8 +810,10 @@ __global__ void __launch_bounds__(kGrpThreads, 8) k_knn_group(KnnGroupArgs a) {
         packets = a.grp->packets;
         fb_base = a.grp->q_begin;
     }
-    // lane roles at an internal node: query qj, children 2 cs and 2 cs + 1
-    const int qj = lane >> 2, cs = lane & 3;
+    // lane roles at an internal node: LPQ lanes per query qj, CPL children each
+    constexpr int LPQ = 32 / G, CPL = 8 / LPQ;
+    static_assert(G == 4 || G == 8, "4 or 8 queries per warp");
+    const int qj = lane / LPQ, cs = lane % LPQ;
     // groups [0, p_chunked) go out in chunks, the rest one at a time
     const uint64_t nw = (uint64_t)gridDim.x * kGrpWarps;
     const uint64_t chunk = a.chunk;
@@ -996,40 +1002,55 @@ __global__ void __launch_bounds__(kGrpThreads, 8) k_knn_group(KnnGroupArgs a) {
                 }
                 continue;
             }
-            // internal node: lane (qj, cs) judges children 2 cs and 2 cs + 1 for query qj
+            // internal node: lane (qj, cs) judges children cs CPL .. cs CPL + CPL - 1 for query qj
             const uint32_t fc = ea;
             const uint32_t cd = depth + 1;
             const bool qa = (m >> qj) & 1u;
-            double lb0 = INFINITY, lb1 = INFINITY;
-            bool k0 = false, k1 = false;
-            if (qa) {
-                const double* c0 = KRQV(centers) + 3ull * (fc + 2 * cs);
-                const double t = thr[qj];
-                lb0 = dist_po(qs[qj], c0, s_radii[cd]);
-                lb1 = dist_po(qs[qj], c0 + 3, s_radii[cd]);
-                k0 = !(lb0 > t);
-                k1 = !(lb1 > t);
-            }
-            const uint32_t B0 = __ballot_sync(0xffffffffu, k0);
-            const uint32_t B1 = __ballot_sync(0xffffffffu, k1);
-            // smallest accepting bound per child, over the lanes judging the same children
-            double v0 = k0 ? lb0 : (double)INFINITY, v1 = k1 ? lb1 : (double)INFINITY;
+            double lb[CPL];
+            bool kp[CPL];
+            uint32_t B[CPL];
+            double v[CPL];
 #pragma unroll
-            for (int off = 4; off < 32; off <<= 1) {
-                v0 = fmin(v0, __shfl_xor_sync(0xffffffffu, v0, off));
-                v1 = fmin(v1, __shfl_xor_sync(0xffffffffu, v1, off));
+            for (int w = 0; w < CPL; ++w) {
+                lb[w] = INFINITY;
+                kp[w] = false;
             }
+            if (qa) {
+                const double* c0 = KRQV(centers) + 3ull * (fc + CPL * cs);
+                const double t = thr[qj];
+#pragma unroll
+                for (int w = 0; w < CPL; ++w) {
+                    lb[w] = dist_po(qs[qj], c0 + 3 * w, s_radii[cd]);
+                    kp[w] = !(lb[w] > t);
+                }
+            }
+            // smallest accepting bound per child, over the lanes judging the same children
+#pragma unroll
+            for (int w = 0; w < CPL; ++w) {
+                B[w] = __ballot_sync(0xffffffffu, kp[w]);
+                v[w] = kp[w] ? lb[w] : (double)INFINITY;
+            }
+#pragma unroll
+            for (int off = LPQ; off < 32; off <<= 1)
+#pragma unroll
+                for (int w = 0; w < CPL; ++w) v[w] = fmin(v[w], __shfl_xor_sync(0xffffffffu, v[w], off));
             // lane c < 8: child c's query mask, bound and record
             const int cc = lane & 7;
-            const double x0 = __shfl_sync(0xffffffffu, v0, cc >> 1);
-            const double x1 = __shfl_sync(0xffffffffu, v1, cc >> 1);
-            double key = (cc & 1) ? x1 : x0;
+            double key = INFINITY;
+            uint32_t Bw = 0;
+#pragma unroll
+            for (int w = 0; w < CPL; ++w) {
+                const double x = __shfl_sync(0xffffffffu, v[w], cc / CPL);
+                if (cc % CPL == w) {
+                    key = x;
+                    Bw = B[w];
+                }
+            }
             uint32_t cm = 0;
             uint32_t ca = 0, cb = 0;
             if (lane < 8) {
-                const uint32_t Bw = (cc & 1) ? B1 : B0;
 #pragma unroll
-                for (int j = 0; j < G; ++j) cm |= ((Bw >> (4 * j + (cc >> 1))) & 1u) << j;
+                for (int j = 0; j < G; ++j) cm |= ((Bw >> (LPQ * j + cc / CPL)) & 1u) << j;
                 const uint32_t child = fc + lane;
                 const uint32_t cfc = KRQV(offsets)[child];
                 const uint2 rg = KRQV(ranges)[child];
@@ -1065,10 +1086,12 @@ __global__ void __launch_bounds__(kGrpThreads, 8) k_knn_group(KnnGroupArgs a) {
                 smk[slot] = (uint8_t)cm;
             }
             // per-query bounds of the pushed children, rounded down
-            const int s0 = __shfl_sync(0xffffffffu, slot, 2 * cs);
-            const int s1 = __shfl_sync(0xffffffffu, slot, 2 * cs + 1);
-            if (k0 && ((pushm >> (2 * cs)) & 1u)) slb[s0][qj] = __double2float_rd(lb0);
-            if (k1 && ((pushm >> (2 * cs + 1)) & 1u)) slb[s1][qj] = __double2float_rd(lb1);
+#pragma unroll
+            for (int w = 0; w < CPL; ++w) {
+                const int c = CPL * cs + w;
+                const int sw = __shfl_sync(0xffffffffu, slot, c);
+                if (kp[w] && ((pushm >> c) & 1u)) slb[sw][qj] = __double2float_rd(lb[w]);
+            }
             __syncwarp();
             sp += np;
         }
@@ -1126,9 +1149,12 @@ int group_blocks_per_sm() {
     return per;
 }
 
+// blocks_per_sm > 0 caps the resident blocks (room for a kernel running beside it).
 template <int R, int MULTI>
-cudaError_t launch_group(const KnnGroupArgs& g, int sms, cudaStream_t s) {
-    uint64_t grid = (uint64_t)sms * group_blocks_per_sm<R, MULTI>();
+cudaError_t launch_group(const KnnGroupArgs& g, int sms, cudaStream_t s, int blocks_per_sm = 0) {
+    int per = group_blocks_per_sm<R, MULTI>();
+    if (blocks_per_sm > 0 && blocks_per_sm < per) per = blocks_per_sm;
+    uint64_t grid = (uint64_t)sms * per;
     if (!g.grp) {
         const uint64_t want = (g.packets + kGrpWarps - 1) / kGrpWarps;
         if (want < grid) grid = want;
@@ -1195,7 +1221,7 @@ cudaError_t launch_knn_group_table(int device, cudaStream_t s, const DynGroup* d
                                    const SearchReq* single, uint32_t kmax, const uint32_t* d_order, uint32_t bucket,
                                    uint32_t* d_idx, double* d_d2, uint32_t* d_counts, uint32_t* d_err,
                                    uint32_t* d_packet_ctr, uint32_t* d_fb_list, double est, uint32_t chunk,
-                                   int fb_blocks_per_sm) {
+                                   int blocks_per_sm) {
     if (kmax > 64) return cudaErrorInvalidValue;
     cudaError_t e;
     if ((e = cudaMemsetAsync(d_packet_ctr, 0, 8, s)) != cudaSuccess) return e;
@@ -1214,12 +1240,13 @@ cudaError_t launch_knn_group_table(int device, cudaStream_t s, const DynGroup* d
     g.fb_list = d_fb_list;
     g.fb_count = reinterpret_cast<unsigned long long*>(&d_fb->nq);
     const int sms = sm_count_k(device);
-    if (single) e = (kmax <= 32) ? launch_group<1, 2>(g, sms, s) : launch_group<2, 2>(g, sms, s);
-    else e = (kmax <= 32) ? launch_group<1, 1>(g, sms, s) : launch_group<2, 1>(g, sms, s);
+    const int bps = blocks_per_sm;
+    if (single) e = (kmax <= 32) ? launch_group<1, 2>(g, sms, s, bps) : launch_group<2, 2>(g, sms, s, bps);
+    else e = (kmax <= 32) ? launch_group<1, 1>(g, sms, s, bps) : launch_group<2, 1>(g, sms, s, bps);
     if (e != cudaSuccess) return e;
     // the queries handed back, exactly and without the provisional threshold
     return launch_knn_table(device, s, d_fb, single, 0, kmax, d_fb_list, bucket, d_idx, d_d2, d_counts, d_err,
-                            fb_blocks_per_sm, 0.0);
+                            bps, 0.0);
 }
 
 cudaError_t prepare_knn_dyn() {

@@ -108,7 +108,7 @@ class LinearOctree:
                           knn_estimate: int = 0, knn_group_run: int = 0):
         """Search path: packet (32 curve-ordered queries per warp) or one query per
         ``radius_lanes`` lanes; FP32 leaf-relative filter with FP64 re-tests; kNN in groups
-        of 8 queries per warp (``knn_packet``; else one warp per query); ``two_pass`` counts
+        of 4 queries per warp (``knn_packet``; else one warp per query); ``two_pass`` counts
         then fills instead of the one-pass packet radius search."""
         cfg = OctSearchConfig(int(bool(packet)), int(bool(fp32_filter)), int(radius_lanes), int(bool(knn_packet)),
                               int(knn_bucket))

@@ -134,7 +134,7 @@ def test_engine_matches_oracle(torch, clouds, port):
 
 @pytest.mark.parametrize("one_cloud", [False, True])
 def test_group_knn_matches_per_query(torch, clouds, one_cloud):
-    """kNN in groups of 8 queries per warp (runs of seeded groups, requests that end mid-group,
+    """kNN in groups of queries per warp (runs of seeded groups, requests that end mid-group,
     the fallback group for centres whose provisional threshold undershoots) against one warp
     per query, on a multi-cloud batch and on a one-cloud batch."""
     rng = np.random.default_rng(5)
