@@ -16,6 +16,7 @@
 // (distance, index) resolves ties at the k-th distance by the lowest index.
 #include <algorithm>
 #include <cfloat>
+#include <cuda_fp16.h>
 
 #include "cloud.h"
 #include "search_kernels.cuh"
@@ -713,7 +714,7 @@ __global__ void __launch_bounds__(kKnnThreads, 8) k_knn_reg(KnnTableArgs a) {
 // warps fit on an SM instead of 16, which this latency-bound walk needs more.
 // The warp walks the tree once for its group, nearest first by the smallest
 // lower bound of the group; a child is pushed with the mask of queries that
-// accept it and, per query, its lower bound rounded down to FP32 (a popped
+// accept it and, per query, its lower bound rounded down to FP16 (a popped
 // entry is skipped for a query whose threshold has since dropped below it; the
 // rounding only keeps entries).  At an internal node 32 / kGrpQ lanes per
 // query judge the 8 children.  A range (leaf, or subtree of at most `bucket`
@@ -736,9 +737,10 @@ __global__ void __launch_bounds__(kKnnThreads, 8) k_knn_reg(KnnTableArgs a) {
 // ---------------------------------------------------------------------------
 
 constexpr int kGrpQ = (int)kKnnGroupQueries;  // queries per warp: 4 or 8 (query masks are 8 bits)
-// blocks as shared memory allows: ~13.8 KB per warp of 8 queries, ~7.5 KB per warp of 4
+// blocks as shared memory allows: ~12.5 KB per warp of 8 queries, ~6.5 KB per warp of 4
+// (8 blocks of 4 warps: 32 warps per SM at up to 64 registers)
 constexpr int kGrpWarps = kGrpQ == 8 ? 2 : 4;
-constexpr int kGrpMinBlocks = kGrpQ == 8 ? 8 : 7;
+constexpr int kGrpMinBlocks = 8;
 constexpr int kGrpThreads = 32 * kGrpWarps;
 constexpr int kGrpStack = 88;
 constexpr double kGrpSeed = 1.3;  // provisional threshold / previous group's largest k-th distance
@@ -777,14 +779,20 @@ __global__ void __launch_bounds__(kGrpThreads, kGrpMinBlocks) k_knn_group(KnnGro
     __shared__ uint32_t s_qg[kGrpWarps][G];
     __shared__ uint32_t st_a[kGrpWarps][kGrpStack];
     __shared__ uint32_t st_b[kGrpWarps][kGrpStack];
-    __shared__ float st_lb[kGrpWarps][kGrpStack][G];
+    __shared__ __half st_lb[kGrpWarps][kGrpStack][G];  // per-query bounds, rounded down to FP16
     __shared__ uint8_t st_d[kGrpWarps][kGrpStack];
     __shared__ uint8_t st_m[kGrpWarps][kGrpStack];
-    __shared__ double s_rad[kGrpWarps][kMaxDepth + 1][3];
+    // level radii: per warp for a table of clouds, once per block for one cloud
+    __shared__ double s_rad[MULTI == 1 ? kGrpWarps : 1][kMaxDepth + 1][3];
     __shared__ CloudView s_view[MULTI == 1 ? kGrpWarps : 1];
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    double (*s_radii)[3] = s_rad[warp];
+    double (*s_radii)[3] = s_rad[MULTI == 1 ? warp : 0];
+    if (MULTI != 1) {
+        const double* gr = &a.single.cv.geom->radii[0][0];
+        for (int t = threadIdx.x; t < (kMaxDepth + 1) * 3; t += kGrpThreads) (&s_rad[0][0][0])[t] = gr[t];
+        __syncthreads();
+    }
     double (*ld)[LC] = s_ld[warp];
     uint32_t (*li)[LC] = s_li[warp];
     double (*bd)[32] = s_bd[warp];
@@ -796,36 +804,37 @@ __global__ void __launch_bounds__(kGrpThreads, kGrpMinBlocks) k_knn_group(KnnGro
     uint32_t* nbs = s_nb[warp];
     uint32_t* sa = st_a[warp];
     uint32_t* sb = st_b[warp];
-    float (*slb)[G] = st_lb[warp];
+    __half (*slb)[G] = st_lb[warp];
     uint8_t* sdp = st_d[warp];
     uint8_t* smk = st_m[warp];
     uint32_t cur_cloud = 0xffffffffu;
     const SearchReq* reqs = nullptr;
     uint32_t nreq = 1;
-    uint64_t packets = a.packets;
-    uint64_t fb_base = 0;  // the fallback entries of a batch group start at its first position
+    // query positions and group indices of a launch fit 32 bits (positions are u32 in the order arrays)
+    uint32_t packets = (uint32_t)a.packets;
+    uint32_t fb_base = 0;  // the fallback entries of a batch group start at its first position
     if (MULTI) {
         reqs = a.grp->reqs;
         nreq = a.grp->nreq;
-        packets = a.grp->packets;
-        fb_base = a.grp->q_begin;
+        packets = (uint32_t)a.grp->packets;
+        fb_base = (uint32_t)a.grp->q_begin;
     }
     // lane roles at an internal node: LPQ lanes per query qj, CPL children each
     constexpr int LPQ = 32 / G, CPL = 8 / LPQ;
     static_assert(G == 4 || G == 8, "4 or 8 queries per warp");
     const int qj = lane / LPQ, cs = lane % LPQ;
     // groups [0, p_chunked) go out in chunks, the rest one at a time
-    const uint64_t nw = (uint64_t)gridDim.x * kGrpWarps;
-    const uint64_t chunk = a.chunk;
-    const uint64_t p_chunked = (chunk > 1 && packets > 2 * nw) ? (packets - 2 * nw) / chunk * chunk : 0;
-    uint64_t next = 0, chunk_end = 0;
+    const uint32_t nw = gridDim.x * kGrpWarps;
+    const uint32_t chunk = a.chunk;
+    const uint32_t p_chunked = (chunk > 1 && packets > 2 * nw) ? (packets - 2 * nw) / chunk * chunk : 0;
+    uint32_t next = 0, chunk_end = 0;
     // seed: the previous group's largest k-th distance (< 0: none), its group and request
     double seed_thr = -1.0;
-    uint64_t seed_packet = 0;
+    uint32_t seed_packet = 0;
     uint32_t seed_ri = 0;
 
     for (;;) {
-        uint64_t packet;
+        uint32_t packet;
         if (next < chunk_end) {
             packet = next++;
         } else {
@@ -834,13 +843,14 @@ __global__ void __launch_bounds__(kGrpThreads, kGrpMinBlocks) k_knn_group(KnnGro
             v = __shfl_sync(0xffffffffu, v, 0);
             const uint64_t c0 = (uint64_t)v * chunk;
             if (c0 < p_chunked) {
-                packet = c0;
-                next = c0 + 1;
-                chunk_end = c0 + chunk;
+                packet = (uint32_t)c0;
+                next = packet + 1;
+                chunk_end = packet + chunk;
             } else {
                 uint32_t s = 0;
                 if (lane == 0) s = atomicAdd(&a.packet_ctr[1], 1u);
                 s = __shfl_sync(0xffffffffu, s, 0);
+                if ((uint64_t)p_chunked + s >= packets) break;
                 packet = p_chunked + s;
                 next = chunk_end = 0;
             }
@@ -856,18 +866,18 @@ __global__ void __launch_bounds__(kGrpThreads, kGrpMinBlocks) k_knn_group(KnnGro
             }
             ri = lo;
         }
-        if (KRQ(cloud_id) != cur_cloud) {
+        if (MULTI == 1 && reqs[ri].cloud_id != cur_cloud) {  // this warp's level radii and cloud follow the group's
             __syncwarp();
-            const double* gr = &KRQ(cv.geom)->radii[0][0];
+            const double* gr = &reqs[ri].cv.geom->radii[0][0];
             for (int t = lane; t < (kMaxDepth + 1) * 3; t += 32) (&s_radii[0][0])[t] = gr[t];
-            if (MULTI == 1 && lane == 0) s_view[warp] = reqs[ri].cv;
-            cur_cloud = KRQ(cloud_id);
+            if (lane == 0) s_view[warp] = reqs[ri].cv;
+            cur_cloud = reqs[ri].cloud_id;
             __syncwarp();
         }
         const uint32_t K = KRQ(k);
-        const uint64_t q_begin = KRQ(q_begin);
-        const uint64_t pos0 = q_begin + (uint64_t)G * (packet - KRQ(packet_begin));
-        const uint64_t q_end = KRQ(q_end);
+        const uint32_t q_begin = (uint32_t)KRQ(q_begin);
+        const uint32_t pos0 = q_begin + (uint32_t)G * (packet - (uint32_t)KRQ(packet_begin));
+        const uint32_t q_end = (uint32_t)KRQ(q_end);
         const bool seeded = a.est > 0.0 && seed_thr >= 0.0 && packet == seed_packet + 1 && ri == seed_ri;
         // lanes j < G: load query j, reset its state
         bool valid = false;
@@ -938,7 +948,7 @@ __global__ void __launch_bounds__(kGrpThreads, kGrpMinBlocks) k_knn_group(KnnGro
                 sdp[0] = 0;
                 smk[0] = (uint8_t)vm;
             }
-            if (lane < G) slb[0][lane] = 0.0f;
+            if (lane < G) slb[0][lane] = __float2half_rz(0.0f);
         }
         __syncwarp();
         int sp = vm ? 1 : 0;
@@ -947,7 +957,7 @@ __global__ void __launch_bounds__(kGrpThreads, kGrpMinBlocks) k_knn_group(KnnGro
             const uint32_t ea = sa[sp], eb = sb[sp];
             const uint32_t depth = sdp[sp];
             bool act = false;
-            if (lane < G) act = ((smk[sp] >> lane) & 1u) && !((double)slb[sp][lane] > thr[lane]);
+            if (lane < G) act = ((smk[sp] >> lane) & 1u) && !((double)__half2float(slb[sp][lane]) > thr[lane]);
             const uint32_t m = __ballot_sync(0xffffffffu, act) & ((1u << G) - 1u);
             __syncwarp();
             if (!m) continue;
@@ -1090,7 +1100,7 @@ __global__ void __launch_bounds__(kGrpThreads, kGrpMinBlocks) k_knn_group(KnnGro
             for (int w = 0; w < CPL; ++w) {
                 const int c = CPL * cs + w;
                 const int sw = __shfl_sync(0xffffffffu, slot, c);
-                if (kp[w] && ((pushm >> c) & 1u)) slb[sw][qj] = __double2float_rd(lb[w]);
+                if (kp[w] && ((pushm >> c) & 1u)) slb[sw][qj] = __float2half_rd(__double2float_rd(lb[w]));
             }
             __syncwarp();
             sp += np;
