@@ -680,9 +680,12 @@ def run_b200(args, rank, world, local_rank):
     # per-kernel times: the engine runs the packet path's kernels side by side, so they are timed there alone
     kpath = args.search if chosen["radius_ms"] is not None else "packet"
     rad_ms, knn_ms = paths[kpath]["radius_ms"], paths[kpath]["knn_ms"]
-    rad = {"kernel": f"radius neighborsPrune sphere, {kpath} path (count + scan + fill)", "ms": rad_ms,
-           "achieved": rad_bytes / (rad_ms / 1e3) / 1e9}
-    knn = {"kernel": "kNN k=50 (k_knn)", "ms": knn_ms, "achieved": knn_bytes / (knn_ms / 1e3) / 1e9}
+    # each time is the whole library call on the cloud's stream (CUDA events): the query ordering plus
+    # the search kernels it launches
+    rad = {"kernel": f"radius neighborsPrune sphere, {kpath} path (query order + k_radius_packet one pass + "
+                     "scan + k_chunk_compact)", "ms": rad_ms, "achieved": rad_bytes / (rad_ms / 1e3) / 1e9}
+    knn = {"kernel": f"kNN k=50, {kpath} path (query order + k_knn_group + fallback k_knn_reg)", "ms": knn_ms,
+           "achieved": knn_bytes / (knn_ms / 1e3) / 1e9}
     dom = knn if knn_ms >= rad_ms else rad
     roofline = {"bound": "hbm", "kernel": dom["kernel"], "achieved": dom["achieved"], "peak": peak, "unit": "GB/s",
                 "frac": dom["achieved"] / peak, "peak_source": peak_kind, "traffic": None,
