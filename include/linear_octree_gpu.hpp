@@ -142,6 +142,15 @@ public:
         std::vector<NeighborSet> r = structBatch(K, c, 1, radius);
         return std::move(r[0]);
     }
+    // neighborsApprox(p, radius, tolerancePercentage, upperBound) (linear_octree.hpp:1089-1093): like
+    // the reference, the percentage is used as the precision level, converted to an unsigned integer
+    template <Kernel K = Kernel::square, class P>
+    NeighborSet neighborsApprox(const P& p, double radius, double tolerancePercentage, bool upperBound) const {
+        const double c[3] = {p.getX(), p.getY(), p.getZ()};
+        std::vector<NeighborSet> r =
+            approxBatch(K, c, 1, radius, static_cast<uint32_t>(tolerancePercentage), upperBound);
+        return std::move(r[0]);
+    }
     template <class P>
     size_t knn(const P& p, size_t k, std::vector<size_t>& indexes, std::vector<double>& dists) const {
         const double c[3] = {p.getX(), p.getY(), p.getZ()};
@@ -174,16 +183,30 @@ public:
                           cloud_, "oct_radius_search");
     }
     std::vector<NeighborSet> structBatch(Kernel k, const double* centers, size_t nq, double radius) const {
+        return rangesBatch(k, centers, nq, radius, false, 0, false);
+    }
+    // neighborsApprox over nq centres at one precision level
+    std::vector<NeighborSet> approxBatch(Kernel k, const double* centers, size_t nq, double radius,
+                                         uint32_t precisionLevel, bool upperBound) const {
+        return rangesBatch(k, centers, nq, radius, true, precisionLevel, upperBound);
+    }
+
+private:
+    std::vector<NeighborSet> rangesBatch(Kernel k, const double* centers, size_t nq, double radius, bool approx,
+                                         uint32_t level, bool upper) const {
         std::vector<uint64_t> offs(nq + 1), npts(nq);
         uint64_t total = 0;
-        int st = oct_struct_search(cloud_, static_cast<int>(k), centers, nq, nullptr, radius, offs.data(), nullptr,
-                                   0, &total, npts.data(), 0);
-        if (st != OCT_OK && st != OCT_ERR_CAPACITY) detail::check(st, cloud_, "oct_struct_search");
+        auto call = [&](uint32_t* pairs, uint64_t cap) {
+            return approx ? oct_approx_search(cloud_, static_cast<int>(k), centers, nq, nullptr, radius, level,
+                                              upper ? 1 : 0, offs.data(), pairs, cap, &total, npts.data(), 0)
+                          : oct_struct_search(cloud_, static_cast<int>(k), centers, nq, nullptr, radius, offs.data(),
+                                              pairs, cap, &total, npts.data(), 0);
+        };
+        const char* what = approx ? "oct_approx_search" : "oct_struct_search";
+        int st = call(nullptr, 0);
+        if (st != OCT_OK && st != OCT_ERR_CAPACITY) detail::check(st, cloud_, what);
         std::vector<uint32_t> pairs(2 * total);
-        if (total)
-            detail::check(oct_struct_search(cloud_, static_cast<int>(k), centers, nq, nullptr, radius, offs.data(),
-                                            pairs.data(), total, &total, npts.data(), 0),
-                          cloud_, "oct_struct_search");
+        if (total) detail::check(call(pairs.data(), total), cloud_, what);
         std::vector<NeighborSet> out(nq);
         for (size_t q = 0; q < nq; ++q) {
             for (uint64_t j = offs[q]; j < offs[q + 1]; ++j) out[q].ranges.emplace_back(pairs[2 * j], pairs[2 * j + 1]);
@@ -191,6 +214,8 @@ public:
         }
         return out;
     }
+
+public:
     void knnBatch(const double* centers, size_t nq, uint32_t k, std::vector<uint32_t>& idx, std::vector<double>& d2,
                   std::vector<uint32_t>& counts) const {
         idx.resize(nq * k);

@@ -58,8 +58,15 @@ typedef enum { OCT_ENC_MORTON_3D = 1, OCT_ENC_HILBERT_3D = 5 } oct_encoder;
 typedef enum { OCT_KERNEL_CIRCLE = 0, OCT_KERNEL_SPHERE = 1, OCT_KERNEL_SQUARE = 2, OCT_KERNEL_CUBE = 3 } oct_kernel;
 
 /* Radius-search variants of LinearOctree (inc/structures/linear_octree.hpp):
- * neighbors 796-816, neighborsPrune 746-784, neighborsStruct 695-736. */
-typedef enum { OCT_NEIGHBORS = 1, OCT_NEIGHBORS_PRUNE = 2, OCT_NEIGHBORS_STRUCT = 3 } oct_algo;
+ * neighbors 796-816, neighborsPrune 746-784, neighborsStruct 695-736,
+ * neighborsApprox 975-1035 (oct_approx_search); the values of the reference's
+ * SearchAlgo (inc/main_options.hpp:29-35). */
+typedef enum {
+    OCT_NEIGHBORS = 1,
+    OCT_NEIGHBORS_PRUNE = 2,
+    OCT_NEIGHBORS_STRUCT = 3,
+    OCT_NEIGHBORS_APPROX = 4
+} oct_algo;
 
 #define OCT_MEM_DEVICE 0x1u /* every buffer of the call is device memory */
 
@@ -199,6 +206,20 @@ int oct_radius_count(oct_cloud cloud, int kernel, int algo, const double* center
 int oct_struct_search(oct_cloud cloud, int kernel, const double* centers, uint64_t nq, const double* radii,
                       double radius, uint64_t* range_offsets, uint32_t* pairs, uint64_t pair_capacity,
                       uint64_t* total_ranges, uint64_t* point_counts, uint32_t flags);
+
+/* neighborsApprox (linear_octree.hpp:975-1035): the neighborsStruct search cut
+ * below depth precision_level.  A child deeper than that level is not judged:
+ * with upper_bound its whole range is added (every octant whose parent the
+ * search reached, so the points are a superset of the exact set), without it
+ * the child is dropped (a subset).  Outputs and capacity handling as
+ * oct_struct_search; the ranges are the reference's, in ascending order.  The
+ * reference's Point overloads (1089-1111) pass their tolerance percentage on as
+ * the precision level (converted to an unsigned integer): the same level here.
+ * A level of 21 or more cuts nothing (the neighborsStruct result). */
+int oct_approx_search(oct_cloud cloud, int kernel, const double* centers, uint64_t nq, const double* radii,
+                      double radius, uint32_t precision_level, int upper_bound, uint64_t* range_offsets,
+                      uint32_t* pairs, uint64_t pair_capacity, uint64_t* total_ranges, uint64_t* point_counts,
+                      uint32_t flags);
 
 /* k nearest neighbours of nq centres.  Replaces LinearOctree::knn
  * (linear_octree.hpp:899-942): idx and d2 are nq x k, ascending by squared

@@ -27,6 +27,7 @@ OCT_NOALLOC_MAX_POINTS = 1 << 18
 ENCODERS = {"morton": 1, "mort": 1, "hilbert": 5, "hilb": 5, 1: 1, 5: 5}
 KERNELS = {"circle": 0, "sphere": 1, "square": 2, "cube": 3, 0: 0, 1: 1, 2: 2, 3: 3}
 ALGOS = {"neighbors": 1, "neighborsPrune": 2, "prune": 2, "neighborsStruct": 3, "struct": 3, 1: 1, 2: 2, 3: 3}
+OCT_NEIGHBORS_APPROX = 4  # oct_approx_search (SearchAlgo::NEIGHBORS_APPROX)
 
 
 class OctParams(C.Structure):
@@ -118,6 +119,8 @@ SIGNATURES = {
     "oct_radius_search": ([_vp, _int, _int, _vp, _u64, _vp, _dbl, _vp, _vp, _u64, C.POINTER(_u64), _u32], _int),
     "oct_radius_count": ([_vp, _int, _int, _vp, _u64, _vp, _dbl, _vp, _u32], _int),
     "oct_struct_search": ([_vp, _int, _vp, _u64, _vp, _dbl, _vp, _vp, _u64, C.POINTER(_u64), _vp, _u32], _int),
+    "oct_approx_search": ([_vp, _int, _vp, _u64, _vp, _dbl, _u32, _int, _vp, _vp, _u64, C.POINTER(_u64), _vp, _u32],
+                          _int),
     "oct_knn": ([_vp, _vp, _u64, _u32, _vp, _vp, _vp, _u32], _int),
     "oct_encode_sort_noalloc": ([_int, _vp, _u64, _vp, _vp, _vp, _vp], _int),
     "oct_engine_create": ([C.POINTER(OctEngineParams), C.POINTER(_vp)], _int),

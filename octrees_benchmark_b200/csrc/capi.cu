@@ -599,12 +599,30 @@ int oct_radius_search(oct_cloud h, int kernel, int algo, const double* centers, 
     return OCT_OK;
 }
 
-int oct_struct_search(oct_cloud h, int kernel, const double* centers, uint64_t nq, const double* radii,
-                      double radius, uint64_t* range_offsets, uint32_t* pairs, uint64_t pair_capacity,
-                      uint64_t* total_ranges, uint64_t* point_counts, uint32_t flags) {
+namespace {
+// The depth cut of a neighborsApprox call, on the cloud for the call's duration.
+struct ApproxCut {
+    Cloud& c;
+    ApproxCut(Cloud& cl, uint32_t cut, int upper) : c(cl) {
+        c.approx_cut = cut;
+        c.approx_upper = upper;
+    }
+    ~ApproxCut() {
+        c.approx_cut = 0;
+        c.approx_upper = 0;
+    }
+};
+}  // namespace
+
+// neighborsStruct, or (approx_cut = precisionLevel + 1) neighborsApprox
+static int ranges_search(oct_cloud h, int kernel, const double* centers, uint64_t nq, const double* radii,
+                         double radius, uint32_t approx_cut, int approx_upper, uint64_t* range_offsets,
+                         uint32_t* pairs, uint64_t pair_capacity, uint64_t* total_ranges, uint64_t* point_counts,
+                         uint32_t flags) {
     if (!h) return OCT_ERR_INVALID_ARG;
     Cloud& c = h->c;
     DeviceGuard g(c.device);
+    ApproxCut cut_scope(c, approx_cut, approx_upper);
     const bool dev = flags & OCT_MEM_DEVICE;
     const double *dq, *dr;
     int st = radius_common(c, kernel, OCT_NEIGHBORS_STRUCT, centers, nq, radii, radius, dev, &dq, &dr);
@@ -644,6 +662,23 @@ int oct_struct_search(oct_cloud h, int kernel, const double* centers, uint64_t n
     if (!dev && tot) CK(cudaMemcpyAsync(pairs, dout, 8 * tot, cudaMemcpyDeviceToHost, c.stream));
     if (!dev) return sync_and_check(c);
     return OCT_OK;
+}
+
+int oct_struct_search(oct_cloud h, int kernel, const double* centers, uint64_t nq, const double* radii,
+                      double radius, uint64_t* range_offsets, uint32_t* pairs, uint64_t pair_capacity,
+                      uint64_t* total_ranges, uint64_t* point_counts, uint32_t flags) {
+    return ranges_search(h, kernel, centers, nq, radii, radius, 0, 0, range_offsets, pairs, pair_capacity,
+                         total_ranges, point_counts, flags);
+}
+
+int oct_approx_search(oct_cloud h, int kernel, const double* centers, uint64_t nq, const double* radii,
+                      double radius, uint32_t precision_level, int upper_bound, uint64_t* range_offsets,
+                      uint32_t* pairs, uint64_t pair_capacity, uint64_t* total_ranges, uint64_t* point_counts,
+                      uint32_t flags) {
+    // a level at or past the deepest possible node cuts nothing: the neighborsStruct search
+    const uint32_t cut = precision_level >= kMaxDepth ? 0u : precision_level + 1;
+    return ranges_search(h, kernel, centers, nq, radii, radius, cut, upper_bound ? 1 : 0, range_offsets, pairs,
+                         pair_capacity, total_ranges, point_counts, flags);
 }
 
 int oct_knn(oct_cloud h, const double* centers, uint64_t nq, uint32_t k, uint32_t* idx, double* d2,

@@ -86,6 +86,8 @@ struct SearchReq {
     uint64_t out_begin;         // kNN: first output slot (previous requests' nq * k)
     uint32_t k;                 // kNN k
     uint32_t cloud_id;          // distinct per cloud within the table (radii reload key)
+    uint32_t approx_cut;        // neighborsStruct: 0, or neighborsApprox's precisionLevel + 1
+    uint32_t approx_upper;      // neighborsApprox: 1 adds the ranges of the cut octants
 };
 
 // Launch sizes of one kernel group of a batch, in device memory.  The host
@@ -163,6 +165,10 @@ struct Cloud {
     int knn_packet = 1;  // kNN (k <= 64, packet path): groups of queries per warp
     uint32_t knn_bucket = 256;
     int two_pass = 0;   // 1: packet radius searches count, then fill (no result chunks)
+    // neighborsStruct searches of the current call: 0, or neighborsApprox's precisionLevel + 1
+    // (children deeper than that level are cut; approx_upper adds their ranges)
+    uint32_t approx_cut = 0;
+    int approx_upper = 0;
     double knn_est = kKnnEstimate;  // register kNN: provisional-threshold factor (0: off)
     uint32_t knn_chunk = kKnnGroupChunk;  // group kNN: consecutive groups per warp fetch
     // one-pass radius search: result chunk pool, links, first chunk per query, counter

@@ -255,6 +255,8 @@ __global__ void __launch_bounds__(kPkThreads) k_radius_packet(PacketArgs a) {
         const uint32_t qi = (uint32_t)qg;
         const double* qc = RQ(centers);
         const double* qrad = RQ(radii);
+        const uint32_t approx_cut = (ALGO == kStruct) ? RQ(approx_cut) : 0u;
+        const bool approx_upper = (ALGO == kStruct) && RQ(approx_upper) != 0;
         SearchKernel k;
         k.init(qc[3 * ql], qc[3 * ql + 1], qc[3 * ql + 2], qrad ? qrad[ql] : RQ(radius));
         if constexpr (kT) put_query<KT>(s_qp[warp], lane, k);  // read by the other lanes after a __syncwarp
@@ -539,6 +541,9 @@ __global__ void __launch_bounds__(kPkThreads) k_radius_packet(PacketArgs a) {
                 my_fc = RQV(offsets)[fc + lane];
                 my_rg = RQV(ranges)[fc + lane];
             }
+            // neighborsApprox (linear_octree.hpp:979-985): below its precision level a
+            // child is cut before any box test, its whole range added in upper-bound mode
+            const bool cut = ALGO == kStruct && approx_cut != 0 && cd >= approx_cut;
 #pragma unroll
             for (int j = 0; j < 8; ++j) {
                 bool o = false, n = false;
@@ -546,6 +551,8 @@ __global__ void __launch_bounds__(kPkThreads) k_radius_packet(PacketArgs a) {
                     const double* oc = RQV(centers) + 3ull * (fc + j);
                     if constexpr (ALGO == kNeighbors) {
                         o = box_overlap<KT>(k, oc, s_radii[cd]);
+                    } else if (cut) {
+                        n = approx_upper;
                     } else {
                         const int jj = box_intersect<KT>(k, oc, s_radii[cd]);
                         n = (jj == kInside);
@@ -806,6 +813,8 @@ cudaError_t launch_radius_packet(Cloud& c, int kernel, int algo, int mode, bool 
     r.out_begin = 0;
     r.k = 0;
     r.cloud_id = 0;
+    r.approx_cut = c.approx_cut;
+    r.approx_upper = (uint32_t)c.approx_upper;
     return launch_radius_table(c.device, c.stream, kernel, algo, mode, fp32, nullptr, &r, (nq + 31) / 32, d_order,
                                d_counts, d_counts2, d_offsets, d_out, out_capacity, c.packet_ctr.as<uint32_t>(),
                                c.stats.as<unsigned long long>(), c.d_err.as<uint32_t>(), 0, chunks);

@@ -42,6 +42,8 @@ struct RadiusArgs {
     uint32_t* out;                     // fill pass: indices, or (first, last) pairs for struct
     uint64_t out_cap;                  // entries (indices or pairs)
     uint32_t* err;
+    uint32_t approx_cut;               // neighborsStruct: 0, or neighborsApprox's precisionLevel + 1
+    uint32_t approx_upper;             // neighborsApprox: 1 adds the ranges of the cut octants
 };
 
 template <int G>
@@ -207,6 +209,11 @@ __global__ void __launch_bounds__(kRadThreads) k_radius(RadiusArgs a) {
                     if constexpr (ALGO == kNeighbors) {
                         push = box_overlap<KT>(k, oc, s_radii[cd]);
                         ckind = leaf ? kKindScan : kKindExpand;
+                    } else if (ALGO == kStruct && a.approx_cut != 0 && cd >= a.approx_cut) {
+                        // neighborsApprox (linear_octree.hpp:979-985): below its precision level a
+                        // child is cut before any box test, its whole range added in upper-bound mode
+                        push = a.approx_upper != 0;
+                        ckind = kKindEmit;
                     } else {
                         const int j = box_intersect<KT>(k, oc, s_radii[cd]);
                         push = (j != kOutside);
@@ -381,6 +388,8 @@ cudaError_t launch_radius(Cloud& c, int kernel, int algo, int group, bool fill, 
     a.out = d_out;
     a.out_cap = out_capacity;
     a.err = c.d_err.as<uint32_t>();
+    a.approx_cut = c.approx_cut;
+    a.approx_upper = (uint32_t)c.approx_upper;
     const int groups_per_block = kRadThreads / group;
     const uint64_t want = (nq + groups_per_block - 1) / groups_per_block;
     const uint64_t cap = (uint64_t)sm_count_r(c.device) * 8;

@@ -198,6 +198,30 @@ class LinearOctree:
         check(st, h, "oct_struct_search")
         return offs, pairs[: total.value], pts
 
+    def neighborsApprox(self, centers, radius, precision_level, upper_bound, kernel="square"):
+        """neighborsApprox (linear_octree.hpp:975-1035): neighborsStruct cut below depth
+        ``precision_level``; ``upper_bound`` adds the ranges of the cut octants (a superset of
+        the exact set), otherwise they are dropped (a subset).  The reference's Point overloads
+        take a tolerance percentage and use it as the level (converted to an unsigned integer).
+        Returns (range offsets uint64[nq+1], pairs uint32[m, 2], numberOfPoints uint64[nq])."""
+        L, h = self._L, self._h
+        centers = _host_f64(centers, 3)
+        nq = centers.shape[0]
+        radii, r0 = self._radii(centers, radius)
+        offs = np.zeros(nq + 1, np.uint64)
+        pts = np.zeros(nq, np.uint64)
+        total = C.c_uint64(0)
+        lvl, up = int(precision_level), int(bool(upper_bound))
+        st = L.oct_approx_search(h, KERNELS[kernel], centers.ctypes.data, nq, _ptr(radii), r0, lvl, up,
+                                 offs.ctypes.data, None, 0, C.byref(total), pts.ctypes.data, 0)
+        pairs = np.zeros((max(1, total.value), 2), np.uint32)
+        if st == capi.OCT_ERR_CAPACITY:
+            st = L.oct_approx_search(h, KERNELS[kernel], centers.ctypes.data, nq, _ptr(radii), r0, lvl, up,
+                                     offs.ctypes.data, pairs.ctypes.data, total.value, C.byref(total),
+                                     pts.ctypes.data, 0)
+        check(st, h, "oct_approx_search")
+        return offs, pairs[: total.value], pts
+
     def radius_count(self, centers, radius, kernel="square", algo="neighborsPrune"):
         L, h = self._L, self._h
         centers = _host_f64(centers, 3)

@@ -594,7 +594,10 @@ typedef struct {
     uint64_t* pairs;     /* range output for neighborsStruct (NULL: count only) */
     uint64_t count;      /* indices emitted (or ranges, in range mode) */
     int range_mode;
+    uint32_t cut;        /* neighborsApprox: precisionLevel (NO_CUT: neighborsStruct) */
+    int upper;           /* neighborsApprox: upperBound */
 } sink;
+#define NO_CUT 0xffffffffu
 
 static void emit_index(sink* s, uint64_t i) {
     if (s->out) s->out[s->count] = i;
@@ -611,11 +614,17 @@ static void emit_range(sink* s, uint64_t f, uint64_t l) {
     }
 }
 
-/* continuationCriterion of neighborsStruct/neighborsPrune (698-714, 749-769) and of
- * neighbors (800-802) */
+/* continuationCriterion of neighborsStruct/neighborsPrune (698-714, 749-769), of
+ * neighbors (800-802) and of neighborsApprox (979-1000: below precisionLevel the
+ * octant's range is added in upper-bound mode and the search is cut, before any
+ * box test) */
 static int criterion(const orc_tree* t, const kern* k, int algo, uint32_t node, uint32_t depth, sink* s) {
     const double* oc = t->centers + 3 * (uint64_t)node;
     const double* orr = t->radii + 3 * depth;
+    if (algo == 3 && depth > s->cut) {
+        if (s->upper) emit_range(s, t->ranges[2 * node], t->ranges[2 * node + 1]);
+        return 0;
+    }
     if (algo == 1) return box_overlap(k, oc, orr);
     int j = box_intersect(k, oc, orr);
     if (j == INSIDE) {
@@ -670,7 +679,7 @@ void orc_radius_count(const orc_tree* t, const double* xyz, int kernel, int algo
     #pragma omp parallel for schedule(dynamic, 64)
     for (int64_t q = 0; q < (int64_t)nq; ++q) {
         kern k = make_kernel(kernel, centers + 3 * q, radii[q]);
-        sink s = {NULL, NULL, 0, 0};
+        sink s = {NULL, NULL, 0, 0, NO_CUT, 0};
         single_traversal(t, xyz, &k, algo, &s);
         counts[q] = s.count;
     }
@@ -681,30 +690,41 @@ void orc_radius_fill(const orc_tree* t, const double* xyz, int kernel, int algo,
     #pragma omp parallel for schedule(dynamic, 64)
     for (int64_t q = 0; q < (int64_t)nq; ++q) {
         kern k = make_kernel(kernel, centers + 3 * q, radii[q]);
-        sink s = {idx + offsets[q], NULL, 0, 0};
+        sink s = {idx + offsets[q], NULL, 0, 0, NO_CUT, 0};
         single_traversal(t, xyz, &k, algo, &s);
     }
 }
 
-void orc_struct_ranges_count(const orc_tree* t, const double* xyz, int kernel, const double* centers,
-                             uint64_t nq, const double* radii, uint64_t* counts) {
+void orc_approx_ranges_count(const orc_tree* t, const double* xyz, int kernel, const double* centers,
+                             uint64_t nq, const double* radii, uint32_t level, int upper, uint64_t* counts) {
     #pragma omp parallel for schedule(dynamic, 64)
     for (int64_t q = 0; q < (int64_t)nq; ++q) {
         kern k = make_kernel(kernel, centers + 3 * q, radii[q]);
-        sink s = {NULL, NULL, 0, 1};
+        sink s = {NULL, NULL, 0, 1, level, upper};
         single_traversal(t, xyz, &k, 3, &s);
         counts[q] = s.count;
     }
 }
 
-void orc_struct_ranges_fill(const orc_tree* t, const double* xyz, int kernel, const double* centers,
-                            uint64_t nq, const double* radii, const uint64_t* offsets, uint64_t* pairs) {
+void orc_approx_ranges_fill(const orc_tree* t, const double* xyz, int kernel, const double* centers,
+                            uint64_t nq, const double* radii, uint32_t level, int upper, const uint64_t* offsets,
+                            uint64_t* pairs) {
     #pragma omp parallel for schedule(dynamic, 64)
     for (int64_t q = 0; q < (int64_t)nq; ++q) {
         kern k = make_kernel(kernel, centers + 3 * q, radii[q]);
-        sink s = {NULL, pairs + 2 * offsets[q], 0, 1};
+        sink s = {NULL, pairs + 2 * offsets[q], 0, 1, level, upper};
         single_traversal(t, xyz, &k, 3, &s);
     }
+}
+
+void orc_struct_ranges_count(const orc_tree* t, const double* xyz, int kernel, const double* centers,
+                             uint64_t nq, const double* radii, uint64_t* counts) {
+    orc_approx_ranges_count(t, xyz, kernel, centers, nq, radii, NO_CUT, 0, counts);
+}
+
+void orc_struct_ranges_fill(const orc_tree* t, const double* xyz, int kernel, const double* centers,
+                            uint64_t nq, const double* radii, const uint64_t* offsets, uint64_t* pairs) {
+    orc_approx_ranges_fill(t, xyz, kernel, centers, nq, radii, NO_CUT, 0, offsets, pairs);
 }
 
 /* ---------------- kNN: best-first search (linear_octree.hpp:819-942) ---------------- */

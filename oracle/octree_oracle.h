@@ -45,6 +45,13 @@ void orc_struct_ranges_count(const orc_tree* t, const double* xyz, int kernel, c
                              uint64_t nq, const double* radii, uint64_t* counts);
 void orc_struct_ranges_fill(const orc_tree* t, const double* xyz, int kernel, const double* centers,
                             uint64_t nq, const double* radii, const uint64_t* offsets, uint64_t* pairs);
+/* neighborsApprox (linear_octree.hpp:945-1035): neighborsStruct cut below depth `level`;
+ * with `upper` the ranges of the cut octants are added */
+void orc_approx_ranges_count(const orc_tree* t, const double* xyz, int kernel, const double* centers,
+                             uint64_t nq, const double* radii, uint32_t level, int upper, uint64_t* counts);
+void orc_approx_ranges_fill(const orc_tree* t, const double* xyz, int kernel, const double* centers,
+                            uint64_t nq, const double* radii, uint32_t level, int upper, const uint64_t* offsets,
+                            uint64_t* pairs);
 void orc_knn(const orc_tree* t, const double* xyz, uint64_t n, const double* centers, uint64_t nq, uint64_t k,
              uint64_t* idx, double* d2, uint64_t* counts);
 

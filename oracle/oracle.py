@@ -85,6 +85,10 @@ class Port:
             L.orc_struct_ranges_count.argtypes = [C.c_void_p, _f64p, C.c_int, _f64p, C.c_uint64, _f64p, _u64p]
             L.orc_struct_ranges_fill.argtypes = [C.c_void_p, _f64p, C.c_int, _f64p, C.c_uint64, _f64p, _u64p,
                                                  _u64p]
+            L.orc_approx_ranges_count.argtypes = [C.c_void_p, _f64p, C.c_int, _f64p, C.c_uint64, _f64p, C.c_uint32,
+                                                  C.c_int, _u64p]
+            L.orc_approx_ranges_fill.argtypes = [C.c_void_p, _f64p, C.c_int, _f64p, C.c_uint64, _f64p, C.c_uint32,
+                                                 C.c_int, _u64p, _u64p]
             L.orc_knn.argtypes = [C.c_void_p, _f64p, C.c_uint64, _f64p, C.c_uint64, C.c_uint64, _u64p, _f64p,
                                   _u64p]
             Port._lib = L
@@ -186,6 +190,20 @@ class PortTree:
         self.L.orc_struct_ranges_fill(self.h, xyz, kernel, centers, nq, radii, offs, pairs)
         return offs, pairs.reshape(-1, 2)
 
+    def approx_ranges(self, xyz, kernel, centers, radii, level, upper):
+        """neighborsApprox ranges (the traversal cut below depth `level`; `upper`: cut octants added)."""
+        xyz, centers = _f64(xyz), _f64(centers)
+        nq = len(centers)
+        radii = _f64(np.broadcast_to(np.asarray(radii, np.float64), (nq,)))
+        counts = np.zeros(nq, np.uint64)
+        self.L.orc_approx_ranges_count(self.h, xyz, kernel, centers, nq, radii, int(level), int(bool(upper)), counts)
+        offs = np.zeros(nq + 1, np.uint64)
+        np.cumsum(counts, out=offs[1:])
+        pairs = np.zeros(2 * int(offs[-1]), np.uint64)
+        self.L.orc_approx_ranges_fill(self.h, xyz, kernel, centers, nq, radii, int(level), int(bool(upper)), offs,
+                                      pairs)
+        return offs, pairs.reshape(-1, 2)
+
     def knn(self, xyz, centers, k):
         xyz, centers = _f64(xyz), _f64(centers)
         nq = len(centers)
@@ -221,6 +239,8 @@ class Reference:
             L.refo_struct_range_total.argtypes = [C.c_void_p]
             L.refo_struct_range_total.restype = C.c_uint64
             L.refo_struct_ranges_fetch.argtypes = [C.c_void_p, _u64p, _u64p]
+            L.refo_approx.argtypes = [C.c_void_p, C.c_int, _f64p, C.c_uint64, _f64p, C.c_double, C.c_int, C.c_int]
+            L.refo_approx.restype = C.c_uint64
             L.refo_knn.argtypes = [C.c_void_p, _f64p, C.c_uint64, C.c_uint64, _u64p, _f64p, _u64p, C.c_int]
             L.refo_time_radius.argtypes = [C.c_void_p, C.c_int, C.c_int, _f64p, C.c_uint64, C.c_double, C.c_int,
                                            C.POINTER(C.c_uint64)]
@@ -293,6 +313,19 @@ class Reference:
         self.radius(kernel, 3, centers, radii, threads)
         m = self.L.refo_struct_range_total(self.h)
         offs = np.zeros(len(centers) + 1, np.uint64)
+        pairs = np.zeros(2 * int(m), np.uint64)
+        self.L.refo_struct_ranges_fetch(self.h, offs, pairs)
+        return offs, pairs.reshape(-1, 2)
+
+    def approx_ranges(self, kernel, centers, radii, tolerance, upper, threads=0):
+        """ranges of neighborsApprox(p, r, tolerancePercentage, upperBound), in the reference's
+        emission order (its overloads pass the percentage on as the precision level)"""
+        centers = _f64(centers)
+        nq = len(centers)
+        radii = _f64(np.broadcast_to(np.asarray(radii, np.float64), (nq,)))
+        self.L.refo_approx(self.h, kernel, centers.reshape(-1), nq, radii, float(tolerance), int(bool(upper)), threads)
+        m = self.L.refo_struct_range_total(self.h)
+        offs = np.zeros(nq + 1, np.uint64)
         pairs = np.zeros(2 * int(m), np.uint64)
         self.L.refo_struct_ranges_fetch(self.h, offs, pairs)
         return offs, pairs.reshape(-1, 2)

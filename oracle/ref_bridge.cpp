@@ -92,6 +92,25 @@ size_t count_one(const ExposedOctree& t, int algo, const Point& c, double r) {
     return t.neighborsStruct<K>(c, r).size();
 }
 
+// neighborsApprox through the reference's public overload (linear_octree.hpp:1089-1093),
+// which passes the tolerance percentage on as the precision level
+template <Kernel_t K>
+void approx_one(const ExposedOctree& t, const Point& c, double r, double tol, bool upper,
+                std::vector<std::pair<size_t, size_t>>& rng) {
+    auto s = t.neighborsApprox<K>(c, r, tol, upper);
+    rng = s.ranges;
+}
+
+void approx_dispatch(const ExposedOctree& t, int kernel, const Point& c, double r, double tol, bool upper,
+                     std::vector<std::pair<size_t, size_t>>& rng) {
+    switch (kernel) {
+        case 0: approx_one<Kernel_t::circle>(t, c, r, tol, upper, rng); break;
+        case 1: approx_one<Kernel_t::sphere>(t, c, r, tol, upper, rng); break;
+        case 2: approx_one<Kernel_t::square>(t, c, r, tol, upper, rng); break;
+        default: approx_one<Kernel_t::cube>(t, c, r, tol, upper, rng); break;
+    }
+}
+
 size_t count_dispatch(const ExposedOctree& t, int kernel, int algo, const Point& c, double r) {
     switch (kernel) {
         case 0: return count_one<Kernel_t::circle>(t, algo, c, r);
@@ -227,6 +246,24 @@ void refo_radius_fetch(void* h, uint64_t* offsets, uint64_t* idx) {
         for (size_t v : rc->res_idx[q]) idx[o++] = v;
     }
     offsets[rc->res_idx.size()] = o;
+}
+
+// neighborsApprox over nq centers; the ranges stay in the handle (refo_struct_ranges_fetch).
+// Returns the number of ranges.
+uint64_t refo_approx(void* h, int kernel, const double* centers, uint64_t nq, const double* radii, double tol,
+                     int upper, int threads) {
+    set_threads(threads);
+    auto* rc = static_cast<RefCloud*>(h);
+    rc->res_idx.assign(nq, {});
+    rc->res_ranges.assign(nq, {});
+    #pragma omp parallel for schedule(runtime)
+    for (int64_t q = 0; q < (int64_t)nq; ++q) {
+        Point c(centers[3 * q], centers[3 * q + 1], centers[3 * q + 2]);
+        approx_dispatch(*rc->tree, kernel, c, radii[q], tol, upper != 0, rc->res_ranges[q]);
+    }
+    uint64_t total = 0;
+    for (auto& v : rc->res_ranges) total += v.size();
+    return total;
 }
 
 uint64_t refo_struct_range_total(void* h) {

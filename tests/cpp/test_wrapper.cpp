@@ -186,6 +186,13 @@ void test_complex_cpp() {  // test_complex.cpp:37-173
             size_t strict = 0;
             for (size_t i = 0; i < pts.size(); ++i) strict += sq(pts[i], Point(5, 5, 5)) < r * r;
             EXPECT(pr.size() == strict);
+            // neighborsApprox bounds (the reference's ApproxSearchBounds, test_complex.cpp:115-141):
+            // upper >= exact >= lower, at its level (maxDepth / 2 = 10) and at levels that cut
+            for (double tol : {10.0, 2.0, 1.0}) {
+                auto up = oct.neighborsApprox<Kernel::sphere>(Point(5, 5, 5), r, tol, true);
+                auto lo = oct.neighborsApprox<Kernel::sphere>(Point(5, 5, 5), r, tol, false);
+                EXPECT(up.size() >= st.size() && lo.size() <= st.size());
+            }
         }
         // points were reordered in place, ids travel with them
         std::vector<size_t> ids;

@@ -146,6 +146,42 @@ def test_gpu_radius_matches_oracle(synth_cases, case, search):
 
 
 @pytest.mark.parametrize("case", range(len(SYNTH)))
+@pytest.mark.parametrize("search", ["lanes8", "lanes32", "packet"])
+def test_gpu_approx_matches_oracle(synth_cases, case, search):
+    """neighborsApprox: the ranges at every cut level, both bounds, every kernel; and the
+    lower-bound points within the exact set within the upper-bound points."""
+    xyz, enc, leaf, keys, perm, box, sxyz, t = synth_cases[case]
+    oc = octree(xyz, enc, leaf, search)
+    q = sxyz[query_indices(200, len(sxyz), seed=case)]
+    rng = np.random.default_rng(case)
+    q = np.concatenate([q, q[:30] + rng.normal(0, 2.0, (30, 3))])
+    depth = t.max_depth
+    levels = sorted({0, 1, 2, depth // 2, max(depth - 1, 0), depth, 25})
+
+    def points(offs, pairs, i):
+        return {p for f, l in pairs[offs[i]:offs[i + 1]] for p in range(int(f), int(l))}
+
+    for kn, kv in KERNELS.items():
+        r = 2.5
+        eo, ep, _ = oc.neighborsStruct(q, r, kn)
+        for level in levels:
+            res = {}
+            for upper in (False, True):
+                ro, pairs, npts = oc.neighborsApprox(q, r, level, upper, kn)
+                o2, p2 = t.approx_ranges(sxyz, kv, q, r, level, upper)
+                assert_ranges_equal(ro, pairs, o2, p2, f"{kn} level {level} upper {upper}")
+                lens = pairs[:, 1].astype(np.int64) - pairs[:, 0].astype(np.int64)
+                csum = np.concatenate([[0], np.cumsum(lens)])
+                want = csum[ro[1:].astype(np.int64)] - csum[ro[:-1].astype(np.int64)]
+                assert np.array_equal(npts.astype(np.int64), want), "numberOfPoints"
+                res[upper] = (ro, pairs)
+            for i in range(0, len(q), 23):
+                exact = points(eo, ep, i)
+                assert points(*res[False], i) <= exact <= points(*res[True], i), f"{kn} level {level} query {i}"
+    oc.close()
+
+
+@pytest.mark.parametrize("case", range(len(SYNTH)))
 @pytest.mark.parametrize("search", ["lanes8", "packet", "knn_packet", "knn_leaves", "knn_bucket2k"])
 def test_gpu_knn_matches_oracle(synth_cases, case, search):
     xyz, enc, leaf, keys, perm, box, sxyz, t = synth_cases[case]

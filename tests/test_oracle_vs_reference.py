@@ -46,6 +46,12 @@ def test_oracle_equals_reference(port, n, tile, seed, enc, leaf):
         o1, p1 = t.struct_ranges(sxyz, kern, q, 1.5)
         o2, p2 = R.struct_ranges(kern, q, 1.5)
         assert_ranges_equal(o1, p1, o2, p2)
+        # neighborsApprox through the reference's public overload (percentage -> level)
+        for level in sorted({0, 2, t.max_depth // 2, t.max_depth, 21}):
+            for upper in (False, True):
+                o1, p1 = t.approx_ranges(sxyz, kern, q, 1.5, level, upper)
+                o2, p2 = R.approx_ranges(kern, q, 1.5, float(level), upper)
+                assert np.array_equal(o1, o2) and np.array_equal(p1, p2), (kern, level, upper)
     for k in (1, 10, 50):
         i1, d1, c1 = t.knn(sxyz, q, k)
         i2, d2, c2 = R.knn(q, k)
