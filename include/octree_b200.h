@@ -182,6 +182,21 @@ int oct_build(oct_cloud cloud, oct_tree_info* info);
 int oct_tree_export(oct_cloud cloud, uint32_t* offsets, uint64_t* ranges, double* centers, double* radii,
                     double* half, uint32_t flags);
 
+/* Restore a sorted and built cloud from a checkpoint, without sorting or
+ * building: info, box12, keys, perm and sorted_xyz as oct_build and
+ * oct_encode_sort returned them, offsets (n_total; the trailing 0 is not
+ * needed), ranges, centers, radii and half as oct_tree_export returned them.
+ * The reference has no counterpart (it rebuilds from the points each run); the
+ * arrays are its LinearOctree members (linear_octree.hpp:112-121, 140).  The
+ * cloud must have been created with the checkpoint's encoder and leaf size.
+ * Host buffers only (flags 0).  The arrays are checked (counts, ascending
+ * keys, a permutation, offsets and ranges in bounds) and OCT_ERR_INVALID_ARG
+ * names the first violation; the cloud then answers every search as the
+ * original did. */
+int oct_tree_import(oct_cloud cloud, const oct_tree_info* info, const double* box12, const uint64_t* keys,
+                    const uint32_t* perm, const double* sorted_xyz, const uint32_t* offsets, const uint64_t* ranges,
+                    const double* centers, const double* radii, const double* half, uint32_t flags);
+
 /* Radius search for nq centres (xyz AoS).  radii: per-query radii (nq
  * doubles) or NULL to use `radius` for every query.
  * Replaces neighbors / neighborsPrune (linear_octree.hpp:1050-1087): the

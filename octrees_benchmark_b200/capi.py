@@ -121,6 +121,7 @@ SIGNATURES = {
     "oct_struct_search": ([_vp, _int, _vp, _u64, _vp, _dbl, _vp, _vp, _u64, C.POINTER(_u64), _vp, _u32], _int),
     "oct_approx_search": ([_vp, _int, _vp, _u64, _vp, _dbl, _u32, _int, _vp, _vp, _u64, C.POINTER(_u64), _vp, _u32],
                           _int),
+    "oct_tree_import": ([_vp, C.POINTER(OctTreeInfo), _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _vp, _u32], _int),
     "oct_knn": ([_vp, _vp, _u64, _u32, _vp, _vp, _vp, _u32], _int),
     "oct_encode_sort_noalloc": ([_int, _vp, _u64, _vp, _vp, _vp, _vp], _int),
     "oct_engine_create": ([C.POINTER(OctEngineParams), C.POINTER(_vp)], _int),

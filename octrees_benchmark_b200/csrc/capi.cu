@@ -5,6 +5,7 @@
 #include <cstring>
 #include <new>
 #include <utility>
+#include <vector>
 
 #include "cloud.h"
 
@@ -516,6 +517,109 @@ int oct_tree_export(oct_cloud h, uint32_t* offsets, uint64_t* ranges, double* ce
     }
     CK(cudaStreamSynchronize(c.stream));
     return OCT_OK;
+}
+
+int oct_tree_import(oct_cloud h, const oct_tree_info* info, const double* box12, const uint64_t* keys,
+                    const uint32_t* perm, const double* sorted_xyz, const uint32_t* offsets, const uint64_t* ranges,
+                    const double* centers, const double* radii, const double* half, uint32_t flags) {
+    if (!h) return OCT_ERR_INVALID_ARG;
+    Cloud& c = h->c;
+    if (flags != 0) return set_error(c, OCT_ERR_INVALID_ARG, "oct_tree_import takes host buffers (flags 0)");
+    if (!info || !box12 || !offsets || !ranges || !centers || !radii || !half)
+        return set_error(c, OCT_ERR_INVALID_ARG, "NULL argument");
+    const uint64_t n = info->n_points;
+    const uint64_t nt = info->n_total;
+    if (n >= 0xffffffffull) return set_error(c, OCT_ERR_INVALID_ARG, "more than 2^32 - 2 points");
+    if (n && (!keys || !perm || !sorted_xyz)) return set_error(c, OCT_ERR_INVALID_ARG, "NULL point array");
+    if (nt == 0 || nt != (uint64_t)info->n_leaf + info->n_internal || nt != 8ull * info->n_internal + 1 ||
+        info->max_depth_seen > kMaxDepth)
+        return set_error(c, OCT_ERR_INVALID_ARG, "inconsistent tree counts");
+    // the checkpoint must describe a valid sorted cloud and tree: nothing is rebuilt
+    for (uint64_t i = 1; i < n; ++i)
+        if (keys[i] < keys[i - 1]) return set_error(c, OCT_ERR_INVALID_ARG, "keys are not ascending");
+    for (uint64_t i = 0; i < n; ++i)
+        if (keys[i] >= kUpperBound) return set_error(c, OCT_ERR_INVALID_ARG, "key above 63 bits");
+    {
+        std::vector<bool> seen(n, false);
+        for (uint64_t i = 0; i < n; ++i) {
+            if (perm[i] >= n || seen[perm[i]]) return set_error(c, OCT_ERR_INVALID_ARG, "perm is not a permutation");
+            seen[perm[i]] = true;
+        }
+    }
+    uint64_t n_parents = 0;
+    for (uint64_t i = 0; i < nt; ++i) {
+        const uint64_t fc = offsets[i];
+        if (fc && (fc <= i || fc + 8 > nt)) return set_error(c, OCT_ERR_INVALID_ARG, "offsets out of range");
+        n_parents += fc != 0;
+        if (ranges[2 * i] > ranges[2 * i + 1] || ranges[2 * i + 1] > n)
+            return set_error(c, OCT_ERR_INVALID_ARG, "ranges out of range");
+    }
+    if (n_parents != info->n_internal) return set_error(c, OCT_ERR_INVALID_ARG, "offsets do not match n_internal");
+    for (uint32_t l = 0; l <= kMaxDepth; ++l)
+        for (int a = 0; a < 3; ++a)
+            if (!(radii[3 * l + a] >= 0.0)) return set_error(c, OCT_ERR_INVALID_ARG, "negative or NaN radii");
+    DeviceGuard g(c.device);
+    CK(c.xs.reserve(8 * (n ? n : 1)));
+    CK(c.ys.reserve(8 * (n ? n : 1)));
+    CK(c.zs.reserve(8 * (n ? n : 1)));
+    CK(c.keys.reserve(8 * (n ? n : 1)));
+    CK(c.perm.reserve(4 * (n ? n : 1)));
+    CK(c.offsets.reserve(4 * (nt + 1)));
+    CK(c.ranges.reserve(8 * nt));
+    CK(c.centers.reserve(24 * nt));
+    CK(c.d_box.reserve(sizeof(BoxD) + sizeof(LevelGeom)));
+    CK(c.d_err.reserve(256));
+    // host staging: SoA coordinates, 32-bit ranges, the box and level geometry
+    std::vector<double> soa(3 * n);
+    for (uint64_t i = 0; i < n; ++i)
+        for (int a = 0; a < 3; ++a) soa[a * n + i] = sorted_xyz[3 * i + a];
+    std::vector<uint32_t> off32(offsets, offsets + nt);
+    off32.push_back(0);  // the sentinel after the last node
+    std::vector<uint32_t> rg32(2 * nt);
+    for (uint64_t i = 0; i < 2 * nt; ++i) rg32[i] = (uint32_t)ranges[i];
+    BoxD box;
+    LevelGeom geom;
+    for (int a = 0; a < 3; ++a) {
+        box.center[a] = box12[a];
+        box.radii[a] = box12[3 + a];
+        box.min[a] = box12[6 + a];
+        box.max[a] = box12[9 + a];
+        geom.half[a] = half[a];
+    }
+    memcpy(geom.radii, radii, sizeof(geom.radii));
+    std::vector<unsigned char> bg(sizeof(BoxD) + sizeof(LevelGeom));
+    memcpy(bg.data(), &box, sizeof(BoxD));
+    memcpy(bg.data() + sizeof(BoxD), &geom, sizeof(LevelGeom));
+    const auto H2D = cudaMemcpyHostToDevice;
+    if (n) {
+        CK(cudaMemcpyAsync(c.xs.ptr, soa.data(), 8 * n, H2D, c.stream));
+        CK(cudaMemcpyAsync(c.ys.ptr, soa.data() + n, 8 * n, H2D, c.stream));
+        CK(cudaMemcpyAsync(c.zs.ptr, soa.data() + 2 * n, 8 * n, H2D, c.stream));
+        CK(cudaMemcpyAsync(c.keys.ptr, keys, 8 * n, H2D, c.stream));
+        CK(cudaMemcpyAsync(c.perm.ptr, perm, 4 * n, H2D, c.stream));
+    }
+    CK(cudaMemcpyAsync(c.offsets.ptr, off32.data(), 4 * (nt + 1), H2D, c.stream));
+    CK(cudaMemcpyAsync(c.ranges.ptr, rg32.data(), 8 * nt, H2D, c.stream));
+    CK(cudaMemcpyAsync(c.centers.ptr, centers, 24 * nt, H2D, c.stream));
+    CK(cudaMemcpyAsync(c.d_box.ptr, bg.data(), bg.size(), H2D, c.stream));
+    CK(cudaMemsetAsync(c.d_err.ptr, 0, 4, c.stream));
+    CK(cudaStreamSynchronize(c.stream));  // the staging vectors go out of scope
+    c.box = box;
+    c.geom = geom;
+    c.n = n;
+    c.n_total = (uint32_t)nt;
+    c.n_internal = info->n_internal;
+    c.n_leaf = info->n_leaf;
+    c.max_depth_seen = info->max_depth_seen;
+    c.node_capacity = (uint32_t)nt;
+    c.sorted = true;
+    c.built = true;
+    c.rel_built = false;
+    if (c.fp32_filter && c.packet) {  // the FP32 search reads leaf-relative coordinates
+        CK(launch_leaf_rel(c));
+        c.rel_built = true;
+    }
+    return sync_and_check(c);
 }
 
 int oct_radius_count(oct_cloud h, int kernel, int algo, const double* centers, uint64_t nq, const double* radii,

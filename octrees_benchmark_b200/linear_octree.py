@@ -55,19 +55,9 @@ class LinearOctree:
     def __init__(self, points, encoder="hilbert", max_points_leaf: int = 128, device: int = 0,
                  radius_group: int = 8, stream=None, packet: bool = True, fp32_filter: bool = False,
                  knn_packet: bool = True, knn_bucket: int = 256):
-        L = lib()
-        self._L = L
-        self.encoder = ENCODERS[encoder]
-        self.max_points_leaf = int(max_points_leaf)
-        p = OctParams(self.max_points_leaf, self.encoder, device, 0)
-        h = C.c_void_p()
-        st = L.oct_cloud_create(C.byref(p), C.byref(h))
-        check(st, None, "oct_cloud_create")
-        self._h = h
-        if stream is not None:
-            check(L.oct_cloud_set_stream(h, C.c_void_p(stream)), h, "oct_cloud_set_stream")
-        self.set_search_config(packet=packet, fp32_filter=fp32_filter, radius_lanes=radius_group,
-                               knn_packet=knn_packet, knn_bucket=knn_bucket)
+        self._open(encoder, max_points_leaf, device, radius_group, stream, packet, fp32_filter, knn_packet,
+                   knn_bucket)
+        L, h = self._L, self._h
         dev = _is_device(points)
         if not dev:
             points = _host_f64(points, 3)
@@ -84,6 +74,53 @@ class LinearOctree:
         self.n_internal = info.n_internal
         self.n_total = info.n_total
         self.max_depth_seen = info.max_depth_seen
+
+    def _open(self, encoder, max_points_leaf, device, radius_group, stream, packet, fp32_filter, knn_packet,
+              knn_bucket):
+        L = lib()
+        self._L = L
+        self.encoder = ENCODERS[encoder] if not isinstance(encoder, (int, np.integer)) else int(encoder)
+        self.max_points_leaf = int(max_points_leaf)
+        p = OctParams(self.max_points_leaf, self.encoder, device, 0)
+        h = C.c_void_p()
+        st = L.oct_cloud_create(C.byref(p), C.byref(h))
+        check(st, None, "oct_cloud_create")
+        self._h = h
+        if stream is not None:
+            check(L.oct_cloud_set_stream(h, C.c_void_p(stream)), h, "oct_cloud_set_stream")
+        self.set_search_config(packet=packet, fp32_filter=fp32_filter, radius_lanes=radius_group,
+                               knn_packet=knn_packet, knn_bucket=knn_bucket)
+
+    # ---- checkpoints -------------------------------------------------------------
+    def checkpoint(self) -> dict:
+        """Everything a built cloud holds, as host arrays (np.savez-able): the sorted
+        cloud (keys, perm, sorted xyz, box), the tree (export()) and its counts."""
+        keys, perm, xyz = self.sorted_points()
+        ck = dict(encoder=np.int32(self.encoder), max_points_leaf=np.uint32(self.max_points_leaf),
+                  info=np.array([self.n, self.n_leaf, self.n_internal, self.n_total, self.max_depth_seen], np.uint64),
+                  box=np.asarray(self.box, np.float64), keys=keys, perm=perm, sorted_xyz=xyz)
+        ck.update(self.export())
+        return ck
+
+    @classmethod
+    def from_checkpoint(cls, ck, device: int = 0, radius_group: int = 8, stream=None, packet: bool = True,
+                        fp32_filter: bool = False, knn_packet: bool = True, knn_bucket: int = 256):
+        """A cloud restored from checkpoint() (or its np.savez file) without sorting or building."""
+        self = cls.__new__(cls)
+        self._open(int(ck["encoder"]), int(ck["max_points_leaf"]), device, radius_group, stream, packet, fp32_filter,
+                   knn_packet, knn_bucket)
+        n, n_leaf, n_internal, n_total, depth = (int(v) for v in ck["info"])
+        info = OctTreeInfo(n, n_leaf, n_internal, n_total, depth)
+        arr = {k: np.ascontiguousarray(ck[k], dt) for k, dt in
+               (("box", np.float64), ("keys", np.uint64), ("perm", np.uint32), ("sorted_xyz", np.float64),
+                ("offsets", np.uint32), ("ranges", np.uint64), ("centers", np.float64), ("radii", np.float64),
+                ("half", np.float64))}
+        check(self._L.oct_tree_import(self._h, C.byref(info), *(arr[k].ctypes.data for k in
+              ("box", "keys", "perm", "sorted_xyz", "offsets", "ranges", "centers", "radii", "half")), 0),
+              self._h, "oct_tree_import")
+        self.n, self.n_leaf, self.n_internal, self.n_total, self.max_depth_seen = n, n_leaf, n_internal, n_total, depth
+        self.box = arr["box"].copy()
+        return self
 
     def close(self):
         if getattr(self, "_h", None):
