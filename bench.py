@@ -60,6 +60,11 @@ LAUNCHES_PER_STEP = {"plain": 6, "packet": 10 + 7, "packet_fp32": 10 + 7, "knn_p
                      "engine": 15}
 BUILD_BYTES_PER_POINT = 112  # encode 32 + sort 20 + reorder 52 + leaf counting 8
 BUILD_BYTES_PER_NODE = 36    # offsets 4 + ranges 8 + centers 24
+# DRAM bytes (read + write) per query of the search kernels, from ncu --set full of
+# `python -m octrees_benchmark_b200.profile_case` (6M points at this tile's density, 200k queries each):
+# k_knn_group k=50 333.7 + 120.3 MB, one-pass k_radius_packet r=2.5 334.8 + 55.7 MB
+KNN_DRAM_BYTES_PER_QUERY = (333.7e6 + 120.3e6) / 200_000
+RADIUS_DRAM_BYTES_PER_QUERY = (334.8e6 + 55.7e6) / 200_000
 
 
 def measured_peak():
@@ -686,9 +691,13 @@ def run_b200(args, rank, world, local_rank):
                      "scan + k_chunk_compact)", "ms": rad_ms, "achieved": rad_bytes / (rad_ms / 1e3) / 1e9}
     knn = {"kernel": f"kNN k=50, {kpath} path (query order + k_knn_group + fallback k_knn_reg)", "ms": knn_ms,
            "achieved": knn_bytes / (knn_ms / 1e3) / 1e9}
+    knn["traffic"] = KNN_DRAM_BYTES_PER_QUERY * Q_KNN
+    rad["traffic"] = RADIUS_DRAM_BYTES_PER_QUERY * Q_RADIUS
     dom = knn if knn_ms >= rad_ms else rad
     roofline = {"bound": "hbm", "kernel": dom["kernel"], "achieved": dom["achieved"], "peak": peak, "unit": "GB/s",
-                "frac": dom["achieved"] / peak, "peak_source": peak_kind, "traffic": None,
+                "frac": dom["achieved"] / peak, "peak_source": peak_kind, "traffic": dom["traffic"],
+                "traffic_source": "DRAM read + write bytes per query of the search kernel from one ncu capture "
+                                  "(6M-point tile at the same density, 200k queries), times this step's queries",
                 "algorithmic_bytes": "radius 24 + 28 per neighbour; kNN 24 + 36 k per query",
                 "other": {"kernel": (rad if dom is knn else knn)["kernel"],
                           "achieved": (rad if dom is knn else knn)["achieved"],
