@@ -128,7 +128,7 @@ cudaError_t radius_pass(Cloud& c, int kernel, int algo, bool fill, const double*
                                 counts2, offs, out, cap);
 }
 
-// Radius search in one traversal (packet path, FP64): every query's results go
+// Radius search in one traversal (packet path, FP64 or FP32 filter): every query's results go
 // to its chain of result chunks, the counts are scanned, and the chains are
 // compacted into the CSR output.  A pool that turned out too small leaves the
 // counts exact: it is sized from the total and the traversal runs once more.
@@ -142,6 +142,10 @@ int radius_one_pass(Cloud& c, int kernel, int algo, const double* dq, uint64_t n
     CK(c.ck_ctr.reserve(256));
     const uint32_t* order = nullptr;
     CK(launch_query_order(c, dq, nq, &order));
+    if (c.fp32_filter && !c.rel_built) {  // the FP32 filter reads leaf-relative coordinates
+        CK(launch_leaf_rel(c));
+        c.rel_built = true;
+    }
     uint64_t tot = 0;
     for (int attempt = 0; attempt < 2; ++attempt) {
         // pool: every query's partial last chunk plus the results (a guess of 128 per query at first)
@@ -156,8 +160,8 @@ int radius_one_pass(Cloud& c, int kernel, int algo, const double* dq, uint64_t n
         ChunkArgs ck{c.ck_pool.as<uint32_t>(), c.ck_next.as<uint32_t>(), c.ck_first.as<uint32_t>(),
                      c.ck_ctr.as<uint32_t>(), c.ck_cap};
         CK(cudaMemsetAsync(ck.ctr, 0, 4, c.stream));
-        CK(launch_radius_packet(c, kernel, pass_algo, 2, false, dq, nq, dr, radius, order, dc, nullptr, nullptr,
-                                nullptr, 0, &ck));
+        CK(launch_radius_packet(c, kernel, pass_algo, 2, c.fp32_filter != 0, dq, nq, dr, radius, order, dc, nullptr,
+                                nullptr, nullptr, 0, &ck));
         CK(launch_scan_u64(c, dc, doffs, nq));
         CK(cudaMemcpyAsync(c.pinned, doffs + nq, 8, cudaMemcpyDeviceToHost, c.stream));
         const int st = sync_and_check(c, kErrChunkCapacity);
@@ -667,9 +671,8 @@ int oct_radius_search(oct_cloud h, int kernel, int algo, const double* centers, 
         doffs = c.q_offsets.as<unsigned long long>();
     }
     const uint32_t* order = nullptr;
-    if (c.packet && !c.fp32_filter && !c.two_pass && nq) return radius_one_pass(c, kernel, algo, dq, nq, dr, radius,
-                                                                               doffs, offsets, idx, idx_capacity,
-                                                                               total, dev);
+    if (c.packet && !c.two_pass && nq)
+        return radius_one_pass(c, kernel, algo, dq, nq, dr, radius, doffs, offsets, idx, idx_capacity, total, dev);
     if (algo == OCT_NEIGHBORS_STRUCT) {
         // expanded indices of the ranges: count points, fill as prune-style runs
         CK(c.q_out2.reserve(8 * (nq ? nq : 1)));

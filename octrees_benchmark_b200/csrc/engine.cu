@@ -413,39 +413,21 @@ cudaError_t enqueue_work(oct_engine e) {
             k_escan_top<<<1, kScanThreads, 0, s>>>(part, kScanBlocks, sum);
             k_escan_apply<<<kScanBlocks, kScanThreads, 0, s>>>(counts, &dyn->n_radius, part, offs);
         };
-        if (!e->fp32) {
-            // one traversal: results into chunk chains, scan, chains compacted into the result array
-            const ChunkArgs ck = chunk_args(e);
-            if ((r = cudaMemsetAsync(ck.ctr, 0, 4, s)) != cudaSuccess) return r;
-            for (int v = 0; v < kRadiusVariants; ++v) {
-                if (!((e->sig >> v) & 1ull)) continue;
-                const int kernel = v >> 2, algo = (v & 2) ? OCT_NEIGHBORS_PRUNE : OCT_NEIGHBORS;
-                if ((r = launch_radius_table(e->device, s, kernel, algo, 2, false, &dyn->groups[v], one, 0, order,
-                                             counts, nullptr, nullptr, nullptr, 0, ctr + 2 * v, stats, err,
-                                             e->radius_bps, &ck)) != cudaSuccess)
-                    return r;
-            }
-            scan();
-            if ((r = launch_chunk_compact(e->device, s, counts, offs, ck, e->out.as<uint32_t>(), e->out.bytes / 4, 0,
-                                          &dyn->n_radius, err)) != cudaSuccess)
+        // one traversal: results into chunk chains, scan, chains compacted into the result array
+        const ChunkArgs ck = chunk_args(e);
+        if ((r = cudaMemsetAsync(ck.ctr, 0, 4, s)) != cudaSuccess) return r;
+        for (int v = 0; v < kRadiusVariants; ++v) {
+            if (!((e->sig >> v) & 1ull)) continue;
+            const int kernel = v >> 2, algo = (v & 2) ? OCT_NEIGHBORS_PRUNE : OCT_NEIGHBORS;
+            if ((r = launch_radius_table(e->device, s, kernel, algo, 2, (v & 1) != 0, &dyn->groups[v], one, 0, order,
+                                         counts, nullptr, nullptr, nullptr, 0, ctr + 2 * v, stats, err,
+                                         e->radius_bps, &ck)) != cudaSuccess)
                 return r;
-        } else {
-            // FP32 filter: count, scan, fill
-            for (int pass = 0; pass < 2; ++pass) {
-                const bool fill = pass == 1;
-                if (fill) scan();
-                for (int v = 0; v < kRadiusVariants; ++v) {
-                    if (!((e->sig >> v) & 1ull)) continue;
-                    const int kernel = v >> 2, algo = (v & 2) ? OCT_NEIGHBORS_PRUNE : OCT_NEIGHBORS;
-                    if ((r = launch_radius_table(e->device, s, kernel, algo, fill ? 1 : 0, (v & 1) != 0,
-                                                 &dyn->groups[v], one, 0, order, fill ? nullptr : counts, nullptr,
-                                                 fill ? offs : nullptr, fill ? e->out.as<uint32_t>() : nullptr,
-                                                 fill ? e->out.bytes / 4 : 0, ctr + 2 * v + pass, stats, err,
-                                                 e->radius_bps)) != cudaSuccess)
-                        return r;
-                }
-            }
         }
+        scan();
+        if ((r = launch_chunk_compact(e->device, s, counts, offs, ck, e->out.as<uint32_t>(), e->out.bytes / 4, 0,
+                                      &dyn->n_radius, err)) != cudaSuccess)
+            return r;
         const int tb = 128;
         const uint32_t cap_req = (uint32_t)(e->totals.bytes / sizeof(ReqTotal));
         k_req_totals<<<(cap_req + tb - 1) / tb, tb, 0, s>>>(dyn, table, offs, e->totals.as<ReqTotal>());
@@ -546,8 +528,7 @@ int finish(oct_engine e) {
         // query's last chunk may be partial) from the exact total and run the batch again
         int st = grow(e, e->out, 4 * (size_t)(sm.radius_total + sm.radius_total / 8 + 1024));
         if (st != OCT_OK) return st;
-        if (!e->fp32 && (st = grow_chunks(e, sm.radius_total / kResultChunk + e->n_radius + 1024)) != OCT_OK)
-            return st;
+        if ((st = grow_chunks(e, sm.radius_total / kResultChunk + e->n_radius + 1024)) != OCT_OK) return st;
         if ((st = launch_batch(e, true)) != OCT_OK) return st;
     }
     return fail(e, OCT_ERR_CAPACITY, "radius results kept outgrowing the result array");
@@ -637,7 +618,7 @@ int submit(oct_engine e, const oct_request* rq, uint32_t n) {
     if ((st = grow(e, e->knn_counts, 4 * std::max<uint64_t>(n_total, 1))) != OCT_OK) return st;
     if (knn_slots && e->knn_group && (st = grow(e, e->knn_fb, 4 * n_total)) != OCT_OK) return st;
     if ((st = grow(e, e->totals, sizeof(ReqTotal) * std::max<uint32_t>(m, 1))) != OCT_OK) return st;
-    if (!e->fp32 && n_radius) {  // one-pass radius: a first chunk per query, a pool of at least 3 chunks per query
+    if (n_radius) {  // one-pass radius: a first chunk per query, a pool of at least 3 chunks per query
         if ((st = grow(e, e->ck_first, 4 * n_radius)) != OCT_OK) return st;
         if ((st = grow(e, e->ck_ctr, 256)) != OCT_OK) return st;
         const uint64_t have = chunk_args(e).cap;

@@ -146,8 +146,8 @@ __device__ __forceinline__ int f32_test(const LeafCtx& c, float4 p) {
 #define RQ(f) (MULTI ? reqs[cur_req].f : a.single.f)
 #define RQV(f) (MULTI == 1 ? s_view[warp].f : a.single.cv.f)
 
-// Query parameters of lane j for the transposed leaf test: sphere / circle
-// (c0, c1, c2, r2), cube / square (bmin0..2, bmax0..2).
+// Query parameters of lane j for the transposed leaf and child tests: sphere /
+// circle (c0, c1, c2, r2, r), cube / square (bmin0..2, bmax0..2).
 template <int KT>
 __device__ __forceinline__ void put_query(double (*q)[32], int lane, const SearchKernel& k) {
     if constexpr (KT == kSphere || KT == kCircle) {
@@ -155,6 +155,7 @@ __device__ __forceinline__ void put_query(double (*q)[32], int lane, const Searc
         q[1][lane] = k.c[1];
         q[2][lane] = k.c[2];
         q[3][lane] = k.r2;
+        q[4][lane] = k.r;
     } else {
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
@@ -162,6 +163,78 @@ __device__ __forceinline__ void put_query(double (*q)[32], int lane, const Searc
             q[3 + a][lane] = k.bmax[a];
         }
     }
+}
+
+// Lane j's SearchKernel back from put_query's copy: the fields the box tests,
+// the leaf tests and the FP32 context read (bounds of a sphere / circle are
+// recomputed by init's own expressions, so they are the same values).
+template <int KT>
+__device__ __forceinline__ SearchKernel kernel_of(const double (*q)[32], int j) {
+    SearchKernel k;
+    if constexpr (KT == kSphere || KT == kCircle) {
+        k.c[0] = q[0][j];
+        k.c[1] = q[1][j];
+        k.c[2] = q[2][j];
+        k.r2 = q[3][j];
+        k.r = q[4][j];
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            k.bmin[a] = dsub(k.c[a], k.r);
+            k.bmax[a] = dadd(k.c[a], k.r);
+        }
+    } else {  // cube / square tests read the bounds only
+        k.r = k.r2 = 0.0;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            k.c[a] = 0.0;
+            k.bmin[a] = q[a][j];
+            k.bmax[a] = q[3 + a][j];
+        }
+    }
+    return k;
+}
+
+// FP32 leaf context of lane j's query for the transposed FP32 test: sphere /
+// circle (qx, qy, qz, r2f, b0, b1), cube / square (lo, hi, tlo, thi per axis).
+template <int KT>
+__device__ __forceinline__ void put_ctx(float (*q)[32], int lane, const LeafCtx& c) {
+    if constexpr (KT == kSphere || KT == kCircle) {
+        q[0][lane] = c.qx;
+        q[1][lane] = c.qy;
+        q[2][lane] = c.qz;
+        q[3][lane] = c.r2f;
+        q[4][lane] = c.b0;
+        q[5][lane] = c.b1;
+    } else {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            q[a][lane] = c.lo[a];
+            q[3 + a][lane] = c.hi[a];
+            q[6 + a][lane] = c.tlo[a];
+            q[9 + a][lane] = c.thi[a];
+        }
+    }
+}
+template <int KT>
+__device__ __forceinline__ LeafCtx get_ctx(const float (*q)[32], int j) {
+    LeafCtx c;
+    if constexpr (KT == kSphere || KT == kCircle) {
+        c.qx = q[0][j];
+        c.qy = q[1][j];
+        c.qz = q[2][j];
+        c.r2f = q[3][j];
+        c.b0 = q[4][j];
+        c.b1 = q[5][j];
+    } else {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            c.lo[a] = q[a][j];
+            c.hi[a] = q[3 + a][j];
+            c.tlo[a] = q[6 + a][j];
+            c.thi[a] = q[9 + a][j];
+        }
+    }
+    return c;
 }
 
 // is_inside of lane j's query for point p: the same expressions, operand for operand.
@@ -185,12 +258,17 @@ __device__ __forceinline__ bool inside_of(const double (*q)[32], int j, double p
 // k_chunk_compact moves every chain into the CSR array after the scan.
 template <int KT, int ALGO, bool FILL, bool F32, int MULTI, bool CHUNK = false>
 __global__ void __launch_bounds__(kPkThreads) k_radius_packet(PacketArgs a) {
-    // Transposed leaf test (FP64, neighbors / neighborsPrune): the lanes hold
-    // consecutive points and test them against one query of the mask at a time,
-    // so every lane does useful work and the ballot is that query's hit mask.
-    constexpr bool kT = (ALGO != kStruct) && !F32;
-    static_assert(!CHUNK || (FILL && kT), "one-pass mode needs the transposed FP64 form");
-    constexpr int kStage = kT ? 1 : kPkWarps;  // point staging, per-lane loop forms only
+    // Transposed leaf test (neighbors / neighborsPrune, FP64 or FP32 filter): the
+    // lanes hold consecutive points and test them against one query of the mask
+    // at a time, so every lane does useful work and the ballot is that query's
+    // hit mask.  The FP32 form reads the points' leaf-relative coordinates and
+    // each query's context for the leaf (made once per leaf by the query's own
+    // lane); a point inside the error band is re-tested in FP64.
+    constexpr bool kT = (ALGO != kStruct);
+    static_assert(!CHUNK || (FILL && kT), "one-pass mode needs the transposed form");
+    constexpr int kStage = (kT || F32) ? 1 : kPkWarps;  // FP64 point staging, per-lane FP64 form only
+    constexpr int kCtxF = (KT == kSphere || KT == kCircle) ? 6 : 12;  // floats of a query's FP32 leaf context
+    __shared__ float s_ctx[(F32 && kT) ? kPkWarps : 1][kCtxF][32];
     __shared__ CloudView s_view[MULTI == 1 ? kPkWarps : 1];
     __shared__ uint32_t st_node[kPkWarps][kPkStack];
     __shared__ uint32_t st_fc[kPkWarps][kPkStack];     // first child, 0 for a leaf
@@ -199,9 +277,9 @@ __global__ void __launch_bounds__(kPkThreads) k_radius_packet(PacketArgs a) {
     __shared__ uint32_t st_in[kPkWarps][kPkStack];
     __shared__ uint8_t st_depth[kPkWarps][kPkStack];
     __shared__ double s_rad[kPkWarps][kMaxDepth + 1][3];
-    __shared__ double s_qp[kT ? kPkWarps : 1][6][32];
+    __shared__ double s_qp[kPkWarps][6][32];
     __shared__ double sx[kStage][32], sy[kStage][32], sz[kStage][32];
-    __shared__ float4 sp[F32 ? kPkWarps : 1][32];
+    __shared__ float4 sp[(F32 && !kT) ? kPkWarps : 1][32];
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     double (*s_radii)[3] = s_rad[warp];
@@ -259,7 +337,8 @@ __global__ void __launch_bounds__(kPkThreads) k_radius_packet(PacketArgs a) {
         const bool approx_upper = (ALGO == kStruct) && RQ(approx_upper) != 0;
         SearchKernel k;
         k.init(qc[3 * ql], qc[3 * ql + 1], qc[3 * ql + 2], qrad ? qrad[ql] : RQ(radius));
-        if constexpr (kT) put_query<KT>(s_qp[warp], lane, k);  // read by the other lanes after a __syncwarp
+        __syncwarp();  // the previous packet's reads of s_qp are done
+        put_query<KT>(s_qp[warp], lane, k);  // read by the other lanes after a __syncwarp
         unsigned long long cnt = 0, cnt2 = 0, base = 0;
         if (FILL && !CHUNK && valid) base = a.offs[qi];
         bool overflow = false;
@@ -356,21 +435,47 @@ __global__ void __launch_bounds__(kPkThreads) k_radius_packet(PacketArgs a) {
         };
         auto scan_leaf = [&](uint32_t node, uint2 rg, uint32_t mask) {
             if constexpr (kT) {
-                (void)node;
+                if constexpr (F32) {  // each query of the mask: its context for this leaf, from its own lane
+                    __syncwarp();
+                    if ((mask >> lane) & 1u) {
+                        LeafCtx ctx;
+                        leaf_ctx<KT>(kernel_of<KT>(s_qp[warp], lane), RQV(centers) + 3ull * node, ctx);
+                        put_ctx<KT>(s_ctx[warp], lane, ctx);
+                    }
+                    __syncwarp();
+                } else {
+                    (void)node;
+                }
                 for (uint32_t b = rg.x; b < rg.y; b += 32) {
                     const uint32_t idx = b + lane;
                     const bool in_range = idx < rg.y;
                     double px = 0.0, py = 0.0, pz = 0.0;
+                    float4 pf = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
                     if (in_range) {
-                        px = RQV(xs)[idx];
-                        py = RQV(ys)[idx];
-                        pz = RQV(zs)[idx];
+                        if constexpr (F32) {
+                            pf = RQV(rel)[idx];
+                        } else {
+                            px = RQV(xs)[idx];
+                            py = RQV(ys)[idx];
+                            pz = RQV(zs)[idx];
+                        }
                     }
                     uint32_t rem = mask;
                     while (rem) {
                         const int j = __ffs(rem) - 1;
                         rem &= rem - 1;
-                        const bool in = in_range && inside_of<KT>(s_qp[warp], j, px, py, pz);
+                        bool in;
+                        if constexpr (F32) {
+                            const int r = in_range ? f32_test<KT>(get_ctx<KT>(s_ctx[warp], j), pf) : 0;
+                            if (r < 0) {  // inside the error band: the reference's FP64 expression decides
+                                in = inside_of<KT>(s_qp[warp], j, RQV(xs)[idx], RQV(ys)[idx], RQV(zs)[idx]);
+                                ++n_retests;
+                            } else {
+                                in = r > 0;
+                            }
+                        } else {
+                            in = in_range && inside_of<KT>(s_qp[warp], j, px, py, pz);
+                        }
                         const uint32_t hb = __ballot_sync(0xffffffffu, in);
                         if constexpr (CHUNK) {
                             if (hb) {
@@ -533,7 +638,6 @@ __global__ void __launch_bounds__(kPkThreads) k_radius_packet(PacketArgs a) {
                 continue;
             }
             const uint32_t cd = depth + 1;
-            const bool mine = (mo & lbit) != 0;
             // lane j (< 8) keeps child j's first-child link, range and lane masks
             uint32_t my_fc = 0, my_mo = 0, my_mi = 0;
             uint2 my_rg = make_uint2(0u, 0u);
@@ -544,26 +648,47 @@ __global__ void __launch_bounds__(kPkThreads) k_radius_packet(PacketArgs a) {
             // neighborsApprox (linear_octree.hpp:979-985): below its precision level a
             // child is cut before any box test, its whole range added in upper-bound mode
             const bool cut = ALGO == kStruct && approx_cut != 0 && cd >= approx_cut;
+            {
+                // child tests transposed: lane = (query slot lane / 8, child lane % 8), the
+                // node's active queries four at a time, so a node that few queries of the
+                // packet reach costs few passes; each lane tests with the query's own
+                // SearchKernel and the child's centre, as the per-query walk does
+                const int slot = lane >> 3;
+                const double* ocp = RQV(centers) + 3ull * (fc + (lane & 7));
+                const double oc[3] = {ocp[0], ocp[1], ocp[2]};
+                uint32_t rem = mo;
+                while (rem) {
+                    int ql[4];
 #pragma unroll
-            for (int j = 0; j < 8; ++j) {
-                bool o = false, n = false;
-                if (mine) {
-                    const double* oc = RQV(centers) + 3ull * (fc + j);
-                    if constexpr (ALGO == kNeighbors) {
-                        o = box_overlap<KT>(k, oc, s_radii[cd]);
-                    } else if (cut) {
-                        n = approx_upper;
-                    } else {
-                        const int jj = box_intersect<KT>(k, oc, s_radii[cd]);
-                        n = (jj == kInside);
-                        o = (jj == kOverlap);
+                    for (int s = 0; s < 4; ++s) {
+                        ql[s] = rem ? __ffs(rem) - 1 : -1;
+                        rem &= rem - 1;
                     }
-                }
-                const uint32_t bo = __ballot_sync(0xffffffffu, o);
-                const uint32_t bi = __ballot_sync(0xffffffffu, n);
-                if (lane == j) {
-                    my_mo = bo;
-                    my_mi = bi;
+                    const int myq = slot == 0 ? ql[0] : slot == 1 ? ql[1] : slot == 2 ? ql[2] : ql[3];
+                    bool o = false, n = false;
+                    if (myq >= 0) {
+                        const SearchKernel kq = kernel_of<KT>(s_qp[warp], myq);
+                        if constexpr (ALGO == kNeighbors) {
+                            o = box_overlap<KT>(kq, oc, s_radii[cd]);
+                        } else if (cut) {
+                            n = approx_upper;
+                        } else {
+                            const int jj = box_intersect<KT>(kq, oc, s_radii[cd]);
+                            n = (jj == kInside);
+                            o = (jj == kOverlap);
+                        }
+                    }
+                    const uint32_t bo = __ballot_sync(0xffffffffu, o);
+                    const uint32_t bi = __ballot_sync(0xffffffffu, n);
+                    if (lane < 8) {  // bit 8 s + j of a ballot: query ql[s] against child j
+#pragma unroll
+                        for (int s = 0; s < 4; ++s) {
+                            if (ql[s] >= 0) {
+                                my_mo |= ((bo >> (8 * s + lane)) & 1u) << ql[s];
+                                my_mi |= ((bi >> (8 * s + lane)) & 1u) << ql[s];
+                            }
+                        }
+                    }
                 }
             }
             if (lane < 8 && my_fc == 0 && my_rg.x == my_rg.y) {  // empty leaf: nothing to scan or add
@@ -647,7 +772,10 @@ cudaError_t launch_pk_m(const PacketArgs& a, int mode, bool fp32, int grid, cuda
         return cudaErrorInvalidValue;
     }
     if (mode == 2) {
-        if constexpr (ALGO != kStruct) k_radius_packet<KT, ALGO, true, false, MULTI, true><<<grid, kPkThreads, 0, s>>>(a);
+        if constexpr (ALGO != kStruct) {
+            if (fp32) k_radius_packet<KT, ALGO, true, true, MULTI, true><<<grid, kPkThreads, 0, s>>>(a);
+            else k_radius_packet<KT, ALGO, true, false, MULTI, true><<<grid, kPkThreads, 0, s>>>(a);
+        }
     } else if (mode == 1) {
         if (fp32) k_radius_packet<KT, ALGO, true, true, MULTI><<<grid, kPkThreads, 0, s>>>(a);
         else k_radius_packet<KT, ALGO, true, false, MULTI><<<grid, kPkThreads, 0, s>>>(a);
@@ -769,7 +897,7 @@ cudaError_t launch_radius_table(int device, cudaStream_t s, int kernel, int algo
     a.chunk_first = chunks ? chunks->first : nullptr;
     a.chunk_ctr = chunks ? chunks->ctr : nullptr;
     a.chunk_cap = chunks ? chunks->cap : 0;
-    if (mode == 2 && (!chunks || fp32 || algo == kStruct)) return cudaErrorInvalidValue;
+    if (mode == 2 && (!chunks || algo == kStruct)) return cudaErrorInvalidValue;
     // persistent grid: warps take packets from the counter until none is left
     const uint64_t cap = (uint64_t)sm_count_p(device) * (blocks_per_sm > 0 ? blocks_per_sm : 12);
     const uint64_t want = d_grp ? cap : (packets + kPkWarps - 1) / kPkWarps;
