@@ -108,6 +108,9 @@ constexpr double kKnnEstimate = 1.2;
 // Group kNN: consecutive query groups a warp takes at a time (the later ones start
 // from the previous group's k-th distances).
 constexpr uint32_t kKnnGroupChunk = 4;
+// group kNN heads: every kKnnHeadStride-th group is searched first, from the
+// density estimate; the others start from a neighbouring group's k-th distance
+constexpr uint32_t kKnnHeadStride = 16;
 // Queries per warp of the group kNN (4 or 8).  4: half the shared memory per
 // warp, so 28 warps per SM instead of 16, for ~1.6x the node visits per query;
 // ~20 % faster on the 10M-point tile (k = 50).
@@ -155,6 +158,7 @@ struct Cloud {
     uint32_t qs_epoch = 0;
     DevBuf packet_ctr;  // dynamic packet counters
     DevBuf knn_fb;      // group kNN: fallback count (u64) at 0, fallback query list (u32) from byte 16
+    DevBuf knn_heads;   // group kNN: the heads' largest k-th distances (f64 per head)
     DevBuf stats;       // device counters: points tested, FP64 band re-tests, ...
     // FP32 leaf-relative coordinates (x, y, z, 0) per sorted point, built on demand
     DevBuf rel;
@@ -240,7 +244,7 @@ cudaError_t launch_knn_group_table(int device, cudaStream_t s, const DynGroup* d
                                    const SearchReq* single, uint32_t kmax, const uint32_t* d_order, uint32_t bucket,
                                    uint32_t* d_idx, double* d_d2, uint32_t* d_counts, uint32_t* d_err,
                                    uint32_t* d_packet_ctr, uint32_t* d_fb_list, double est, uint32_t chunk,
-                                   int blocks_per_sm);
+                                   int blocks_per_sm, double* d_head_kth, size_t head_bytes);
 CloudView cloud_view(const Cloud& c);
 // Batched engine: the sort of query keys with device-side sizes (encode_sort.cu),
 // and the shared-memory limits of the table kNN list kernels (knn_search.cu).

@@ -255,6 +255,7 @@ struct oct_engine_s {
     DevBuf ctrs, stats, summary, totals;
     DevBuf ck_pool, ck_next, ck_first, ck_ctr;  // one-pass radius: result chunks (ck_next has one word per chunk)
     DevBuf knn_fb;  // group kNN fallback list, one entry per query position
+    DevBuf knn_heads;  // group kNN: the heads' largest k-th distances (f64 per head)
     // pinned host staging
     unsigned char* h_stage = nullptr;
     size_t h_stage_bytes = 0;
@@ -389,8 +390,9 @@ cudaError_t enqueue_work(oct_engine e) {
                 r2 = launch_knn_group_table(e->device, ks, &dyn->groups[kRadiusVariants + v], &dyn->fb[v], one,
                                             32u << v, order, e->bucket, e->knn_idx.as<uint32_t>(),
                                             e->knn_d2.as<double>(), e->knn_counts.as<uint32_t>(), err,
-                                            ctr + 2 * kRadiusVariants + 2 * v, e->knn_fb.as<uint32_t>(),
-                                            kKnnEstimate, kKnnGroupChunk, e->knn_bps);
+                                            ctr + 2 * kRadiusVariants + 4 * v, e->knn_fb.as<uint32_t>(),
+                                            kKnnEstimate, kKnnGroupChunk, e->knn_bps, e->knn_heads.as<double>(),
+                                            e->knn_heads.bytes);
             else
                 r2 = launch_knn_table(e->device, ks, &dyn->groups[kRadiusVariants + v], one, 0, 32u << v,
                                       order, e->bucket, e->knn_idx.as<uint32_t>(), e->knn_d2.as<double>(),
@@ -616,7 +618,12 @@ int submit(oct_engine e, const oct_request* rq, uint32_t n) {
     if ((st = grow(e, e->knn_idx, 4 * std::max<uint64_t>(knn_slots, 1))) != OCT_OK) return st;
     if ((st = grow(e, e->knn_d2, 8 * std::max<uint64_t>(knn_slots, 1))) != OCT_OK) return st;
     if ((st = grow(e, e->knn_counts, 4 * std::max<uint64_t>(n_total, 1))) != OCT_OK) return st;
-    if (knn_slots && e->knn_group && (st = grow(e, e->knn_fb, 4 * n_total)) != OCT_OK) return st;
+    if (knn_slots && e->knn_group) {
+        if ((st = grow(e, e->knn_fb, 4 * n_total)) != OCT_OK) return st;
+        // heads: one per kKnnHeadStride groups of every request (each request's groups round up)
+        const uint64_t groups = n_total / kKnnGroupQueries + m;
+        if ((st = grow(e, e->knn_heads, 8 * (groups / kKnnHeadStride + 2))) != OCT_OK) return st;
+    }
     if ((st = grow(e, e->totals, sizeof(ReqTotal) * std::max<uint32_t>(m, 1))) != OCT_OK) return st;
     if (n_radius) {  // one-pass radius: a first chunk per query, a pool of at least 3 chunks per query
         if ((st = grow(e, e->ck_first, 4 * n_radius)) != OCT_OK) return st;
@@ -768,7 +775,7 @@ int oct_engine_create(const oct_engine_params* p, oct_engine* out) {
     if (r == cudaSuccess) r = prepare_knn_dyn();
     if (r == cudaSuccess) r = e->sort_ctl.reserve(sizeof(SortCtl));
     if (r == cudaSuccess) r = e->epoch.reserve(256);
-    if (r == cudaSuccess) r = e->ctrs.reserve(4 * 2 * (kRadiusVariants + 2));  // + group kNN (2 per variant)
+    if (r == cudaSuccess) r = e->ctrs.reserve(4 * (2 * kRadiusVariants + 4 * 2));  // + group kNN (3 of 4 per variant)
     if (r == cudaSuccess) r = e->stats.reserve(64);
     if (r == cudaSuccess) r = e->summary.reserve(256);
     if (r == cudaSuccess) r = e->part.reserve(8 * (kScanBlocks + 1));
@@ -797,7 +804,8 @@ int oct_engine_destroy(oct_engine e) {
         DevBuf* bufs[] = {&e->desc, &e->keys[0], &e->keys[1], &e->ord[0], &e->ord[1], &e->sort_ctl, &e->sort_status,
                           &e->epoch, &e->counts, &e->offs, &e->part, &e->out, &e->knn_idx, &e->knn_d2,
                           &e->knn_counts, &e->ctrs, &e->stats, &e->summary, &e->totals,
-                          &e->ck_pool, &e->ck_next, &e->ck_first, &e->ck_ctr, &e->knn_fb};
+                          &e->ck_pool, &e->ck_next, &e->ck_first, &e->ck_ctr, &e->knn_fb,
+                          &e->knn_heads};
         for (DevBuf* b : bufs) b->release();
         if (e->h_stage) cudaFreeHost(e->h_stage);
         if (e->h_summary) cudaFreeHost(e->h_summary);
@@ -993,7 +1001,8 @@ int oct_engine_memory(oct_engine e, uint64_t* bytes) {
     const DevBuf* bufs[] = {&e->desc, &e->keys[0], &e->keys[1], &e->ord[0], &e->ord[1], &e->sort_ctl,
                             &e->sort_status, &e->epoch, &e->counts, &e->offs, &e->part, &e->out, &e->knn_idx,
                             &e->knn_d2, &e->knn_counts, &e->ctrs, &e->stats, &e->summary, &e->totals,
-                            &e->ck_pool, &e->ck_next, &e->ck_first, &e->ck_ctr, &e->knn_fb};
+                            &e->ck_pool, &e->ck_next, &e->ck_first, &e->ck_ctr, &e->knn_fb,
+                          &e->knn_heads};
     uint64_t s = 0;
     for (const DevBuf* b : bufs) s += b->bytes;
     *bytes = s;

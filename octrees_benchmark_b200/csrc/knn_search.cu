@@ -756,8 +756,10 @@ struct KnnGroupArgs {
     uint32_t* counts;
     uint32_t* err;
     double est;                       // provisional-threshold factor (0: off, also no seeding)
-    uint32_t* packet_ctr;             // [0] runs of `chunk` groups, [1] single groups at the end
+    uint32_t* packet_ctr;             // [0] runs of `chunk` groups, [1] single groups at the end, [2] heads
     uint32_t chunk;                   // consecutive groups per fetch (>= 1)
+    uint32_t head_stride;             // S > 1: every S-th group is a head, taken first (0: no heads)
+    double* head_kth;                 // per head: the largest k-th distance it found (NaN: not yet, < 0: none)
     uint32_t* fb_list;                // queries left to k_knn_reg (global positions; a batch group's
                                       // entries start at its q_begin)
     unsigned long long* fb_count;
@@ -823,39 +825,56 @@ __global__ void __launch_bounds__(kGrpThreads, kGrpMinBlocks) k_knn_group(KnnGro
     constexpr int LPQ = 32 / G, CPL = 8 / LPQ;
     static_assert(G == 4 || G == 8, "4 or 8 queries per warp");
     const int qj = lane / LPQ, cs = lane % LPQ;
-    // groups [0, p_chunked) go out in chunks, the rest one at a time
+    // heads (every S-th group) go out first, one at a time; the other groups are
+    // slots: slot s is the s-th group that is not a head (every group without heads)
+    const uint32_t S = a.head_stride;
+    const uint32_t n_heads = S ? (packets + S - 1) / S : 0;
+    const uint32_t slots = packets - n_heads;
+    bool heads_left = n_heads != 0;
+    // slots [0, p_chunked) go out in chunks, the rest one at a time
     const uint32_t nw = gridDim.x * kGrpWarps;
     const uint32_t chunk = a.chunk;
-    const uint32_t p_chunked = (chunk > 1 && packets > 2 * nw) ? (packets - 2 * nw) / chunk * chunk : 0;
+    const uint32_t p_chunked = (chunk > 1 && slots > 2 * nw) ? (slots - 2 * nw) / chunk * chunk : 0;
     uint32_t next = 0, chunk_end = 0;
-    // seed: the previous group's largest k-th distance (< 0: none), its group and request
+    // seed: the previous group's largest k-th distance (< 0: none), its slot and request
     double seed_thr = -1.0;
-    uint32_t seed_packet = 0;
+    uint32_t seed_slot = 0;
     uint32_t seed_ri = 0;
 
     for (;;) {
-        uint32_t packet;
-        if (next < chunk_end) {
-            packet = next++;
-        } else {
-            uint32_t v = 0;
-            if (lane == 0) v = atomicAdd(&a.packet_ctr[0], 1u);
-            v = __shfl_sync(0xffffffffu, v, 0);
-            const uint64_t c0 = (uint64_t)v * chunk;
-            if (c0 < p_chunked) {
-                packet = (uint32_t)c0;
-                next = packet + 1;
-                chunk_end = packet + chunk;
-            } else {
-                uint32_t s = 0;
-                if (lane == 0) s = atomicAdd(&a.packet_ctr[1], 1u);
-                s = __shfl_sync(0xffffffffu, s, 0);
-                if ((uint64_t)p_chunked + s >= packets) break;
-                packet = p_chunked + s;
-                next = chunk_end = 0;
-            }
+        uint32_t slot = 0xffffffffu;  // the head's group index when a head
+        bool head = false;
+        if (heads_left) {
+            uint32_t h = 0;
+            if (lane == 0) h = atomicAdd(&a.packet_ctr[2], 1u);
+            h = __shfl_sync(0xffffffffu, h, 0);
+            if (h < n_heads) head = true, slot = h;
+            else heads_left = false;
         }
-        if (packet >= packets) break;
+        if (!head) {
+            if (next < chunk_end) {
+                slot = next++;
+            } else {
+                uint32_t v = 0;
+                if (lane == 0) v = atomicAdd(&a.packet_ctr[0], 1u);
+                v = __shfl_sync(0xffffffffu, v, 0);
+                const uint64_t c0 = (uint64_t)v * chunk;
+                if (c0 < p_chunked) {
+                    slot = (uint32_t)c0;
+                    next = slot + 1;
+                    chunk_end = slot + chunk;
+                } else {
+                    uint32_t s = 0;
+                    if (lane == 0) s = atomicAdd(&a.packet_ctr[1], 1u);
+                    s = __shfl_sync(0xffffffffu, s, 0);
+                    if ((uint64_t)p_chunked + s >= slots) break;
+                    slot = p_chunked + s;
+                    next = chunk_end = 0;
+                }
+            }
+            if (slot >= slots) break;
+        }
+        const uint32_t packet = head ? slot * S : !S ? slot : slot + slot / (S - 1) + 1;
         uint32_t ri = 0;
         if (MULTI) {  // the request of this group (packet_begin ascending over the table)
             uint32_t lo = 0, hi = nreq;
@@ -878,7 +897,22 @@ __global__ void __launch_bounds__(kGrpThreads, kGrpMinBlocks) k_knn_group(KnnGro
         const uint32_t q_begin = (uint32_t)KRQ(q_begin);
         const uint32_t pos0 = q_begin + (uint32_t)G * (packet - (uint32_t)KRQ(packet_begin));
         const uint32_t q_end = (uint32_t)KRQ(q_end);
-        const bool seeded = a.est > 0.0 && seed_thr >= 0.0 && packet == seed_packet + 1 && ri == seed_ri;
+        // seed: the group before this one in the warp's run, else (between heads) the
+        // nearest head of the same request
+        // heads start from the density estimate
+        double seed = (a.est > 0.0 && !head && seed_thr >= 0.0 && slot == seed_slot + 1 && ri == seed_ri)
+                          ? seed_thr : -1.0;
+        if (seed < 0.0 && a.est > 0.0 && S && !head) {
+            const uint32_t pb = (uint32_t)KRQ(packet_begin);
+            const uint32_t pe = pb + (uint32_t)((KRQ(q_end) - KRQ(q_begin) + G - 1) / G);
+            const uint32_t hlo = packet / S, hhi = hlo + 1;  // heads hlo S < packet < hhi S
+            const bool lo_ok = hlo * S >= pb, hi_ok = hhi < n_heads && hhi * S < pe;
+            const bool use_hi = hi_ok && (!lo_ok || hhi * S - packet < packet - hlo * S);
+            // a head not finished yet reads NaN: no seed (nothing waits for it)
+            if (use_hi || lo_ok) seed = __ldcg(&a.head_kth[use_hi ? hhi : hlo]);
+            if (!(seed >= 0.0)) seed = -1.0;
+        }
+        const bool seeded = seed >= 0.0;
         // lanes j < G: load query j, reset its state
         bool valid = false;
         if (lane < G) {
@@ -890,7 +924,7 @@ __global__ void __launch_bounds__(kGrpThreads, kGrpMinBlocks) k_knn_group(KnnGro
             qs[lane][0] = qc[3 * ql];
             qs[lane][1] = qc[3 * ql + 1];
             qs[lane][2] = qc[3 * ql + 2];
-            thr[lane] = seeded ? kGrpSeed * seed_thr : (double)INFINITY;
+            thr[lane] = seeded ? kGrpSeed * seed : (double)INFINITY;
             thri[lane] = 0xffffffffu;  // with the pair order a provisional threshold accepts d <= thr
             nls[lane] = 0;
             nbs[lane] = 0;
@@ -1140,8 +1174,9 @@ __global__ void __launch_bounds__(kGrpThreads, kGrpMinBlocks) k_knn_group(KnnGro
         for (int off = 4; off > 0; off >>= 1) mx = fmax(mx, __shfl_xor_sync(0xffffffffu, mx, off));
         mx = __shfl_sync(0xffffffffu, mx, 0);
         seed_thr = mx;
-        seed_packet = packet;
+        seed_slot = head ? 0xfffffffeu : slot;  // a head seeds no slot of the run
         seed_ri = ri;
+        if (head && lane == 0) __stcg(&a.head_kth[slot], mx);
         __syncwarp();
     }
 }
@@ -1172,6 +1207,23 @@ cudaError_t launch_group(const KnnGroupArgs& g, int sms, cudaStream_t s, int blo
     if (grid == 0) return cudaSuccess;
     k_knn_group<R, MULTI><<<(int)grid, kGrpThreads, 0, s>>>(g);
     return cudaGetLastError();
+}
+
+// The group search of a launch.  With seeding, every kKnnHeadStride-th group
+// is a head: the heads go out first and start from the density estimate; every
+// other group starts from its run's previous group or, when it leads its run,
+// from the nearest head that has finished.  packet_ctr holds 3 counters (zeroed);
+// head_kth one double per head, set to NaN here.
+template <int R, int MULTI>
+cudaError_t launch_group_passes(KnnGroupArgs g, int sms, cudaStream_t s, int blocks_per_sm, double* head_kth,
+                                size_t head_bytes) {
+    g.head_stride = (g.est > 0.0 && head_kth) ? kKnnHeadStride : 0;
+    g.head_kth = head_kth;
+    if (g.head_stride) {
+        const cudaError_t e = cudaMemsetAsync(head_kth, 0xff, head_bytes, s);
+        if (e != cudaSuccess) return e;
+    }
+    return launch_group<R, MULTI>(g, sms, s, blocks_per_sm);
 }
 
 int sm_count_k(int device) {
@@ -1231,10 +1283,10 @@ cudaError_t launch_knn_group_table(int device, cudaStream_t s, const DynGroup* d
                                    const SearchReq* single, uint32_t kmax, const uint32_t* d_order, uint32_t bucket,
                                    uint32_t* d_idx, double* d_d2, uint32_t* d_counts, uint32_t* d_err,
                                    uint32_t* d_packet_ctr, uint32_t* d_fb_list, double est, uint32_t chunk,
-                                   int blocks_per_sm) {
+                                   int blocks_per_sm, double* d_head_kth, size_t head_bytes) {
     if (kmax > 64) return cudaErrorInvalidValue;
     cudaError_t e;
-    if ((e = cudaMemsetAsync(d_packet_ctr, 0, 8, s)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(d_packet_ctr, 0, 12, s)) != cudaSuccess) return e;
     KnnGroupArgs g{};
     g.single = single ? *single : SearchReq{};
     g.grp = d_grp;
@@ -1251,8 +1303,12 @@ cudaError_t launch_knn_group_table(int device, cudaStream_t s, const DynGroup* d
     g.fb_count = reinterpret_cast<unsigned long long*>(&d_fb->nq);
     const int sms = sm_count_k(device);
     const int bps = blocks_per_sm;
-    if (single) e = (kmax <= 32) ? launch_group<1, 2>(g, sms, s, bps) : launch_group<2, 2>(g, sms, s, bps);
-    else e = (kmax <= 32) ? launch_group<1, 1>(g, sms, s, bps) : launch_group<2, 1>(g, sms, s, bps);
+    if (single)
+        e = (kmax <= 32) ? launch_group_passes<1, 2>(g, sms, s, bps, d_head_kth, head_bytes)
+                         : launch_group_passes<2, 2>(g, sms, s, bps, d_head_kth, head_bytes);
+    else
+        e = (kmax <= 32) ? launch_group_passes<1, 1>(g, sms, s, bps, d_head_kth, head_bytes)
+                         : launch_group_passes<2, 1>(g, sms, s, bps, d_head_kth, head_bytes);
     if (e != cudaSuccess) return e;
     // the queries handed back, exactly and without the provisional threshold
     return launch_knn_table(device, s, d_fb, single, 0, kmax, d_fb_list, bucket, d_idx, d_d2, d_counts, d_err,
@@ -1315,7 +1371,10 @@ cudaError_t launch_knn(Cloud& c, const double* d_centers, uint64_t nq, uint32_t 
         cudaError_t e;
         if ((e = c.packet_ctr.reserve(256)) != cudaSuccess) return e;
         if ((e = c.knn_fb.reserve(16 + 4 * nq)) != cudaSuccess) return e;
-        if ((e = cudaMemsetAsync(c.packet_ctr.ptr, 0, 8, c.stream)) != cudaSuccess) return e;
+        const uint64_t n_groups = (nq + kGrpQ - 1) / kGrpQ;
+        const size_t head_bytes = 8 * (n_groups / kKnnHeadStride + 1);
+        if ((e = c.knn_heads.reserve(head_bytes)) != cudaSuccess) return e;
+        if ((e = cudaMemsetAsync(c.packet_ctr.ptr, 0, 12, c.stream)) != cudaSuccess) return e;
         if ((e = cudaMemsetAsync(c.knn_fb.ptr, 0, 8, c.stream)) != cudaSuccess) return e;
         KnnGroupArgs g{};
         g.single = r;
@@ -1333,7 +1392,9 @@ cudaError_t launch_knn(Cloud& c, const double* d_centers, uint64_t nq, uint32_t 
         g.fb_count = c.knn_fb.as<unsigned long long>();
         g.fb_list = reinterpret_cast<uint32_t*>(c.knn_fb.as<unsigned char>() + 16);
         const int sms = sm_count_k(c.device);
-        e = (k <= 32) ? launch_group<1, 0>(g, sms, c.stream) : launch_group<2, 0>(g, sms, c.stream);
+        double* heads = c.knn_heads.as<double>();
+        e = (k <= 32) ? launch_group_passes<1, 0>(g, sms, c.stream, 0, heads, head_bytes)
+                      : launch_group_passes<2, 0>(g, sms, c.stream, 0, heads, head_bytes);
         if (e != cudaSuccess) return e;
         KnnTableArgs f{};
         f.single = r;
