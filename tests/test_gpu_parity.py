@@ -108,6 +108,34 @@ def test_gpu_build_matches_oracle(synth_cases, case):
     oc.close()
 
 
+@pytest.mark.parametrize("enc", [1, 5])
+def test_gpu_build_dense_cluster(port, enc):
+    """20k of 40k points inside one tiny cell (most with equal keys): the sort
+    keeps them in input order and the deep leaves match the oracle."""
+    xyz = lidar_tile(40_000, 80.0, 35)
+    xyz[:20_000] = xyz[7] + 1e-9 * np.arange(20_000, dtype=np.float64)[:, None]
+    keys, perm, box, sxyz = port.encode_sort(enc, xyz)
+    t = port.build(enc, keys, 32, box)
+    oc = LinearOctree(xyz, encoder=enc, max_points_leaf=32)
+    info = [t.n, t.n_leaf, t.n_internal, t.n_total, t.max_depth]
+    check_cloud_against(oc, keys, perm, box, sxyz, info, t.arrays())
+    oc.close()
+
+
+@pytest.mark.parametrize("n", [1, 2, 100, 3071, 3072, 3073, 8193, 70_000])
+def test_gpu_sort_sizes(port, n):
+    """Keys, order and sorted points at sizes around the sort's 3072-key tiles
+    and its single-tile and many-tile cases."""
+    xyz = lidar_tile(max(n, 2), 120.0, 36)[:n]
+    keys, perm, box, sxyz = port.encode_sort(5, xyz)
+    oc = LinearOctree(xyz, encoder="hilbert", max_points_leaf=64)
+    gk, gp, gx = oc.sorted_points()
+    assert np.array_equal(gk, keys)
+    assert np.array_equal(gp.astype(np.uint64), np.asarray(perm, np.uint64))
+    assert same_f64(gx, sxyz)
+    oc.close()
+
+
 @pytest.mark.parametrize("case", range(len(SYNTH)))
 @pytest.mark.parametrize("search", [p for p in PATHS if not p.startswith("knn")])
 def test_gpu_radius_matches_oracle(synth_cases, case, search):
