@@ -7,7 +7,8 @@
 // B200 design:
 //  * k_bbox: one pass over the AoS input, block min/max, the last block folds
 //    the partials and writes the Box and the per-level geometry.
-//  * k_encode: anchor coordinates + Morton/Hilbert key per point, and in the
+//  * k_encode: anchor coordinates + Morton/Hilbert key per point (Hilbert: the
+//    24-state automaton walked two levels per shared-memory lookup), and in the
 //    same pass the 8 digit histograms of every key (so no pass re-reads keys
 //    to count).
 //  * k_onesweep: one kernel per 8-bit digit, single-pass "onesweep" radix
@@ -169,8 +170,12 @@ __global__ void __launch_bounds__(kEncThreads) k_encode(const double* __restrict
                                                         SortCtl* ctl) {
     __shared__ uint32_t hist[8 * 256];
     __shared__ uint8_t htbl[kHilbertStates * 8];
+    __shared__ uint16_t htbl2[ENC == 5 ? kHilbertTable2Size : 1];
     for (int j = threadIdx.x; j < 8 * 256; j += blockDim.x) hist[j] = 0;
-    for (int j = threadIdx.x; j < kHilbertStates * 8; j += blockDim.x) htbl[j] = kHilbertTable[j];
+    if constexpr (ENC == 5) {
+        for (int j = threadIdx.x; j < kHilbertStates * 8; j += blockDim.x) htbl[j] = kHilbertTable[j];
+        hilbert_table2_fill(htbl2, threadIdx.x, blockDim.x);
+    }
     const double c0 = bg->box.center[0], c1 = bg->box.center[1], c2 = bg->box.center[2];
     const double r0 = bg->box.radii[0], r1 = bg->box.radii[1], r2 = bg->box.radii[2];
     const double i0 = __drcp_rn(dmul(2.0, r0)), i1 = __drcp_rn(dmul(2.0, r1)), i2 = __drcp_rn(dmul(2.0, r2));
@@ -180,7 +185,7 @@ __global__ void __launch_bounds__(kEncThreads) k_encode(const double* __restrict
         const uint32_t ax = anchor_coord_fast(px, c0, r0, i0);
         const uint32_t ay = anchor_coord_fast(py, c1, r1, i1);
         const uint32_t az = anchor_coord_fast(pz, c2, r2, i2);
-        const uint64_t k = (ENC == 5) ? hilbert_encode_tbl(ax, ay, az, htbl) : morton_encode(ax, ay, az);
+        const uint64_t k = (ENC == 5) ? hilbert_encode_tbl2(ax, ay, az, htbl, htbl2) : morton_encode(ax, ay, az);
 #pragma unroll
         for (int p = 0; p < 8; ++p) atomicAdd(&hist[p * 256 + (uint32_t)((k >> (8 * p)) & 255u)], 1u);
         return k;
@@ -420,11 +425,24 @@ size_t onesweep_smem() {
 
 }  // namespace
 
+// Resident k_bbox blocks per SM: its grid is one full wave (with 4 blocks per
+// SM asked and 3 resident, the partial second wave cost 116 against 89 us on
+// 10M points).
+int bbox_blocks_per_sm() {
+    static int per = 0;
+    if (per == 0) {
+        int v = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, k_bbox, kBboxThreads, 0) != cudaSuccess || v < 1) v = 1;
+        per = v;
+    }
+    return per;
+}
+
 cudaError_t launch_bbox_encode(Cloud& c, const double* d_xyz) {
     cudaError_t e;
     const uint64_t n = c.n;
     const int sms = sm_count(c.device);
-    const int grid_bbox = sms * 4;
+    const int grid_bbox = sms * bbox_blocks_per_sm();
     if ((e = c.d_box.reserve(sizeof(BoxGeom))) != cudaSuccess) return e;
     if ((e = c.d_ctl.reserve(sizeof(SortCtl))) != cudaSuccess) return e;
     if ((e = c.parts.reserve(sizeof(double) * 6 * grid_bbox + 64)) != cudaSuccess) return e;

@@ -156,6 +156,33 @@ __device__ __forceinline__ uint64_t hilbert_encode_tbl(uint32_t x, uint32_t y, u
     return key;
 }
 
+// Two levels per lookup: entry = next_state << 6 | first digit << 3 | second
+// digit, indexed [state * 64 + octant at level L * 8 + octant at level L - 1],
+// composed from kHilbertTable (the same walk, half the lookups).  The octant
+// pairs come from one bit interleave with x in the high bit of each triple.
+constexpr int kHilbertTable2Size = kHilbertStates * 64;
+__device__ __forceinline__ void hilbert_table2_fill(uint16_t* t2, int tid, int nthreads) {
+    for (int i = tid; i < kHilbertTable2Size; i += nthreads) {
+        const uint32_t e1 = kHilbertTable[(i >> 6) * 8 + ((i >> 3) & 7)];
+        const uint32_t e2 = kHilbertTable[(e1 >> 3) * 8 + (i & 7)];
+        t2[i] = (uint16_t)(((e2 >> 3) << 6) | ((e1 & 7u) << 3) | (e2 & 7u));
+    }
+}
+__device__ __forceinline__ uint64_t hilbert_encode_tbl2(uint32_t x, uint32_t y, uint32_t z, const uint8_t* t1,
+                                                        const uint16_t* t2) {
+    const uint64_t m = spread3(z) | (spread3(y) << 1) | (spread3(x) << 2);
+    const uint32_t e = t1[(uint32_t)(m >> 60) & 7u];  // level 20 alone (21 levels)
+    uint64_t key = e & 7u;
+    uint32_t st = e >> 3;
+#pragma unroll
+    for (int level = 19; level > 0; level -= 2) {
+        const uint32_t e2 = t2[st * 64 + ((uint32_t)(m >> (3 * (level - 1))) & 63u)];
+        key = (key << 6) | (e2 & 63u);
+        st = e2 >> 6;
+    }
+    return key;
+}
+
 // Anchor coordinate through a reciprocal: t' = x * RN(1 / 2r) differs from the
 // reference's t = RN(x / 2r) by at most 1.5 * 2^-52 |t|, so for |t| <= 1 the
 // scaled values differ by at most 2^-30.  When t' * 2^21 lies in [0, 2^21) and
