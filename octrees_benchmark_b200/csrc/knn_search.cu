@@ -943,12 +943,25 @@ __global__ void __launch_bounds__(kGrpThreads, kGrpMinBlocks) k_knn_group(KnnGro
             const double cdv = (lane < (int)nb) ? bd[j][lane] : (double)INFINITY;
             const uint32_t civ = (lane < (int)nb) ? bi[j][lane] : 0xffffffffu;
             RegList<R> L;
+            if (nls[j] == 0) {  // an empty list (every entry +inf): the sorted candidates are the merge
+                double sd = cdv;
+                uint32_t si = civ;
+                warp_sort32(sd, si);
+                L.d[0] = sd;
+                L.i[0] = si;
 #pragma unroll
-            for (int r = 0; r < R; ++r) {
-                L.d[r] = ld[j][r * 32 + lane];
-                L.i[r] = li[j][r * 32 + lane];
+                for (int r = 1; r < R; ++r) {
+                    L.d[r] = INFINITY;
+                    L.i[r] = 0xffffffffu;
+                }
+            } else {
+#pragma unroll
+                for (int r = 0; r < R; ++r) {
+                    L.d[r] = ld[j][r * 32 + lane];
+                    L.i[r] = li[j][r * 32 + lane];
+                }
+                reglist_merge32<R>(L, cdv, civ);
             }
-            reglist_merge32<R>(L, cdv, civ);
 #pragma unroll
             for (int r = 0; r < R; ++r) {
                 ld[j][r * 32 + lane] = L.d[r];
