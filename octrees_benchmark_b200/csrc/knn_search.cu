@@ -729,9 +729,12 @@ __global__ void __launch_bounds__(kKnnThreads, 8) k_knn_reg(KnnTableArgs a) {
 // distance varies slowly along the curve: this holds ~1.4 k points where the
 // density estimate of k_knn_reg holds several times more, so half the
 // candidates and merges go; longer runs widen the stretch of the curve that
-// the warps work on at once, which costs L2 hits).  The first group of a run,
-// and groups handed out one at a time at the end, take k_knn_reg's density
-// estimate from the first range each query reaches.  A query that ends with fewer than k pairs
+// the warps work on at once, which costs L2 hits).  Every kKnnHeadStride-th
+// group is a head: heads are handed out first and take k_knn_reg's density
+// estimate from the first range each query reaches; the first group of a run
+// (and each group handed out alone at the end) starts from the nearest head
+// of its request that has finished, or from the density estimate when none
+// has (no group waits for a head).  A query that ends with fewer than k pairs
 // inside its provisional threshold, and every query of a group whose stack
 // overflowed, is appended to a fallback list that k_knn_reg completes exactly.
 // ---------------------------------------------------------------------------
@@ -1228,7 +1231,7 @@ cudaError_t launch_group(const KnnGroupArgs& g, int sms, cudaStream_t s, int blo
 // from the nearest head that has finished.  packet_ctr holds 3 counters (zeroed);
 // head_kth one double per head, set to NaN here.
 template <int R, int MULTI>
-cudaError_t launch_group_passes(KnnGroupArgs g, int sms, cudaStream_t s, int blocks_per_sm, double* head_kth,
+cudaError_t launch_group_seeded(KnnGroupArgs g, int sms, cudaStream_t s, int blocks_per_sm, double* head_kth,
                                 size_t head_bytes) {
     g.head_stride = (g.est > 0.0 && head_kth) ? kKnnHeadStride : 0;
     g.head_kth = head_kth;
@@ -1317,11 +1320,11 @@ cudaError_t launch_knn_group_table(int device, cudaStream_t s, const DynGroup* d
     const int sms = sm_count_k(device);
     const int bps = blocks_per_sm;
     if (single)
-        e = (kmax <= 32) ? launch_group_passes<1, 2>(g, sms, s, bps, d_head_kth, head_bytes)
-                         : launch_group_passes<2, 2>(g, sms, s, bps, d_head_kth, head_bytes);
+        e = (kmax <= 32) ? launch_group_seeded<1, 2>(g, sms, s, bps, d_head_kth, head_bytes)
+                         : launch_group_seeded<2, 2>(g, sms, s, bps, d_head_kth, head_bytes);
     else
-        e = (kmax <= 32) ? launch_group_passes<1, 1>(g, sms, s, bps, d_head_kth, head_bytes)
-                         : launch_group_passes<2, 1>(g, sms, s, bps, d_head_kth, head_bytes);
+        e = (kmax <= 32) ? launch_group_seeded<1, 1>(g, sms, s, bps, d_head_kth, head_bytes)
+                         : launch_group_seeded<2, 1>(g, sms, s, bps, d_head_kth, head_bytes);
     if (e != cudaSuccess) return e;
     // the queries handed back, exactly and without the provisional threshold
     return launch_knn_table(device, s, d_fb, single, 0, kmax, d_fb_list, bucket, d_idx, d_d2, d_counts, d_err,
@@ -1406,8 +1409,8 @@ cudaError_t launch_knn(Cloud& c, const double* d_centers, uint64_t nq, uint32_t 
         g.fb_list = reinterpret_cast<uint32_t*>(c.knn_fb.as<unsigned char>() + 16);
         const int sms = sm_count_k(c.device);
         double* heads = c.knn_heads.as<double>();
-        e = (k <= 32) ? launch_group_passes<1, 0>(g, sms, c.stream, 0, heads, head_bytes)
-                      : launch_group_passes<2, 0>(g, sms, c.stream, 0, heads, head_bytes);
+        e = (k <= 32) ? launch_group_seeded<1, 0>(g, sms, c.stream, 0, heads, head_bytes)
+                      : launch_group_seeded<2, 0>(g, sms, c.stream, 0, heads, head_bytes);
         if (e != cudaSuccess) return e;
         KnnTableArgs f{};
         f.single = r;
