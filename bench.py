@@ -64,9 +64,9 @@ BUILD_BYTES_PER_POINT = 112  # encode 32 + sort 20 + reorder 52 + leaf counting 
 BUILD_BYTES_PER_NODE = 36    # offsets 4 + ranges 8 + centers 24
 # DRAM bytes (read + write) per query of the search kernels, from ncu --set full of
 # `python -m octrees_benchmark_b200.profile_case` (6M points at this tile's density, 200k queries each):
-# k_knn_group k=50 481.4 + 136.3 MB, one-pass k_radius_packet r=2.5 336.4 + 57.3 MB
-KNN_DRAM_BYTES_PER_QUERY = (481.4e6 + 136.3e6) / 200_000
-RADIUS_DRAM_BYTES_PER_QUERY = (336.4e6 + 57.3e6) / 200_000
+# k_knn_group k=50 503.2 + 144.2 MB, one-pass k_radius_packet r=2.5 342.1 + 55.1 MB
+KNN_DRAM_BYTES_PER_QUERY = (503.2e6 + 144.2e6) / 200_000
+RADIUS_DRAM_BYTES_PER_QUERY = (342.1e6 + 55.1e6) / 200_000
 
 
 def measured_peak():
