@@ -146,21 +146,26 @@ __device__ __forceinline__ int f32_test(const LeafCtx& c, float4 p) {
 #define RQ(f) (MULTI ? reqs[cur_req].f : a.single.f)
 #define RQV(f) (MULTI == 1 ? s_view[warp].f : a.single.cv.f)
 
-// Query parameters of lane j for the transposed leaf and child tests: sphere /
-// circle (c0, c1, c2, r2, r), cube / square (bmin0..2, bmax0..2).
+// Query parameters of lane j for the transposed leaf and child tests, one
+// 48-byte row per query so that a test reads them with 16-byte loads: sphere /
+// circle (c0, c1, c2, r2, r, -), cube / square (bmin0..2, bmax0..2).
+constexpr int kQpRow = 6;
+__device__ __forceinline__ double2 ld_d2(const double* p) { return *reinterpret_cast<const double2*>(p); }
+__device__ __forceinline__ float4 ld_f4(const float* p) { return *reinterpret_cast<const float4*>(p); }
+
 template <int KT>
-__device__ __forceinline__ void put_query(double (*q)[32], int lane, const SearchKernel& k) {
+__device__ __forceinline__ void put_query(double (*q)[kQpRow], int lane, const SearchKernel& k) {
     if constexpr (KT == kSphere || KT == kCircle) {
-        q[0][lane] = k.c[0];
-        q[1][lane] = k.c[1];
-        q[2][lane] = k.c[2];
-        q[3][lane] = k.r2;
-        q[4][lane] = k.r;
+        q[lane][0] = k.c[0];
+        q[lane][1] = k.c[1];
+        q[lane][2] = k.c[2];
+        q[lane][3] = k.r2;
+        q[lane][4] = k.r;
     } else {
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
-            q[a][lane] = k.bmin[a];
-            q[3 + a][lane] = k.bmax[a];
+            q[lane][a] = k.bmin[a];
+            q[lane][3 + a] = k.bmax[a];
         }
     }
 }
@@ -169,85 +174,102 @@ __device__ __forceinline__ void put_query(double (*q)[32], int lane, const Searc
 // the leaf tests and the FP32 context read (bounds of a sphere / circle are
 // recomputed by init's own expressions, so they are the same values).
 template <int KT>
-__device__ __forceinline__ SearchKernel kernel_of(const double (*q)[32], int j) {
+__device__ __forceinline__ SearchKernel kernel_of(const double (*q)[kQpRow], int j) {
     SearchKernel k;
     if constexpr (KT == kSphere || KT == kCircle) {
-        k.c[0] = q[0][j];
-        k.c[1] = q[1][j];
-        k.c[2] = q[2][j];
-        k.r2 = q[3][j];
-        k.r = q[4][j];
+        const double2 a = ld_d2(&q[j][0]), b = ld_d2(&q[j][2]);
+        k.c[0] = a.x;
+        k.c[1] = a.y;
+        k.c[2] = b.x;
+        k.r2 = b.y;
+        k.r = q[j][4];
 #pragma unroll
-        for (int a = 0; a < 3; ++a) {
-            k.bmin[a] = dsub(k.c[a], k.r);
-            k.bmax[a] = dadd(k.c[a], k.r);
+        for (int a2 = 0; a2 < 3; ++a2) {
+            k.bmin[a2] = dsub(k.c[a2], k.r);
+            k.bmax[a2] = dadd(k.c[a2], k.r);
         }
     } else {  // cube / square tests read the bounds only
+        const double2 a = ld_d2(&q[j][0]), b = ld_d2(&q[j][2]), c = ld_d2(&q[j][4]);
         k.r = k.r2 = 0.0;
-#pragma unroll
-        for (int a = 0; a < 3; ++a) {
-            k.c[a] = 0.0;
-            k.bmin[a] = q[a][j];
-            k.bmax[a] = q[3 + a][j];
-        }
+        k.c[0] = k.c[1] = k.c[2] = 0.0;
+        k.bmin[0] = a.x;
+        k.bmin[1] = a.y;
+        k.bmin[2] = b.x;
+        k.bmax[0] = b.y;
+        k.bmax[1] = c.x;
+        k.bmax[2] = c.y;
     }
     return k;
 }
 
-// FP32 leaf context of lane j's query for the transposed FP32 test: sphere /
-// circle (qx, qy, qz, r2f, b0, b1), cube / square (lo, hi, tlo, thi per axis).
+// FP32 leaf context of lane j's query for the transposed FP32 test, one row
+// per query: sphere / circle (qx, qy, qz, r2f | b0, b1, -, -), cube / square
+// (lo0..2, hi0 | hi1, hi2, tlo0, tlo1 | tlo2, thi0..2).
 template <int KT>
-__device__ __forceinline__ void put_ctx(float (*q)[32], int lane, const LeafCtx& c) {
+__device__ __forceinline__ void put_ctx(float* row, const LeafCtx& c) {
     if constexpr (KT == kSphere || KT == kCircle) {
-        q[0][lane] = c.qx;
-        q[1][lane] = c.qy;
-        q[2][lane] = c.qz;
-        q[3][lane] = c.r2f;
-        q[4][lane] = c.b0;
-        q[5][lane] = c.b1;
+        row[0] = c.qx;
+        row[1] = c.qy;
+        row[2] = c.qz;
+        row[3] = c.r2f;
+        row[4] = c.b0;
+        row[5] = c.b1;
     } else {
 #pragma unroll
         for (int a = 0; a < 3; ++a) {
-            q[a][lane] = c.lo[a];
-            q[3 + a][lane] = c.hi[a];
-            q[6 + a][lane] = c.tlo[a];
-            q[9 + a][lane] = c.thi[a];
+            row[a] = c.lo[a];
+            row[3 + a] = c.hi[a];
+            row[6 + a] = c.tlo[a];
+            row[9 + a] = c.thi[a];
         }
     }
 }
 template <int KT>
-__device__ __forceinline__ LeafCtx get_ctx(const float (*q)[32], int j) {
+__device__ __forceinline__ LeafCtx get_ctx(const float* row) {
     LeafCtx c;
     if constexpr (KT == kSphere || KT == kCircle) {
-        c.qx = q[0][j];
-        c.qy = q[1][j];
-        c.qz = q[2][j];
-        c.r2f = q[3][j];
-        c.b0 = q[4][j];
-        c.b1 = q[5][j];
+        const float4 a = ld_f4(row);
+        const float2 b = *reinterpret_cast<const float2*>(row + 4);
+        c.qx = a.x;
+        c.qy = a.y;
+        c.qz = a.z;
+        c.r2f = a.w;
+        c.b0 = b.x;
+        c.b1 = b.y;
     } else {
-#pragma unroll
-        for (int a = 0; a < 3; ++a) {
-            c.lo[a] = q[a][j];
-            c.hi[a] = q[3 + a][j];
-            c.tlo[a] = q[6 + a][j];
-            c.thi[a] = q[9 + a][j];
-        }
+        const float4 a = ld_f4(row), b = ld_f4(row + 4), d = ld_f4(row + 8);
+        c.lo[0] = a.x;
+        c.lo[1] = a.y;
+        c.lo[2] = a.z;
+        c.hi[0] = a.w;
+        c.hi[1] = b.x;
+        c.hi[2] = b.y;
+        c.tlo[0] = b.z;
+        c.tlo[1] = b.w;
+        c.tlo[2] = d.x;
+        c.thi[0] = d.y;
+        c.thi[1] = d.z;
+        c.thi[2] = d.w;
     }
     return c;
 }
 
 // is_inside of lane j's query for point p: the same expressions, operand for operand.
 template <int KT>
-__device__ __forceinline__ bool inside_of(const double (*q)[32], int j, double px, double py, double pz) {
+__device__ __forceinline__ bool inside_of(const double (*q)[kQpRow], int j, double px, double py, double pz) {
     if constexpr (KT == kSphere) {
-        return dsq3(dsub(px, q[0][j]), dsub(py, q[1][j]), dsub(pz, q[2][j])) < q[3][j];
+        const double2 a = ld_d2(&q[j][0]), b = ld_d2(&q[j][2]);
+        return dsq3(dsub(px, a.x), dsub(py, a.y), dsub(pz, b.x)) < b.y;
     } else if constexpr (KT == kCircle) {
-        return dsq2(dsub(px, q[0][j]), dsub(py, q[1][j])) <= q[3][j];
-    } else if constexpr (KT == kCube) {
-        return px >= q[0][j] && px <= q[3][j] && py >= q[1][j] && py <= q[4][j] && pz >= q[2][j] && pz <= q[5][j];
+        const double2 a = ld_d2(&q[j][0]), b = ld_d2(&q[j][2]);
+        return dsq2(dsub(px, a.x), dsub(py, a.y)) <= b.y;
     } else {
-        return px >= q[0][j] && px <= q[3][j] && py >= q[1][j] && py <= q[4][j];
+        const double2 a = ld_d2(&q[j][0]), b = ld_d2(&q[j][2]), c = ld_d2(&q[j][4]);
+        // bmin = (a.x, a.y, b.x), bmax = (b.y, c.x, c.y)
+        if constexpr (KT == kCube)
+            return px >= a.x && px <= b.y && py >= a.y && py <= c.x && pz >= b.x && pz <= c.y;
+        else
+            return px >= a.x && px <= b.y && py >= a.y && py <= c.x;
     }
 }
 
@@ -267,8 +289,8 @@ __global__ void __launch_bounds__(kPkThreads) k_radius_packet(PacketArgs a) {
     constexpr bool kT = (ALGO != kStruct);
     static_assert(!CHUNK || (FILL && kT), "one-pass mode needs the transposed form");
     constexpr int kStage = (kT || F32) ? 1 : kPkWarps;  // FP64 point staging, per-lane FP64 form only
-    constexpr int kCtxF = (KT == kSphere || KT == kCircle) ? 6 : 12;  // floats of a query's FP32 leaf context
-    __shared__ float s_ctx[(F32 && kT) ? kPkWarps : 1][kCtxF][32];
+    constexpr int kCtxF = (KT == kSphere || KT == kCircle) ? 8 : 12;  // floats of a query's FP32 leaf context row
+    __shared__ __align__(16) float s_ctx[(F32 && kT) ? kPkWarps : 1][32][kCtxF];
     __shared__ CloudView s_view[MULTI == 1 ? kPkWarps : 1];
     __shared__ uint32_t st_node[kPkWarps][kPkStack];
     __shared__ uint32_t st_fc[kPkWarps][kPkStack];     // first child, 0 for a leaf
@@ -277,7 +299,7 @@ __global__ void __launch_bounds__(kPkThreads) k_radius_packet(PacketArgs a) {
     __shared__ uint32_t st_in[kPkWarps][kPkStack];
     __shared__ uint8_t st_depth[kPkWarps][kPkStack];
     __shared__ double s_rad[kPkWarps][kMaxDepth + 1][3];
-    __shared__ double s_qp[kPkWarps][6][32];
+    __shared__ __align__(16) double s_qp[kPkWarps][32][kQpRow];
     __shared__ double sx[kStage][32], sy[kStage][32], sz[kStage][32];
     __shared__ float4 sp[(F32 && !kT) ? kPkWarps : 1][32];
 
@@ -440,7 +462,7 @@ __global__ void __launch_bounds__(kPkThreads) k_radius_packet(PacketArgs a) {
                     if ((mask >> lane) & 1u) {
                         LeafCtx ctx;
                         leaf_ctx<KT>(kernel_of<KT>(s_qp[warp], lane), RQV(centers) + 3ull * node, ctx);
-                        put_ctx<KT>(s_ctx[warp], lane, ctx);
+                        put_ctx<KT>(s_ctx[warp][lane], ctx);
                     }
                     __syncwarp();
                 } else {
@@ -466,7 +488,7 @@ __global__ void __launch_bounds__(kPkThreads) k_radius_packet(PacketArgs a) {
                         rem &= rem - 1;
                         bool in;
                         if constexpr (F32) {
-                            const int r = in_range ? f32_test<KT>(get_ctx<KT>(s_ctx[warp], j), pf) : 0;
+                            const int r = in_range ? f32_test<KT>(get_ctx<KT>(s_ctx[warp][j]), pf) : 0;
                             if (r < 0) {  // inside the error band: the reference's FP64 expression decides
                                 in = inside_of<KT>(s_qp[warp], j, RQV(xs)[idx], RQV(ys)[idx], RQV(zs)[idx]);
                                 ++n_retests;
