@@ -747,6 +747,7 @@ constexpr int kGrpMinBlocks = 8;
 constexpr int kGrpThreads = 32 * kGrpWarps;
 constexpr int kGrpStack = 88;
 constexpr double kGrpSeed = 1.3;  // provisional threshold / previous group's largest k-th distance
+static_assert(kKnnHeadStride >= 2, "the groups between heads are numbered modulo kKnnHeadStride - 1");
 
 struct KnnGroupArgs {
     SearchReq single;                 // one request (grp == null)
