@@ -12,8 +12,9 @@
 //    same pass the 8 digit histograms of every key (so no pass re-reads keys
 //    to count).
 //  * k_onesweep: one kernel per 8-bit digit, single-pass "onesweep" radix
-//    scatter: each 4096-key tile ranks its keys stably in shared memory (warp
-//    match + per-warp counters), publishes its digit counts, resolves its
+//    scatter: each 3072-key tile ranks its keys stably in shared memory (the
+//    lanes holding the same digit found by 8 ballots, per-warp counters),
+//    publishes its digit counts, resolves its
 //    global digit offsets by decoupled look-back over the preceding tiles
 //    (bounded waits), and writes keys and 32-bit point ids out digit-grouped,
 //    which keeps the writes coalesced.  Digits equal for every key are
