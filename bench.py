@@ -559,6 +559,7 @@ def run_b200(args, rank, world, local_rank):
             torch.distributed.barrier()
         torch.cuda.synchronize()
         L.oct_search_stats(h, None, None, 1)
+        L.oct_knn_filter_stats(h, None, None, None, 1)
         t_count = t_search = t_knn = 0.0
         nbrs = 0
         for s in range(args.steps):
@@ -570,6 +571,8 @@ def run_b200(args, rank, world, local_rank):
         torch.cuda.synchronize()
         tests, retests = C.c_uint64(), C.c_uint64()
         L.oct_search_stats(h, C.byref(tests), C.byref(retests), 1)
+        k_tests, k_f64, k_band = C.c_uint64(), C.c_uint64(), C.c_uint64()
+        L.oct_knn_filter_stats(h, C.byref(k_tests), C.byref(k_f64), C.byref(k_band), 1)
         step_ms = (t_search + t_knn) / args.steps  # the count-only call is a separate measurement
         tmax = torch.tensor([step_ms, t_search / args.steps, t_knn / args.steps], dtype=torch.float64, device="cuda")
         if world > 1:
@@ -585,7 +588,11 @@ def run_b200(args, rank, world, local_rank):
                        "radius_count_only_ms": t_count / args.steps if name != "engine" else None,
                        "avg_neighbours": nbrs / args.steps / Q_RADIUS, "nbrs_per_step": nbrs / args.steps,
                        "point_tests": tests.value, "fp64_retests": retests.value,
-                       "band_hit_fraction": (retests.value / tests.value) if tests.value else None}
+                       "band_hit_fraction": (retests.value / tests.value) if tests.value else None,
+                       # the group kNN's FP32 filter: FP32 point tests, the FP64 tests they leave
+                       # (candidates + band), band hits (FP64 tests of points that then fail)
+                       "knn_fp32_tests": k_tests.value, "knn_fp64_tests": k_f64.value,
+                       "knn_band_hit_fraction": (k_band.value / k_tests.value) if k_tests.value else None}
     clk = clocks.stop()
     chosen = paths[args.search]
     configure(args.search)

@@ -155,6 +155,13 @@ int oct_set_search_config(oct_cloud cloud, const oct_search_config* config);
  * and FP64 re-tests of points inside the FP32 error band (the band-hit
  * fraction is their ratio).  Waits for the cloud's stream. */
 int oct_search_stats(oct_cloud cloud, uint64_t* point_tests, uint64_t* fp64_retests, int reset);
+/* Counters of the group kNN's FP32 filter (k <= 64, packet path, fp32_filter
+ * on) since the last reset: point tests made in FP32, those that went on to the
+ * exact FP64 distance (the candidates and the band), and band hits (FP64 tests
+ * whose point then failed the exact test: the filter's only extra work).  No
+ * reference counterpart. */
+int oct_knn_filter_stats(oct_cloud cloud, uint64_t* point_tests, uint64_t* fp64_tests, uint64_t* band_hits,
+                         int reset);
 
 /* Upload n points (xyz AoS).  Replaces filling the reference's PointsAoS
  * container (inc/geometry/point_containers.hpp:32-65). */

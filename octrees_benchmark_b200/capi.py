@@ -112,6 +112,7 @@ SIGNATURES = {
     "oct_set_radius_group": ([_vp, _int], _int),
     "oct_set_search_config": ([_vp, C.POINTER(OctSearchConfig)], _int),
     "oct_search_stats": ([_vp, C.POINTER(_u64), C.POINTER(_u64), _int], _int),
+    "oct_knn_filter_stats": ([_vp, C.POINTER(_u64), C.POINTER(_u64), C.POINTER(_u64), _int], _int),
     "oct_set_points": ([_vp, _vp, _u64, _u32], _int),
     "oct_encode_sort": ([_vp, _vp, _vp, _vp, _vp, _u32], _int),
     "oct_build": ([_vp, C.POINTER(OctTreeInfo)], _int),

@@ -298,7 +298,7 @@ int oct_cloud_destroy(oct_cloud h) {
                           &c.frontier, &c.masks, &c.parts, &c.d_build, &c.q_centers, &c.q_radii, &c.q_counts,
                           &c.q_offsets, &c.q_out, &c.q_out2, &c.q_scan_tmp, &c.qs_keys, &c.qs_keys_alt, &c.qs_ord,
                           &c.qs_ord_alt, &c.qs_status, &c.qs_ctl, &c.packet_ctr, &c.stats, &c.rel,
-                          &c.ck_pool, &c.ck_next, &c.ck_first, &c.ck_ctr, &c.knn_fb, &c.knn_heads};
+                          &c.ck_pool, &c.ck_next, &c.ck_first, &c.ck_ctr, &c.knn_fb, &c.knn_heads, &c.crel};
         for (DevBuf* b : bufs) b->release();
         if (c.pinned) cudaFreeHost(c.pinned);
         if (c.own_stream && c.stream) cudaStreamDestroy(c.stream);
@@ -359,6 +359,22 @@ int oct_set_search_config(oct_cloud h, const oct_search_config* cfg) {
     return OCT_OK;
 }
 
+int oct_knn_filter_stats(oct_cloud h, uint64_t* point_tests, uint64_t* fp64_tests, uint64_t* band_hits,
+                         int reset) {
+    if (!h) return OCT_ERR_INVALID_ARG;
+    Cloud& c = h->c;
+    DeviceGuard g(c.device);
+    CK(c.stats.reserve(64));
+    unsigned long long v[3] = {0, 0, 0};
+    CK(cudaStreamSynchronize(c.stream));
+    CK(cudaMemcpy(v, static_cast<unsigned long long*>(c.stats.ptr) + 2, sizeof(v), cudaMemcpyDeviceToHost));
+    if (point_tests) *point_tests = v[0];
+    if (fp64_tests) *fp64_tests = v[1];
+    if (band_hits) *band_hits = v[2];
+    if (reset) CK(cudaMemset(static_cast<unsigned long long*>(c.stats.ptr) + 2, 0, sizeof(v)));
+    return OCT_OK;
+}
+
 int oct_search_stats(oct_cloud h, uint64_t* point_tests, uint64_t* fp64_retests, int reset) {
     if (!h) return OCT_ERR_INVALID_ARG;
     Cloud& c = h->c;
@@ -369,7 +385,7 @@ int oct_search_stats(oct_cloud h, uint64_t* point_tests, uint64_t* fp64_retests,
     CK(cudaMemcpy(v, c.stats.ptr, sizeof(v), cudaMemcpyDeviceToHost));
     if (point_tests) *point_tests = v[0];
     if (fp64_retests) *fp64_retests = v[1];
-    if (reset) CK(cudaMemset(c.stats.ptr, 0, 64));
+    if (reset) CK(cudaMemset(c.stats.ptr, 0, sizeof(v)));
     return OCT_OK;
 }
 
@@ -381,7 +397,7 @@ int oct_cloud_memory(oct_cloud h, uint64_t* bytes) {
                             &c.frontier, &c.masks, &c.parts, &c.d_build, &c.q_centers, &c.q_radii, &c.q_counts,
                             &c.q_offsets, &c.q_out, &c.q_out2, &c.q_scan_tmp, &c.qs_keys, &c.qs_keys_alt, &c.qs_ord,
                             &c.qs_ord_alt, &c.qs_status, &c.qs_ctl, &c.packet_ctr, &c.stats, &c.rel,
-                            &c.ck_pool, &c.ck_next, &c.ck_first, &c.ck_ctr, &c.knn_fb, &c.knn_heads};
+                            &c.ck_pool, &c.ck_next, &c.ck_first, &c.ck_ctr, &c.knn_fb, &c.knn_heads, &c.crel};
     uint64_t s = 0;
     for (const DevBuf* b : bufs) s += b->bytes;
     *bytes = s;
@@ -403,6 +419,7 @@ int oct_set_points(oct_cloud h, const double* xyz, uint64_t n, uint32_t flags) {
     c.sorted = false;
     c.built = false;
     c.rel_built = false;
+    c.crel_built = false;
     c.node_capacity = 0;
     if (!(flags & OCT_MEM_DEVICE)) CK(cudaStreamSynchronize(c.stream));
     return OCT_OK;
@@ -471,6 +488,7 @@ int oct_build(oct_cloud h, oct_tree_info* info) {
         c.max_depth_seen = bc.max_depth_seen;
         CK(cudaMemsetAsync(c.offsets.as<uint32_t>() + c.n_total, 0, 4, c.stream));
         c.rel_built = false;
+        c.crel_built = false;
         if (c.fp32_filter && c.packet) {  // the FP32 search reads leaf-relative coordinates
             CK(launch_leaf_rel(c));
             c.rel_built = true;
@@ -619,6 +637,7 @@ int oct_tree_import(oct_cloud h, const oct_tree_info* info, const double* box12,
     c.sorted = true;
     c.built = true;
     c.rel_built = false;
+    c.crel_built = false;
     if (c.fp32_filter && c.packet) {  // the FP32 search reads leaf-relative coordinates
         CK(launch_leaf_rel(c));
         c.rel_built = true;

@@ -64,6 +64,7 @@ struct CloudView {
     const double* ys;
     const double* zs;
     const float4* rel;          // FP32 leaf-relative points (packet FP32 path), may be null
+    const float4* crel;         // FP32 points relative to the box centre (group kNN FP32 path), may be null
     const uint32_t* offsets;
     const uint2* ranges;
     const double* centers;
@@ -163,6 +164,8 @@ struct Cloud {
     // FP32 leaf-relative coordinates (x, y, z, 0) per sorted point, built on demand
     DevBuf rel;
     bool rel_built = false;
+    DevBuf crel;  // FP32 (x, y, z) - box centre per point, for the group kNN's FP32 filter
+    bool crel_built = false;
     // search configuration (oct_set_search_config)
     int packet = 1;
     int fp32_filter = 0;
@@ -195,6 +198,8 @@ cudaError_t launch_radius(Cloud& c, int kernel, int algo, int group, bool fill, 
 cudaError_t launch_scan_u64(Cloud& c, const unsigned long long* d_in, unsigned long long* d_out, uint64_t n);
 cudaError_t launch_query_order(Cloud& c, const double* d_centers, uint64_t nq, const uint32_t** d_order);
 cudaError_t launch_leaf_rel(Cloud& c);
+// FP32 coordinates relative to the box centre (group kNN FP32 filter), into c.crel.
+cudaError_t launch_center_rel(Cloud& c);
 struct ChunkArgs;
 // mode as launch_radius_table (0 count, 1 fill, 2 one pass into `chunks`)
 cudaError_t launch_radius_packet(Cloud& c, int kernel, int algo, int mode, bool fp32, const double* d_centers,
@@ -244,7 +249,8 @@ cudaError_t launch_knn_group_table(int device, cudaStream_t s, const DynGroup* d
                                    const SearchReq* single, uint32_t kmax, const uint32_t* d_order, uint32_t bucket,
                                    uint32_t* d_idx, double* d_d2, uint32_t* d_counts, uint32_t* d_err,
                                    uint32_t* d_packet_ctr, uint32_t* d_fb_list, double est, uint32_t chunk,
-                                   int blocks_per_sm, double* d_head_kth, size_t head_bytes);
+                                   int blocks_per_sm, double* d_head_kth, size_t head_bytes, bool fp32,
+                                   unsigned long long* d_stats);
 CloudView cloud_view(const Cloud& c);
 // Batched engine: the sort of query keys with device-side sizes (encode_sort.cu),
 // and the shared-memory limits of the table kNN list kernels (knn_search.cu).

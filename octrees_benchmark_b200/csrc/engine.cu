@@ -392,7 +392,7 @@ cudaError_t enqueue_work(oct_engine e) {
                                             e->knn_d2.as<double>(), e->knn_counts.as<uint32_t>(), err,
                                             ctr + 2 * kRadiusVariants + 4 * v, e->knn_fb.as<uint32_t>(),
                                             kKnnEstimate, kKnnGroupChunk, e->knn_bps, e->knn_heads.as<double>(),
-                                            e->knn_heads.bytes);
+                                            e->knn_heads.bytes, e->fp32 != 0, stats + 2);
             else
                 r2 = launch_knn_table(e->device, ks, &dyn->groups[kRadiusVariants + v], one, 0, 32u << v,
                                       order, e->bucket, e->knn_idx.as<uint32_t>(), e->knn_d2.as<double>(),
@@ -575,17 +575,18 @@ int submit(oct_engine e, const oct_request* rq, uint32_t n) {
     std::stable_sort(rows.begin(), rows.end(), [&](uint32_t a, uint32_t b) { return var[a] < var[b]; });
     const uint32_t m = (uint32_t)rows.size();
     if (m > (1u << 16)) return fail(e, OCT_ERR_INVALID_ARG, "more than 65536 non-empty requests in one batch");
-    // FP32 filter: the leaf-relative copies of the clouds it reads
+    // FP32 filter: the leaf-relative copies of the clouds the radius requests read,
+    // the centre-relative copies of those the group kNN (k <= 64) reads
     if (e->fp32) {
         for (uint32_t i : rows) {
-            if (rq[i].type != OCT_REQ_RADIUS) continue;
             Cloud& c = rq[i].cloud->c;
-            if (!c.rel_built) {
-                DeviceGuardE gc(c.device);
-                EK(launch_leaf_rel(c));
-                EK(cudaStreamSynchronize(c.stream));
-                c.rel_built = true;
-            }
+            const bool radius = rq[i].type == OCT_REQ_RADIUS;
+            if (radius ? c.rel_built : (c.crel_built || !e->knn_group || rq[i].k > 64)) continue;
+            DeviceGuardE gc(c.device);
+            if (radius) EK(launch_leaf_rel(c));
+            else EK(launch_center_rel(c));
+            EK(cudaStreamSynchronize(c.stream));
+            (radius ? c.rel_built : c.crel_built) = true;
         }
     }
     // sizes, then capacities (growing drops graphs), then the packed table

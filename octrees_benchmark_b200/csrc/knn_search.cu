@@ -767,12 +767,33 @@ struct KnnGroupArgs {
     uint32_t chunk;                   // consecutive groups per fetch (>= 1)
     uint32_t head_stride;             // S > 1: every S-th group is a head, taken first (0: no heads)
     double* head_kth;                 // per head: the largest k-th distance it found (NaN: not yet, < 0: none)
+    unsigned long long* stats;        // FP32 filter: point tests, FP64 tests, band hits (may be null)
     uint32_t* fb_list;                // queries left to k_knn_reg (global positions; a batch group's
                                       // entries start at its q_begin)
     unsigned long long* fb_count;
 };
 
-template <int R, int MULTI>
+// FP32 filter of the group kNN: a point whose FP32 squared distance D_f to
+// the query exceeds the returned value has an exact squared distance above
+// thr.  Per axis a = p - centre (|a| <= A, the box radius) and b = q - centre
+// (|b| <= B) are each rounded once to FP32 from their FP64 differences, and
+// delta_f = fl32(a_f - b_f); with u = 2^-24, |delta_f - delta| <= 1.0002 u
+// (A + B + |delta|).  For D <= thr (|delta| <= s = sqrt thr, M = A + B + s):
+// |sum delta_f^2 - D| <= 2 * 1.0002 u M sqrt(3) s + 3.0012 u^2 M^2, and the
+// FP32 product and two fused adds add at most 3.0001 u sum delta_f^2 <=
+// 3.0001 u (s + 1.733 u M)^2.  The threshold is thr plus twice that bound,
+// rounded up to FP32.  ab = A + B.
+__device__ __forceinline__ float knn_f32_threshold(double thr, double ab) {
+    if (!(thr < (double)INFINITY)) return INFINITY;
+    const double u = 5.9604644775390625e-08;  // 2^-24
+    const double sr = sqrt(thr) * (1.0 + 1.0e-12);
+    const double M = ab + sr;
+    const double t = sr + 1.74 * u * M;
+    const double err = 3.47 * u * M * sr + 3.01 * u * u * M * M + 3.01 * u * t * t;
+    return __double2float_ru(thr + 2.0 * err);
+}
+
+template <int R, int MULTI, bool F32>
 __global__ void __launch_bounds__(kGrpThreads, kGrpMinBlocks) k_knn_group(KnnGroupArgs a) {
     constexpr int G = kGrpQ;
     constexpr int LC = 32 * R;
@@ -786,6 +807,11 @@ __global__ void __launch_bounds__(kGrpThreads, kGrpMinBlocks) k_knn_group(KnnGro
     __shared__ uint32_t s_nl[kGrpWarps][G];
     __shared__ uint32_t s_nb[kGrpWarps][G];
     __shared__ uint32_t s_qg[kGrpWarps][G];
+    // FP32 filter: query - box centre in FP32 with the query's FP32 threshold in w,
+    // and the query's A + B (box radius + |query - centre|_inf) for new thresholds
+    __shared__ float4 s_qf[F32 ? kGrpWarps : 1][G];
+    __shared__ double s_qab[F32 ? kGrpWarps : 1][G];
+    unsigned long long f_tests = 0, f_64 = 0, f_band = 0;
     __shared__ uint32_t st_a[kGrpWarps][kGrpStack];
     __shared__ uint32_t st_b[kGrpWarps][kGrpStack];
     __shared__ __half st_lb[kGrpWarps][kGrpStack][G];  // per-query bounds, rounded down to FP16
@@ -936,6 +962,17 @@ __global__ void __launch_bounds__(kGrpThreads, kGrpMinBlocks) k_knn_group(KnnGro
             nls[lane] = 0;
             nbs[lane] = 0;
             s_qg[warp][lane] = (uint32_t)q;
+            if constexpr (F32) {
+                const BoxD* bx = KRQV(box);
+                const double bqx = dsub(qc[3 * ql], bx->center[0]);
+                const double bqy = dsub(qc[3 * ql + 1], bx->center[1]);
+                const double bqz = dsub(qc[3 * ql + 2], bx->center[2]);
+                const double A = smax(smax(bx->radii[0], bx->radii[1]), bx->radii[2]);
+                const double B = smax(smax(fabs(bqx), fabs(bqy)), fabs(bqz));
+                const double ab = (A + B) * (1.0 + 1.0e-12);
+                s_qab[warp][lane] = ab;
+                s_qf[warp][lane] = make_float4((float)bqx, (float)bqy, (float)bqz, knn_f32_threshold(thr[lane], ab));
+            }
         }
         for (int t = lane; t < G * LC; t += 32) {
             (&ld[0][0])[t] = INFINITY;
@@ -986,6 +1023,7 @@ __global__ void __launch_bounds__(kGrpThreads, kGrpMinBlocks) k_knn_group(KnnGro
                 if (nl == K) {
                     thr[j] = td;
                     thri[j] = ti;
+                    if constexpr (F32) s_qf[warp][j].w = knn_f32_threshold(td, s_qab[warp][j]);
                 }
             }
             __syncwarp();
@@ -1024,6 +1062,7 @@ __global__ void __launch_bounds__(kGrpThreads, kGrpMinBlocks) k_knn_group(KnnGro
                         if (lane < G && ((pend >> lane) & 1u)) {
                             thr[lane] = a.est * (double)K * area / (3.14159265358979323846 * (double)(eb - ea));
                             thri[lane] = 0xffffffffu;  // with the pair order this accepts d <= thr
+                            if constexpr (F32) s_qf[warp][lane].w = knn_f32_threshold(thr[lane], s_qab[warp][lane]);
                         }
                         est_used |= pend;
                     }
@@ -1034,17 +1073,44 @@ __global__ void __launch_bounds__(kGrpThreads, kGrpMinBlocks) k_knn_group(KnnGro
                     const uint32_t i = b + lane;
                     const bool in = i < eb;
                     double px = 0.0, py = 0.0, pz = 0.0;
+                    float4 pf = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+                    bool have64 = !F32;  // the FP32 form reads FP64 coordinates only for points near a threshold
                     if (in) {
-                        px = KRQV(xs)[i];
-                        py = KRQV(ys)[i];
-                        pz = KRQV(zs)[i];
+                        if constexpr (F32) {
+                            pf = KRQV(crel)[i];
+                        } else {
+                            px = KRQV(xs)[i];
+                            py = KRQV(ys)[i];
+                            pz = KRQV(zs)[i];
+                        }
                     }
+                    if (F32 && lane == 0) f_tests += (unsigned long long)__popc(m) * ((eb - b < 32u) ? (eb - b) : 32u);
                     uint32_t rem = m;
                     while (rem) {
                         const int j = __ffs(rem) - 1;
                         rem &= rem - 1;
-                        const double d = dist_pp(qs[j][0], qs[j][1], qs[j][2], px, py, pz);
-                        bool cand = in && pair_less(d, i, thr[j], thri[j]);
+                        double d = (double)INFINITY;
+                        bool cand = false;
+                        if constexpr (F32) {
+                            const float4 q4 = s_qf[warp][j];
+                            const float dx = pf.x - q4.x, dy = pf.y - q4.y, dz = pf.z - q4.z;
+                            const float df = __fmaf_rn(dz, dz, __fmaf_rn(dy, dy, __fmul_rn(dx, dx)));
+                            if (in && !(df > q4.w)) {  // near the threshold or inside: the exact FP64 test
+                                if (!have64) {
+                                    px = KRQV(xs)[i];
+                                    py = KRQV(ys)[i];
+                                    pz = KRQV(zs)[i];
+                                    have64 = true;
+                                }
+                                d = dist_pp(qs[j][0], qs[j][1], qs[j][2], px, py, pz);
+                                cand = pair_less(d, i, thr[j], thri[j]);
+                                ++f_64;
+                                f_band += cand ? 0u : 1u;
+                            }
+                        } else {
+                            d = dist_pp(qs[j][0], qs[j][1], qs[j][2], px, py, pz);
+                            cand = in && pair_less(d, i, thr[j], thri[j]);
+                        }
                         uint32_t hb = __ballot_sync(0xffffffffu, cand);
                         if (!hb) continue;
                         uint32_t nb = nbs[j];
@@ -1199,15 +1265,30 @@ __global__ void __launch_bounds__(kGrpThreads, kGrpMinBlocks) k_knn_group(KnnGro
         if (head && lane == 0) __stcg(&a.head_kth[slot], mx);
         __syncwarp();
     }
+    if constexpr (F32) {
+        if (a.stats) {
+#pragma unroll
+            for (int off = 16; off > 0; off >>= 1) {
+                f_64 += __shfl_xor_sync(0xffffffffu, f_64, off);
+                f_band += __shfl_xor_sync(0xffffffffu, f_band, off);
+            }
+            if (lane == 0) {
+                atomicAdd(&a.stats[0], f_tests);
+                atomicAdd(&a.stats[1], f_64);
+                atomicAdd(&a.stats[2], f_band);
+            }
+        }
+    }
 }
 
 // Blocks per SM of a group-kNN instantiation (its shared memory sets it).
-template <int R, int MULTI>
+template <int R, int MULTI, bool F32>
 int group_blocks_per_sm() {
     static int per = 0;
     if (per == 0) {
         int v = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, k_knn_group<R, MULTI>, kGrpThreads, 0) != cudaSuccess)
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&v, k_knn_group<R, MULTI, F32>, kGrpThreads, 0) !=
+            cudaSuccess)
             v = 1;
         per = v > 0 ? v : 1;
     }
@@ -1215,9 +1296,9 @@ int group_blocks_per_sm() {
 }
 
 // blocks_per_sm > 0 caps the resident blocks (room for a kernel running beside it).
-template <int R, int MULTI>
+template <int R, int MULTI, bool F32>
 cudaError_t launch_group(const KnnGroupArgs& g, int sms, cudaStream_t s, int blocks_per_sm = 0) {
-    int per = group_blocks_per_sm<R, MULTI>();
+    int per = group_blocks_per_sm<R, MULTI, F32>();
     if (blocks_per_sm > 0 && blocks_per_sm < per) per = blocks_per_sm;
     uint64_t grid = (uint64_t)sms * per;
     if (!g.grp) {
@@ -1225,7 +1306,7 @@ cudaError_t launch_group(const KnnGroupArgs& g, int sms, cudaStream_t s, int blo
         if (want < grid) grid = want;
     }
     if (grid == 0) return cudaSuccess;
-    k_knn_group<R, MULTI><<<(int)grid, kGrpThreads, 0, s>>>(g);
+    k_knn_group<R, MULTI, F32><<<(int)grid, kGrpThreads, 0, s>>>(g);
     return cudaGetLastError();
 }
 
@@ -1233,17 +1314,19 @@ cudaError_t launch_group(const KnnGroupArgs& g, int sms, cudaStream_t s, int blo
 // is a head: the heads go out first and start from the density estimate; every
 // other group starts from its run's previous group or, when it leads its run,
 // from the nearest head that has finished.  packet_ctr holds 3 counters (zeroed);
-// head_kth one double per head, set to NaN here.
+// head_kth one double per head, set to NaN here.  fp32: the FP32-filter form
+// (every cloud of the launch has its centre-relative FP32 copy).
 template <int R, int MULTI>
 cudaError_t launch_group_seeded(KnnGroupArgs g, int sms, cudaStream_t s, int blocks_per_sm, double* head_kth,
-                                size_t head_bytes) {
+                                size_t head_bytes, bool fp32) {
     g.head_stride = (g.est > 0.0 && head_kth) ? kKnnHeadStride : 0;
     g.head_kth = head_kth;
     if (g.head_stride) {
         const cudaError_t e = cudaMemsetAsync(head_kth, 0xff, head_bytes, s);
         if (e != cudaSuccess) return e;
     }
-    return launch_group<R, MULTI>(g, sms, s, blocks_per_sm);
+    if (fp32) return launch_group<R, MULTI, true>(g, sms, s, blocks_per_sm);
+    return launch_group<R, MULTI, false>(g, sms, s, blocks_per_sm);
 }
 
 int sm_count_k(int device) {
@@ -1303,7 +1386,8 @@ cudaError_t launch_knn_group_table(int device, cudaStream_t s, const DynGroup* d
                                    const SearchReq* single, uint32_t kmax, const uint32_t* d_order, uint32_t bucket,
                                    uint32_t* d_idx, double* d_d2, uint32_t* d_counts, uint32_t* d_err,
                                    uint32_t* d_packet_ctr, uint32_t* d_fb_list, double est, uint32_t chunk,
-                                   int blocks_per_sm, double* d_head_kth, size_t head_bytes) {
+                                   int blocks_per_sm, double* d_head_kth, size_t head_bytes, bool fp32,
+                                   unsigned long long* d_stats) {
     if (kmax > 64) return cudaErrorInvalidValue;
     cudaError_t e;
     if ((e = cudaMemsetAsync(d_packet_ctr, 0, 12, s)) != cudaSuccess) return e;
@@ -1320,15 +1404,16 @@ cudaError_t launch_knn_group_table(int device, cudaStream_t s, const DynGroup* d
     g.packet_ctr = d_packet_ctr;
     g.chunk = chunk > 0 ? chunk : 1;
     g.fb_list = d_fb_list;
+    g.stats = d_stats;
     g.fb_count = reinterpret_cast<unsigned long long*>(&d_fb->nq);
     const int sms = sm_count_k(device);
     const int bps = blocks_per_sm;
     if (single)
-        e = (kmax <= 32) ? launch_group_seeded<1, 2>(g, sms, s, bps, d_head_kth, head_bytes)
-                         : launch_group_seeded<2, 2>(g, sms, s, bps, d_head_kth, head_bytes);
+        e = (kmax <= 32) ? launch_group_seeded<1, 2>(g, sms, s, bps, d_head_kth, head_bytes, fp32)
+                         : launch_group_seeded<2, 2>(g, sms, s, bps, d_head_kth, head_bytes, fp32);
     else
-        e = (kmax <= 32) ? launch_group_seeded<1, 1>(g, sms, s, bps, d_head_kth, head_bytes)
-                         : launch_group_seeded<2, 1>(g, sms, s, bps, d_head_kth, head_bytes);
+        e = (kmax <= 32) ? launch_group_seeded<1, 1>(g, sms, s, bps, d_head_kth, head_bytes, fp32)
+                         : launch_group_seeded<2, 1>(g, sms, s, bps, d_head_kth, head_bytes, fp32);
     if (e != cudaSuccess) return e;
     // the queries handed back, exactly and without the provisional threshold
     return launch_knn_table(device, s, d_fb, single, 0, kmax, d_fb_list, bucket, d_idx, d_d2, d_counts, d_err,
@@ -1378,6 +1463,13 @@ cudaError_t launch_knn(Cloud& c, const double* d_centers, uint64_t nq, uint32_t 
     const uint64_t cap = (uint64_t)sm_count_k(c.device) * 16;
     const int grid = (int)(want < cap ? want : cap);
     if (c.packet && k <= 64) {
+        // the FP32 filter (group kernel): centre-relative FP32 points, built on first use
+        const bool f32 = c.fp32_filter != 0 && c.knn_packet != 0;
+        if (f32 && !c.crel_built) {
+            cudaError_t e;
+            if ((e = launch_center_rel(c)) != cudaSuccess) return e;
+            c.crel_built = true;
+        }
         SearchReq r{};
         r.cv = cloud_view(c);
         r.centers = d_centers;
@@ -1411,10 +1503,11 @@ cudaError_t launch_knn(Cloud& c, const double* d_centers, uint64_t nq, uint32_t 
         g.chunk = c.knn_chunk;
         g.fb_count = c.knn_fb.as<unsigned long long>();
         g.fb_list = reinterpret_cast<uint32_t*>(c.knn_fb.as<unsigned char>() + 16);
+        g.stats = f32 ? c.stats.as<unsigned long long>() + 2 : nullptr;  // oct_knn_filter_stats
         const int sms = sm_count_k(c.device);
         double* heads = c.knn_heads.as<double>();
-        e = (k <= 32) ? launch_group_seeded<1, 0>(g, sms, c.stream, 0, heads, head_bytes)
-                      : launch_group_seeded<2, 0>(g, sms, c.stream, 0, heads, head_bytes);
+        e = (k <= 32) ? launch_group_seeded<1, 0>(g, sms, c.stream, 0, heads, head_bytes, f32)
+                      : launch_group_seeded<2, 0>(g, sms, c.stream, 0, heads, head_bytes, f32);
         if (e != cudaSuccess) return e;
         KnnTableArgs f{};
         f.single = r;

@@ -864,6 +864,27 @@ __global__ void __launch_bounds__(256) k_chunk_compact(const unsigned long long*
 
 }  // namespace
 
+// FP32 (x, y, z) of every point relative to the box centre, each rounded once
+// from the FP64 difference; w = 0.
+__global__ void k_center_rel(const double* __restrict__ xs, const double* __restrict__ ys,
+                             const double* __restrict__ zs, const BoxD* __restrict__ box, uint64_t n,
+                             float4* __restrict__ out) {
+    const double cx = box->center[0], cy = box->center[1], cz = box->center[2];
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        out[i] = make_float4((float)dsub(xs[i], cx), (float)dsub(ys[i], cy), (float)dsub(zs[i], cz), 0.0f);
+}
+
+cudaError_t launch_center_rel(Cloud& c) {
+    cudaError_t e;
+    if ((e = c.crel.reserve(16 * (c.n ? c.n : 1))) != cudaSuccess) return e;
+    if (c.n == 0) return cudaSuccess;
+    const uint64_t want = (c.n + 255) / 256;
+    const unsigned grid = (unsigned)(want < 148ull * 16 ? want : 148ull * 16);
+    k_center_rel<<<grid, 256, 0, c.stream>>>(c.xs.as<double>(), c.ys.as<double>(), c.zs.as<double>(),
+                                             c.d_box.as<BoxD>(), c.n, c.crel.as<float4>());
+    return cudaGetLastError();
+}
+
 cudaError_t launch_leaf_rel(Cloud& c) {
     cudaError_t e;
     if ((e = c.rel.reserve(16 * (c.n ? c.n : 1))) != cudaSuccess) return e;
@@ -881,6 +902,7 @@ CloudView cloud_view(const Cloud& c) {
     v.ys = c.ys.as<double>();
     v.zs = c.zs.as<double>();
     v.rel = c.rel.as<float4>();
+    v.crel = c.crel_built ? c.crel.as<float4>() : nullptr;
     v.offsets = c.offsets.as<uint32_t>();
     v.ranges = c.ranges.as<uint2>();
     v.centers = c.centers.as<double>();

@@ -22,6 +22,7 @@ ALGO_NAMES = {1: "neighbors", 2: "neighborsPrune", 3: "neighborsStruct"}
 PATHS = {"lanes8": (False, False, 8, False, 256), "lanes16": (False, False, 16, False, 256),
          "lanes32": (False, False, 32, False, 256), "packet": (True, False, 8, False, 256),
          "packet_fp32": (True, True, 8, False, 256), "knn_packet": (True, False, 8, True, 256),
+         "knn_packet_fp32": (True, True, 8, True, 256),
          "knn_leaves": (True, False, 8, False, 0), "knn_bucket2k": (True, False, 8, False, 2048)}
 
 
@@ -210,7 +211,8 @@ def test_gpu_approx_matches_oracle(synth_cases, case, search):
 
 
 @pytest.mark.parametrize("case", range(len(SYNTH)))
-@pytest.mark.parametrize("search", ["lanes8", "packet", "knn_packet", "knn_leaves", "knn_bucket2k"])
+@pytest.mark.parametrize("search", ["lanes8", "packet", "knn_packet", "knn_packet_fp32", "knn_leaves",
+                                    "knn_bucket2k"])
 def test_gpu_knn_matches_oracle(synth_cases, case, search):
     xyz, enc, leaf, keys, perm, box, sxyz, t = synth_cases[case]
     oc = octree(xyz, enc, leaf, search)
