@@ -118,10 +118,13 @@ int oct_set_radius_group(oct_cloud cloud, int lanes);
  *  packet       1 (default): the query centres are ordered along the cloud's
  *               curve and each warp walks the tree once for 32 neighbouring
  *               queries; 0: one query per group of radius_lanes lanes.
- *  fp32_filter  1: leaf points are tested in FP32 relative to their leaf's
- *               centre and only points within a rigorous error band of the
- *               boundary are re-tested in FP64 (packet path); 0 (default):
- *               every test in FP64.
+ *  fp32_filter  1: radius searches test leaf points in FP32 relative to
+ *               their leaf's centre and re-test in FP64 only points within a
+ *               rigorous error band of the boundary (packet path); the group
+ *               kNN (knn_packet, k <= 64) tests points in FP32 relative to the
+ *               box centre and computes the exact FP64 distance only for points
+ *               within a rigorous band of the query's k-th distance or inside
+ *               it; 0 (default): every test in FP64.  Results are the same.
  *  radius_lanes lanes per query when packet is 0: 8 (default), 16 or 32.
  *  knn_packet   1 (default): kNN with k <= 64 on the packet path walks the
  *               tree once per group of 4 curve-ordered queries per warp
