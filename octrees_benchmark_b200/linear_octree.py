@@ -144,7 +144,8 @@ class LinearOctree:
                           knn_packet: bool = True, knn_bucket: int = 256, two_pass: bool = False,
                           knn_estimate: int = 0, knn_group_run: int = 0):
         """Search path: packet (32 curve-ordered queries per warp) or one query per
-        ``radius_lanes`` lanes; FP32 leaf-relative filter with FP64 re-tests; kNN in groups
+        ``radius_lanes`` lanes; FP32 filter with FP64 re-tests (radius: leaf-relative points;
+        group kNN: points relative to the box centre, FP64 only near the k-th distance); kNN in groups
         of 4 queries per warp (``knn_packet``; else one warp per query); ``two_pass`` counts
         then fills instead of the one-pass packet radius search."""
         cfg = OctSearchConfig(int(bool(packet)), int(bool(fp32_filter)), int(radius_lanes), int(bool(knn_packet)),
@@ -159,6 +160,12 @@ class LinearOctree:
         a, b = C.c_uint64(), C.c_uint64()
         check(self._L.oct_search_stats(self._h, C.byref(a), C.byref(b), int(reset)), self._h)
         return a.value, b.value
+
+    def knn_filter_stats(self, reset: bool = False):
+        """(FP32 point tests, FP64 tests, band hits) of the group kNN's FP32 filter since the last reset."""
+        a, b, c = C.c_uint64(), C.c_uint64(), C.c_uint64()
+        check(self._L.oct_knn_filter_stats(self._h, C.byref(a), C.byref(b), C.byref(c), int(reset)), self._h)
+        return a.value, b.value, c.value
 
     # ---- sortPoints outputs ------------------------------------------------
     def sorted_points(self):
