@@ -734,7 +734,9 @@ __global__ void __launch_bounds__(kKnnThreads, 8) k_knn_reg(KnnTableArgs a) {
 // estimate from the first range each query reaches; the first group of a run
 // (and each group handed out alone at the end) starts from the nearest head
 // of its request that has finished, or from the density estimate when none
-// has (no group waits for a head).  A query that ends with fewer than k pairs
+// has (no group waits for a head).  F32: range points are first tested in FP32
+// (centre-relative copies) against a per-query FP32 bound of the threshold
+// (knn_f32_threshold); only points not rejected take the FP64 distance.  A query that ends with fewer than k pairs
 // inside its provisional threshold, and every query of a group whose stack
 // overflowed, is appended to a fallback list that k_knn_reg completes exactly.
 // ---------------------------------------------------------------------------
