@@ -583,10 +583,15 @@ int submit(oct_engine e, const oct_request* rq, uint32_t n) {
             const bool radius = rq[i].type == OCT_REQ_RADIUS;
             if (radius ? c.rel_built : (c.crel_built || !e->knn_group || rq[i].k > 64)) continue;
             DeviceGuardE gc(c.device);
-            if (radius) EK(launch_leaf_rel(c));
-            else EK(launch_center_rel(c));
-            EK(cudaStreamSynchronize(c.stream));
-            (radius ? c.rel_built : c.crel_built) = true;
+            if (radius) {
+                EK(launch_leaf_rel(c));
+                EK(cudaStreamSynchronize(c.stream));
+                c.rel_built = true;
+            } else {
+                EK(launch_center_rel(c));
+                EK(cudaStreamSynchronize(c.stream));
+                c.crel_built = true;
+            }
         }
     }
     // sizes, then capacities (growing drops graphs), then the packed table
