@@ -34,7 +34,9 @@ import statistics
 import subprocess
 import sys
 import tempfile
+import threading
 import time
+import traceback
 
 import numpy as np
 
@@ -160,6 +162,12 @@ def cpu_arm(xyz, threads: int, target_s: float = 10.0):
             tr, _ = R.time_radius(1, 2, qr, RADIUS, threads)
             tk, _ = R.time_knn(qk, KNN_K, threads)
             return tr, tk
+
+        def ref_radius(qr, kernel=1, algo=2, r=RADIUS):
+            return R.radius(kernel, algo, qr, r, threads)
+
+        def ref_knn(qk, k=KNN_K):
+            return R.knn(qk, k, threads)
     else:
         P = orc.Port()
         keys, perm, box, sxyz = P.encode_sort(ENCODER, xyz)
@@ -173,6 +181,12 @@ def cpu_arm(xyz, threads: int, target_s: float = 10.0):
             t1 = time.perf_counter()
             T.knn(sxyz, qk, KNN_K)
             return t1 - t0, time.perf_counter() - t1
+
+        def ref_radius(qr, kernel=1, algo=2, r=RADIUS):
+            return T.radius(sxyz, kernel, algo, qr, r)
+
+        def ref_knn(qk, k=KNN_K):
+            return T.knn(sxyz, qk, k)
     # calibrate the sample so that one run is about target_s / 2 of CPU work
     cal = 4000
     q = sxyz[query_indices(2 * cal, len(sxyz), seed=99)]
@@ -180,7 +194,102 @@ def cpu_arm(xyz, threads: int, target_s: float = 10.0):
     per_q = (tr + tk) / (2 * cal)
     m = int(max(cal, min(Q_RADIUS, target_s / 2 / max(per_q, 1e-9) / 2)))
     sample = sxyz[query_indices(2 * m, len(sxyz), seed=98)]
-    return dict(kind=kind, cores=int(cores), sample_per_kind=m, run=run, sample=sample)
+    return dict(kind=kind, cores=int(cores), sample_per_kind=m, run=run, sample=sample, sorted_xyz=sxyz,
+                ref_radius=ref_radius, ref_knn=ref_knn)
+
+
+PARITY_QUERIES = 20_000  # per kind: radius and kNN centres of the CPU sample checked on every GPU path
+
+
+def cpu_leg(args, xyz_h, h, eng, proxy, eng_cfg):
+    """The reference CPU path timed on a bounded sample of the step's query mix (all host threads), then the
+    first PARITY_QUERIES radius and kNN centres of that sample answered by every GPU search path and compared
+    with the reference's answers: neighbour sets (sorted), kNN squared distances (bitwise) and indices (ties at
+    the k-th distance by lowest index)."""
+    import torch
+
+    from octrees_benchmark_b200 import capi
+    from octrees_benchmark_b200.engine import Request
+    from tests.parity import csr_set_diffs, knn_diffs
+
+    L = capi.lib()
+    MD = capi.OCT_MEM_DEVICE
+    arm = cpu_arm(xyz_h, threads=0, target_s=args.cpu_seconds)
+    m = arm["sample_per_kind"]
+    tr, tk = arm["run"](arm["sample"][:m], arm["sample"][m:])
+    cpu = {"value": 2 * m / (tr + tk), "unit": "queries/s", "cores": arm["cores"], "kind": arm["kind"],
+           "sample": f"{m} radius (sphere, neighborsPrune, r={RADIUS}) + {m} kNN (k={KNN_K}) queries at random "
+                     f"points of the same {N_POINTS:,}-point cloud, all host threads",
+           "radius_qps": m / tr, "knn_qps": m / tk}
+    p = min(m, PARITY_QUERIES)
+    qr_h = np.ascontiguousarray(arm["sample"][:p])
+    qk_h = np.ascontiguousarray(arm["sample"][m:m + p])
+    t0 = time.perf_counter()
+    ro, ri = arm["ref_radius"](qr_h)
+    ki, kd, kc = arm["ref_knn"](qk_h)
+    ref_s = time.perf_counter() - t0
+    sxyz = arm["sorted_xyz"]
+    qr, qk = torch.from_numpy(qr_h).cuda(), torch.from_numpy(qk_h).cuda()
+    torch.cuda.synchronize()
+
+    def single(packet, fp32, lanes, knn_group):
+        cfg = capi.OctSearchConfig(packet, fp32, lanes, knn_group, args.knn_bucket)
+        capi.check(L.oct_set_search_config(h, C.byref(cfg)), h, "search config")
+        L.oct_search_stats(h, None, None, 1)
+        L.oct_knn_filter_stats(h, None, None, None, 1)
+        offs = torch.zeros(p + 1, dtype=torch.int64, device="cuda")
+        tot = C.c_uint64()
+        st = L.oct_radius_search(h, 1, 2, qr.data_ptr(), p, None, RADIUS, offs.data_ptr(), None, 0, C.byref(tot), MD)
+        assert st in (capi.OCT_OK, capi.OCT_ERR_CAPACITY)
+        out = torch.empty(max(1, tot.value), dtype=torch.int32, device="cuda")
+        capi.check(L.oct_radius_search(h, 1, 2, qr.data_ptr(), p, None, RADIUS, offs.data_ptr(), out.data_ptr(),
+                                       tot.value, C.byref(tot), MD), h, "parity radius")
+        kidx = torch.empty((p, KNN_K), dtype=torch.int32, device="cuda")
+        kd2 = torch.empty((p, KNN_K), dtype=torch.float64, device="cuda")
+        kcnt = torch.empty(p, dtype=torch.int32, device="cuda")
+        capi.check(L.oct_knn(h, qk.data_ptr(), p, KNN_K, kidx.data_ptr(), kd2.data_ptr(), kcnt.data_ptr(), MD), h,
+                   "parity kNN")
+        capi.check(L.oct_synchronize(h), h)
+        tests, retests = C.c_uint64(), C.c_uint64()
+        L.oct_search_stats(h, C.byref(tests), C.byref(retests), 1)
+        k_tests, k_f64, k_band = C.c_uint64(), C.c_uint64(), C.c_uint64()
+        L.oct_knn_filter_stats(h, C.byref(k_tests), C.byref(k_f64), C.byref(k_band), 1)
+        band = {"radius_band_hit_fraction": retests.value / tests.value if tests.value else None,
+                "knn_band_hit_fraction": k_band.value / k_tests.value if k_tests.value else None}
+        return (offs.cpu().numpy(), out[: tot.value].cpu().numpy().view(np.uint32), kidx.cpu().numpy().view(np.uint32),
+                kd2.cpu().numpy(), kcnt.cpu().numpy(), band)
+
+    def engine(fp32):
+        eng.set_config(**dict(eng_cfg, fp32_filter=fp32))
+        try:
+            places = eng.run([Request(proxy, "radius", qr, radius=RADIUS, kernel="sphere", algo="neighborsPrune"),
+                              Request(proxy, "knn", qk, k=KNN_K)])
+            offs, idx = eng.radius_result(places[0])
+            kidx, kd2, kcnt = eng.knn_result(places[1], KNN_K)
+        finally:
+            eng.set_config(**eng_cfg)
+        return offs, idx, kidx, kd2, kcnt, {}
+
+    runs = {"plain": lambda: single(0, 0, args.radius_group, 0), "packet": lambda: single(1, 0, 8, 1),
+            "packet_fp32": lambda: single(1, 1, 8, 1), "engine": lambda: engine(0), "engine_fp32": lambda: engine(1)}
+    out = {}
+    total_diffs, max_err = 0, 0.0
+    for name, fn in runs.items():
+        offs, idx, kidx, kd2, kcnt, band = fn()
+        rd = csr_set_diffs(offs, idx, ro, ri)
+        kdiff, kerr, ties = knn_diffs(kidx, kd2, kcnt, ki, kd, kc, sxyz, qk_h)
+        out[name] = dict(radius_set_diffs=rd, knn_diffs=kdiff, max_d2_err=kerr, knn_tie_groups_checked=ties,
+                         radius_neighbours=int(offs[-1]), **band)
+        total_diffs += rd + kdiff
+        max_err = max(max_err, kerr)
+    cfg0 = capi.OctSearchConfig(1, 0, 8, 1, args.knn_bucket)  # the headline path's configuration again
+    capi.check(L.oct_set_search_config(h, C.byref(cfg0)), h, "search config")
+    parity = {"against": arm["kind"], "centres": {"radius": p, "knn": p},
+              "query": f"sphere neighborsPrune r={RADIUS} m and kNN k={KNN_K} at the CPU sample's centres",
+              "set_diffs": total_diffs, "max_d2_err": max_err, "paths": out, "reference_s": ref_s,
+              "rule": "radius: sorted neighbour index sets equal; kNN: counts and squared distances bitwise equal, "
+                      "index sets equal below the k-th distance, ties at the k-th distance the lowest indices"}
+    return {"cpu": cpu, "parity": parity}
 
 
 def run_reference_arm(args, rank, world):
@@ -412,12 +521,16 @@ def run_serving(args, dev):
     clocks = ClockSampler(dev)
     clocks.start()
     srv = Server(device=dev)
-    batched = replay(wl, srv, drain_s=args.serve_drain)
-    srv.close()
-    clk = clocks.stop()
+    try:
+        batched = replay(wl, srv, drain_s=args.serve_drain)
+    finally:
+        srv.close()
+        clk = clocks.stop()
     srv = Server(device=dev, plain=True)
-    plain = replay(wl, srv, drain_s=args.serve_drain)
-    srv.close()
+    try:
+        plain = replay(wl, srv, drain_s=args.serve_drain)
+    finally:
+        srv.close()
     return {
         "workload": wl.describe(),
         "batched": batched, "plain": plain,
@@ -757,33 +870,7 @@ def run_b200(args, rank, world, local_rank):
              "includes": "bbox + encode + 8-bit onesweep sort + reorder + octree build from points resident in "
                          "HBM, host syncs included (wall clock)"}
 
-    batched = None
-    if world == 1 and not args.no_batched:
-        batched = run_batched(args, dev)
-        gc.collect()
-        torch.cuda.empty_cache()
-    serving = None
-    if world == 1 and not args.no_serve:
-        serving = run_serving(args, dev)
-        gc.collect()
-        torch.cuda.empty_cache()
-    large = None
-    if world == 1 and args.large:
-        L.oct_cloud_destroy(h)  # room for the large cloud
-        h = None
-        gc.collect()
-        torch.cuda.empty_cache()
-        large = run_large(args, dev)
-
-    cpu = None
-    if rank == 0 and world == 1 and not args.no_cpu:
-        arm = cpu_arm(xyz_h, threads=0, target_s=args.cpu_seconds)
-        m = arm["sample_per_kind"]
-        tr, tk = arm["run"](arm["sample"][:m], arm["sample"][m:])
-        cpu = {"value": 2 * m / (tr + tk), "unit": "queries/s", "cores": arm["cores"], "kind": arm["kind"],
-               "sample": f"{m} radius (sphere, neighborsPrune, r={RADIUS}) + {m} kNN (k={KNN_K}) queries at random "
-                         f"points of the same 10M cloud, all host threads",
-               "radius_qps": m / tr, "knn_qps": m / tk}
+    line = None
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": "queries/s", "n_gpus": world, "steps": args.steps,
@@ -793,14 +880,92 @@ def run_b200(args, rank, world, local_rank):
             "radius_qps": chosen["radius_qps"], "knn_qps": chosen["knn_qps"],
             "avg_neighbours": chosen["avg_neighbours"], "paths": paths,
             "batched_vs_plain": paths["engine"]["qps"] / paths["plain"]["qps"], "engine_config": eng_cfg,
-            "build": build, "batched": batched, "serving": serving, "large": large, "roofline": roofline, "cpu_baseline": cpu,
+            "build": build, "roofline": roofline, "cpu_baseline": None, "parity": None,
+            "batched": None, "serving": None, "large": None,
             "e2e": {"value": e2e_val, "unit": "queries/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
                     "detail": e2e_detail},
             "gpu_launches": LAUNCHES_PER_STEP[args.search] * args.steps, "clocks": clk,
         }
-        print(json.dumps(line), flush=True)
-    L.oct_cloud_destroy(h)
+        _STATE["line"] = line  # from here on the deadline prints what has been measured
+
+    # the reference CPU path on a bounded sample of the same queries, and that sample's results through every
+    # GPU search path compared with the reference's (set differences, kNN differences, max d^2 error)
+    if rank == 0 and world == 1 and not args.no_cpu:
+        res = _section("cpu_baseline", lambda: cpu_leg(args, xyz_h, h, eng, proxy, eng_cfg))
+        if "error" in res:
+            line["cpu_baseline"] = None
+            line["parity"] = res
+        else:
+            line["cpu_baseline"], line["parity"] = res["cpu"], res["parity"]
+    if world == 1 and not args.no_batched:
+        line["batched"] = _section("batched", lambda: run_batched(args, dev))
+        gc.collect()
+        torch.cuda.empty_cache()
+    if world == 1 and not args.no_serve:
+        line["serving"] = _section("serving", lambda: run_serving(args, dev))
+        gc.collect()
+        torch.cuda.empty_cache()
+    if world == 1 and args.large:
+        L.oct_cloud_destroy(h)  # room for the large cloud
+        h = None
+        eng.close()
+        gc.collect()
+        torch.cuda.empty_cache()
+        line["large"] = _section("large", lambda: run_large(args, dev))
+    if rank == 0:
+        _emit(line)
+    if h is not None:
+        L.oct_cloud_destroy(h)
     return 0
+
+
+# ----------------------------------------------------- deadline and sections ---
+_STATE = {"line": None, "section": None, "printed": False}
+_PRINT_LOCK = threading.Lock()
+
+
+def _emit(line):
+    with _PRINT_LOCK:
+        if _STATE["printed"]:
+            return
+        _STATE["printed"] = True
+        print(json.dumps(line), flush=True)
+
+
+def _start_deadline(seconds: float):
+    """After ``seconds`` print the line measured so far (the unfinished section named) and exit; a run whose
+    headline is not measured by then exits non-zero."""
+    def fire():
+        line = _STATE["line"]
+        if line is None:
+            sys.stderr.write(f"bench: deadline of {seconds:g} s passed in section {_STATE['section']!r} before the "
+                             "headline was measured\n")
+            sys.stderr.flush()
+            os._exit(3)
+        line = dict(line)
+        line["incomplete"] = {"section": _STATE["section"], "deadline_s": seconds}
+        _emit(line)
+        os._exit(0)
+
+    t = threading.Timer(seconds, fire)
+    t.daemon = True
+    t.start()
+    return t
+
+
+def _section(name, fn):
+    """Run one auxiliary section; an exception is reported in its place instead of ending the run."""
+    _STATE["section"] = name
+    t0 = time.perf_counter()
+    try:
+        out = fn()
+    except Exception as exc:  # noqa: BLE001 - reported in the JSON line
+        traceback.print_exc()
+        out = {"error": f"{type(exc).__name__}: {exc}"}
+    if isinstance(out, dict):
+        out["section_s"] = round(time.perf_counter() - t0, 2)
+    _STATE["section"] = None
+    return out
 
 
 def main():
@@ -821,7 +986,7 @@ def main():
     ap.add_argument("--batched-steps", type=int, default=3, help="timed repetitions of the 256-cloud batch")
     ap.add_argument("--no-serve", action="store_true", help="skip the serving stream")
     ap.add_argument("--serve-seconds", type=float, default=60.0, help="length of the serving request stream")
-    ap.add_argument("--serve-drain", type=float, default=30.0,
+    ap.add_argument("--serve-drain", type=float, default=10.0,
                     help="seconds each server may take after the stream ends before it is stopped")
     ap.add_argument("--large", action="store_true", help="also run the 500M-point skewed cloud (not in the default run)")
     ap.add_argument("--large-points", type=int, default=500_000_000)
@@ -829,6 +994,8 @@ def main():
     ap.add_argument("--large-k", type=int, default=1000)
     ap.add_argument("--points", type=int, default=N_POINTS, help="cloud size (smaller cases for profiling)")
     ap.add_argument("--queries", type=int, default=Q_RADIUS, help="radius and kNN queries per step, each")
+    ap.add_argument("--deadline", type=float, default=1200.0,
+                    help="seconds after which the line measured so far is printed (unfinished section named)")
     args = ap.parse_args()
     if args.points != N_POINTS:
         TILE_M = TILE_M * math.sqrt(args.points / N_POINTS)  # same point density
@@ -839,6 +1006,8 @@ def main():
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))
     if args.impl == "reference":
         return run_reference_arm(args, rank, world)
+    if args.deadline > 0:
+        _start_deadline(args.deadline)
     if world > 1:
         import datetime
 

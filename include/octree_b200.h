@@ -444,7 +444,15 @@ int oct_server_get_stats(oct_server server, oct_server_stats* stats);
  *    any stream capture;
  *  - every call on a device shares the one scratch array and clears what must
  *    start at zero itself, so calls whose work overlaps on the GPU (other
- *    streams, other host threads) race and must be serialised by the caller. */
+ *    streams, other host threads) race and must be serialised by the caller;
+ *  - the address looked up at the first call is kept for the life of the
+ *    process: do not call this entry point on a device after cudaDeviceReset
+ *    (or after its primary context was released and made again);
+ *  - errors found on the device arrive with the results, not in the return
+ *    code (the call does not wait): if a sort pass's bounded wait for an
+ *    earlier tile gave up, some keys and ids were not written and d_box12's
+ *    radii (elements 3..5) hold -1.0, which no Box can hold.  Check them after
+ *    synchronising the stream. */
 int oct_encode_sort_noalloc(int encoder, const double* d_xyz, uint64_t n, uint64_t* d_keys, uint32_t* d_perm,
                             double* d_box12, void* stream);
 

@@ -481,13 +481,10 @@ cudaError_t launch_sort_passes(Cloud& c, const uint32_t skip[8], int* final_sel)
         if ((e = cudaMemsetAsync(c.sort_status.ptr, 0, c.sort_status.bytes, c.stream)) != cudaSuccess) return e;
         c.sort_epoch = 0;
     }
-    static bool attr_set[2] = {false, false};
+    // the shared-memory limit is an attribute of the current device's copy of the kernel: set it on every call
+    // (cheap, host side), so that clouds on any device and from any host thread launch with it
     const size_t smem = onesweep_smem();
-    if (!attr_set[0]) {
-        cudaFuncSetAttribute(k_onesweep<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        cudaFuncSetAttribute(k_onesweep<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        attr_set[0] = attr_set[1] = true;
-    }
+    if ((e = prepare_sort_dyn()) != cudaSuccess) return e;
     DevBuf* kb[2] = {&c.keys, &c.keys_alt};
     DevBuf* vb[2] = {&c.perm, &c.perm_alt};
     int sel = 0;
@@ -628,8 +625,7 @@ cudaError_t launch_query_order(Cloud& c, const double* d_centers, uint64_t nq, c
         c.qs_epoch = 0;
     }
     const size_t smem = onesweep_smem();
-    cudaFuncSetAttribute(k_onesweep<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    cudaFuncSetAttribute(k_onesweep<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if ((e = prepare_sort_dyn()) != cudaSuccess) return e;
     SortCtl* ctl = c.qs_ctl.as<SortCtl>();
     if ((e = cudaMemsetAsync(ctl, 0, sizeof(SortCtl), c.stream)) != cudaSuccess) return e;
     const int sms = sm_count(c.device);
@@ -691,6 +687,17 @@ struct NoAllocScratch {
 };
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[sizeof(NoAllocScratch)];
+
+// The Box (center, radii, min, max: the 12 leading doubles of BoxGeom) into
+// the caller's buffer.  If a sort pass's bounded look-back gave up (its error
+// word is set) some keys and ids were never written; the radii are then set
+// to -1.0, a value no Box can hold (radii are half the extent: >= 0 or NaN).
+__global__ void k_noalloc_box(const BoxGeom* bg, const uint32_t* err, double* box12) {
+    const int i = threadIdx.x;
+    if (i >= 12) return;
+    const double* src = reinterpret_cast<const double*>(&bg->box);
+    box12[i] = (*err != 0u && i >= 3 && i < 6) ? -1.0 : src[i];
+}
 
 namespace {
 
@@ -774,9 +781,8 @@ extern "C" int oct_encode_sort_noalloc(int encoder, const double* d_xyz, uint64_
                                                                               sc->status, (uint32_t)(p + 1), err);
         }
     }
-    // Box (center, radii, min, max): the 12 leading doubles of the scratch BoxGeom
-    if (cudaMemcpyAsync(d_box12, &sc->bg.box, 12 * sizeof(double), cudaMemcpyDeviceToDevice, s) != cudaSuccess)
-        return OCT_ERR_CUDA;
+    // Box (center, radii, min, max), radii -1.0 if a look-back gave up
+    k_noalloc_box<<<1, 32, 0, s>>>(&sc->bg, reinterpret_cast<const uint32_t*>(&ctl->pad), d_box12);
     const cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? OCT_OK : OCT_ERR_CUDA;
 }

@@ -182,17 +182,19 @@ class ServingWorkload:
     """Resident clouds, their centre pools, the inserted clouds' points and the request stream."""
 
     def __init__(self, device: int = 0, seconds: float = 60.0, rate: float = 2000.0, n_clouds: int = 16,
-                 insert_every: float = 10.0, pool: int = 200_000, workers=None):
+                 insert_every: float = 10.0, pool: int = 200_000, workers=None, cloud_points=(1_000_000, 50_000_000),
+                 insert_points=(1_000_000, 10_000_000), max_batch: int = 100_000):
         import torch
 
         from .linear_octree import LinearOctree
         from .workloads import generate_points
 
         self.seconds, self.rate, self.insert_every = seconds, rate, insert_every
-        self.specs = serving_cloud_specs(n_clouds)
+        self.specs = serving_cloud_specs(n_clouds, n_min=cloud_points[0], n_max=cloud_points[1])
         n_ins = int(seconds // insert_every) if insert_every > 0 else 0
         rng = np.random.default_rng(44)
-        self.insert_specs = [dict(n=int(round(math.exp(rng.uniform(math.log(1e6), math.log(1e7))))), seed=30 + j,
+        lo, hi = math.log(insert_points[0]), math.log(insert_points[1])
+        self.insert_specs = [dict(n=int(round(math.exp(rng.uniform(lo, hi)))), seed=30 + j,
                                   encoder=5, max_leaf=64, n_queries=0) for j in range(n_ins)]
         for s in self.insert_specs:
             s["tile_m"] = math.sqrt(s["n"] / SERVE_DENSITY)
@@ -208,7 +210,8 @@ class ServingWorkload:
             self.pools.append(d[torch.randint(0, spec["n"], (pool,), device="cuda", generator=g)].contiguous())
             del d
         self.insert_points = pts[len(self.specs):]
-        self.stream = serving_stream(rate, seconds, n_clouds=n_clouds, insert_every=insert_every)
+        self.stream = serving_stream(rate, seconds, n_clouds=n_clouds, max_batch=min(max_batch, pool),
+                                     insert_every=insert_every)
         self.n_points = sum(s["n"] for s in self.specs)
         self.pool = pool
         torch.cuda.synchronize()
@@ -228,8 +231,17 @@ def _pct(v, q):
     return float(np.percentile(np.asarray(v, np.float64), q)) if len(v) else None
 
 
-def replay(wl: ServingWorkload, server: Server, drain_s: float = 60.0, owned_inserts: bool = True):
-    """Submit the stream at its arrival times; returns latency / throughput figures."""
+def replay(wl: ServingWorkload, server: Server, drain_s: float = 60.0, owned_inserts: bool = True,
+           insert_wait_s: float = 120.0):
+    """Submit the stream at its arrival times; returns latency / throughput figures.
+
+    Inserted clouds are built by a background thread on its own stream, each
+    during the epoch before its own.  That thread waits for its own stream
+    only: a device-wide synchronisation would fail while the server's
+    scheduler captures a batch graph on another stream.  Every wait here is
+    bounded; a failed or late insertion is reported (its requests are counted
+    as skipped) instead of stalling the stream, and an error raised in a
+    helper thread is re-raised here once the stream has been submitted."""
     import torch
 
     from .linear_octree import LinearOctree
@@ -237,19 +249,35 @@ def replay(wl: ServingWorkload, server: Server, drain_s: float = 60.0, owned_ins
     for oc in wl.clouds:
         server.add_cloud(oc)
     inserted = {}  # epoch -> (handle, centre pool), registered with the server
-    # inserted clouds are built in the background, each during the epoch before its own
     built = {}
+    failed_epochs = set()
+    thread_errors = []  # (thread name, exception)
     ready = {e: threading.Event() for e in range(1, len(wl.insert_specs) + 1)}
+    dev = torch.cuda.current_device()
 
     def builder():
         brng = np.random.default_rng(8)
-        for e in range(1, len(wl.insert_specs) + 1):
-            p, spec = wl.insert_points[e - 1], wl.insert_specs[e - 1]
-            oc = LinearOctree(torch.from_numpy(p).cuda(), encoder=spec["encoder"], max_points_leaf=spec["max_leaf"])
-            pool = torch.from_numpy(p[brng.integers(0, spec["n"], wl.pool)]).cuda()
-            torch.cuda.synchronize()
-            built[e] = (oc, pool)
-            ready[e].set()
+        bstream = torch.cuda.Stream(device=dev)
+        try:
+            for e in range(1, len(wl.insert_specs) + 1):
+                p, spec = wl.insert_points[e - 1], wl.insert_specs[e - 1]
+                sel = brng.integers(0, spec["n"], wl.pool)
+                try:
+                    with torch.cuda.stream(bstream):
+                        d = torch.from_numpy(p).cuda(dev)
+                        pool = torch.from_numpy(p[sel]).cuda(dev)
+                        oc = LinearOctree(d, encoder=spec["encoder"], max_points_leaf=spec["max_leaf"], device=dev)
+                    bstream.synchronize()  # this stream only: never the device
+                    del d
+                    built[e] = (oc, pool)
+                except Exception as exc:  # noqa: BLE001 - reported with the figures
+                    thread_errors.append(("insert builder", exc))
+                    failed_epochs.add(e)
+                finally:
+                    ready[e].set()
+        finally:
+            for ev in ready.values():
+                ev.set()
 
     removers = []
     bt = threading.Thread(target=builder, daemon=True)
@@ -257,76 +285,101 @@ def replay(wl: ServingWorkload, server: Server, drain_s: float = 60.0, owned_ins
     lat, qms, nq_done = [], [], [0]
     errors = [0]
     done_evt = threading.Event()
+    skipped = [0]
     n_total = len(wl.stream)
 
     def collector():
         got = 0
-        while got < n_total and not done_evt.is_set():
-            for c in server.poll(4096, wait_ms=5):
-                got += 1
-                if c["status"] != capi.OCT_OK:
-                    errors[0] += 1
-                else:
-                    lat.append(c["latency_ms"])
-                    qms.append(c["queue_ms"])
-                    nq_done[0] += c["nq"]
-                server.release(c["ticket"])
-        done_evt.set()
+        try:
+            while got + skipped[0] < n_total and not done_evt.is_set():
+                for c in server.poll(4096, wait_ms=5):
+                    got += 1
+                    if c["status"] != capi.OCT_OK:
+                        errors[0] += 1
+                    else:
+                        lat.append(c["latency_ms"])
+                        qms.append(c["queue_ms"])
+                        nq_done[0] += c["nq"]
+                    server.release(c["ticket"])
+        except Exception as exc:  # noqa: BLE001
+            thread_errors.append(("collector", exc))
+        finally:
+            done_evt.set()
+
+    def remover(old):
+        try:
+            server.remove_cloud(C.c_void_p(old))
+        except Exception as exc:  # noqa: BLE001
+            thread_errors.append(("remover", exc))
 
     th = threading.Thread(target=collector, daemon=True)
     th.start()
     rng = np.random.default_rng(7)
     t0 = time.perf_counter()
     late = []
-    for it in wl.stream:
-        epoch = int(it.t // wl.insert_every) if wl.insert_every > 0 else 0
-        if epoch > 0 and epoch not in inserted:  # insert this epoch's cloud, evict the previous one
-            ready[epoch].wait()
-            oc, pool = built.pop(epoch)
-            h = oc.handle.value
-            server.add_cloud(oc, owned=owned_inserts)
-            inserted[epoch] = (h, pool)
-            if epoch - 1 in inserted:  # removed once its requests have finished, off the submit thread
-                old = inserted.pop(epoch - 1)[0]
-                rt = threading.Thread(target=server.remove_cloud, args=(C.c_void_p(old),), daemon=True)
-                rt.start()
-                removers.append(rt)
-        now = time.perf_counter() - t0
-        if it.t > now:
-            time.sleep(it.t - now)
-        late.append(max(0.0, time.perf_counter() - t0 - it.t))
-        if it.cloud >= 0:
-            handle, pool = wl.clouds[it.cloud].handle, wl.pools[it.cloud]
-        else:
-            handle, pool = inserted[-it.cloud]
-        off = int(rng.integers(0, wl.pool - it.nq + 1))
-        centres = pool[off: off + it.nq]
-        proxy = _Handle(handle)
-        if it.kind == "radius":
-            req = Request(proxy, "radius", centres, radius=it.radius, kernel="sphere", algo="neighborsPrune")
-        else:
-            req = Request(proxy, "knn", centres, k=it.k)
-        server.submit(req, sync=False)  # the pools were complete before the stream started
-    t_sub = time.perf_counter() - t0
-    th.join(timeout=max(1.0, drain_s))
-    done_evt.set()
-    t_end = time.perf_counter() - t0
-    for rt in removers:
-        rt.join(timeout=5.0)
-    bt.join(timeout=5.0)
+    try:
+        for it in wl.stream:
+            if done_evt.is_set() and thread_errors:
+                break  # the collector died: nothing would be collected
+            epoch = int(it.t // wl.insert_every) if wl.insert_every > 0 else 0
+            if epoch > 0 and epoch not in inserted and epoch not in failed_epochs:
+                # insert this epoch's cloud, evict the previous one
+                if not ready[epoch].wait(timeout=insert_wait_s) or epoch not in built:
+                    failed_epochs.add(epoch)
+                else:
+                    oc, pool = built.pop(epoch)
+                    h = oc.handle.value
+                    server.add_cloud(oc, owned=owned_inserts)
+                    inserted[epoch] = (h, pool)
+                    if epoch - 1 in inserted:  # removed once its requests have finished, off the submit thread
+                        old = inserted.pop(epoch - 1)[0]
+                        rt = threading.Thread(target=remover, args=(old,), daemon=True)
+                        rt.start()
+                        removers.append(rt)
+            now = time.perf_counter() - t0
+            if it.t > now:
+                time.sleep(it.t - now)
+            late.append(max(0.0, time.perf_counter() - t0 - it.t))
+            if it.cloud >= 0:
+                handle, pool = wl.clouds[it.cloud].handle, wl.pools[it.cloud]
+            elif -it.cloud in inserted:
+                handle, pool = inserted[-it.cloud]
+            else:  # its cloud's insertion failed
+                skipped[0] += 1
+                continue
+            off = int(rng.integers(0, wl.pool - it.nq + 1))
+            centres = pool[off: off + it.nq]
+            proxy = _Handle(handle)
+            if it.kind == "radius":
+                req = Request(proxy, "radius", centres, radius=it.radius, kernel="sphere", algo="neighborsPrune")
+            else:
+                req = Request(proxy, "knn", centres, k=it.k)
+            server.submit(req, sync=False)  # the pools were complete before the stream started
+    finally:
+        t_sub = time.perf_counter() - t0
+        th.join(timeout=max(1.0, drain_s))
+        done_evt.set()
+        th.join(timeout=5.0)
+        t_end = time.perf_counter() - t0
+        for rt in removers:
+            rt.join(timeout=5.0)
+        bt.join(timeout=5.0)
+    if thread_errors:
+        name, exc = thread_errors[0]
+        raise RuntimeError(f"serving replay: the {name} thread failed: {exc!r}") from exc
     st = server.stats()
     completed = len(lat)
     return {
         "requests": n_total, "completed": completed, "errors": errors[0],
-        "unfinished": n_total - completed - errors[0],
+        "unfinished": n_total - completed - errors[0] - skipped[0], "skipped": skipped[0],
         "p50_ms": _pct(lat, 50), "p90_ms": _pct(lat, 90), "p99_ms": _pct(lat, 99), "max_ms": max(lat) if lat else None,
         "queue_p50_ms": _pct(qms, 50), "queue_p99_ms": _pct(qms, 99),
         "queries_completed": nq_done[0], "wall_s": t_end, "submit_s": t_sub,
         "qps": nq_done[0] / t_end if t_end > 0 else None,
-        "submit_lag_p99_ms": 1e3 * _pct(late, 99),
+        "submit_lag_p99_ms": 1e3 * _pct(late, 99) if late else None,
         "batches": st["batches"], "admission_stalls": st["admission_stalls"],
-        "budget_evictions": st["evictions"], "clouds_inserted": len(wl.insert_specs),
-        "clouds_removed": len(removers), "peak_budget_bytes": st["peak_bytes"],
+        "budget_evictions": st["evictions"], "clouds_inserted": len(inserted) + len(removers),
+        "insert_failures": len(failed_epochs), "clouds_removed": len(removers), "peak_budget_bytes": st["peak_bytes"],
     }
 
 

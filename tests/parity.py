@@ -109,3 +109,65 @@ def assert_knn_equal(idx_g, d2_g, cnt_g, idx_r, d2_r, cnt_r, xyz, centers, what=
         else:
             assert len(tie_g) == len(tie_r) and np.all(np.isin(tie_g, allk)), f"{what}: bad tie group at query {q}"
     return n_ties
+
+
+# ---- vectorised counts of differences (large query sets) --------------------
+def csr_set_diffs(offs_a, idx_a, offs_b, idx_b) -> int:
+    """Number of queries whose neighbour sets differ between two CSR results
+    (the order within a query is free)."""
+    offs_a = np.asarray(offs_a, np.int64)
+    offs_b = np.asarray(offs_b, np.int64)
+    idx_a = np.asarray(idx_a, np.int64)[: offs_a[-1]]
+    idx_b = np.asarray(idx_b, np.int64)[: offs_b[-1]]
+    ca, cb = np.diff(offs_a), np.diff(offs_b)
+    nq = len(ca)
+    same_cnt = ca == cb
+    bad = ~same_cnt
+    keep_a = np.repeat(same_cnt, ca)
+    keep_b = np.repeat(same_cnt, cb)
+    seg = np.repeat(np.arange(nq), np.where(same_cnt, ca, 0))
+    va, vb = idx_a[keep_a], idx_b[keep_b]
+    sa = va[np.lexsort((va, seg))]
+    sb = vb[np.lexsort((vb, seg))]
+    diff = sa != sb
+    if diff.any():
+        bad[np.unique(seg[diff])] = True
+    return int(bad.sum())
+
+
+def knn_diffs(idx_g, d2_g, cnt_g, idx_r, d2_r, cnt_r, xyz, centers, max_tie_checks: int = 64):
+    """kNN result g against reference r, vectorised.  Returns (queries that
+    differ, max |d2_g - d2_r|, tie groups checked by brute force).  A query
+    differs when its count, any squared distance (bitwise) or its index set
+    below the k-th distance differs, or when its tie group at the k-th
+    distance is not the lowest indices of all points at that distance."""
+    idx_g = np.asarray(idx_g, np.int64)
+    idx_r = np.asarray(idx_r, np.int64)
+    d2_g = np.asarray(d2_g, np.float64)
+    d2_r = np.asarray(d2_r, np.float64)
+    cnt_g = np.asarray(cnt_g, np.int64)
+    cnt_r = np.asarray(cnt_r, np.int64)
+    nq, k = d2_g.shape
+    bad = cnt_g != cnt_r
+    valid = np.arange(k)[None, :] < np.minimum(cnt_g, cnt_r)[:, None]
+    err = np.where(valid, np.abs(d2_g - d2_r), 0.0)
+    max_err = float(err.max()) if err.size else 0.0
+    bad |= ((d2_g.view(np.uint64) != d2_r.view(np.uint64)) & valid).any(axis=1)
+    last = np.maximum(np.minimum(cnt_g, cnt_r) - 1, 0)
+    kth = d2_g[np.arange(nq), last][:, None]
+    big = np.iinfo(np.int64).max
+    below_g = np.sort(np.where(valid & (d2_g < kth), idx_g, big), axis=1)
+    below_r = np.sort(np.where(valid & (d2_r < kth), idx_r, big), axis=1)
+    bad |= (below_g != below_r).any(axis=1)
+    tie_g = np.sort(np.where(valid & (d2_g == kth), idx_g, big), axis=1)
+    tie_r = np.sort(np.where(valid & (d2_r == kth), idx_r, big), axis=1)
+    tie_rows = np.nonzero(~bad & (tie_g != tie_r).any(axis=1))[0]
+    checked = 0
+    for q in tie_rows[:max_tie_checks]:
+        checked += 1
+        allk = np.sort(np.nonzero(sq_dist(xyz, centers[q]) == kth[q, 0])[0])
+        mine = tie_g[q][tie_g[q] != big]
+        if not np.array_equal(mine, allk[: len(mine)]):
+            bad[q] = True
+    bad[tie_rows[max_tie_checks:]] = True  # not checked: counted as differences
+    return int(bad.sum()), max_err, checked

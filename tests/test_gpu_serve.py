@@ -176,6 +176,26 @@ def test_bad_requests_are_rejected(torch, clouds):
     srv.close()
 
 
+def test_replay_inserts_clouds_while_batches_capture(torch):
+    """Clouds built by a background thread and inserted while the scheduler
+    captures and replays batch graphs (a batch on one cloud is captured per
+    cloud, so every insert brings new captures): the replay ends by itself,
+    every request completes and every insertion lands."""
+    from octrees_benchmark_b200.serve import ServingWorkload, replay
+
+    wl = ServingWorkload(seconds=3.0, rate=300.0, n_clouds=3, insert_every=0.5, pool=4000, workers=1,
+                         cloud_points=(40_000, 120_000), insert_points=(30_000, 80_000), max_batch=2000)
+    epochs = {int(it.t // wl.insert_every) for it in wl.stream} - {0}
+    srv = Server(slots=3)
+    try:
+        res = replay(wl, srv, drain_s=30.0, insert_wait_s=60.0)
+    finally:
+        srv.close()
+    assert res["errors"] == 0 and res["insert_failures"] == 0 and res["skipped"] == 0
+    assert res["completed"] == res["requests"] and res["unfinished"] == 0
+    assert res["clouds_inserted"] == len(epochs) and len(epochs) >= 4
+
+
 class _H:
     def __init__(self, h):
         self.handle = C.c_void_p(h)

@@ -6,8 +6,9 @@ cudaFree on their streams, and latency-bound loops that cannot afford the
 device-wide synchronisation an allocation causes.  For them the library keeps
 its sort scratch in one fixed device array and the caller passes only the
 points and the outputs.  This test calls that entry point through the C ABI,
-twice in a row on one stream (two different clouds, so the second call runs on
-scratch the first call left behind), and checks each result bit for bit
+three times in a row on one stream (different clouds, large after small and
+small after large, so each call runs on scratch the previous call left
+behind) and once on an empty cloud, and checks each result bit for bit
 against the regular entry point oct_encode_sort.  It lives in a file of its
 own that pytest collects last, and it passes both alone in a fresh process and
 after the other tests.
@@ -42,11 +43,14 @@ def regular_encode_sort(xyz, encoder):
         L.oct_cloud_destroy(h)
 
 
-def test_noalloc_matches_regular_entry_point_on_two_calls_in_a_row():
+def test_noalloc_matches_regular_entry_point_on_calls_in_a_row():
     torch = pytest.importorskip("torch")
     L = capi.lib()
+    # small after large too: the third call runs on scratch (look-back words beyond its own tiles) that the
+    # largest cloud left behind
     clouds = [(lidar_tile(200_003, 220.0, seed=41), capi.ENCODERS["hilbert"]),
-              (lidar_tile(capi.OCT_NOALLOC_MAX_POINTS, 240.0, seed=42), capi.ENCODERS["morton"])]
+              (lidar_tile(capi.OCT_NOALLOC_MAX_POINTS, 240.0, seed=42), capi.ENCODERS["morton"]),
+              (lidar_tile(5_000, 30.0, seed=44), capi.ENCODERS["hilbert"])]
     dev_in, dev_out = [], []
     for xyz, _ in clouds:
         n = len(xyz)
@@ -55,7 +59,7 @@ def test_noalloc_matches_regular_entry_point_on_two_calls_in_a_row():
                         torch.empty(n, dtype=torch.int32, device="cuda"),
                         torch.empty(12, dtype=torch.float64, device="cuda")))
     torch.cuda.synchronize()
-    # two calls in a row on the default stream; the second reuses the scratch the first left behind
+    # calls in a row on the default stream; each reuses the scratch the previous one left behind
     free_before_second = None
     for i, ((xyz, enc), d_xyz, (keys, perm, box)) in enumerate(zip(clouds, dev_in, dev_out)):
         if i == 1:
@@ -65,13 +69,25 @@ def test_noalloc_matches_regular_entry_point_on_two_calls_in_a_row():
                                        box.data_ptr(), None)
         assert st == capi.OCT_OK
     torch.cuda.synchronize()
-    # the second call allocated nothing on the device
+    # the later calls allocated nothing on the device
     assert torch.cuda.mem_get_info()[0] == free_before_second
     for (xyz, enc), (keys, perm, box) in zip(clouds, dev_out):
         rk, rp, rb = regular_encode_sort(xyz, enc)
         assert np.array_equal(keys.cpu().numpy().view(np.uint64), rk)
         assert np.array_equal(perm.cpu().numpy().view(np.uint32), rp)
         assert same_f64(box.cpu().numpy(), rb)
+        assert np.all(box.cpu().numpy()[3:6] >= 0.0)  # -1.0 would flag a sort pass that gave up
+
+
+def test_noalloc_empty_cloud_gives_the_regular_box():
+    torch = pytest.importorskip("torch")
+    L = capi.lib()
+    box = torch.full((12,), 7.0, dtype=torch.float64, device="cuda")
+    st = L.oct_encode_sort_noalloc(5, None, 0, None, None, box.data_ptr(), None)
+    assert st == capi.OCT_OK
+    torch.cuda.synchronize()
+    _, _, rb = regular_encode_sort(np.zeros((0, 3)), 5)
+    assert same_f64(box.cpu().numpy(), rb)
 
 
 def test_noalloc_accepts_a_buffer_that_is_only_8_byte_aligned():
