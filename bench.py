@@ -149,7 +149,7 @@ class ClockSampler:
 def cpu_arm(xyz, threads: int, target_s: float = 10.0):
     """Time the reference CPU implementation on a bounded sample of the query mix.
     Returns a dict describing the baseline and a function running one sample."""
-    from octrees_benchmark_b200.synth import query_indices
+    from octrees_benchmark_b200.synth import query_indices, search_set
     from oracle import oracle as orc
 
     if orc.reference_available():
@@ -193,7 +193,7 @@ def cpu_arm(xyz, threads: int, target_s: float = 10.0):
     tr, tk = run(q[:cal], q[cal:])
     per_q = (tr + tk) / (2 * cal)
     m = int(max(cal, min(Q_RADIUS, target_s / 2 / max(per_q, 1e-9) / 2)))
-    sample = sxyz[query_indices(2 * m, len(sxyz), seed=98)]
+    sample = sxyz[search_set(2 * m, len(sxyz))]  # the reference's SearchSet stream (mt19937 seeded 42)
     return dict(kind=kind, cores=int(cores), sample_per_kind=m, run=run, sample=sample, sorted_xyz=sxyz,
                 ref_radius=ref_radius, ref_knn=ref_knn)
 
@@ -663,7 +663,8 @@ def run_b200(args, rank, world, local_rank):
                           if os.environ.get("CUDA_VISIBLE_DEVICES", "").split(",")[0].isdigit() else dev)
     paths = {}
     clocks.start()
-    for name in SEARCH_PATHS:
+    run_paths = [p_ for p_ in SEARCH_PATHS if not args.paths or p_ in args.paths.split(",") or p_ == args.search]
+    for name in run_paths:
         configure(name)
         run_step = engine_step if name == "engine" else step
         for b in range(args.warmup):
@@ -844,8 +845,10 @@ def run_b200(args, rank, world, local_rank):
     rad_bytes = 24 * Q_RADIUS + 28 * chosen["nbrs_per_step"]
     knn_bytes = (24 + 36 * KNN_K) * Q_KNN
     # per-kernel times: the engine runs the packet path's kernels side by side, so they are timed there alone
-    kpath = args.search if chosen["radius_ms"] is not None else "packet"
+    kpath = args.search if chosen["radius_ms"] is not None else ("packet" if "packet" in paths else args.search)
     rad_ms, knn_ms = paths[kpath]["radius_ms"], paths[kpath]["knn_ms"]
+    if rad_ms is None or knn_ms is None:  # only the engine path ran: its kernels overlap, no per-kernel time
+        rad_ms = knn_ms = float("nan")
     # each time is the whole library call on the cloud's stream (CUDA events): the query ordering plus
     # the search kernels it launches
     rad = {"kernel": f"radius neighborsPrune sphere, {kpath} path (query order + k_radius_packet one pass + "
@@ -879,7 +882,8 @@ def run_b200(args, rank, world, local_rank):
             "config": workload_config(world, {"search_path": args.search}),
             "radius_qps": chosen["radius_qps"], "knn_qps": chosen["knn_qps"],
             "avg_neighbours": chosen["avg_neighbours"], "paths": paths,
-            "batched_vs_plain": paths["engine"]["qps"] / paths["plain"]["qps"], "engine_config": eng_cfg,
+            "batched_vs_plain": (paths["engine"]["qps"] / paths["plain"]["qps"]
+                                 if "engine" in paths and "plain" in paths else None), "engine_config": eng_cfg,
             "build": build, "roofline": roofline, "cpu_baseline": None, "parity": None,
             "batched": None, "serving": None, "large": None,
             "e2e": {"value": e2e_val, "unit": "queries/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,
@@ -994,6 +998,8 @@ def main():
     ap.add_argument("--large-k", type=int, default=1000)
     ap.add_argument("--points", type=int, default=N_POINTS, help="cloud size (smaller cases for profiling)")
     ap.add_argument("--queries", type=int, default=Q_RADIUS, help="radius and kNN queries per step, each")
+    ap.add_argument("--paths", default="", help="comma-separated search paths to time (default: all); the "
+                                                 "--search path always runs")
     ap.add_argument("--deadline", type=float, default=1200.0,
                     help="seconds after which the line measured so far is printed (unfinished section named)")
     args = ap.parse_args()

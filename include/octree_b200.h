@@ -179,6 +179,17 @@ int oct_set_points(oct_cloud cloud, const double* xyz, uint64_t n, uint32_t flag
 int oct_encode_sort(oct_cloud cloud, double* box12, uint64_t* keys, uint32_t* perm, double* sorted_xyz,
                     uint32_t flags);
 
+/* A cloud that is already sorted: n points (xyz AoS) in curve order with
+ * their ascending 63-bit codes and the Box they were encoded in (box12:
+ * center, radii, min, max, as oct_encode_sort returns it).  This is the input
+ * of the reference's LinearOctree(points, codes, box, enc) constructor
+ * (inc/structures/linear_octree.hpp:614-623) when sortPoints ran separately;
+ * oct_build follows.  The points are taken in the order given (perm is the
+ * identity); host codes are checked to be ascending and below 2^63, device
+ * codes (OCT_MEM_DEVICE) are not. */
+int oct_set_sorted_points(oct_cloud cloud, const double* sorted_xyz, const uint64_t* keys, uint64_t n,
+                          const double* box12, uint32_t flags);
+
 /* Build the linear octree over the sorted cloud.  Replaces the
  * LinearOctree(points, codes, box, enc) constructor
  * (inc/structures/linear_octree.hpp:614-623, buildOctree 567-605). */
@@ -231,6 +242,23 @@ int oct_radius_count(oct_cloud cloud, int kernel, int algo, const double* center
 int oct_struct_search(oct_cloud cloud, int kernel, const double* centers, uint64_t nq, const double* radii,
                       double radius, uint64_t* range_offsets, uint32_t* pairs, uint64_t pair_capacity,
                       uint64_t* total_ranges, uint64_t* point_counts, uint32_t flags);
+
+/* The Vector-radii overloads of neighbors / neighborsPrune / neighborsStruct
+ * (linear_octree.hpp:1044-1048, 1056-1060, 1069-1074; kernelFactory(center,
+ * Vector), kernels/kernel_factory.hpp:33-41): the kernel's box is
+ * centre -/+ (rx, ry, rz).  Square and cube kernels only (the reference's
+ * static_assert); other kernels are rejected with OCT_ERR_INVALID_ARG.
+ * radii_xyz: nq x 3 half extents when per_query is non-zero, else one (x, y, z)
+ * for every query (the same buffer kind as the centres: host, or device with
+ * OCT_MEM_DEVICE).  Outputs and capacity handling as oct_radius_search /
+ * oct_struct_search.  These calls run the group-per-query search path whatever
+ * the cloud's search configuration. */
+int oct_radius_search_axes(oct_cloud cloud, int kernel, int algo, const double* centers, uint64_t nq,
+                           const double* radii_xyz, int per_query, uint64_t* offsets, uint32_t* idx,
+                           uint64_t idx_capacity, uint64_t* total, uint32_t flags);
+int oct_struct_search_axes(oct_cloud cloud, int kernel, const double* centers, uint64_t nq, const double* radii_xyz,
+                           int per_query, uint64_t* range_offsets, uint32_t* pairs, uint64_t pair_capacity,
+                           uint64_t* total_ranges, uint64_t* point_counts, uint32_t flags);
 
 /* neighborsApprox (linear_octree.hpp:975-1035): the neighborsStruct search cut
  * below depth precision_level.  A child deeper than that level is not judged:

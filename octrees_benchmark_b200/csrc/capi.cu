@@ -106,6 +106,17 @@ __global__ void k_widen_pairs(const uint2* in, uint64_t n, unsigned long long* o
     }
 }
 
+__global__ void k_aos_to_soa_iota(const double* xyz, uint64_t n, double* xs, double* ys, double* zs,
+                                  uint32_t* perm) {
+    const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) {
+        xs[i] = xyz[3 * i];
+        ys[i] = xyz[3 * i + 1];
+        zs[i] = xyz[3 * i + 2];
+        perm[i] = (uint32_t)i;
+    }
+}
+
 bool valid_kernel(int k) { return k >= OCT_KERNEL_CIRCLE && k <= OCT_KERNEL_CUBE; }
 bool valid_algo(int a) { return a >= OCT_NEIGHBORS && a <= OCT_NEIGHBORS_STRUCT; }
 
@@ -298,7 +309,7 @@ int oct_cloud_destroy(oct_cloud h) {
                           &c.frontier, &c.masks, &c.parts, &c.d_build, &c.q_centers, &c.q_radii, &c.q_counts,
                           &c.q_offsets, &c.q_out, &c.q_out2, &c.q_scan_tmp, &c.qs_keys, &c.qs_keys_alt, &c.qs_ord,
                           &c.qs_ord_alt, &c.qs_status, &c.qs_ctl, &c.packet_ctr, &c.stats, &c.rel,
-                          &c.ck_pool, &c.ck_next, &c.ck_first, &c.ck_ctr, &c.knn_fb, &c.knn_heads, &c.crel};
+                          &c.ck_pool, &c.ck_next, &c.ck_first, &c.ck_ctr, &c.knn_fb, &c.knn_heads, &c.crel, &c.q_axes};
         for (DevBuf* b : bufs) b->release();
         if (c.pinned) cudaFreeHost(c.pinned);
         if (c.own_stream && c.stream) cudaStreamDestroy(c.stream);
@@ -397,7 +408,7 @@ int oct_cloud_memory(oct_cloud h, uint64_t* bytes) {
                             &c.frontier, &c.masks, &c.parts, &c.d_build, &c.q_centers, &c.q_radii, &c.q_counts,
                             &c.q_offsets, &c.q_out, &c.q_out2, &c.q_scan_tmp, &c.qs_keys, &c.qs_keys_alt, &c.qs_ord,
                             &c.qs_ord_alt, &c.qs_status, &c.qs_ctl, &c.packet_ctr, &c.stats, &c.rel,
-                            &c.ck_pool, &c.ck_next, &c.ck_first, &c.ck_ctr, &c.knn_fb, &c.knn_heads, &c.crel};
+                            &c.ck_pool, &c.ck_next, &c.ck_first, &c.ck_ctr, &c.knn_fb, &c.knn_heads, &c.crel, &c.q_axes};
     uint64_t s = 0;
     for (const DevBuf* b : bufs) s += b->bytes;
     *bytes = s;
@@ -459,6 +470,69 @@ int oct_encode_sort(oct_cloud h, double* box12, uint64_t* keys, uint32_t* perm, 
     c.built = false;
     c.node_capacity = 0;
     return emit_sorted(c, box12, keys, perm, sorted_xyz, dev);
+}
+
+int oct_set_sorted_points(oct_cloud h, const double* sorted_xyz, const uint64_t* keys, uint64_t n,
+                          const double* box12, uint32_t flags) {
+    if (!h) return OCT_ERR_INVALID_ARG;
+    Cloud& c = h->c;
+    if (!box12) return set_error(c, OCT_ERR_INVALID_ARG, "box12 is NULL");
+    if (n && (!sorted_xyz || !keys)) return set_error(c, OCT_ERR_INVALID_ARG, "NULL point array");
+    if (n >= 0xffffffffull) return set_error(c, OCT_ERR_INVALID_ARG, "more than 2^32 - 2 points");
+    const bool dev = flags & OCT_MEM_DEVICE;
+    if (!dev) {  // host codes are checked here; device codes are the caller's promise
+        for (uint64_t i = 0; i < n; ++i) {
+            if (keys[i] >= kUpperBound) return set_error(c, OCT_ERR_INVALID_ARG, "key above 63 bits");
+            if (i && keys[i] < keys[i - 1]) return set_error(c, OCT_ERR_INVALID_ARG, "keys are not ascending");
+        }
+    }
+    for (int a = 0; a < 3; ++a)
+        if (!(box12[3 + a] >= 0.0)) return set_error(c, OCT_ERR_INVALID_ARG, "negative or NaN box radii");
+    DeviceGuard g(c.device);
+    const auto kind = dev ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    CK(c.xyz_in.reserve(24 * (n ? n : 1)));
+    CK(c.xs.reserve(8 * (n ? n : 1)));
+    CK(c.ys.reserve(8 * (n ? n : 1)));
+    CK(c.zs.reserve(8 * (n ? n : 1)));
+    CK(c.keys.reserve(8 * (n ? n : 1)));
+    CK(c.perm.reserve(4 * (n ? n : 1)));
+    CK(c.d_box.reserve(sizeof(BoxD) + sizeof(LevelGeom)));
+    // LinearOctree::setupBbox (linear_octree.hpp:439-455) from the caller's Box: half = 0.5f * eps * (max - min),
+    // the level radii 2^(21 - l) * half, in the same FP64 operations as the device build
+    BoxD box;
+    LevelGeom geom;
+    const double eps = 4.76837158203125e-07;  // (double)(1.0f / 2^21)
+    for (int a = 0; a < 3; ++a) {
+        box.center[a] = box12[a];
+        box.radii[a] = box12[3 + a];
+        box.min[a] = box12[6 + a];
+        box.max[a] = box12[9 + a];
+        geom.half[a] = (0.5 * eps) * (box.max[a] - box.min[a]);
+    }
+    for (uint32_t l = 0; l <= kMaxDepth; ++l)
+        for (int a = 0; a < 3; ++a) geom.radii[l][a] = (double)(1u << (kMaxDepth - l)) * geom.half[a];
+    unsigned char* stage = static_cast<unsigned char*>(c.pinned);
+    CK(cudaStreamSynchronize(c.stream));  // the pinned staging area is free
+    memcpy(stage, &box, sizeof(BoxD));
+    memcpy(stage + sizeof(BoxD), &geom, sizeof(LevelGeom));
+    CK(cudaMemcpyAsync(c.d_box.ptr, stage, sizeof(BoxD) + sizeof(LevelGeom), cudaMemcpyHostToDevice, c.stream));
+    if (n) {
+        CK(cudaMemcpyAsync(c.xyz_in.ptr, sorted_xyz, 24 * n, kind, c.stream));
+        CK(cudaMemcpyAsync(c.keys.ptr, keys, 8 * n, kind, c.stream));
+        k_aos_to_soa_iota<<<(unsigned)((n + 255) / 256), 256, 0, c.stream>>>(
+            c.xyz_in.as<double>(), n, c.xs.as<double>(), c.ys.as<double>(), c.zs.as<double>(), c.perm.as<uint32_t>());
+        CK(cudaGetLastError());
+    }
+    CK(cudaStreamSynchronize(c.stream));
+    c.n = n;
+    c.box = box;
+    c.geom = geom;
+    c.sorted = true;
+    c.built = false;
+    c.rel_built = false;
+    c.crel_built = false;
+    c.node_capacity = 0;
+    return OCT_OK;
 }
 
 int oct_build(oct_cloud h, oct_tree_info* info) {
@@ -805,6 +879,64 @@ int oct_approx_search(oct_cloud h, int kernel, const double* centers, uint64_t n
     const uint32_t cut = precision_level >= kMaxDepth ? 0u : precision_level + 1;
     return ranges_search(h, kernel, centers, nq, radii, radius, cut, upper_bound ? 1 : 0, range_offsets, pairs,
                          pair_capacity, total_ranges, point_counts, flags);
+}
+
+namespace {
+// Per-axis radii for the duration of one call.  They are read by the plain
+// radius kernel (one group of lanes per query), which the call is routed to.
+struct AxesScope {
+    Cloud& c;
+    int packet;
+    AxesScope(Cloud& cl, const double* d_axes, uint32_t stride) : c(cl), packet(cl.packet) {
+        c.axes = d_axes;
+        c.axes_stride = stride;
+        c.packet = 0;
+    }
+    ~AxesScope() {
+        c.axes = nullptr;
+        c.axes_stride = 0;
+        c.packet = packet;
+    }
+};
+
+int stage_axes(Cloud& c, int kernel, const double* radii_xyz, uint64_t nq, int per_query, bool dev,
+               const double** out) {
+    if (kernel != OCT_KERNEL_SQUARE && kernel != OCT_KERNEL_CUBE)
+        return set_error(c, OCT_ERR_INVALID_ARG, "per-axis radii take the square or cube kernel");
+    if (!radii_xyz && nq) return set_error(c, OCT_ERR_INVALID_ARG, "radii_xyz is NULL");
+    if (!radii_xyz) {
+        *out = nullptr;
+        return OCT_OK;
+    }
+    return stage_in(c, c.q_axes, radii_xyz, per_query ? 3 * nq : 3, dev, out);
+}
+}  // namespace
+
+int oct_radius_search_axes(oct_cloud h, int kernel, int algo, const double* centers, uint64_t nq,
+                           const double* radii_xyz, int per_query, uint64_t* offsets, uint32_t* idx,
+                           uint64_t idx_capacity, uint64_t* total, uint32_t flags) {
+    if (!h) return OCT_ERR_INVALID_ARG;
+    Cloud& c = h->c;
+    DeviceGuard g(c.device);
+    const double* da = nullptr;
+    const int st = stage_axes(c, kernel, radii_xyz, nq, per_query, (flags & OCT_MEM_DEVICE) != 0, &da);
+    if (st != OCT_OK) return st;
+    AxesScope scope(c, da, per_query ? 3u : 0u);
+    return oct_radius_search(h, kernel, algo, centers, nq, nullptr, 0.0, offsets, idx, idx_capacity, total, flags);
+}
+
+int oct_struct_search_axes(oct_cloud h, int kernel, const double* centers, uint64_t nq, const double* radii_xyz,
+                           int per_query, uint64_t* range_offsets, uint32_t* pairs, uint64_t pair_capacity,
+                           uint64_t* total_ranges, uint64_t* point_counts, uint32_t flags) {
+    if (!h) return OCT_ERR_INVALID_ARG;
+    Cloud& c = h->c;
+    DeviceGuard g(c.device);
+    const double* da = nullptr;
+    const int st = stage_axes(c, kernel, radii_xyz, nq, per_query, (flags & OCT_MEM_DEVICE) != 0, &da);
+    if (st != OCT_OK) return st;
+    AxesScope scope(c, da, per_query ? 3u : 0u);
+    return ranges_search(h, kernel, centers, nq, nullptr, 0.0, 0, 0, range_offsets, pairs, pair_capacity,
+                         total_ranges, point_counts, flags);
 }
 
 int oct_knn(oct_cloud h, const double* centers, uint64_t nq, uint32_t k, uint32_t* idx, double* d2,

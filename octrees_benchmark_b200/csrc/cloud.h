@@ -176,6 +176,11 @@ struct Cloud {
     // (children deeper than that level are cut; approx_upper adds their ranges)
     uint32_t approx_cut = 0;
     int approx_upper = 0;
+    // per-axis radii of the current call (the Vector-radii overloads, cube and square): device pointer to
+    // nq x 3 half extents (axes_stride 3) or one (x, y, z) for every query (axes_stride 0); nullptr otherwise
+    const double* axes = nullptr;
+    uint32_t axes_stride = 0;
+    DevBuf q_axes;
     double knn_est = kKnnEstimate;  // register kNN: provisional-threshold factor (0: off)
     uint32_t knn_chunk = kKnnGroupChunk;  // group kNN: consecutive groups per warp fetch
     // one-pass radius search: result chunk pool, links, first chunk per query, counter

@@ -44,6 +44,8 @@ struct RadiusArgs {
     uint32_t* err;
     uint32_t approx_cut;               // neighborsStruct: 0, or neighborsApprox's precisionLevel + 1
     uint32_t approx_upper;             // neighborsApprox: 1 adds the ranges of the cut octants
+    const double* axes;                // per-axis radii (cube / square), or nullptr
+    uint32_t axes_stride;              // 3: one (x, y, z) per query; 0: one for all queries
 };
 
 template <int G>
@@ -74,7 +76,8 @@ __global__ void __launch_bounds__(kRadThreads) k_radius(RadiusArgs a) {
     const uint64_t ngroups = (uint64_t)gridDim.x * kGroups;
     for (uint64_t q = (uint64_t)blockIdx.x * kGroups + gib; q < a.nq; q += ngroups) {
         SearchKernel k;
-        k.init(a.q[3 * q], a.q[3 * q + 1], a.q[3 * q + 2], a.qr ? a.qr[q] : a.radius);
+        if (a.axes) k.init_axes(a.q[3 * q], a.q[3 * q + 1], a.q[3 * q + 2], a.axes + (uint64_t)a.axes_stride * q);
+        else k.init(a.q[3 * q], a.q[3 * q + 1], a.q[3 * q + 2], a.qr ? a.qr[q] : a.radius);
         unsigned long long cnt = 0;   // indices (prune/neighbors) or ranges (struct)
         unsigned long long cnt2 = 0;  // struct: points
         unsigned long long base = 0;
@@ -390,6 +393,8 @@ cudaError_t launch_radius(Cloud& c, int kernel, int algo, int group, bool fill, 
     a.err = c.d_err.as<uint32_t>();
     a.approx_cut = c.approx_cut;
     a.approx_upper = (uint32_t)c.approx_upper;
+    a.axes = c.axes;
+    a.axes_stride = c.axes_stride;
     const int groups_per_block = kRadThreads / group;
     const uint64_t want = (nq + groups_per_block - 1) / groups_per_block;
     const uint64_t cap = (uint64_t)sm_count_r(c.device) * 8;

@@ -30,6 +30,20 @@ struct SearchKernel {
             bmax[a] = dadd(c[a], radius);
         }
     }
+
+    // KernelAbstract(center, Vector radii) + makeBox (kernel_abstract.hpp:36, 41-45): the box
+    // center -/+ radii per axis; only the cube and square kernels take it (kernel_factory.hpp:33-41),
+    // and they read nothing but the box
+    __device__ __forceinline__ void init_axes(double cx, double cy, double cz, const double* rad) {
+        c[0] = cx; c[1] = cy; c[2] = cz;
+        r = rad[0];
+        r2 = 0.0;
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            bmin[a] = dsub(c[a], rad[a]);
+            bmax[a] = dadd(c[a], rad[a]);
+        }
+    }
 };
 
 // isInside: sphere strict < (kernel_3d.hpp:168-179), circle <= (kernel_2d.hpp:53-63),

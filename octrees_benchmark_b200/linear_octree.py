@@ -122,6 +122,30 @@ class LinearOctree:
         self.box = arr["box"].copy()
         return self
 
+    @classmethod
+    def from_sorted(cls, sorted_points, keys, box, encoder="hilbert", max_points_leaf: int = 128, device: int = 0,
+                    **search):
+        """The reference's LinearOctree(points, codes, box, enc) constructor: a cloud already in curve order with
+        its ascending codes and the Box (12 doubles: center, radii, min, max) it was encoded in."""
+        self = cls.__new__(cls)
+        cfg = dict(radius_group=8, stream=None, packet=True, fp32_filter=False, knn_packet=True, knn_bucket=256)
+        cfg.update(search)
+        self._open(encoder, max_points_leaf, device, cfg["radius_group"], cfg["stream"], cfg["packet"],
+                   cfg["fp32_filter"], cfg["knn_packet"], cfg["knn_bucket"])
+        pts = _host_f64(sorted_points, 3)
+        k = np.ascontiguousarray(keys, dtype=np.uint64)
+        b = np.ascontiguousarray(box, dtype=np.float64).reshape(12)
+        self.n = int(pts.shape[0])
+        assert k.shape[0] == self.n
+        check(self._L.oct_set_sorted_points(self._h, pts.ctypes.data, k.ctypes.data, self.n, b.ctypes.data, 0),
+              self._h, "oct_set_sorted_points")
+        self.box = b.copy()
+        info = OctTreeInfo()
+        check(self._L.oct_build(self._h, C.byref(info)), self._h, "oct_build")
+        self.n_leaf, self.n_internal, self.n_total = info.n_leaf, info.n_internal, info.n_total
+        self.max_depth_seen = info.max_depth_seen
+        return self
+
     def close(self):
         if getattr(self, "_h", None):
             self._L.oct_cloud_destroy(self._h)
@@ -217,6 +241,51 @@ class LinearOctree:
                                          offs.ctypes.data, idx.ctypes.data, idx.shape[0], C.byref(total), 0)
         check(st, h, "oct_radius_search")
         return offs, idx[: total.value]
+
+    def _axes(self, centers, radii_xyz):
+        r = np.ascontiguousarray(radii_xyz, dtype=np.float64)
+        if r.ndim == 1:
+            assert r.shape[0] == 3, "one (x, y, z) radius vector, or one per centre"
+            return r, 0
+        assert r.shape == (centers.shape[0], 3)
+        return r, 1
+
+    def radius_search_axes(self, centers, radii_xyz, kernel="cube", algo="neighborsPrune"):
+        """The Vector-radii overloads (cube and square kernels): ``radii_xyz`` is one (x, y, z) half-extent
+        vector or one per centre (nq, 3).  CSR result as radius_search."""
+        L, h = self._L, self._h
+        centers = _host_f64(centers, 3)
+        nq = centers.shape[0]
+        r, per = self._axes(centers, radii_xyz)
+        offs = np.zeros(nq + 1, np.uint64)
+        total = C.c_uint64(0)
+        st = L.oct_radius_search_axes(h, KERNELS[kernel], ALGOS[algo], centers.ctypes.data, nq, r.ctypes.data, per,
+                                      offs.ctypes.data, None, 0, C.byref(total), 0)
+        idx = np.zeros(max(1, total.value), np.uint32)
+        if st == capi.OCT_ERR_CAPACITY:
+            st = L.oct_radius_search_axes(h, KERNELS[kernel], ALGOS[algo], centers.ctypes.data, nq, r.ctypes.data,
+                                          per, offs.ctypes.data, idx.ctypes.data, idx.shape[0], C.byref(total), 0)
+        check(st, h, "oct_radius_search_axes")
+        return offs, idx[: total.value]
+
+    def neighborsStruct_axes(self, centers, radii_xyz, kernel="cube"):
+        """neighborsStruct with per-axis radii: (range offsets, pairs uint32[m, 2], numberOfPoints)."""
+        L, h = self._L, self._h
+        centers = _host_f64(centers, 3)
+        nq = centers.shape[0]
+        r, per = self._axes(centers, radii_xyz)
+        offs = np.zeros(nq + 1, np.uint64)
+        pts = np.zeros(nq, np.uint64)
+        total = C.c_uint64(0)
+        st = L.oct_struct_search_axes(h, KERNELS[kernel], centers.ctypes.data, nq, r.ctypes.data, per,
+                                      offs.ctypes.data, None, 0, C.byref(total), pts.ctypes.data, 0)
+        pairs = np.zeros((max(1, total.value), 2), np.uint32)
+        if st == capi.OCT_ERR_CAPACITY:
+            st = L.oct_struct_search_axes(h, KERNELS[kernel], centers.ctypes.data, nq, r.ctypes.data, per,
+                                          offs.ctypes.data, pairs.ctypes.data, total.value, C.byref(total),
+                                          pts.ctypes.data, 0)
+        check(st, h, "oct_struct_search_axes")
+        return offs, pairs[: total.value], pts
 
     def neighbors(self, centers, radius, kernel="square"):
         return self.radius_search(centers, radius, kernel, "neighbors")

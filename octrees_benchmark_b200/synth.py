@@ -14,9 +14,10 @@ seeded tiles stand in for them with the same shape of data:
 
 Everything is drawn from ``numpy.random.default_rng(seed)``, so a (n, tile,
 seed) triple always gives the same float64 (n, 3) array.  Query centres are
-cloud points picked uniformly at random, as the reference's SearchSet does
-(inc/benchmarking/search_set.hpp:23-44); its mt19937(42) stream is replaced by
-numpy's PCG64 with the same seed.
+cloud points picked uniformly at random: ``search_set`` reproduces the
+reference's SearchSet (inc/benchmarking/search_set.hpp:23-44) index for index
+(mt19937 seeded 42, uniform_int_distribution); ``query_indices`` draws other
+seeded sets from numpy's PCG64.
 """
 from __future__ import annotations
 
@@ -125,9 +126,102 @@ def large_tile_device(n: int = 500_000_000, tile_m: float = 10_000.0, seed: int 
 
 
 def query_indices(n_queries: int, cloud_size: int, seed: int = 42) -> np.ndarray:
-    """SearchSet-style random centre indices into the (sorted) cloud."""
+    """Random centre indices into the (sorted) cloud from numpy's PCG64 (seeded sets for the tests and the
+    bench's per-step batches); ``search_set`` gives the reference's own SearchSet stream."""
     rng = np.random.default_rng(seed)
     return rng.integers(0, cloud_size, n_queries, dtype=np.int64)
+
+
+class MT19937:
+    """The 32-bit Mersenne Twister of Matsumoto and Nishimura (1998), as
+    std::mt19937: seeded by the init_genrand recurrence, 624-word twist,
+    tempered 32-bit outputs.  The twist is vectorised in the three blocks
+    whose inputs are already final (i < 227 reads only old words; 227 <= i <
+    454 and 454 <= i < 623 read words the previous block rewrote; i = 623 reads
+    the new word 0)."""
+
+    N, M = 624, 397
+    MATRIX_A, UPPER, LOWER = 0x9908B0DF, 0x80000000, 0x7FFFFFFF
+
+    def __init__(self, seed: int = 5489):
+        mt = [int(seed) & 0xFFFFFFFF]
+        for i in range(1, self.N):
+            prev = mt[-1]
+            mt.append((1812433253 * (prev ^ (prev >> 30)) + i) & 0xFFFFFFFF)
+        self.mt = np.array(mt, np.uint64)
+        self.pos = self.N
+
+    def _twist_block(self, lo, hi, nxt, far):
+        y = (self.mt[lo:hi] & self.UPPER) | (nxt & self.LOWER)
+        self.mt[lo:hi] = far ^ (y >> np.uint64(1)) ^ np.where((y & np.uint64(1)) != 0, np.uint64(self.MATRIX_A),
+                                                              np.uint64(0))
+
+    def _twist(self):
+        mt, N, M = self.mt, self.N, self.M
+        self._twist_block(0, N - M, mt[1:N - M + 1].copy(), mt[M:N].copy())
+        self._twist_block(N - M, 2 * (N - M), mt[N - M + 1:2 * (N - M) + 1].copy(), mt[0:N - M].copy())
+        self._twist_block(2 * (N - M), N - 1, mt[2 * (N - M) + 1:N].copy(), mt[N - M:M - 1].copy())
+        self._twist_block(N - 1, N, mt[0:1].copy(), mt[M - 1:M].copy())
+        self.pos = 0
+
+    @staticmethod
+    def _temper(y):
+        y = y.copy()
+        y ^= y >> np.uint64(11)
+        y ^= (y << np.uint64(7)) & np.uint64(0x9D2C5680)
+        y ^= (y << np.uint64(15)) & np.uint64(0xEFC60000)
+        y ^= y >> np.uint64(18)
+        return y & np.uint64(0xFFFFFFFF)
+
+    def _peek(self, n: int) -> np.ndarray:
+        """Up to n next outputs from the current state block, without consuming them."""
+        if self.pos >= self.N:
+            self._twist()
+        return self._temper(self.mt[self.pos:self.pos + min(n, self.N - self.pos)])
+
+    def next_u32(self, n: int) -> np.ndarray:
+        out = []
+        while n > 0:
+            y = self._peek(n)
+            self.pos += len(y)
+            n -= len(y)
+            out.append(y)
+        return np.concatenate(out) if out else np.empty(0, np.uint64)
+
+    def uniform_int(self, n: int, lo: int, hi: int) -> np.ndarray:
+        """n draws of std::uniform_int_distribution(lo, hi) with a 32-bit engine and a range below 2^32:
+        Lemire's nearly divisionless method (2019) - the 64-bit product of a draw and the range, its high
+        word the value, a draw rejected while its low word is below 2^32 mod range."""
+        rng = hi - lo + 1
+        assert 0 < rng < (1 << 32)
+        thresh = np.uint64(((1 << 32) - rng) % rng)
+        parts, got = [], 0
+        while got < n:
+            x = self._peek(n - got)
+            prod = x * np.uint64(rng)
+            ok = (prod & np.uint64(0xFFFFFFFF)) >= thresh
+            take = len(x) if ok.all() else int(np.argmin(ok))  # accepted draws before the first rejection
+            parts.append(prod[:take] >> np.uint64(32))
+            got += take
+            self.pos += take if take == len(x) else take + 1  # a rejected draw is consumed too
+        out = np.concatenate(parts) if parts else np.empty(0, np.uint64)
+        return (out + np.uint64(lo)).astype(np.int64)
+
+
+def search_set(n_queries: int, cloud_size: int, sequential: bool = False, repeat: int = 0,
+               seed: int = 42) -> np.ndarray:
+    """The reference's SearchSet centre indices (inc/benchmarking/search_set.hpp:23-44): one mt19937 seeded
+    42 over all repeats; each repeat draws n indices uniform in [0, cloud_size - 1], or with ``sequential``
+    one start uniform in [0, cloud_size - n] and the slice after it.  Returns repeat ``repeat``'s row."""
+    g = MT19937(seed)
+    row = None
+    for _ in range(repeat + 1):
+        if sequential:
+            start = int(g.uniform_int(1, 0, cloud_size - n_queries)[0])
+            row = np.arange(start, start + n_queries, dtype=np.int64)
+        else:
+            row = g.uniform_int(n_queries, 0, cloud_size - 1)
+    return row
 
 
 # The workloads the benchmark and the parity tests use, by name.

@@ -3,7 +3,7 @@
 * ``Port`` loads oracle/_build/liboctree_oracle.so, the plain-C restatement of
   the reference algorithm (octree_oracle.c).
 * ``Reference`` loads oracle/_ref/libref_octree.so, the UNMODIFIED reference
-  headers compiled by ``make -C oracle ref`` behind a thin C bridge
+  headers compiled by ``make -C oracle ref REFERENCE=<dir>`` behind a thin C bridge
   (ref_bridge.cpp).  It exists wherever it was built (it is git-ignored but
   travels with the working tree); ``reference_available()`` says whether it is.
 
@@ -37,10 +37,11 @@ def build_port() -> str:
     return PORT_SO
 
 
-def build_reference() -> str | None:
-    """Compile the reference bridge when the reference sources are present."""
-    ref = os.environ.get("OCTREE_REFERENCE_DIR", "/root/reference")
-    if not os.path.isdir(os.path.join(ref, "inc")):
+def build_reference(reference_dir: str | None = None) -> str | None:
+    """Compile the reference bridge from the reference checkout ``reference_dir``
+    (else $OCTREE_REFERENCE_DIR).  Without one, keeps a prebuilt library."""
+    ref = reference_dir or os.environ.get("OCTREE_REFERENCE_DIR")
+    if not ref or not os.path.isdir(os.path.join(ref, "inc")):
         return REF_SO if os.path.exists(REF_SO) else None
     subprocess.run(["make", "-s", "-C", HERE, "ref", f"REFERENCE={ref}"], check=True)
     return REF_SO
@@ -223,7 +224,7 @@ class Reference:
     def lib():
         if Reference._lib is None:
             if not os.path.exists(REF_SO):
-                raise RuntimeError("oracle/_ref/libref_octree.so is not built (make -C oracle ref)")
+                raise RuntimeError("oracle/_ref/libref_octree.so is not built (make -C oracle ref REFERENCE=<dir>)")
             L = C.CDLL(REF_SO)
             L.refo_build.argtypes = [C.c_int, _f64p, C.c_uint64, C.c_uint64, C.c_int]
             L.refo_build.restype = C.c_void_p
@@ -248,6 +249,11 @@ class Reference:
             L.refo_time_knn.argtypes = [C.c_void_p, _f64p, C.c_uint64, C.c_uint64, C.c_int,
                                         C.POINTER(C.c_double)]
             L.refo_time_knn.restype = C.c_double
+            L.refo_radius_hash.argtypes = [C.c_void_p, C.c_int, C.c_int, _f64p, C.c_uint64, C.c_double, C.c_int,
+                                           _u64p, _u64p]
+            L.refo_search_set.argtypes = [C.c_uint64, C.c_uint64, C.c_int, C.c_int, C.c_uint64, _u64p]
+            L.refo_radius_axes.argtypes = [C.c_void_p, C.c_int, C.c_int, _f64p, C.c_uint64, _f64p, C.c_int]
+            L.refo_radius_axes.restype = C.c_uint64
             L.refo_max_threads.restype = C.c_int
             L.refo_anchor.argtypes = [C.c_double] * 3
             L.refo_anchor.restype = C.c_uint64
@@ -308,6 +314,22 @@ class Reference:
         self.L.refo_radius_fetch(self.h, offs, idx)
         return offs, idx
 
+    def radius_axes(self, kernel, algo, centers, radii_xyz, threads=0):
+        """The Vector-radii overloads (square 2 / cube 3): CSR of indices in the reference's emission order,
+        and for algo 3 the ranges as well: (offs, idx, range_offs, pairs)."""
+        centers = _f64(centers)
+        nq = len(centers)
+        r3 = _f64(np.broadcast_to(np.asarray(radii_xyz, np.float64), (nq, 3)))
+        total = self.L.refo_radius_axes(self.h, kernel, algo, centers.reshape(-1), nq, r3.reshape(-1), threads)
+        offs = np.zeros(nq + 1, np.uint64)
+        idx = np.zeros(int(total), np.uint64)
+        self.L.refo_radius_fetch(self.h, offs, idx)
+        m = self.L.refo_struct_range_total(self.h)
+        ro = np.zeros(nq + 1, np.uint64)
+        pairs = np.zeros(2 * int(m), np.uint64)
+        self.L.refo_struct_ranges_fetch(self.h, ro, pairs)
+        return offs, idx, ro, pairs.reshape(-1, 2)
+
     def struct_ranges(self, kernel, centers, radii, threads=0):
         """ranges of neighborsStruct in the reference's emission order"""
         self.radius(kernel, 3, centers, radii, threads)
@@ -339,6 +361,15 @@ class Reference:
         self.L.refo_knn(self.h, centers.reshape(-1), nq, k, idx, d2, cnt, threads)
         return idx.reshape(nq, k), d2.reshape(nq, k), cnt
 
+    def radius_hash(self, kernel, algo, centers, radius, threads=0):
+        """Per-query neighbour counts and order-independent set hashes (sum of splitmix64(index) mod 2^64)."""
+        centers = _f64(centers)
+        nq = len(centers)
+        counts = np.zeros(nq, np.uint64)
+        hashes = np.zeros(nq, np.uint64)
+        self.L.refo_radius_hash(self.h, kernel, algo, centers.reshape(-1), nq, float(radius), threads, counts, hashes)
+        return counts, hashes
+
     def time_radius(self, kernel, algo, centers, radius, threads=0):
         tot = C.c_uint64()
         centers = _f64(centers)
@@ -365,6 +396,14 @@ class Reference:
         out = np.zeros(3, np.uint64)
         Reference.lib().refo_decode(encoder, key, out)
         return tuple(int(v) for v in out)
+
+    @staticmethod
+    def search_set(n, cloud_size, sequential=False, all_points=False, repeats=1):
+        """The reference's SearchSet indices, (repeats, n) (n = cloud_size with all_points)."""
+        m = cloud_size if all_points else n
+        out = np.zeros(repeats * m, np.uint64)
+        Reference.lib().refo_search_set(n, cloud_size, int(bool(sequential)), int(bool(all_points)), repeats, out)
+        return out.reshape(repeats, m)
 
     @staticmethod
     def max_threads():

@@ -18,6 +18,7 @@
 #include <optional>
 #include <vector>
 
+#include "benchmarking/search_set.hpp"
 #include "encoding/point_encoder_factory.hpp"
 #include "structures/linear_octree.hpp"
 
@@ -117,6 +118,22 @@ size_t count_dispatch(const ExposedOctree& t, int kernel, int algo, const Point&
         case 1: return count_one<Kernel_t::sphere>(t, algo, c, r);
         case 2: return count_one<Kernel_t::square>(t, algo, c, r);
         default: return count_one<Kernel_t::cube>(t, algo, c, r);
+    }
+}
+
+template <Kernel_t K>
+void axes_one(const ExposedOctree& t, int algo, const Point& c, const Vector& r, std::vector<size_t>& idx,
+              std::vector<std::pair<size_t, size_t>>& rng) {
+    if (algo == 1) {
+        idx = t.neighbors<K>(c, r);
+    } else if (algo == 2) {
+        idx = t.neighborsPrune<K>(c, r);
+    } else {
+        auto s = t.neighborsStruct<K>(c, r);
+        rng = s.ranges;
+        idx.clear();
+        for (auto& pr : s.ranges)
+            for (size_t i = pr.first; i < pr.second; ++i) idx.push_back(i);
     }
 }
 
@@ -248,6 +265,27 @@ void refo_radius_fetch(void* h, uint64_t* offsets, uint64_t* idx) {
     offsets[rc->res_idx.size()] = o;
 }
 
+// The Vector-radii overloads (linear_octree.hpp:1044-1048, 1056-1060, 1069-1074) over nq centers with
+// per-query (rx, ry, rz) radii (nq x 3); kernel 2 square or 3 cube, algo as refo_radius.  Results stay
+// in the handle like refo_radius's (refo_radius_fetch, refo_struct_ranges_fetch).
+uint64_t refo_radius_axes(void* h, int kernel, int algo, const double* centers, uint64_t nq, const double* radii3,
+                          int threads) {
+    set_threads(threads);
+    auto* rc = static_cast<RefCloud*>(h);
+    rc->res_idx.assign(nq, {});
+    rc->res_ranges.assign(nq, {});
+    #pragma omp parallel for schedule(runtime)
+    for (int64_t q = 0; q < (int64_t)nq; ++q) {
+        Point c(centers[3 * q], centers[3 * q + 1], centers[3 * q + 2]);
+        Vector r(radii3[3 * q], radii3[3 * q + 1], radii3[3 * q + 2]);
+        if (kernel == 2) axes_one<Kernel_t::square>(*rc->tree, algo, c, r, rc->res_idx[q], rc->res_ranges[q]);
+        else axes_one<Kernel_t::cube>(*rc->tree, algo, c, r, rc->res_idx[q], rc->res_ranges[q]);
+    }
+    uint64_t total = 0;
+    for (auto& v : rc->res_idx) total += v.size();
+    return total;
+}
+
 // neighborsApprox over nq centers; the ranges stay in the handle (refo_struct_ranges_fetch).
 // Returns the number of ranges.
 uint64_t refo_approx(void* h, int kernel, const double* centers, uint64_t nq, const double* radii, double tol,
@@ -300,6 +338,38 @@ void refo_knn(void* h, const double* centers, uint64_t nq, uint64_t k, uint64_t*
     }
 }
 
+// splitmix64's output function: the per-index term of the set hash below.
+static inline uint64_t mix64(uint64_t x) {
+    uint64_t z = x + 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+// Radius search over nq centers with one radius, kept as a per-query count and
+// an order-independent hash of the neighbour index set (the sum of mix64 of
+// every index, modulo 2^64), so that sweeps over whole clouds need no result
+// storage.  Same kernels and algos as refo_radius.
+void refo_radius_hash(void* h, int kernel, int algo, const double* centers, uint64_t nq, double radius, int threads,
+                      uint64_t* counts, uint64_t* hashes) {
+    set_threads(threads);
+    auto* rc = static_cast<RefCloud*>(h);
+    #pragma omp parallel
+    {
+        std::vector<size_t> idx;
+        std::vector<std::pair<size_t, size_t>> rng;
+        #pragma omp for schedule(runtime)
+        for (int64_t q = 0; q < (int64_t)nq; ++q) {
+            Point c(centers[3 * q], centers[3 * q + 1], centers[3 * q + 2]);
+            radius_dispatch(*rc->tree, kernel, algo, c, radius, idx, rng);
+            uint64_t s = 0;
+            for (size_t v : idx) s += mix64((uint64_t)v);
+            counts[q] = idx.size();
+            hashes[q] = s;
+        }
+    }
+}
+
 // ---- timed loops for the CPU baseline (steady_clock wall time, seconds) ----
 
 double refo_time_radius(void* h, int kernel, int algo, const double* centers, uint64_t nq, double radius,
@@ -340,6 +410,18 @@ double refo_time_knn(void* h, const double* centers, uint64_t nq, uint64_t k, in
 }
 
 int refo_max_threads() { return omp_get_max_threads(); }
+
+// The reference's SearchSet (inc/benchmarking/search_set.hpp:23-44): `repeats`
+// rows of n centre indices into a cloud of cloud_size points, random
+// (mt19937 seeded 42, uniform_int_distribution) or a sequential slice.
+// out: repeats x n' indices, n' = cloud_size when `all` is set, else n.
+void refo_search_set(uint64_t n, uint64_t cloud_size, int sequential, int all, uint64_t repeats, uint64_t* out) {
+    mainOptions.repeats = (size_t)repeats;
+    SearchSet s((size_t)n, (size_t)cloud_size, sequential != 0, all != 0);
+    uint64_t o = 0;
+    for (const auto& row : s.searchPoints)
+        for (size_t v : row) out[o++] = v;
+}
 
 // PointEncoder::getAnchorCoords (point_encoder.hpp:37-49) on one axis value,
 // with the box given by its center and radii (Box(center, radii), box.hpp:17).

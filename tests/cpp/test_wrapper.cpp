@@ -7,6 +7,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <optional>
 #include <random>
 #include <vector>
 
@@ -219,6 +220,85 @@ void test_encoders_cpp() {  // test_encoders.cpp:29-64
     }
 }
 
+struct Vec {  // the reference's Vector: per-axis radii
+    double x, y, z;
+    double getX() const { return x; }
+    double getY() const { return y; }
+    double getZ() const { return z; }
+};
+
+struct Meta {  // stands in for PointMetadata: it travels with its point
+    size_t tag;
+};
+
+void test_example_cpp() {  // examples/example.cpp:14-47, the same calls in namespace octree_b200
+    using namespace octree_b200;
+    PointsAoS points;
+    points.push_back(Point(1.2, 3.4, 5.6));
+    points.push_back(Point(7.8, 9.0, 1.2));
+    points.push_back(Point(3.4, 5.6, 7.8));
+    points.push_back(Point(9.0, 1.2, 3.4));
+    std::optional<std::vector<Meta>> metadata = std::nullopt;
+    PointEncoding::MortonEncoder3D enc;
+    auto [codes, box] = enc.sortPoints(points, metadata);
+    LinearOctree octree(points, codes, box, enc);
+    size_t k = 2;
+    std::vector<size_t> indexes(k);
+    std::vector<double> distances(k);
+    Point searchPoint(5.0, 5.0, 5.0);
+    EXPECT(octree.knn(searchPoint, k, indexes, distances) == 2);
+    for (size_t i = 0; i < k; ++i) EXPECT(std::fabs(distances[i] - sq(points[indexes[i]], searchPoint)) < 1e-12);
+    EXPECT(distances[0] <= distances[1]);
+}
+
+void test_two_step_equals_one_step_cpp() {
+    // sortPoints + LinearOctree(points, codes, box, enc) (with metadata moved along) against the one-step octree
+    using namespace octree_b200;
+    for (EncoderType et : {MORTON_ENCODER_3D, HILBERT_ENCODER_3D}) {
+        PointsAoS a, b;
+        std::mt19937 gen(7);
+        std::uniform_real_distribution<> dis(0, 50);
+        for (int i = 0; i < 3000; ++i) {
+            Point p(dis(gen), dis(gen), dis(gen) * 0.2);
+            a.push_back(p);
+            b.push_back(p);
+        }
+        std::optional<std::vector<Meta>> meta = std::vector<Meta>();
+        for (size_t i = 0; i < a.size(); ++i) meta->push_back(Meta{i});
+        mainOptions.maxPointsLeaf = 16;
+        auto& enc = PointEncoding::getEncoder(et);
+        auto [codes, box] = enc.sortPoints(a, meta);
+        LinearOctree two(a, codes, box, enc);
+        std::vector<uint64_t> codes1;
+        Oct one(b, codes1, et == MORTON_ENCODER_3D ? Encoder::morton : Encoder::hilbert, 16);
+        mainOptions.maxPointsLeaf = 128;
+        EXPECT(codes == codes1);
+        EXPECT(two.nTotal() == one.nTotal() && two.nLeaf() == one.nLeaf());
+        for (size_t i = 0; i < a.size(); ++i) EXPECT(a[i].id() == b[i].id() && (*meta)[i].tag == a[i].id());
+        for (int q = 0; q < 50; ++q) {
+            const Point& c = a[(q * 61) % a.size()];
+            auto r1 = two.neighborsPrune<Kernel_t::sphere>(c, 3.0);
+            auto r2 = one.neighborsPrune<Kernel_t::sphere>(c, 3.0);
+            std::sort(r1.begin(), r1.end());
+            std::sort(r2.begin(), r2.end());
+            EXPECT(r1 == r2);
+            // Vector radii: cube and square against brute force (closed intervals)
+            const Vec rv{2.5, 0.7, 1.4};
+            auto cu = two.neighborsPrune<Kernel_t::cube>(c, rv);
+            auto sqr = two.neighbors<Kernel_t::square>(c, rv);
+            auto st = two.neighborsStruct<Kernel_t::cube>(c, rv);
+            size_t n3 = 0, n2 = 0;
+            for (size_t i = 0; i < a.size(); ++i) {
+                const bool in2 = a[i].getX() >= c.getX() - rv.x && a[i].getX() <= c.getX() + rv.x &&
+                                 a[i].getY() >= c.getY() - rv.y && a[i].getY() <= c.getY() + rv.y;
+                n2 += in2;
+                n3 += in2 && a[i].getZ() >= c.getZ() - rv.z && a[i].getZ() <= c.getZ() + rv.z;
+            }
+            EXPECT(cu.size() == n3 && st.size() == n3 && sqr.size() == n2);
+        }
+    }
+}
+
 }  // namespace
 
 int main() {
@@ -227,6 +307,8 @@ int main() {
         test_octree_advanced_cpp();
         test_complex_cpp();
         test_encoders_cpp();
+        test_example_cpp();
+        test_two_step_equals_one_step_cpp();
     } catch (const octree_b200::Error& e) {
         std::fprintf(stderr, "octree_b200::Error status %d: %s\n", e.status(), e.what());
         return 2;

@@ -171,3 +171,63 @@ def knn_diffs(idx_g, d2_g, cnt_g, idx_r, d2_r, cnt_r, xyz, centers, max_tie_chec
             bad[q] = True
     bad[tie_rows[max_tie_checks:]] = True  # not checked: counted as differences
     return int(bad.sum()), max_err, checked
+
+
+def ranges_diffs(offs_a, pairs_a, offs_b, pairs_b) -> int:
+    """Number of queries whose neighborsStruct ranges differ, each query's
+    ranges compared as a sorted list of (first, last) pairs."""
+    offs_a = np.asarray(offs_a, np.int64)
+    offs_b = np.asarray(offs_b, np.int64)
+    pa = np.asarray(pairs_a, np.int64).reshape(-1, 2)[: offs_a[-1]]
+    pb = np.asarray(pairs_b, np.int64).reshape(-1, 2)[: offs_b[-1]]
+    ca, cb = np.diff(offs_a), np.diff(offs_b)
+    same = ca == cb
+    bad = ~same
+    seg = np.repeat(np.arange(len(ca)), np.where(same, ca, 0))
+    va, vb = pa[np.repeat(same, ca)], pb[np.repeat(same, cb)]
+    sa = va[np.lexsort((va[:, 1], va[:, 0], seg))]
+    sb = vb[np.lexsort((vb[:, 1], vb[:, 0], seg))]
+    diff = (sa != sb).any(axis=1)
+    if diff.any():
+        bad[np.unique(seg[diff])] = True
+    return int(bad.sum())
+
+
+MIX64_C = (0x9E3779B97F4A7C15, 0xBF58476D1CE4E5B9, 0x94D049BB133111EB)
+
+
+def mix64_np(v):
+    """splitmix64's output function on uint64 values (the set-hash term of the
+    reference bridge's refo_radius_hash)."""
+    z = np.asarray(v, np.uint64) + np.uint64(MIX64_C[0])
+    z = (z ^ (z >> np.uint64(30))) * np.uint64(MIX64_C[1])
+    z = (z ^ (z >> np.uint64(27))) * np.uint64(MIX64_C[2])
+    return z ^ (z >> np.uint64(31))
+
+
+def mix64_torch(t):
+    """mix64_np on an int64 torch tensor (two's complement wrap-around, logical
+    right shifts by masking)."""
+    def s64(c):
+        return c - (1 << 64) if c >= (1 << 63) else c
+
+    def srl(z, s):
+        return (z >> s) & ((1 << (64 - s)) - 1)
+
+    import torch
+
+    z = t.to(torch.int64) + s64(MIX64_C[0])
+    z = (z ^ srl(z, 30)) * s64(MIX64_C[1])
+    z = (z ^ srl(z, 27)) * s64(MIX64_C[2])
+    return z ^ srl(z, 31)
+
+
+def csr_count_hash_torch(offs, idx):
+    """Per-query (count, sum of mix64(index) mod 2^64) of a device CSR result,
+    as int64 tensors (the hash's bits are those of the uint64 sum)."""
+    import torch
+
+    offs = offs.to(torch.int64)
+    h = mix64_torch(idx[: int(offs[-1].item())].to(torch.int64))
+    cs = torch.cat([torch.zeros(1, dtype=torch.int64, device=h.device), torch.cumsum(h, 0)])
+    return offs[1:] - offs[:-1], cs[offs[1:]] - cs[offs[:-1]]
