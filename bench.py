@@ -520,7 +520,7 @@ def run_serving(args, dev):
     wl = ServingWorkload(device=dev, seconds=args.serve_seconds)
     clocks = ClockSampler(dev)
     clocks.start()
-    srv = Server(device=dev)
+    srv = Server(device=dev, slots=args.serve_slots, max_batch_queries=args.serve_max_batch)
     try:
         batched = replay(wl, srv, drain_s=args.serve_drain)
     finally:
@@ -617,7 +617,7 @@ def run_b200(args, rank, world, local_rank):
 
     # (packet, fp32_filter, lanes, kNN in groups of 4 queries per warp)
     SEARCH_PATHS = {"plain": (0, 0, args.radius_group, 0), "packet": (1, 0, 8, 1), "packet_fp32": (1, 1, 8, 1),
-                    "knn_per_query": (1, 0, 8, 0), "engine": (1, 0, 8, 1)}
+                    "knn_per_query": (1, 0, 8, 0), "engine": (1, 0, 8, 1), "engine_fp32": (1, 1, 8, 1)}
 
     # the batched engine: both request sets of a step in one graph launch (kNN beside the radius search)
     from types import SimpleNamespace
@@ -639,6 +639,8 @@ def run_b200(args, rank, world, local_rank):
         return None, ms, 0.0, int(places[0].n_results)
 
     def configure(name):
+        if name.startswith("engine"):  # the batched engine: its autotuned configuration, FP32 filter on or off
+            eng.set_config(**dict(eng_cfg, fp32_filter=int(name == "engine_fp32")))
         packet, fp32, lanes, knn_packet = SEARCH_PATHS[name]
         cfg = capi.OctSearchConfig(packet, fp32, lanes, knn_packet, args.knn_bucket)
         capi.check(L.oct_set_search_config(h, C.byref(cfg)), h, "search config")
@@ -666,7 +668,7 @@ def run_b200(args, rank, world, local_rank):
     run_paths = [p_ for p_ in SEARCH_PATHS if not args.paths or p_ in args.paths.split(",") or p_ == args.search]
     for name in run_paths:
         configure(name)
-        run_step = engine_step if name == "engine" else step
+        run_step = engine_step if name.startswith("engine") else step
         for b in range(args.warmup):
             run_step(b)
         if world > 1:
@@ -674,6 +676,8 @@ def run_b200(args, rank, world, local_rank):
         torch.cuda.synchronize()
         L.oct_search_stats(h, None, None, 1)
         L.oct_knn_filter_stats(h, None, None, None, 1)
+        L.oct_search_timing(h, 1)  # CUDA events around the search kernels themselves (single-cloud paths)
+        L.oct_search_kernel_times(h, None, None, None, None, 1)
         t_count = t_search = t_knn = 0.0
         nbrs = 0
         for s in range(args.steps):
@@ -683,6 +687,9 @@ def run_b200(args, rank, world, local_rank):
             t_knn += c_
             nbrs += tt
         torch.cuda.synchronize()
+        kr_ms, kr_n, kk_ms, kk_n = C.c_double(), C.c_uint64(), C.c_double(), C.c_uint64()
+        L.oct_search_kernel_times(h, C.byref(kr_ms), C.byref(kr_n), C.byref(kk_ms), C.byref(kk_n), 1)
+        L.oct_search_timing(h, 0)
         tests, retests = C.c_uint64(), C.c_uint64()
         L.oct_search_stats(h, C.byref(tests), C.byref(retests), 1)
         k_tests, k_f64, k_band = C.c_uint64(), C.c_uint64(), C.c_uint64()
@@ -693,20 +700,25 @@ def run_b200(args, rank, world, local_rank):
             torch.distributed.barrier()
             torch.distributed.all_reduce(tmax, op=torch.distributed.ReduceOp.MAX)
         step_ms, rad_ms, knn_ms = (float(v) for v in tmax.tolist())
-        if name == "engine":  # radius and kNN overlap: one device time for the whole batch
+        if name.startswith("engine"):  # radius and kNN overlap: one device time for the whole batch
             rad_ms = knn_ms = float("nan")
         paths[name] = {"ms_per_step": step_ms, "qps": world * (Q_RADIUS + Q_KNN) / (step_ms / 1e3),
                        "radius_qps": world * Q_RADIUS / (rad_ms / 1e3) if rad_ms == rad_ms else None,
                        "knn_qps": world * Q_KNN / (knn_ms / 1e3) if knn_ms == knn_ms else None,
                        "radius_ms": rad_ms if rad_ms == rad_ms else None, "knn_ms": knn_ms if knn_ms == knn_ms else None,
-                       "radius_count_only_ms": t_count / args.steps if name != "engine" else None,
+                       "radius_count_only_ms": t_count / args.steps if not name.startswith("engine") else None,
                        "avg_neighbours": nbrs / args.steps / Q_RADIUS, "nbrs_per_step": nbrs / args.steps,
                        "point_tests": tests.value, "fp64_retests": retests.value,
                        "band_hit_fraction": (retests.value / tests.value) if tests.value else None,
                        # the group kNN's FP32 filter: FP32 point tests, the FP64 tests they leave
                        # (candidates + band), band hits (FP64 tests of points that then fail)
                        "knn_fp32_tests": k_tests.value, "knn_fp64_tests": k_f64.value,
-                       "knn_band_hit_fraction": (k_band.value / k_tests.value) if k_tests.value else None}
+                       "knn_band_hit_fraction": (k_band.value / k_tests.value) if k_tests.value else None,
+                       # device time of the search kernels alone (CUDA events on the cloud's stream around each
+                       # k_radius_packet / k_knn_group launch), per launch; every launch answers one step's queries
+                       "kernel_ms": {"k_radius_packet": kr_ms.value / kr_n.value if kr_n.value else None,
+                                     "k_knn_group": kk_ms.value / kk_n.value if kk_n.value else None,
+                                     "launches": [kr_n.value, kk_n.value]}}
     clk = clocks.stop()
     chosen = paths[args.search]
     configure(args.search)
@@ -846,26 +858,30 @@ def run_b200(args, rank, world, local_rank):
     knn_bytes = (24 + 36 * KNN_K) * Q_KNN
     # per-kernel times: the engine runs the packet path's kernels side by side, so they are timed there alone
     kpath = args.search if chosen["radius_ms"] is not None else ("packet" if "packet" in paths else args.search)
-    rad_ms, knn_ms = paths[kpath]["radius_ms"], paths[kpath]["knn_ms"]
+    km = paths[kpath].get("kernel_ms") or {}
+    rad_ms, knn_ms = km.get("k_radius_packet"), km.get("k_knn_group")
     if rad_ms is None or knn_ms is None:  # only the engine path ran: its kernels overlap, no per-kernel time
         rad_ms = knn_ms = float("nan")
-    # each time is the whole library call on the cloud's stream (CUDA events): the query ordering plus
-    # the search kernels it launches
-    rad = {"kernel": f"radius neighborsPrune sphere, {kpath} path (query order + k_radius_packet one pass + "
-                     "scan + k_chunk_compact)", "ms": rad_ms, "achieved": rad_bytes / (rad_ms / 1e3) / 1e9}
-    knn = {"kernel": f"kNN k=50, {kpath} path (query order + k_knn_group + fallback k_knn_reg)", "ms": knn_ms,
-           "achieved": knn_bytes / (knn_ms / 1e3) / 1e9}
+    # each time is the kernel's own launch on the cloud's stream (CUDA events around the launch), averaged over
+    # the timed steps' launches; one launch answers one step's queries of its kind
+    rad = {"kernel": f"k_radius_packet (neighborsPrune sphere r={RADIUS}, one pass, {kpath} path)", "ms": rad_ms,
+           "achieved": rad_bytes / (rad_ms / 1e3) / 1e9,
+           "call_ms": paths[kpath]["radius_ms"]}
+    knn = {"kernel": f"k_knn_group (k={KNN_K}, {kpath} path)", "ms": knn_ms,
+           "achieved": knn_bytes / (knn_ms / 1e3) / 1e9, "call_ms": paths[kpath]["knn_ms"]}
     knn["traffic"] = KNN_DRAM_BYTES_PER_QUERY * Q_KNN
     rad["traffic"] = RADIUS_DRAM_BYTES_PER_QUERY * Q_RADIUS
     dom = knn if knn_ms >= rad_ms else rad
     roofline = {"bound": "hbm", "kernel": dom["kernel"], "achieved": dom["achieved"], "peak": peak, "unit": "GB/s",
                 "frac": dom["achieved"] / peak, "peak_source": peak_kind, "traffic": dom["traffic"],
+                "ms_per_launch": dom["ms"], "call_ms": dom["call_ms"],
                 "traffic_source": "DRAM read + write bytes per query of the search kernel from one ncu capture "
                                   "(6M-point tile at the same density, 200k queries), times this step's queries",
                 "algorithmic_bytes": "radius 24 + 28 per neighbour; kNN 24 + 36 k per query",
                 "other": {"kernel": (rad if dom is knn else knn)["kernel"],
                           "achieved": (rad if dom is knn else knn)["achieved"],
-                          "frac": (rad if dom is knn else knn)["achieved"] / peak}}
+                          "frac": (rad if dom is knn else knn)["achieved"] / peak,
+                          "ms_per_launch": (rad if dom is knn else knn)["ms"]}}
     build_bytes = BUILD_BYTES_PER_POINT * N_POINTS + BUILD_BYTES_PER_NODE * info.n_total
     build = {"ms": 1e3 * build_s, "mpts_s": N_POINTS / build_s / 1e6, "gbs": build_bytes / build_s / 1e9,
              "frac": build_bytes / build_s / 1e9 / peak, "nodes": info.n_total, "leaves": info.n_leaf,
@@ -992,6 +1008,8 @@ def main():
     ap.add_argument("--serve-seconds", type=float, default=60.0, help="length of the serving request stream")
     ap.add_argument("--serve-drain", type=float, default=10.0,
                     help="seconds each server may take after the stream ends before it is stopped")
+    ap.add_argument("--serve-slots", type=int, default=3, help="batches the serving scheduler keeps in flight")
+    ap.add_argument("--serve-max-batch", type=int, default=4 << 20, help="centres per serving batch at most")
     ap.add_argument("--large", action="store_true", help="also run the 500M-point skewed cloud (not in the default run)")
     ap.add_argument("--large-points", type=int, default=500_000_000)
     ap.add_argument("--large-queries", type=int, default=10_000_000)

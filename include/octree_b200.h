@@ -166,6 +166,16 @@ int oct_search_stats(oct_cloud cloud, uint64_t* point_tests, uint64_t* fp64_rete
 int oct_knn_filter_stats(oct_cloud cloud, uint64_t* point_tests, uint64_t* fp64_tests, uint64_t* band_hits,
                          int reset);
 
+/* Device timing of the main search kernel of each call on this cloud: with
+ * timing on, CUDA events on the cloud's stream bracket the packet radius
+ * kernel (k_radius_packet) and the group kNN kernel (k_knn_group) of every
+ * call; oct_search_kernel_times waits for the stream and returns the summed
+ * milliseconds and launch counts since the last reset (any pointer may be
+ * NULL).  For roofline measurements; no reference counterpart. */
+int oct_search_timing(oct_cloud cloud, int enable);
+int oct_search_kernel_times(oct_cloud cloud, double* radius_ms, uint64_t* radius_launches, double* knn_ms,
+                            uint64_t* knn_launches, int reset);
+
 /* Upload n points (xyz AoS).  Replaces filling the reference's PointsAoS
  * container (inc/geometry/point_containers.hpp:32-65). */
 int oct_set_points(oct_cloud cloud, const double* xyz, uint64_t n, uint32_t flags);

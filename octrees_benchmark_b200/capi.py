@@ -120,6 +120,9 @@ SIGNATURES = {
     "oct_radius_search": ([_vp, _int, _int, _vp, _u64, _vp, _dbl, _vp, _vp, _u64, C.POINTER(_u64), _u32], _int),
     "oct_radius_count": ([_vp, _int, _int, _vp, _u64, _vp, _dbl, _vp, _u32], _int),
     "oct_struct_search": ([_vp, _int, _vp, _u64, _vp, _dbl, _vp, _vp, _u64, C.POINTER(_u64), _vp, _u32], _int),
+    "oct_search_timing": ([_vp, _int], _int),
+    "oct_search_kernel_times": ([_vp, C.POINTER(_dbl), C.POINTER(_u64), C.POINTER(_dbl), C.POINTER(_u64), _int],
+                                _int),
     "oct_set_sorted_points": ([_vp, _vp, _vp, _u64, _vp, _u32], _int),
     "oct_radius_search_axes": ([_vp, _int, _int, _vp, _u64, _vp, _int, _vp, _vp, _u64, C.POINTER(_u64), _u32], _int),
     "oct_struct_search_axes": ([_vp, _int, _vp, _u64, _vp, _int, _vp, _vp, _u64, C.POINTER(_u64), _vp, _u32], _int),

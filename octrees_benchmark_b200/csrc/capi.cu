@@ -312,6 +312,9 @@ int oct_cloud_destroy(oct_cloud h) {
                           &c.ck_pool, &c.ck_next, &c.ck_first, &c.ck_ctr, &c.knn_fb, &c.knn_heads, &c.crel, &c.q_axes};
         for (DevBuf* b : bufs) b->release();
         if (c.pinned) cudaFreeHost(c.pinned);
+        for (auto& v : c.ev_pend)
+            for (auto& pr : v) c.ev_free.insert(c.ev_free.end(), {pr.first, pr.second});
+        for (cudaEvent_t ev : c.ev_free) cudaEventDestroy(ev);
         if (c.own_stream && c.stream) cudaStreamDestroy(c.stream);
     }
     delete h;
@@ -911,6 +914,42 @@ int stage_axes(Cloud& c, int kernel, const double* radii_xyz, uint64_t nq, int p
     return stage_in(c, c.q_axes, radii_xyz, per_query ? 3 * nq : 3, dev, out);
 }
 }  // namespace
+
+int oct_search_timing(oct_cloud h, int enable) {
+    if (!h) return OCT_ERR_INVALID_ARG;
+    h->c.time_kernels = enable != 0;
+    return OCT_OK;
+}
+
+int oct_search_kernel_times(oct_cloud h, double* radius_ms, uint64_t* radius_launches, double* knn_ms,
+                            uint64_t* knn_launches, int reset) {
+    if (!h) return OCT_ERR_INVALID_ARG;
+    Cloud& c = h->c;
+    DeviceGuard g(c.device);
+    CK(cudaStreamSynchronize(c.stream));
+    for (int kind = 0; kind < 2; ++kind) {
+        for (auto& pr : c.ev_pend[kind]) {
+            float ms = 0.f;
+            if (cudaEventElapsedTime(&ms, pr.first, pr.second) == cudaSuccess) {
+                c.kernel_ms[kind] += ms;
+                ++c.kernel_launches[kind];
+            }
+            cudaGetLastError();
+            c.ev_free.push_back(pr.first);
+            c.ev_free.push_back(pr.second);
+        }
+        c.ev_pend[kind].clear();
+    }
+    if (radius_ms) *radius_ms = c.kernel_ms[0];
+    if (radius_launches) *radius_launches = c.kernel_launches[0];
+    if (knn_ms) *knn_ms = c.kernel_ms[1];
+    if (knn_launches) *knn_launches = c.kernel_launches[1];
+    if (reset) {
+        c.kernel_ms[0] = c.kernel_ms[1] = 0.0;
+        c.kernel_launches[0] = c.kernel_launches[1] = 0;
+    }
+    return OCT_OK;
+}
 
 int oct_radius_search_axes(oct_cloud h, int kernel, int algo, const double* centers, uint64_t nq,
                            const double* radii_xyz, int per_query, uint64_t* offsets, uint32_t* idx,

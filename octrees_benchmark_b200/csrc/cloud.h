@@ -5,6 +5,8 @@
 
 #include <cstdint>
 #include <string>
+#include <utility>
+#include <vector>
 
 #include "../../include/octree_b200.h"
 #include "oct_common.cuh"
@@ -189,6 +191,43 @@ struct Cloud {
 
     // pinned host staging for small readbacks
     void* pinned = nullptr;
+
+    // oct_search_timing: CUDA events on the cloud's stream around the main search kernel of each call
+    // (kind 0: the packet radius search, 1: the group kNN), summed by oct_search_kernel_times
+    bool time_kernels = false;
+    std::vector<cudaEvent_t> ev_free;
+    std::vector<std::pair<cudaEvent_t, cudaEvent_t>> ev_pend[2];
+    double kernel_ms[2] = {0.0, 0.0};
+    uint64_t kernel_launches[2] = {0, 0};
+};
+
+// Records the start of a timed kernel on the cloud's stream (no-op unless timing is on); stop() records the end.
+struct KernelClock {
+    Cloud& c;
+    int kind;
+    cudaEvent_t a = nullptr, b = nullptr;
+    KernelClock(Cloud& cl, int k) : c(cl), kind(k) {
+        if (!c.time_kernels) return;
+        for (cudaEvent_t* e : {&a, &b}) {
+            if (!c.ev_free.empty()) {
+                *e = c.ev_free.back();
+                c.ev_free.pop_back();
+            } else if (cudaEventCreate(e) != cudaSuccess) {
+                *e = nullptr;
+            }
+        }
+        if (a && b) cudaEventRecord(a, c.stream);
+    }
+    void stop() {
+        if (a && b) {
+            cudaEventRecord(b, c.stream);
+            c.ev_pend[kind].emplace_back(a, b);
+        } else {
+            if (a) c.ev_free.push_back(a);
+            if (b) c.ev_free.push_back(b);
+        }
+        a = b = nullptr;
+    }
 };
 
 // ---- launchers (each returns a cudaError_t of the launch) ----

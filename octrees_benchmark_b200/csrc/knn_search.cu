@@ -1508,8 +1508,10 @@ cudaError_t launch_knn(Cloud& c, const double* d_centers, uint64_t nq, uint32_t 
         g.stats = f32 ? c.stats.as<unsigned long long>() + 2 : nullptr;  // oct_knn_filter_stats
         const int sms = sm_count_k(c.device);
         double* heads = c.knn_heads.as<double>();
+        KernelClock clk(c, 1);
         e = (k <= 32) ? launch_group_seeded<1, 0>(g, sms, c.stream, 0, heads, head_bytes, f32)
                       : launch_group_seeded<2, 0>(g, sms, c.stream, 0, heads, head_bytes, f32);
+        clk.stop();
         if (e != cudaSuccess) return e;
         KnnTableArgs f{};
         f.single = r;

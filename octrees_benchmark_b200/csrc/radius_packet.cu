@@ -987,9 +987,12 @@ cudaError_t launch_radius_packet(Cloud& c, int kernel, int algo, int mode, bool 
     r.cloud_id = 0;
     r.approx_cut = c.approx_cut;
     r.approx_upper = (uint32_t)c.approx_upper;
-    return launch_radius_table(c.device, c.stream, kernel, algo, mode, fp32, nullptr, &r, (nq + 31) / 32, d_order,
-                               d_counts, d_counts2, d_offsets, d_out, out_capacity, c.packet_ctr.as<uint32_t>(),
-                               c.stats.as<unsigned long long>(), c.d_err.as<uint32_t>(), 0, chunks);
+    KernelClock clk(c, 0);
+    e = launch_radius_table(c.device, c.stream, kernel, algo, mode, fp32, nullptr, &r, (nq + 31) / 32, d_order,
+                            d_counts, d_counts2, d_offsets, d_out, out_capacity, c.packet_ctr.as<uint32_t>(),
+                            c.stats.as<unsigned long long>(), c.d_err.as<uint32_t>(), 0, chunks);
+    clk.stop();
+    return e;
 }
 
 }  // namespace octb
