@@ -558,7 +558,7 @@ def run_b200(args, rank, world, local_rank):
     stream = torch.cuda.Stream()
     xyz_h = lidar_tile(N_POINTS, TILE_M, SEED)
     xyz_d = torch.from_numpy(xyz_h).cuda()
-    p = capi.OctParams(MAX_LEAF, ENCODER, dev, 0)
+    p = capi.OctParams(MAX_LEAF, ENCODER, dev, capi.OCT_CLOUD_SORT_8PASS if args.sort_8pass else 0)
     h = C.c_void_p()
     capi.check(L.oct_cloud_create(C.byref(p), C.byref(h)), None, "create")
     capi.check(L.oct_cloud_set_stream(h, C.c_void_p(stream.cuda_stream)), h)
@@ -628,7 +628,10 @@ def run_b200(args, rank, world, local_rank):
     eng = BatchEngine(device=dev, reserve_results=cap)
     eng_reqs = [[Request(proxy, "radius", qr, radius=RADIUS, kernel="sphere", algo="neighborsPrune"),
                  Request(proxy, "knn", qk, k=KNN_K)] for qr, qk in batches]
-    eng_cfg = eng.autotune(eng_reqs[0])
+    wanted = [p_ for p_ in args.paths.split(",") if p_] if args.paths else ["engine"]
+    # the engine is autotuned when an engine path runs (a profile of the single-cloud kernels skips it)
+    eng_cfg = eng.autotune(eng_reqs[0]) if args.search == "engine" or any(
+        p_.startswith("engine") for p_ in wanted) else eng.config()
 
     def engine_step(b):
         with torch.cuda.stream(stream):
@@ -650,7 +653,9 @@ def run_b200(args, rank, world, local_rank):
         with torch.cuda.stream(stream):
             flush.zero_()
             ev[0].record(stream)
+            L.oct_search_timing(h, 0)  # the kernel times cover the search calls below, not this count-only call
             capi.check(L.oct_radius_count(h, 1, 2, qr.data_ptr(), Q_RADIUS, None, RADIUS, offs.data_ptr(), MD), h)
+            L.oct_search_timing(h, 1)
             ev[1].record(stream)
             capi.check(L.oct_radius_search(h, 1, 2, qr.data_ptr(), Q_RADIUS, None, RADIUS, offs.data_ptr(),
                                            idx_out.data_ptr(), cap, C.byref(tot), MD), h, "radius_search")
@@ -886,8 +891,10 @@ def run_b200(args, rank, world, local_rank):
     build = {"ms": 1e3 * build_s, "mpts_s": N_POINTS / build_s / 1e6, "gbs": build_bytes / build_s / 1e9,
              "frac": build_bytes / build_s / 1e9 / peak, "nodes": info.n_total, "leaves": info.n_leaf,
              "depth": info.max_depth_seen, "upload_ms": 1e3 * upload_s,
-             "includes": "bbox + encode + 8-bit onesweep sort + reorder + octree build from points resident in "
-                         "HBM, host syncs included (wall clock)"}
+             "sort": "8 passes over the whole keys" if args.sort_8pass else
+                     "4 passes over the upper key halves, then the runs of equal upper halves",
+             "includes": "bbox + encode + sort + reorder + octree build from points resident in HBM, host syncs "
+                         "included (wall clock)"}
 
     line = None
     if rank == 0:
@@ -1016,6 +1023,7 @@ def main():
     ap.add_argument("--large-k", type=int, default=1000)
     ap.add_argument("--points", type=int, default=N_POINTS, help="cloud size (smaller cases for profiling)")
     ap.add_argument("--queries", type=int, default=Q_RADIUS, help="radius and kNN queries per step, each")
+    ap.add_argument("--sort-8pass", action="store_true", help="build with the 8-pass sort (the split sort by default)")
     ap.add_argument("--paths", default="", help="comma-separated search paths to time (default: all); the "
                                                  "--search path always runs")
     ap.add_argument("--deadline", type=float, default=1200.0,

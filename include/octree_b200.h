@@ -70,11 +70,17 @@ typedef enum {
 
 #define OCT_MEM_DEVICE 0x1u /* every buffer of the call is device memory */
 
+/* oct_params.flags: sort with eight 8-bit passes over the whole keys instead of
+ * four passes over their upper halves followed by the runs of equal upper
+ * halves (same result; the split sort is the default and takes the 8-pass
+ * sort by itself when a run is longer than 4096 points) */
+#define OCT_CLOUD_SORT_8PASS 0x1u
+
 typedef struct {
     uint32_t max_points_leaf; /* mainOptions.maxPointsLeaf (main_options.hpp:210); default 128 */
     int32_t encoder;          /* oct_encoder */
     int32_t device;           /* CUDA device ordinal */
-    uint32_t flags;           /* reserved, 0 */
+    uint32_t flags;           /* OCT_CLOUD_* */
 } oct_params;
 
 typedef struct {
@@ -404,6 +410,7 @@ int oct_cloud_memory(oct_cloud cloud, uint64_t* bytes);
 typedef struct oct_server_s* oct_server;
 
 #define OCT_SERVER_PLAIN 0x1u /* one request per launch, single-cloud plain path */
+#define OCT_SERVER_FIFO 0x2u  /* batched: admit in arrival order only (no smallest-first admission) */
 #define OCT_CLOUD_OWNED 0x1u  /* oct_server_add_cloud: the server destroys the cloud when it evicts or removes it */
 
 typedef struct {
@@ -411,8 +418,10 @@ typedef struct {
     uint32_t flags;              /* OCT_SERVER_* */
     uint32_t slots;              /* batches in flight at once; 0: 3 */
     uint32_t max_batch_requests; /* 0: 1024 */
-    uint64_t max_batch_queries;  /* 0: 4M */
+    uint64_t max_batch_queries;  /* 0: 512K */
     uint64_t hbm_budget;         /* bytes for the clouds and the admitted batches; 0: 120 GB */
+    double max_wait_ms;          /* requests queued longer than this are admitted first, in arrival
+                                    order; the others smallest estimated work first; 0: 40 ms */
 } oct_server_params;
 
 typedef struct {

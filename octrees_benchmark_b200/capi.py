@@ -22,6 +22,7 @@ OCT_ERR_CAPACITY = 5
 OCT_ERR_DEVICE_LIMIT = 6
 OCT_ERR_NO_DEVICE = 7
 OCT_MEM_DEVICE = 0x1
+OCT_CLOUD_SORT_8PASS = 0x1
 OCT_NOALLOC_MAX_POINTS = 1 << 18
 
 ENCODERS = {"morton": 1, "mort": 1, "hilbert": 5, "hilb": 5, 1: 1, 5: 5}
@@ -67,12 +68,14 @@ class OctRequestPlace(C.Structure):
 
 
 OCT_SERVER_PLAIN = 0x1
+OCT_SERVER_FIFO = 0x2
 OCT_CLOUD_OWNED = 0x1
 
 
 class OctServerParams(C.Structure):
     _fields_ = [("device", C.c_int32), ("flags", C.c_uint32), ("slots", C.c_uint32),
-                ("max_batch_requests", C.c_uint32), ("max_batch_queries", C.c_uint64), ("hbm_budget", C.c_uint64)]
+                ("max_batch_requests", C.c_uint32), ("max_batch_queries", C.c_uint64), ("hbm_budget", C.c_uint64),
+                ("max_wait_ms", C.c_double)]
 
 
 class OctCompletion(C.Structure):

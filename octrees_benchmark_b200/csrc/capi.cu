@@ -278,6 +278,7 @@ int oct_cloud_create(const oct_params* p, oct_cloud* out) {
     Cloud& c = h->c;
     c.params = *p;
     c.device = p->device;
+    c.split_sort = (p->flags & OCT_CLOUD_SORT_8PASS) ? 0 : 1;
     DeviceGuard g(c.device);
     cudaError_t e = cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) {
@@ -309,7 +310,8 @@ int oct_cloud_destroy(oct_cloud h) {
                           &c.frontier, &c.masks, &c.parts, &c.d_build, &c.q_centers, &c.q_radii, &c.q_counts,
                           &c.q_offsets, &c.q_out, &c.q_out2, &c.q_scan_tmp, &c.qs_keys, &c.qs_keys_alt, &c.qs_ord,
                           &c.qs_ord_alt, &c.qs_status, &c.qs_ctl, &c.packet_ctr, &c.stats, &c.rel,
-                          &c.ck_pool, &c.ck_next, &c.ck_first, &c.ck_ctr, &c.knn_fb, &c.knn_heads, &c.crel, &c.q_axes};
+                          &c.ck_pool, &c.ck_next, &c.ck_first, &c.ck_ctr, &c.knn_fb, &c.knn_heads, &c.crel, &c.q_axes,
+                          &c.keys_hi, &c.keys_hi_alt, &c.run_ctl, &c.run_list};
         for (DevBuf* b : bufs) b->release();
         if (c.pinned) cudaFreeHost(c.pinned);
         for (auto& v : c.ev_pend)
@@ -411,7 +413,8 @@ int oct_cloud_memory(oct_cloud h, uint64_t* bytes) {
                             &c.frontier, &c.masks, &c.parts, &c.d_build, &c.q_centers, &c.q_radii, &c.q_counts,
                             &c.q_offsets, &c.q_out, &c.q_out2, &c.q_scan_tmp, &c.qs_keys, &c.qs_keys_alt, &c.qs_ord,
                             &c.qs_ord_alt, &c.qs_status, &c.qs_ctl, &c.packet_ctr, &c.stats, &c.rel,
-                            &c.ck_pool, &c.ck_next, &c.ck_first, &c.ck_ctr, &c.knn_fb, &c.knn_heads, &c.crel, &c.q_axes};
+                            &c.ck_pool, &c.ck_next, &c.ck_first, &c.ck_ctr, &c.knn_fb, &c.knn_heads, &c.crel, &c.q_axes,
+                          &c.keys_hi, &c.keys_hi_alt, &c.run_ctl, &c.run_list};
     uint64_t s = 0;
     for (const DevBuf* b : bufs) s += b->bytes;
     *bytes = s;
@@ -448,7 +451,9 @@ int oct_encode_sort(oct_cloud h, double* box12, uint64_t* keys, uint32_t* perm, 
     if (c.sorted) return emit_sorted(c, box12, keys, perm, sorted_xyz, dev);  // points unchanged since the last sort
     const double* xyz = c.xyz_in.as<double>();
     CK(cudaMemsetAsync(c.d_err.ptr, 0, 4, c.stream));
-    CK(launch_bbox_encode(c, xyz));
+    const bool split = c.split_sort && c.n;
+    if (split) CK(c.keys_hi.reserve(4 * c.n));
+    CK(launch_bbox_encode(c, xyz, split ? c.keys_hi.as<uint32_t>() : nullptr));
     uint32_t skip[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     if (c.n) {
         CK(cudaMemcpyAsync(c.pinned, &c.d_ctl.as<SortCtl>()->skip[0], sizeof(skip), cudaMemcpyDeviceToHost,
@@ -456,17 +461,40 @@ int oct_encode_sort(oct_cloud h, double* box12, uint64_t* keys, uint32_t* perm, 
         CK(cudaStreamSynchronize(c.stream));
         memcpy(skip, c.pinned, sizeof(skip));
     }
-    int sel = 0;
-    CK(launch_sort_passes(c, skip, &sel));
-    if (sel == 1) {
-        std::swap(c.keys, c.keys_alt);
-        std::swap(c.perm, c.perm_alt);
+    // the split sort (upper halves, then runs); a run too long for it falls back to the 8-pass sort
+    bool done = false;
+    unsigned char* pin = static_cast<unsigned char*>(c.pinned);
+    if (split) {
+        int psel = 0;
+        CK(launch_sort_split(c, skip, xyz, &psel));
+        // the run flags and the box and level geometry back to the host in one wait
+        CK(cudaMemcpyAsync(pin + 2048, c.run_ctl.ptr, 16, cudaMemcpyDeviceToHost, c.stream));
+        CK(cudaMemcpyAsync(pin, c.d_box.ptr, sizeof(BoxD) + sizeof(LevelGeom), cudaMemcpyDeviceToHost, c.stream));
+        const int st = sync_and_check(c);
+        if (st != OCT_OK) return st;
+        uint32_t rc[4];
+        memcpy(rc, pin + 2048, sizeof(rc));
+        if (rc[2] == 0) {  // no run too long: the outputs are the sorted cloud
+            std::swap(c.keys, c.keys_alt);
+            if (psel == 1) std::swap(c.perm, c.perm_alt);
+            done = true;
+        }
     }
-    CK(launch_gather(c, xyz, c.perm.as<uint32_t>(), 0));
-    // box and level geometry back to the host
-    CK(cudaMemcpyAsync(c.pinned, c.d_box.ptr, sizeof(BoxD) + sizeof(LevelGeom), cudaMemcpyDeviceToHost, c.stream));
-    int st = sync_and_check(c);
-    if (st != OCT_OK) return st;
+    if (!done) {
+        if (split)  // the split sort's passes took tiles from the upper digits' counters: rewind them
+            CK(cudaMemsetAsync(&c.d_ctl.as<SortCtl>()->tile_ctr[0], 0, sizeof(SortCtl::tile_ctr), c.stream));
+        int sel = 0;
+        CK(launch_sort_passes(c, skip, &sel));
+        if (sel == 1) {
+            std::swap(c.keys, c.keys_alt);
+            std::swap(c.perm, c.perm_alt);
+        }
+        CK(launch_gather(c, xyz, c.perm.as<uint32_t>(), 0));
+        // box and level geometry back to the host
+        CK(cudaMemcpyAsync(pin, c.d_box.ptr, sizeof(BoxD) + sizeof(LevelGeom), cudaMemcpyDeviceToHost, c.stream));
+        const int st = sync_and_check(c);
+        if (st != OCT_OK) return st;
+    }
     memcpy(&c.box, c.pinned, sizeof(BoxD));
     memcpy(&c.geom, static_cast<unsigned char*>(c.pinned) + sizeof(BoxD), sizeof(LevelGeom));
     c.sorted = true;

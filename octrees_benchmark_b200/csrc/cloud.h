@@ -135,6 +135,9 @@ struct Cloud {
     DevBuf xs, ys, zs;      // SFC-sorted coordinates, SoA f64
     DevBuf keys, keys_alt;  // u64 keys (sorted result lives in `keys`)
     DevBuf perm, perm_alt;  // u32 input position of each sorted point
+    DevBuf keys_hi, keys_hi_alt;  // u32 upper key halves (the split sort)
+    DevBuf run_ctl, run_list;     // the split sort's run bookkeeping
+    int split_sort = 1;           // sort the upper halves, then the runs (0: the 8-pass sort)
     DevBuf sort_status;     // onesweep look-back words
     uint32_t sort_epoch = 0;
     DevBuf d_ctl;           // SortCtl
@@ -231,7 +234,8 @@ struct KernelClock {
 };
 
 // ---- launchers (each returns a cudaError_t of the launch) ----
-cudaError_t launch_bbox_encode(Cloud& c, const double* d_xyz_aos);
+cudaError_t launch_bbox_encode(Cloud& c, const double* d_xyz_aos, uint32_t* d_hi = nullptr);
+cudaError_t launch_sort_split(Cloud& c, const uint32_t skip[8], const double* d_xyz_aos, int* out_sel);
 cudaError_t launch_sort_passes(Cloud& c, const uint32_t skip[8], int* final_sel);
 cudaError_t launch_gather(Cloud& c, const double* d_xyz_aos, const uint32_t* d_perm, int sel);
 cudaError_t launch_build(Cloud& c, bool* capacity_ok);

@@ -168,7 +168,7 @@ __global__ void __launch_bounds__(kBboxThreads) k_bbox(const double* __restrict_
 template <int ENC>
 __global__ void __launch_bounds__(kEncThreads) k_encode(const double* __restrict__ xyz, uint64_t n,
                                                         const BoxGeom* __restrict__ bg, uint64_t* __restrict__ keys,
-                                                        SortCtl* ctl) {
+                                                        SortCtl* ctl, uint32_t* __restrict__ hi = nullptr) {
     __shared__ uint32_t hist[8 * 256];
     __shared__ uint8_t htbl[kHilbertStates * 8];
     __shared__ uint16_t htbl2[ENC == 5 ? kHilbertTable2Size : 1];
@@ -195,8 +195,12 @@ __global__ void __launch_bounds__(kEncThreads) k_encode(const double* __restrict
     // buffers that are not 16-byte aligned take the scalar loop
     const bool vec = ((reinterpret_cast<uintptr_t>(xyz) | reinterpret_cast<uintptr_t>(keys)) & 15u) == 0;
     const uint64_t npairs = vec ? n / 2 : 0;
-    for (uint64_t i = vec ? n : (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
-        keys[i] = key_of(xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]);
+    // hi (optional): the upper 32 bits of every key as well, for the sort on the upper halves
+    for (uint64_t i = vec ? n : (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const uint64_t k = key_of(xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]);
+        keys[i] = k;
+        if (hi) hi[i] = (uint32_t)(k >> 32);
+    }
     const double2* xyz2 = reinterpret_cast<const double2*>(xyz);
     ulonglong2* keys2 = reinterpret_cast<ulonglong2*>(keys);
     for (uint64_t t = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; t < npairs; t += stride) {
@@ -205,9 +209,16 @@ __global__ void __launch_bounds__(kEncThreads) k_encode(const double* __restrict
         kk.x = key_of(a.x, a.y, b.x);
         kk.y = key_of(b.y, c.x, c.y);
         keys2[t] = kk;
+        if (hi) {
+            hi[2 * t] = (uint32_t)(kk.x >> 32);
+            hi[2 * t + 1] = (uint32_t)(kk.y >> 32);
+        }
     }
-    if (vec && (n & 1) && blockIdx.x == 0 && threadIdx.x == 0)
-        keys[n - 1] = key_of(xyz[3 * (n - 1)], xyz[3 * (n - 1) + 1], xyz[3 * (n - 1) + 2]);
+    if (vec && (n & 1) && blockIdx.x == 0 && threadIdx.x == 0) {
+        const uint64_t k = key_of(xyz[3 * (n - 1)], xyz[3 * (n - 1) + 1], xyz[3 * (n - 1) + 2]);
+        keys[n - 1] = k;
+        if (hi) hi[n - 1] = (uint32_t)(k >> 32);
+    }
     __syncthreads();
     for (int j = threadIdx.x; j < 8 * 256; j += blockDim.x) {
         const uint32_t v = hist[j];
@@ -243,16 +254,18 @@ __global__ void __launch_bounds__(256) k_scan_hist(SortCtl* ctl, uint64_t n, con
     }
 }
 
-template <bool FIRST>
-__global__ void __launch_bounds__(kSortThreads, 3) k_onesweep(const uint64_t* __restrict__ kin,
+// K: uint64_t (the full keys; digit `pass` is bits 8 pass .. 8 pass + 7) or
+// uint32_t (the upper key halves; digit `pass` (4..7) is bits 8 pass - 32 ..)
+template <bool FIRST, class K = uint64_t>
+__global__ void __launch_bounds__(kSortThreads, 3) k_onesweep(const K* __restrict__ kin,
                                                            const uint32_t* __restrict__ vin,
-                                                           uint64_t* __restrict__ kout, uint32_t* __restrict__ vout,
+                                                           K* __restrict__ kout, uint32_t* __restrict__ vout,
                                                            uint64_t n, int pass, SortCtl* ctl,
                                                            unsigned long long* status, uint32_t epoch,
                                                            uint32_t* err, const uint64_t* d_n = nullptr,
                                                            const uint32_t* d_epoch = nullptr) {
     extern __shared__ __align__(16) unsigned char smem[];
-    uint64_t* skeys = reinterpret_cast<uint64_t*>(smem);                       // kSortTile
+    K* skeys = reinterpret_cast<K*>(smem);                                     // kSortTile
     uint32_t* svals = reinterpret_cast<uint32_t*>(skeys + kSortTile);          // kSortTile
     uint32_t* wcnt = svals + kSortTile;                                        // kSortWarps x 256
     uint32_t* tstart = wcnt + kSortWarps * 256;                                // 256
@@ -261,7 +274,7 @@ __global__ void __launch_bounds__(kSortThreads, 3) k_onesweep(const uint64_t* __
     __shared__ uint32_t s_wsum[kSortWarps];
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-    const int shift = 8 * pass;
+    const int shift = 8 * pass - (sizeof(K) == 4 ? 32 : 0);
     // sizes set on the device (batched launches): key count, and the epoch base
     // of this batch's passes
     if (d_n) n = *d_n;
@@ -277,14 +290,14 @@ __global__ void __launch_bounds__(kSortThreads, 3) k_onesweep(const uint64_t* __
     if ((uint64_t)tile >= ntiles) break;
     const uint64_t base = (uint64_t)tile * kSortTile;
 
-    uint64_t k[kSortItems];
+    K k[kSortItems];
     uint32_t v[kSortItems];
     uint32_t rank[kSortItems];
 #pragma unroll
     for (int j = 0; j < kSortItems; ++j) {
         const uint64_t idx = base + (uint64_t)warp * (32 * kSortItems) + (uint64_t)j * 32 + lane;
         const bool valid = idx < n;
-        k[j] = valid ? kin[idx] : ~0ull;
+        k[j] = valid ? kin[idx] : (K)~0ull;
         if (FIRST) v[j] = (uint32_t)idx;
         else v[j] = valid ? vin[idx] : 0u;
     }
@@ -382,7 +395,7 @@ __global__ void __launch_bounds__(kSortThreads, 3) k_onesweep(const uint64_t* __
     __syncthreads();
     const uint32_t cnt_tile = (uint32_t)((n - base) < (uint64_t)kSortTile ? (n - base) : (uint64_t)kSortTile);
     for (uint32_t s = tid; s < cnt_tile; s += kSortThreads) {
-        const uint64_t key = skeys[s];
+        const K key = skeys[s];
         const uint32_t dd = (uint32_t)((key >> shift) & 255u);
         const unsigned long long o = gbase[dd] + (s - tstart[dd]);
         if (o < n) {  // always true unless a look-back gave up (then err is set)
@@ -391,6 +404,146 @@ __global__ void __launch_bounds__(kSortThreads, 3) k_onesweep(const uint64_t* __
         }
     }
     __syncthreads();  // shared memory and s_tile are reused by the next tile
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Sort on the upper key halves, then the runs of equal upper halves by the
+// lower halves.  A stable order by the upper 32 bits (4 onesweep passes on
+// 32-bit keys: 16 bytes per key and pass instead of 24) leaves the points of
+// each run (equal upper halves: one cell at depth ~10.7) in input order; a
+// stable order of each run by its full keys then gives the stable order of the
+// whole 63-bit keys, which is the reference's (point_encoder.hpp:285-383).
+// Runs on this path are short (a 10M-point 1.5 km tile: a few points), so a
+// thread sorts one run of up to kRunSmall points by insertion, a block sorts a
+// run of up to kRunMid in shared memory (bitonic over (low half, position in
+// run): unique, so the order is stable), and a longer run sends the cloud to
+// the 8-pass sort.  The same kernels write the sorted keys, the permutation
+// and the reordered SoA coordinates.
+// ---------------------------------------------------------------------------
+constexpr uint32_t kRunSmall = 32;
+constexpr uint32_t kRunMid = 4096;
+constexpr int kRunMidThreads = 1024;
+
+struct RunCtl {
+    uint32_t mid_count;  // runs for k_runs_mid
+    uint32_t mid_next;   // k_runs_mid's work counter
+    uint32_t big;        // a run longer than kRunMid was found
+    uint32_t pad;
+};
+
+__device__ __forceinline__ void put_sorted(uint64_t o, uint32_t p, const uint64_t* __restrict__ keys_in,
+                                           const double* __restrict__ xyz, uint64_t* __restrict__ keys_out,
+                                           uint32_t* __restrict__ perm_out, double* __restrict__ xs,
+                                           double* __restrict__ ys, double* __restrict__ zs) {
+    keys_out[o] = keys_in[p];
+    perm_out[o] = p;
+    xs[o] = xyz[3ull * p];
+    ys[o] = xyz[3ull * p + 1];
+    zs[o] = xyz[3ull * p + 2];
+}
+
+// One thread per run start: runs of one point are copied, runs of up to
+// kRunSmall sorted by insertion (strict >, so equal keys keep their order),
+// longer runs listed for k_runs_mid (start, length) or flagged.
+__global__ void __launch_bounds__(256) k_runs_small(const uint32_t* __restrict__ hi,
+                                                    const uint32_t* __restrict__ perm_hi,
+                                                    const uint64_t* __restrict__ keys_in,
+                                                    const double* __restrict__ xyz, uint64_t n,
+                                                    uint64_t* __restrict__ keys_out, uint32_t* __restrict__ perm_out,
+                                                    double* __restrict__ xs, double* __restrict__ ys,
+                                                    double* __restrict__ zs, RunCtl* rc, uint32_t* mid_list) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const uint32_t h = hi[i];
+        if (i > 0 && hi[i - 1] == h) continue;  // inside a run: its start handles it
+        uint64_t e = i + 1;
+        while (e < n && e - i <= kRunSmall && hi[e] == h) ++e;
+        const uint64_t len = e - i;
+        if (len == 1) {
+            put_sorted(i, perm_hi[i], keys_in, xyz, keys_out, perm_out, xs, ys, zs);
+            continue;
+        }
+        if (len > kRunSmall) {
+            while (e < n && e - i <= kRunMid && hi[e] == h) ++e;
+            if (e - i > kRunMid) {
+                atomicOr(&rc->big, 1u);
+            } else {
+                const uint32_t slot = atomicAdd(&rc->mid_count, 1u);
+                mid_list[2 * slot] = (uint32_t)i;
+                mid_list[2 * slot + 1] = (uint32_t)(e - i);
+            }
+            continue;
+        }
+        uint64_t kk[kRunSmall];
+        uint32_t pp[kRunSmall];
+        for (uint32_t j = 0; j < (uint32_t)len; ++j) {
+            const uint32_t p = perm_hi[i + j];
+            const uint64_t key = keys_in[p];
+            uint32_t m = j;
+            while (m > 0 && kk[m - 1] > key) {
+                kk[m] = kk[m - 1];
+                pp[m] = pp[m - 1];
+                --m;
+            }
+            kk[m] = key;
+            pp[m] = p;
+        }
+        for (uint32_t j = 0; j < (uint32_t)len; ++j) {
+            const uint32_t p = pp[j];
+            keys_out[i + j] = kk[j];
+            perm_out[i + j] = p;
+            xs[i + j] = xyz[3ull * p];
+            ys[i + j] = xyz[3ull * p + 1];
+            zs[i + j] = xyz[3ull * p + 2];
+        }
+    }
+}
+
+// One block per listed run (persistent blocks take runs from a counter):
+// bitonic sort of (low key half << 32 | position in run) in shared memory.
+__global__ void __launch_bounds__(kRunMidThreads) k_runs_mid(const uint32_t* __restrict__ perm_hi,
+                                                             const uint64_t* __restrict__ keys_in,
+                                                             const double* __restrict__ xyz,
+                                                             uint64_t* __restrict__ keys_out,
+                                                             uint32_t* __restrict__ perm_out, double* __restrict__ xs,
+                                                             double* __restrict__ ys, double* __restrict__ zs,
+                                                             RunCtl* rc, const uint32_t* __restrict__ mid_list) {
+    __shared__ unsigned long long s[kRunMid];
+    __shared__ uint32_t s_r;
+    const int tid = threadIdx.x;
+    const uint32_t count = rc->mid_count;
+    for (;;) {
+        if (tid == 0) s_r = atomicAdd(&rc->mid_next, 1u);
+        __syncthreads();
+        const uint32_t r = s_r;
+        if (r >= count) break;
+        const uint32_t start = mid_list[2 * r], len = mid_list[2 * r + 1];
+        uint32_t P = 64;
+        while (P < len) P <<= 1;
+        for (uint32_t t = tid; t < P; t += kRunMidThreads)
+            s[t] = t < len ? ((keys_in[perm_hi[start + t]] & 0xffffffffull) << 32) | t : ~0ull;
+        __syncthreads();
+        for (uint32_t k = 2; k <= P; k <<= 1) {
+            for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+                for (uint32_t t = tid; t < P; t += kRunMidThreads) {
+                    const uint32_t o = t ^ j;
+                    if (o > t) {
+                        const unsigned long long a = s[t], b = s[o];
+                        if ((a > b) == ((t & k) == 0)) {
+                            s[t] = b;
+                            s[o] = a;
+                        }
+                    }
+                }
+                __syncthreads();
+            }
+        }
+        for (uint32_t t = tid; t < len; t += kRunMidThreads) {
+            const uint32_t local = (uint32_t)(s[t] & 0xffffffffull);
+            put_sorted(start + t, perm_hi[start + local], keys_in, xyz, keys_out, perm_out, xs, ys, zs);
+        }
+        __syncthreads();  // s and s_r are reused by the next run
     }
 }
 
@@ -439,7 +592,7 @@ int bbox_blocks_per_sm() {
     return per;
 }
 
-cudaError_t launch_bbox_encode(Cloud& c, const double* d_xyz) {
+cudaError_t launch_bbox_encode(Cloud& c, const double* d_xyz, uint32_t* d_hi) {
     cudaError_t e;
     const uint64_t n = c.n;
     const int sms = sm_count(c.device);
@@ -457,10 +610,10 @@ cudaError_t launch_bbox_encode(Cloud& c, const double* d_xyz) {
         const int grid = (int)(want < (uint64_t)sms * kEncGridPerSM ? want : (uint64_t)sms * kEncGridPerSM);
         if (c.params.encoder == OCT_ENC_HILBERT_3D)
             k_encode<5><<<grid, kEncThreads, 0, c.stream>>>(d_xyz, n, c.d_box.as<BoxGeom>(), c.keys.as<uint64_t>(),
-                                                            ctl);
+                                                            ctl, d_hi);
         else
             k_encode<1><<<grid, kEncThreads, 0, c.stream>>>(d_xyz, n, c.d_box.as<BoxGeom>(), c.keys.as<uint64_t>(),
-                                                            ctl);
+                                                            ctl, d_hi);
         k_scan_hist<<<1, 256, 0, c.stream>>>(ctl, n);
     }
     return cudaGetLastError();
@@ -517,6 +670,84 @@ cudaError_t launch_sort_passes(Cloud& c, const uint32_t skip[8], int* final_sel)
         sel = 0;
     }
     *final_sel = sel;
+    return cudaGetLastError();
+}
+
+// The split sort (upper halves, then runs): keys stay in input order in c.keys
+// (so the 8-pass sort can still run from them), the sorted keys go to
+// c.keys_alt, the permutation to the perm buffer *out_sel names, the sorted
+// coordinates to xs / ys / zs.  RunCtl::big (d_run_ctl) says whether a run was
+// too long, in which case nothing of the outputs may be used.
+cudaError_t launch_sort_split(Cloud& c, const uint32_t skip[8], const double* d_xyz, int* out_sel) {
+    cudaError_t e;
+    const uint64_t n = c.n;
+    *out_sel = 0;
+    if ((e = c.keys_alt.reserve(8 * (n ? n : 1))) != cudaSuccess) return e;
+    if ((e = c.perm.reserve(4 * (n ? n : 1))) != cudaSuccess) return e;
+    if ((e = c.perm_alt.reserve(4 * (n ? n : 1))) != cudaSuccess) return e;
+    if ((e = c.keys_hi_alt.reserve(4 * (n ? n : 1))) != cudaSuccess) return e;
+    if ((e = c.run_ctl.reserve(sizeof(RunCtl))) != cudaSuccess) return e;
+    if ((e = c.run_list.reserve(8 * (n / (kRunSmall + 1) + 1))) != cudaSuccess) return e;
+    const size_t b = 8 * (n ? n : 1);
+    if ((e = c.xs.reserve(b)) != cudaSuccess) return e;
+    if ((e = c.ys.reserve(b)) != cudaSuccess) return e;
+    if ((e = c.zs.reserve(b)) != cudaSuccess) return e;
+    RunCtl* rc = c.run_ctl.as<RunCtl>();
+    if ((e = cudaMemsetAsync(rc, 0, sizeof(RunCtl), c.stream)) != cudaSuccess) return e;
+    if (n == 0) return cudaSuccess;
+    const uint64_t tiles = (n + kSortTile - 1) / kSortTile;
+    const size_t status_bytes = tiles * 256 * sizeof(unsigned long long);
+    if (status_bytes > c.sort_status.bytes) {
+        if ((e = c.sort_status.reserve(status_bytes)) != cudaSuccess) return e;
+        if ((e = cudaMemsetAsync(c.sort_status.ptr, 0, c.sort_status.bytes, c.stream)) != cudaSuccess) return e;
+        c.sort_epoch = 0;
+    }
+    // 32-bit keys: tile 3072 x 8 bytes + counters, under the default 48 KB of dynamic shared memory
+    const size_t smem = (size_t)kSortTile * 4 + (size_t)kSortTile * 4 + (size_t)kSortWarps * 256 * 4 + 256 * 4 +
+                        256 * 8;
+    DevBuf* kb[2] = {&c.keys_hi, &c.keys_hi_alt};
+    DevBuf* vb[2] = {&c.perm, &c.perm_alt};
+    int sel = 0;
+    bool first = true;
+    SortCtl* ctl = c.d_ctl.as<SortCtl>();
+    for (int p = 4; p < 8; ++p) {  // the digits of the upper halves
+        if (skip[p]) continue;
+        c.sort_epoch = (c.sort_epoch + 1) & ((1u << 22) - 1);
+        if (c.sort_epoch == 0) {
+            if ((e = cudaMemsetAsync(c.sort_status.ptr, 0, c.sort_status.bytes, c.stream)) != cudaSuccess) return e;
+            c.sort_epoch = 1;
+        }
+        const uint32_t* kin = kb[sel]->as<uint32_t>();
+        uint32_t* kout = kb[sel ^ 1]->as<uint32_t>();
+        const uint32_t* vin = vb[sel]->as<uint32_t>();
+        uint32_t* vout = vb[sel ^ 1]->as<uint32_t>();
+        if (first)
+            k_onesweep<true, uint32_t><<<(unsigned)tiles, kSortThreads, smem, c.stream>>>(
+                kin, nullptr, kout, vout, n, p, ctl, c.sort_status.as<unsigned long long>(), c.sort_epoch,
+                c.d_err.as<uint32_t>());
+        else
+            k_onesweep<false, uint32_t><<<(unsigned)tiles, kSortThreads, smem, c.stream>>>(
+                kin, vin, kout, vout, n, p, ctl, c.sort_status.as<unsigned long long>(), c.sort_epoch,
+                c.d_err.as<uint32_t>());
+        first = false;
+        sel ^= 1;
+    }
+    if (first) {  // every upper digit constant: one run in input order
+        k_iota<<<(unsigned)((n + 255) / 256), 256, 0, c.stream>>>(c.perm.as<uint32_t>(), n);
+        sel = 0;
+    }
+    const int sms = sm_count(c.device);
+    const uint64_t want = (n + 255) / 256;
+    const int grid = (int)(want < (uint64_t)sms * 8 ? want : (uint64_t)sms * 8);
+    uint32_t* perm_out = vb[sel ^ 1]->as<uint32_t>();
+    k_runs_small<<<grid, 256, 0, c.stream>>>(kb[sel]->as<uint32_t>(), vb[sel]->as<uint32_t>(), c.keys.as<uint64_t>(),
+                                            d_xyz, n, c.keys_alt.as<uint64_t>(), perm_out, c.xs.as<double>(),
+                                            c.ys.as<double>(), c.zs.as<double>(), rc, c.run_list.as<uint32_t>());
+    k_runs_mid<<<sms, kRunMidThreads, 0, c.stream>>>(vb[sel]->as<uint32_t>(), c.keys.as<uint64_t>(), d_xyz,
+                                                     c.keys_alt.as<uint64_t>(), perm_out, c.xs.as<double>(),
+                                                     c.ys.as<double>(), c.zs.as<double>(), rc,
+                                                     c.run_list.as<uint32_t>());
+    *out_sel = sel ^ 1;
     return cudaGetLastError();
 }
 

@@ -54,9 +54,9 @@ class LinearOctree:
 
     def __init__(self, points, encoder="hilbert", max_points_leaf: int = 128, device: int = 0,
                  radius_group: int = 8, stream=None, packet: bool = True, fp32_filter: bool = False,
-                 knn_packet: bool = True, knn_bucket: int = 256):
+                 knn_packet: bool = True, knn_bucket: int = 256, sort_8pass: bool = False):
         self._open(encoder, max_points_leaf, device, radius_group, stream, packet, fp32_filter, knn_packet,
-                   knn_bucket)
+                   knn_bucket, capi.OCT_CLOUD_SORT_8PASS if sort_8pass else 0)
         L, h = self._L, self._h
         dev = _is_device(points)
         if not dev:
@@ -76,12 +76,12 @@ class LinearOctree:
         self.max_depth_seen = info.max_depth_seen
 
     def _open(self, encoder, max_points_leaf, device, radius_group, stream, packet, fp32_filter, knn_packet,
-              knn_bucket):
+              knn_bucket, flags=0):
         L = lib()
         self._L = L
         self.encoder = ENCODERS[encoder] if not isinstance(encoder, (int, np.integer)) else int(encoder)
         self.max_points_leaf = int(max_points_leaf)
-        p = OctParams(self.max_points_leaf, self.encoder, device, 0)
+        p = OctParams(self.max_points_leaf, self.encoder, device, flags)
         h = C.c_void_p()
         st = L.oct_cloud_create(C.byref(p), C.byref(h))
         check(st, None, "oct_cloud_create")

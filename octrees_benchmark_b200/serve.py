@@ -283,6 +283,8 @@ def replay(wl: ServingWorkload, server: Server, drain_s: float = 60.0, owned_ins
     bt = threading.Thread(target=builder, daemon=True)
     bt.start()
     lat, qms, nq_done = [], [], [0]
+    info = {}  # ticket -> request class, for the latency split by class
+    done_lat = []  # (ticket, latency) of every completion
     errors = [0]
     done_evt = threading.Event()
     skipped = [0]
@@ -300,6 +302,7 @@ def replay(wl: ServingWorkload, server: Server, drain_s: float = 60.0, owned_ins
                         lat.append(c["latency_ms"])
                         qms.append(c["queue_ms"])
                         nq_done[0] += c["nq"]
+                        done_lat.append((c["ticket"], c["latency_ms"]))
                     server.release(c["ticket"])
         except Exception as exc:  # noqa: BLE001
             thread_errors.append(("collector", exc))
@@ -354,7 +357,11 @@ def replay(wl: ServingWorkload, server: Server, drain_s: float = 60.0, owned_ins
                 req = Request(proxy, "radius", centres, radius=it.radius, kernel="sphere", algo="neighborsPrune")
             else:
                 req = Request(proxy, "knn", centres, k=it.k)
-            server.submit(req, sync=False)  # the pools were complete before the stream started
+            size = "centres<=1k" if it.nq <= 1000 else ("centres<=10k" if it.nq <= 10_000 else "centres>10k")
+            kind = f"knn k={it.k}" if it.kind == "knn" else ("radius r<=5" if it.radius <= 5.0 else "radius r>5")
+            cl = f"{kind}, {size}"
+            t = server.submit(req, sync=False)  # the pools were complete before the stream started
+            info[t] = cl
     finally:
         t_sub = time.perf_counter() - t0
         th.join(timeout=max(1.0, drain_s))
@@ -369,6 +376,11 @@ def replay(wl: ServingWorkload, server: Server, drain_s: float = 60.0, owned_ins
         raise RuntimeError(f"serving replay: the {name} thread failed: {exc!r}") from exc
     st = server.stats()
     completed = len(lat)
+    cls_lat = {}
+    for t, v in done_lat:
+        cl = info.get(t)
+        if cl is not None:
+            cls_lat.setdefault(cl, []).append(v)
     return {
         "requests": n_total, "completed": completed, "errors": errors[0],
         "unfinished": n_total - completed - errors[0] - skipped[0], "skipped": skipped[0],
@@ -380,6 +392,8 @@ def replay(wl: ServingWorkload, server: Server, drain_s: float = 60.0, owned_ins
         "batches": st["batches"], "admission_stalls": st["admission_stalls"],
         "budget_evictions": st["evictions"], "clouds_inserted": len(inserted) + len(removers),
         "insert_failures": len(failed_epochs), "clouds_removed": len(removers), "peak_budget_bytes": st["peak_bytes"],
+        "by_class": {k: {"requests": len(v), "p50_ms": _pct(v, 50), "p99_ms": _pct(v, 99)}
+                     for k, v in sorted(cls_lat.items())},
     }
 
 
