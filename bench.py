@@ -520,7 +520,8 @@ def run_serving(args, dev):
     wl = ServingWorkload(device=dev, seconds=args.serve_seconds)
     clocks = ClockSampler(dev)
     clocks.start()
-    srv = Server(device=dev, slots=args.serve_slots, max_batch_queries=args.serve_max_batch)
+    srv = Server(device=dev, slots=args.serve_slots, max_batch_queries=args.serve_max_batch,
+                 max_wait_ms=args.serve_max_wait, fifo=args.serve_fifo)
     try:
         batched = replay(wl, srv, drain_s=args.serve_drain)
     finally:
@@ -1016,7 +1017,10 @@ def main():
     ap.add_argument("--serve-drain", type=float, default=10.0,
                     help="seconds each server may take after the stream ends before it is stopped")
     ap.add_argument("--serve-slots", type=int, default=3, help="batches the serving scheduler keeps in flight")
-    ap.add_argument("--serve-max-batch", type=int, default=4 << 20, help="centres per serving batch at most")
+    ap.add_argument("--serve-max-batch", type=int, default=512 << 10, help="centres per serving batch at most")
+    ap.add_argument("--serve-max-wait", type=float, default=40.0,
+                    help="ms after which a queued request is admitted ahead of smaller ones")
+    ap.add_argument("--serve-fifo", action="store_true", help="admit serving requests in arrival order only")
     ap.add_argument("--large", action="store_true", help="also run the 500M-point skewed cloud (not in the default run)")
     ap.add_argument("--large-points", type=int, default=500_000_000)
     ap.add_argument("--large-queries", type=int, default=10_000_000)

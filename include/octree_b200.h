@@ -438,6 +438,8 @@ typedef struct {
     uint64_t submitted, completed, batches, admission_stalls, evictions, queries;
     uint64_t cloud_bytes, inflight_bytes, peak_bytes;
     uint32_t queued, in_flight;
+    double max_submit_ms; /* the longest host call that launched a batch (graph capture included) */
+    double max_finish_ms; /* the longest host call that completed a batch (result-array growth included) */
 } oct_server_stats;
 
 int oct_server_create(const oct_server_params* params, oct_server* out);

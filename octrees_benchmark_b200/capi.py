@@ -87,7 +87,8 @@ class OctServerStats(C.Structure):
     _fields_ = [("submitted", C.c_uint64), ("completed", C.c_uint64), ("batches", C.c_uint64),
                 ("admission_stalls", C.c_uint64), ("evictions", C.c_uint64), ("queries", C.c_uint64),
                 ("cloud_bytes", C.c_uint64), ("inflight_bytes", C.c_uint64), ("peak_bytes", C.c_uint64),
-                ("queued", C.c_uint32), ("in_flight", C.c_uint32)]
+                ("queued", C.c_uint32), ("in_flight", C.c_uint32), ("max_submit_ms", C.c_double),
+                ("max_finish_ms", C.c_double)]
 
 
 class OctError(RuntimeError):

@@ -443,9 +443,11 @@ __device__ __forceinline__ void put_sorted(uint64_t o, uint32_t p, const uint64_
     zs[o] = xyz[3ull * p + 2];
 }
 
-// One thread per run start: runs of one point are copied, runs of up to
-// kRunSmall sorted by insertion (strict >, so equal keys keep their order),
-// longer runs listed for k_runs_mid (start, length) or flagged.
+// One thread per point.  A point of a run of at most kRunSmall points finds
+// its place in the run by counting the run's points that precede it in the
+// stable order (a smaller key, or an equal key earlier in the run) and writes
+// itself there; the first point of a longer run lists it for k_runs_mid
+// (start, length) or flags it when it is longer than kRunMid.
 __global__ void __launch_bounds__(256) k_runs_small(const uint32_t* __restrict__ hi,
                                                     const uint32_t* __restrict__ perm_hi,
                                                     const uint64_t* __restrict__ keys_in,
@@ -456,47 +458,36 @@ __global__ void __launch_bounds__(256) k_runs_small(const uint32_t* __restrict__
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
     for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
         const uint32_t h = hi[i];
-        if (i > 0 && hi[i - 1] == h) continue;  // inside a run: its start handles it
-        uint64_t e = i + 1;
-        while (e < n && e - i <= kRunSmall && hi[e] == h) ++e;
-        const uint64_t len = e - i;
-        if (len == 1) {
-            put_sorted(i, perm_hi[i], keys_in, xyz, keys_out, perm_out, xs, ys, zs);
-            continue;
-        }
-        if (len > kRunSmall) {
-            while (e < n && e - i <= kRunMid && hi[e] == h) ++e;
-            if (e - i > kRunMid) {
+        uint64_t s = i, e = i + 1;
+        while (s > 0 && i - s <= kRunSmall && hi[s - 1] == h) --s;
+        while (e < n && e - s <= kRunSmall && hi[e] == h) ++e;
+        if (e - s > kRunSmall) {  // a longer run: its first point (if this is it) measures and lists it
+            if (s > 0 && hi[s - 1] == h) continue;
+            if (s != i) continue;
+            while (e < n && e - s <= kRunMid && hi[e] == h) ++e;
+            if (e - s > kRunMid) {
                 atomicOr(&rc->big, 1u);
             } else {
                 const uint32_t slot = atomicAdd(&rc->mid_count, 1u);
-                mid_list[2 * slot] = (uint32_t)i;
-                mid_list[2 * slot + 1] = (uint32_t)(e - i);
+                mid_list[2 * slot] = (uint32_t)s;
+                mid_list[2 * slot + 1] = (uint32_t)(e - s);
             }
             continue;
         }
-        uint64_t kk[kRunSmall];
-        uint32_t pp[kRunSmall];
-        for (uint32_t j = 0; j < (uint32_t)len; ++j) {
-            const uint32_t p = perm_hi[i + j];
-            const uint64_t key = keys_in[p];
-            uint32_t m = j;
-            while (m > 0 && kk[m - 1] > key) {
-                kk[m] = kk[m - 1];
-                pp[m] = pp[m - 1];
-                --m;
-            }
-            kk[m] = key;
-            pp[m] = p;
+        const uint32_t p = perm_hi[i];
+        const uint64_t key = keys_in[p];
+        uint64_t rank = 0;
+        for (uint64_t j = s; j < e; ++j) {
+            if (j == i) continue;
+            const uint64_t kj = keys_in[perm_hi[j]];
+            rank += (kj < key || (kj == key && j < i)) ? 1u : 0u;
         }
-        for (uint32_t j = 0; j < (uint32_t)len; ++j) {
-            const uint32_t p = pp[j];
-            keys_out[i + j] = kk[j];
-            perm_out[i + j] = p;
-            xs[i + j] = xyz[3ull * p];
-            ys[i + j] = xyz[3ull * p + 1];
-            zs[i + j] = xyz[3ull * p + 2];
-        }
+        const uint64_t o = s + rank;
+        keys_out[o] = key;
+        perm_out[o] = p;
+        xs[o] = xyz[3ull * p];
+        ys[o] = xyz[3ull * p + 1];
+        zs[o] = xyz[3ull * p + 2];
     }
 }
 

@@ -256,6 +256,10 @@ struct oct_engine_s {
     DevBuf ck_pool, ck_next, ck_first, ck_ctr;  // one-pass radius: result chunks (ck_next has one word per chunk)
     DevBuf knn_fb;  // group kNN fallback list, one entry per query position
     DevBuf knn_heads;  // group kNN: the heads' largest k-th distances (f64 per head)
+    // the growable device arrays above come from this pool in stream order (cudaMallocFromPoolAsync /
+    // cudaFreeAsync on `stream`), so growing one never waits for the device: with batches of other engines
+    // running, a cudaFree / cudaMalloc would wait for all of them
+    cudaMemPool_t pool = nullptr;
     // pinned host staging
     unsigned char* h_stage = nullptr;
     size_t h_stage_bytes = 0;
@@ -314,26 +318,36 @@ void drop_graphs(oct_engine e) {
 
 // Grow a device array (by half again at least); a new address drops the
 // captured graphs, whose nodes hold the old one.
+// A growable array of the engine: the old storage is freed and the new one
+// taken from the engine's pool in the engine stream's order (every earlier use
+// of the old storage is on that stream, or joined into it).
 int grow(oct_engine e, DevBuf& b, size_t bytes) {
     if (bytes <= b.bytes) return OCT_OK;
     drop_graphs(e);
-    size_t want = bytes;
+    size_t want = bytes < 256 ? 256 : bytes;
     if (b.bytes && want < b.bytes + b.bytes / 2) want = b.bytes + b.bytes / 2;
-    cudaError_t r = b.reserve(want);
+    if (b.ptr) EK(cudaFreeAsync(b.ptr, e->stream));
+    b.ptr = nullptr;
+    b.bytes = 0;
+    void* p = nullptr;
+    cudaError_t r = cudaMallocFromPoolAsync(&p, want, e->pool, e->stream);
     if (r != cudaSuccess) {
         cudaGetLastError();
-        r = b.reserve(bytes);
+        want = bytes;
+        r = cudaMallocFromPoolAsync(&p, want, e->pool, e->stream);
     }
     EK(r);
+    b.ptr = p;
+    b.bytes = want;
     return OCT_OK;
 }
 
 int grow_pinned(oct_engine e, size_t bytes) {
     if (bytes <= e->h_stage_bytes) return OCT_OK;
+    const size_t want = std::max(bytes, std::max((size_t)256 << 10, e->h_stage_bytes * 2));
     if (e->h_stage) cudaFreeHost(e->h_stage);
     e->h_stage = nullptr;
     e->h_stage_bytes = 0;
-    const size_t want = std::max(bytes, (size_t)64 << 10);
     EK(cudaMallocHost(reinterpret_cast<void**>(&e->h_stage), want));
     e->h_stage_bytes = want;
     return OCT_OK;
@@ -788,7 +802,26 @@ int oct_engine_create(const oct_engine_params* p, oct_engine* out) {
     if (r == cudaSuccess) r = cudaMemsetAsync(e->epoch.ptr, 0, 256, e->stream);
     if (r == cudaSuccess) r = cudaMemsetAsync(e->stats.ptr, 0, 64, e->stream);
     if (r == cudaSuccess) r = cudaMallocHost(reinterpret_cast<void**>(&e->h_summary), sizeof(Summary));
-    if (r == cudaSuccess && p->reserve_results) r = e->out.reserve(4 * p->reserve_results);
+    if (r == cudaSuccess) {  // the pool of the growable arrays: keeps what it frees, for the next growth
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = e->device;
+        r = cudaMemPoolCreate(&e->pool, &props);
+        uint64_t keep = UINT64_MAX;
+        if (r == cudaSuccess) r = cudaMemPoolSetAttribute(e->pool, cudaMemPoolAttrReleaseThreshold, &keep);
+    }
+    if (r == cudaSuccess && p->reserve_results && grow(e, e->out, 4 * p->reserve_results) != OCT_OK)
+        r = cudaErrorMemoryAllocation;
+    if (r == cudaSuccess && p->reserve_queries) {  // a batch of this many centres grows nothing of these
+        const uint64_t q = p->reserve_queries;
+        DevBuf* per_q8[] = {&e->keys[0], &e->keys[1], &e->counts, &e->offs};
+        for (DevBuf* b : per_q8)
+            if (r == cudaSuccess && grow(e, *b, 8 * (q + 1)) != OCT_OK) r = cudaErrorMemoryAllocation;
+        DevBuf* per_q4[] = {&e->ord[0], &e->ord[1], &e->knn_counts, &e->knn_fb, &e->ck_first};
+        for (DevBuf* b : per_q4)
+            if (r == cudaSuccess && grow(e, *b, 4 * (q + 1)) != OCT_OK) r = cudaErrorMemoryAllocation;
+    }
     if (r == cudaSuccess) r = cudaStreamSynchronize(e->stream);
     if (r != cudaSuccess) {
         cudaGetLastError();
@@ -807,12 +840,18 @@ int oct_engine_destroy(oct_engine e) {
         DeviceGuardE g(e->device);
         if (e->stream) cudaStreamSynchronize(e->stream);
         drop_graphs(e);
-        DevBuf* bufs[] = {&e->desc, &e->keys[0], &e->keys[1], &e->ord[0], &e->ord[1], &e->sort_ctl, &e->sort_status,
-                          &e->epoch, &e->counts, &e->offs, &e->part, &e->out, &e->knn_idx, &e->knn_d2,
-                          &e->knn_counts, &e->ctrs, &e->stats, &e->summary, &e->totals,
-                          &e->ck_pool, &e->ck_next, &e->ck_first, &e->ck_ctr, &e->knn_fb,
-                          &e->knn_heads};
-        for (DevBuf* b : bufs) b->release();
+        DevBuf* fixed[] = {&e->sort_ctl, &e->epoch, &e->part, &e->ctrs, &e->stats, &e->summary};
+        for (DevBuf* b : fixed) b->release();
+        DevBuf* pooled[] = {&e->desc, &e->keys[0], &e->keys[1], &e->ord[0], &e->ord[1], &e->sort_status,
+                            &e->counts, &e->offs, &e->out, &e->knn_idx, &e->knn_d2, &e->knn_counts, &e->totals,
+                            &e->ck_pool, &e->ck_next, &e->ck_first, &e->ck_ctr, &e->knn_fb, &e->knn_heads};
+        for (DevBuf* b : pooled) {
+            if (b->ptr && e->stream) cudaFreeAsync(b->ptr, e->stream);
+            b->ptr = nullptr;
+            b->bytes = 0;
+        }
+        if (e->stream) cudaStreamSynchronize(e->stream);
+        if (e->pool) cudaMemPoolDestroy(e->pool);
         if (e->h_stage) cudaFreeHost(e->h_stage);
         if (e->h_summary) cudaFreeHost(e->h_summary);
         if (e->h_totals) cudaFreeHost(e->h_totals);

@@ -9,11 +9,13 @@
 // steps: (1) batches whose stream has drained are completed - every request of
 // the batch gets its completion record and stays readable in its slot until
 // the client releases it; (2) slots whose requests are all released become
-// free; (3) each free slot takes queued requests in arrival order while the
-// batch stays within the request and centre limits and while the registered
-// clouds, the admitted batches and this batch fit the HBM budget.  A head
-// request that does not fit waits for batches to finish (one admission stall
-// per request), unless nothing is running, in which case it is admitted alone.
+// free; (3) each free slot takes queued requests - first those queued longer
+// than max_wait_ms, in arrival order, then the others smallest estimated work
+// first (OCT_SERVER_FIFO: arrival order only) - while the batch stays within
+// the request and centre limits and while the registered clouds, the admitted
+// batches and this batch fit the HBM budget.  A request that does not fit
+// waits for batches to finish (one admission stall per request), unless
+// nothing is running, in which case it is admitted alone.
 // Batches on different slots overlap on the device.  The budget counts each
 // cloud's device bytes and, per admitted request, its engine arrays (44 B per
 // centre, 12 B per kNN slot) and an estimate of its radius results (pi r^2
@@ -44,6 +46,7 @@ using Clock = std::chrono::steady_clock;
 namespace {
 
 constexpr double kPi = 3.14159265358979323846;
+constexpr size_t kAdmitWindow = 4096;  // queued requests considered per admission
 
 struct CloudEntry {
     uint64_t bytes = 0;
@@ -98,6 +101,7 @@ struct oct_server_s {
     uint64_t cloud_bytes = 0, inflight = 0;
     oct_server_stats st{};
     bool stop = false;
+    bool fifo = false;
     bool head_stalled = false;
     std::thread worker;
     std::string last_error;
@@ -216,10 +220,18 @@ void worker_plain(oct_server s) {
     }
 }
 
+struct Cand {
+    uint32_t cls;  // 0: waited longer than max_wait_ms, 1: the others
+    uint64_t key;  // arrival position (class 0) or estimated work (class 1)
+    uint32_t pos;  // position in the queue
+};
+
 void worker_batched(oct_server s) {
     std::vector<oct_request> reqs;
     std::vector<uint64_t> ids;
     std::vector<oct_request_place> places;
+    std::vector<Cand> cand;
+    std::vector<uint8_t> taken;
     cudaSetDevice(s->p.device);
     std::unique_lock<std::mutex> lk(s->mu);
     while (!s->stop) {
@@ -233,11 +245,15 @@ void worker_batched(oct_server s) {
             int ready = 0;
             const int rs = oct_engine_ready(sl.eng, &ready);
             int st = rs;
+            double wait_ms = 0.0;
             if (rs == OCT_OK && ready) {
                 places.assign(sl.tickets.size(), oct_request_place{});
+                const Clock::time_point w0 = Clock::now();
                 st = oct_engine_wait(sl.eng, places.data(), nullptr);
+                wait_ms = ms_between(w0, Clock::now());
             }
             lk.lock();
+            s->st.max_finish_ms = std::max(s->st.max_finish_ms, wait_ms);
             if (rs == OCT_OK && !ready) continue;
             for (size_t j = 0; j < sl.tickets.size(); ++j) {
                 Ticket& t = s->tickets[sl.tickets[j]];
@@ -257,16 +273,34 @@ void worker_batched(oct_server s) {
                 sl.tickets.clear();
             }
         }
-        // (3) admission into free slots
+        // (3) admission into free slots.  Candidates (the first kAdmitWindow queued requests) in order:
+        // those queued longer than max_wait_ms in arrival order, then the rest smallest estimated work
+        // first (FIFO mode: arrival order only), so that small requests do not wait behind large ones
+        // and no request waits for ever.
         for (size_t i = 0; i < s->slots.size() && !s->queue.empty(); ++i) {
             Slot& sl = s->slots[i];
             if (sl.state != kFree) continue;
             reqs.clear();
             ids.clear();
+            cand.clear();
+            const Clock::time_point now = Clock::now();
+            const size_t window = std::min<size_t>(s->queue.size(), kAdmitWindow);
+            for (size_t pos = 0; pos < window; ++pos) {
+                const Ticket& t = s->tickets[s->queue[pos]];
+                const bool aged = s->fifo || ms_between(t.t_submit, now) > s->p.max_wait_ms;
+                cand.push_back({aged ? 0u : 1u, aged ? (uint64_t)pos : t.est, (uint32_t)pos});
+            }
+            std::sort(cand.begin(), cand.end(), [](const Cand& a, const Cand& b) {
+                return a.cls != b.cls ? a.cls < b.cls : (a.key != b.key ? a.key < b.key : a.pos < b.pos);
+            });
+            taken.assign(window, 0);
             uint64_t q = 0, est = 0;
-            while (!s->queue.empty() && reqs.size() < s->p.max_batch_requests) {
-                Ticket& t = s->tickets[s->queue.front()];
-                if (!reqs.empty() && q + t.req.nq > s->p.max_batch_queries) break;
+            for (size_t ci = 0; ci < cand.size() && reqs.size() < s->p.max_batch_requests; ++ci) {
+                Ticket& t = s->tickets[s->queue[cand[ci].pos]];
+                if (!reqs.empty() && q + t.req.nq > s->p.max_batch_queries) {
+                    if (s->fifo) break;
+                    continue;  // a smaller one may still fit
+                }
                 const bool fits = s->cloud_bytes + s->inflight + est + t.est <= s->p.hbm_budget;
                 const bool alone = reqs.empty() && s->inflight == 0;  // nothing to wait for: admit it alone
                 if (!fits && !alone) {
@@ -281,22 +315,31 @@ void worker_batched(oct_server s) {
                 ids.push_back(t.id);
                 q += t.req.nq;
                 est += t.est;
-                s->queue.pop_front();
+                taken[cand[ci].pos] = 1;
                 if (!fits) break;
             }
             if (reqs.empty()) break;
+            {  // drop the admitted requests from the queue, keeping the others in arrival order
+                std::deque<uint64_t> rest;
+                for (size_t pos = 0; pos < s->queue.size(); ++pos)
+                    if (pos >= window || !taken[pos]) rest.push_back(s->queue[pos]);
+                s->queue.swap(rest);
+            }
             sl.tickets = ids;
             sl.outstanding = (uint32_t)ids.size();
             sl.state = kRunning;  // claimed: clients do not touch it while the lock is dropped
             lk.unlock();
+            const Clock::time_point s0 = Clock::now();
             const int st = oct_engine_submit(sl.eng, reqs.data(), (uint32_t)reqs.size(), nullptr);
+            const double submit_ms = ms_between(s0, Clock::now());
             lk.lock();
-            const Clock::time_point now = Clock::now();
+            s->st.max_submit_ms = std::max(s->st.max_submit_ms, submit_ms);
+            const Clock::time_point launched = Clock::now();
             for (uint64_t id : ids) {
                 Ticket& t = s->tickets[id];
                 t.slot = (int)i;
                 t.launched = true;
-                t.t_launch = now;
+                t.t_launch = launched;
             }
             if (st != OCT_OK) {
                 char buf[512] = {0};
@@ -340,10 +383,12 @@ int oct_server_create(const oct_server_params* p, oct_server* out) {
     if (!s) return OCT_ERR_OUT_OF_MEMORY;
     s->p = *p;
     s->plain = (p->flags & OCT_SERVER_PLAIN) != 0;
+    s->fifo = (p->flags & OCT_SERVER_FIFO) != 0;
     if (s->p.slots == 0) s->p.slots = 3;
     if (s->plain) s->p.slots = 1;
     if (s->p.max_batch_requests == 0) s->p.max_batch_requests = 1024;
-    if (s->p.max_batch_queries == 0) s->p.max_batch_queries = 4ull << 20;
+    if (s->p.max_batch_queries == 0) s->p.max_batch_queries = 512ull << 10;
+    if (!(s->p.max_wait_ms > 0.0)) s->p.max_wait_ms = 40.0;
     if (s->p.hbm_budget == 0) s->p.hbm_budget = 120ull << 30;
     s->slots.resize(s->p.slots);
     if (!s->plain) {
@@ -351,6 +396,7 @@ int oct_server_create(const oct_server_params* p, oct_server* out) {
             oct_engine_params ep{};
             ep.device = p->device;
             ep.reserve_results = 64ull << 20;  // 256 MB of results per slot before the first batch grows it
+            ep.reserve_queries = s->p.max_batch_queries;  // the per-centre arrays of the largest batch
             const int st = oct_engine_create(&ep, &sl.eng);
             if (st != OCT_OK) {
                 oct_server_destroy(s);

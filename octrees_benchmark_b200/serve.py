@@ -21,7 +21,7 @@ from dataclasses import dataclass
 import numpy as np
 
 from . import capi
-from .capi import (OCT_CLOUD_OWNED, OCT_SERVER_PLAIN, OctCompletion, OctRequest, OctSearchConfig, OctServerParams,
+from .capi import (OCT_CLOUD_OWNED, OCT_SERVER_FIFO, OCT_SERVER_PLAIN, OctCompletion, OctRequest, OctSearchConfig, OctServerParams,
                    OctServerStats, lib)
 from .engine import Request
 from .linear_octree import _sync_current_stream
@@ -44,11 +44,12 @@ class Server:
     """A serving scheduler on one device."""
 
     def __init__(self, device: int = 0, plain: bool = False, slots: int = 3, max_batch_requests: int = 1024,
-                 max_batch_queries: int = 4 << 20, hbm_budget: int = 120 << 30):
+                 max_batch_queries: int = 512 << 10, hbm_budget: int = 120 << 30, max_wait_ms: float = 40.0,
+                 fifo: bool = False):
         L = lib()
         self._L = L
-        p = OctServerParams(device, OCT_SERVER_PLAIN if plain else 0, slots, max_batch_requests, max_batch_queries,
-                            hbm_budget)
+        flags = (OCT_SERVER_PLAIN if plain else 0) | (OCT_SERVER_FIFO if fifo else 0)
+        p = OctServerParams(device, flags, slots, max_batch_requests, max_batch_queries, hbm_budget, max_wait_ms)
         h = C.c_void_p()
         _check(L.oct_server_create(C.byref(p), C.byref(h)), None, "oct_server_create")
         self._h = h
@@ -390,6 +391,7 @@ def replay(wl: ServingWorkload, server: Server, drain_s: float = 60.0, owned_ins
         "qps": nq_done[0] / t_end if t_end > 0 else None,
         "submit_lag_p99_ms": 1e3 * _pct(late, 99) if late else None,
         "batches": st["batches"], "admission_stalls": st["admission_stalls"],
+        "max_submit_ms": st["max_submit_ms"], "max_finish_ms": st["max_finish_ms"],
         "budget_evictions": st["evictions"], "clouds_inserted": len(inserted) + len(removers),
         "insert_failures": len(failed_epochs), "clouds_removed": len(removers), "peak_budget_bytes": st["peak_bytes"],
         "by_class": {k: {"requests": len(v), "p50_ms": _pct(v, 50), "p99_ms": _pct(v, 99)}
