@@ -455,26 +455,29 @@ int oct_encode_sort(oct_cloud h, double* box12, uint64_t* keys, uint32_t* perm, 
     if (split) CK(c.keys_hi.reserve(4 * c.n));
     CK(launch_bbox_encode(c, xyz, split ? c.keys_hi.as<uint32_t>() : nullptr));
     uint32_t skip[8] = {0, 0, 0, 0, 0, 0, 0, 0};
-    if (c.n) {
+    auto read_skips = [&]() -> int {  // which digits are the same for every key (their passes are skipped)
         CK(cudaMemcpyAsync(c.pinned, &c.d_ctl.as<SortCtl>()->skip[0], sizeof(skip), cudaMemcpyDeviceToHost,
                            c.stream));
         CK(cudaStreamSynchronize(c.stream));
         memcpy(skip, c.pinned, sizeof(skip));
-    }
-    // the split sort (upper halves, then runs); a run too long for it falls back to the 8-pass sort
+        return OCT_OK;
+    };
+    // the split sort (upper halves, then runs); a run too long for it falls back to the 8-pass sort.
+    // The split sort runs its four passes without reading the skip flags (a pass over a constant digit
+    // keeps the order), so nothing waits for the host between the encode and the end of the sort.
     bool done = false;
     unsigned char* pin = static_cast<unsigned char*>(c.pinned);
     if (split) {
         int psel = 0;
         CK(launch_sort_split(c, skip, xyz, &psel));
         // the run flags and the box and level geometry back to the host in one wait
-        CK(cudaMemcpyAsync(pin + 2048, c.run_ctl.ptr, 16, cudaMemcpyDeviceToHost, c.stream));
+        CK(cudaMemcpyAsync(pin + 2048, c.run_ctl.ptr, 32, cudaMemcpyDeviceToHost, c.stream));
         CK(cudaMemcpyAsync(pin, c.d_box.ptr, sizeof(BoxD) + sizeof(LevelGeom), cudaMemcpyDeviceToHost, c.stream));
         const int st = sync_and_check(c);
         if (st != OCT_OK) return st;
-        uint32_t rc[4];
+        uint32_t rc[8];  // RunCtl: w_count, w_next, b_count, b_next, big, cap, pad
         memcpy(rc, pin + 2048, sizeof(rc));
-        if (rc[2] == 0) {  // no run too long: the outputs are the sorted cloud
+        if (rc[4] == 0) {  // no run too long: the outputs are the sorted cloud
             std::swap(c.keys, c.keys_alt);
             if (psel == 1) std::swap(c.perm, c.perm_alt);
             done = true;
@@ -483,6 +486,10 @@ int oct_encode_sort(oct_cloud h, double* box12, uint64_t* keys, uint32_t* perm, 
     if (!done) {
         if (split)  // the split sort's passes took tiles from the upper digits' counters: rewind them
             CK(cudaMemsetAsync(&c.d_ctl.as<SortCtl>()->tile_ctr[0], 0, sizeof(SortCtl::tile_ctr), c.stream));
+        if (c.n) {
+            const int st = read_skips();
+            if (st != OCT_OK) return st;
+        }
         int sel = 0;
         CK(launch_sort_passes(c, skip, &sel));
         if (sel == 1) {

@@ -422,14 +422,19 @@ __global__ void __launch_bounds__(kSortThreads, 3) k_onesweep(const K* __restric
 // and the reordered SoA coordinates.
 // ---------------------------------------------------------------------------
 constexpr uint32_t kRunSmall = 32;
-constexpr uint32_t kRunMid = 4096;
+constexpr uint32_t kRunWarp = 256;   // runs a warp sorts (kRunSmall < len <= kRunWarp)
+constexpr uint32_t kRunMid = 4096;   // runs a block sorts (kRunWarp < len <= kRunMid)
 constexpr int kRunMidThreads = 1024;
+constexpr int kRunWarpThreads = 256;
 
+// Runs for k_runs_warp are listed from the front of the run list, runs for
+// k_runs_mid from its back (both as (start, length) pairs).
 struct RunCtl {
-    uint32_t mid_count;  // runs for k_runs_mid
-    uint32_t mid_next;   // k_runs_mid's work counter
-    uint32_t big;        // a run longer than kRunMid was found
-    uint32_t pad;
+    uint32_t w_count, w_next;  // warp runs listed, and k_runs_warp's work counter
+    uint32_t b_count, b_next;  // block runs listed, and k_runs_mid's work counter
+    uint32_t big;              // a run longer than kRunMid was found
+    uint32_t cap;              // entries of the run list
+    uint32_t pad[2];
 };
 
 __device__ __forceinline__ void put_sorted(uint64_t o, uint32_t p, const uint64_t* __restrict__ keys_in,
@@ -467,8 +472,12 @@ __global__ void __launch_bounds__(256) k_runs_small(const uint32_t* __restrict__
             while (e < n && e - s <= kRunMid && hi[e] == h) ++e;
             if (e - s > kRunMid) {
                 atomicOr(&rc->big, 1u);
+            } else if (e - s <= kRunWarp) {
+                const uint32_t slot = atomicAdd(&rc->w_count, 1u);
+                mid_list[2 * slot] = (uint32_t)s;
+                mid_list[2 * slot + 1] = (uint32_t)(e - s);
             } else {
-                const uint32_t slot = atomicAdd(&rc->mid_count, 1u);
+                const uint32_t slot = rc->cap - 1u - atomicAdd(&rc->b_count, 1u);
                 mid_list[2 * slot] = (uint32_t)s;
                 mid_list[2 * slot + 1] = (uint32_t)(e - s);
             }
@@ -503,13 +512,14 @@ __global__ void __launch_bounds__(kRunMidThreads) k_runs_mid(const uint32_t* __r
     __shared__ unsigned long long s[kRunMid];
     __shared__ uint32_t s_r;
     const int tid = threadIdx.x;
-    const uint32_t count = rc->mid_count;
+    const uint32_t count = rc->b_count;
     for (;;) {
-        if (tid == 0) s_r = atomicAdd(&rc->mid_next, 1u);
+        if (tid == 0) s_r = atomicAdd(&rc->b_next, 1u);
         __syncthreads();
         const uint32_t r = s_r;
         if (r >= count) break;
-        const uint32_t start = mid_list[2 * r], len = mid_list[2 * r + 1];
+        const uint32_t slot = rc->cap - 1u - r;
+        const uint32_t start = mid_list[2 * slot], len = mid_list[2 * slot + 1];
         uint32_t P = 64;
         while (P < len) P <<= 1;
         for (uint32_t t = tid; t < P; t += kRunMidThreads)
@@ -535,6 +545,54 @@ __global__ void __launch_bounds__(kRunMidThreads) k_runs_mid(const uint32_t* __r
             put_sorted(start + t, perm_hi[start + local], keys_in, xyz, keys_out, perm_out, xs, ys, zs);
         }
         __syncthreads();  // s and s_r are reused by the next run
+    }
+}
+
+// One warp per listed run of kRunSmall < length <= kRunWarp: the same bitonic
+// sort as k_runs_mid in a warp's slice of shared memory.
+__global__ void __launch_bounds__(kRunWarpThreads) k_runs_warp(const uint32_t* __restrict__ perm_hi,
+                                                               const uint64_t* __restrict__ keys_in,
+                                                               const double* __restrict__ xyz,
+                                                               uint64_t* __restrict__ keys_out,
+                                                               uint32_t* __restrict__ perm_out,
+                                                               double* __restrict__ xs, double* __restrict__ ys,
+                                                               double* __restrict__ zs, RunCtl* rc,
+                                                               const uint32_t* __restrict__ mid_list) {
+    __shared__ unsigned long long sw[kRunWarpThreads / 32][kRunWarp];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    unsigned long long* s = sw[warp];
+    const uint32_t count = rc->w_count;
+    for (;;) {
+        uint32_t r = 0;
+        if (lane == 0) r = atomicAdd(&rc->w_next, 1u);
+        r = __shfl_sync(0xffffffffu, r, 0);
+        if (r >= count) break;
+        const uint32_t start = mid_list[2 * r], len = mid_list[2 * r + 1];
+        uint32_t P = 64;
+        while (P < len) P <<= 1;
+        for (uint32_t t = lane; t < P; t += 32)
+            s[t] = t < len ? ((keys_in[perm_hi[start + t]] & 0xffffffffull) << 32) | t : ~0ull;
+        __syncwarp();
+        for (uint32_t k = 2; k <= P; k <<= 1) {
+            for (uint32_t j = k >> 1; j > 0; j >>= 1) {
+                for (uint32_t t = lane; t < P; t += 32) {
+                    const uint32_t o = t ^ j;
+                    if (o > t) {
+                        const unsigned long long a = s[t], b = s[o];
+                        if ((a > b) == ((t & k) == 0)) {
+                            s[t] = b;
+                            s[o] = a;
+                        }
+                    }
+                }
+                __syncwarp();
+            }
+        }
+        for (uint32_t t = lane; t < len; t += 32) {
+            const uint32_t local = (uint32_t)(s[t] & 0xffffffffull);
+            put_sorted(start + t, perm_hi[start + local], keys_in, xyz, keys_out, perm_out, xs, ys, zs);
+        }
+        __syncwarp();
     }
 }
 
@@ -684,7 +742,9 @@ cudaError_t launch_sort_split(Cloud& c, const uint32_t skip[8], const double* d_
     if ((e = c.ys.reserve(b)) != cudaSuccess) return e;
     if ((e = c.zs.reserve(b)) != cudaSuccess) return e;
     RunCtl* rc = c.run_ctl.as<RunCtl>();
-    if ((e = cudaMemsetAsync(rc, 0, sizeof(RunCtl), c.stream)) != cudaSuccess) return e;
+    RunCtl rc0{};
+    rc0.cap = (uint32_t)(n / (kRunSmall + 1) + 1);
+    if ((e = cudaMemcpyAsync(rc, &rc0, sizeof(RunCtl), cudaMemcpyHostToDevice, c.stream)) != cudaSuccess) return e;
     if (n == 0) return cudaSuccess;
     const uint64_t tiles = (n + kSortTile - 1) / kSortTile;
     const size_t status_bytes = tiles * 256 * sizeof(unsigned long long);
@@ -734,6 +794,10 @@ cudaError_t launch_sort_split(Cloud& c, const uint32_t skip[8], const double* d_
     k_runs_small<<<grid, 256, 0, c.stream>>>(kb[sel]->as<uint32_t>(), vb[sel]->as<uint32_t>(), c.keys.as<uint64_t>(),
                                             d_xyz, n, c.keys_alt.as<uint64_t>(), perm_out, c.xs.as<double>(),
                                             c.ys.as<double>(), c.zs.as<double>(), rc, c.run_list.as<uint32_t>());
+    k_runs_warp<<<sms * 8, kRunWarpThreads, 0, c.stream>>>(vb[sel]->as<uint32_t>(), c.keys.as<uint64_t>(), d_xyz,
+                                                           c.keys_alt.as<uint64_t>(), perm_out, c.xs.as<double>(),
+                                                           c.ys.as<double>(), c.zs.as<double>(), rc,
+                                                           c.run_list.as<uint32_t>());
     k_runs_mid<<<sms, kRunMidThreads, 0, c.stream>>>(vb[sel]->as<uint32_t>(), c.keys.as<uint64_t>(), d_xyz,
                                                      c.keys_alt.as<uint64_t>(), perm_out, c.xs.as<double>(),
                                                      c.ys.as<double>(), c.zs.as<double>(), rc,

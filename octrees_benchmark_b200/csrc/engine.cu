@@ -477,7 +477,7 @@ int launch_batch(oct_engine e, bool record_start) {
                 (!e->one_cloud || std::memcmp(&p.view, &e->one_view, sizeof(CloudView)) == 0))
                 exec = p.exec;
         if (!exec) {
-            if (e->graphs.size() >= 16) {  // keep the cache small: the oldest graph goes
+            if (e->graphs.size() >= 64) {  // keep the cache bounded: the oldest graph goes
                 cudaGraphExecDestroy(e->graphs.front().exec);
                 e->graphs.erase(e->graphs.begin());
             }
