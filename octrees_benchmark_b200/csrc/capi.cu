@@ -7,6 +7,8 @@
 #include <utility>
 #include <vector>
 
+#include <mutex>
+
 #include "cloud.h"
 
 using namespace octb;
@@ -45,7 +47,6 @@ int cuda_fail(Cloud& c, cudaError_t e, const char* what) {
         if (_e != cudaSuccess) return cuda_fail(c, _e, #expr); \
     } while (0)
 
-constexpr size_t kPinnedBytes = 4096;
 
 // Synchronise the stream and turn the latched device error word into a status.
 // Pinned staging layout: [0, 2048) readbacks of structs, [2048, 2056) the error word.
@@ -245,6 +246,70 @@ int emit_sorted(Cloud& c, double* box12, uint64_t* keys, uint32_t* perm, double*
 
 }  // namespace
 
+namespace octb {
+
+cudaMemPool_t cloud_pool(int device) {
+    static std::mutex mu;
+    static cudaMemPool_t pools[64] = {};
+    if (device < 0 || device >= 64) return nullptr;
+    std::lock_guard<std::mutex> lk(mu);
+    if (!pools[device]) {
+        cudaMemPoolProps props{};
+        props.allocType = cudaMemAllocationTypePinned;
+        props.location.type = cudaMemLocationTypeDevice;
+        props.location.id = device;
+        cudaMemPool_t pool = nullptr;
+        if (cudaMemPoolCreate(&pool, &props) != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;
+        }
+        uint64_t keep = 8ull << 30;
+        cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
+        pools[device] = pool;
+    }
+    return pools[device];
+}
+
+static std::mutex g_pinned_mu;
+static std::vector<void*> g_pinned_free;
+
+void* pinned_block_get() {
+    {
+        std::lock_guard<std::mutex> lk(g_pinned_mu);
+        if (!g_pinned_free.empty()) {
+            void* p = g_pinned_free.back();
+            g_pinned_free.pop_back();
+            return p;
+        }
+    }
+    void* p = nullptr;
+    if (cudaMallocHost(&p, kPinnedBlock) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    return p;
+}
+
+void pinned_block_put(void* p) {
+    if (!p) return;
+    std::lock_guard<std::mutex> lk(g_pinned_mu);
+    g_pinned_free.push_back(p);
+}
+
+}  // namespace octb
+
+namespace {
+// Every device array of a cloud.
+std::vector<DevBuf*> cloud_bufs(Cloud& c) {
+    return {&c.xyz_in, &c.xs, &c.ys, &c.zs, &c.keys, &c.keys_alt, &c.perm, &c.perm_alt, &c.keys_hi,
+            &c.keys_hi_alt, &c.run_ctl, &c.run_list, &c.sort_status, &c.d_ctl, &c.d_box, &c.d_err, &c.offsets,
+            &c.ranges, &c.centers, &c.frontier, &c.masks, &c.parts, &c.d_build, &c.q_centers, &c.q_radii,
+            &c.q_counts, &c.q_offsets, &c.q_out, &c.q_out2, &c.q_scan_tmp, &c.qs_keys, &c.qs_keys_alt, &c.qs_ord,
+            &c.qs_ord_alt, &c.qs_status, &c.qs_ctl, &c.packet_ctr, &c.knn_fb, &c.knn_heads, &c.stats, &c.rel,
+            &c.crel, &c.cbox, &c.q_axes, &c.ck_pool, &c.ck_next, &c.ck_first, &c.ck_ctr};
+}
+}  // namespace
+
 extern "C" {
 
 int oct_abi_version(void) { return OCT_ABI_VERSION; }
@@ -283,12 +348,18 @@ int oct_cloud_create(const oct_params* p, oct_cloud* out) {
     cudaError_t e = cudaStreamCreateWithFlags(&c.stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) {
         c.own_stream = true;
-        e = c.d_err.reserve(256);
+        cudaMemPool_t pool = cloud_pool(c.device);
+        if (!pool) e = cudaErrorMemoryAllocation;
+        for (DevBuf* b : cloud_bufs(c)) b->bind(pool, &c.stream);
     }
+    if (e == cudaSuccess) e = c.d_err.reserve(256);
     if (e == cudaSuccess) e = cudaMemsetAsync(c.d_err.ptr, 0, 256, c.stream);
     if (e == cudaSuccess) e = c.stats.reserve(64);
     if (e == cudaSuccess) e = cudaMemsetAsync(c.stats.ptr, 0, 64, c.stream);
-    if (e == cudaSuccess) e = cudaMallocHost(&c.pinned, kPinnedBytes);
+    if (e == cudaSuccess) {
+        c.pinned = pinned_block_get();
+        if (!c.pinned) e = cudaErrorMemoryAllocation;
+    }
     if (e == cudaSuccess) e = cudaStreamSynchronize(c.stream);
     if (e != cudaSuccess) {
         cudaGetLastError();
@@ -305,15 +376,9 @@ int oct_cloud_destroy(oct_cloud h) {
     {
         DeviceGuard g(c.device);
         if (c.stream) cudaStreamSynchronize(c.stream);
-        DevBuf* bufs[] = {&c.xyz_in, &c.xs, &c.ys, &c.zs, &c.keys, &c.keys_alt, &c.perm, &c.perm_alt,
-                          &c.sort_status, &c.d_ctl, &c.d_box, &c.d_err, &c.offsets, &c.ranges, &c.centers,
-                          &c.frontier, &c.masks, &c.parts, &c.d_build, &c.q_centers, &c.q_radii, &c.q_counts,
-                          &c.q_offsets, &c.q_out, &c.q_out2, &c.q_scan_tmp, &c.qs_keys, &c.qs_keys_alt, &c.qs_ord,
-                          &c.qs_ord_alt, &c.qs_status, &c.qs_ctl, &c.packet_ctr, &c.stats, &c.rel,
-                          &c.ck_pool, &c.ck_next, &c.ck_first, &c.ck_ctr, &c.knn_fb, &c.knn_heads, &c.crel, &c.q_axes,
-                          &c.keys_hi, &c.keys_hi_alt, &c.run_ctl, &c.run_list};
-        for (DevBuf* b : bufs) b->release();
-        if (c.pinned) cudaFreeHost(c.pinned);
+        for (DevBuf* b : cloud_bufs(c)) b->release();  // in the stream's order: waits for nothing else
+        if (c.stream) cudaStreamSynchronize(c.stream);
+        pinned_block_put(c.pinned);
         for (auto& v : c.ev_pend)
             for (auto& pr : v) c.ev_free.insert(c.ev_free.end(), {pr.first, pr.second});
         for (cudaEvent_t ev : c.ev_free) cudaEventDestroy(ev);
@@ -408,15 +473,8 @@ int oct_search_stats(oct_cloud h, uint64_t* point_tests, uint64_t* fp64_retests,
 int oct_cloud_memory(oct_cloud h, uint64_t* bytes) {
     if (!h || !bytes) return OCT_ERR_INVALID_ARG;
     Cloud& c = h->c;
-    const DevBuf* bufs[] = {&c.xyz_in, &c.xs, &c.ys, &c.zs, &c.keys, &c.keys_alt, &c.perm, &c.perm_alt,
-                            &c.sort_status, &c.d_ctl, &c.d_box, &c.d_err, &c.offsets, &c.ranges, &c.centers,
-                            &c.frontier, &c.masks, &c.parts, &c.d_build, &c.q_centers, &c.q_radii, &c.q_counts,
-                            &c.q_offsets, &c.q_out, &c.q_out2, &c.q_scan_tmp, &c.qs_keys, &c.qs_keys_alt, &c.qs_ord,
-                            &c.qs_ord_alt, &c.qs_status, &c.qs_ctl, &c.packet_ctr, &c.stats, &c.rel,
-                            &c.ck_pool, &c.ck_next, &c.ck_first, &c.ck_ctr, &c.knn_fb, &c.knn_heads, &c.crel, &c.q_axes,
-                          &c.keys_hi, &c.keys_hi_alt, &c.run_ctl, &c.run_list};
     uint64_t s = 0;
-    for (const DevBuf* b : bufs) s += b->bytes;
+    for (const DevBuf* b : cloud_bufs(c)) s += b->bytes;
     *bytes = s;
     return OCT_OK;
 }
@@ -437,6 +495,7 @@ int oct_set_points(oct_cloud h, const double* xyz, uint64_t n, uint32_t flags) {
     c.built = false;
     c.rel_built = false;
     c.crel_built = false;
+    c.cbox_built = false;
     c.node_capacity = 0;
     if (!(flags & OCT_MEM_DEVICE)) CK(cudaStreamSynchronize(c.stream));
     return OCT_OK;
@@ -569,6 +628,7 @@ int oct_set_sorted_points(oct_cloud h, const double* sorted_xyz, const uint64_t*
     c.built = false;
     c.rel_built = false;
     c.crel_built = false;
+    c.cbox_built = false;
     c.node_capacity = 0;
     return OCT_OK;
 }
@@ -601,6 +661,7 @@ int oct_build(oct_cloud h, oct_tree_info* info) {
         CK(cudaMemsetAsync(c.offsets.as<uint32_t>() + c.n_total, 0, 4, c.stream));
         c.rel_built = false;
         c.crel_built = false;
+    c.cbox_built = false;
         if (c.fp32_filter && c.packet) {  // the FP32 search reads leaf-relative coordinates
             CK(launch_leaf_rel(c));
             c.rel_built = true;
@@ -750,6 +811,7 @@ int oct_tree_import(oct_cloud h, const oct_tree_info* info, const double* box12,
     c.built = true;
     c.rel_built = false;
     c.crel_built = false;
+    c.cbox_built = false;
     if (c.fp32_filter && c.packet) {  // the FP32 search reads leaf-relative coordinates
         CK(launch_leaf_rel(c));
         c.rel_built = true;

@@ -13,28 +13,49 @@
 
 namespace octb {
 
-// A grow-only device allocation.
+// A grow-only device allocation.  Bound to a memory pool and a stream (a
+// cloud's arrays), its storage comes from the pool in that stream's order
+// (cudaMallocFromPoolAsync / cudaFreeAsync): building or destroying a cloud
+// then waits for nothing but its own stream, where cudaMalloc / cudaFree would
+// wait for all work on the device (every other cloud's and engine's).
+// Unbound, it uses cudaMalloc / cudaFree.
 struct DevBuf {
     void* ptr = nullptr;
     size_t bytes = 0;
+    cudaMemPool_t pool = nullptr;
+    const cudaStream_t* stream = nullptr;  // the owner's current stream (followed when the owner switches it)
+    void bind(cudaMemPool_t p, const cudaStream_t* s) {
+        pool = p;
+        stream = s;
+    }
     cudaError_t reserve(size_t want) {
         if (want <= bytes) return cudaSuccess;
-        if (ptr) cudaFree(ptr);
-        ptr = nullptr;
-        bytes = 0;
+        release();
         size_t b = want < 256 ? 256 : want;
-        cudaError_t e = cudaMalloc(&ptr, b);
+        cudaError_t e = pool ? cudaMallocFromPoolAsync(&ptr, b, pool, *stream) : cudaMalloc(&ptr, b);
         if (e == cudaSuccess) bytes = b;
+        else ptr = nullptr;
         return e;
     }
     void release() {
-        if (ptr) cudaFree(ptr);
+        if (ptr) {
+            if (pool) cudaFreeAsync(ptr, *stream);
+            else cudaFree(ptr);
+        }
         ptr = nullptr;
         bytes = 0;
     }
     template <class T>
     T* as() const { return static_cast<T*>(ptr); }
 };
+
+// The memory pool of every cloud's arrays on a device (created on first use,
+// kept for the process; it holds up to 8 GB of freed storage for reuse).
+cudaMemPool_t cloud_pool(int device);
+// Pinned host blocks of kPinnedBlock bytes, reused across clouds (cudaFreeHost can wait for the device).
+constexpr size_t kPinnedBlock = 4096;
+void* pinned_block_get();
+void pinned_block_put(void* p);
 
 // Device-side record of the sort (one per cloud): the 8 digit histograms of
 // the keys, their exclusive scans, which passes are skipped (all keys share
@@ -67,6 +88,8 @@ struct CloudView {
     const double* zs;
     const float4* rel;          // FP32 leaf-relative points (packet FP32 path), may be null
     const float4* crel;         // FP32 points relative to the box centre (group kNN FP32 path), may be null
+    const float4* cbox;         // per aligned 32-point chunk of the sorted points: (min xyz, -), (max xyz, -)
+                                // rounded outwards to FP32 (group kNN chunk culling), may be null
     const uint32_t* offsets;
     const uint2* ranges;
     const double* centers;
@@ -171,6 +194,8 @@ struct Cloud {
     bool rel_built = false;
     DevBuf crel;  // FP32 (x, y, z) - box centre per point, for the group kNN's FP32 filter
     bool crel_built = false;
+    DevBuf cbox;  // the chunk boxes of CloudView::cbox, built on the first kNN search
+    bool cbox_built = false;
     // search configuration (oct_set_search_config)
     int packet = 1;
     int fp32_filter = 0;
@@ -248,6 +273,7 @@ cudaError_t launch_query_order(Cloud& c, const double* d_centers, uint64_t nq, c
 cudaError_t launch_leaf_rel(Cloud& c);
 // FP32 coordinates relative to the box centre (group kNN FP32 filter), into c.crel.
 cudaError_t launch_center_rel(Cloud& c);
+cudaError_t launch_chunk_boxes(Cloud& c);
 struct ChunkArgs;
 // mode as launch_radius_table (0 count, 1 fill, 2 one pass into `chunks`)
 cudaError_t launch_radius_packet(Cloud& c, int kernel, int algo, int mode, bool fp32, const double* d_centers,

@@ -608,6 +608,17 @@ int submit(oct_engine e, const oct_request* rq, uint32_t n) {
             }
         }
     }
+    // the chunk boxes the kNN kernels cull with, built on a cloud's first kNN request
+    {
+        for (uint32_t i : rows) {
+            Cloud& c = rq[i].cloud->c;
+            if (rq[i].type != OCT_REQ_KNN || c.cbox_built) continue;
+            DeviceGuardE gc(c.device);
+            EK(launch_chunk_boxes(c));
+            EK(cudaStreamSynchronize(c.stream));
+            c.cbox_built = true;
+        }
+    }
     // sizes, then capacities (growing drops graphs), then the packed table
     uint64_t n_total = 0, n_radius = 0, knn_slots = 0;
     for (uint32_t i : rows) {

@@ -210,7 +210,15 @@ class ServingWorkload:
             self.clouds.append(oc)
             self.pools.append(d[torch.randint(0, spec["n"], (pool,), device="cuda", generator=g)].contiguous())
             del d
-        self.insert_points = pts[len(self.specs):]
+        # the inserted clouds' points and centre pools are on the device before the stream starts, so that
+        # an insertion during the stream allocates nothing outside the library's own pool
+        brng = np.random.default_rng(8)
+        self.insert_points, self.insert_pools = [], []
+        for spec, p in zip(self.insert_specs, pts[len(self.specs):]):
+            d = torch.from_numpy(p).cuda(device)
+            sel = torch.from_numpy(brng.integers(0, spec["n"], pool)).cuda(device)
+            self.insert_points.append(d)
+            self.insert_pools.append(d[sel].contiguous())
         self.stream = serving_stream(rate, seconds, n_clouds=n_clouds, max_batch=min(max_batch, pool),
                                      insert_every=insert_every)
         self.n_points = sum(s["n"] for s in self.specs)
@@ -257,19 +265,14 @@ def replay(wl: ServingWorkload, server: Server, drain_s: float = 60.0, owned_ins
     dev = torch.cuda.current_device()
 
     def builder():
-        brng = np.random.default_rng(8)
         bstream = torch.cuda.Stream(device=dev)
         try:
             for e in range(1, len(wl.insert_specs) + 1):
-                p, spec = wl.insert_points[e - 1], wl.insert_specs[e - 1]
-                sel = brng.integers(0, spec["n"], wl.pool)
+                d, pool, spec = wl.insert_points[e - 1], wl.insert_pools[e - 1], wl.insert_specs[e - 1]
                 try:
                     with torch.cuda.stream(bstream):
-                        d = torch.from_numpy(p).cuda(dev)
-                        pool = torch.from_numpy(p[sel]).cuda(dev)
                         oc = LinearOctree(d, encoder=spec["encoder"], max_points_leaf=spec["max_leaf"], device=dev)
                     bstream.synchronize()  # this stream only: never the device
-                    del d
                     built[e] = (oc, pool)
                 except Exception as exc:  # noqa: BLE001 - reported with the figures
                     thread_errors.append(("insert builder", exc))
