@@ -447,6 +447,17 @@ def run_large(args, dev):
     tests, retests = C.c_uint64(), C.c_uint64()
     L.oct_search_stats(h, C.byref(tests), C.byref(retests), 1)
     total_nbrs = int(counts.sum().item())
+    # the same counts in FP64 (no filter), for the FP32 filter's effect on a cloud far larger than L2
+    config(1, 0)
+    counts64 = torch.empty(nq, dtype=torch.int64, device="cuda")
+    ev0.record(stream)
+    capi.check(L.oct_radius_count(h, 1, 2, qr.data_ptr(), nq, None, RADIUS, counts64.data_ptr(), MD), h)
+    ev1.record(stream)
+    capi.check(L.oct_synchronize(h), h)
+    rad64_ms = ev0.elapsed_time(ev1)
+    counts_equal = bool(torch.equal(counts, counts64))
+    del counts64
+    config(1, 1)
     # kNN k = 1000 in batches (the outputs of all 10M centres would be 120 GB)
     K = args.large_k
     kb = min(nq, 1_000_000)
@@ -501,6 +512,7 @@ def run_large(args, dev):
         "build_ms": 1e3 * build_s, "build_mpts_s": n / build_s / 1e6,
         "build_frac_of_hbm": build_bytes / build_s / 1e9 / peak, "nodes": info.n_total, "depth": info.max_depth_seen,
         "radius_ms": rad_ms, "radius_qps": nq / (rad_ms / 1e3), "radius_neighbours": total_nbrs,
+        "radius_fp64_ms": rad64_ms, "radius_fp32_vs_fp64": rad64_ms / rad_ms, "radius_counts_equal_fp64": counts_equal,
         "radius_neighbours_per_s": total_nbrs / (rad_ms / 1e3),
         "band_hit_fraction": retests.value / tests.value if tests.value else None,
         "knn_ms": knn_ms, "knn_qps": nq / (knn_ms / 1e3),

@@ -306,7 +306,7 @@ std::vector<DevBuf*> cloud_bufs(Cloud& c) {
             &c.ranges, &c.centers, &c.frontier, &c.masks, &c.parts, &c.d_build, &c.q_centers, &c.q_radii,
             &c.q_counts, &c.q_offsets, &c.q_out, &c.q_out2, &c.q_scan_tmp, &c.qs_keys, &c.qs_keys_alt, &c.qs_ord,
             &c.qs_ord_alt, &c.qs_status, &c.qs_ctl, &c.packet_ctr, &c.knn_fb, &c.knn_heads, &c.stats, &c.rel,
-            &c.crel, &c.cbox, &c.q_axes, &c.ck_pool, &c.ck_next, &c.ck_first, &c.ck_ctr};
+            &c.crel, &c.q_axes, &c.ck_pool, &c.ck_next, &c.ck_first, &c.ck_ctr};
 }
 }  // namespace
 
@@ -495,7 +495,6 @@ int oct_set_points(oct_cloud h, const double* xyz, uint64_t n, uint32_t flags) {
     c.built = false;
     c.rel_built = false;
     c.crel_built = false;
-    c.cbox_built = false;
     c.node_capacity = 0;
     if (!(flags & OCT_MEM_DEVICE)) CK(cudaStreamSynchronize(c.stream));
     return OCT_OK;
@@ -628,7 +627,6 @@ int oct_set_sorted_points(oct_cloud h, const double* sorted_xyz, const uint64_t*
     c.built = false;
     c.rel_built = false;
     c.crel_built = false;
-    c.cbox_built = false;
     c.node_capacity = 0;
     return OCT_OK;
 }
@@ -661,7 +659,6 @@ int oct_build(oct_cloud h, oct_tree_info* info) {
         CK(cudaMemsetAsync(c.offsets.as<uint32_t>() + c.n_total, 0, 4, c.stream));
         c.rel_built = false;
         c.crel_built = false;
-    c.cbox_built = false;
         if (c.fp32_filter && c.packet) {  // the FP32 search reads leaf-relative coordinates
             CK(launch_leaf_rel(c));
             c.rel_built = true;
@@ -811,7 +808,6 @@ int oct_tree_import(oct_cloud h, const oct_tree_info* info, const double* box12,
     c.built = true;
     c.rel_built = false;
     c.crel_built = false;
-    c.cbox_built = false;
     if (c.fp32_filter && c.packet) {  // the FP32 search reads leaf-relative coordinates
         CK(launch_leaf_rel(c));
         c.rel_built = true;

@@ -88,8 +88,6 @@ struct CloudView {
     const double* zs;
     const float4* rel;          // FP32 leaf-relative points (packet FP32 path), may be null
     const float4* crel;         // FP32 points relative to the box centre (group kNN FP32 path), may be null
-    const float4* cbox;         // per aligned 32-point chunk of the sorted points: (min xyz, -), (max xyz, -)
-                                // rounded outwards to FP32 (group kNN chunk culling), may be null
     const uint32_t* offsets;
     const uint2* ranges;
     const double* centers;
@@ -194,8 +192,6 @@ struct Cloud {
     bool rel_built = false;
     DevBuf crel;  // FP32 (x, y, z) - box centre per point, for the group kNN's FP32 filter
     bool crel_built = false;
-    DevBuf cbox;  // the chunk boxes of CloudView::cbox, built on the first kNN search
-    bool cbox_built = false;
     // search configuration (oct_set_search_config)
     int packet = 1;
     int fp32_filter = 0;
@@ -273,7 +269,6 @@ cudaError_t launch_query_order(Cloud& c, const double* d_centers, uint64_t nq, c
 cudaError_t launch_leaf_rel(Cloud& c);
 // FP32 coordinates relative to the box centre (group kNN FP32 filter), into c.crel.
 cudaError_t launch_center_rel(Cloud& c);
-cudaError_t launch_chunk_boxes(Cloud& c);
 struct ChunkArgs;
 // mode as launch_radius_table (0 count, 1 fill, 2 one pass into `chunks`)
 cudaError_t launch_radius_packet(Cloud& c, int kernel, int algo, int mode, bool fp32, const double* d_centers,

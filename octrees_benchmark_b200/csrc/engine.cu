@@ -608,17 +608,6 @@ int submit(oct_engine e, const oct_request* rq, uint32_t n) {
             }
         }
     }
-    // the chunk boxes the kNN kernels cull with, built on a cloud's first kNN request
-    {
-        for (uint32_t i : rows) {
-            Cloud& c = rq[i].cloud->c;
-            if (rq[i].type != OCT_REQ_KNN || c.cbox_built) continue;
-            DeviceGuardE gc(c.device);
-            EK(launch_chunk_boxes(c));
-            EK(cudaStreamSynchronize(c.stream));
-            c.cbox_built = true;
-        }
-    }
     // sizes, then capacities (growing drops graphs), then the packed table
     uint64_t n_total = 0, n_radius = 0, knn_slots = 0;
     for (uint32_t i : rows) {
@@ -832,6 +821,24 @@ int oct_engine_create(const oct_engine_params* p, oct_engine* out) {
         DevBuf* per_q4[] = {&e->ord[0], &e->ord[1], &e->knn_counts, &e->knn_fb, &e->ck_first};
         for (DevBuf* b : per_q4)
             if (r == cudaSuccess && grow(e, *b, 4 * (q + 1)) != OCT_OK) r = cudaErrorMemoryAllocation;
+        // kNN results of up to 256 neighbours per centre, the request table of 1024 requests, the sort's
+        // look-back words, the group kNN's heads and the one-pass radius search's chunk pool
+        const uint64_t tiles = (q + sort_tile_keys() - 1) / sort_tile_keys();
+        const size_t want[][2] = {{0, 4 * q * 256}, {1, 8 * q * 256}, {2, sizeof(ReqTotal) * 1024},
+                                  {3, table_offset() + 1024 * sizeof(SearchReq)}, {4, 256 * 8 * tiles},
+                                  {5, 8 * (q / kKnnGroupQueries / kKnnHeadStride + 1026)}, {6, 256}};
+        DevBuf* bufs[] = {&e->knn_idx, &e->knn_d2, &e->totals, &e->desc, &e->sort_status, &e->knn_heads, &e->ck_ctr};
+        for (const auto& w : want)
+            if (r == cudaSuccess && grow(e, *bufs[w[0]], w[1]) != OCT_OK) r = cudaErrorMemoryAllocation;
+        if (r == cudaSuccess) r = cudaMemsetAsync(e->sort_status.ptr, 0, e->sort_status.bytes, e->stream);
+        const uint64_t chunks = std::max<uint64_t>(3 * q + 1024, e->out.bytes / (4ull * kResultChunk) + q);
+        if (r == cudaSuccess && grow_chunks(e, chunks) != OCT_OK) r = cudaErrorMemoryAllocation;
+        if (r == cudaSuccess && grow_pinned(e, table_offset() + 1024 * sizeof(SearchReq)) != OCT_OK)
+            r = cudaErrorMemoryAllocation;
+        if (r == cudaSuccess) {
+            r = cudaMallocHost(reinterpret_cast<void**>(&e->h_totals), sizeof(ReqTotal) * 1024);
+            if (r == cudaSuccess) e->h_totals_cap = 1024;
+        }
     }
     if (r == cudaSuccess) r = cudaStreamSynchronize(e->stream);
     if (r != cudaSuccess) {

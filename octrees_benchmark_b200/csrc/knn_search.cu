@@ -47,7 +47,6 @@ struct KnnArgs {
     const uint32_t* order;  // query visiting order (curve order), or nullptr
     uint32_t bucket;        // subtrees with at most this many points are scanned as one range
     const DynGroup* grp;    // table launch (k_knn<LCAP, true>): sizes and requests on the device
-    const float4* cbox;     // chunk boxes (CloudView::cbox), or nullptr
 };
 
 __device__ __forceinline__ bool pair_less(double da, uint32_t ia, double db, uint32_t ib) {
@@ -238,23 +237,12 @@ __global__ void __launch_bounds__(kKnnThreads) k_knn(KnnArgs a) {
                 }
             }
             if (eb != 0xffffffffu) {
-                // points [ea, eb): distances, candidates into the buffer.  With chunk boxes (the packet
-                // path), aligned 32-point chunks whose box lies beyond the threshold are skipped (every lane
-                // computes the same bound, so the skip is uniform)
-                const float4* cbox = CARRY ? KV(cbox) : nullptr;
-                for (uint32_t b = cbox ? (ea & ~31u) : ea; b < eb; b += 32) {
-                    if (cbox) {
-                        const float4 lo = cbox[2 * (b >> 5)], hi = cbox[2 * (b >> 5) + 1];
-                        const double blo[3] = {lo.x, lo.y, lo.z}, bhi[3] = {hi.x, hi.y, hi.z};
-                        double dd[3];
-#pragma unroll
-                        for (int ax = 0; ax < 3; ++ax) dd[ax] = dsub(p[ax], smax(blo[ax], smin(p[ax], bhi[ax])));
-                        if (dsq3(dd[0], dd[1], dd[2]) > thr) continue;
-                    }
+                // points [ea, eb): distances, candidates into the buffer
+                for (uint32_t b = ea; b < eb; b += 32) {
                     const uint32_t i = b + lane;
                     double d = INFINITY;
                     bool cand = false;
-                    if (i >= ea && i < eb) {
+                    if (i < eb) {
                         d = dist_pp(p[0], p[1], p[2], KV(xs)[i], KV(ys)[i], KV(zs)[i]);
                         cand = pair_less(d, i, thr, thr_i);
                     }
@@ -1083,30 +1071,9 @@ __global__ void __launch_bounds__(kGrpThreads, kGrpMinBlocks) k_knn_group(KnnGro
                     est_pend &= ~pend;
                     __syncwarp();
                 }
-                // aligned 32-point chunks; with chunk boxes, a chunk is tested only against the queries whose
-                // lower bound to its box is within their threshold (lanes j < G judge query j; a culled chunk's
-                // points are neither read nor tested)
-                const float4* cbox = KRQV(cbox);
-                for (uint32_t b = cbox ? (ea & ~31u) : ea; b < eb; b += 32) {
-                    uint32_t mc = m;
-                    if (cbox) {
-                        bool keep = false;
-                        if (lane < G && ((m >> lane) & 1u)) {
-                            const float4 lo = cbox[2 * (b >> 5)], hi = cbox[2 * (b >> 5) + 1];
-                            double d[3];
-                            const double blo[3] = {lo.x, lo.y, lo.z}, bhi[3] = {hi.x, hi.y, hi.z};
-#pragma unroll
-                            for (int ax = 0; ax < 3; ++ax) {
-                                const double cl = smax(blo[ax], smin(qs[lane][ax], bhi[ax]));
-                                d[ax] = dsub(qs[lane][ax], cl);
-                            }
-                            keep = !(dsq3(d[0], d[1], d[2]) > thr[lane]);
-                        }
-                        mc = __ballot_sync(0xffffffffu, keep) & m;
-                        if (!mc) continue;
-                    }
+                for (uint32_t b = ea; b < eb; b += 32) {
                     const uint32_t i = b + lane;
-                    const bool in = i >= ea && i < eb;
+                    const bool in = i < eb;
                     double px = 0.0, py = 0.0, pz = 0.0;
                     float4 pf = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
                     bool have64 = !F32;  // the FP32 form reads FP64 coordinates only for points near a threshold
@@ -1119,11 +1086,8 @@ __global__ void __launch_bounds__(kGrpThreads, kGrpMinBlocks) k_knn_group(KnnGro
                             pz = KRQV(zs)[i];
                         }
                     }
-                    if (F32 && lane == 0) {
-                        const uint32_t lo_i = b > ea ? b : ea, hi_i = eb - b < 32u ? eb : b + 32;
-                        f_tests += (unsigned long long)__popc(mc) * (hi_i - lo_i);
-                    }
-                    uint32_t rem = mc;
+                    if (F32 && lane == 0) f_tests += (unsigned long long)__popc(m) * ((eb - b < 32u) ? (eb - b) : 32u);
+                    uint32_t rem = m;
                     while (rem) {
                         const int j = __ffs(rem) - 1;
                         rem &= rem - 1;
@@ -1496,11 +1460,6 @@ cudaError_t launch_knn(Cloud& c, const double* d_centers, uint64_t nq, uint32_t 
     if (c.packet) {  // curve-ordered queries: neighbouring warps share octants in cache
         cudaError_t e;
         if ((e = launch_query_order(c, d_centers, nq, &a.order)) != cudaSuccess) return e;
-        if (!c.cbox_built) {  // the chunk boxes the packet path's kernels cull with, built on first use
-            if ((e = launch_chunk_boxes(c)) != cudaSuccess) return e;
-            c.cbox_built = true;
-        }
-        a.cbox = c.cbox.as<float4>();
     }
     const uint64_t want = (nq + kKnnWarps - 1) / kKnnWarps;
     const uint64_t cap = (uint64_t)sm_count_k(c.device) * 16;

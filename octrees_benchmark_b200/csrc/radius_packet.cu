@@ -885,42 +885,6 @@ cudaError_t launch_center_rel(Cloud& c) {
     return cudaGetLastError();
 }
 
-// Bounding box of each aligned 32-point chunk of the sorted points (one warp
-// per chunk), rounded outwards to FP32: every point of the chunk lies in it,
-// so the FP64 lower bound of a query's distance to it (the clamp-to-box form
-// of distPointOctantSquared) is at most the FP64 distance to any of its points.
-__global__ void k_chunk_boxes(const double* __restrict__ xs, const double* __restrict__ ys,
-                              const double* __restrict__ zs, uint64_t n, float4* __restrict__ out) {
-    const uint64_t w = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
-    const int lane = threadIdx.x & 31;
-    const uint64_t chunks = (n + 31) / 32;
-    if (w >= chunks) return;
-    const uint64_t i = 32 * w + lane;
-    const uint64_t j = i < n ? i : 32 * w;  // the chunk's first point stands in for missing ones
-    double lo[3] = {xs[j], ys[j], zs[j]}, hi[3] = {lo[0], lo[1], lo[2]};
-#pragma unroll
-    for (int off = 16; off > 0; off >>= 1)
-#pragma unroll
-        for (int a = 0; a < 3; ++a) {
-            lo[a] = fmin(lo[a], __shfl_xor_sync(0xffffffffu, lo[a], off));
-            hi[a] = fmax(hi[a], __shfl_xor_sync(0xffffffffu, hi[a], off));
-        }
-    if (lane == 0) {
-        out[2 * w] = make_float4(__double2float_rd(lo[0]), __double2float_rd(lo[1]), __double2float_rd(lo[2]), 0.f);
-        out[2 * w + 1] = make_float4(__double2float_ru(hi[0]), __double2float_ru(hi[1]), __double2float_ru(hi[2]), 0.f);
-    }
-}
-
-cudaError_t launch_chunk_boxes(Cloud& c) {
-    cudaError_t e;
-    const uint64_t chunks = (c.n + 31) / 32;
-    if ((e = c.cbox.reserve(32 * (chunks ? chunks : 1))) != cudaSuccess) return e;
-    if (c.n == 0) return cudaSuccess;
-    k_chunk_boxes<<<(unsigned)((32 * chunks + 255) / 256), 256, 0, c.stream>>>(
-        c.xs.as<double>(), c.ys.as<double>(), c.zs.as<double>(), c.n, c.cbox.as<float4>());
-    return cudaGetLastError();
-}
-
 cudaError_t launch_leaf_rel(Cloud& c) {
     cudaError_t e;
     if ((e = c.rel.reserve(16 * (c.n ? c.n : 1))) != cudaSuccess) return e;
@@ -939,7 +903,6 @@ CloudView cloud_view(const Cloud& c) {
     v.zs = c.zs.as<double>();
     v.rel = c.rel.as<float4>();
     v.crel = c.crel_built ? c.crel.as<float4>() : nullptr;
-    v.cbox = c.cbox_built ? c.cbox.as<float4>() : nullptr;
     v.offsets = c.offsets.as<uint32_t>();
     v.ranges = c.ranges.as<uint2>();
     v.centers = c.centers.as<double>();
