@@ -9,6 +9,8 @@
 
 #include <mutex>
 
+#include <cudaTypedefs.h>
+
 #include "cloud.h"
 
 using namespace octb;
@@ -296,17 +298,80 @@ void pinned_block_put(void* p) {
     g_pinned_free.push_back(p);
 }
 
+const void* kernel_anchor_capi() { return reinterpret_cast<const void*>(&k_soa_to_aos); }
+
+// Every kernel of the library's device code loaded into the current device's
+// context: the device library of each source file is found from one of its
+// kernels, its kernels enumerated and each loaded (cuFuncLoad, CUDA 12.4+,
+// reached through the runtime's driver entry points, so the library does not
+// link the driver).  Once per device; a driver without these entry points
+// leaves loading to the first launches.
+int preload_kernels(int device) {
+    static std::mutex mu;
+    static bool done[64] = {};
+    if (device < 0 || device >= 64) return OCT_ERR_INVALID_ARG;
+    std::lock_guard<std::mutex> lk(mu);
+    if (done[device]) return OCT_OK;
+    PFN_cuKernelGetLibrary_v12050 get_lib = nullptr;
+    PFN_cuLibraryGetKernelCount_v12040 count_kernels = nullptr;
+    PFN_cuLibraryEnumerateKernels_v12040 list_kernels = nullptr;
+    PFN_cuKernelGetFunction_v12000 get_func = nullptr;
+    PFN_cuFuncLoad_v12040 load = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    bool ok = cudaGetDriverEntryPointByVersion("cuKernelGetLibrary", reinterpret_cast<void**>(&get_lib), 12050,
+                                               cudaEnableDefault, &q) == cudaSuccess && get_lib;
+    ok = ok && cudaGetDriverEntryPointByVersion("cuLibraryGetKernelCount", reinterpret_cast<void**>(&count_kernels),
+                                                12040, cudaEnableDefault, &q) == cudaSuccess && count_kernels;
+    ok = ok && cudaGetDriverEntryPointByVersion("cuLibraryEnumerateKernels", reinterpret_cast<void**>(&list_kernels),
+                                                12040, cudaEnableDefault, &q) == cudaSuccess && list_kernels;
+    ok = ok && cudaGetDriverEntryPointByVersion("cuKernelGetFunction", reinterpret_cast<void**>(&get_func), 12000,
+                                                cudaEnableDefault, &q) == cudaSuccess && get_func;
+    ok = ok && cudaGetDriverEntryPointByVersion("cuFuncLoad", reinterpret_cast<void**>(&load), 12040,
+                                                cudaEnableDefault, &q) == cudaSuccess && load;
+    if (!ok) {
+        cudaGetLastError();
+        done[device] = true;
+        return OCT_OK;
+    }
+    const void* anchors[] = {kernel_anchor_capi(),          kernel_anchor_encode_sort(),
+                             kernel_anchor_engine(),        kernel_anchor_knn_search(),
+                             kernel_anchor_octree_build(),  kernel_anchor_radius_packet(),
+                             kernel_anchor_radius_search()};
+    std::vector<CUkernel> kernels;
+    for (const void* a : anchors) {
+        cudaKernel_t k = nullptr;
+        CUlibrary lib = nullptr;
+        unsigned int n = 0;
+        if (cudaGetKernel(&k, a) != cudaSuccess || get_lib(&lib, k) != CUDA_SUCCESS ||
+            count_kernels(&n, lib) != CUDA_SUCCESS) {
+            cudaGetLastError();
+            return OCT_ERR_CUDA;
+        }
+        kernels.resize(n);
+        if (n && list_kernels(kernels.data(), n, lib) != CUDA_SUCCESS) return OCT_ERR_CUDA;
+        for (CUkernel kk : kernels) {
+            CUfunction f = nullptr;
+            if (get_func(&f, kk) != CUDA_SUCCESS || load(f) != CUDA_SUCCESS) return OCT_ERR_CUDA;
+        }
+    }
+    done[device] = true;
+    return OCT_OK;
+}
+
 }  // namespace octb
 
 namespace {
 // Every device array of a cloud.
 std::vector<DevBuf*> cloud_bufs(Cloud& c) {
-    return {&c.xyz_in, &c.xs, &c.ys, &c.zs, &c.keys, &c.keys_alt, &c.perm, &c.perm_alt, &c.keys_hi,
-            &c.keys_hi_alt, &c.run_ctl, &c.run_list, &c.sort_status, &c.d_ctl, &c.d_box, &c.d_err, &c.offsets,
-            &c.ranges, &c.centers, &c.frontier, &c.masks, &c.parts, &c.d_build, &c.q_centers, &c.q_radii,
-            &c.q_counts, &c.q_offsets, &c.q_out, &c.q_out2, &c.q_scan_tmp, &c.qs_keys, &c.qs_keys_alt, &c.qs_ord,
-            &c.qs_ord_alt, &c.qs_status, &c.qs_ctl, &c.packet_ctr, &c.knn_fb, &c.knn_heads, &c.stats, &c.rel,
-            &c.crel, &c.q_axes, &c.ck_pool, &c.ck_next, &c.ck_first, &c.ck_ctr};
+    return {&c.xyz_in,   &c.xs,        &c.ys,          &c.zs,          &c.keys,       &c.keys_alt,
+            &c.perm,     &c.perm_alt,  &c.keys_hi,     &c.keys_hi_alt, &c.run_pv,     &c.run_pv_alt,
+            &c.run_ctl,  &c.run_list,  &c.sort_status, &c.d_ctl,       &c.d_box,      &c.d_err,
+            &c.offsets,  &c.ranges,    &c.centers,     &c.frontier,    &c.masks,      &c.parts,
+            &c.d_build,  &c.q_centers, &c.q_radii,     &c.q_counts,    &c.q_offsets,  &c.q_out,
+            &c.q_out2,   &c.q_scan_tmp, &c.qs_keys,    &c.qs_keys_alt, &c.qs_ord,     &c.qs_ord_alt,
+            &c.qs_status, &c.qs_ctl,   &c.packet_ctr,  &c.knn_fb,      &c.knn_heads,  &c.stats,
+            &c.rel,      &c.crel,      &c.q_axes,      &c.ck_pool,     &c.ck_next,    &c.ck_first,
+            &c.ck_ctr};
 }
 }  // namespace
 

@@ -157,6 +157,7 @@ struct Cloud {
     DevBuf keys, keys_alt;  // u64 keys (sorted result lives in `keys`)
     DevBuf perm, perm_alt;  // u32 input position of each sorted point
     DevBuf keys_hi, keys_hi_alt;  // u32 upper key halves (the split sort)
+    DevBuf run_pv, run_pv_alt;    // u64 lower key half << 32 | input position (the split sort)
     DevBuf run_ctl, run_list;     // the split sort's run bookkeeping
     int split_sort = 1;           // sort the upper halves, then the runs (0: the 8-pass sort)
     DevBuf sort_status;     // onesweep look-back words
@@ -332,6 +333,22 @@ cudaError_t launch_sort_dyn(int device, cudaStream_t s, uint64_t* k0, uint64_t* 
                             uint32_t** result_vals);
 cudaError_t launch_knn(Cloud& c, const double* d_centers, uint64_t nq, uint32_t k, uint32_t* d_idx, double* d_d2,
                        uint32_t* d_counts);
+
+// One kernel of each source file's device code (each file is its own device
+// library), and the loading of every kernel of those libraries on a device
+// (capi.cu).  Under lazy module loading, the CUDA default, a kernel is loaded
+// at its first launch and the load can wait for the work in flight on the
+// device; a server meeting a kernel variant for the first time mid-stream
+// would hold its batches that long.  preload_kernels loads them all once per
+// device up front.
+const void* kernel_anchor_capi();
+const void* kernel_anchor_encode_sort();
+const void* kernel_anchor_engine();
+const void* kernel_anchor_knn_search();
+const void* kernel_anchor_octree_build();
+const void* kernel_anchor_radius_packet();
+const void* kernel_anchor_radius_search();
+int preload_kernels(int device);
 
 }  // namespace octb
 

@@ -255,19 +255,23 @@ __global__ void __launch_bounds__(256) k_scan_hist(SortCtl* ctl, uint64_t n, con
 }
 
 // K: uint64_t (the full keys; digit `pass` is bits 8 pass .. 8 pass + 7) or
-// uint32_t (the upper key halves; digit `pass` (4..7) is bits 8 pass - 32 ..)
-template <bool FIRST, class K = uint64_t>
+// uint32_t (the upper key halves; digit `pass` (4..7) is bits 8 pass - 32 ..).
+// V: uint32_t (the input position) or uint64_t (the lower key half << 32 | the
+// input position; the first pass takes the lower halves from `lo_src`, the
+// whole keys in input order).
+template <bool FIRST, class K = uint64_t, class V = uint32_t>
 __global__ void __launch_bounds__(kSortThreads, 3) k_onesweep(const K* __restrict__ kin,
-                                                           const uint32_t* __restrict__ vin,
-                                                           K* __restrict__ kout, uint32_t* __restrict__ vout,
+                                                           const V* __restrict__ vin,
+                                                           K* __restrict__ kout, V* __restrict__ vout,
                                                            uint64_t n, int pass, SortCtl* ctl,
                                                            unsigned long long* status, uint32_t epoch,
                                                            uint32_t* err, const uint64_t* d_n = nullptr,
-                                                           const uint32_t* d_epoch = nullptr) {
+                                                           const uint32_t* d_epoch = nullptr,
+                                                           const uint64_t* __restrict__ lo_src = nullptr) {
     extern __shared__ __align__(16) unsigned char smem[];
-    K* skeys = reinterpret_cast<K*>(smem);                                     // kSortTile
-    uint32_t* svals = reinterpret_cast<uint32_t*>(skeys + kSortTile);          // kSortTile
-    uint32_t* wcnt = svals + kSortTile;                                        // kSortWarps x 256
+    V* svals = reinterpret_cast<V*>(smem);                                     // kSortTile
+    K* skeys = reinterpret_cast<K*>(svals + kSortTile);                        // kSortTile
+    uint32_t* wcnt = reinterpret_cast<uint32_t*>(skeys + kSortTile);           // kSortWarps x 256
     uint32_t* tstart = wcnt + kSortWarps * 256;                                // 256
     unsigned long long* gbase = reinterpret_cast<unsigned long long*>(tstart + 256);  // 256
     __shared__ uint32_t s_tile;
@@ -291,15 +295,19 @@ __global__ void __launch_bounds__(kSortThreads, 3) k_onesweep(const K* __restric
     const uint64_t base = (uint64_t)tile * kSortTile;
 
     K k[kSortItems];
-    uint32_t v[kSortItems];
+    V v[kSortItems];
     uint32_t rank[kSortItems];
 #pragma unroll
     for (int j = 0; j < kSortItems; ++j) {
         const uint64_t idx = base + (uint64_t)warp * (32 * kSortItems) + (uint64_t)j * 32 + lane;
         const bool valid = idx < n;
         k[j] = valid ? kin[idx] : (K)~0ull;
-        if (FIRST) v[j] = (uint32_t)idx;
-        else v[j] = valid ? vin[idx] : 0u;
+        if (FIRST) {
+            if constexpr (sizeof(V) == 8) v[j] = ((valid ? lo_src[idx] : 0ull) << 32) | (uint64_t)(uint32_t)idx;
+            else v[j] = (V)(uint32_t)idx;
+        } else {
+            v[j] = valid ? vin[idx] : (V)0;
+        }
     }
     // stable rank inside the warp: item j of lane l precedes item j of lane l+1,
     // and every item j precedes item j+1.  The lanes holding the same digit are
@@ -437,11 +445,14 @@ struct RunCtl {
     uint32_t pad[2];
 };
 
-__device__ __forceinline__ void put_sorted(uint64_t o, uint32_t p, const uint64_t* __restrict__ keys_in,
-                                           const double* __restrict__ xyz, uint64_t* __restrict__ keys_out,
-                                           uint32_t* __restrict__ perm_out, double* __restrict__ xs,
-                                           double* __restrict__ ys, double* __restrict__ zs) {
-    keys_out[o] = keys_in[p];
+// The sorted point at output position o: its key (upper half `h`, lower half
+// and input position packed in `pv`), its id and its SoA coordinates.
+__device__ __forceinline__ void put_sorted(uint64_t o, uint32_t h, uint64_t pv, const double* __restrict__ xyz,
+                                           uint64_t* __restrict__ keys_out, uint32_t* __restrict__ perm_out,
+                                           double* __restrict__ xs, double* __restrict__ ys,
+                                           double* __restrict__ zs) {
+    const uint32_t p = (uint32_t)pv;
+    keys_out[o] = ((uint64_t)h << 32) | (pv >> 32);
     perm_out[o] = p;
     xs[o] = xyz[3ull * p];
     ys[o] = xyz[3ull * p + 1];
@@ -450,12 +461,12 @@ __device__ __forceinline__ void put_sorted(uint64_t o, uint32_t p, const uint64_
 
 // One thread per point.  A point of a run of at most kRunSmall points finds
 // its place in the run by counting the run's points that precede it in the
-// stable order (a smaller key, or an equal key earlier in the run) and writes
-// itself there; the first point of a longer run lists it for k_runs_mid
-// (start, length) or flags it when it is longer than kRunMid.
+// stable order (a smaller lower key half, or an equal one earlier in the run)
+// and writes itself there; the first point of a longer run lists it for
+// k_runs_warp / k_runs_mid (start, length) or flags it when it is longer than
+// kRunMid.  hi: the sorted upper halves; pv: lower half << 32 | input position.
 __global__ void __launch_bounds__(256) k_runs_small(const uint32_t* __restrict__ hi,
-                                                    const uint32_t* __restrict__ perm_hi,
-                                                    const uint64_t* __restrict__ keys_in,
+                                                    const uint64_t* __restrict__ pv,
                                                     const double* __restrict__ xyz, uint64_t n,
                                                     uint64_t* __restrict__ keys_out, uint32_t* __restrict__ perm_out,
                                                     double* __restrict__ xs, double* __restrict__ ys,
@@ -483,27 +494,23 @@ __global__ void __launch_bounds__(256) k_runs_small(const uint32_t* __restrict__
             }
             continue;
         }
-        const uint32_t p = perm_hi[i];
-        const uint64_t key = keys_in[p];
+        const uint64_t mine = pv[i];
+        const uint32_t lo = (uint32_t)(mine >> 32);
         uint64_t rank = 0;
         for (uint64_t j = s; j < e; ++j) {
             if (j == i) continue;
-            const uint64_t kj = keys_in[perm_hi[j]];
-            rank += (kj < key || (kj == key && j < i)) ? 1u : 0u;
+            const uint32_t lj = (uint32_t)(pv[j] >> 32);
+            rank += (lj < lo || (lj == lo && j < i)) ? 1u : 0u;
         }
-        const uint64_t o = s + rank;
-        keys_out[o] = key;
-        perm_out[o] = p;
-        xs[o] = xyz[3ull * p];
-        ys[o] = xyz[3ull * p + 1];
-        zs[o] = xyz[3ull * p + 2];
+        put_sorted(s + rank, h, mine, xyz, keys_out, perm_out, xs, ys, zs);
     }
 }
 
-// One block per listed run (persistent blocks take runs from a counter):
-// bitonic sort of (low key half << 32 | position in run) in shared memory.
-__global__ void __launch_bounds__(kRunMidThreads) k_runs_mid(const uint32_t* __restrict__ perm_hi,
-                                                             const uint64_t* __restrict__ keys_in,
+// One block per listed run of kRunWarp < length <= kRunMid (persistent blocks
+// take runs from a counter): bitonic sort of (lower key half << 32 | position in
+// run) in shared memory - unique values, so the order is stable.
+__global__ void __launch_bounds__(kRunMidThreads) k_runs_mid(const uint32_t* __restrict__ hi,
+                                                             const uint64_t* __restrict__ pv,
                                                              const double* __restrict__ xyz,
                                                              uint64_t* __restrict__ keys_out,
                                                              uint32_t* __restrict__ perm_out, double* __restrict__ xs,
@@ -523,7 +530,7 @@ __global__ void __launch_bounds__(kRunMidThreads) k_runs_mid(const uint32_t* __r
         uint32_t P = 64;
         while (P < len) P <<= 1;
         for (uint32_t t = tid; t < P; t += kRunMidThreads)
-            s[t] = t < len ? ((keys_in[perm_hi[start + t]] & 0xffffffffull) << 32) | t : ~0ull;
+            s[t] = t < len ? ((pv[start + t] >> 32) << 32) | t : ~0ull;
         __syncthreads();
         for (uint32_t k = 2; k <= P; k <<= 1) {
             for (uint32_t j = k >> 1; j > 0; j >>= 1) {
@@ -540,9 +547,10 @@ __global__ void __launch_bounds__(kRunMidThreads) k_runs_mid(const uint32_t* __r
                 __syncthreads();
             }
         }
+        const uint32_t h = hi[start];
         for (uint32_t t = tid; t < len; t += kRunMidThreads) {
             const uint32_t local = (uint32_t)(s[t] & 0xffffffffull);
-            put_sorted(start + t, perm_hi[start + local], keys_in, xyz, keys_out, perm_out, xs, ys, zs);
+            put_sorted(start + t, h, pv[start + local], xyz, keys_out, perm_out, xs, ys, zs);
         }
         __syncthreads();  // s and s_r are reused by the next run
     }
@@ -550,8 +558,8 @@ __global__ void __launch_bounds__(kRunMidThreads) k_runs_mid(const uint32_t* __r
 
 // One warp per listed run of kRunSmall < length <= kRunWarp: the same bitonic
 // sort as k_runs_mid in a warp's slice of shared memory.
-__global__ void __launch_bounds__(kRunWarpThreads) k_runs_warp(const uint32_t* __restrict__ perm_hi,
-                                                               const uint64_t* __restrict__ keys_in,
+__global__ void __launch_bounds__(kRunWarpThreads) k_runs_warp(const uint32_t* __restrict__ hi,
+                                                               const uint64_t* __restrict__ pv,
                                                                const double* __restrict__ xyz,
                                                                uint64_t* __restrict__ keys_out,
                                                                uint32_t* __restrict__ perm_out,
@@ -570,8 +578,7 @@ __global__ void __launch_bounds__(kRunWarpThreads) k_runs_warp(const uint32_t* _
         const uint32_t start = mid_list[2 * r], len = mid_list[2 * r + 1];
         uint32_t P = 64;
         while (P < len) P <<= 1;
-        for (uint32_t t = lane; t < P; t += 32)
-            s[t] = t < len ? ((keys_in[perm_hi[start + t]] & 0xffffffffull) << 32) | t : ~0ull;
+        for (uint32_t t = lane; t < P; t += 32) s[t] = t < len ? ((pv[start + t] >> 32) << 32) | t : ~0ull;
         __syncwarp();
         for (uint32_t k = 2; k <= P; k <<= 1) {
             for (uint32_t j = k >> 1; j > 0; j >>= 1) {
@@ -588,12 +595,20 @@ __global__ void __launch_bounds__(kRunWarpThreads) k_runs_warp(const uint32_t* _
                 __syncwarp();
             }
         }
+        const uint32_t h = hi[start];
         for (uint32_t t = lane; t < len; t += 32) {
             const uint32_t local = (uint32_t)(s[t] & 0xffffffffull);
-            put_sorted(start + t, perm_hi[start + local], keys_in, xyz, keys_out, perm_out, xs, ys, zs);
+            put_sorted(start + t, h, pv[start + local], xyz, keys_out, perm_out, xs, ys, zs);
         }
         __syncwarp();
     }
+}
+
+// Lower key half << 32 | input position, for a cloud whose upper halves are all equal.
+__global__ void k_pack_iota(const uint64_t* __restrict__ keys, uint64_t* __restrict__ pv, uint64_t n) {
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+        pv[i] = (keys[i] << 32) | i;
 }
 
 __global__ void k_iota(uint32_t* perm, uint64_t n) {
@@ -704,11 +719,11 @@ cudaError_t launch_sort_passes(Cloud& c, const uint32_t skip[8], int* final_sel)
         const uint32_t* vin = vb[sel]->as<uint32_t>();
         uint32_t* vout = vb[sel ^ 1]->as<uint32_t>();
         if (first)
-            k_onesweep<true><<<(unsigned)tiles, kSortThreads, smem, c.stream>>>(
+            k_onesweep<true, uint64_t, uint32_t><<<(unsigned)tiles, kSortThreads, smem, c.stream>>>(
                 kin, nullptr, kout, vout, n, p, ctl, c.sort_status.as<unsigned long long>(), c.sort_epoch,
                 c.d_err.as<uint32_t>());
         else
-            k_onesweep<false><<<(unsigned)tiles, kSortThreads, smem, c.stream>>>(
+            k_onesweep<false, uint64_t, uint32_t><<<(unsigned)tiles, kSortThreads, smem, c.stream>>>(
                 kin, vin, kout, vout, n, p, ctl, c.sort_status.as<unsigned long long>(), c.sort_epoch,
                 c.d_err.as<uint32_t>());
         first = false;
@@ -724,23 +739,26 @@ cudaError_t launch_sort_passes(Cloud& c, const uint32_t skip[8], int* final_sel)
 
 // The split sort (upper halves, then runs): keys stay in input order in c.keys
 // (so the 8-pass sort can still run from them), the sorted keys go to
-// c.keys_alt, the permutation to the perm buffer *out_sel names, the sorted
-// coordinates to xs / ys / zs.  RunCtl::big (d_run_ctl) says whether a run was
-// too long, in which case nothing of the outputs may be used.
+// c.keys_alt, the permutation to c.perm, the sorted coordinates to xs / ys /
+// zs.  The passes carry each key's lower half with its input position (one
+// 64-bit value), so the runs read them in order instead of gathering keys.
+// RunCtl::big (d_run_ctl) says whether a run was too long, in which case
+// nothing of the outputs may be used.
 cudaError_t launch_sort_split(Cloud& c, const uint32_t skip[8], const double* d_xyz, int* out_sel) {
     cudaError_t e;
     const uint64_t n = c.n;
     *out_sel = 0;
-    if ((e = c.keys_alt.reserve(8 * (n ? n : 1))) != cudaSuccess) return e;
-    if ((e = c.perm.reserve(4 * (n ? n : 1))) != cudaSuccess) return e;
-    if ((e = c.perm_alt.reserve(4 * (n ? n : 1))) != cudaSuccess) return e;
-    if ((e = c.keys_hi_alt.reserve(4 * (n ? n : 1))) != cudaSuccess) return e;
+    const size_t nn = n ? n : 1;
+    if ((e = c.keys_alt.reserve(8 * nn)) != cudaSuccess) return e;
+    if ((e = c.perm.reserve(4 * nn)) != cudaSuccess) return e;
+    if ((e = c.keys_hi_alt.reserve(4 * nn)) != cudaSuccess) return e;
+    if ((e = c.run_pv.reserve(8 * nn)) != cudaSuccess) return e;
+    if ((e = c.run_pv_alt.reserve(8 * nn)) != cudaSuccess) return e;
     if ((e = c.run_ctl.reserve(sizeof(RunCtl))) != cudaSuccess) return e;
     if ((e = c.run_list.reserve(8 * (n / (kRunSmall + 1) + 1))) != cudaSuccess) return e;
-    const size_t b = 8 * (n ? n : 1);
-    if ((e = c.xs.reserve(b)) != cudaSuccess) return e;
-    if ((e = c.ys.reserve(b)) != cudaSuccess) return e;
-    if ((e = c.zs.reserve(b)) != cudaSuccess) return e;
+    if ((e = c.xs.reserve(8 * nn)) != cudaSuccess) return e;
+    if ((e = c.ys.reserve(8 * nn)) != cudaSuccess) return e;
+    if ((e = c.zs.reserve(8 * nn)) != cudaSuccess) return e;
     RunCtl* rc = c.run_ctl.as<RunCtl>();
     RunCtl rc0{};
     rc0.cap = (uint32_t)(n / (kRunSmall + 1) + 1);
@@ -753,11 +771,16 @@ cudaError_t launch_sort_split(Cloud& c, const uint32_t skip[8], const double* d_
         if ((e = cudaMemsetAsync(c.sort_status.ptr, 0, c.sort_status.bytes, c.stream)) != cudaSuccess) return e;
         c.sort_epoch = 0;
     }
-    // 32-bit keys: tile 3072 x 8 bytes + counters, under the default 48 KB of dynamic shared memory
-    const size_t smem = (size_t)kSortTile * 4 + (size_t)kSortTile * 4 + (size_t)kSortWarps * 256 * 4 + 256 * 4 +
-                        256 * 8;
+    // 32-bit keys with 64-bit values: the same 12 bytes per tile slot as the 8-pass sort's
+    const size_t smem = onesweep_smem();
+    if ((e = cudaFuncSetAttribute(k_onesweep<true, uint32_t, uint64_t>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)smem)) != cudaSuccess)
+        return e;
+    if ((e = cudaFuncSetAttribute(k_onesweep<false, uint32_t, uint64_t>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                  (int)smem)) != cudaSuccess)
+        return e;
     DevBuf* kb[2] = {&c.keys_hi, &c.keys_hi_alt};
-    DevBuf* vb[2] = {&c.perm, &c.perm_alt};
+    DevBuf* vb[2] = {&c.run_pv, &c.run_pv_alt};
     int sel = 0;
     bool first = true;
     SortCtl* ctl = c.d_ctl.as<SortCtl>();
@@ -770,39 +793,37 @@ cudaError_t launch_sort_split(Cloud& c, const uint32_t skip[8], const double* d_
         }
         const uint32_t* kin = kb[sel]->as<uint32_t>();
         uint32_t* kout = kb[sel ^ 1]->as<uint32_t>();
-        const uint32_t* vin = vb[sel]->as<uint32_t>();
-        uint32_t* vout = vb[sel ^ 1]->as<uint32_t>();
+        const uint64_t* vin = vb[sel]->as<uint64_t>();
+        uint64_t* vout = vb[sel ^ 1]->as<uint64_t>();
         if (first)
-            k_onesweep<true, uint32_t><<<(unsigned)tiles, kSortThreads, smem, c.stream>>>(
+            k_onesweep<true, uint32_t, uint64_t><<<(unsigned)tiles, kSortThreads, smem, c.stream>>>(
                 kin, nullptr, kout, vout, n, p, ctl, c.sort_status.as<unsigned long long>(), c.sort_epoch,
-                c.d_err.as<uint32_t>());
+                c.d_err.as<uint32_t>(), nullptr, nullptr, c.keys.as<uint64_t>());
         else
-            k_onesweep<false, uint32_t><<<(unsigned)tiles, kSortThreads, smem, c.stream>>>(
+            k_onesweep<false, uint32_t, uint64_t><<<(unsigned)tiles, kSortThreads, smem, c.stream>>>(
                 kin, vin, kout, vout, n, p, ctl, c.sort_status.as<unsigned long long>(), c.sort_epoch,
                 c.d_err.as<uint32_t>());
         first = false;
         sel ^= 1;
     }
-    if (first) {  // every upper digit constant: one run in input order
-        k_iota<<<(unsigned)((n + 255) / 256), 256, 0, c.stream>>>(c.perm.as<uint32_t>(), n);
-        sel = 0;
-    }
     const int sms = sm_count(c.device);
     const uint64_t want = (n + 255) / 256;
     const int grid = (int)(want < (uint64_t)sms * 8 ? want : (uint64_t)sms * 8);
-    uint32_t* perm_out = vb[sel ^ 1]->as<uint32_t>();
-    k_runs_small<<<grid, 256, 0, c.stream>>>(kb[sel]->as<uint32_t>(), vb[sel]->as<uint32_t>(), c.keys.as<uint64_t>(),
-                                            d_xyz, n, c.keys_alt.as<uint64_t>(), perm_out, c.xs.as<double>(),
+    if (first) {  // every upper digit constant: one run in input order
+        k_pack_iota<<<grid, 256, 0, c.stream>>>(c.keys.as<uint64_t>(), c.run_pv.as<uint64_t>(), n);
+        sel = 0;
+    }
+    const uint32_t* hi = kb[sel]->as<uint32_t>();
+    const uint64_t* pv = vb[sel]->as<uint64_t>();
+    uint32_t* perm_out = c.perm.as<uint32_t>();
+    k_runs_small<<<grid, 256, 0, c.stream>>>(hi, pv, d_xyz, n, c.keys_alt.as<uint64_t>(), perm_out, c.xs.as<double>(),
                                             c.ys.as<double>(), c.zs.as<double>(), rc, c.run_list.as<uint32_t>());
-    k_runs_warp<<<sms * 8, kRunWarpThreads, 0, c.stream>>>(vb[sel]->as<uint32_t>(), c.keys.as<uint64_t>(), d_xyz,
-                                                           c.keys_alt.as<uint64_t>(), perm_out, c.xs.as<double>(),
-                                                           c.ys.as<double>(), c.zs.as<double>(), rc,
-                                                           c.run_list.as<uint32_t>());
-    k_runs_mid<<<sms, kRunMidThreads, 0, c.stream>>>(vb[sel]->as<uint32_t>(), c.keys.as<uint64_t>(), d_xyz,
-                                                     c.keys_alt.as<uint64_t>(), perm_out, c.xs.as<double>(),
-                                                     c.ys.as<double>(), c.zs.as<double>(), rc,
+    k_runs_warp<<<sms * 8, kRunWarpThreads, 0, c.stream>>>(hi, pv, d_xyz, c.keys_alt.as<uint64_t>(), perm_out,
+                                                           c.xs.as<double>(), c.ys.as<double>(), c.zs.as<double>(),
+                                                           rc, c.run_list.as<uint32_t>());
+    k_runs_mid<<<sms, kRunMidThreads, 0, c.stream>>>(hi, pv, d_xyz, c.keys_alt.as<uint64_t>(), perm_out,
+                                                     c.xs.as<double>(), c.ys.as<double>(), c.zs.as<double>(), rc,
                                                      c.run_list.as<uint32_t>());
-    *out_sel = sel ^ 1;
     return cudaGetLastError();
 }
 
@@ -854,11 +875,11 @@ cudaError_t launch_sort_dyn(int device, cudaStream_t s, uint64_t* k0, uint64_t* 
     for (int p = 0; p < passes; ++p) {
         const int i = p & 1, o = i ^ 1;
         if (p == 0)
-            k_onesweep<true><<<grid, kSortThreads, smem, s>>>(kb[i], nullptr, kb[o], vb[o], 0, p, ctl, status, 0,
-                                                              err, d_n, d_epoch);
+            k_onesweep<true, uint64_t, uint32_t><<<grid, kSortThreads, smem, s>>>(
+                kb[i], nullptr, kb[o], vb[o], 0, p, ctl, status, 0, err, d_n, d_epoch);
         else
-            k_onesweep<false><<<grid, kSortThreads, smem, s>>>(kb[i], vb[i], kb[o], vb[o], 0, p, ctl, status, 0,
-                                                               err, d_n, d_epoch);
+            k_onesweep<false, uint64_t, uint32_t><<<grid, kSortThreads, smem, s>>>(
+                kb[i], vb[i], kb[o], vb[o], 0, p, ctl, status, 0, err, d_n, d_epoch);
     }
     *result_vals = vb[passes & 1];
     return cudaGetLastError();
@@ -933,11 +954,11 @@ cudaError_t launch_query_order(Cloud& c, const double* d_centers, uint64_t nq, c
             c.qs_epoch = 1;
         }
         if (p == 5)
-            k_onesweep<true><<<(unsigned)tiles, kSortThreads, smem, c.stream>>>(
+            k_onesweep<true, uint64_t, uint32_t><<<(unsigned)tiles, kSortThreads, smem, c.stream>>>(
                 kb[sel]->as<uint64_t>(), nullptr, kb[sel ^ 1]->as<uint64_t>(), vb[sel ^ 1]->as<uint32_t>(), nq, p,
                 ctl, c.qs_status.as<unsigned long long>(), c.qs_epoch, c.d_err.as<uint32_t>());
         else
-            k_onesweep<false><<<(unsigned)tiles, kSortThreads, smem, c.stream>>>(
+            k_onesweep<false, uint64_t, uint32_t><<<(unsigned)tiles, kSortThreads, smem, c.stream>>>(
                 kb[sel]->as<uint64_t>(), vb[sel]->as<uint32_t>(), kb[sel ^ 1]->as<uint64_t>(),
                 vb[sel ^ 1]->as<uint32_t>(), nq, p, ctl, c.qs_status.as<unsigned long long>(), c.qs_epoch,
                 c.d_err.as<uint32_t>());
@@ -1018,6 +1039,9 @@ int noalloc_setup(int dev, NoAllocScratch** out) {
 
 }  // namespace
 
+// A kernel of this file's device code, for preload_kernels.
+const void* kernel_anchor_encode_sort() { return reinterpret_cast<const void*>(&k_iota); }
+
 }  // namespace octb
 
 extern "C" int oct_encode_sort_noalloc(int encoder, const double* d_xyz, uint64_t n, uint64_t* d_keys,
@@ -1060,11 +1084,11 @@ extern "C" int oct_encode_sort_noalloc(int encoder, const double* d_xyz, uint64_
             const uint32_t* vin = to_scratch ? d_perm : sc->perm_alt;
             uint32_t* vout = to_scratch ? sc->perm_alt : d_perm;
             if (p == 0)
-                k_onesweep<true><<<(unsigned)tiles, kSortThreads, smem, s>>>(kin, nullptr, kout, vout, n, p, ctl,
-                                                                             sc->status, (uint32_t)(p + 1), err);
+                k_onesweep<true, uint64_t, uint32_t><<<(unsigned)tiles, kSortThreads, smem, s>>>(
+                    kin, nullptr, kout, vout, n, p, ctl, sc->status, (uint32_t)(p + 1), err);
             else
-                k_onesweep<false><<<(unsigned)tiles, kSortThreads, smem, s>>>(kin, vin, kout, vout, n, p, ctl,
-                                                                              sc->status, (uint32_t)(p + 1), err);
+                k_onesweep<false, uint64_t, uint32_t><<<(unsigned)tiles, kSortThreads, smem, s>>>(
+                    kin, vin, kout, vout, n, p, ctl, sc->status, (uint32_t)(p + 1), err);
         }
     }
     // Box (center, radii, min, max), radii -1.0 if a look-back gave up

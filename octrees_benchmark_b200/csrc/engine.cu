@@ -232,6 +232,11 @@ struct DeviceGuardE {
 
 }  // namespace
 
+namespace octb {
+// A kernel of this file's device code, for preload_kernels.
+const void* kernel_anchor_engine() { return reinterpret_cast<const void*>(&k_epoch_advance); }
+}  // namespace octb
+
 struct oct_engine_s {
     int device = 0;
     uint32_t flags = 0;
@@ -541,10 +546,12 @@ int finish(oct_engine e) {
             return OCT_OK;
         }
         // the results did not fit: grow the result array (and the chunk pool: every
-        // query's last chunk may be partial) from the exact total and run the batch again
-        int st = grow(e, e->out, 4 * (size_t)(sm.radius_total + sm.radius_total / 8 + 1024));
+        // query's last chunk may be partial) to at least twice its size and the exact
+        // total, and run the batch again
+        const uint64_t want = std::max<uint64_t>(2 * cap, sm.radius_total + sm.radius_total / 8 + 1024);
+        int st = grow(e, e->out, 4 * (size_t)want);
         if (st != OCT_OK) return st;
-        if ((st = grow_chunks(e, sm.radius_total / kResultChunk + e->n_radius + 1024)) != OCT_OK) return st;
+        if ((st = grow_chunks(e, want / kResultChunk + e->n_radius + 1024)) != OCT_OK) return st;
         if ((st = launch_batch(e, true)) != OCT_OK) return st;
     }
     return fail(e, OCT_ERR_CAPACITY, "radius results kept outgrowing the result array");
@@ -793,6 +800,8 @@ int oct_engine_create(const oct_engine_params* p, oct_engine* out) {
     if (r == cudaSuccess) r = cudaEventCreate(&e->ev_t1);
     if (r == cudaSuccess) r = prepare_sort_dyn();
     if (r == cudaSuccess) r = prepare_knn_dyn();
+    // every kernel loaded now, not at its first launch in the middle of a stream of batches
+    if (r == cudaSuccess && preload_kernels(e->device) != OCT_OK) r = cudaErrorInitializationError;
     if (r == cudaSuccess) r = e->sort_ctl.reserve(sizeof(SortCtl));
     if (r == cudaSuccess) r = e->epoch.reserve(256);
     if (r == cudaSuccess) r = e->ctrs.reserve(4 * (2 * kRadiusVariants + 4 * 2));  // + group kNN (3 of 4 per variant)

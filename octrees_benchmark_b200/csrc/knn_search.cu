@@ -1537,4 +1537,7 @@ cudaError_t launch_knn(Cloud& c, const double* d_centers, uint64_t nq, uint32_t 
     return launch_l<1024>(a, grid, c.stream, c.packet != 0);
 }
 
+// A kernel of this file's device code, for preload_kernels.
+const void* kernel_anchor_knn_search() { return reinterpret_cast<const void*>(&k_knn_reg<2, 0>); }
+
 }  // namespace octb

@@ -331,4 +331,7 @@ cudaError_t launch_build(Cloud& c, bool* capacity_ok) {
     return e;
 }
 
+// A kernel of this file's device code, for preload_kernels.
+const void* kernel_anchor_octree_build() { return reinterpret_cast<const void*>(&k_build<1>); }
+
 }  // namespace octb

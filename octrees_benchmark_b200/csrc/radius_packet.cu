@@ -995,4 +995,7 @@ cudaError_t launch_radius_packet(Cloud& c, int kernel, int algo, int mode, bool 
     return e;
 }
 
+// A kernel of this file's device code, for preload_kernels.
+const void* kernel_anchor_radius_packet() { return reinterpret_cast<const void*>(&k_center_rel); }
+
 }  // namespace octb

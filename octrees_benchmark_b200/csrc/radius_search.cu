@@ -419,4 +419,7 @@ cudaError_t launch_scan_u64(Cloud& c, const unsigned long long* d_in, unsigned l
     return cudaGetLastError();
 }
 
+// A kernel of this file's device code, for preload_kernels.
+const void* kernel_anchor_radius_search() { return reinterpret_cast<const void*>(&k_scan_top); }
+
 }  // namespace octb

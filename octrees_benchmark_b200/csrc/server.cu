@@ -395,9 +395,9 @@ int oct_server_create(const oct_server_params* p, oct_server* out) {
         for (Slot& sl : s->slots) {
             oct_engine_params ep{};
             ep.device = p->device;
-            // results of a full batch at ~512 neighbours per centre (1 GB per slot at 512K centres): batches
+            // results of a full batch at ~1024 neighbours per centre (2 GB per slot at 512K centres): batches
             // rarely outgrow it, and one that does is run again on the scheduler thread
-            ep.reserve_results = std::max<uint64_t>(64ull << 20, 512ull * s->p.max_batch_queries);
+            ep.reserve_results = std::max<uint64_t>(64ull << 20, 1024ull * s->p.max_batch_queries);
             ep.reserve_queries = s->p.max_batch_queries;  // the per-centre arrays of the largest batch
             const int st = oct_engine_create(&ep, &sl.eng);
             if (st != OCT_OK) {
