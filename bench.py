@@ -533,7 +533,7 @@ def run_serving(args, dev):
     clocks = ClockSampler(dev)
     clocks.start()
     srv = Server(device=dev, slots=args.serve_slots, max_batch_queries=args.serve_max_batch,
-                 max_wait_ms=args.serve_max_wait, fifo=args.serve_fifo)
+                 max_wait_ms=args.serve_max_wait, fifo=args.serve_fifo, graph=not args.serve_no_graph)
     try:
         batched = replay(wl, srv, drain_s=args.serve_drain)
     finally:
@@ -1033,6 +1033,7 @@ def main():
     ap.add_argument("--serve-max-wait", type=float, default=40.0,
                     help="ms after which a queued request is admitted ahead of smaller ones")
     ap.add_argument("--serve-fifo", action="store_true", help="admit serving requests in arrival order only")
+    ap.add_argument("--serve-no-graph", action="store_true", help="serving batches launched directly, not as graphs")
     ap.add_argument("--large", action="store_true", help="also run the 500M-point skewed cloud (not in the default run)")
     ap.add_argument("--large-points", type=int, default=500_000_000)
     ap.add_argument("--large-queries", type=int, default=10_000_000)

@@ -395,14 +395,21 @@ int oct_engine_memory(oct_engine engine, uint64_t* bytes);
 /* Device bytes a cloud holds (points, keys, tree, search scratch). */
 int oct_cloud_memory(oct_cloud cloud, uint64_t* bytes);
 
+/* Clouds take their device arrays from one stream-ordered pool per device,
+ * which keeps what destroyed clouds free for the next clouds (returning it to
+ * the driver would make other threads' CUDA calls wait).  This returns the
+ * pool's unused memory to the driver. */
+int oct_trim_cloud_memory(int device);
+
 /* ---- Serving: continuous batching over device-resident clouds ------------
  *
  * No reference counterpart.  A server owns `slots` engines, each on its own
  * stream.  Clients submit requests from any thread; a scheduler thread forms a
- * batch from the queue (arrival order) whenever a slot is free, admitting
- * requests while the registered clouds, the batches in flight and the new
- * batch fit the HBM budget (a request that does not fit waits: an admission
- * stall), and launches it.  Batches on different slots overlap on the device.
+ * batch from the queue whenever a slot is free - smallest expected work first,
+ * a request waiting longer than max_wait_ms first of all (OCT_SERVER_FIFO:
+ * arrival order) - admitting requests while the registered clouds, the
+ * batches in flight and the new batch fit the HBM budget (a request that does
+ * not fit waits: an admission stall), and launches it.  Batches on different slots overlap on the device.
  * A completed request's results stay in its slot until the client releases
  * the ticket; a slot is reused once all its tickets are released.  With
  * OCT_SERVER_PLAIN the server instead runs one request per launch through the
@@ -411,6 +418,7 @@ typedef struct oct_server_s* oct_server;
 
 #define OCT_SERVER_PLAIN 0x1u /* one request per launch, single-cloud plain path */
 #define OCT_SERVER_FIFO 0x2u  /* batched: admit in arrival order only (no smallest-first admission) */
+#define OCT_SERVER_NO_GRAPH 0x4u /* batched: launch each batch's kernels directly, not from captured graphs */
 #define OCT_CLOUD_OWNED 0x1u  /* oct_server_add_cloud: the server destroys the cloud when it evicts or removes it */
 
 typedef struct {

@@ -69,6 +69,7 @@ class OctRequestPlace(C.Structure):
 
 OCT_SERVER_PLAIN = 0x1
 OCT_SERVER_FIFO = 0x2
+OCT_SERVER_NO_GRAPH = 0x4
 OCT_CLOUD_OWNED = 0x1
 
 
@@ -153,6 +154,7 @@ SIGNATURES = {
     "oct_engine_ready": ([_vp, C.POINTER(_int)], _int),
     "oct_engine_memory": ([_vp, C.POINTER(_u64)], _int),
     "oct_cloud_memory": ([_vp, C.POINTER(_u64)], _int),
+    "oct_trim_cloud_memory": ([_int], _int),
     "oct_server_create": ([C.POINTER(OctServerParams), C.POINTER(_vp)], _int),
     "oct_server_destroy": ([_vp], _int),
     "oct_server_last_error": ([_vp, C.c_char_p, C.c_size_t], _int),

@@ -265,7 +265,10 @@ cudaMemPool_t cloud_pool(int device) {
             cudaGetLastError();
             return nullptr;
         }
-        uint64_t keep = 8ull << 30;
+        // the pool keeps what clouds free, for the next cloud: returning memory to the driver at a
+        // synchronisation goes through the driver's resource manager, which a server's other threads
+        // would wait on
+        uint64_t keep = UINT64_MAX;
         cudaMemPoolSetAttribute(pool, cudaMemPoolAttrReleaseThreshold, &keep);
         pools[device] = pool;
     }
@@ -541,6 +544,23 @@ int oct_cloud_memory(oct_cloud h, uint64_t* bytes) {
     uint64_t s = 0;
     for (const DevBuf* b : cloud_bufs(c)) s += b->bytes;
     *bytes = s;
+    return OCT_OK;
+}
+
+int oct_trim_cloud_memory(int device) {
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return OCT_ERR_NO_DEVICE;
+    }
+    if (device < 0 || device >= ndev) return OCT_ERR_INVALID_ARG;
+    cudaMemPool_t pool = cloud_pool(device);
+    if (!pool) return OCT_ERR_CUDA;
+    DeviceGuard g(device);
+    if (cudaMemPoolTrimTo(pool, 0) != cudaSuccess) {
+        cudaGetLastError();
+        return OCT_ERR_CUDA;
+    }
     return OCT_OK;
 }
 

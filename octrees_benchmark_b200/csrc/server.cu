@@ -395,6 +395,7 @@ int oct_server_create(const oct_server_params* p, oct_server* out) {
         for (Slot& sl : s->slots) {
             oct_engine_params ep{};
             ep.device = p->device;
+            if (p->flags & OCT_SERVER_NO_GRAPH) ep.flags |= OCT_ENGINE_NO_GRAPH;
             // results of a full batch at ~1024 neighbours per centre (2 GB per slot at 512K centres): batches
             // rarely outgrow it, and one that does is run again on the scheduler thread
             ep.reserve_results = std::max<uint64_t>(64ull << 20, 1024ull * s->p.max_batch_queries);

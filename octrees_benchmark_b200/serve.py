@@ -21,8 +21,8 @@ from dataclasses import dataclass
 import numpy as np
 
 from . import capi
-from .capi import (OCT_CLOUD_OWNED, OCT_SERVER_FIFO, OCT_SERVER_PLAIN, OctCompletion, OctRequest, OctSearchConfig, OctServerParams,
-                   OctServerStats, lib)
+from .capi import (OCT_CLOUD_OWNED, OCT_SERVER_FIFO, OCT_SERVER_NO_GRAPH, OCT_SERVER_PLAIN, OctCompletion,
+                   OctRequest, OctSearchConfig, OctServerParams, OctServerStats, lib)
 from .engine import Request
 from .linear_octree import _sync_current_stream
 
@@ -45,10 +45,11 @@ class Server:
 
     def __init__(self, device: int = 0, plain: bool = False, slots: int = 3, max_batch_requests: int = 1024,
                  max_batch_queries: int = 512 << 10, hbm_budget: int = 120 << 30, max_wait_ms: float = 40.0,
-                 fifo: bool = False):
+                 fifo: bool = False, graph: bool = True):
         L = lib()
         self._L = L
-        flags = (OCT_SERVER_PLAIN if plain else 0) | (OCT_SERVER_FIFO if fifo else 0)
+        flags = ((OCT_SERVER_PLAIN if plain else 0) | (OCT_SERVER_FIFO if fifo else 0) |
+                 (0 if graph else OCT_SERVER_NO_GRAPH))
         p = OctServerParams(device, flags, slots, max_batch_requests, max_batch_queries, hbm_budget, max_wait_ms)
         h = C.c_void_p()
         _check(L.oct_server_create(C.byref(p), C.byref(h)), None, "oct_server_create")
