@@ -627,8 +627,9 @@ int oct_encode_sort(oct_cloud h, double* box12, uint64_t* keys, uint32_t* perm, 
         }
     }
     if (!done) {
-        if (split)  // the split sort's passes took tiles from the upper digits' counters: rewind them
-            CK(cudaMemsetAsync(&c.d_ctl.as<SortCtl>()->tile_ctr[0], 0, sizeof(SortCtl::tile_ctr), c.stream));
+        // the split sort's encode counted the upper digits only, and its passes took tiles from their
+        // counters: count the lower digits and scan again (which rewinds the counters)
+        if (split) CK(launch_hist_low(c));
         if (c.n) {
             const int st = read_skips();
             if (st != OCT_OK) return st;

@@ -138,13 +138,33 @@ __global__ void __launch_bounds__(kBboxThreads) k_bbox(const double* __restrict_
         last = (atomicAdd(ctr, 1u) == gridDim.x - 1);
     }
     __syncthreads();
-    if (!last || threadIdx.x != 0) return;
+    if (!last) return;
     __threadfence();
+    // the last block folds the blocks' partials with all its threads (one thread alone
+    // waited for the grid's ~450 partials one L2 round trip at a time)
     double gmn[3] = {DBL_MAX, DBL_MAX, DBL_MAX}, gmx[3] = {-DBL_MAX, -DBL_MAX, -DBL_MAX};
-    for (unsigned b = 0; b < gridDim.x; ++b)
+    for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x)
+#pragma unroll
         for (int a = 0; a < 3; ++a) {
-            gmn[a] = smin(gmn[a], ((volatile double*)partial)[6 * b + a]);
-            gmx[a] = smax(gmx[a], ((volatile double*)partial)[6 * b + 3 + a]);
+            gmn[a] = smin(gmn[a], __ldcg(&partial[6 * b + a]));
+            gmx[a] = smax(gmx[a], __ldcg(&partial[6 * b + 3 + a]));
+        }
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) {
+            gmn[a] = smin(gmn[a], __shfl_down_sync(0xffffffffu, gmn[a], off));
+            gmx[a] = smax(gmx[a], __shfl_down_sync(0xffffffffu, gmx[a], off));
+        }
+    }
+    if (lane == 0)
+        for (int a = 0; a < 3; ++a) { s[warp][a] = gmn[a]; s[warp][3 + a] = gmx[a]; }
+    __syncthreads();
+    if (threadIdx.x != 0) return;
+    for (int w = 0; w < kBboxThreads / 32; ++w)
+        for (int a = 0; a < 3; ++a) {
+            gmn[a] = smin(gmn[a], s[w][a]);
+            gmx[a] = smax(gmx[a], s[w][3 + a]);
         }
     // Box(pair{min, max}) then Box(center, radii) (box.hpp:17-21, point_encoder.hpp:492-494)
     BoxGeom bg;
@@ -165,7 +185,9 @@ __global__ void __launch_bounds__(kBboxThreads) k_bbox(const double* __restrict_
     *ctr = 0;
 }
 
-template <int ENC>
+// LOW: the histograms of all 8 digits; otherwise of the upper 4 only (the split
+// sort; its fallback to the 8-pass sort counts the lower digits with k_hist_low).
+template <int ENC, bool LOW = true>
 __global__ void __launch_bounds__(kEncThreads) k_encode(const double* __restrict__ xyz, uint64_t n,
                                                         const BoxGeom* __restrict__ bg, uint64_t* __restrict__ keys,
                                                         SortCtl* ctl, uint32_t* __restrict__ hi = nullptr) {
@@ -188,7 +210,7 @@ __global__ void __launch_bounds__(kEncThreads) k_encode(const double* __restrict
         const uint32_t az = anchor_coord_fast(pz, c2, r2, i2);
         const uint64_t k = (ENC == 5) ? hilbert_encode_tbl2(ax, ay, az, htbl, htbl2) : morton_encode(ax, ay, az);
 #pragma unroll
-        for (int p = 0; p < 8; ++p) atomicAdd(&hist[p * 256 + (uint32_t)((k >> (8 * p)) & 255u)], 1u);
+        for (int p = LOW ? 0 : 4; p < 8; ++p) atomicAdd(&hist[p * 256 + (uint32_t)((k >> (8 * p)) & 255u)], 1u);
         return k;
     };
     // two points per thread and step: three aligned 16-byte loads, one 16-byte store;
@@ -251,6 +273,25 @@ __global__ void __launch_bounds__(256) k_scan_hist(SortCtl* ctl, uint64_t n, con
             ctl->tile_ctr[p] = 0;
         }
         __syncthreads();
+    }
+}
+
+// Histograms of the 4 lower digits of the keys (the split sort's encode counts
+// the upper 4 only).
+__global__ void __launch_bounds__(256) k_hist_low(const uint64_t* __restrict__ keys, uint64_t n, SortCtl* ctl) {
+    __shared__ uint32_t hist[4 * 256];
+    for (int j = threadIdx.x; j < 4 * 256; j += blockDim.x) hist[j] = 0;
+    __syncthreads();
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const uint64_t k = keys[i];
+#pragma unroll
+        for (int p = 0; p < 4; ++p) atomicAdd(&hist[p * 256 + (uint32_t)((k >> (8 * p)) & 255u)], 1u);
+    }
+    __syncthreads();
+    for (int j = threadIdx.x; j < 4 * 256; j += blockDim.x) {
+        const uint32_t v = hist[j];
+        if (v) atomicAdd(&ctl->hist[j >> 8][j & 255], v);
     }
 }
 
@@ -672,14 +713,27 @@ cudaError_t launch_bbox_encode(Cloud& c, const double* d_xyz, uint32_t* d_hi) {
     if (n) {
         const uint64_t want = (n / 2 + kEncThreads) / kEncThreads;
         const int grid = (int)(want < (uint64_t)sms * kEncGridPerSM ? want : (uint64_t)sms * kEncGridPerSM);
-        if (c.params.encoder == OCT_ENC_HILBERT_3D)
-            k_encode<5><<<grid, kEncThreads, 0, c.stream>>>(d_xyz, n, c.d_box.as<BoxGeom>(), c.keys.as<uint64_t>(),
-                                                            ctl, d_hi);
-        else
-            k_encode<1><<<grid, kEncThreads, 0, c.stream>>>(d_xyz, n, c.d_box.as<BoxGeom>(), c.keys.as<uint64_t>(),
-                                                            ctl, d_hi);
+        const bool hil = c.params.encoder == OCT_ENC_HILBERT_3D;
+        BoxGeom* bg = c.d_box.as<BoxGeom>();
+        uint64_t* keys = c.keys.as<uint64_t>();
+        if (d_hi == nullptr && hil) k_encode<5><<<grid, kEncThreads, 0, c.stream>>>(d_xyz, n, bg, keys, ctl);
+        else if (d_hi == nullptr) k_encode<1><<<grid, kEncThreads, 0, c.stream>>>(d_xyz, n, bg, keys, ctl);
+        else if (hil) k_encode<5, false><<<grid, kEncThreads, 0, c.stream>>>(d_xyz, n, bg, keys, ctl, d_hi);
+        else k_encode<1, false><<<grid, kEncThreads, 0, c.stream>>>(d_xyz, n, bg, keys, ctl, d_hi);
         k_scan_hist<<<1, 256, 0, c.stream>>>(ctl, n);
     }
+    return cudaGetLastError();
+}
+
+cudaError_t launch_hist_low(Cloud& c) {
+    const uint64_t n = c.n;
+    if (n == 0) return cudaSuccess;
+    const int sms = sm_count(c.device);
+    const uint64_t want = (n + 255) / 256;
+    const int grid = (int)(want < (uint64_t)sms * 4 ? want : (uint64_t)sms * 4);
+    SortCtl* ctl = c.d_ctl.as<SortCtl>();
+    k_hist_low<<<grid, 256, 0, c.stream>>>(c.keys.as<uint64_t>(), n, ctl);
+    k_scan_hist<<<1, 256, 0, c.stream>>>(ctl, n);
     return cudaGetLastError();
 }
 
