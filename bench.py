@@ -64,11 +64,11 @@ LAUNCHES_PER_STEP = {"plain": 6, "packet": 10 + 7, "packet_fp32": 10 + 7, "knn_p
                      "engine": 15}
 BUILD_BYTES_PER_POINT = 112  # encode 32 + sort 20 + reorder 52 + leaf counting 8
 BUILD_BYTES_PER_NODE = 36    # offsets 4 + ranges 8 + centers 24
-# DRAM bytes (read + write) per query of the search kernels, from ncu --set full of
-# `python -m octrees_benchmark_b200.profile_case` (6M points at this tile's density, 200k queries each):
-# k_knn_group k=50 503.2 + 144.2 MB, one-pass k_radius_packet r=2.5 342.1 + 55.1 MB
-KNN_DRAM_BYTES_PER_QUERY = (503.2e6 + 144.2e6) / 200_000
-RADIUS_DRAM_BYTES_PER_QUERY = (342.1e6 + 55.1e6) / 200_000
+# DRAM bytes (read + write) per query of the search kernels, from ncu --set full of this script's
+# `--points 6000000 --queries 200000 --search packet --paths packet` case (6M points at this tile's density,
+# 200k queries each): k_knn_group k=50 511.8 + 143.8 MB, one-pass k_radius_packet r=2.5 342.3 + 58.8 MB
+KNN_DRAM_BYTES_PER_QUERY = (511.8e6 + 143.8e6) / 200_000
+RADIUS_DRAM_BYTES_PER_QUERY = (342.3e6 + 58.8e6) / 200_000
 
 
 def measured_peak():

@@ -595,8 +595,7 @@ int oct_encode_sort(oct_cloud h, double* box12, uint64_t* keys, uint32_t* perm, 
     const double* xyz = c.xyz_in.as<double>();
     CK(cudaMemsetAsync(c.d_err.ptr, 0, 4, c.stream));
     const bool split = c.split_sort && c.n;
-    if (split) CK(c.keys_hi.reserve(4 * c.n));
-    CK(launch_bbox_encode(c, xyz, split ? c.keys_hi.as<uint32_t>() : nullptr));
+    CK(launch_bbox_encode(c, xyz, split));
     uint32_t skip[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     auto read_skips = [&]() -> int {  // which digits are the same for every key (their passes are skipped)
         CK(cudaMemcpyAsync(c.pinned, &c.d_ctl.as<SortCtl>()->skip[0], sizeof(skip), cudaMemcpyDeviceToHost,

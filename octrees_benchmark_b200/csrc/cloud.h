@@ -256,7 +256,8 @@ struct KernelClock {
 };
 
 // ---- launchers (each returns a cudaError_t of the launch) ----
-cudaError_t launch_bbox_encode(Cloud& c, const double* d_xyz_aos, uint32_t* d_hi = nullptr);
+// upper_hist_only: the split sort follows (the lower digits' histograms are not needed)
+cudaError_t launch_bbox_encode(Cloud& c, const double* d_xyz_aos, bool upper_hist_only = false);
 cudaError_t launch_sort_split(Cloud& c, const uint32_t skip[8], const double* d_xyz_aos, int* out_sel);
 cudaError_t launch_hist_low(Cloud& c);  // the lower digits' histograms (before a split sort's fallback)
 cudaError_t launch_sort_passes(Cloud& c, const uint32_t skip[8], int* final_sel);

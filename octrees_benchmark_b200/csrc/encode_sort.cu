@@ -35,9 +35,12 @@ constexpr int kEncThreads = 256;
 // onesweep tiles: 8 keys per thread x 384 threads, 3 blocks per SM (measured on 10M keys, 8
 // passes: 112 us per pass against 128 us for 16 x 256, 4096-key tiles)
 constexpr int kSortThreads = 384;
-constexpr int kSortItems = 8;
-constexpr int kSortTile = kSortThreads * kSortItems;  // 3072 keys
+constexpr int kSortItems = 12;
+constexpr int kSortTile = kSortThreads * kSortItems;  // 4608 keys
 constexpr int kSortWarps = kSortThreads / 32;
+// resident onesweep blocks per SM (registers: 12 keys and values per thread; 3 blocks of
+// 384 x 8 keys measured 1.8 % slower on the 10M-point build)
+constexpr int kSortBlocksPerSM = 2;
 static_assert(kSortThreads >= 256, "threads 0..255 own one digit each");
 constexpr int kEncGridPerSM = 4;
 
@@ -190,7 +193,7 @@ __global__ void __launch_bounds__(kBboxThreads) k_bbox(const double* __restrict_
 template <int ENC, bool LOW = true>
 __global__ void __launch_bounds__(kEncThreads) k_encode(const double* __restrict__ xyz, uint64_t n,
                                                         const BoxGeom* __restrict__ bg, uint64_t* __restrict__ keys,
-                                                        SortCtl* ctl, uint32_t* __restrict__ hi = nullptr) {
+                                                        SortCtl* ctl) {
     __shared__ uint32_t hist[8 * 256];
     __shared__ uint8_t htbl[kHilbertStates * 8];
     __shared__ uint16_t htbl2[ENC == 5 ? kHilbertTable2Size : 1];
@@ -217,11 +220,9 @@ __global__ void __launch_bounds__(kEncThreads) k_encode(const double* __restrict
     // buffers that are not 16-byte aligned take the scalar loop
     const bool vec = ((reinterpret_cast<uintptr_t>(xyz) | reinterpret_cast<uintptr_t>(keys)) & 15u) == 0;
     const uint64_t npairs = vec ? n / 2 : 0;
-    // hi (optional): the upper 32 bits of every key as well, for the sort on the upper halves
     for (uint64_t i = vec ? n : (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
         const uint64_t k = key_of(xyz[3 * i], xyz[3 * i + 1], xyz[3 * i + 2]);
         keys[i] = k;
-        if (hi) hi[i] = (uint32_t)(k >> 32);
     }
     const double2* xyz2 = reinterpret_cast<const double2*>(xyz);
     ulonglong2* keys2 = reinterpret_cast<ulonglong2*>(keys);
@@ -231,15 +232,10 @@ __global__ void __launch_bounds__(kEncThreads) k_encode(const double* __restrict
         kk.x = key_of(a.x, a.y, b.x);
         kk.y = key_of(b.y, c.x, c.y);
         keys2[t] = kk;
-        if (hi) {
-            hi[2 * t] = (uint32_t)(kk.x >> 32);
-            hi[2 * t + 1] = (uint32_t)(kk.y >> 32);
-        }
     }
     if (vec && (n & 1) && blockIdx.x == 0 && threadIdx.x == 0) {
         const uint64_t k = key_of(xyz[3 * (n - 1)], xyz[3 * (n - 1) + 1], xyz[3 * (n - 1) + 2]);
         keys[n - 1] = k;
-        if (hi) hi[n - 1] = (uint32_t)(k >> 32);
     }
     __syncthreads();
     for (int j = threadIdx.x; j < 8 * 256; j += blockDim.x) {
@@ -298,10 +294,10 @@ __global__ void __launch_bounds__(256) k_hist_low(const uint64_t* __restrict__ k
 // K: uint64_t (the full keys; digit `pass` is bits 8 pass .. 8 pass + 7) or
 // uint32_t (the upper key halves; digit `pass` (4..7) is bits 8 pass - 32 ..).
 // V: uint32_t (the input position) or uint64_t (the lower key half << 32 | the
-// input position; the first pass takes the lower halves from `lo_src`, the
-// whole keys in input order).
+// input position; the first pass reads both halves from `lo_src`, the whole
+// keys in input order, and no `kin`).
 template <bool FIRST, class K = uint64_t, class V = uint32_t>
-__global__ void __launch_bounds__(kSortThreads, 3) k_onesweep(const K* __restrict__ kin,
+__global__ void __launch_bounds__(kSortThreads, kSortBlocksPerSM) k_onesweep(const K* __restrict__ kin,
                                                            const V* __restrict__ vin,
                                                            K* __restrict__ kout, V* __restrict__ vout,
                                                            uint64_t n, int pass, SortCtl* ctl,
@@ -342,10 +338,15 @@ __global__ void __launch_bounds__(kSortThreads, 3) k_onesweep(const K* __restric
     for (int j = 0; j < kSortItems; ++j) {
         const uint64_t idx = base + (uint64_t)warp * (32 * kSortItems) + (uint64_t)j * 32 + lane;
         const bool valid = idx < n;
-        k[j] = valid ? kin[idx] : (K)~0ull;
+        if constexpr (FIRST && sizeof(V) == 8) {  // the split sort's first pass reads the whole keys only
+            const uint64_t whole = valid ? lo_src[idx] : ~0ull;
+            k[j] = (K)(whole >> 32);
+            v[j] = (whole << 32) | (uint64_t)(uint32_t)idx;
+        } else {
+            k[j] = valid ? kin[idx] : (K)~0ull;
+        }
         if (FIRST) {
-            if constexpr (sizeof(V) == 8) v[j] = ((valid ? lo_src[idx] : 0ull) << 32) | (uint64_t)(uint32_t)idx;
-            else v[j] = (V)(uint32_t)idx;
+            if constexpr (sizeof(V) != 8) v[j] = (V)(uint32_t)idx;
         } else {
             v[j] = valid ? vin[idx] : (V)0;
         }
@@ -506,6 +507,11 @@ __device__ __forceinline__ void put_sorted(uint64_t o, uint32_t h, uint64_t pv, 
 // and writes itself there; the first point of a longer run lists it for
 // k_runs_warp / k_runs_mid (start, length) or flags it when it is longer than
 // kRunMid.  hi: the sorted upper halves; pv: lower half << 32 | input position.
+// A thread takes kRunsPer points (a grid stride apart) at a time: their places
+// first, then the coordinate gathers of all of them (random reads from the
+// input, the kernel's DRAM traffic), then the writes, so that each thread has
+// kRunsPer gathers in flight instead of one.
+constexpr int kRunsPer = 4;
 __global__ void __launch_bounds__(256) k_runs_small(const uint32_t* __restrict__ hi,
                                                     const uint64_t* __restrict__ pv,
                                                     const double* __restrict__ xyz, uint64_t n,
@@ -513,37 +519,70 @@ __global__ void __launch_bounds__(256) k_runs_small(const uint32_t* __restrict__
                                                     double* __restrict__ xs, double* __restrict__ ys,
                                                     double* __restrict__ zs, RunCtl* rc, uint32_t* mid_list) {
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-        const uint32_t h = hi[i];
-        uint64_t s = i, e = i + 1;
-        while (s > 0 && i - s <= kRunSmall && hi[s - 1] == h) --s;
-        while (e < n && e - s <= kRunSmall && hi[e] == h) ++e;
-        if (e - s > kRunSmall) {  // a longer run: its first point (if this is it) measures and lists it
-            if (s > 0 && hi[s - 1] == h) continue;
-            if (s != i) continue;
-            while (e < n && e - s <= kRunMid && hi[e] == h) ++e;
-            if (e - s > kRunMid) {
-                atomicOr(&rc->big, 1u);
-            } else if (e - s <= kRunWarp) {
-                const uint32_t slot = atomicAdd(&rc->w_count, 1u);
-                mid_list[2 * slot] = (uint32_t)s;
-                mid_list[2 * slot + 1] = (uint32_t)(e - s);
-            } else {
-                const uint32_t slot = rc->cap - 1u - atomicAdd(&rc->b_count, 1u);
-                mid_list[2 * slot] = (uint32_t)s;
-                mid_list[2 * slot + 1] = (uint32_t)(e - s);
+    for (uint64_t i0 = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i0 < n; i0 += kRunsPer * stride) {
+        uint64_t dst[kRunsPer], val[kRunsPer];
+        uint32_t hv[kRunsPer];
+        bool put[kRunsPer];
+#pragma unroll
+        for (int u = 0; u < kRunsPer; ++u) {
+            const uint64_t i = i0 + (uint64_t)u * stride;
+            put[u] = false;
+            dst[u] = 0;
+            val[u] = 0;
+            hv[u] = 0;
+            if (i >= n) continue;
+            const uint32_t h = hi[i];
+            uint64_t s = i, e = i + 1;
+            while (s > 0 && i - s <= kRunSmall && hi[s - 1] == h) --s;
+            while (e < n && e - s <= kRunSmall && hi[e] == h) ++e;
+            if (e - s > kRunSmall) {  // a longer run: its first point (if this is it) measures and lists it
+                if (s > 0 && hi[s - 1] == h) continue;
+                if (s != i) continue;
+                while (e < n && e - s <= kRunMid && hi[e] == h) ++e;
+                if (e - s > kRunMid) {
+                    atomicOr(&rc->big, 1u);
+                } else if (e - s <= kRunWarp) {
+                    const uint32_t slot = atomicAdd(&rc->w_count, 1u);
+                    mid_list[2 * slot] = (uint32_t)s;
+                    mid_list[2 * slot + 1] = (uint32_t)(e - s);
+                } else {
+                    const uint32_t slot = rc->cap - 1u - atomicAdd(&rc->b_count, 1u);
+                    mid_list[2 * slot] = (uint32_t)s;
+                    mid_list[2 * slot + 1] = (uint32_t)(e - s);
+                }
+                continue;
             }
-            continue;
+            const uint64_t mine = pv[i];
+            const uint32_t lo = (uint32_t)(mine >> 32);
+            uint64_t rank = 0;
+            for (uint64_t j = s; j < e; ++j) {
+                if (j == i) continue;
+                const uint32_t lj = (uint32_t)(pv[j] >> 32);
+                rank += (lj < lo || (lj == lo && j < i)) ? 1u : 0u;
+            }
+            put[u] = true;
+            dst[u] = s + rank;
+            val[u] = mine;
+            hv[u] = h;
         }
-        const uint64_t mine = pv[i];
-        const uint32_t lo = (uint32_t)(mine >> 32);
-        uint64_t rank = 0;
-        for (uint64_t j = s; j < e; ++j) {
-            if (j == i) continue;
-            const uint32_t lj = (uint32_t)(pv[j] >> 32);
-            rank += (lj < lo || (lj == lo && j < i)) ? 1u : 0u;
+        double px[kRunsPer], py[kRunsPer], pz[kRunsPer];
+#pragma unroll
+        for (int u = 0; u < kRunsPer; ++u) {
+            const uint64_t p = (uint32_t)val[u];
+            px[u] = put[u] ? xyz[3 * p] : 0.0;
+            py[u] = put[u] ? xyz[3 * p + 1] : 0.0;
+            pz[u] = put[u] ? xyz[3 * p + 2] : 0.0;
         }
-        put_sorted(s + rank, h, mine, xyz, keys_out, perm_out, xs, ys, zs);
+#pragma unroll
+        for (int u = 0; u < kRunsPer; ++u) {
+            if (!put[u]) continue;
+            const uint64_t o = dst[u];
+            keys_out[o] = ((uint64_t)hv[u] << 32) | (val[u] >> 32);
+            perm_out[o] = (uint32_t)val[u];
+            xs[o] = px[u];
+            ys[o] = py[u];
+            zs[o] = pz[u];
+        }
     }
 }
 
@@ -645,11 +684,15 @@ __global__ void __launch_bounds__(kRunWarpThreads) k_runs_warp(const uint32_t* _
     }
 }
 
-// Lower key half << 32 | input position, for a cloud whose upper halves are all equal.
-__global__ void k_pack_iota(const uint64_t* __restrict__ keys, uint64_t* __restrict__ pv, uint64_t n) {
+// The split sort's arrays in input order (no upper-digit pass ran): the upper
+// halves, and lower half << 32 | input position.
+__global__ void k_pack_iota(const uint64_t* __restrict__ keys, uint32_t* __restrict__ hi, uint64_t* __restrict__ pv,
+                            uint64_t n) {
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride)
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        hi[i] = (uint32_t)(keys[i] >> 32);
         pv[i] = (keys[i] << 32) | i;
+    }
 }
 
 __global__ void k_iota(uint32_t* perm, uint64_t n) {
@@ -697,7 +740,7 @@ int bbox_blocks_per_sm() {
     return per;
 }
 
-cudaError_t launch_bbox_encode(Cloud& c, const double* d_xyz, uint32_t* d_hi) {
+cudaError_t launch_bbox_encode(Cloud& c, const double* d_xyz, bool upper_hist_only) {
     cudaError_t e;
     const uint64_t n = c.n;
     const int sms = sm_count(c.device);
@@ -716,10 +759,10 @@ cudaError_t launch_bbox_encode(Cloud& c, const double* d_xyz, uint32_t* d_hi) {
         const bool hil = c.params.encoder == OCT_ENC_HILBERT_3D;
         BoxGeom* bg = c.d_box.as<BoxGeom>();
         uint64_t* keys = c.keys.as<uint64_t>();
-        if (d_hi == nullptr && hil) k_encode<5><<<grid, kEncThreads, 0, c.stream>>>(d_xyz, n, bg, keys, ctl);
-        else if (d_hi == nullptr) k_encode<1><<<grid, kEncThreads, 0, c.stream>>>(d_xyz, n, bg, keys, ctl);
-        else if (hil) k_encode<5, false><<<grid, kEncThreads, 0, c.stream>>>(d_xyz, n, bg, keys, ctl, d_hi);
-        else k_encode<1, false><<<grid, kEncThreads, 0, c.stream>>>(d_xyz, n, bg, keys, ctl, d_hi);
+        if (!upper_hist_only && hil) k_encode<5><<<grid, kEncThreads, 0, c.stream>>>(d_xyz, n, bg, keys, ctl);
+        else if (!upper_hist_only) k_encode<1><<<grid, kEncThreads, 0, c.stream>>>(d_xyz, n, bg, keys, ctl);
+        else if (hil) k_encode<5, false><<<grid, kEncThreads, 0, c.stream>>>(d_xyz, n, bg, keys, ctl);
+        else k_encode<1, false><<<grid, kEncThreads, 0, c.stream>>>(d_xyz, n, bg, keys, ctl);
         k_scan_hist<<<1, 256, 0, c.stream>>>(ctl, n);
     }
     return cudaGetLastError();
@@ -805,6 +848,7 @@ cudaError_t launch_sort_split(Cloud& c, const uint32_t skip[8], const double* d_
     const size_t nn = n ? n : 1;
     if ((e = c.keys_alt.reserve(8 * nn)) != cudaSuccess) return e;
     if ((e = c.perm.reserve(4 * nn)) != cudaSuccess) return e;
+    if ((e = c.keys_hi.reserve(4 * nn)) != cudaSuccess) return e;
     if ((e = c.keys_hi_alt.reserve(4 * nn)) != cudaSuccess) return e;
     if ((e = c.run_pv.reserve(8 * nn)) != cudaSuccess) return e;
     if ((e = c.run_pv_alt.reserve(8 * nn)) != cudaSuccess) return e;
@@ -851,7 +895,7 @@ cudaError_t launch_sort_split(Cloud& c, const uint32_t skip[8], const double* d_
         uint64_t* vout = vb[sel ^ 1]->as<uint64_t>();
         if (first)
             k_onesweep<true, uint32_t, uint64_t><<<(unsigned)tiles, kSortThreads, smem, c.stream>>>(
-                kin, nullptr, kout, vout, n, p, ctl, c.sort_status.as<unsigned long long>(), c.sort_epoch,
+                nullptr, nullptr, kout, vout, n, p, ctl, c.sort_status.as<unsigned long long>(), c.sort_epoch,
                 c.d_err.as<uint32_t>(), nullptr, nullptr, c.keys.as<uint64_t>());
         else
             k_onesweep<false, uint32_t, uint64_t><<<(unsigned)tiles, kSortThreads, smem, c.stream>>>(
@@ -864,7 +908,8 @@ cudaError_t launch_sort_split(Cloud& c, const uint32_t skip[8], const double* d_
     const uint64_t want = (n + 255) / 256;
     const int grid = (int)(want < (uint64_t)sms * 8 ? want : (uint64_t)sms * 8);
     if (first) {  // every upper digit constant: one run in input order
-        k_pack_iota<<<grid, 256, 0, c.stream>>>(c.keys.as<uint64_t>(), c.run_pv.as<uint64_t>(), n);
+        k_pack_iota<<<grid, 256, 0, c.stream>>>(c.keys.as<uint64_t>(), c.keys_hi.as<uint32_t>(),
+                                                 c.run_pv.as<uint64_t>(), n);
         sel = 0;
     }
     const uint32_t* hi = kb[sel]->as<uint32_t>();
@@ -921,7 +966,7 @@ cudaError_t launch_sort_dyn(int device, cudaStream_t s, uint64_t* k0, uint64_t* 
                             uint32_t** result_vals) {
     const size_t smem = onesweep_smem();
     const uint64_t max_tiles = (max_n + kSortTile - 1) / kSortTile;
-    const uint64_t resident = (uint64_t)sm_count(device) * 3;  // 3 x 60 KB tiles per SM
+    const uint64_t resident = (uint64_t)sm_count(device) * kSortBlocksPerSM;
     const unsigned grid = (unsigned)(max_tiles < resident ? (max_tiles ? max_tiles : 1) : resident);
     k_scan_hist<<<1, 256, 0, s>>>(ctl, 0, d_n);
     uint64_t* kb[2] = {k0, k1};
@@ -1041,7 +1086,7 @@ constexpr int kNoAllocBboxGrid = 148 * 4;
 struct NoAllocScratch {
     uint64_t keys_alt[OCT_NOALLOC_MAX_POINTS];            // 2 MiB
     uint32_t perm_alt[OCT_NOALLOC_MAX_POINTS];            // 1 MiB
-    unsigned long long status[kNoAllocTiles * 256];       // 172 KiB look-back words (86 tiles)
+    unsigned long long status[kNoAllocTiles * 256];       // look-back words, 256 per tile
     SortCtl ctl;
     BoxGeom bg;
     double partial[6 * kNoAllocBboxGrid];

@@ -23,9 +23,12 @@
 // Kernel: one cooperative, persistent launch.  Per level, phase A computes the
 // 8 children of every internal node (one lane per child: a binary search in the
 // parent's point range, the centre, the split flag) and ballots the split flags
-// per 32 children; phase B ranks the split children with a device-wide
-// exclusive scan (block partials + per-block scan) and writes the next
-// frontier and the offsets.  Grid barriers are bounded waits.
+// per 32 children; phase B ranks the split children and writes the next
+// frontier and the offsets.  A block's phase B reads only what its own phase A
+// wrote, plus the number of split children of the blocks before it, which it
+// takes by decoupled look-back over per-block status words (flag | count) —
+// so one grid barrier per level (the next level reads every block's frontier)
+// instead of two.  Grid barriers and look-back waits are bounded.
 #include "cloud.h"
 #include "sfc.cuh"
 
@@ -51,6 +54,20 @@ __device__ __forceinline__ uint32_t ld_acquire_u32(const uint32_t* p) {
     asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
     return v;
 }
+
+__device__ __forceinline__ unsigned long long ld_acquire_u64(const unsigned long long* p) {
+    unsigned long long v;
+    asm volatile("ld.acquire.gpu.global.u64 %0, [%1];" : "=l"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_release_u64(unsigned long long* p, unsigned long long v) {
+    asm volatile("st.release.gpu.global.u64 [%0], %1;" ::"l"(p), "l"(v) : "memory");
+}
+
+// look-back status word of a block at one level: flag (bits 62-63) | split children (low 32 bits)
+constexpr unsigned long long kLbLocal = 1ull << 62;   // this block's count
+constexpr unsigned long long kLbPrefix = 2ull << 62;  // this block's and every earlier block's
+constexpr unsigned long long kLbFlags = 3ull << 62;
 
 // Grid-wide barrier for a cooperative launch; gives up after kSpinLimit polls.
 __device__ void grid_barrier(BuildCtl* ctl, uint32_t* err) {
@@ -106,11 +123,13 @@ __global__ void __launch_bounds__(kBuildThreads) k_build(const uint64_t* __restr
                                                          uint32_t* __restrict__ offsets, uint2* __restrict__ ranges,
                                                          double* __restrict__ centers, uint32_t node_cap,
                                                          FrontierNode* __restrict__ fa, FrontierNode* __restrict__ fb,
-                                                         uint32_t* __restrict__ masks, uint32_t* __restrict__ parts,
-                                                         BuildCtl* ctl, uint32_t* err) {
+                                                         uint32_t* __restrict__ masks,
+                                                         unsigned long long* __restrict__ lb, BuildCtl* ctl,
+                                                         uint32_t* err) {
     __shared__ BoxGeom bg;
     __shared__ uint32_t red[kBuildWarps];
     __shared__ uint32_t chunk_pre[kBuildThreads];
+    __shared__ uint32_t s_excl;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     if (tid == 0) bg = *bgp;
     __syncthreads();
@@ -141,9 +160,12 @@ __global__ void __launch_bounds__(kBuildThreads) k_build(const uint64_t* __restr
     FrontierNode* nxt = fb;
     uint32_t F = ld_acquire_u32(&ctl->level_internal[0]);
     uint32_t n_internal = F;
+    // first node of the level being created, kept by every block (block 0 writes the
+    // level starts for the host after the level's barrier, so they are not read back here)
+    uint32_t level_first = 1;
     for (uint32_t l = 0; l < kMaxDepth && F > 0; ++l) {
         const uint32_t child_level = l + 1;
-        const uint32_t lstart = ld_acquire_u32(&ctl->level_start[l + 1]);
+        const uint32_t lstart = level_first;
         const uint64_t nchild = 8ull * F;
         const uint64_t next_start = (uint64_t)lstart + nchild;
         if (next_start > node_cap) {  // uniform across blocks: every block sees the same values
@@ -194,20 +216,44 @@ __global__ void __launch_bounds__(kBuildThreads) k_build(const uint64_t* __restr
             }
         }
         const uint32_t bsum = block_sum(my_count, red);
-        if (tid == 0) parts[blockIdx.x] = bsum;
-        grid_barrier(ctl, err);
-        // ---- phase B: rank split children, next frontier, offsets ----
-        uint32_t pre = 0, tot = 0;
-        {
-            uint32_t a = 0, b = 0;
-            for (uint32_t i = tid; i < gridDim.x; i += kBuildThreads) {
-                const uint32_t v = ((volatile uint32_t*)parts)[i];
-                if (i < blockIdx.x) a += v;
-                b += v;
+        // ---- the split children of the blocks before this one: decoupled look-back ----
+        unsigned long long* st = lb + (uint64_t)l * gridDim.x;
+        if (warp == 0) {
+            if (lane == 0)
+                st_release_u64(&st[blockIdx.x], (blockIdx.x == 0 ? kLbPrefix : kLbLocal) | bsum);
+            uint32_t excl = 0;
+            int64_t t = (int64_t)blockIdx.x - 1;  // the nearest predecessor not summed yet
+            uint32_t spins = 0;
+            while (t >= 0) {
+                const int64_t ti = t - lane;  // lane 0: the nearest
+                const unsigned long long v = ti >= 0 ? ld_acquire_u64(&st[ti]) : kLbPrefix;
+                const uint32_t ready = __ballot_sync(0xffffffffu, (v & kLbFlags) != 0);
+                const uint32_t pref = __ballot_sync(0xffffffffu, (v & kLbFlags) == kLbPrefix);
+                // lanes up to the nearest prefix must all have published; else wait for them
+                const uint32_t upto = pref ? ((pref & (0u - pref)) << 1) - 1u : 0xffffffffu;
+                if ((ready & upto) != upto) {
+                    if (++spins > kSpinLimit) {
+                        if (lane == 0) set_err(err, kErrSpinLimit);
+                        break;
+                    }
+                    __nanosleep(32);
+                    continue;
+                }
+                uint32_t c = ((upto >> lane) & 1u) && ti >= 0 ? (uint32_t)(v & 0xffffffffull) : 0u;
+#pragma unroll
+                for (int off = 16; off > 0; off >>= 1) c += __shfl_xor_sync(0xffffffffu, c, off);
+                excl += c;
+                if (pref) break;
+                t -= 32;
             }
-            pre = block_sum(a, red);
-            tot = block_sum(b, red);
+            if (lane == 0) {
+                if (blockIdx.x > 0) st_release_u64(&st[blockIdx.x], kLbPrefix | (excl + bsum));
+                s_excl = excl;
+            }
         }
+        __syncthreads();
+        // ---- phase B: rank split children, next frontier, offsets ----
+        const uint32_t pre = s_excl;
         const uint32_t next_level_start = (uint32_t)next_start;
         uint32_t carry = pre;
         for (uint32_t seg = w0; seg < w1; seg += kBuildThreads) {
@@ -249,6 +295,9 @@ __global__ void __launch_bounds__(kBuildThreads) k_build(const uint64_t* __restr
             carry += segsum;
             __syncthreads();
         }
+        grid_barrier(ctl, err);
+        // every block has published its inclusive prefix before the barrier: the last one's is the total
+        const uint32_t tot = (uint32_t)(ld_acquire_u64(&st[gridDim.x - 1]) & 0xffffffffull);
         if (blockIdx.x == 0 && tid == 0) {
             ctl->level_start[l + 2] = next_level_start;
             ctl->level_internal[l + 1] = tot;
@@ -256,7 +305,7 @@ __global__ void __launch_bounds__(kBuildThreads) k_build(const uint64_t* __restr
             if (tot > 0) ctl->max_depth_seen = l + 2;
         }
         n_internal += tot;
-        grid_barrier(ctl, err);
+        level_first = next_level_start;
         FrontierNode* tmp = cur;
         cur = nxt;
         nxt = tmp;
@@ -292,12 +341,11 @@ cudaError_t launch_build(Cloud& c, bool* capacity_ok) {
     if ((e = c.centers.reserve(24 * cap)) != cudaSuccess) return e;
     if ((e = c.frontier.reserve(2 * sizeof(FrontierNode) * fcap)) != cudaSuccess) return e;
     if ((e = c.masks.reserve(4 * ((8 * fcap + 31) / 32 + 1))) != cudaSuccess) return e;
-    if ((e = c.d_build.reserve(sizeof(BuildCtl))) != cudaSuccess) return e;
 
     int dev = c.device;
     int per_sm = 0;
     void (*kfn)(const uint64_t*, uint32_t, uint32_t, const BoxGeom*, uint32_t*, uint2*, double*, uint32_t,
-                FrontierNode*, FrontierNode*, uint32_t*, uint32_t*, BuildCtl*, uint32_t*) =
+                FrontierNode*, FrontierNode*, uint32_t*, unsigned long long*, BuildCtl*, uint32_t*) =
         (c.params.encoder == OCT_ENC_HILBERT_3D) ? k_build<5> : k_build<1>;
     if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kfn, kBuildThreads, 0)) != cudaSuccess)
         return e;
@@ -308,8 +356,11 @@ cudaError_t launch_build(Cloud& c, bool* capacity_ok) {
     const uint64_t max_useful = (8 * fcap + 31) / 32 / kBuildWarps + 1;
     if (grid > max_useful) grid = (unsigned)max_useful;
     if (grid < 1) grid = 1;
-    if ((e = c.parts.reserve(4 * (size_t)grid + 64)) != cudaSuccess) return e;
-    if ((e = cudaMemsetAsync(c.d_build.ptr, 0, sizeof(BuildCtl), c.stream)) != cudaSuccess) return e;
+    // BuildCtl, then the look-back status words of every level and block (zeroed: no flag)
+    const size_t ctl_bytes = (sizeof(BuildCtl) + 255) / 256 * 256;
+    const size_t lb_bytes = sizeof(unsigned long long) * (kMaxDepth + 1) * (size_t)grid;
+    if ((e = c.d_build.reserve(ctl_bytes + lb_bytes)) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(c.d_build.ptr, 0, ctl_bytes + lb_bytes, c.stream)) != cudaSuccess) return e;
 
     const uint64_t* keys = c.keys.as<uint64_t>();
     uint32_t nn = (uint32_t)n;
@@ -322,10 +373,11 @@ cudaError_t launch_build(Cloud& c, bool* capacity_ok) {
     FrontierNode* fa = c.frontier.as<FrontierNode>();
     FrontierNode* fb = fa + fcap;
     uint32_t* masks = c.masks.as<uint32_t>();
-    uint32_t* parts = c.parts.as<uint32_t>();
     BuildCtl* ctl = c.d_build.as<BuildCtl>();
+    unsigned long long* lb = reinterpret_cast<unsigned long long*>(static_cast<unsigned char*>(c.d_build.ptr) +
+                                                                   ctl_bytes);
     uint32_t* err = c.d_err.as<uint32_t>();
-    void* args[] = {(void*)&keys, &nn, &ml, (void*)&bg, &offs, &rng, &ctr, &ncap, &fa, &fb, &masks, &parts,
+    void* args[] = {(void*)&keys, &nn, &ml, (void*)&bg, &offs, &rng, &ctr, &ncap, &fa, &fb, &masks, &lb,
                     &ctl, &err};
     e = cudaLaunchCooperativeKernel((const void*)kfn, dim3(grid), dim3(kBuildThreads), args, 0, c.stream);
     return e;

@@ -123,10 +123,11 @@ def test_gpu_build_dense_cluster(port, enc):
     oc.close()
 
 
-@pytest.mark.parametrize("n", [1, 2, 100, 3071, 3072, 3073, 8193, 70_000])
+@pytest.mark.parametrize("n", [1, 2, 100, 3071, 3072, 3073, 4607, 4608, 4609, 8193, 9217, 70_000])
 def test_gpu_sort_sizes(port, n):
-    """Keys, order and sorted points at sizes around the sort's 3072-key tiles
-    and its single-tile and many-tile cases."""
+    """Keys, order and sorted points at sizes around the sort's 4608-key tiles
+    (and the 3072-key tiles of its earlier shape) and its single-tile and
+    many-tile cases."""
     xyz = lidar_tile(max(n, 2), 120.0, 36)[:n]
     keys, perm, box, sxyz = port.encode_sort(5, xyz)
     oc = LinearOctree(xyz, encoder="hilbert", max_points_leaf=64)
