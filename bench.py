@@ -271,7 +271,8 @@ def cpu_leg(args, xyz_h, h, eng, proxy, eng_cfg):
         return offs, idx, kidx, kd2, kcnt, {}
 
     runs = {"plain": lambda: single(0, 0, args.radius_group, 0), "packet": lambda: single(1, 0, 8, 1),
-            "packet_fp32": lambda: single(1, 1, 8, 1), "engine": lambda: engine(0), "engine_fp32": lambda: engine(1)}
+            "packet_fp32": lambda: single(1, 1, 8, 1), "packet_fp32_radius": lambda: single(1, 2, 8, 1),
+            "engine": lambda: engine(0), "engine_fp32": lambda: engine(1), "engine_fp32_radius": lambda: engine(2)}
     out = {}
     total_diffs, max_err = 0, 0.0
     for name, fn in runs.items():
@@ -629,8 +630,10 @@ def run_b200(args, rank, world, local_rank):
     ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
 
     # (packet, fp32_filter, lanes, kNN in groups of 4 queries per warp)
+    # (packet, fp32_filter, lanes, knn_packet); fp32_filter 1: the radius and kNN FP32 filters, 2: radius only
     SEARCH_PATHS = {"plain": (0, 0, args.radius_group, 0), "packet": (1, 0, 8, 1), "packet_fp32": (1, 1, 8, 1),
-                    "knn_per_query": (1, 0, 8, 0), "engine": (1, 0, 8, 1), "engine_fp32": (1, 1, 8, 1)}
+                    "packet_fp32_radius": (1, 2, 8, 1), "knn_per_query": (1, 0, 8, 0), "engine": (1, 0, 8, 1),
+                    "engine_fp32": (1, 1, 8, 1), "engine_fp32_radius": (1, 2, 8, 1)}
 
     # the batched engine: both request sets of a step in one graph launch (kNN beside the radius search)
     from types import SimpleNamespace
@@ -655,8 +658,9 @@ def run_b200(args, rank, world, local_rank):
         return None, ms, 0.0, int(places[0].n_results)
 
     def configure(name):
-        if name.startswith("engine"):  # the batched engine: its autotuned configuration, FP32 filter on or off
-            eng.set_config(**dict(eng_cfg, fp32_filter=int(name == "engine_fp32")))
+        if name.startswith("engine"):  # the batched engine: its autotuned configuration, FP32 filters as named
+            eng.set_config(**dict(eng_cfg, fp32_filter={"engine_fp32": 1, "engine_fp32_radius": 2}.get(
+                name, eng_cfg["fp32_filter"])))
         packet, fp32, lanes, knn_packet = SEARCH_PATHS[name]
         cfg = capi.OctSearchConfig(packet, fp32, lanes, knn_packet, args.knn_bucket)
         capi.check(L.oct_set_search_config(h, C.byref(cfg)), h, "search config")
@@ -919,7 +923,11 @@ def run_b200(args, rank, world, local_rank):
             "radius_qps": chosen["radius_qps"], "knn_qps": chosen["knn_qps"],
             "avg_neighbours": chosen["avg_neighbours"], "paths": paths,
             "batched_vs_plain": (paths["engine"]["qps"] / paths["plain"]["qps"]
-                                 if "engine" in paths and "plain" in paths else None), "engine_config": eng_cfg,
+                                 if "engine" in paths and "plain" in paths else None),
+            # the batched search with FP32 filters (both; the radius filter only) against the plain FP64 path
+            "batched_fp32_vs_plain": {k: paths[k]["qps"] / paths["plain"]["qps"]
+                                      for k in ("engine_fp32", "engine_fp32_radius") if k in paths and "plain" in paths},
+            "engine_config": eng_cfg,
             "build": build, "roofline": roofline, "cpu_baseline": None, "parity": None,
             "batched": None, "serving": None, "large": None,
             "e2e": {"value": e2e_val, "unit": "queries/s", "h2d_bytes_per_step": h2d, "d2h_bytes_per_step": d2h,

@@ -124,13 +124,15 @@ int oct_set_radius_group(oct_cloud cloud, int lanes);
  *  packet       1 (default): the query centres are ordered along the cloud's
  *               curve and each warp walks the tree once for 32 neighbouring
  *               queries; 0: one query per group of radius_lanes lanes.
- *  fp32_filter  1: radius searches test leaf points in FP32 relative to
- *               their leaf's centre and re-test in FP64 only points within a
- *               rigorous error band of the boundary (packet path); the group
- *               kNN (knn_packet, k <= 64) tests points in FP32 relative to the
- *               box centre and computes the exact FP64 distance only for points
- *               within a rigorous band of the query's k-th distance or inside
- *               it; 0 (default): every test in FP64.  Results are the same.
+ *  fp32_filter  OCT_FP32_ALL (1): radius searches test leaf points in FP32
+ *               relative to their leaf's centre and re-test in FP64 only points
+ *               within a rigorous error band of the boundary (packet path); the
+ *               group kNN (knn_packet, k <= 64) tests points in FP32 relative
+ *               to the box centre and computes the exact FP64 distance only for
+ *               points within a rigorous band of the query's k-th distance or
+ *               inside it.  OCT_FP32_RADIUS (2): the radius filter only;
+ *               OCT_FP32_KNN (3): the kNN filter only; 0 (default): every test
+ *               in FP64.  Results are the same.
  *  radius_lanes lanes per query when packet is 0: 8 (default), 16 or 32.
  *  knn_packet   1 (default): kNN with k <= 64 on the packet path walks the
  *               tree once per group of 4 curve-ordered queries per warp
@@ -150,6 +152,9 @@ int oct_set_radius_group(oct_cloud cloud, int lanes);
  *               (1-64; 0 = the default); every group after the first of a
  *               run starts from the previous group's k-th distances.  Results
  *               are the same. */
+#define OCT_FP32_ALL 1    /* oct_search_config.fp32_filter: radius and kNN FP32 filters */
+#define OCT_FP32_RADIUS 2 /* the radius filter only */
+#define OCT_FP32_KNN 3    /* the kNN filter only */
 typedef struct {
     int32_t packet;
     int32_t fp32_filter;
@@ -353,7 +358,8 @@ int oct_engine_destroy(oct_engine engine);
 /* Run on this CUDA stream (cudaStream_t); kNN work forks onto a private stream and joins back. */
 int oct_engine_set_stream(oct_engine engine, void* cuda_stream);
 int oct_engine_last_error(oct_engine engine, char* buf, size_t len);
-/* Search configuration of the engine (oct_search_config: fp32_filter, knn_bucket;
+/* Search configuration of the engine (oct_search_config: fp32_filter (0-3, as for
+ * a cloud), knn_bucket;
  * knn_packet = 1 (the engine's default): kNN with k <= 64 in groups of 4
  * curve-ordered queries per warp, 0: one warp per query;
  * reserved[0] = radius blocks per SM, reserved[1] = kNN blocks per SM, 0 = default;

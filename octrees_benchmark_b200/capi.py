@@ -70,6 +70,9 @@ class OctRequestPlace(C.Structure):
 OCT_SERVER_PLAIN = 0x1
 OCT_SERVER_FIFO = 0x2
 OCT_SERVER_NO_GRAPH = 0x4
+OCT_FP32_ALL = 1
+OCT_FP32_RADIUS = 2
+OCT_FP32_KNN = 3
 OCT_CLOUD_OWNED = 0x1
 
 

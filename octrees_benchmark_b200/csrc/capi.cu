@@ -132,14 +132,14 @@ cudaError_t radius_pass(Cloud& c, int kernel, int algo, bool fill, const double*
     if (!c.packet) return launch_radius(c, kernel, algo, c.radius_group, fill, dq, nq, dr, radius, counts, counts2, offs,
                                         out, cap);
     cudaError_t e;
-    if (c.fp32_filter && !c.rel_built) {
+    if (fp32_on_radius(c.fp32_filter) && !c.rel_built) {
         if ((e = launch_leaf_rel(c)) != cudaSuccess) return e;
         c.rel_built = true;
     }
     if ((e = c.stats.reserve(64)) != cudaSuccess) return e;
     if (!*order && (e = launch_query_order(c, dq, nq, order)) != cudaSuccess) return e;
-    return launch_radius_packet(c, kernel, algo, fill ? 1 : 0, c.fp32_filter != 0, dq, nq, dr, radius, *order, counts,
-                                counts2, offs, out, cap);
+    return launch_radius_packet(c, kernel, algo, fill ? 1 : 0, fp32_on_radius(c.fp32_filter), dq, nq, dr, radius,
+                                *order, counts, counts2, offs, out, cap);
 }
 
 // Radius search in one traversal (packet path, FP64 or FP32 filter): every query's results go
@@ -156,7 +156,7 @@ int radius_one_pass(Cloud& c, int kernel, int algo, const double* dq, uint64_t n
     CK(c.ck_ctr.reserve(256));
     const uint32_t* order = nullptr;
     CK(launch_query_order(c, dq, nq, &order));
-    if (c.fp32_filter && !c.rel_built) {  // the FP32 filter reads leaf-relative coordinates
+    if (fp32_on_radius(c.fp32_filter) && !c.rel_built) {  // the FP32 filter reads leaf-relative coordinates
         CK(launch_leaf_rel(c));
         c.rel_built = true;
     }
@@ -174,8 +174,8 @@ int radius_one_pass(Cloud& c, int kernel, int algo, const double* dq, uint64_t n
         ChunkArgs ck{c.ck_pool.as<uint32_t>(), c.ck_next.as<uint32_t>(), c.ck_first.as<uint32_t>(),
                      c.ck_ctr.as<uint32_t>(), c.ck_cap};
         CK(cudaMemsetAsync(ck.ctr, 0, 4, c.stream));
-        CK(launch_radius_packet(c, kernel, pass_algo, 2, c.fp32_filter != 0, dq, nq, dr, radius, order, dc, nullptr,
-                                nullptr, nullptr, 0, &ck));
+        CK(launch_radius_packet(c, kernel, pass_algo, 2, fp32_on_radius(c.fp32_filter), dq, nq, dr, radius, order,
+                                dc, nullptr, nullptr, nullptr, 0, &ck));
         CK(launch_scan_u64(c, dc, doffs, nq));
         CK(cudaMemcpyAsync(c.pinned, doffs + nq, 8, cudaMemcpyDeviceToHost, c.stream));
         const int st = sync_and_check(c, kErrChunkCapacity);
@@ -492,8 +492,8 @@ int oct_set_radius_group(oct_cloud h, int lanes) {
 int oct_set_search_config(oct_cloud h, const oct_search_config* cfg) {
     if (!h || !cfg) return OCT_ERR_INVALID_ARG;
     Cloud& c = h->c;
-    if (cfg->packet < 0 || cfg->packet > 1 || cfg->fp32_filter < 0 || cfg->fp32_filter > 1)
-        return set_error(c, OCT_ERR_INVALID_ARG, "packet and fp32_filter are 0 or 1");
+    if (cfg->packet < 0 || cfg->packet > 1 || cfg->fp32_filter < 0 || cfg->fp32_filter > OCT_FP32_KNN)
+        return set_error(c, OCT_ERR_INVALID_ARG, "packet is 0 or 1, fp32_filter 0-3");
     c.packet = cfg->packet;
     c.fp32_filter = cfg->fp32_filter;
     c.radius_group = (cfg->radius_lanes == 16 || cfg->radius_lanes == 32) ? cfg->radius_lanes : 8;
@@ -744,7 +744,7 @@ int oct_build(oct_cloud h, oct_tree_info* info) {
         CK(cudaMemsetAsync(c.offsets.as<uint32_t>() + c.n_total, 0, 4, c.stream));
         c.rel_built = false;
         c.crel_built = false;
-        if (c.fp32_filter && c.packet) {  // the FP32 search reads leaf-relative coordinates
+        if (fp32_on_radius(c.fp32_filter) && c.packet) {  // the FP32 search reads leaf-relative coordinates
             CK(launch_leaf_rel(c));
             c.rel_built = true;
         }
@@ -893,7 +893,7 @@ int oct_tree_import(oct_cloud h, const oct_tree_info* info, const double* box12,
     c.built = true;
     c.rel_built = false;
     c.crel_built = false;
-    if (c.fp32_filter && c.packet) {  // the FP32 search reads leaf-relative coordinates
+    if (fp32_on_radius(c.fp32_filter) && c.packet) {  // the FP32 search reads leaf-relative coordinates
         CK(launch_leaf_rel(c));
         c.rel_built = true;
     }

@@ -195,7 +195,7 @@ struct Cloud {
     bool crel_built = false;
     // search configuration (oct_set_search_config)
     int packet = 1;
-    int fp32_filter = 0;
+    int fp32_filter = 0;  // 0, OCT_FP32_ALL, OCT_FP32_RADIUS or OCT_FP32_KNN
     int knn_packet = 1;  // kNN (k <= 64, packet path): groups of queries per warp
     uint32_t knn_bucket = 256;
     int two_pass = 0;   // 1: packet radius searches count, then fill (no result chunks)
@@ -335,6 +335,10 @@ cudaError_t launch_sort_dyn(int device, cudaStream_t s, uint64_t* k0, uint64_t* 
                             uint32_t** result_vals);
 cudaError_t launch_knn(Cloud& c, const double* d_centers, uint64_t nq, uint32_t k, uint32_t* d_idx, double* d_d2,
                        uint32_t* d_counts);
+
+// oct_search_config.fp32_filter: which searches run their FP32 filter.
+inline bool fp32_on_radius(int f) { return f == OCT_FP32_ALL || f == OCT_FP32_RADIUS; }
+inline bool fp32_on_knn(int f) { return f == OCT_FP32_ALL || f == OCT_FP32_KNN; }
 
 // One kernel of each source file's device code (each file is its own device
 // library), and the loading of every kernel of those libraries on a device

@@ -411,7 +411,7 @@ cudaError_t enqueue_work(oct_engine e) {
                                             e->knn_d2.as<double>(), e->knn_counts.as<uint32_t>(), err,
                                             ctr + 2 * kRadiusVariants + 4 * v, e->knn_fb.as<uint32_t>(),
                                             kKnnEstimate, kKnnGroupChunk, e->knn_bps, e->knn_heads.as<double>(),
-                                            e->knn_heads.bytes, e->fp32 != 0, stats + 2);
+                                            e->knn_heads.bytes, fp32_on_knn(e->fp32), stats + 2);
             else
                 r2 = launch_knn_table(e->device, ks, &dyn->groups[kRadiusVariants + v], one, 0, 32u << v,
                                       order, e->bucket, e->knn_idx.as<uint32_t>(), e->knn_d2.as<double>(),
@@ -460,6 +460,10 @@ cudaError_t enqueue_work(oct_engine e) {
     return cudaGetLastError();
 }
 
+// Captured graphs kept per engine (a shape is its request variants, sort passes
+// and, for a single-cloud batch, the cloud).
+constexpr size_t kGraphCache = 1024;
+
 // Launch the current batch: the captured graph of its shape (captured now if
 // new) or the direct sequence.
 int launch_batch(oct_engine e, bool record_start) {
@@ -482,7 +486,9 @@ int launch_batch(oct_engine e, bool record_start) {
                 (!e->one_cloud || std::memcmp(&p.view, &e->one_view, sizeof(CloudView)) == 0))
                 exec = p.exec;
         if (!exec) {
-            if (e->graphs.size() >= 64) {  // keep the cache bounded: the oldest graph goes
+            // keep the cache bounded (the oldest graph goes), but large enough for every shape a
+            // serving mix produces: an instantiation now and then takes tens of ms instead of ~0.2
+            if (e->graphs.size() >= kGraphCache) {
                 cudaGraphExecDestroy(e->graphs.front().exec);
                 e->graphs.erase(e->graphs.begin());
             }
@@ -590,7 +596,8 @@ int submit(oct_engine e, const oct_request* rq, uint32_t n) {
     for (uint32_t i = 0; i < n; ++i) {
         int kv = 0;
         while (rq[i].type == OCT_REQ_KNN && (32u << kv) < rq[i].k) ++kv;
-        var[i] = rq[i].type == OCT_REQ_RADIUS ? radius_variant(rq[i].kernel, rq[i].algo, e->fp32) : kRadiusVariants + kv;
+        var[i] = rq[i].type == OCT_REQ_RADIUS ? radius_variant(rq[i].kernel, rq[i].algo, fp32_on_radius(e->fp32))
+                                              : kRadiusVariants + kv;
         if (rq[i].nq) rows.push_back(i);
     }
     std::stable_sort(rows.begin(), rows.end(), [&](uint32_t a, uint32_t b) { return var[a] < var[b]; });
@@ -602,7 +609,9 @@ int submit(oct_engine e, const oct_request* rq, uint32_t n) {
         for (uint32_t i : rows) {
             Cloud& c = rq[i].cloud->c;
             const bool radius = rq[i].type == OCT_REQ_RADIUS;
-            if (radius ? c.rel_built : (c.crel_built || !e->knn_group || rq[i].k > 64)) continue;
+            if (radius ? (c.rel_built || !fp32_on_radius(e->fp32))
+                       : (c.crel_built || !fp32_on_knn(e->fp32) || !e->knn_group || rq[i].k > 64))
+                continue;
             DeviceGuardE gc(c.device);
             if (radius) {
                 EK(launch_leaf_rel(c));
@@ -919,13 +928,14 @@ int oct_engine_last_error(oct_engine e, char* buf, size_t len) {
 int oct_engine_set_config(oct_engine e, const oct_search_config* cfg) {
     if (!e || !cfg) return OCT_ERR_INVALID_ARG;
     if (cfg->knn_bucket < 0 || cfg->reserved[0] < 0 || cfg->reserved[0] > 16 || cfg->reserved[1] < 0 ||
-        cfg->reserved[1] > 16 || cfg->reserved[2] < 0 || cfg->reserved[2] > 1)
+        cfg->reserved[1] > 16 || cfg->reserved[2] < 0 || cfg->reserved[2] > 1 || cfg->fp32_filter < 0 ||
+        cfg->fp32_filter > OCT_FP32_KNN)
         return fail(e, OCT_ERR_INVALID_ARG, "bad engine configuration");
     if (e->in_flight) {
         const int st = finish(e);
         if (st != OCT_OK) return st;
     }
-    const int fp32 = cfg->fp32_filter ? 1 : 0;
+    const int fp32 = cfg->fp32_filter;
     const uint32_t bucket = (uint32_t)cfg->knn_bucket;
     const int knn_group = cfg->knn_packet ? 1 : 0;
     if (fp32 != e->fp32 || bucket != e->bucket || cfg->reserved[0] != e->radius_bps ||
@@ -1099,8 +1109,11 @@ int oct_engine_autotune(oct_engine e, const oct_request* rq, uint32_t n, oct_sea
     };
     oct_search_config cfg;
     oct_engine_get_config(e, &cfg);
+    // the radius filter and the kNN filter are chosen separately (each on its own kind of request)
+    bool radius_f32 = fp32_on_radius(cfg.fp32_filter), knn_f32 = fp32_on_knn(cfg.fp32_filter);
+    auto combined = [](bool r, bool k) { return r ? (k ? OCT_FP32_ALL : OCT_FP32_RADIUS) : (k ? OCT_FP32_KNN : 0); };
     if (!radius.empty()) {
-        const int fp32s[2] = {0, 1};
+        const int fp32s[2] = {0, OCT_FP32_RADIUS};
         const int bps[3] = {4, 8, 12};
         float best = 1e30f;
         oct_search_config pick = cfg;
@@ -1117,20 +1130,24 @@ int oct_engine_autotune(oct_engine e, const oct_request* rq, uint32_t n, oct_sea
                     pick = c2;
                 }
             }
-        cfg.fp32_filter = pick.fp32_filter;
+        radius_f32 = fp32_on_radius(pick.fp32_filter);
+        cfg.fp32_filter = combined(radius_f32, knn_f32);
         cfg.reserved[0] = pick.reserved[0];
     }
     if (!knn.empty()) {
         // groups of queries per warp (blocks per SM follow from its shared memory), then one warp per query
+        // (the group kernel with and without its FP32 filter)
         struct KnnCfg {
-            int group, bucket, bps;
+            int group, bucket, bps, f32;
         };
-        const KnnCfg cands[10] = {{1, 128, 0}, {1, 256, 0}, {0, 0, 8},   {0, 0, 16},  {0, 64, 8},
-                                  {0, 64, 16}, {0, 128, 8}, {0, 128, 16}, {0, 256, 8}, {0, 256, 16}};
+        const KnnCfg cands[12] = {{1, 128, 0, 0},  {1, 256, 0, 0}, {1, 128, 0, 1},  {1, 256, 0, 1},
+                                  {0, 0, 8, 0},    {0, 0, 16, 0},  {0, 64, 8, 0},   {0, 64, 16, 0},
+                                  {0, 128, 8, 0},  {0, 128, 16, 0}, {0, 256, 8, 0}, {0, 256, 16, 0}};
         float best = 1e30f;
         oct_search_config pick = cfg;
         for (const KnnCfg& kc : cands) {
             oct_search_config c2 = cfg;
+            c2.fp32_filter = combined(radius_f32, kc.f32 != 0);
             c2.knn_packet = kc.group;
             c2.knn_bucket = kc.bucket;
             c2.reserved[1] = kc.bps;
@@ -1142,6 +1159,8 @@ int oct_engine_autotune(oct_engine e, const oct_request* rq, uint32_t n, oct_sea
                 pick = c2;
             }
         }
+        knn_f32 = fp32_on_knn(pick.fp32_filter);
+        cfg.fp32_filter = combined(radius_f32, knn_f32);
         cfg.knn_packet = pick.knn_packet;
         cfg.knn_bucket = pick.knn_bucket;
         cfg.reserved[1] = pick.reserved[1];

@@ -1466,7 +1466,7 @@ cudaError_t launch_knn(Cloud& c, const double* d_centers, uint64_t nq, uint32_t 
     const int grid = (int)(want < cap ? want : cap);
     if (c.packet && k <= 64) {
         // the FP32 filter (group kernel): centre-relative FP32 points, built on first use
-        const bool f32 = c.fp32_filter != 0 && c.knn_packet != 0;
+        const bool f32 = fp32_on_knn(c.fp32_filter) && c.knn_packet != 0;
         if (f32 && !c.crel_built) {
             cudaError_t e;
             if ((e = launch_center_rel(c)) != cudaSuccess) return e;

@@ -93,7 +93,7 @@ class BatchEngine:
     # ---- configuration ------------------------------------------------------
     def set_config(self, fp32_filter: bool = False, knn_bucket: int = 128, radius_blocks_per_sm: int = 0,
                    knn_blocks_per_sm: int = 0, serial: bool = False, knn_group: bool = True):
-        cfg = OctSearchConfig(1, int(bool(fp32_filter)), 32, int(bool(knn_group)), int(knn_bucket))
+        cfg = OctSearchConfig(1, int(fp32_filter), 32, int(bool(knn_group)), int(knn_bucket))
         cfg.reserved[0] = int(radius_blocks_per_sm)
         cfg.reserved[1] = int(knn_blocks_per_sm)
         cfg.reserved[2] = int(bool(serial))

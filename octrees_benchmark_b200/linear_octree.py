@@ -169,10 +169,11 @@ class LinearOctree:
                           knn_estimate: int = 0, knn_group_run: int = 0):
         """Search path: packet (32 curve-ordered queries per warp) or one query per
         ``radius_lanes`` lanes; FP32 filter with FP64 re-tests (radius: leaf-relative points;
-        group kNN: points relative to the box centre, FP64 only near the k-th distance); kNN in groups
+        group kNN: points relative to the box centre, FP64 only near the k-th distance; ``fp32_filter``
+        True / OCT_FP32_ALL both, OCT_FP32_RADIUS or OCT_FP32_KNN one of them); kNN in groups
         of 4 queries per warp (``knn_packet``; else one warp per query); ``two_pass`` counts
         then fills instead of the one-pass packet radius search."""
-        cfg = OctSearchConfig(int(bool(packet)), int(bool(fp32_filter)), int(radius_lanes), int(bool(knn_packet)),
+        cfg = OctSearchConfig(int(bool(packet)), int(fp32_filter), int(radius_lanes), int(bool(knn_packet)),
                               int(knn_bucket))
         cfg.reserved[0] = int(bool(two_pass))
         cfg.reserved[1] = int(knn_estimate)  # kNN provisional threshold, percent; 0 default, < 0 off

@@ -70,7 +70,7 @@ class Server:
 
     def set_config(self, fp32_filter=False, knn_bucket=128, radius_blocks_per_sm=0, knn_blocks_per_sm=0,
                    serial=False, knn_group=True):
-        cfg = OctSearchConfig(1, int(bool(fp32_filter)), 32, int(bool(knn_group)), int(knn_bucket))
+        cfg = OctSearchConfig(1, int(fp32_filter), 32, int(bool(knn_group)), int(knn_bucket))
         cfg.reserved[0], cfg.reserved[1], cfg.reserved[2] = radius_blocks_per_sm, knn_blocks_per_sm, int(serial)
         _check(self._L.oct_server_set_config(self._h, C.byref(cfg)), self._h, "oct_server_set_config")
 

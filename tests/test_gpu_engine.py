@@ -169,7 +169,12 @@ def test_graph_replay_direct_and_fp32_agree(torch, clouds):
     direct = engine_results(direct_eng, direct_eng.run(reqs), host)
     eng.set_config(fp32_filter=True, knn_bucket=0, radius_blocks_per_sm=4, knn_blocks_per_sm=8)
     fp32 = engine_results(eng, eng.run(reqs), host)
-    for other, name in ((replay, "replay"), (direct, "direct"), (fp32, "fp32/bucket0")):
+    runs = [(replay, "replay"), (direct, "direct"), (fp32, "fp32/bucket0")]
+    for sel in (capi.OCT_FP32_RADIUS, capi.OCT_FP32_KNN):  # one filter at a time
+        eng.set_config(fp32_filter=sel, knn_bucket=256)
+        assert eng.config()["fp32_filter"] == sel
+        runs.append((engine_results(eng, eng.run(reqs), host), f"fp32 selector {sel}"))
+    for other, name in runs:
         for i, (a, b) in enumerate(zip(base, other)):
             assert_same(a, b, f"{name}, request {i}")
 

@@ -33,11 +33,11 @@ def test_fp32_filter_identical(offset, k):
     _, _, sxyz = oc.sorted_points()
     c = centres(sxyz, 4)
     res = {}
-    for fp32 in (False, True):
+    for fp32 in (0, capi.OCT_FP32_ALL, capi.OCT_FP32_KNN, capi.OCT_FP32_RADIUS):
         for est in (0, -1):
             oc.set_search_config(packet=True, fp32_filter=fp32, knn_packet=True, knn_estimate=est)
             res[(fp32, est)] = oc.knn(c, k)
-    base = res[(False, 0)]
+    base = res[(0, 0)]
     for key, r in res.items():
         for a, b in zip(base, r):
             assert np.array_equal(a, b), key

@@ -18,11 +18,13 @@ GOLDEN = os.path.join(os.path.dirname(__file__), "golden")
 CLOUDS = sorted(p for p in glob.glob(os.path.join(GOLDEN, "*.npz")) if not p.endswith("keys_anchor.npz"))
 KERNELS = {"sphere": 1, "circle": 0, "cube": 3, "square": 2}
 ALGO_NAMES = {1: "neighbors", 2: "neighborsPrune", 3: "neighborsStruct"}
-# search paths: (packet, fp32_filter, lanes per query of the non-packet path)
+# search paths: (packet, fp32_filter, lanes per query of the non-packet path, kNN in groups, kNN bucket)
 PATHS = {"lanes8": (False, False, 8, False, 256), "lanes16": (False, False, 16, False, 256),
          "lanes32": (False, False, 32, False, 256), "packet": (True, False, 8, False, 256),
          "packet_fp32": (True, True, 8, False, 256), "knn_packet": (True, False, 8, True, 256),
          "knn_packet_fp32": (True, True, 8, True, 256),
+         # one FP32 filter at a time (2: the radius filter, 3: the kNN filter)
+         "packet_fp32_radius": (True, 2, 8, True, 256), "packet_fp32_knn": (True, 3, 8, True, 256),
          "knn_leaves": (True, False, 8, False, 0), "knn_bucket2k": (True, False, 8, False, 2048)}
 
 
@@ -213,7 +215,7 @@ def test_gpu_approx_matches_oracle(synth_cases, case, search):
 
 @pytest.mark.parametrize("case", range(len(SYNTH)))
 @pytest.mark.parametrize("search", ["lanes8", "packet", "knn_packet", "knn_packet_fp32", "knn_leaves",
-                                    "knn_bucket2k"])
+                                    "knn_bucket2k", "packet_fp32_radius", "packet_fp32_knn"])
 def test_gpu_knn_matches_oracle(synth_cases, case, search):
     xyz, enc, leaf, keys, perm, box, sxyz, t = synth_cases[case]
     oc = octree(xyz, enc, leaf, search)
