@@ -959,6 +959,7 @@ def run_b200(args, rank, world, local_rank):
         eng.close()
         gc.collect()
         torch.cuda.empty_cache()
+        L.oct_trim_cloud_memory(dev)  # what earlier sections' clouds left in the cloud pool goes back too
         line["large"] = _section("large", lambda: run_large(args, dev))
     if rank == 0:
         _emit(line)

@@ -401,6 +401,15 @@ int oct_engine_memory(oct_engine engine, uint64_t* bytes);
 /* Device bytes a cloud holds (points, keys, tree, search scratch). */
 int oct_cloud_memory(oct_cloud cloud, uint64_t* bytes);
 
+/* Health check of the bounded device waits.  Launches one kernel on `device`
+ * that waits for a device flag nothing sets, the way the library's cross-block
+ * waits wait (poll, back off, give up after spin_limit polls; 0 = the library's
+ * own limit, 2^26 polls, a few seconds), and reads its status back.  Returns
+ * OCT_ERR_DEVICE_LIMIT when the wait ran out, as it must, with *polls (may be
+ * NULL) the polls it made; the device stays usable.  OCT_OK would mean the
+ * flag was seen set. */
+int oct_device_wait_probe(int device, uint32_t spin_limit, uint32_t* polls);
+
 /* Clouds take their device arrays from one stream-ordered pool per device,
  * which keeps what destroyed clouds free for the next clouds (returning it to
  * the driver would make other threads' CUDA calls wait).  This returns the

@@ -158,6 +158,7 @@ SIGNATURES = {
     "oct_engine_memory": ([_vp, C.POINTER(_u64)], _int),
     "oct_cloud_memory": ([_vp, C.POINTER(_u64)], _int),
     "oct_trim_cloud_memory": ([_int], _int),
+    "oct_device_wait_probe": ([_int, C.c_uint32, C.POINTER(C.c_uint32)], _int),
     "oct_server_create": ([C.POINTER(OctServerParams), C.POINTER(_vp)], _int),
     "oct_server_destroy": ([_vp], _int),
     "oct_server_last_error": ([_vp, C.c_char_p, C.c_size_t], _int),

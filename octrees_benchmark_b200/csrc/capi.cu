@@ -303,6 +303,24 @@ void pinned_block_put(void* p) {
 
 const void* kernel_anchor_capi() { return reinterpret_cast<const void*>(&k_soa_to_aos); }
 
+// The bounded wait of oct_device_wait_probe: poll a flag nothing sets, back off,
+// give up after `limit` polls with the error bit set (lane 0 of one warp).
+__global__ void k_wait_probe(const uint32_t* flag, uint32_t limit, uint32_t* err, uint32_t* polls) {
+    if (threadIdx.x != 0) return;
+    uint32_t n = 0;
+    for (;;) {
+        uint32_t v;
+        asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(flag) : "memory");
+        if (v != 0) break;
+        if (++n >= limit) {
+            set_err(err, kErrSpinLimit);
+            break;
+        }
+        __nanosleep(64);
+    }
+    *polls = n;
+}
+
 // Every kernel of the library's device code loaded into the current device's
 // context: the device library of each source file is found from one of its
 // kernels, its kernels enumerated and each loaded (cuFuncLoad, CUDA 12.4+,
@@ -368,7 +386,7 @@ namespace {
 std::vector<DevBuf*> cloud_bufs(Cloud& c) {
     return {&c.xyz_in,   &c.xs,        &c.ys,          &c.zs,          &c.keys,       &c.keys_alt,
             &c.perm,     &c.perm_alt,  &c.keys_hi,     &c.keys_hi_alt, &c.run_pv,     &c.run_pv_alt,
-            &c.run_ctl,  &c.run_list,  &c.sort_status, &c.d_ctl,       &c.d_box,      &c.d_err,
+            &c.run_ctl,  &c.run_list,  &c.run_long,  &c.sort_status, &c.d_ctl,       &c.d_box,      &c.d_err,
             &c.offsets,  &c.ranges,    &c.centers,     &c.frontier,    &c.masks,      &c.parts,
             &c.d_build,  &c.q_centers, &c.q_radii,     &c.q_counts,    &c.q_offsets,  &c.q_out,
             &c.q_out2,   &c.q_scan_tmp, &c.qs_keys,    &c.qs_keys_alt, &c.qs_ord,     &c.qs_ord_alt,
@@ -547,6 +565,40 @@ int oct_cloud_memory(oct_cloud h, uint64_t* bytes) {
     return OCT_OK;
 }
 
+int oct_device_wait_probe(int device, uint32_t spin_limit, uint32_t* polls) {
+    int ndev = 0;
+    if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+        cudaGetLastError();
+        return OCT_ERR_NO_DEVICE;
+    }
+    if (device < 0 || device >= ndev) return OCT_ERR_INVALID_ARG;
+    DeviceGuard g(device);
+    const uint32_t limit = spin_limit ? spin_limit : kSpinLimit;
+    uint32_t* d = nullptr;  // flag, error word, polls
+    cudaStream_t s = nullptr;
+    uint32_t h[3] = {0, 0, 0};
+    cudaError_t e = cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaMallocAsync(reinterpret_cast<void**>(&d), 3 * sizeof(uint32_t), s);
+    if (e == cudaSuccess) e = cudaMemsetAsync(d, 0, 3 * sizeof(uint32_t), s);
+    if (e == cudaSuccess) {
+        k_wait_probe<<<1, 32, 0, s>>>(d, limit, d + 1, d + 2);
+        e = cudaGetLastError();
+    }
+    if (e == cudaSuccess) e = cudaMemcpyAsync(h, d, sizeof(h), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (d) cudaFreeAsync(d, s);
+    if (s) {
+        cudaStreamSynchronize(s);
+        cudaStreamDestroy(s);
+    }
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return OCT_ERR_CUDA;
+    }
+    if (polls) *polls = h[2];
+    return (h[1] & kErrSpinLimit) ? OCT_ERR_DEVICE_LIMIT : OCT_OK;
+}
+
 int oct_trim_cloud_memory(int device) {
     int ndev = 0;
     if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
@@ -604,7 +656,7 @@ int oct_encode_sort(oct_cloud h, double* box12, uint64_t* keys, uint32_t* perm, 
         memcpy(skip, c.pinned, sizeof(skip));
         return OCT_OK;
     };
-    // the split sort (upper halves, then runs); a run too long for it falls back to the 8-pass sort.
+    // the split sort (upper halves, then runs; runs longer than 4096 points in a stage of their own).
     // The split sort runs its four passes without reading the skip flags (a pass over a constant digit
     // keeps the order), so nothing waits for the host between the encode and the end of the sort.
     bool done = false;
@@ -617,18 +669,19 @@ int oct_encode_sort(oct_cloud h, double* box12, uint64_t* keys, uint32_t* perm, 
         CK(cudaMemcpyAsync(pin, c.d_box.ptr, sizeof(BoxD) + sizeof(LevelGeom), cudaMemcpyDeviceToHost, c.stream));
         const int st = sync_and_check(c);
         if (st != OCT_OK) return st;
-        uint32_t rc[8];  // RunCtl: w_count, w_next, b_count, b_next, big, cap, pad
+        uint32_t rc[8];  // RunCtl: w_count, w_next, b_count, b_next, big, cap, long-run points, long runs
         memcpy(rc, pin + 2048, sizeof(rc));
-        if (rc[4] == 0) {  // no run too long: the outputs are the sorted cloud
-            std::swap(c.keys, c.keys_alt);
-            if (psel == 1) std::swap(c.perm, c.perm_alt);
-            done = true;
+        if (rc[4] != 0) {  // runs longer than 4096 points: sorted by their lower halves in a stage of their own
+            CK(launch_sort_long(c, xyz, rc[7], rc[6]));
+            const int st2 = sync_and_check(c);
+            if (st2 != OCT_OK) return st2;
         }
+        // the outputs are the sorted cloud
+        std::swap(c.keys, c.keys_alt);
+        if (psel == 1) std::swap(c.perm, c.perm_alt);
+        done = true;
     }
     if (!done) {
-        // the split sort's encode counted the upper digits only, and its passes took tiles from their
-        // counters: count the lower digits and scan again (which rewinds the counters)
-        if (split) CK(launch_hist_low(c));
         if (c.n) {
             const int st = read_skips();
             if (st != OCT_OK) return st;

@@ -159,6 +159,8 @@ struct Cloud {
     DevBuf keys_hi, keys_hi_alt;  // u32 upper key halves (the split sort)
     DevBuf run_pv, run_pv_alt;    // u64 lower key half << 32 | input position (the split sort)
     DevBuf run_ctl, run_list;     // the split sort's run bookkeeping
+    DevBuf run_long;              // its runs longer than 4096 points (LongRun entries)
+    int split_sel = 0;            // which keys_hi / run_pv buffer holds the split sort's result
     int split_sort = 1;           // sort the upper halves, then the runs (0: the 8-pass sort)
     DevBuf sort_status;     // onesweep look-back words
     uint32_t sort_epoch = 0;
@@ -259,7 +261,7 @@ struct KernelClock {
 // upper_hist_only: the split sort follows (the lower digits' histograms are not needed)
 cudaError_t launch_bbox_encode(Cloud& c, const double* d_xyz_aos, bool upper_hist_only = false);
 cudaError_t launch_sort_split(Cloud& c, const uint32_t skip[8], const double* d_xyz_aos, int* out_sel);
-cudaError_t launch_hist_low(Cloud& c);  // the lower digits' histograms (before a split sort's fallback)
+cudaError_t launch_sort_long(Cloud& c, const double* d_xyz_aos, uint32_t l_count, uint32_t l_total);
 cudaError_t launch_sort_passes(Cloud& c, const uint32_t skip[8], int* final_sel);
 cudaError_t launch_gather(Cloud& c, const double* d_xyz_aos, const uint32_t* d_perm, int sel);
 cudaError_t launch_build(Cloud& c, bool* capacity_ok);

@@ -21,6 +21,7 @@
 //    skipped.  Values are generated on the fly in the first pass.
 //  * k_gather: reorders the coordinates into SoA float64 arrays.
 #include <cfloat>
+#include <cstddef>
 #include <mutex>
 
 #include "cloud.h"
@@ -189,7 +190,8 @@ __global__ void __launch_bounds__(kBboxThreads) k_bbox(const double* __restrict_
 }
 
 // LOW: the histograms of all 8 digits; otherwise of the upper 4 only (the split
-// sort; its fallback to the 8-pass sort counts the lower digits with k_hist_low).
+// sort, which sorts the lower halves only inside runs, and counts its long
+// runs' digits itself).
 template <int ENC, bool LOW = true>
 __global__ void __launch_bounds__(kEncThreads) k_encode(const double* __restrict__ xyz, uint64_t n,
                                                         const BoxGeom* __restrict__ bg, uint64_t* __restrict__ keys,
@@ -269,25 +271,6 @@ __global__ void __launch_bounds__(256) k_scan_hist(SortCtl* ctl, uint64_t n, con
             ctl->tile_ctr[p] = 0;
         }
         __syncthreads();
-    }
-}
-
-// Histograms of the 4 lower digits of the keys (the split sort's encode counts
-// the upper 4 only).
-__global__ void __launch_bounds__(256) k_hist_low(const uint64_t* __restrict__ keys, uint64_t n, SortCtl* ctl) {
-    __shared__ uint32_t hist[4 * 256];
-    for (int j = threadIdx.x; j < 4 * 256; j += blockDim.x) hist[j] = 0;
-    __syncthreads();
-    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
-    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
-        const uint64_t k = keys[i];
-#pragma unroll
-        for (int p = 0; p < 4; ++p) atomicAdd(&hist[p * 256 + (uint32_t)((k >> (8 * p)) & 255u)], 1u);
-    }
-    __syncthreads();
-    for (int j = threadIdx.x; j < 4 * 256; j += blockDim.x) {
-        const uint32_t v = hist[j];
-        if (v) atomicAdd(&ctl->hist[j >> 8][j & 255], v);
     }
 }
 
@@ -464,12 +447,13 @@ __global__ void __launch_bounds__(kSortThreads, kSortBlocksPerSM) k_onesweep(con
 // each run (equal upper halves: one cell at depth ~10.7) in input order; a
 // stable order of each run by its full keys then gives the stable order of the
 // whole 63-bit keys, which is the reference's (point_encoder.hpp:285-383).
-// Runs on this path are short (a 10M-point 1.5 km tile: a few points), so a
-// thread sorts one run of up to kRunSmall points by insertion, a block sorts a
-// run of up to kRunMid in shared memory (bitonic over (low half, position in
-// run): unique, so the order is stable), and a longer run sends the cloud to
-// the 8-pass sort.  The same kernels write the sorted keys, the permutation
-// and the reordered SoA coordinates.
+// Runs are mostly short (a 10M-point 1.5 km tile: a few points), so a thread
+// places each point of a run of up to kRunSmall points, a warp or a block sorts
+// a run of up to kRunMid in shared memory (bitonic over (low half, position in
+// run): unique, so the order is stable), and the runs longer than that (dense
+// clusters) are compacted and sorted by (run, lower half) with onesweep passes
+// of their own (launch_sort_long).  The same kernels write the sorted keys, the
+// permutation and the reordered SoA coordinates.
 // ---------------------------------------------------------------------------
 constexpr uint32_t kRunSmall = 32;
 constexpr uint32_t kRunWarp = 256;   // runs a warp sorts (kRunSmall < len <= kRunWarp)
@@ -484,7 +468,18 @@ struct RunCtl {
     uint32_t b_count, b_next;  // block runs listed, and k_runs_mid's work counter
     uint32_t big;              // a run longer than kRunMid was found
     uint32_t cap;              // entries of the run list
-    uint32_t pad[2];
+    // runs longer than kRunMid listed (high 32 bits) and their points (low 32 bits), taken
+    // together by one atomic, so a run's slot and its place among the compacted points
+    // follow the same order (slot r's points come after those of every slot below r)
+    unsigned long long l_packed;
+};
+static_assert(sizeof(RunCtl) == 32 && offsetof(RunCtl, l_packed) == 24, "the host reads RunCtl as 8 u32");
+
+// A run longer than kRunMid: its first point, length, and where its points sit
+// in the compacted arrays of all such runs (also where they sit once those are
+// sorted by (slot, lower half): the slots follow the same order).
+struct LongRun {
+    uint32_t start, len, off, pad;
 };
 
 // The sorted point at output position o: its key (upper half `h`, lower half
@@ -505,8 +500,9 @@ __device__ __forceinline__ void put_sorted(uint64_t o, uint32_t h, uint64_t pv, 
 // its place in the run by counting the run's points that precede it in the
 // stable order (a smaller lower key half, or an equal one earlier in the run)
 // and writes itself there; the first point of a longer run lists it for
-// k_runs_warp / k_runs_mid (start, length) or flags it when it is longer than
-// kRunMid.  hi: the sorted upper halves; pv: lower half << 32 | input position.
+// k_runs_warp / k_runs_mid (start, length), or, when it is longer than kRunMid,
+// lists it for the long-run stage (k_long_*).  hi: the sorted upper halves;
+// pv: lower half << 32 | input position.
 // A thread takes kRunsPer points (a grid stride apart) at a time: their places
 // first, then the coordinate gathers of all of them (random reads from the
 // input, the kernel's DRAM traffic), then the writes, so that each thread has
@@ -517,7 +513,8 @@ __global__ void __launch_bounds__(256) k_runs_small(const uint32_t* __restrict__
                                                     const double* __restrict__ xyz, uint64_t n,
                                                     uint64_t* __restrict__ keys_out, uint32_t* __restrict__ perm_out,
                                                     double* __restrict__ xs, double* __restrict__ ys,
-                                                    double* __restrict__ zs, RunCtl* rc, uint32_t* mid_list) {
+                                                    double* __restrict__ zs, RunCtl* rc, uint32_t* mid_list,
+                                                    LongRun* __restrict__ long_list) {
     const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
     for (uint64_t i0 = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i0 < n; i0 += kRunsPer * stride) {
         uint64_t dst[kRunsPer], val[kRunsPer];
@@ -539,7 +536,22 @@ __global__ void __launch_bounds__(256) k_runs_small(const uint32_t* __restrict__
                 if (s > 0 && hi[s - 1] == h) continue;
                 if (s != i) continue;
                 while (e < n && e - s <= kRunMid && hi[e] == h) ++e;
-                if (e - s > kRunMid) {
+                if (e - s > kRunMid) {  // its end by doubling steps, then bisection (hi is sorted)
+                    uint64_t a = e, b = e, step = 1;
+                    while (b < n && hi[b] == h) {
+                        a = b + 1;
+                        b += step;
+                        step <<= 1;
+                    }
+                    if (b > n) b = n;
+                    while (a < b) {
+                        const uint64_t mid = a + ((b - a) >> 1);
+                        if (hi[mid] == h) a = mid + 1;
+                        else b = mid;
+                    }
+                    e = a;
+                    const unsigned long long old = atomicAdd(&rc->l_packed, (1ull << 32) | (e - s));
+                    long_list[old >> 32] = LongRun{(uint32_t)s, (uint32_t)(e - s), (uint32_t)old, 0u};
                     atomicOr(&rc->big, 1u);
                 } else if (e - s <= kRunWarp) {
                     const uint32_t slot = atomicAdd(&rc->w_count, 1u);
@@ -684,6 +696,60 @@ __global__ void __launch_bounds__(kRunWarpThreads) k_runs_warp(const uint32_t* _
     }
 }
 
+// Long runs (more than kRunMid points with equal upper halves, e.g. a dense
+// cluster inside one cell): their points are compacted into one array keyed by
+// (run slot << 32 | lower half), sorted by the onesweep passes (stable: equal
+// keys keep the run's input order), and put in place.  One block per run.
+__global__ void __launch_bounds__(256) k_long_compact(const uint64_t* __restrict__ pv,
+                                                      const LongRun* __restrict__ runs, const RunCtl* rc,
+                                                      uint64_t* __restrict__ ckeys) {
+    const uint32_t count = (uint32_t)(rc->l_packed >> 32);
+    for (uint32_t r = blockIdx.x; r < count; r += gridDim.x) {
+        const LongRun lr = runs[r];
+        for (uint32_t t = threadIdx.x; t < lr.len; t += blockDim.x)
+            ckeys[lr.off + t] = ((uint64_t)r << 32) | (pv[lr.start + t] >> 32);
+    }
+}
+
+// Digit histograms of the compacted keys (all 8 digits; the slot digits that
+// are constant are skipped by the scan's flags).
+__global__ void __launch_bounds__(256) k_hist_all(const uint64_t* __restrict__ keys, const RunCtl* rc,
+                                                  SortCtl* ctl) {
+    __shared__ uint32_t hist[8 * 256];
+    for (int j = threadIdx.x; j < 8 * 256; j += blockDim.x) hist[j] = 0;
+    __syncthreads();
+    const uint64_t n = rc->l_packed & 0xffffffffull;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += stride) {
+        const uint64_t k = keys[i];
+#pragma unroll
+        for (int p = 0; p < 8; ++p) atomicAdd(&hist[p * 256 + (uint32_t)((k >> (8 * p)) & 255u)], 1u);
+    }
+    __syncthreads();
+    for (int j = threadIdx.x; j < 8 * 256; j += blockDim.x) {
+        const uint32_t v = hist[j];
+        if (v) atomicAdd(&ctl->hist[j >> 8][j & 255], v);
+    }
+}
+
+// The sorted compacted points into place: position c of the sorted array holds
+// the point that sat at compacted position c0 (its value) of run `slot`.
+__global__ void __launch_bounds__(256) k_long_put(const uint64_t* __restrict__ ckeys,
+                                                  const uint32_t* __restrict__ cvals,
+                                                  const LongRun* __restrict__ runs, const RunCtl* rc,
+                                                  const uint32_t* __restrict__ hi, const uint64_t* __restrict__ pv,
+                                                  const double* __restrict__ xyz, uint64_t* __restrict__ keys_out,
+                                                  uint32_t* __restrict__ perm_out, double* __restrict__ xs,
+                                                  double* __restrict__ ys, double* __restrict__ zs) {
+    const uint64_t n = rc->l_packed & 0xffffffffull;
+    const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+    for (uint64_t c = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; c < n; c += stride) {
+        const LongRun lr = runs[(uint32_t)(ckeys[c] >> 32)];
+        const uint64_t i = (uint64_t)lr.start + (cvals[c] - lr.off);  // where the point sat after the passes
+        put_sorted((uint64_t)lr.start + (c - lr.off), hi[i], pv[i], xyz, keys_out, perm_out, xs, ys, zs);
+    }
+}
+
 // The split sort's arrays in input order (no upper-digit pass ran): the upper
 // halves, and lower half << 32 | input position.
 __global__ void k_pack_iota(const uint64_t* __restrict__ keys, uint32_t* __restrict__ hi, uint64_t* __restrict__ pv,
@@ -768,18 +834,6 @@ cudaError_t launch_bbox_encode(Cloud& c, const double* d_xyz, bool upper_hist_on
     return cudaGetLastError();
 }
 
-cudaError_t launch_hist_low(Cloud& c) {
-    const uint64_t n = c.n;
-    if (n == 0) return cudaSuccess;
-    const int sms = sm_count(c.device);
-    const uint64_t want = (n + 255) / 256;
-    const int grid = (int)(want < (uint64_t)sms * 4 ? want : (uint64_t)sms * 4);
-    SortCtl* ctl = c.d_ctl.as<SortCtl>();
-    k_hist_low<<<grid, 256, 0, c.stream>>>(c.keys.as<uint64_t>(), n, ctl);
-    k_scan_hist<<<1, 256, 0, c.stream>>>(ctl, n);
-    return cudaGetLastError();
-}
-
 cudaError_t launch_sort_passes(Cloud& c, const uint32_t skip[8], int* final_sel) {
     cudaError_t e;
     const uint64_t n = c.n;
@@ -834,13 +888,12 @@ cudaError_t launch_sort_passes(Cloud& c, const uint32_t skip[8], int* final_sel)
     return cudaGetLastError();
 }
 
-// The split sort (upper halves, then runs): keys stay in input order in c.keys
-// (so the 8-pass sort can still run from them), the sorted keys go to
-// c.keys_alt, the permutation to c.perm, the sorted coordinates to xs / ys /
-// zs.  The passes carry each key's lower half with its input position (one
-// 64-bit value), so the runs read them in order instead of gathering keys.
-// RunCtl::big (d_run_ctl) says whether a run was too long, in which case
-// nothing of the outputs may be used.
+// The split sort (upper halves, then runs): the sorted keys go to c.keys_alt,
+// the permutation to c.perm, the sorted coordinates to xs / ys / zs.  The
+// passes carry each key's lower half with its input position (one 64-bit
+// value), so the runs read them in order instead of gathering keys.  When
+// RunCtl::big is set (d_run_ctl), runs longer than kRunMid were listed and
+// their points are not written yet: launch_sort_long places them.
 cudaError_t launch_sort_split(Cloud& c, const uint32_t skip[8], const double* d_xyz, int* out_sel) {
     cudaError_t e;
     const uint64_t n = c.n;
@@ -854,6 +907,7 @@ cudaError_t launch_sort_split(Cloud& c, const uint32_t skip[8], const double* d_
     if ((e = c.run_pv_alt.reserve(8 * nn)) != cudaSuccess) return e;
     if ((e = c.run_ctl.reserve(sizeof(RunCtl))) != cudaSuccess) return e;
     if ((e = c.run_list.reserve(8 * (n / (kRunSmall + 1) + 1))) != cudaSuccess) return e;
+    if ((e = c.run_long.reserve(sizeof(LongRun) * (n / (kRunMid + 1) + 1))) != cudaSuccess) return e;
     if ((e = c.xs.reserve(8 * nn)) != cudaSuccess) return e;
     if ((e = c.ys.reserve(8 * nn)) != cudaSuccess) return e;
     if ((e = c.zs.reserve(8 * nn)) != cudaSuccess) return e;
@@ -912,17 +966,88 @@ cudaError_t launch_sort_split(Cloud& c, const uint32_t skip[8], const double* d_
                                                  c.run_pv.as<uint64_t>(), n);
         sel = 0;
     }
+    c.split_sel = sel;  // the upper halves and payloads the runs read (and the long-run stage)
     const uint32_t* hi = kb[sel]->as<uint32_t>();
     const uint64_t* pv = vb[sel]->as<uint64_t>();
     uint32_t* perm_out = c.perm.as<uint32_t>();
     k_runs_small<<<grid, 256, 0, c.stream>>>(hi, pv, d_xyz, n, c.keys_alt.as<uint64_t>(), perm_out, c.xs.as<double>(),
-                                            c.ys.as<double>(), c.zs.as<double>(), rc, c.run_list.as<uint32_t>());
+                                            c.ys.as<double>(), c.zs.as<double>(), rc, c.run_list.as<uint32_t>(),
+                                            c.run_long.as<LongRun>());
     k_runs_warp<<<sms * 8, kRunWarpThreads, 0, c.stream>>>(hi, pv, d_xyz, c.keys_alt.as<uint64_t>(), perm_out,
                                                            c.xs.as<double>(), c.ys.as<double>(), c.zs.as<double>(),
                                                            rc, c.run_list.as<uint32_t>());
     k_runs_mid<<<sms, kRunMidThreads, 0, c.stream>>>(hi, pv, d_xyz, c.keys_alt.as<uint64_t>(), perm_out,
                                                      c.xs.as<double>(), c.ys.as<double>(), c.zs.as<double>(), rc,
                                                      c.run_list.as<uint32_t>());
+    return cudaGetLastError();
+}
+
+// The split sort's long runs (after launch_sort_split, when RunCtl::big is set;
+// l_count runs, l_total points, as RunCtl::l_packed holds them): compact their points
+// keyed by (run slot, lower key half), sort them with 4 + (slot bytes) onesweep
+// passes, put them in place.  The compacted keys use c.keys (the encode's keys,
+// not read again) and c.run_pv_alt, the values c.perm_alt and c.keys_hi_alt.
+cudaError_t launch_sort_long(Cloud& c, const double* d_xyz, uint32_t l_count, uint32_t l_total) {
+    cudaError_t e;
+    const uint64_t T = l_total;
+    if (l_count == 0 || T == 0) return cudaSuccess;
+    if ((e = c.keys.reserve(8 * T)) != cudaSuccess) return e;
+    if ((e = c.run_pv_alt.reserve(8 * T)) != cudaSuccess) return e;
+    if ((e = c.perm_alt.reserve(4 * T)) != cudaSuccess) return e;
+    if ((e = c.keys_hi_alt.reserve(4 * T)) != cudaSuccess) return e;
+    const uint64_t tiles = (T + kSortTile - 1) / kSortTile;
+    const size_t status_bytes = tiles * 256 * sizeof(unsigned long long);
+    if (status_bytes > c.sort_status.bytes) {
+        if ((e = c.sort_status.reserve(status_bytes)) != cudaSuccess) return e;
+        if ((e = cudaMemsetAsync(c.sort_status.ptr, 0, c.sort_status.bytes, c.stream)) != cudaSuccess) return e;
+        c.sort_epoch = 0;
+    }
+    const size_t smem = onesweep_smem();
+    if ((e = prepare_sort_dyn()) != cudaSuccess) return e;
+    const RunCtl* rc = c.run_ctl.as<RunCtl>();
+    const LongRun* runs = c.run_long.as<LongRun>();
+    DevBuf* hb[2] = {&c.keys_hi, &c.keys_hi_alt};
+    DevBuf* pb[2] = {&c.run_pv, &c.run_pv_alt};
+    const uint32_t* hi = hb[c.split_sel]->as<uint32_t>();
+    const uint64_t* pv = pb[c.split_sel]->as<uint64_t>();
+    if (c.split_sel != 0) return cudaErrorInvalidValue;  // the split sort always ends in its first buffers
+    SortCtl* ctl = c.d_ctl.as<SortCtl>();
+    if ((e = cudaMemsetAsync(ctl, 0, sizeof(SortCtl), c.stream)) != cudaSuccess) return e;
+    const int sms = sm_count(c.device);
+    DevBuf* kb[2] = {&c.keys, &c.run_pv_alt};
+    DevBuf* vb[2] = {&c.perm_alt, &c.keys_hi_alt};
+    k_long_compact<<<(unsigned)(l_count < (uint32_t)sms * 8 ? l_count : (uint32_t)sms * 8), 256, 0, c.stream>>>(
+        pv, runs, rc, kb[0]->as<uint64_t>());
+    const uint64_t want = (T + 255) / 256;
+    const int grid = (int)(want < (uint64_t)sms * 4 ? want : (uint64_t)sms * 4);
+    k_hist_all<<<grid, 256, 0, c.stream>>>(kb[0]->as<uint64_t>(), rc, ctl);
+    k_scan_hist<<<1, 256, 0, c.stream>>>(ctl, T);
+    int slot_bytes = 0;
+    for (uint32_t v = l_count - 1; v; v >>= 8) ++slot_bytes;
+    int sel = 0;
+    for (int p = 0; p < 4 + slot_bytes; ++p) {
+        c.sort_epoch = (c.sort_epoch + 1) & ((1u << 22) - 1);
+        if (c.sort_epoch == 0) {
+            if ((e = cudaMemsetAsync(c.sort_status.ptr, 0, c.sort_status.bytes, c.stream)) != cudaSuccess) return e;
+            c.sort_epoch = 1;
+        }
+        const uint64_t* kin = kb[sel]->as<uint64_t>();
+        uint64_t* kout = kb[sel ^ 1]->as<uint64_t>();
+        const uint32_t* vin = vb[sel]->as<uint32_t>();
+        uint32_t* vout = vb[sel ^ 1]->as<uint32_t>();
+        if (p == 0)
+            k_onesweep<true, uint64_t, uint32_t><<<(unsigned)tiles, kSortThreads, smem, c.stream>>>(
+                kin, nullptr, kout, vout, T, p, ctl, c.sort_status.as<unsigned long long>(), c.sort_epoch,
+                c.d_err.as<uint32_t>());
+        else
+            k_onesweep<false, uint64_t, uint32_t><<<(unsigned)tiles, kSortThreads, smem, c.stream>>>(
+                kin, vin, kout, vout, T, p, ctl, c.sort_status.as<unsigned long long>(), c.sort_epoch,
+                c.d_err.as<uint32_t>());
+        sel ^= 1;
+    }
+    k_long_put<<<grid, 256, 0, c.stream>>>(kb[sel]->as<uint64_t>(), vb[sel]->as<uint32_t>(), runs, rc, hi, pv, d_xyz,
+                                           c.keys_alt.as<uint64_t>(), c.perm.as<uint32_t>(), c.xs.as<double>(),
+                                           c.ys.as<double>(), c.zs.as<double>());
     return cudaGetLastError();
 }
 

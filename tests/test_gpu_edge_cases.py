@@ -186,3 +186,40 @@ def test_error_statuses(port):
     buf = C.create_string_buffer(256)
     assert L.oct_last_error(h, buf, 256) == capi.OCT_OK and b"capacity" in buf.value
     assert L.oct_cloud_destroy(h) == capi.OCT_OK
+
+
+def test_cloud_pool_trim_between_clouds(port):
+    """Clouds reuse the memory destroyed clouds left in the per-device pool; returning it to the
+    driver (oct_trim_cloud_memory) between clouds changes no result, and a bad device is refused."""
+    from octrees_benchmark_b200.synth import lidar_tile
+
+    L = capi.lib()
+    xyz = lidar_tile(40_000, 80.0, 61)
+    first = LinearOctree(xyz, encoder="hilbert", max_points_leaf=32)
+    want = first.knn(xyz[:300], 8)
+    first.close()
+    assert L.oct_trim_cloud_memory(0) == capi.OCT_OK
+    assert L.oct_trim_cloud_memory(-1) == capi.OCT_ERR_INVALID_ARG
+    again = LinearOctree(xyz, encoder="hilbert", max_points_leaf=32)
+    got = again.knn(xyz[:300], 8)
+    for a, b in zip(want, got):
+        assert np.array_equal(a, b)
+    again.close()
+
+
+def test_bounded_device_wait_runs_out_and_reports(port):
+    """A device wait on a flag nothing sets gives up after its poll limit and the host reads
+    OCT_ERR_DEVICE_LIMIT from the device's error word (no trap, no hang); the device stays usable."""
+    from octrees_benchmark_b200.synth import lidar_tile
+
+    L = capi.lib()
+    polls = C.c_uint32()
+    assert L.oct_device_wait_probe(0, 200_000, C.byref(polls)) == capi.OCT_ERR_DEVICE_LIMIT
+    assert polls.value == 200_000
+    assert L.oct_device_wait_probe(-1, 10, None) == capi.OCT_ERR_INVALID_ARG
+    xyz = lidar_tile(20_000, 60.0, 62)  # the context still runs kernels
+    keys, perm, box, sxyz = port.encode_sort(5, xyz)
+    oc = LinearOctree(xyz, encoder="hilbert", max_points_leaf=32)
+    gk, gp, gx = oc.sorted_points()
+    assert np.array_equal(gk, keys)
+    oc.close()

@@ -3,8 +3,9 @@ equal upper halves by their full keys) against the oracle's stable sort and
 against the cloud's 8-pass sort (OCT_CLOUD_SORT_8PASS): keys, permutation,
 sorted points and the tree arrays bitwise.  The clouds exercise every run
 path: short runs (the synthetic tile), runs of 33..4096 points (dense
-clusters, sorted in shared memory), and a run above 4096 points (a cluster
-of 6000 points in one cell), which sends the cloud to the 8-pass sort."""
+clusters, sorted in shared memory), and runs above 4096 points (clusters of
+thousands of points in one cell: one such run, and 300 of them, which takes
+two bytes of run slot in the long-run stage's keys)."""
 import numpy as np
 import pytest
 
@@ -31,6 +32,7 @@ CASES = {
     "tile": clustered(300_000, [], 1),
     "mid_runs": clustered(200_000, [(40, 1e-7), (300, 1e-7), (1500, 1e-8), (4000, 1e-9), (700, 0.0)], 2),
     "long_run": clustered(100_000, [(6000, 1e-9), (200, 1e-7)], 3),
+    "many_long_runs": clustered(60_000, [(4100 + 7 * j, 1e-9 if j % 3 else 0.0) for j in range(300)], 4),
 }
 
 
