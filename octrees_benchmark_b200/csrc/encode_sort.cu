@@ -458,7 +458,7 @@ __global__ void __launch_bounds__(kSortThreads, kSortBlocksPerSM) k_onesweep(con
 constexpr uint32_t kRunSmall = 32;
 constexpr uint32_t kRunWarp = 256;   // runs a warp sorts (kRunSmall < len <= kRunWarp)
 constexpr uint32_t kRunMid = 4096;   // runs a block sorts (kRunWarp < len <= kRunMid)
-constexpr int kRunMidThreads = 1024;
+constexpr int kRunMidThreads = 512;  // 4 blocks (32 KB of shared memory each) per SM
 constexpr int kRunWarpThreads = 256;
 
 // Runs for k_runs_warp are listed from the front of the run list, runs for
@@ -530,26 +530,32 @@ __global__ void __launch_bounds__(256) k_runs_small(const uint32_t* __restrict__
             if (i >= n) continue;
             const uint32_t h = hi[i];
             uint64_t s = i, e = i + 1;
-            while (s > 0 && i - s <= kRunSmall && hi[s - 1] == h) --s;
-            while (e < n && e - s <= kRunSmall && hi[e] == h) ++e;
-            if (e - s > kRunSmall) {  // a longer run: its first point (if this is it) measures and lists it
-                if (s > 0 && hi[s - 1] == h) continue;
-                if (s != i) continue;
-                while (e < n && e - s <= kRunMid && hi[e] == h) ++e;
-                if (e - s > kRunMid) {  // its end by doubling steps, then bisection (hi is sorted)
-                    uint64_t a = e, b = e, step = 1;
-                    while (b < n && hi[b] == h) {
-                        a = b + 1;
-                        b += step;
-                        step <<= 1;
-                    }
-                    if (b > n) b = n;
-                    while (a < b) {
-                        const uint64_t mid = a + ((b - a) >> 1);
-                        if (hi[mid] == h) a = mid + 1;
-                        else b = mid;
-                    }
-                    e = a;
+            if (i > 0 && hi[i - 1] == h) {
+                // inside a run: a run of more than kRunSmall points is its first point's business, and
+                // two probes kRunSmall away tell (a point deep in a long run reads 3 words, not 2 x 33)
+                if (i >= kRunSmall && hi[i - kRunSmall] == h) continue;
+                if (i + kRunSmall < n && hi[i + kRunSmall] == h) continue;
+                --s;
+                while (s > 0 && hi[s - 1] == h) --s;  // the run lies within (i - kRunSmall, i + kRunSmall)
+                while (e < n && hi[e] == h) ++e;
+                if (e - s > kRunSmall) continue;
+            } else if (i + kRunSmall < n && hi[i + kRunSmall] == h) {
+                // the first point of a run of more than kRunSmall points: its end by doubling steps,
+                // then bisection (hi is sorted), and the run listed by its length
+                uint64_t a = i + kRunSmall + 1, b = a, step = 1;
+                while (b < n && hi[b] == h) {
+                    a = b + 1;
+                    b += step;
+                    step <<= 1;
+                }
+                if (b > n) b = n;
+                while (a < b) {
+                    const uint64_t mid = a + ((b - a) >> 1);
+                    if (hi[mid] == h) a = mid + 1;
+                    else b = mid;
+                }
+                e = a;
+                if (e - s > kRunMid) {
                     const unsigned long long old = atomicAdd(&rc->l_packed, (1ull << 32) | (e - s));
                     long_list[old >> 32] = LongRun{(uint32_t)s, (uint32_t)(e - s), (uint32_t)old, 0u};
                     atomicOr(&rc->big, 1u);
@@ -563,6 +569,8 @@ __global__ void __launch_bounds__(256) k_runs_small(const uint32_t* __restrict__
                     mid_list[2 * slot + 1] = (uint32_t)(e - s);
                 }
                 continue;
+            } else {
+                while (e < n && hi[e] == h) ++e;  // at most kRunSmall points
             }
             const uint64_t mine = pv[i];
             const uint32_t lo = (uint32_t)(mine >> 32);
@@ -976,7 +984,7 @@ cudaError_t launch_sort_split(Cloud& c, const uint32_t skip[8], const double* d_
     k_runs_warp<<<sms * 8, kRunWarpThreads, 0, c.stream>>>(hi, pv, d_xyz, c.keys_alt.as<uint64_t>(), perm_out,
                                                            c.xs.as<double>(), c.ys.as<double>(), c.zs.as<double>(),
                                                            rc, c.run_list.as<uint32_t>());
-    k_runs_mid<<<sms, kRunMidThreads, 0, c.stream>>>(hi, pv, d_xyz, c.keys_alt.as<uint64_t>(), perm_out,
+    k_runs_mid<<<sms * 4, kRunMidThreads, 0, c.stream>>>(hi, pv, d_xyz, c.keys_alt.as<uint64_t>(), perm_out,
                                                      c.xs.as<double>(), c.ys.as<double>(), c.zs.as<double>(), rc,
                                                      c.run_list.as<uint32_t>());
     return cudaGetLastError();
