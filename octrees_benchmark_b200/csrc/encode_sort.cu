@@ -634,14 +634,12 @@ __global__ void __launch_bounds__(kRunMidThreads) k_runs_mid(const uint32_t* __r
         __syncthreads();
         for (uint32_t k = 2; k <= P; k <<= 1) {
             for (uint32_t j = k >> 1; j > 0; j >>= 1) {
-                for (uint32_t t = tid; t < P; t += kRunMidThreads) {
-                    const uint32_t o = t ^ j;
-                    if (o > t) {
-                        const unsigned long long a = s[t], b = s[o];
-                        if ((a > b) == ((t & k) == 0)) {
-                            s[t] = b;
-                            s[o] = a;
-                        }
+                for (uint32_t i = tid; i < P / 2; i += kRunMidThreads) {  // pair i: t and t + j
+                    const uint32_t t = ((i & ~(j - 1)) << 1) | (i & (j - 1)), o = t + j;
+                    const unsigned long long a = s[t], b = s[o];
+                    if ((a > b) == ((t & k) == 0)) {
+                        s[t] = b;
+                        s[o] = a;
                     }
                 }
                 __syncthreads();
@@ -682,14 +680,12 @@ __global__ void __launch_bounds__(kRunWarpThreads) k_runs_warp(const uint32_t* _
         __syncwarp();
         for (uint32_t k = 2; k <= P; k <<= 1) {
             for (uint32_t j = k >> 1; j > 0; j >>= 1) {
-                for (uint32_t t = lane; t < P; t += 32) {
-                    const uint32_t o = t ^ j;
-                    if (o > t) {
-                        const unsigned long long a = s[t], b = s[o];
-                        if ((a > b) == ((t & k) == 0)) {
-                            s[t] = b;
-                            s[o] = a;
-                        }
+                for (uint32_t i = lane; i < P / 2; i += 32) {  // pair i: its lower element t, and t + j
+                    const uint32_t t = ((i & ~(j - 1)) << 1) | (i & (j - 1)), o = t + j;
+                    const unsigned long long a = s[t], b = s[o];
+                    if ((a > b) == ((t & k) == 0)) {
+                        s[t] = b;
+                        s[o] = a;
                     }
                 }
                 __syncwarp();
