@@ -254,6 +254,17 @@ int oct_radius_search(oct_cloud cloud, int kernel, int algo, const double* cente
 int oct_radius_count(oct_cloud cloud, int kernel, int algo, const double* centers, uint64_t nq, const double* radii,
                      double radius, uint64_t* counts, uint32_t flags);
 
+/* Neighbour counts and an order-independent hash of each neighbour set, per
+ * query, without the neighbour lists (for sweeps whose lists would not fit
+ * anywhere, e.g. every point of a large cloud as a centre, and for checking
+ * sets against another implementation): hashes[q] = sum over the neighbours i
+ * of splitmix64's output function of i, modulo 2^64 (z = i + 0x9E3779B97F4A7C15;
+ * z = (z ^ z >> 30) * 0xBF58476D1CE4E5B9; z = (z ^ z >> 27) * 0x94D049BB133111EB;
+ * z ^ z >> 31).  Sets as oct_radius_search (OCT_NEIGHBORS_STRUCT: the expanded
+ * ranges).  counts and hashes: nq entries each. */
+int oct_radius_hash(oct_cloud cloud, int kernel, int algo, const double* centers, uint64_t nq, const double* radii,
+                    double radius, uint64_t* counts, uint64_t* hashes, uint32_t flags);
+
 /* neighborsStruct ranges (linear_octree.hpp:1038-1042, NeighborSet
  * neighbor_set.hpp:16-90): CSR over half-open ranges, range_offsets (nq + 1)
  * and pairs (first, last) in ascending order, exactly the ranges the reference

@@ -146,9 +146,8 @@ cudaError_t radius_pass(Cloud& c, int kernel, int algo, bool fill, const double*
 // to its chain of result chunks, the counts are scanned, and the chains are
 // compacted into the CSR output.  A pool that turned out too small leaves the
 // counts exact: it is sized from the total and the traversal runs once more.
-int radius_one_pass(Cloud& c, int kernel, int algo, const double* dq, uint64_t nq, const double* dr, double radius,
-                    unsigned long long* doffs, uint64_t* offsets, uint32_t* idx, uint64_t idx_capacity,
-                    uint64_t* total, bool dev) {
+int radius_chunks(Cloud& c, int kernel, int algo, const double* dq, uint64_t nq, const double* dr, double radius,
+                  unsigned long long* doffs, uint64_t* total) {
     const int pass_algo = (algo == OCT_NEIGHBORS_STRUCT) ? OCT_NEIGHBORS_PRUNE : algo;  // same index set
     unsigned long long* dc = c.q_counts.as<unsigned long long>();
     CK(c.stats.reserve(64));
@@ -186,6 +185,18 @@ int radius_one_pass(Cloud& c, int kernel, int algo, const double* dq, uint64_t n
         if (!pool_short) break;
         if (attempt == 1) return set_error(c, OCT_ERR_DEVICE_LIMIT, "result chunk pool still too small");
     }
+    *total = tot;
+    return OCT_OK;
+}
+
+// One pass into result chunks (radius_chunks), then the chains compacted into the CSR output.
+int radius_one_pass(Cloud& c, int kernel, int algo, const double* dq, uint64_t nq, const double* dr, double radius,
+                    unsigned long long* doffs, uint64_t* offsets, uint32_t* idx, uint64_t idx_capacity,
+                    uint64_t* total, bool dev) {
+    uint64_t tot = 0;
+    const int st0 = radius_chunks(c, kernel, algo, dq, nq, dr, radius, doffs, &tot);
+    if (st0 != OCT_OK) return st0;
+    unsigned long long* dc = c.q_counts.as<unsigned long long>();
     if (total) *total = tot;
     if (!dev && offsets) CK(cudaMemcpyAsync(offsets, doffs, 8 * (nq + 1), cudaMemcpyDeviceToHost, c.stream));
     if (tot > idx_capacity || (tot && !idx)) {
@@ -978,6 +989,41 @@ int oct_radius_count(oct_cloud h, int kernel, int algo, const double* centers, u
     if (!dev && counts && nq) CK(cudaMemcpyAsync(counts, dc, 8 * nq, cudaMemcpyDeviceToHost, c.stream));
     if (!dev) return sync_and_check(c);
     return OCT_OK;
+}
+
+int oct_radius_hash(oct_cloud h, int kernel, int algo, const double* centers, uint64_t nq, const double* radii,
+                    double radius, uint64_t* counts, uint64_t* hashes, uint32_t flags) {
+    if (!h) return OCT_ERR_INVALID_ARG;
+    Cloud& c = h->c;
+    DeviceGuard g(c.device);
+    const bool dev = flags & OCT_MEM_DEVICE;
+    if (nq && (!counts || !hashes)) return set_error(c, OCT_ERR_INVALID_ARG, "counts or hashes is NULL");
+    const double *dq, *dr;
+    int st = radius_common(c, kernel, algo, centers, nq, radii, radius, dev, &dq, &dr);
+    if (st != OCT_OK || nq == 0) return st;
+    // the one-pass search into result chunks (whatever the cloud's search configuration: the sets are the same),
+    // then per query the sum over its chain instead of the CSR lists
+    CK(c.q_counts.reserve(8 * nq));
+    CK(c.q_offsets.reserve(8 * (nq + 1)));
+    uint64_t tot = 0;
+    if ((st = radius_chunks(c, kernel, algo, dq, nq, dr, radius, c.q_offsets.as<unsigned long long>(), &tot)) != OCT_OK)
+        return st;
+    unsigned long long* dh = reinterpret_cast<unsigned long long*>(hashes);
+    if (!dev) {
+        CK(c.q_out2.reserve(8 * nq));
+        dh = c.q_out2.as<unsigned long long>();
+    }
+    ChunkArgs ck{c.ck_pool.as<uint32_t>(), c.ck_next.as<uint32_t>(), c.ck_first.as<uint32_t>(),
+                 c.ck_ctr.as<uint32_t>(), c.ck_cap};
+    const unsigned long long* dc = c.q_counts.as<unsigned long long>();
+    CK(launch_chunk_hash(c.device, c.stream, dc, ck, dh, nq, c.d_err.as<uint32_t>()));
+    if (dev) {
+        CK(cudaMemcpyAsync(counts, dc, 8 * nq, cudaMemcpyDeviceToDevice, c.stream));
+        return OCT_OK;
+    }
+    CK(cudaMemcpyAsync(counts, dc, 8 * nq, cudaMemcpyDeviceToHost, c.stream));
+    CK(cudaMemcpyAsync(hashes, dh, 8 * nq, cudaMemcpyDeviceToHost, c.stream));
+    return sync_and_check(c);
 }
 
 int oct_radius_search(oct_cloud h, int kernel, int algo, const double* centers, uint64_t nq, const double* radii,

@@ -305,6 +305,9 @@ cudaError_t launch_radius_table(int device, cudaStream_t s, int kernel, int algo
                                 uint32_t* d_packet_ctr, unsigned long long* d_stats, uint32_t* d_err,
                                 int blocks_per_sm = 0, const ChunkArgs* chunks = nullptr);
 // Chains of result chunks into CSR (after the counts are scanned into d_offsets).
+// Per query, the sum of splitmix64's output function over its result chain.
+cudaError_t launch_chunk_hash(int device, cudaStream_t s, const unsigned long long* d_counts, const ChunkArgs& chunks,
+                              unsigned long long* d_hashes, uint64_t n, uint32_t* d_err);
 cudaError_t launch_chunk_compact(int device, cudaStream_t s, const unsigned long long* d_counts,
                                  const unsigned long long* d_offsets, const ChunkArgs& chunks, uint32_t* d_out,
                                  uint64_t out_capacity, uint64_t n, const uint64_t* d_n, uint32_t* d_err);

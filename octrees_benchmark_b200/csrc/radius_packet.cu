@@ -862,6 +862,46 @@ __global__ void __launch_bounds__(256) k_chunk_compact(const unsigned long long*
     }
 }
 
+// splitmix64's output function (the set hash's term for one neighbour index).
+__device__ __forceinline__ unsigned long long mix64(unsigned long long z) {
+    z += 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
+// One warp per query: the sum of mix64 over the query's result chain (the
+// count is the search's), instead of moving the chain into a CSR array.
+__global__ void __launch_bounds__(256) k_chunk_hash(const unsigned long long* __restrict__ counts,
+                                                    const uint32_t* __restrict__ first,
+                                                    const uint32_t* __restrict__ next,
+                                                    const uint32_t* __restrict__ pool, uint64_t chunk_cap,
+                                                    unsigned long long* __restrict__ hashes, uint64_t n,
+                                                    uint32_t* err) {
+    const int lane = threadIdx.x & 31;
+    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t q = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; q < n; q += nwarps) {
+        const unsigned long long cnt = counts[q];
+        unsigned long long h = 0;
+        uint32_t c = first[q];
+        bool bad = false;
+        for (unsigned long long done = 0; done < cnt;) {
+            if (c >= chunk_cap) {  // a chain cut short by a pool overflow (reported by the search kernel)
+                bad = true;
+                break;
+            }
+            const unsigned long long m = (cnt - done < kChunk) ? (cnt - done) : kChunk;
+            for (uint32_t t = lane; t < m; t += 32) h += mix64(pool[(uint64_t)c * kChunk + t]);
+            done += m;
+            if (done < cnt) c = next[c];
+        }
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) h += __shfl_xor_sync(0xffffffffu, h, off);
+        if (lane == 0) hashes[q] = h;
+        if (bad && lane == 0) set_err(err, kErrOutputCapacity);
+    }
+}
+
 }  // namespace
 
 // FP32 (x, y, z) of every point relative to the box centre, each rounded once
@@ -952,6 +992,17 @@ cudaError_t launch_radius_table(int device, cudaStream_t s, int kernel, int algo
         case kCube: return launch_pk_a<kCube>(a, algo, mode, fp32, grid, s);
         default: return launch_pk_a<kSphere>(a, algo, mode, fp32, grid, s);
     }
+}
+
+cudaError_t launch_chunk_hash(int device, cudaStream_t s, const unsigned long long* d_counts, const ChunkArgs& chunks,
+                              unsigned long long* d_hashes, uint64_t n, uint32_t* d_err) {
+    if (n == 0) return cudaSuccess;
+    const uint64_t cap = (uint64_t)sm_count_p(device) * 8;
+    const uint64_t want = (n + 7) / 8;
+    const int grid = (int)(want < cap ? want : cap);
+    k_chunk_hash<<<grid, 256, 0, s>>>(d_counts, chunks.first, chunks.next, chunks.pool, chunks.cap, d_hashes, n,
+                                      d_err);
+    return cudaGetLastError();
 }
 
 cudaError_t launch_chunk_compact(int device, cudaStream_t s, const unsigned long long* d_counts,

@@ -346,6 +346,34 @@ class LinearOctree:
                                  cnt.ctypes.data, 0), h, "oct_radius_count")
         return cnt
 
+    def radius_hash(self, centers, radius, kernel="square", algo="neighborsPrune"):
+        """(counts uint64[nq], hashes uint64[nq]): each neighbour set's size and the sum of splitmix64's
+        output function over its indices (mod 2^64), without the lists.  ``centers`` may be a CUDA tensor
+        (then the outputs are CUDA tensors too)."""
+        L, h = self._L, self._h
+        if hasattr(centers, "is_cuda") and centers.is_cuda:
+            import torch
+
+            nq = int(centers.shape[0])
+            assert centers.dtype == torch.float64 and centers.is_contiguous()
+            radii, r0 = (None, float(radius)) if np.isscalar(radius) else (radius, 0.0)
+            cnt = torch.empty(nq, dtype=torch.int64, device=centers.device)
+            hsh = torch.empty(nq, dtype=torch.int64, device=centers.device)
+            _sync_current_stream()  # the cloud reads the tensors on its own stream
+            check(L.oct_radius_hash(h, KERNELS[kernel], ALGOS[algo], centers.data_ptr(), nq,
+                                    radii.data_ptr() if radii is not None else None, r0, cnt.data_ptr(),
+                                    hsh.data_ptr(), capi.OCT_MEM_DEVICE), h, "oct_radius_hash")
+            check(L.oct_synchronize(h), h, "oct_synchronize")  # the outputs are written on that stream
+            return cnt, hsh
+        centers = _host_f64(centers, 3)
+        nq = centers.shape[0]
+        radii, r0 = self._radii(centers, radius)
+        cnt = np.zeros(nq, np.uint64)
+        hsh = np.zeros(nq, np.uint64)
+        check(L.oct_radius_hash(h, KERNELS[kernel], ALGOS[algo], centers.ctypes.data, nq, _ptr(radii), r0,
+                                cnt.ctypes.data, hsh.ctypes.data, 0), h, "oct_radius_hash")
+        return cnt, hsh
+
     def knn(self, centers, k: int):
         """(idx uint32[nq, k], d2 float64[nq, k], counts uint32[nq])."""
         L, h = self._L, self._h

@@ -158,7 +158,8 @@ def test_c2_all_kernels_variants_full_sets(c2, radius):
 @pytest.mark.parametrize("kernel,radius", [("sphere", 2.5), ("sphere", 1.0), ("circle", 1.0), ("square", 1.0),
                                            ("cube", 1.0)])
 def test_c2_every_point_count_and_hash(torch, c2, kernel, radius):
-    """neighborsPrune with every point of the sorted cloud as a centre, in order."""
+    """neighborsPrune with every point of the sorted cloud as a centre, in order, through the
+    count-and-hash mode (oct_radius_hash); the first million also as lists, hashed here."""
     oc, R, sxyz = c2
     set_path(oc, "packet")
     kv = KERNELS[kernel]
@@ -167,13 +168,17 @@ def test_c2_every_point_count_and_hash(torch, c2, kernel, radius):
     bad = 0
     for s in range(0, len(sxyz), chunk):
         qd = torch.from_numpy(np.ascontiguousarray(sxyz[s:s + chunk])).cuda()
-        offs, idx = device_radius(torch, oc, qd, kv, 2, radius)
-        gc, gh = csr_count_hash_torch(offs, idx)
-        gc = gc.cpu().numpy()
+        if s == 0:  # the lists, counted and hashed here, on the first chunk
+            offs, idx = device_radius(torch, oc, qd, kv, 2, radius)
+            lc, lh = csr_count_hash_torch(offs, idx)
+            del offs, idx
+        gc, gh = oc.radius_hash(qd, radius, kernel, "neighborsPrune")  # counts and hashes on the device
+        if s == 0:
+            assert torch.equal(gc, lc.to(gc.dtype)) and torch.equal(gh, lh.to(gh.dtype))
+        gc = gc.cpu().numpy().view(np.uint64)
         gh = gh.cpu().numpy().view(np.uint64)
         m = len(gc)
-        bad += int(((gc.astype(np.uint64) != rc[s:s + m]) | (gh != rh[s:s + m])).sum())
-        del offs, idx
+        bad += int(((gc != rc[s:s + m]) | (gh != rh[s:s + m])).sum())
     assert bad == 0, f"{bad} of {len(sxyz)} queries differ"
     assert rc.sum() > len(sxyz)
 
