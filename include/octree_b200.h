@@ -392,6 +392,12 @@ int oct_engine_run(oct_engine engine, const oct_request* requests, uint32_t n, o
 /* Device pointers of the output arrays of the last completed batch (valid until the next submit). */
 int oct_engine_outputs(oct_engine engine, uint64_t** offsets, uint32_t** indices, uint32_t** knn_idx,
                        double** knn_d2, uint32_t** knn_counts);
+/* A radius request's per-centre neighbour counts and set hashes (as
+ * oct_radius_hash), computed on the device from the batch's results: 16 bytes
+ * per centre cross to the host instead of the lists.  counts and hashes: nq
+ * entries each (host buffers, or device buffers with OCT_MEM_DEVICE). */
+int oct_engine_copy_radius_hash(oct_engine engine, const oct_request_place* place, uint64_t* counts,
+                                uint64_t* hashes, uint32_t flags);
 /* Copy one request's results out (host memory unless flags has OCT_MEM_DEVICE).
  * Radius: offsets (nq + 1, rebased to 0) and idx (up to idx_capacity).  kNN:
  * idx, d2 (nq x k) and counts (nq); any may be NULL. */

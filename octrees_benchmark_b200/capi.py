@@ -159,6 +159,7 @@ SIGNATURES = {
     "oct_cloud_memory": ([_vp, C.POINTER(_u64)], _int),
     "oct_trim_cloud_memory": ([_int], _int),
     "oct_radius_hash": ([_vp, _int, _int, _vp, _u64, _vp, _dbl, _vp, _vp, _u32], _int),
+    "oct_engine_copy_radius_hash": ([_vp, _vp, _vp, _vp, _u32], _int),
     "oct_device_wait_probe": ([_int, C.c_uint32, C.POINTER(C.c_uint32)], _int),
     "oct_server_create": ([C.POINTER(OctServerParams), C.POINTER(_vp)], _int),
     "oct_server_destroy": ([_vp], _int),

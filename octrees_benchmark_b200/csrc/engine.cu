@@ -207,6 +207,27 @@ __global__ void k_req_totals(const EngineDyn* __restrict__ dyn, const SearchReq*
     }
 }
 
+// One warp per centre of a radius request: its neighbour count and the sum of
+// mix64 over its neighbours (the CSR offsets are the batch's, not rebased).
+__global__ void __launch_bounds__(256) k_csr_hash(const unsigned long long* __restrict__ offs,
+                                                  const uint32_t* __restrict__ out, uint64_t nq,
+                                                  unsigned long long* __restrict__ counts,
+                                                  unsigned long long* __restrict__ hashes) {
+    const int lane = threadIdx.x & 31;
+    const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    for (uint64_t q = ((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5; q < nq; q += nwarps) {
+        const unsigned long long b = offs[q], e = offs[q + 1];
+        unsigned long long h = 0;
+        for (unsigned long long j = b + lane; j < e; j += 32) h += mix64(out[j]);
+#pragma unroll
+        for (int off = 16; off > 0; off >>= 1) h += __shfl_xor_sync(0xffffffffu, h, off);
+        if (lane == 0) {
+            counts[q] = e - b;
+            hashes[q] = h;
+        }
+    }
+}
+
 __global__ void k_rebase(const unsigned long long* __restrict__ in, uint64_t n, unsigned long long* __restrict__ out) {
     const uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i < n) out[i] = in[i] - in[0];
@@ -261,6 +282,7 @@ struct oct_engine_s {
     DevBuf ck_pool, ck_next, ck_first, ck_ctr;  // one-pass radius: result chunks (ck_next has one word per chunk)
     DevBuf knn_fb;  // group kNN fallback list, one entry per query position
     DevBuf knn_heads;  // group kNN: the heads' largest k-th distances (f64 per head)
+    DevBuf hash_out;   // oct_engine_copy_radius_hash's counts and hashes before they go to the host
     // the growable device arrays above come from this pool in stream order (cudaMallocFromPoolAsync /
     // cudaFreeAsync on `stream`), so growing one never waits for the device: with batches of other engines
     // running, a cudaFree / cudaMalloc would wait for all of them
@@ -880,7 +902,8 @@ int oct_engine_destroy(oct_engine e) {
         for (DevBuf* b : fixed) b->release();
         DevBuf* pooled[] = {&e->desc, &e->keys[0], &e->keys[1], &e->ord[0], &e->ord[1], &e->sort_status,
                             &e->counts, &e->offs, &e->out, &e->knn_idx, &e->knn_d2, &e->knn_counts, &e->totals,
-                            &e->ck_pool, &e->ck_next, &e->ck_first, &e->ck_ctr, &e->knn_fb, &e->knn_heads};
+                            &e->ck_pool, &e->ck_next, &e->ck_first, &e->ck_ctr, &e->knn_fb, &e->knn_heads,
+                            &e->hash_out};
         for (DevBuf* b : pooled) {
             if (b->ptr && e->stream) cudaFreeAsync(b->ptr, e->stream);
             b->ptr = nullptr;
@@ -1037,6 +1060,38 @@ int oct_engine_copy_radius(oct_engine e, const oct_request_place* pl, uint64_t* 
     return OCT_OK;
 }
 
+int oct_engine_copy_radius_hash(oct_engine e, const oct_request_place* pl, uint64_t* counts, uint64_t* hashes,
+                                uint32_t flags) {
+    if (!e || !pl) return OCT_ERR_INVALID_ARG;
+    if (e->in_flight || !e->have_results) return fail(e, OCT_ERR_STATE, "no completed batch");
+    const uint64_t nq = pl->nq;
+    if (nq == 0) return OCT_OK;
+    if (!counts || !hashes) return fail(e, OCT_ERR_INVALID_ARG, "counts or hashes is NULL");
+    if (pl->q_begin + nq > e->n_radius)
+        return fail(e, OCT_ERR_INVALID_ARG, "place is not a radius request of the last batch");
+    DeviceGuardE g(e->device);
+    const bool dev = (flags & OCT_MEM_DEVICE) != 0;
+    unsigned long long* dc = reinterpret_cast<unsigned long long*>(counts);
+    unsigned long long* dh = reinterpret_cast<unsigned long long*>(hashes);
+    if (!dev) {
+        int st;
+        if ((st = grow(e, e->hash_out, 16 * nq)) != OCT_OK) return st;
+        dc = e->hash_out.as<unsigned long long>();
+        dh = dc + nq;
+    }
+    const uint64_t want = (nq + 7) / 8;
+    const uint64_t cap = (uint64_t)e->sms * 8;
+    k_csr_hash<<<(unsigned)(want < cap ? want : cap), 256, 0, e->stream>>>(
+        e->offs.as<unsigned long long>() + pl->q_begin, e->out.as<uint32_t>(), nq, dc, dh);
+    EK(cudaGetLastError());
+    if (!dev) {
+        EK(cudaMemcpyAsync(counts, dc, 8 * nq, cudaMemcpyDeviceToHost, e->stream));
+        EK(cudaMemcpyAsync(hashes, dh, 8 * nq, cudaMemcpyDeviceToHost, e->stream));
+    }
+    EK(cudaStreamSynchronize(e->stream));
+    return OCT_OK;
+}
+
 int oct_engine_copy_knn(oct_engine e, const oct_request_place* pl, uint32_t k, uint32_t* idx, double* d2,
                         uint32_t* counts, uint32_t flags) {
     if (!e || !pl) return OCT_ERR_INVALID_ARG;
@@ -1084,7 +1139,7 @@ int oct_engine_memory(oct_engine e, uint64_t* bytes) {
                             &e->sort_status, &e->epoch, &e->counts, &e->offs, &e->part, &e->out, &e->knn_idx,
                             &e->knn_d2, &e->knn_counts, &e->ctrs, &e->stats, &e->summary, &e->totals,
                             &e->ck_pool, &e->ck_next, &e->ck_first, &e->ck_ctr, &e->knn_fb,
-                          &e->knn_heads};
+                            &e->knn_heads, &e->hash_out};
     uint64_t s = 0;
     for (const DevBuf* b : bufs) s += b->bytes;
     *bytes = s;

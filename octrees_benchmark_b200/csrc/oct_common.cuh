@@ -24,6 +24,15 @@ constexpr uint32_t kSpinLimit = 1u << 26;
 
 __device__ __forceinline__ void set_err(uint32_t* err, uint32_t bits) { atomicOr(err, bits); }
 
+// splitmix64's output function: the term of one neighbour index in the
+// order-independent set hash of oct_radius_hash (the sum of the terms mod 2^64).
+__device__ __forceinline__ unsigned long long mix64(unsigned long long z) {
+    z += 0x9E3779B97F4A7C15ull;
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    return z ^ (z >> 31);
+}
+
 __device__ __forceinline__ uint32_t lanemask_lt() {
     uint32_t m;
     asm volatile("mov.u32 %0, %%lanemask_lt;" : "=r"(m));

@@ -862,14 +862,6 @@ __global__ void __launch_bounds__(256) k_chunk_compact(const unsigned long long*
     }
 }
 
-// splitmix64's output function (the set hash's term for one neighbour index).
-__device__ __forceinline__ unsigned long long mix64(unsigned long long z) {
-    z += 0x9E3779B97F4A7C15ull;
-    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
-    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
-    return z ^ (z >> 31);
-}
-
 // One warp per query: the sum of mix64 over the query's result chain (the
 // count is the search's), instead of moving the chain into a CSR array.
 __global__ void __launch_bounds__(256) k_chunk_hash(const unsigned long long* __restrict__ counts,

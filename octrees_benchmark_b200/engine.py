@@ -150,6 +150,15 @@ class BatchEngine:
                                                      idx.shape[0], 0), self._h, "oct_engine_copy_radius")
         return offs, idx[: place.n_results]
 
+    def radius_hash_result(self, place: OctRequestPlace):
+        """(counts uint64[nq], hashes uint64[nq]) of a radius request, computed on the device: each
+        centre's neighbour count and the sum of splitmix64's output function over its neighbours."""
+        cnt = np.zeros(place.nq, np.uint64)
+        hsh = np.zeros(place.nq, np.uint64)
+        _engine_check(self._L.oct_engine_copy_radius_hash(self._h, C.byref(place), cnt.ctypes.data,
+                                                          hsh.ctypes.data, 0), self._h, "oct_engine_copy_radius_hash")
+        return cnt, hsh
+
     def knn_result(self, place: OctRequestPlace, k: int):
         """(idx uint32[nq, k], d2 float64[nq, k], counts uint32[nq]) of a kNN request, host arrays."""
         idx = np.zeros((place.nq, k), np.uint32)

@@ -63,3 +63,29 @@ def test_hash_equals_lists_and_device_buffers(clouds):
     assert np.array_equal(dh.cpu().numpy().view(np.uint64), want_h)
     e0c, e0h = oc.radius_hash(np.zeros((0, 3)), 2.5, "sphere", "neighborsPrune")
     assert len(e0c) == 0 and len(e0h) == 0
+
+
+def test_engine_hash_copy_out(clouds):
+    """oct_engine_copy_radius_hash: the counts and hashes of a batched radius request equal the
+    single-cloud oct_radius_hash ones (and thus the reference's)."""
+    torch = pytest.importorskip("torch")
+    from octrees_benchmark_b200.engine import BatchEngine, Request
+
+    oc, R = clouds
+    sxyz = R.points()[0]
+    q = np.ascontiguousarray(sxyz[::29])
+    dq = torch.from_numpy(q).cuda()
+    eng = BatchEngine()
+    try:
+        places = eng.run([Request(oc, "radius", dq, radius=3.0, kernel="cube", algo="neighbors"),
+                          Request(oc, "knn", dq, k=8),
+                          Request(oc, "radius", dq[:1000].contiguous(), radius=1.5, kernel="sphere")])
+        for pl, (r, kern, algo, n) in zip((places[0], places[2]), ((3.0, "cube", "neighbors", len(q)),
+                                                                 (1.5, "sphere", "neighborsPrune", 1000))):
+            gc, gh = eng.radius_hash_result(pl)
+            wc, wh = oc.radius_hash(q[:n], r, kern, algo)
+            assert np.array_equal(gc, wc) and np.array_equal(gh, wh)
+        with pytest.raises(capi.OctError):
+            eng.radius_hash_result(places[1])  # a kNN request's place
+    finally:
+        eng.close()
