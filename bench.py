@@ -772,18 +772,25 @@ def run_b200(args, rank, world, local_rank):
         eng2 = BatchEngine(device=dev, reserve_results=cap)
         eng2.set_config(**eng_cfg)
         engs = [eng, eng2]
+        # three device input sets: step s reads set s % 3, so the next step's centres are copied in while the
+        # step before is still computing (its own set) and the one before that has its results copied out
         dbufs = [(torch.empty((Q_RADIUS, 3), dtype=torch.float64, device="cuda"),
-                  torch.empty((Q_KNN, 3), dtype=torch.float64, device="cuda")) for _ in range(2)]
+                  torch.empty((Q_KNN, 3), dtype=torch.float64, device="cuda")) for _ in range(3)]
         reqs_e2e = [[Request(proxy, "radius", qrd, radius=RADIUS, kernel="sphere", algo="neighborsPrune"),
                      Request(proxy, "knn", qkd, k=KNN_K)] for qrd, qkd in dbufs]
+        in_ev = [torch.cuda.Event() for _ in range(3)]
         torch.cuda.synchronize()
 
-        def copy_in(s_, slot):
-            qrd, qkd = dbufs[slot]
+        def copy_in_async(s_):
+            qrd, qkd = dbufs[s_ % 3]
             with torch.cuda.stream(stream):
                 qrd.copy_(qrh_all[s_], non_blocking=True)
                 qkd.copy_(qkh_all[s_], non_blocking=True)
-            stream.synchronize()
+                in_ev[s_ % 3].record(stream)
+
+        def copy_in(s_, slot=None):
+            copy_in_async(s_)
+            in_ev[s_ % 3].synchronize()
 
         def copy_out(e):
             pl = e.wait()
@@ -794,21 +801,26 @@ def run_b200(args, rank, world, local_rank):
             return pl
 
         def pipelined(first, count):
-            pl = None
+            # step j: its centres are already in (copied while step j - 1 ran), submit it, start copying step
+            # j + 1's centres in (set (j + 1) % 3: step j - 2 used it and its results are out), then copy step
+            # j - 1's results out while step j computes
+            copy_in_async(first)
             for j in range(count):
                 slot = j % 2
-                copy_in(first + j, slot)
-                engs[slot].submit(reqs_e2e[slot])
+                in_ev[(first + j) % 3].synchronize()
+                engs[slot].submit(reqs_e2e[(first + j) % 3])
+                if j + 1 < count:
+                    copy_in_async(first + j + 1)
                 if j > 0:
-                    pl = copy_out(engs[1 - slot])
+                    copy_out(engs[1 - slot])
             return copy_out(engs[(count - 1) % 2])
 
         et = []  # serial steps
         for s_ in range(n_all):
             torch.cuda.synchronize()
             t0 = time.perf_counter()
-            copy_in(s_, 0)
-            eng.submit(reqs_e2e[0])
+            copy_in(s_)
+            eng.submit(reqs_e2e[s_ % 3])
             pl = copy_out(eng)
             t1 = time.perf_counter()
             if s_ >= args.warmup:
@@ -829,7 +841,8 @@ def run_b200(args, rank, world, local_rank):
                       "serial_step_ms_all": [round(1e3 * v, 2) for v in et],
                       "serial_qps": world * (Q_RADIUS + Q_KNN) / statistics.median(et),
                       "timing": "wall clock over the timed steps; pipelined: two engines alternate (each step's "
-                                "results copied out while the next step computes), fill and drain included"}
+                                "results copied out while the next step computes and the one after is copied in), "
+                                "fill and drain included"}
         eng2.close()
     elif not args.no_e2e:
         qrh = torch.empty((Q_RADIUS, 3), dtype=torch.float64).pin_memory().numpy()
