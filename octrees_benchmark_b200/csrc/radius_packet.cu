@@ -482,31 +482,18 @@ __global__ void __launch_bounds__(kPkThreads) k_radius_packet(PacketArgs a) {
                             pz = RQV(zs)[idx];
                         }
                     }
-                    uint32_t rem = mask;
-                    while (rem) {
-                        const int j = __ffs(rem) - 1;
-                        rem &= rem - 1;
-                        bool in;
-                        if constexpr (F32) {
-                            const int r = in_range ? f32_test<KT>(get_ctx<KT>(s_ctx[warp][j]), pf) : 0;
-                            if (r < 0) {  // inside the error band: the reference's FP64 expression decides
-                                in = inside_of<KT>(s_qp[warp], j, RQV(xs)[idx], RQV(ys)[idx], RQV(zs)[idx]);
-                                ++n_retests;
-                            } else {
-                                in = r > 0;
-                            }
-                        } else {
-                            in = in_range && inside_of<KT>(s_qp[warp], j, px, py, pz);
-                        }
+                    // query j's hits among the lanes' points: appended to its chunks, or stored ascending
+                    // in one coalesced store (FILL), and counted
+                    auto take = [&](int j, bool in) {
                         const uint32_t hb = __ballot_sync(0xffffffffu, in);
                         if constexpr (CHUNK) {
                             if (hb) {
                                 const ChunkPos p = chunk_reserve(j, __popc(hb));
                                 if (in) chunk_store(p, __popc(hb & lanemask_lt()), idx);
                             }
-                            continue;
+                            return;
                         }
-                        if (FILL && hb) {  // query j's hits, ascending, in one coalesced store
+                        if (FILL && hb) {
                             const unsigned long long o0 = __shfl_sync(0xffffffffu, base + cnt, j);
                             if (in) {
                                 const unsigned long long o = o0 + __popc(hb & lanemask_lt());
@@ -515,6 +502,32 @@ __global__ void __launch_bounds__(kPkThreads) k_radius_packet(PacketArgs a) {
                             }
                         }
                         if (lane == j) cnt += __popc(hb);
+                    };
+                    uint32_t rem = mask;
+                    while (rem) {
+                        const int j = __ffs(rem) - 1;
+                        rem &= rem - 1;
+                        if constexpr (F32) {
+                            bool in;
+                            const int r = in_range ? f32_test<KT>(get_ctx<KT>(s_ctx[warp][j]), pf) : 0;
+                            if (r < 0) {  // inside the error band: the reference's FP64 expression decides
+                                in = inside_of<KT>(s_qp[warp], j, RQV(xs)[idx], RQV(ys)[idx], RQV(zs)[idx]);
+                                ++n_retests;
+                            } else {
+                                in = r > 0;
+                            }
+                            take(j, in);
+                        } else {
+                            // two queries at a time: their FP64 tests are independent, so their latencies
+                            // overlap instead of adding up
+                            const bool two = rem != 0;
+                            const int j2 = two ? __ffs(rem) - 1 : j;
+                            if (two) rem &= rem - 1;
+                            const bool in = in_range && inside_of<KT>(s_qp[warp], j, px, py, pz);
+                            const bool in2 = two && in_range && inside_of<KT>(s_qp[warp], j2, px, py, pz);
+                            take(j, in);
+                            if (two) take(j2, in2);
+                        }
                     }
                     if (lane == 0) n_tests += (unsigned long long)__popc(mask) * ((rg.y - b < 32u) ? (rg.y - b) : 32u);
                 }
