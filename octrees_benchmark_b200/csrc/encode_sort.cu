@@ -43,6 +43,8 @@ constexpr int kSortWarps = kSortThreads / 32;
 // 384 x 8 keys measured 1.8 % slower on the 10M-point build)
 constexpr int kSortBlocksPerSM = 2;
 static_assert(kSortThreads >= 256, "threads 0..255 own one digit each");
+// predecessor tiles a digit's look-back reads per round trip
+constexpr int kLookAhead = 4;
 constexpr int kEncGridPerSM = 4;
 
 // look-back status word: flag (2 bits) | epoch (22 bits) | count (40 bits)
@@ -390,25 +392,40 @@ __global__ void __launch_bounds__(kSortThreads, kSortBlocksPerSM) k_onesweep(con
             tstart[d] = pre + x - total;
         }
     }
-    // decoupled look-back over the preceding tiles (bounded wait)
+    // decoupled look-back over the preceding tiles (bounded wait); each round
+    // reads kLookAhead predecessors at once and sums them nearest first up to
+    // the first prefix, or up to one that has not published
     unsigned long long excl = 0;
     if (d < 256 && tile > 0) {
         int64_t t = (int64_t)tile - 1;
         uint32_t spins = 0;
         while (t >= 0) {
-            const unsigned long long s = ld_volatile_u64(status + (uint64_t)t * 256 + d);
-            const unsigned long long flag = s & (3ull << 62);
-            if ((s & kEpochMask) != ep || flag == 0) {
+            unsigned long long s[kLookAhead];
+#pragma unroll
+            for (int q = 0; q < kLookAhead; ++q)  // tile 0 is a prefix: a walk never passes below it
+                s[q] = (t - q >= 0) ? ld_volatile_u64(status + (uint64_t)(t - q) * 256 + d) : 0ull;
+            int used = 0;
+            bool found = false;
+#pragma unroll
+            for (int q = 0; q < kLookAhead; ++q) {
+                const unsigned long long flag = s[q] & (3ull << 62);
+                if ((s[q] & kEpochMask) != ep || flag == 0) break;
+                excl += s[q] & kCountMask;
+                ++used;
+                if (flag == kFlagPrefix) {
+                    found = true;
+                    break;
+                }
+            }
+            if (found) break;
+            t -= used;
+            if (used == 0) {
                 if (++spins > kSpinLimit) {
                     set_err(err, kErrSpinLimit);
                     break;
                 }
                 __nanosleep(32);
-                continue;
             }
-            excl += s & kCountMask;
-            if (flag == kFlagPrefix) break;
-            --t;
         }
         st_volatile_u64(my, kFlagPrefix | ep | (excl + total));
     }

@@ -36,7 +36,7 @@ namespace octb {
 
 namespace {
 
-constexpr int kBuildThreads = 256;
+constexpr int kBuildThreads = 1024;
 constexpr int kBuildWarps = kBuildThreads / 32;
 
 struct FrontierNode {
@@ -95,8 +95,26 @@ __device__ void grid_barrier(BuildCtl* ctl, uint32_t* err) {
     __syncthreads();
 }
 
+// lower_bound over a child's parent range.  Ranges longer than kKaryMin are
+// first narrowed kKaryWays-fold per step by kKaryWays - 1 independent probes
+// (one round trip each step instead of log2(kKaryWays) dependent ones: the top
+// levels' searches span millions of keys), then bisected.
+constexpr uint32_t kKaryWays = 8;
+constexpr uint32_t kKaryMin = 256;
+static_assert(kKaryMin >= kKaryWays, "a k-ary step needs a stride of at least one key");
+
 __device__ __forceinline__ uint32_t lower_bound_keys(const uint64_t* __restrict__ keys, uint32_t lo, uint32_t hi,
                                                      uint64_t v) {
+    while (hi - lo > kKaryMin) {
+        // keys [lo, hi) ascending; the answer lies in [lo, hi]
+        const uint32_t s = (hi - lo) / kKaryWays;
+        uint32_t below = 0;  // probes lo + p s (p = 1 .. ways - 1) under v: a prefix of them
+#pragma unroll
+        for (uint32_t p = 1; p < kKaryWays; ++p) below += keys[lo + p * s] < v ? 1u : 0u;
+        const uint32_t nlo = below ? lo + below * s + 1 : lo;
+        if (below < kKaryWays - 1) hi = lo + (below + 1) * s;
+        lo = nlo;
+    }
     while (lo < hi) {
         const uint32_t mid = lo + ((hi - lo) >> 1);
         if (keys[mid] < v) lo = mid + 1;
