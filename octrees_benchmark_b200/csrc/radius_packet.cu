@@ -840,12 +840,13 @@ cudaError_t launch_pk_a(const PacketArgs& a, int algo, int mode, bool fp32, int 
 }
 
 // Each radius query's chain of result chunks into its CSR slot.  A warp takes
-// 32 queries: their counts, offsets and first two chunks come in two coalesced
-// round trips; then the first two chunks of kCompactBatch queries at a time are
-// loaded before any is stored, so their loads overlap; chains longer than two
-// chunks are walked on one chunk at a time.
+// S queries at a time (S from 4 up to 32, as many as keep every warp busy):
+// their counts, offsets and first chunks come in one coalesced round trip; then
+// the chains of kCompactBatch queries are walked in lockstep, each step loading
+// one chunk of every one of them (and their next links) before storing any, so
+// the four latency chains overlap.
 constexpr int kCompactBatch = 4;
-static_assert(kChunk == 64, "the first two chunks are four 32-entry rows");
+static_assert(kChunk == 64, "a chunk is two 32-entry rows");
 
 __global__ void __launch_bounds__(256) k_chunk_compact(const unsigned long long* __restrict__ counts,
                                                        const unsigned long long* __restrict__ offs,
@@ -857,78 +858,72 @@ __global__ void __launch_bounds__(256) k_chunk_compact(const unsigned long long*
     if (d_n) n = *d_n;
     const int lane = threadIdx.x & 31;
     const uint64_t nwarps = ((uint64_t)gridDim.x * blockDim.x) >> 5;
+    uint32_t S = kCompactBatch;
+    while (S < 32 && (uint64_t)S * nwarps < n) S <<= 1;
     bool bad = false;  // a chain cut short by a pool overflow (reported by the search kernel), or no room
-    for (uint64_t q0 = (((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * 32; q0 < n; q0 += nwarps * 32) {
+    for (uint64_t q0 = (((uint64_t)blockIdx.x * blockDim.x + threadIdx.x) >> 5) * S; q0 < n; q0 += nwarps * S) {
         const uint64_t q = q0 + lane;
         unsigned long long cnt = 0, o = 0;
-        uint32_t c0 = kNoChunk, c1 = kNoChunk;
-        if (q < n) {
+        uint32_t c0 = kNoChunk;
+        if ((uint32_t)lane < S && q < n) {
             cnt = counts[q];
             if (cnt) {
                 o = offs[q];
                 c0 = first[q];
             }
         }
-        if (cnt > kChunk && c0 < chunk_cap) c1 = next[c0];
         uint32_t todo = __ballot_sync(0xffffffffu, cnt != 0);
         while (todo) {
-            int js[kCompactBatch];
+            unsigned long long cj[kCompactBatch], dst[kCompactBatch], done[kCompactBatch];
+            uint32_t cur[kCompactBatch];
 #pragma unroll
             for (int b = 0; b < kCompactBatch; ++b) {
-                js[b] = todo ? __ffs(todo) - 1 : -1;
+                const int j = todo ? __ffs(todo) - 1 : -1;
                 todo &= todo - 1;
+                const unsigned long long cb = __shfl_sync(0xffffffffu, cnt, j & 31);
+                cj[b] = j >= 0 ? cb : 0ull;
+                dst[b] = __shfl_sync(0xffffffffu, o, j & 31);
+                cur[b] = __shfl_sync(0xffffffffu, c0, j & 31);
+                done[b] = 0;
             }
-            uint32_t val[kCompactBatch][4];
-            unsigned long long dst[kCompactBatch];
-            unsigned long long cj[kCompactBatch];
+            for (;;) {  // one chunk of every unfinished chain per step (warp-uniform)
+                bool any = false;
 #pragma unroll
-            for (int b = 0; b < kCompactBatch; ++b) {
-                const int j = js[b] & 31;
-                const unsigned long long cb = __shfl_sync(0xffffffffu, cnt, j);
-                cj[b] = js[b] >= 0 ? cb : 0ull;
-                dst[b] = __shfl_sync(0xffffffffu, o, j);
-                const uint32_t a0 = __shfl_sync(0xffffffffu, c0, j), a1 = __shfl_sync(0xffffffffu, c1, j);
+                for (int b = 0; b < kCompactBatch; ++b) any = any || done[b] < cj[b];
+                if (!any) break;
+                uint32_t v[kCompactBatch][2], nx[kCompactBatch];
 #pragma unroll
-                for (int h = 0; h < 4; ++h) {
-                    const uint32_t t = 32u * h + lane;
-                    const uint32_t ch = h < 2 ? a0 : a1;
-                    val[b][h] = 0;
-                    if (t < cj[b]) {
-                        if (ch < chunk_cap) val[b][h] = pool[(uint64_t)ch * kChunk + (t & (kChunk - 1))];
-                        else bad = true;
+                for (int b = 0; b < kCompactBatch; ++b) {
+                    v[b][0] = v[b][1] = 0;
+                    nx[b] = kNoChunk;
+                    if (done[b] < cj[b] && cur[b] < chunk_cap) {
+#pragma unroll
+                        for (int h = 0; h < 2; ++h) {
+                            const uint32_t t = 32u * h + lane;
+                            if (done[b] + t < cj[b]) v[b][h] = pool[(uint64_t)cur[b] * kChunk + t];
+                        }
+                        if (done[b] + kChunk < cj[b]) nx[b] = next[cur[b]];
                     }
                 }
-            }
 #pragma unroll
-            for (int b = 0; b < kCompactBatch; ++b) {
-#pragma unroll
-                for (int h = 0; h < 4; ++h) {
-                    const uint32_t t = 32u * h + lane;
-                    if (t < cj[b]) {
-                        const unsigned long long w = dst[b] + t;
-                        if (w < out_cap) out[w] = val[b][h];
-                        else bad = true;
-                    }
-                }
-            }
-            // the rest of chains longer than two chunks
-#pragma unroll
-            for (int b = 0; b < kCompactBatch; ++b) {
-                uint32_t c = __shfl_sync(0xffffffffu, c1, js[b] & 31);
-                if (cj[b] <= 2 * kChunk) continue;  // warp-uniform
-                for (unsigned long long done = 2 * kChunk; done < cj[b];) {
-                    c = c < chunk_cap ? next[c] : kNoChunk;
-                    if (c >= chunk_cap) {
+                for (int b = 0; b < kCompactBatch; ++b) {
+                    if (done[b] >= cj[b]) continue;
+                    if (cur[b] >= chunk_cap) {
                         bad = true;
-                        break;
+                        done[b] = cj[b];
+                        continue;
                     }
-                    const unsigned long long m = (cj[b] - done < kChunk) ? (cj[b] - done) : kChunk;
-                    for (uint32_t t = lane; t < m; t += 32) {
-                        const unsigned long long w = dst[b] + done + t;
-                        if (w < out_cap) out[w] = pool[(uint64_t)c * kChunk + t];
-                        else bad = true;
+#pragma unroll
+                    for (int h = 0; h < 2; ++h) {
+                        const uint32_t t = 32u * h + lane;
+                        if (done[b] + t < cj[b]) {
+                            const unsigned long long w = dst[b] + done[b] + t;
+                            if (w < out_cap) out[w] = v[b][h];
+                            else bad = true;
+                        }
                     }
-                    done += m;
+                    done[b] = (cj[b] - done[b] > kChunk) ? done[b] + kChunk : cj[b];
+                    cur[b] = nx[b];
                 }
             }
         }
@@ -1076,7 +1071,7 @@ cudaError_t launch_chunk_compact(int device, cudaStream_t s, const unsigned long
                                  uint64_t out_capacity, uint64_t n, const uint64_t* d_n, uint32_t* d_err) {
     if (!d_n && n == 0) return cudaSuccess;
     const uint64_t cap = (uint64_t)sm_count_p(device) * 8;
-    const uint64_t want = d_n ? cap : (n + 255) / 256;  // 8 warps of 32 queries per block
+    const uint64_t want = d_n ? cap : (n + 31) / 32;  // 8 warps of at least 4 queries per block
     const int grid = (int)(want < cap ? (want ? want : 1) : cap);
     k_chunk_compact<<<grid, 256, 0, s>>>(d_counts, d_offsets, chunks.first, chunks.next, chunks.pool, chunks.cap,
                                          d_out, out_capacity, n, d_n, d_err);
