@@ -800,7 +800,16 @@ def run_b200(args, rank, world, local_rank):
                                               kcnt_h.ctypes.data, 0), None, "e2e copy kNN")
             return pl
 
-        def pipelined(first, count):
+        copy_out_s = []  # wall time of each copy-out call inside the timed pipelined run
+
+        def timed_copy_out(e, record):
+            t0_ = time.perf_counter()
+            pl_ = copy_out(e)
+            if record:
+                copy_out_s.append(time.perf_counter() - t0_)
+            return pl_
+
+        def pipelined(first, count, record=False):
             # step j: its centres are already in (copied while step j - 1 ran), submit it, start copying step
             # j + 1's centres in (set (j + 1) % 3: step j - 2 used it and its results are out), then copy step
             # j - 1's results out while step j computes
@@ -812,8 +821,8 @@ def run_b200(args, rank, world, local_rank):
                 if j + 1 < count:
                     copy_in_async(first + j + 1)
                 if j > 0:
-                    copy_out(engs[1 - slot])
-            return copy_out(engs[(count - 1) % 2])
+                    timed_copy_out(engs[1 - slot], record)
+            return timed_copy_out(engs[(count - 1) % 2], record)
 
         et = []  # serial steps
         for s_ in range(n_all):
@@ -828,7 +837,7 @@ def run_b200(args, rank, world, local_rank):
         pipelined(0, args.warmup)  # engine 2's graphs captured, both warm
         torch.cuda.synchronize()
         t0 = time.perf_counter()
-        pl = pipelined(args.warmup, args.steps)
+        pl = pipelined(args.warmup, args.steps, record=True)
         t_pipe = (time.perf_counter() - t0) / args.steps
         h2d = 24 * (Q_RADIUS + Q_KNN)
         d2h = 8 * (Q_RADIUS + 1) + 4 * int(pl[0].n_results) + Q_KNN * KNN_K * 12 + 4 * Q_KNN
@@ -838,6 +847,8 @@ def run_b200(args, rank, world, local_rank):
         e2e_val = world * (Q_RADIUS + Q_KNN) / float(e2e_t.item())
         e2e_detail = {"api": "oct_engine_submit / oct_engine_wait + oct_engine_copy_radius / oct_engine_copy_knn",
                       "pipelined_step_ms": round(1e3 * t_pipe, 3),
+                      # one step's copy-out call (455 MB at this size), the step's floor once the link is busy
+                      "copy_out_ms_median": round(1e3 * statistics.median(copy_out_s), 3) if copy_out_s else None,
                       "serial_step_ms_all": [round(1e3 * v, 2) for v in et],
                       "serial_qps": world * (Q_RADIUS + Q_KNN) / statistics.median(et),
                       "timing": "wall clock over the timed steps; pipelined: two engines alternate (each step's "

@@ -1054,7 +1054,8 @@ int oct_engine_copy_radius(oct_engine e, const oct_request_place* pl, uint64_t* 
     EK(cudaStreamSynchronize(e->stream));
     if (offsets && !dev && nq) {
         const uint64_t b = offsets[0];
-        for (uint64_t i = 0; i <= nq; ++i) offsets[i] -= b;
+        if (b != 0)  // the batch's first radius request starts at 0 already
+            for (uint64_t i = 0; i <= nq; ++i) offsets[i] -= b;
     }
     if (idx && !fits) return fail(e, OCT_ERR_CAPACITY, "idx_capacity smaller than the request's results");
     return OCT_OK;
