@@ -1,6 +1,6 @@
 """The large skewed cloud at full size against the compiled reference (opt-in:
 the reference's copy of the cloud holds tens of GB of host memory and the
-run takes about a minute (53 s on a B200 box with 196 GB), so it runs only with
+run takes about a minute (53 s on a B200 machine with 196 GB of RAM), so it runs only with
 OCT_LARGE=1, e.g. `OCT_LARGE=1 python -m pytest tests/test_gpu_large.py -m gpu`).
 
 500,000,000 points on a 10 km tile (seed 3, generated on the device: rural
