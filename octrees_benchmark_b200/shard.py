@@ -5,7 +5,9 @@ rank; every rank answers its slice on its own replica of the cloud (built from
 the same points, or restored from a checkpoint) and the slices' results are
 gathered.  The search itself has no collective; the gather is two all_gather
 calls (sizes, then the padded results).  With the NCCL backend the tensors are
-CUDA tensors, with gloo host tensors.
+CUDA tensors, with gloo host tensors.  A replica either builds from the same
+points on every rank or is restored from the checkpoint one rank built and
+broadcast (broadcast_checkpoint).
 
 The reference has no counterpart: it answers queries on OpenMP threads of one
 host (neighbor_benchmarks.hpp:518-567).
@@ -60,3 +62,53 @@ def gather_rows(*tensors, group=None):
     import torch
 
     return tuple(torch.cat(_gather_padded(t, group)) for t in tensors)
+
+
+def broadcast_checkpoint(ck, src: int = 0, group=None):
+    """A built cloud's checkpoint (LinearOctree.checkpoint(): a dict of host arrays) from rank `src` (its
+    rank in the default group) to every rank, so that one rank sorts and builds and the others restore
+    the same tree with LinearOctree.from_checkpoint instead of building it again.  Ranks other than src
+    pass None.  Returns the checkpoint on every rank, each value a numpy array (0-d for scalars).
+
+    One broadcast carries the names, dtypes and shapes, then one broadcast per non-empty array carries its
+    raw bytes, so every dtype crosses unchanged.  With the NCCL backend the bytes go through this rank's
+    current CUDA device (over NVLink between the GPUs), with gloo they stay on the host.  Every rank makes
+    the same calls in the same order."""
+    import numpy as np
+    import torch
+    import torch.distributed as dist
+
+    is_src = dist.get_rank() == src
+    if is_src:
+        if ck is None:
+            raise ValueError("the source rank must pass the checkpoint")
+        arrays = {}
+        for k, v in ck.items():
+            a = np.asarray(v)
+            arrays[str(k)] = a if a.flags.c_contiguous else np.ascontiguousarray(a)  # keeps 0-d scalars 0-d
+        meta = [(k, a.dtype.str, tuple(a.shape)) for k, a in arrays.items()]
+    else:
+        arrays, meta = {}, None
+    box = [meta]
+    dist.broadcast_object_list(box, src=src, group=group)
+    meta = box[0]
+    dev = torch.device("cuda", torch.cuda.current_device()) if dist.get_backend(group) == "nccl" else None
+    out = {}
+    for name, dt, shape in meta:
+        dtype = np.dtype(dt)
+        nbytes = int(np.prod(shape, dtype=np.int64)) * dtype.itemsize
+        if nbytes == 0:
+            out[name] = np.zeros(shape, dtype)
+            continue
+        if is_src:
+            buf = torch.from_numpy(arrays[name].reshape(-1).view(np.uint8))
+        else:
+            buf = torch.empty(nbytes, dtype=torch.uint8)
+        moved = buf.to(dev) if dev is not None else buf
+        dist.broadcast(moved, src=src, group=group)
+        if is_src:
+            out[name] = arrays[name]
+        else:
+            host = moved.cpu() if dev is not None else moved
+            out[name] = host.numpy().view(dtype).reshape(shape).copy()
+    return out

@@ -70,3 +70,53 @@ def test_two_ranks_gather_equals_one_rank(tmp_path):
     out = str(tmp_path / "result.txt")
     mp.start_processes(_rank_main, args=(2, port, out), nprocs=2, join=True, start_method="spawn")
     assert open(out).read() == "ok"
+
+
+def _checkpoint_like(seed):
+    """A dict with a checkpoint's names and dtypes (0-d scalars, an empty array, 2-D arrays)."""
+    rng = np.random.default_rng(seed)
+    n, m = 1_003, 77
+    return dict(encoder=np.int32(5), max_points_leaf=np.uint32(64),
+                info=np.array([n, 60, 17, 77, 6], np.uint64), box=rng.random(12),
+                keys=np.sort(rng.integers(0, 1 << 63, n, dtype=np.uint64)),
+                perm=rng.permutation(n).astype(np.uint32), sorted_xyz=rng.random((n, 3)),
+                offsets=rng.integers(0, m, m, dtype=np.uint32), ranges=rng.integers(0, n, (m, 2), dtype=np.uint64),
+                centers=rng.random((m, 3)), radii=rng.random((7, 3)), half=rng.random(3),
+                empty=np.zeros((0, 3), np.float64))
+
+
+def _bcast_main(rank, world, port, out_path):
+    import torch.distributed as dist
+
+    from octrees_benchmark_b200.shard import broadcast_checkpoint
+
+    os.environ["MASTER_ADDR"] = "127.0.0.1"
+    os.environ["MASTER_PORT"] = str(port)
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        got = broadcast_checkpoint(_checkpoint_like(7) if rank == 1 else None, src=1)
+        want = _checkpoint_like(7)
+        ok = list(got) == list(want) and all(
+            got[k].dtype == np.asarray(want[k]).dtype and got[k].shape == np.asarray(want[k]).shape
+            and np.array_equal(got[k], want[k]) for k in want)
+        ok = ok and int(got["encoder"]) == 5 and got["encoder"].ndim == 0
+        with open(f"{out_path}.{rank}", "w") as f:
+            f.write("ok" if ok else "mismatch")
+    finally:
+        dist.destroy_process_group()
+
+
+def test_checkpoint_broadcast_reaches_every_rank_unchanged(tmp_path):
+    """One rank builds, the others restore: a checkpoint broadcast from rank 1 arrives on both ranks with
+    every name, dtype, shape and byte unchanged."""
+    pytest.importorskip("torch")
+    import socket
+
+    import torch.multiprocessing as mp
+
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    out = str(tmp_path / "bcast")
+    mp.start_processes(_bcast_main, args=(2, port, out), nprocs=2, join=True, start_method="spawn")
+    assert [open(f"{out}.{r}").read() for r in range(2)] == ["ok", "ok"]
